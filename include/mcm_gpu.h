@@ -1,0 +1,200 @@
+/*
+ * mcm_gpu.h -- C ABI of the B200 (sm_100a) SPH explicit step for MCM 2.07.
+ *
+ * The reference (MarkoTopalovic/MCMtop) has no plugin or FFI layer: its time
+ * loop MCM/mcm_solution.f90:37-138 calls argument-less subroutines that act on
+ * the module arrays of MCM/mcm_database.f90 (par, gpar, mcm_mat).  This ABI
+ * replaces the physics calls of that loop; the Fortran loop, its output,
+ * termination test and Ctrl-C handling stay on the host:
+ *
+ *   reference loop body (mcm_solution.f90)       this ABI
+ *   :41  mcm_neighbours  \
+ *   :45  mcm_strain       > mcm_gpu_step_a(h, dt, &critts)
+ *   :53  mcm_constitutive/
+ *   :58-62 dt update     (host, unchanged)
+ *   :69  mcm_momentum    \
+ *   :73  mcm_boundcond    > mcm_gpu_step_b(h, energies)
+ *   :77  mcm_calctotale  /
+ *   :81-108 output / termination / ctrl-c (host, unchanged)
+ *   :112 mcm_update_velocity \ mcm_gpu_step_c(h, dt, dtold, coord_maxmin)
+ *   :116 mcm_move            /
+ *
+ * mcm_gpu_run() fuses whole loop iterations (dt update on the device) for
+ * stretches with no output in between.
+ *
+ * Conventions: plain pointers and sizes; host arrays use the Fortran layout of
+ * the reference (vectors (3,np), tensors (3,3,np), column-major); particle ids
+ * are 1-based reference indices.  Host pointers are borrowed for the call only.
+ * Every entry point returns an mcm_gpu_status; the library never exits, aborts
+ * or traps a device.  One host thread per handle; handles are independent.
+ */
+#ifndef MCM_GPU_H
+#define MCM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCM_GPU_ABI_VERSION 1
+#define MCM_GPU_MAX_MATERIALS 16
+
+/* Status codes.  The reference's fatal paths call mcm_shutdown(2)
+ * (MCM/mcm_shutdown.f90); here they return a code instead. */
+typedef enum {
+    MCM_OK = 0,
+    MCM_ENBR_OVERFLOW = 1,     /* neighbour table too narrow; regrown and retried internally
+                                  (MCM/mcm_ll_neighbours.f90:44,301-309) */
+    MCM_EGHOST_OVERFLOW = 2,   /* ghost storage too small; regrown and retried internally
+                                  (MCM/mcm_ghost_setup.f90:269-282) */
+    MCM_ECOMPLEX_C = 3,        /* eos41 c^2 < 0 (MCM/mcm_eos41c.f90:282-288) */
+    MCM_ECAP_NOCONV = 4,       /* cap model Newton loop did not converge (MCM/mcm_f3dm25.f90) */
+    MCM_ETIMEOUT = 5,          /* a bounded device wait ran out */
+    MCM_ECUDA = 6,             /* CUDA runtime error (see mcm_gpu_last_error) */
+    MCM_ENOMEM = 7,            /* device allocation failed */
+    MCM_EINVAL = 8,            /* bad argument */
+    MCM_EUNSUPPORTED = 9,      /* option outside the ported path (e.g. contacttype > 0) */
+    MCM_EGRID_OVERFLOW = 10,   /* cell grid larger than its storage; regrown and retried internally */
+    MCM_EGHOST_LAYER = 11,     /* a real particle lies in a ghost-layer cell (undefined in the reference) */
+    MCM_EGRID_TOO_LARGE = 12   /* the linked-list grid would exceed 2^31 cells
+                                  (MCM/mcm_setuplist.f90:295-302 shuts down) */
+} mcm_gpu_status;
+
+/* Arithmetic of the step. */
+typedef enum {
+    MCM_PREC_FP64_EXACT = 0,   /* FP64, no fused multiply-add, reference accumulation order */
+    MCM_PREC_FP64 = 1,         /* FP64 with fused multiply-add */
+    MCM_PREC_MIXED = 2         /* FP32 pair sums with Kahan compensation and FP32 constitutive
+                                  update on cell-relative positions; FP64 position/velocity
+                                  integration, energy and critical-timestep reductions */
+} mcm_gpu_precision;
+
+/* One material, as the reference holds it after mcm_matin, the mcm_sets routines and mcm_calcg:
+ * `type material` of MCM/mcm_database.f90:235-257. */
+typedef struct {
+    int model;                 /* 1, 3, 9, 10 (4: cap model) */
+    int eos;                   /* 1, 4, 13, 28, 41 (models 9, 10) */
+    int visc_type;             /* 1: nodal artificial viscosity */
+    double rho;                /* reference density (rho0 of every particle of this material) */
+    double g;                  /* shear modulus (mcm_calcg) */
+    double av_l, av_q;         /* artificial viscosity coefficients */
+    double mass;               /* total material mass (massopt 0) */
+    double h;                  /* smoothing length */
+    double rho_min, rho_max;   /* density limits */
+    double strinput[48];       /* constitutive constants after mcm_sets* */
+    double eosinput[24];       /* EOS constants */
+} mcm_gpu_material;
+
+/* Run options: control cards (MCM/mcm_control_v2.f90:88-124), boundary planes
+ * (MCM/mcm_inp_symmetry_v2.f90:115-137), base accelerations. */
+typedef struct {
+    int ndim;                  /* 3 (1-D and 2-D return MCM_EUNSUPPORTED) */
+    int disctype;              /* 0 basic SPH, 1 Bonet mixed-corrected SPH */
+    int tcrit_opt;             /* 0 DYNA formula, 1 h/(c+|v|), 2 mindist/(c+|v|) */
+    int contacttype;           /* must be 0 (kernel contact) */
+    int h_opt;                 /* must be 0 (constant h) */
+    int veloc_opt;             /* must be 0 (no XSPH) */
+    int krtype;                /* 1: cubic B-spline */
+    int drelax;                /* dynamic relaxation active */
+    double drelax_scale;
+    int boundary;              /* mcm_boundary: ghost planes active */
+    int boundary_code[6];      /* (side,dim) as mcm_boundary_code(2,3): xmin xmax ymin ymax zmin zmax;
+                                  0 none, 1 symmetry, 2 periodic */
+    double boundary_x[6];      /* plane coordinates, same order */
+    int baseaccel;
+    double base_a[3];
+    double tssf;               /* timestep scale factor */
+    double hmax;               /* mcm_hmax (grid cell = 2 hmax) */
+    int precision;             /* mcm_gpu_precision */
+    int nbr_stride;            /* initial neighbour-table stride (0: automatic) */
+    int reorder_interval;      /* steps between particle re-sorts (0: never) */
+    int block_size;            /* threads per block for the pair kernels (0: tuned default) */
+} mcm_gpu_config;
+
+/* Host views of the particle arrays (Fortran layout, np particles).  NULL
+ * members are skipped.  Mirrors the fields of `type particle`
+ * (MCM/mcm_database.f90:159-216) that the step reads or writes. */
+typedef struct {
+    double *x, *v, *a;                         /* (3,np) */
+    double *mass, *h, *hold, *rho, *rhoold, *e, *p, *c, *vabs;
+    double *efps, *pcut, *p_cut, *fail, *mindist, *critts, *tracerod;
+    double *etry, *einc, *capa;
+    double *sigma, *s, *q, *qold, *alfa, *rod, *spin;   /* (3,3,np) */
+    int *mat, *dispbc, *nnbr, *g_nnbr, *ptype;
+} mcm_gpu_fields;
+
+typedef struct mcm_gpu_handle mcm_gpu_handle;
+
+/* Time scalars of mcm_database (mcm_dt, mcm_dtold, mcm_ptime, mcm_endtime). */
+typedef struct {
+    double dt, dtold, ptime, endtime;
+} mcm_gpu_time;
+
+/* ---------------------------------------------------------------- set-up */
+
+/* Applies the deck defaults and rearrangements of MCM/mcm_matin.f90:46-56,
+ * MCM/mcm_sets1.f90, mcm_sets3.f90, mcm_sets10.f90 and mcm_calcg.f90 to a
+ * material given as read from its cards.  Replaces those routines for callers
+ * that do not run the Fortran input phase. */
+int mcm_gpu_material_from_deck(mcm_gpu_material *m);
+
+/* Allocates device storage for np particles.  Replaces the allocation part of
+ * MCM/mcm_database.f90:mcm_allocate_memory and MCM/mcm_init_neighb.f90:364-384. */
+int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int nmat,
+                   int np, mcm_gpu_handle **out);
+int mcm_gpu_destroy(mcm_gpu_handle *h);
+
+/* Copies an already initialised particle state (what mcm_initial leaves in
+ * par) to the device.  coord_maxmin (mcm_coord_maxmin(2,3), may be NULL: then
+ * it is recomputed from x as MCM/mcm_initvbls.f90:81-91 does). */
+int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coord_maxmin);
+
+/* Runs mcm_initial (MCM/mcm_initial.f90:33-101) on the device from deck-level
+ * particle data: f->x, f->v, f->mat, f->dispbc, and, when the deck gives them,
+ * f->mass (massopt 1), f->h (init_h_opt 1), f->rho and f->e (init_rhoe 1).
+ * massopt/init_h_opt/init_rhoe select which of those are read.  On return *t
+ * holds the first dt (MCM/mcm_initial.f90:85-93) with ptime = 0. */
+int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, int init_h_opt,
+                       int init_rhoe, double itss, mcm_gpu_time *t);
+
+int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f);
+
+/* ------------------------------------------------------------------ step */
+
+int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts);
+/* energies: per material ke, ie, mom(3) -> 5*nmat doubles (mcm_mat%ke, %ie, %mom),
+ * then kinetice, internale, totale.  May be NULL. */
+int mcm_gpu_step_b(mcm_gpu_handle *h, double *energies);
+int mcm_gpu_step_c(mcm_gpu_handle *h, double dt, double dtold, double *coord_maxmin);
+
+/* Up to nsteps whole loop iterations with the dt update of
+ * MCM/mcm_solution.f90:58-62 and the termination test of :101 on the device.
+ * *done receives the iterations completed (the last one may end at the
+ * termination test, before the velocity and position update). */
+int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done);
+
+/* ----------------------------------------------------------- inspection */
+
+/* Neighbour lists of the last search in reference order, 1-based ids.
+ * nbr: (stride, np) like mcm_nbrlist(maxnbr,np); g_nbr: ghost indices like
+ * mcm_g_nbrlist.  Either array may be NULL.  Returns MCM_EINVAL if a stride
+ * is too small (the required strides are written to *stride / *g_stride). */
+int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride,
+                       int *g_nnbr, int *g_nbr, int *g_stride);
+/* Ghosts of the last mcm_ghost_setup: *ngp, source particle (1-based), x (3,ngp), v (3,ngp). */
+int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, int cap);
+/* Linked-list grid of the last search: gridlim(3), gridmin(3), gridsize(3). */
+int mcm_gpu_grid(mcm_gpu_handle *h, int *gridlim, double *gridmin, double *gridsize);
+int mcm_gpu_energies(mcm_gpu_handle *h, double *energies);
+
+/* Mean neighbour count of the last search (for the roofline accounting). */
+int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp);
+
+const char *mcm_gpu_strerror(int status);
+/* Text of the last CUDA error or failed check on this handle. */
+const char *mcm_gpu_last_error(mcm_gpu_handle *h);
+int mcm_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1031 @@
+// abi.cu -- host side of the C ABI declared in include/mcm_gpu.h.
+//
+// A handle owns one CUDA stream and the device state of one body.  Each entry
+// point enqueues the kernels of its part of the loop body of
+// MCM/mcm_solution.f90 and reads back the device status.  The neighbour table,
+// ghost storage and cell arrays are sized on demand: when a kernel reports that
+// one is too small, the step is re-run after the storage has been regrown,
+// which mirrors the regrow-and-retry of MCM/mcm_ll_neighbours.f90:44,301-309.
+// The particle state is untouched by a step that stops at such a check,
+// because the search and ghost set-up precede every state update.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+using namespace mcm;
+
+struct mcm_gpu_handle {
+    mcm_gpu_config cfg;
+    int np = 0, npad = 0, nmat = 0;
+    std::vector<mcm_gpu_material> mats;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    StepArgs A;
+    // owned allocations
+    double *d_fields = nullptr;
+    int *d_ints = nullptr;
+    DevMaterial *d_mats = nullptr;
+    void *d_scalars = nullptr;     // DevTime, DevStatus, DevGrid, bbox, energy, counters
+    int *d_nppermat = nullptr;
+    // host mirrors (pinned)
+    DevTime *h_time = nullptr;
+    DevStatus *h_status = nullptr;
+    DevGrid *h_grid = nullptr;
+    double *h_bbox = nullptr;
+    double *h_energy = nullptr;
+    int *h_ngp = nullptr;
+    std::string last_error;
+    bool initialised = false;
+    int red_cap = 0;
+    double mean_nbr = 0.0;
+};
+
+namespace {
+
+int set_error(mcm_gpu_handle *h, int code, const std::string &msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_error(h, e_ == cudaErrorMemoryAllocation ? MCM_ENOMEM : MCM_ECUDA,          \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+    } while (0)
+
+template <typename T>
+int dalloc(mcm_gpu_handle *h, T **p, size_t count) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) count = 1;
+    CK(cudaMalloc((void **)p, sizeof(T) * count));
+    return MCM_OK;
+}
+
+inline int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
+
+DevParams make_params(const mcm_gpu_config &c, int nmat) {
+    DevParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.ndim = c.ndim;
+    p.disctype = c.disctype;
+    p.tcrit_opt = c.tcrit_opt;
+    p.boundary = c.boundary;
+    p.baseaccel = c.baseaccel;
+    p.drelax = c.drelax;
+    p.nmat = nmat;
+    p.diag = 1;
+    p.drelax_scale = c.drelax_scale;
+    p.tssf = c.tssf;
+    p.hmax = c.hmax;
+    for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
+    DevPlanes &pl = p.planes;
+    for (int d = 0; d < 3; ++d) {
+        for (int side = 0; side < 2; ++side) {
+            int code = c.boundary ? c.boundary_code[2 * d + side] : 0;
+            pl.code[side][d] = code;
+            pl.bx[side][d] = c.boundary_x[2 * d + side];
+        }
+        pl.type[d] = 1;
+        if (pl.code[0][d] > 0) pl.type[d] += 1;
+        if (pl.code[1][d] > 0) pl.type[d] += 2;
+    }
+    // MCM/mcm_init_boundary.f90:28-116
+    for (int d = 0; d < 3; ++d) {
+        for (int side = 0; side < 2; ++side) {
+            int plane = 2 * d + side;
+            for (int k = 0; k < 3; ++k) { pl.mult[plane][k] = 1.0; pl.add[plane][k] = 0.0; }
+            int code = pl.code[side][d];
+            if (code == 1) {
+                pl.mult[plane][d] = -1.0;
+                pl.add[plane][d] = 2.0 * pl.bx[side][d];
+            } else if (code == 2) {
+                double span = pl.bx[1][d] - pl.bx[0][d];
+                pl.add[plane][d] = (side == 0) ? -span : span;
+            }
+        }
+    }
+    return p;
+}
+
+// ------------------------------------------------------------ allocation
+int alloc_particles(mcm_gpu_handle *h) {
+    const size_t np = h->npad;
+    int st;
+    if ((st = dalloc(h, &h->d_fields, (size_t)NFIELD * np))) return st;
+    CK(cudaMemsetAsync(h->d_fields, 0, sizeof(double) * NFIELD * np, h->stream));
+    for (int f = 0; f < NFIELD; ++f) h->A.F.f[f] = h->d_fields + (size_t)f * np;
+    if ((st = dalloc(h, &h->d_ints, 4 * np))) return st;
+    CK(cudaMemsetAsync(h->d_ints, 0, sizeof(int) * 4 * np, h->stream));
+    h->A.F.mat = h->d_ints;
+    h->A.F.dispbc = h->d_ints + np;
+    h->A.F.orig = h->d_ints + 2 * np;
+    h->A.F.ptype = h->d_ints + 3 * np;
+    if ((st = dalloc(h, &h->A.key, np))) return st;
+    if ((st = dalloc(h, &h->A.cell_list, np))) return st;
+    if ((st = dalloc(h, &h->A.nnbr, np))) return st;
+    if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
+    CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
+    CK(cudaMemsetAsync(h->A.gnnbr, 0, sizeof(int) * np, h->stream));
+    if ((st = dalloc(h, &h->A.rec0, np))) return st;
+    if ((st = dalloc(h, &h->A.rec1, np))) return st;
+    if ((st = dalloc(h, &h->A.rec2, np))) return st;
+    h->red_cap = (int)((np + kRedThreads - 1) / kRedThreads) + 8;
+    if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
+    return MCM_OK;
+}
+
+int alloc_cells(mcm_gpu_handle *h, long long cap) {
+    int st;
+    h->A.cell_cap = cap;
+    if ((st = dalloc(h, &h->A.cell_count, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.cell_start, (size_t)cap + 1))) return st;
+    long long nsum = (cap + 4095) / 4096 + 2;
+    if ((st = dalloc(h, &h->A.scan_sums, (size_t)nsum))) return st;
+    if ((st = dalloc(h, &h->A.gcell, (size_t)cap))) return st;
+    h->A.layer_cap = (int)std::min<long long>(cap, 1LL << 30);
+    if ((st = dalloc(h, &h->A.layer_count, (size_t)h->A.layer_cap))) return st;
+    if ((st = dalloc(h, &h->A.layer_off, (size_t)h->A.layer_cap))) return st;
+    return MCM_OK;
+}
+
+int alloc_ghosts(mcm_gpu_handle *h, int cap) {
+    int st;
+    h->A.ghost_cap = cap;
+    double **dd[] = {&h->A.gx, &h->A.gy, &h->A.gz, &h->A.gvx, &h->A.gvy, &h->A.gvz,
+                     &h->A.gmass, &h->A.gh, &h->A.ghold, &h->A.grho};
+    for (double **p : dd)
+        if ((st = dalloc(h, p, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.gpar, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.gmat, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.grec0, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.grec1, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.grec2, (size_t)cap))) return st;
+    return MCM_OK;
+}
+
+int alloc_table(mcm_gpu_handle *h, int stride, int gstride) {
+    int st;
+    h->A.stride = stride;
+    h->A.gstride = gstride;
+    if ((st = dalloc(h, &h->A.nbr, (size_t)stride * h->npad))) return st;
+    if ((st = dalloc(h, &h->A.gnbr, (size_t)gstride * h->npad))) return st;
+    return MCM_OK;
+}
+
+int reset_status(mcm_gpu_handle *h) {
+    CK(cudaMemsetAsync(h->A.status, 0, sizeof(DevStatus), h->stream));
+    return MCM_OK;
+}
+
+int sync_status(mcm_gpu_handle *h) {
+    CK(cudaMemcpyAsync(h->h_status, h->A.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    return MCM_OK;
+}
+
+// Regrows whatever the last status asked for.  Returns 1 if something grew.
+int regrow(mcm_gpu_handle *h, int *grew) {
+    *grew = 0;
+    const DevStatus &s = *h->h_status;
+    int st;
+    switch (s.code) {
+        case MCM_ENBR_OVERFLOW: {
+            int ns = h->A.stride, ng = h->A.gstride;
+            if (s.req_stride > ns) ns = round_up(s.req_stride + s.req_stride / 8 + 8, 8);
+            if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
+            if ((st = alloc_table(h, ns, ng))) return st;
+            *grew = 1;
+            break;
+        }
+        case MCM_EGHOST_OVERFLOW: {
+            int cap = std::max(s.req_ngp + s.req_ngp / 4 + 1024, h->A.ghost_cap * 2);
+            if ((st = alloc_ghosts(h, cap))) return st;
+            *grew = 1;
+            break;
+        }
+        case MCM_EGRID_OVERFLOW: {
+            long long need = std::max<long long>(s.req_cells, h->A.cell_cap * 2);
+            long long cap = need + need / 2 + 1024;
+            if ((st = alloc_cells(h, cap))) return st;
+            *grew = 1;
+            break;
+        }
+        default: break;
+    }
+    return MCM_OK;
+}
+
+// ---------------------------------------------------------------- dispatch
+int launch_strain(mcm_gpu_handle *h) {
+    switch (h->cfg.precision) {
+        case MCM_PREC_FP64_EXACT: return exact::launch_strain_constitutive(h->A, h->stream);
+        default: return fast::launch_strain_constitutive(h->A, h->stream);
+    }
+}
+int launch_mom(mcm_gpu_handle *h, int integrate) {
+    switch (h->cfg.precision) {
+        case MCM_PREC_FP64_EXACT: return exact::launch_momentum(h->A, h->stream, integrate);
+        default: return fast::launch_momentum(h->A, h->stream, integrate);
+    }
+}
+int launch_move(mcm_gpu_handle *h) {
+    switch (h->cfg.precision) {
+        case MCM_PREC_FP64_EXACT: return exact::launch_update_move(h->A, h->stream);
+        default: return fast::launch_update_move(h->A, h->stream);
+    }
+}
+
+// neighbours -> strain -> constitutive -> critts (MCM/mcm_solution.f90:41-53)
+void enqueue_part_a(mcm_gpu_handle *h) {
+    StepArgs &a = h->A;
+    launch_grid_setup(a, h->stream);
+    launch_cell_build(a, h->stream);
+    if (a.prm.boundary) launch_ghosts(a, h->stream);
+    launch_search(a, h->stream);
+    int nb = launch_strain(h);
+    launch_critts_reduce(a, h->stream, nb);
+}
+
+// momentum -> boundcond -> calctotale (-> update_velocity -> move)
+void enqueue_part_b(mcm_gpu_handle *h, int integrate) {
+    int nb = launch_mom(h, integrate);
+    launch_energy_bbox_reduce(h->A, h->stream, nb, 1, integrate);
+}
+
+int check_handle(mcm_gpu_handle *h) {
+    if (!h) return MCM_EINVAL;
+    if (!h->initialised) return set_error(h, MCM_EINVAL, "state not uploaded");
+    CK(cudaSetDevice(h->device));
+    return MCM_OK;
+}
+
+// ------------------------------------------------------------- transfers
+// Fortran (3,np) vector -> three device arrays
+int put_vec3(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
+    const int n = h->np;
+    for (int k = 0; k < 3; ++k) {
+        for (int i = 0; i < n; ++i) tmp[i] = src[3 * (size_t)i + k];
+        CK(cudaMemcpy(h->A.F.f[f0 + k], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    return MCM_OK;
+}
+
+// Fortran (3,3,np) symmetric tensor -> six device arrays (11 22 33 12 13 23)
+int put_sym(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
+    static const int rc[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    const int n = h->np;
+    for (int t = 0; t < 6; ++t) {
+        for (int i = 0; i < n; ++i) tmp[i] = src[9 * (size_t)i + rc[t][0] + 3 * rc[t][1]];
+        CK(cudaMemcpy(h->A.F.f[f0 + t], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    return MCM_OK;
+}
+
+int put_scalar(mcm_gpu_handle *h, const double *src, int f) {
+    CK(cudaMemcpy(h->A.F.f[f], src, sizeof(double) * h->np, cudaMemcpyHostToDevice));
+    return MCM_OK;
+}
+
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+int mcm_gpu_abi_version(void) { return MCM_GPU_ABI_VERSION; }
+
+const char *mcm_gpu_strerror(int status) {
+    switch (status) {
+        case MCM_OK: return "ok";
+        case MCM_ENBR_OVERFLOW: return "neighbour table overflow";
+        case MCM_EGHOST_OVERFLOW: return "ghost storage overflow";
+        case MCM_ECOMPLEX_C: return "complex speed of sound (eos41 c^2 < 0)";
+        case MCM_ECAP_NOCONV: return "cap model iteration did not converge";
+        case MCM_ETIMEOUT: return "bounded device wait timed out";
+        case MCM_ECUDA: return "CUDA runtime error";
+        case MCM_ENOMEM: return "device allocation failed";
+        case MCM_EINVAL: return "invalid argument";
+        case MCM_EUNSUPPORTED: return "option not supported by the GPU step";
+        case MCM_EGRID_OVERFLOW: return "cell grid storage overflow";
+        case MCM_EGHOST_LAYER: return "real particle in a ghost-layer cell";
+        case MCM_EGRID_TOO_LARGE: return "linked-list grid too large";
+    }
+    return "unknown status";
+}
+
+const char *mcm_gpu_last_error(mcm_gpu_handle *h) { return h ? h->last_error.c_str() : "no handle"; }
+
+// MCM/mcm_matin.f90:46-56, MCM/mcm_sets1.f90:23-51, mcm_sets3.f90:78-96,
+// mcm_sets10.f90:121-134, MCM/mcm_calcg.f90:31-59.
+int mcm_gpu_material_from_deck(mcm_gpu_material *m) {
+    if (!m) return MCM_EINVAL;
+    if (m->visc_type == 0) m->visc_type = 1;
+    if (m->av_l == 0.0) m->av_l = 0.06;
+    if (m->av_q == 0.0) m->av_q = 1.5;
+    if (m->rho_min == 0.0) m->rho_min = 1.0E-10;
+    if (m->rho_max == 0.0) m->rho_max = 1.0E+10;
+    double *cm = m->strinput;
+    auto C = [cm](int i, int j) -> double & { return cm[(i - 1) + 5 * (j - 1)]; };
+    switch (m->model) {
+        case 1: {
+            double p6 = C(2, 1), p7 = C(3, 1);
+            for (int i = 2; i <= 5; ++i)
+                for (int j = 1; j <= 5; ++j) C(i, j) = 0.0;
+            double q1 = C(1, 1) * C(1, 2) / ((1.0 + C(1, 2)) * (1.0 - 2.0 * C(1, 2)));
+            double q2 = C(1, 1) * 0.5 / (1.0 + C(1, 2));
+            double q3 = q1 + 2.0 * q2;
+            C(2, 1) = q3; C(3, 2) = q3; C(4, 3) = q3; C(5, 4) = q2;
+            C(2, 2) = q1; C(2, 3) = q1; C(3, 1) = q1; C(3, 3) = q1; C(4, 1) = q1; C(4, 2) = q1;
+            C(2, 6) = C(1, 6);
+            C(1, 6) = C(1, 1) * C(1, 4) / (C(1, 1) - C(1, 4));
+            C(1, 7) = p6;
+            C(2, 7) = p7;
+            if (m->eos != 0) return MCM_EINVAL;
+            m->g = cm[0] / (2.0 * (1.0 + cm[5]));
+            break;
+        }
+        case 3: {
+            double p7 = C(2, 6);
+            for (int i = 2; i <= 5; ++i)
+                for (int j = 1; j <= 6; ++j) C(i, j) = 0.0;
+            double q1 = C(1, 1) * C(1, 2) / ((1.0 + C(1, 2)) * (1.0 - 2.0 * C(1, 2)));
+            double q2 = C(1, 1) * 0.5 / (1.0 + C(1, 2));
+            double q3 = q1 + 2.0 * q2;
+            C(2, 1) = q3;
+            C(5, 4) = q2;
+            C(2, 4) = C(1, 1) * C(1, 4) / (C(1, 1) - C(1, 4));
+            C(2, 6) = p7;
+            if (m->eos != 0) return MCM_EINVAL;
+            m->g = cm[0] / (2.0 * (1.0 + cm[5]));
+            break;
+        }
+        case 9:
+            m->g = 0.0;
+            if (!(m->eos == 1 || m->eos == 4 || m->eos == 13 || m->eos == 28 || m->eos == 41)) return MCM_EINVAL;
+            break;
+        case 10: {
+            double prop[48];
+            for (int i = 0; i < 48; ++i) prop[i] = cm[i];
+            if (prop[3] == 0.0) prop[3] = (double)-1.e30f;
+            if (prop[6] == 0.0) prop[6] = (double)1.000000001f;
+            for (int i = 0; i < 48; ++i) cm[i] = prop[i];
+            for (int i = 2; i <= 16; ++i)
+                if (prop[i + 14] < prop[i + 15]) cm[15] = (double)i;
+            m->g = cm[0];
+            if (!(m->eos == 1 || m->eos == 4 || m->eos == 13 || m->eos == 28 || m->eos == 41)) return MCM_EINVAL;
+            break;
+        }
+        case 4:
+            return MCM_EUNSUPPORTED;
+        default:
+            return MCM_EINVAL;
+    }
+    return MCM_OK;
+}
+
+int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int nmat, int np,
+                   mcm_gpu_handle **out) {
+    if (!cfg || !mats || !out || np <= 0 || nmat <= 0 || nmat > MCM_GPU_MAX_MATERIALS) return MCM_EINVAL;
+    *out = nullptr;
+    if (cfg->ndim != 3) return MCM_EUNSUPPORTED;
+    if (cfg->contacttype != 0 || cfg->h_opt != 0 || cfg->veloc_opt != 0) return MCM_EUNSUPPORTED;
+    if (cfg->krtype != 0 && cfg->krtype != 1) return MCM_EUNSUPPORTED;
+    if (cfg->disctype != 0 && cfg->disctype != 1) return MCM_EINVAL;
+    if (cfg->tcrit_opt < 0 || cfg->tcrit_opt > 2) return MCM_EINVAL;
+    if (cfg->precision < 0 || cfg->precision > 2) return MCM_EINVAL;
+    for (int m = 0; m < nmat; ++m) {
+        int md = mats[m].model;
+        if (md == 4) return MCM_EUNSUPPORTED;
+        if (md != 1 && md != 3 && md != 9 && md != 10) return MCM_EINVAL;
+    }
+    if (cfg->boundary) {
+        for (int d = 0; d < 3; ++d) {
+            bool p0 = cfg->boundary_code[2 * d] == 2, p1 = cfg->boundary_code[2 * d + 1] == 2;
+            if (p0 != p1) return MCM_EINVAL;   // MCM/mcm_inp_symmetry_v2.f90:89-109
+        }
+    }
+    if (cfg->precision == MCM_PREC_MIXED) return MCM_EUNSUPPORTED;
+    mcm_gpu_handle *h = new mcm_gpu_handle();
+    h->cfg = *cfg;
+    if (h->cfg.tssf == 0.0) h->cfg.tssf = 0.8;   // MCM/mcm_control_v2.f90:193
+    h->np = np;
+    h->npad = round_up(np, 32);
+    h->nmat = nmat;
+    h->mats.assign(mats, mats + nmat);
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e != cudaSuccess) { delete h; return MCM_ECUDA; }
+    int st = MCM_OK;
+#define TRY(x) do { st = (x); if (st) { mcm_gpu_destroy(h); return st; } } while (0)
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return MCM_ECUDA; }
+    std::memset(&h->A, 0, sizeof(h->A));
+    h->A.n = np;
+    h->A.npad = h->npad;
+    h->A.nmat = nmat;
+    h->A.split_mode = 1;
+    h->A.prm = make_params(h->cfg, nmat);
+    // materials
+    std::vector<DevMaterial> dm(nmat);
+    for (int m = 0; m < nmat; ++m) {
+        DevMaterial &d = dm[m];
+        std::memset(&d, 0, sizeof(d));
+        d.model = mats[m].model; d.eos = mats[m].eos; d.visc_type = mats[m].visc_type;
+        d.rho = mats[m].rho; d.g = mats[m].g; d.av_l = mats[m].av_l; d.av_q = mats[m].av_q;
+        d.mass = mats[m].mass; d.h = mats[m].h; d.rho_min = mats[m].rho_min; d.rho_max = mats[m].rho_max;
+        std::memcpy(d.strinput, mats[m].strinput, sizeof(d.strinput));
+        std::memcpy(d.eosinput, mats[m].eosinput, sizeof(d.eosinput));
+    }
+    TRY(dalloc(h, &h->d_mats, (size_t)nmat));
+    if (cudaMemcpy(h->d_mats, dm.data(), sizeof(DevMaterial) * nmat, cudaMemcpyHostToDevice) != cudaSuccess) {
+        mcm_gpu_destroy(h);
+        return MCM_ECUDA;
+    }
+    h->A.mats = h->d_mats;
+    // scalars
+    size_t scal = sizeof(DevTime) + sizeof(DevStatus) + sizeof(DevGrid) + 64 + sizeof(double) * (5 * nmat + 8) + 64;
+    if (cudaMalloc(&h->d_scalars, 4096 + scal) != cudaSuccess) { mcm_gpu_destroy(h); return MCM_ENOMEM; }
+    cudaMemset(h->d_scalars, 0, 4096 + scal);
+    char *p = (char *)h->d_scalars;
+    h->A.time = (DevTime *)p; p += 256;
+    h->A.status = (DevStatus *)p; p += 256;
+    h->A.grid = (DevGrid *)p; p += 256;
+    h->A.bbox = (double *)p; p += 256;
+    h->A.ngp = (int *)p; p += 64;
+    h->A.plane_base = (int *)p; p += 64;
+    h->A.energy = (double *)p;
+    cudaMallocHost((void **)&h->h_time, 4096);
+    char *q = (char *)h->h_time;
+    h->h_status = (DevStatus *)(q + 256);
+    h->h_grid = (DevGrid *)(q + 512);
+    h->h_bbox = (double *)(q + 768);
+    h->h_ngp = (int *)(q + 1024);
+    h->h_energy = (double *)(q + 1088);
+    TRY(alloc_particles(h));
+    int stride = cfg->nbr_stride > 0 ? round_up(cfg->nbr_stride, 8) : 96;
+    TRY(alloc_table(h, stride, cfg->boundary ? 48 : 8));
+    TRY(alloc_cells(h, 1 << 16));
+    TRY(alloc_ghosts(h, cfg->boundary ? std::max(4096, np / 8) : 32));
+    TRY(dalloc(h, &h->d_nppermat, (size_t)nmat));
+#undef TRY
+    *out = h;
+    return MCM_OK;
+}
+
+int mcm_gpu_destroy(mcm_gpu_handle *h) {
+    if (!h) return MCM_EINVAL;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void *ptrs[] = {h->d_fields, h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
+                    h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
+                    h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
+                    h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
+                    h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat,
+                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.nbr, h->A.gnbr};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_time) cudaFreeHost(h->h_time);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MCM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// bbox from x (MCM/mcm_initvbls.f90:81-91) when none is supplied
+__global__ void k_bbox_partials(StepArgs a) {
+    __shared__ double sm[2][32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nv = 5 * a.nmat + 6;
+    double *out = a.red + (size_t)blockIdx.x * nv;
+    for (int d = 0; d < 3; ++d) {
+        double lo = 1.0e20, hi = -1.0e20;
+        if (i < a.n) { lo = a.F.f[FX + d][i]; hi = lo; }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        __syncthreads();
+        if (lane == 0) { sm[0][w] = lo; sm[1][w] = hi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { lo = fmin(lo, sm[0][k]); hi = fmax(hi, sm[1][k]); }
+            out[5 * a.nmat + d] = lo;
+            out[5 * a.nmat + 3 + d] = hi;
+        }
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < 5 * a.nmat; ++v) out[v] = 0.0;
+}
+
+__global__ void k_energy_partials(StepArgs a) {
+    __shared__ double sm[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nv = 5 * a.nmat + 6;
+    double *out = a.red + (size_t)blockIdx.x * nv;
+    int mati = 0;
+    double vals[5] = {0, 0, 0, 0, 0};
+    if (i < a.n) {
+        mati = a.F.mat[i];
+        double mass = a.F.f[FMASS][i], vabs = a.F.f[FVABS][i];
+        vals[0] = 0.5 * mass * (vabs * vabs);
+        vals[1] = a.F.f[FE][i];
+        vals[2] = mass * fabs(a.F.f[FVX][i]);
+        vals[3] = mass * fabs(a.F.f[FVY][i]);
+        vals[4] = mass * fabs(a.F.f[FVZ][i]);
+    }
+    for (int m = 1; m <= a.nmat; ++m) {
+        for (int v = 0; v < 5; ++v) {
+            double x = (mati == m) ? vals[v] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            __syncthreads();
+            if (lane == 0) sm[w] = x;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double r = 0.0;
+                for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sm[k];
+                out[5 * (m - 1) + v] = r;
+            }
+        }
+    }
+}
+
+__global__ void k_copy_field(double *dst, const double *src, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+__global__ void k_iota(int *p, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
+int compute_bbox(mcm_gpu_handle *h) {
+    int nb = (h->np + kRedThreads - 1) / kRedThreads;
+    k_bbox_partials<<<nb, kRedThreads, 0, h->stream>>>(h->A);
+    launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
+    CK(cudaGetLastError());
+    return MCM_OK;
+}
+
+int compute_energy(mcm_gpu_handle *h) {
+    int nb = (h->np + kRedThreads - 1) / kRedThreads;
+    k_energy_partials<<<nb, kRedThreads, 0, h->stream>>>(h->A);
+    launch_energy_bbox_reduce(h->A, h->stream, nb, 1, 0);
+    CK(cudaGetLastError());
+    return MCM_OK;
+}
+
+// Runs the neighbour search alone (mcm_init_neighb), regrowing storage.
+int run_search_only(mcm_gpu_handle *h) {
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int st;
+        if ((st = reset_status(h))) return st;
+        StepArgs &a = h->A;
+        launch_grid_setup(a, h->stream);
+        launch_cell_build(a, h->stream);
+        if (a.prm.boundary) launch_ghosts(a, h->stream);
+        launch_search(a, h->stream);
+        if ((st = sync_status(h))) return st;
+        int code = h->h_status->code;
+        if (code == MCM_OK) return MCM_OK;
+        int grew = 0;
+        if ((st = regrow(h, &grew))) return st;
+        if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
+    }
+    return set_error(h, MCM_ENBR_OVERFLOW, "storage did not converge");
+}
+
+// Enqueues part a with retries; returns the final status.
+int run_part_a(mcm_gpu_handle *h) {
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int st;
+        if ((st = reset_status(h))) return st;
+        enqueue_part_a(h);
+        if ((st = sync_status(h))) return st;
+        int code = h->h_status->code;
+        if (code == MCM_OK) return MCM_OK;
+        int grew = 0;
+        if ((st = regrow(h, &grew))) return st;
+        if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
+    }
+    return set_error(h, MCM_ENBR_OVERFLOW, "storage did not converge");
+}
+
+int finish_upload(mcm_gpu_handle *h, const double *coord_maxmin) {
+    int st;
+    k_iota<<<256, 256, 0, h->stream>>>(h->A.F.orig, h->np);
+    if (coord_maxmin) {
+        double b[6];
+        for (int d = 0; d < 3; ++d) { b[d] = coord_maxmin[2 * d]; b[3 + d] = coord_maxmin[2 * d + 1]; }
+        CK(cudaMemcpyAsync(h->A.bbox, b, sizeof(b), cudaMemcpyHostToDevice, h->stream));
+    } else {
+        if ((st = compute_bbox(h))) return st;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->initialised = true;
+    return MCM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coord_maxmin) {
+    if (!h || !f || !f->x || !f->mat) return MCM_EINVAL;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    const int n = h->np;
+    std::vector<double> tmp(n);
+    int st;
+    if ((st = put_vec3(h, f->x, FX, tmp))) return st;
+    if (f->v && (st = put_vec3(h, f->v, FVX, tmp))) return st;
+    if (f->a && (st = put_vec3(h, f->a, FAX, tmp))) return st;
+    struct { const double *p; int f; } sc[] = {
+        {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
+        {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
+        {f->fail, FFAIL}, {f->mindist, FMINDIST}, {f->critts, FCRITTS}, {f->tracerod, FTR},
+        {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}};
+    for (auto &s : sc)
+        if (s.p && (st = put_scalar(h, s.p, s.f))) return st;
+    if (f->sigma && (st = put_sym(h, f->sigma, FS11, tmp))) return st;
+    if (f->s && (st = put_sym(h, f->s, FD11, tmp))) return st;
+    if (f->alfa && (st = put_sym(h, f->alfa, FA11, tmp))) return st;
+    if (f->rod && (st = put_sym(h, f->rod, FR11, tmp))) return st;
+    if (f->q) {
+        for (int i = 0; i < n; ++i) tmp[i] = f->q[9 * (size_t)i];
+        CK(cudaMemcpy(h->A.F.f[FQ], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    for (int i = 0; i < n; ++i)
+        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
+    CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->A.F.dispbc, 0, sizeof(int) * n));
+    if (f->ptype) CK(cudaMemcpy(h->A.F.ptype, f->ptype, sizeof(int) * n, cudaMemcpyHostToDevice));
+    return finish_upload(h, coord_maxmin);
+}
+
+int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, int init_h_opt, int init_rhoe,
+                       double itss, mcm_gpu_time *t) {
+    if (!h || !f || !f->x || !f->mat || !t) return MCM_EINVAL;
+    CK(cudaSetDevice(h->device));
+    const int n = h->np;
+    std::vector<double> tmp(n);
+    int st;
+    if ((st = put_vec3(h, f->x, FX, tmp))) return st;
+    if (f->v) { if ((st = put_vec3(h, f->v, FVX, tmp))) return st; }
+    else {
+        for (int k = 0; k < 3; ++k) CK(cudaMemset(h->A.F.f[FVX + k], 0, sizeof(double) * n));
+    }
+    if (massopt == 1) { if (!f->mass) return MCM_EINVAL; if ((st = put_scalar(h, f->mass, FMASS))) return st; }
+    if (init_h_opt == 1) { if (!f->h) return MCM_EINVAL; if ((st = put_scalar(h, f->h, FH))) return st; }
+    if (init_rhoe == 1) {
+        if (!f->rho || !f->e) return MCM_EINVAL;
+        if ((st = put_scalar(h, f->rho, FRHO))) return st;
+        if ((st = put_scalar(h, f->e, FE))) return st;
+    }
+    std::vector<int> cnt(h->nmat, 0);
+    for (int i = 0; i < n; ++i) {
+        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
+        cnt[f->mat[i] - 1] += 1;
+    }
+    CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->A.F.dispbc, 0, sizeof(int) * n));
+    CK(cudaMemcpy(h->d_nppermat, cnt.data(), sizeof(int) * h->nmat, cudaMemcpyHostToDevice));
+    // hmax (MCM/mcm_init_h.f90:22-37; the material loop indexes particles 1..nummat)
+    double hmax = 0.0;
+    if (init_h_opt == 0) {
+        for (int i = 0; i < h->nmat && i < n; ++i) hmax = std::max(hmax, h->mats[f->mat[i] - 1].h);
+    } else {
+        for (int i = 0; i < n; ++i) hmax = std::max(hmax, f->h[i]);
+    }
+    h->cfg.hmax = hmax;
+    h->A.prm.hmax = hmax;
+    if ((st = reset_status(h))) return st;
+    switch (h->cfg.precision) {
+        case MCM_PREC_FP64_EXACT: exact::launch_initial(h->A, h->stream, massopt, init_h_opt, init_rhoe, h->d_nppermat); break;
+        default: fast::launch_initial(h->A, h->stream, massopt, init_h_opt, init_rhoe, h->d_nppermat); break;
+    }
+    CK(cudaGetLastError());
+    if ((st = finish_upload(h, nullptr))) return st;
+    if ((st = sync_status(h))) return st;
+    if (h->h_status->code) return set_error(h, h->h_status->code, "initialisation");
+    // init_neighb (MCM/mcm_initial.f90:74) and calccritts (:81)
+    if ((st = run_search_only(h))) return st;
+    int nb = (h->cfg.precision == MCM_PREC_FP64_EXACT) ? exact::launch_init_critts(h->A, h->stream)
+                                                        : fast::launch_init_critts(h->A, h->stream);
+    launch_init_critts_reduce(h->A, h->stream, nb);
+    if ((st = compute_energy(h))) return st;
+    if ((st = sync_status(h))) return st;
+    double critts = h->h_time->critts;
+    double dt = (itss != 0.0) ? std::min(itss, critts * h->cfg.tssf) : critts * h->cfg.tssf;
+    t->dt = dt;
+    t->dtold = 0.0;
+    t->ptime = 0.0;
+    DevTime dtm;
+    std::memset(&dtm, 0, sizeof(dtm));
+    dtm.dt = dt; dtm.dtold = 0.0; dtm.ptime = 0.0; dtm.endtime = t->endtime; dtm.critts = critts;
+    CK(cudaMemcpy(h->A.time, &dtm, sizeof(dtm), cudaMemcpyHostToDevice));
+    return MCM_OK;
+}
+
+int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    h->A.split_mode = 1;
+    launch_set_time(h->A, h->stream, dt, 0.0, 0);
+    if ((st = run_part_a(h))) return st;
+    if (critts) *critts = h->h_time->critts;
+    return MCM_OK;
+}
+
+int mcm_gpu_step_b(mcm_gpu_handle *h, double *energies) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    h->A.split_mode = 1;
+    if ((st = reset_status(h))) return st;
+    enqueue_part_b(h, 0);
+    if (energies) {
+        CK(cudaMemcpyAsync(h->h_energy, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost,
+                           h->stream));
+    }
+    if ((st = sync_status(h))) return st;
+    if (h->h_status->code) return set_error(h, h->h_status->code, "step_b");
+    if (energies) std::memcpy(energies, h->h_energy, sizeof(double) * (5 * h->nmat + 3));
+    return MCM_OK;
+}
+
+int mcm_gpu_step_c(mcm_gpu_handle *h, double dt, double dtold, double *coord_maxmin) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    h->A.split_mode = 1;
+    if ((st = reset_status(h))) return st;
+    launch_set_time(h->A, h->stream, dt, dtold, 1);
+    int nb = launch_move(h);
+    launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
+    CK(cudaMemcpyAsync(h->h_bbox, h->A.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream));
+    if ((st = sync_status(h))) return st;
+    if (h->h_status->code) return set_error(h, h->h_status->code, "step_c");
+    if (coord_maxmin)
+        for (int d = 0; d < 3; ++d) { coord_maxmin[2 * d] = h->h_bbox[d]; coord_maxmin[2 * d + 1] = h->h_bbox[3 + d]; }
+    return MCM_OK;
+}
+
+int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (!t || nsteps < 0) return MCM_EINVAL;
+    if (done) *done = 0;
+    h->A.split_mode = 0;
+    DevTime dtm;
+    std::memset(&dtm, 0, sizeof(dtm));
+    dtm.dt = t->dt; dtm.dtold = t->dtold; dtm.ptime = t->ptime; dtm.endtime = t->endtime;
+    CK(cudaMemcpyAsync(h->A.time, &dtm, sizeof(dtm), cudaMemcpyHostToDevice, h->stream));
+    int total = 0;
+    int attempts = 0;
+    int finished = 0;
+    while (total < nsteps && !finished) {
+        int batch = std::min(nsteps - total, 64);
+        if ((st = reset_status(h))) return st;
+        for (int k = 0; k < batch; ++k) {
+            enqueue_part_a(h);
+            enqueue_part_b(h, 1);
+            launch_finish_step(h->A, h->stream);
+        }
+        if ((st = sync_status(h))) return st;
+        int ran = h->h_time->steps_done;
+        total += ran;
+        // clear the per-batch counter
+        CK(cudaMemsetAsync(&h->A.time->steps_done, 0, sizeof(int), h->stream));
+        if (h->h_time->ended >= 2) finished = 1;
+        int code = h->h_status->code;
+        if (code != MCM_OK) {
+            int grew = 0;
+            if ((st = regrow(h, &grew))) return st;
+            if (!grew || ++attempts > 16) {
+                if (done) *done = total;
+                CK(cudaMemcpy(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
+                t->dt = h->h_time->dt; t->dtold = h->h_time->dtold; t->ptime = h->h_time->ptime;
+                return set_error(h, code, mcm_gpu_strerror(code));
+            }
+        }
+    }
+    CK(cudaMemcpy(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
+    t->dt = h->h_time->dt; t->dtold = h->h_time->dtold; t->ptime = h->h_time->ptime;
+    if (done) *done = total;
+    h->A.split_mode = 1;
+    return MCM_OK;
+}
+
+int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (!f) return MCM_EINVAL;
+    CK(cudaStreamSynchronize(h->stream));
+    const int n = h->np;
+    std::vector<int> orig(n);
+    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    std::vector<double> tmp(n);
+    auto get = [&](int fld) -> int {
+        CK(cudaMemcpy(tmp.data(), h->A.F.f[fld], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        return MCM_OK;
+    };
+    auto vec3 = [&](double *dst, int f0) -> int {
+        for (int k = 0; k < 3; ++k) {
+            int s = get(f0 + k); if (s) return s;
+            for (int p = 0; p < n; ++p) dst[3 * (size_t)orig[p] + k] = tmp[p];
+        }
+        return MCM_OK;
+    };
+    auto sym = [&](double *dst, int f0) -> int {
+        static const int rc[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+        for (int t = 0; t < 6; ++t) {
+            int s = get(f0 + t); if (s) return s;
+            for (int p = 0; p < n; ++p) {
+                size_t b = 9 * (size_t)orig[p];
+                dst[b + rc[t][0] + 3 * rc[t][1]] = tmp[p];
+                dst[b + rc[t][1] + 3 * rc[t][0]] = tmp[p];
+            }
+        }
+        return MCM_OK;
+    };
+    auto scal = [&](double *dst, int fld) -> int {
+        int s = get(fld); if (s) return s;
+        for (int p = 0; p < n; ++p) dst[orig[p]] = tmp[p];
+        return MCM_OK;
+    };
+    if (f->x && (st = vec3(f->x, FX))) return st;
+    if (f->v && (st = vec3(f->v, FVX))) return st;
+    if (f->a && (st = vec3(f->a, FAX))) return st;
+    struct { double *p; int f; } sc[] = {
+        {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
+        {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
+        {f->fail, FFAIL}, {f->mindist, FMINDIST}, {f->critts, FCRITTS}, {f->tracerod, FTR},
+        {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}};
+    for (auto &s : sc)
+        if (s.p && (st = scal(s.p, s.f))) return st;
+    if (f->sigma && (st = sym(f->sigma, FS11))) return st;
+    if (f->s && (st = sym(f->s, FD11))) return st;
+    if (f->alfa && (st = sym(f->alfa, FA11))) return st;
+    if (f->rod && (st = sym(f->rod, FR11))) return st;
+    if (f->spin) {
+        // spin(n,m) = -spin(m,n), zero diagonal
+        static const int fl[3] = {FW12, FW13, FW23};
+        static const int rc[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+        for (int p = 0; p < n; ++p)
+            for (int k = 0; k < 9; ++k) f->spin[9 * (size_t)orig[p] + k] = 0.0;
+        for (int t = 0; t < 3; ++t) {
+            if ((st = get(fl[t]))) return st;
+            for (int p = 0; p < n; ++p) {
+                size_t b = 9 * (size_t)orig[p];
+                f->spin[b + rc[t][0] + 3 * rc[t][1]] = tmp[p];
+                f->spin[b + rc[t][1] + 3 * rc[t][0]] = -tmp[p];
+            }
+        }
+    }
+    if (f->q || f->qold) {
+        if ((st = get(FQ))) return st;
+        double *dsts[2] = {f->q, f->qold};
+        for (double *dst : dsts) {
+            if (!dst) continue;
+            for (int p = 0; p < n; ++p) {
+                size_t b = 9 * (size_t)orig[p];
+                for (int k = 0; k < 9; ++k) dst[b + k] = 0.0;
+                dst[b] = dst[b + 4] = dst[b + 8] = tmp[p];
+            }
+        }
+    }
+    std::vector<int> itmp(n);
+    auto geti = [&](int *dst, const int *src) -> int {
+        CK(cudaMemcpy(itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        for (int p = 0; p < n; ++p) dst[orig[p]] = itmp[p];
+        return MCM_OK;
+    };
+    if (f->mat && (st = geti(f->mat, h->A.F.mat))) return st;
+    if (f->dispbc && (st = geti(f->dispbc, h->A.F.dispbc))) return st;
+    if (f->nnbr && (st = geti(f->nnbr, h->A.nnbr))) return st;
+    if (f->g_nnbr && (st = geti(f->g_nnbr, h->A.gnnbr))) return st;
+    if (f->ptype && (st = geti(f->ptype, h->A.F.ptype))) return st;
+    return MCM_OK;
+}
+
+int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int *g_nnbr, int *g_nbr, int *g_stride) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    const int n = h->np, np = h->npad;
+    std::vector<int> orig(n), cnt(n), gcnt(n);
+    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cnt.data(), h->A.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(gcnt.data(), h->A.gnnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    int need = 0, gneed = 0;
+    for (int p = 0; p < n; ++p) { need = std::max(need, cnt[p]); gneed = std::max(gneed, gcnt[p]); }
+    if (nnbr) for (int p = 0; p < n; ++p) nnbr[orig[p]] = cnt[p];
+    if (g_nnbr) for (int p = 0; p < n; ++p) g_nnbr[orig[p]] = gcnt[p];
+    bool small = (nbr && stride && *stride < need) || (g_nbr && g_stride && *g_stride < gneed);
+    if (stride) { if (small || !nbr) *stride = std::max(*stride, need); }
+    if (g_stride) { if (small || !g_nbr) *g_stride = std::max(*g_stride, gneed); }
+    if (small) return MCM_EINVAL;
+    if (nbr && stride) {
+        std::vector<int> tab((size_t)h->A.stride * np);
+        CK(cudaMemcpy(tab.data(), h->A.nbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < n; ++p)
+            for (int k = 0; k < cnt[p]; ++k) nbr[(size_t)orig[p] * *stride + k] = orig[tab[(size_t)k * np + p]] + 1;
+    }
+    if (g_nbr && g_stride) {
+        std::vector<int> tab((size_t)h->A.gstride * np);
+        CK(cudaMemcpy(tab.data(), h->A.gnbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < n; ++p)
+            for (int k = 0; k < gcnt[p]; ++k) g_nbr[(size_t)orig[p] * *g_stride + k] = tab[(size_t)k * np + p] + 1;
+    }
+    return MCM_OK;
+}
+
+int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, int cap) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    int n = 0;
+    CK(cudaMemcpy(&n, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ngp) *ngp = n;
+    int m = std::min(n, cap);
+    if (m <= 0) return MCM_OK;
+    std::vector<int> orig(h->np);
+    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+    if (par) {
+        std::vector<int> gp(m);
+        CK(cudaMemcpy(gp.data(), h->A.gpar, sizeof(int) * m, cudaMemcpyDeviceToHost));
+        for (int g = 0; g < m; ++g) par[g] = orig[gp[g]] + 1;
+    }
+    std::vector<double> tmp(m);
+    double *const xs[3] = {h->A.gx, h->A.gy, h->A.gz};
+    double *const vs[3] = {h->A.gvx, h->A.gvy, h->A.gvz};
+    for (int k = 0; k < 3; ++k) {
+        if (x) {
+            CK(cudaMemcpy(tmp.data(), xs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
+            for (int g = 0; g < m; ++g) x[3 * (size_t)g + k] = tmp[g];
+        }
+        if (v) {
+            CK(cudaMemcpy(tmp.data(), vs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
+            for (int g = 0; g < m; ++g) v[3 * (size_t)g + k] = tmp[g];
+        }
+    }
+    return MCM_OK;
+}
+
+int mcm_gpu_grid(mcm_gpu_handle *h, int *gridlim, double *gridmin, double *gridsize) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    DevGrid g;
+    CK(cudaMemcpy(&g, h->A.grid, sizeof(g), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3; ++k) {
+        if (gridlim) gridlim[k] = g.gridlim[k];
+        if (gridmin) gridmin[k] = g.gridmin[k];
+        if (gridsize) gridsize[k] = g.gridsize[k];
+    }
+    return MCM_OK;
+}
+
+int mcm_gpu_energies(mcm_gpu_handle *h, double *energies) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (!energies) return MCM_EINVAL;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(energies, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost));
+    return MCM_OK;
+}
+
+int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    if (mean_nbr) {
+        std::vector<int> cnt(h->np), gcnt(h->np);
+        CK(cudaMemcpy(cnt.data(), h->A.nnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gcnt.data(), h->A.gnnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+        double s = 0.0;
+        for (int p = 0; p < h->np; ++p) s += cnt[p] + gcnt[p];
+        *mean_nbr = s / h->np;
+    }
+    if (max_nbr) {
+        DevStatus s;
+        CK(cudaMemcpy(&s, h->A.status, sizeof(s), cudaMemcpyDeviceToHost));
+        *max_nbr = s.max_nbr;
+    }
+    if (stride) *stride = h->A.stride;
+    if (ngp) CK(cudaMemcpy(ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
+    return MCM_OK;
+}
+
+}  // extern "C"

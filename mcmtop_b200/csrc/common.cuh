@@ -1,0 +1,98 @@
+// common.cuh -- device data layout shared by the kernels of the MCM step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mcm_gpu.h"
+
+namespace mcm {
+
+constexpr int kMaxMat = MCM_GPU_MAX_MATERIALS;
+constexpr int kWarp = 32;
+constexpr int kNoCell = -1;
+
+// Material constants on the device (mirrors mcm_gpu_material).
+struct DevMaterial {
+    int model, eos, visc_type, pad;
+    double rho, g, av_l, av_q, mass, h, rho_min, rho_max;
+    double strinput[48];
+    double eosinput[24];
+};
+
+// Scalars of the time loop kept on the device so that whole steps can be
+// enqueued (and captured) without host round trips.
+struct DevTime {
+    double dt, dtold, ptime, endtime;
+    double critts;
+    int ended;        // MCM/mcm_solution.f90:101 fired
+    int steps_done;   // completed loop iterations in the current mcm_gpu_run
+};
+
+// First error raised on the device; later kernels of the step return early.
+struct DevStatus {
+    int code;
+    int req_stride;   // neighbour-table width needed (real part)
+    int req_gstride;  // neighbour-table width needed (ghost part)
+    int req_ngp;      // ghost storage needed
+    long long req_cells;
+    int bad_index;
+    int max_nbr, max_gnbr;
+    unsigned long long sum_nbr;  // for the mean neighbour count
+};
+
+// Linked-list grid of MCM/mcm_setuplist.f90, recomputed every step.
+struct DevGrid {
+    double gridmin[3];
+    double gridsize[3];
+    int gridlim[3];
+    int pad;
+    long long ncells;
+};
+
+// Boundary planes (MCM/mcm_init_boundary.f90:28-116).
+struct DevPlanes {
+    int code[2][3];
+    double bx[2][3];
+    int type[3];
+    double mult[6][3];
+    double add[6][3];
+};
+
+// Run options used inside kernels.
+struct DevParams {
+    int ndim, disctype, tcrit_opt, boundary, baseaccel, drelax, nmat, diag;
+    double drelax_scale, tssf, hmax;
+    double base_a[3];
+    DevPlanes planes;
+};
+
+// Per-particle field identifiers of the FP64 state (one array of npad
+// doubles each).  Symmetric tensors keep 6 components: 11 22 33 12 13 23.
+enum Field {
+    FX = 0, FY, FZ, FVX, FVY, FVZ, FH, FMASS, FRHO, FE, FP, FC, FEFPS, FPCUT, FPCUT2, FFAIL, FVABS, FHOLD,
+    FS11, FS22, FS33, FS12, FS13, FS23,      // sigma
+    FQ,                                      // isotropic artificial viscosity
+    FD11, FD22, FD33, FD12, FD13, FD23,      // deviator s
+    FA11, FA22, FA33, FA12, FA13, FA23,      // back stress alfa (model 3)
+    FCAPA,
+    // diagnostics refreshed by the split path (and on request)
+    FR11, FR22, FR33, FR12, FR13, FR23,      // rod
+    FW12, FW13, FW23,                        // spin
+    FTR, FETRY, FEINC, FRHOOLD, FMINDIST, FCRITTS, FAX, FAY, FAZ,
+    NFIELD
+};
+
+struct Fields {
+    double *f[NFIELD];
+    int *mat, *dispbc, *orig, *ptype;
+};
+
+__host__ __device__ inline long long cell_key(int bx, int by, int bz, const int *gl) {
+    return (long long)(bx - 1) + (long long)gl[0] * ((long long)(by - 1) + (long long)gl[1] * (long long)(bz - 1));
+}
+
+__device__ __forceinline__ void raise_status(DevStatus *st, int code, int idx = -1) {
+    if (atomicCAS(&st->code, 0, code) == 0) st->bad_index = idx;
+}
+
+}  // namespace mcm

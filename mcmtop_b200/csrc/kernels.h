@@ -1,0 +1,81 @@
+// kernels.h -- launch interface between the C-ABI host code and the kernel
+// translation units.  StepArgs carries every device pointer and size a step
+// needs; it is passed by value to the kernels.
+#pragma once
+#include "common.cuh"
+
+namespace mcm {
+
+struct StepArgs {
+    int n;            // particles
+    int npad;         // column pitch of per-particle arrays (multiple of 32)
+    int nmat;
+    int stride;       // neighbour-table width, real neighbours (incl. contacts and self)
+    int gstride;      // neighbour-table width, ghost neighbours
+    int ghost_cap;    // ghost storage
+    long long cell_cap;   // cell-array storage
+    int layer_cap;    // scratch for one boundary layer
+    int split_mode;   // 1: step_a/b/c entry points (dt supplied by the host); 0: fused run
+    DevParams prm;
+    const DevMaterial *mats;
+    Fields F;
+    DevTime *time;
+    DevStatus *status;
+    DevGrid *grid;
+    double *bbox;     // [2][3]: min, max (mcm_coord_maxmin)
+    // cell list
+    int *key;         // per particle cell key or -1
+    int *cell_count;  // cell_cap
+    int *cell_start;  // cell_cap + 1
+    int *cell_list;   // npad
+    int *scan_sums;   // block sums of the scan
+    int2 *gcell;      // per cell: first ghost index, ghost count
+    // ghosts (SoA, ghost_cap each)
+    double *gx, *gy, *gz, *gvx, *gvy, *gvz, *gmass, *gh, *ghold, *grho;
+    int *gpar, *gmat;
+    int *ngp;         // device ghost counter
+    int *plane_base;  // ghost index base of the plane being built
+    int *layer_count, *layer_off;
+    // neighbour table (column-major: entry k of particle i at k*npad + i)
+    int *nbr, *gnbr, *nnbr, *gnnbr;
+    // gather records
+    double4 *rec0, *rec1, *rec2;   // per particle
+    double4 *grec0, *grec1, *grec2;  // per ghost
+    float4 *frec0, *frec1, *frec2;   // mixed path
+    float4 *gfrec0, *gfrec1, *gfrec2;
+    // reductions
+    double *red;      // block partials
+    int red_blocks;
+    double *energy;   // 5*nmat + 3
+};
+
+// cells.cu
+void launch_grid_setup(const StepArgs &a, cudaStream_t s);
+void launch_cell_build(const StepArgs &a, cudaStream_t s);
+void launch_ghosts(const StepArgs &a, cudaStream_t s);
+void launch_search(const StepArgs &a, cudaStream_t s);
+size_t search_smem_bytes(const StepArgs &a);
+
+// reduce.cu
+void launch_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks);
+void launch_init_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks);
+void launch_energy_bbox_reduce(const StepArgs &a, cudaStream_t s, int nblocks, int energy, int bbox);
+void launch_set_time(const StepArgs &a, cudaStream_t s, double dt, double dtold, int set_dtold);
+void launch_finish_step(const StepArgs &a, cudaStream_t s);
+
+// step kernels (one namespace per arithmetic flavour)
+#define MCM_DECLARE_STEP(NS)                                                        \
+    namespace NS {                                                                  \
+    int launch_strain_constitutive(const StepArgs &a, cudaStream_t s);              \
+    int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);          \
+    int launch_update_move(const StepArgs &a, cudaStream_t s);                      \
+    int launch_initial(const StepArgs &a, cudaStream_t s, int massopt, int init_h_opt, int init_rhoe, const int *nppermat); \
+    int launch_init_critts(const StepArgs &a, cudaStream_t s);                      \
+    }
+MCM_DECLARE_STEP(exact)
+MCM_DECLARE_STEP(fast)
+#undef MCM_DECLARE_STEP
+
+constexpr int kRedThreads = 256;
+
+}  // namespace mcm

@@ -1,0 +1,801 @@
+// step_fp64.cuh -- FP64 kernels of the MCM explicit step: strain-rate gather
+// fused with the constitutive update and the critical-timestep reduction, and
+// the momentum gather fused with boundary conditions, energy sums, velocity
+// update and position update.
+//
+// Included by two translation units: MCM_FLAVOUR_EXACT (compiled without
+// fused multiply-add; reference expression order and divisions, so the
+// result follows the reference arithmetic) and MCM_FLAVOUR_FAST (fused
+// multiply-add and reciprocals).  Each thread owns one particle and walks its
+// neighbours in the reference order; the sums are sequential, so there are no
+// atomics and the FP64-exact flavour accumulates in the reference's order.
+#pragma once
+#include "kernels.h"
+#include "physics.cuh"
+
+#ifndef MCM_FLAVOUR_NS
+#error "define MCM_FLAVOUR_NS (exact or fast)"
+#endif
+
+namespace mcm {
+namespace MCM_FLAVOUR_NS {
+
+constexpr double kPi = 3.141592653589793;   // acos(-1) (MCM/mcm_startup.f90:33)
+
+// A step is skipped once an error is raised or after the terminating step
+// (time->ended == 2); the terminating step itself (ended == 1) still runs the
+// momentum and energy part, as MCM/mcm_solution.f90:69-101 does.
+__device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
+
+// Cubic B-spline gradient, 3-D (MCM/mcm_gradw.f90:321-383), xij = xi - xj.
+__device__ __forceinline__ void gradw(double x0, double x1, double x2, double havg, double &d0, double &d1,
+                                      double &d2) {
+#if MCM_EXACT
+    double const1 = 1.0 / (kPi * havg * havg * havg);
+    double const2 = const1 * 0.25;
+    double rad = x0 * x0;
+    rad = rad + x1 * x1;
+    rad = rad + x2 * x2;
+    rad = sqrt(rad);
+    double z = rad / havg;
+    double dw;
+    if (z < 1.0) dw = const1 * ((9.0 / 4.0 * z - 3.0) * z);
+    else if (z < 2.0) { double t = 2.0 - z; dw = -3.0 * const2 * (t * t); }
+    else dw = 0.0;
+    if (rad == 0.0) { d0 = d1 = d2 = 0.0; }
+    else {
+        double den = rad * havg;
+        d0 = dw * x0 / den;
+        d1 = dw * x1 / den;
+        d2 = dw * x2 / den;
+    }
+#else
+    double ih = 1.0 / havg;
+    double r2 = fma(x0, x0, fma(x1, x1, x2 * x2));
+    double rad = sqrt(r2);
+    double z = rad * ih;
+    double const1 = (1.0 / kPi) * ih * ih * ih;
+    double dw;
+    if (z < 1.0) dw = const1 * ((2.25 * z - 3.0) * z);
+    else if (z < 2.0) { double t = 2.0 - z; dw = -0.75 * const1 * (t * t); }
+    else dw = 0.0;
+    if (rad == 0.0) { d0 = d1 = d2 = 0.0; }
+    else {
+        double f = dw * ih / rad;
+        d0 = f * x0; d1 = f * x1; d2 = f * x2;
+    }
+#endif
+}
+
+// Cubic B-spline kernel, 3-D (MCM/mcm_kernel.f90:227-280).
+__device__ __forceinline__ double kernelw(double x0, double x1, double x2, double havg) {
+#if MCM_EXACT
+    double const1 = 1.0 / (kPi * havg * havg * havg);
+    double const2 = const1 / 4.0;
+    double rad = x0 * x0;
+    rad = rad + x1 * x1;
+    rad = rad + x2 * x2;
+    rad = sqrt(rad);
+    double z = rad / havg;
+    if (z < 1.0) return const1 * (((0.75 * z - 1.5) * z) * z + 1.0);
+    if (z < 2.0) { double t = 2.0 - z; return const2 * (t * t * t); }
+    return 0.0;
+#else
+    double ih = 1.0 / havg;
+    double rad = sqrt(fma(x0, x0, fma(x1, x1, x2 * x2)));
+    double z = rad * ih;
+    double const1 = (1.0 / kPi) * ih * ih * ih;
+    if (z < 1.0) return const1 * (((0.75 * z - 1.5) * z) * z + 1.0);
+    if (z < 2.0) { double t = 2.0 - z; return 0.25 * const1 * (t * t * t); }
+    return 0.0;
+#endif
+}
+
+// 3x3 inverse with the reference's singular fallback (MCM/mcm_math_func.f90:199-228).
+__device__ __forceinline__ void inverse3(const double M[3][3], double inv[3][3]) {
+    double sd00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+    double sd01 = M[1][0] * M[2][2] - M[1][2] * M[2][0];
+    double sd02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+    double sd10 = M[0][1] * M[2][2] - M[0][2] * M[2][1];
+    double sd11 = M[0][0] * M[2][2] - M[0][2] * M[2][0];
+    double sd12 = M[0][0] * M[2][1] - M[0][1] * M[2][0];
+    double sd20 = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+    double sd21 = M[0][0] * M[1][2] - M[0][2] * M[1][0];
+    double sd22 = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+    double det = M[0][0] * sd00 - M[0][1] * sd01 + M[0][2] * sd02;
+    if (fabs(det) < 1.0e-08) {
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) inv[r][c] = (r == c) ? 1.0 : 0.0;
+    } else {
+        double invdet = 1.0 / det;
+        inv[0][0] = sd00 * invdet; inv[0][1] = -sd10 * invdet; inv[0][2] = sd20 * invdet;
+        inv[1][0] = -sd01 * invdet; inv[1][1] = sd11 * invdet; inv[1][2] = -sd21 * invdet;
+        inv[2][0] = sd02 * invdet; inv[2][1] = -sd12 * invdet; inv[2][2] = sd22 * invdet;
+    }
+}
+
+// Loads the state one particle's constitutive update reads.  The deviator s
+// persists only for model 9 (s(1,2) is never reassigned, MCM/mcm_f3dm9.f90:
+// 273-281), alfa only for model 3 and the previous q only for models 1 and 3
+// (their energy increment uses it before mcm_aviscosity).
+__device__ __forceinline__ void load_state(const StepArgs &a, int i, PState<double> &P, int model) {
+    const double *const *f = a.F.f;
+    P.mat = a.F.mat[i];
+    P.mass = f[FMASS][i]; P.h = f[FH][i]; P.hold = f[FHOLD][i];
+    P.rho = f[FRHO][i]; P.e = f[FE][i]; P.p = f[FP][i]; P.c = f[FC][i];
+    P.efps = f[FEFPS][i]; P.pcut = f[FPCUT][i]; P.p_cut = f[FPCUT2][i]; P.fail = f[FFAIL][i];
+    P.capa = 0.0;
+    P.rho0 = a.mats[P.mat - 1].rho;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) { P.sig[t] = f[FS11 + t][i]; P.s[t] = 0.0; P.alfa[t] = 0.0; }
+    if (model == 9) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) P.s[t] = f[FD11 + t][i];
+    }
+    if (model == 3) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) P.alfa[t] = f[FA11 + t][i];
+    }
+    P.q = (model == 1 || model == 3) ? f[FQ][i] : 0.0;
+    P.etry = 0.0; P.einc = 0.0; P.rhoold = P.rho;
+}
+
+__device__ __forceinline__ void store_state(const StepArgs &a, int i, const PState<double> &P, int model) {
+    double *const *f = a.F.f;
+    f[FH][i] = P.h;
+    f[FRHO][i] = P.rho; f[FE][i] = P.e; f[FP][i] = P.p; f[FC][i] = P.c;
+    f[FEFPS][i] = P.efps; f[FPCUT][i] = P.pcut; f[FPCUT2][i] = P.p_cut; f[FFAIL][i] = P.fail;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) f[FS11 + t][i] = P.sig[t];
+    f[FQ][i] = P.q;
+    if (a.prm.diag || model == 9) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) f[FD11 + t][i] = P.s[t];
+    }
+    if (model == 3) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) f[FA11 + t][i] = P.alfa[t];
+    }
+    if (a.prm.diag) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) f[FR11 + t][i] = P.rod[t];
+        f[FW12][i] = P.spin[0]; f[FW13][i] = P.spin[1]; f[FW23][i] = P.spin[2];
+        f[FTR][i] = P.tracerod; f[FETRY][i] = P.etry; f[FEINC][i] = P.einc; f[FRHOOLD][i] = P.rhoold;
+    }
+}
+
+// ------------------------------------------------------------ strain prep
+// Gather records for the strain loop: positions shifted back half a step
+// (MCM/mcm_strain.f90:27-31) and V_j = m_j/rho_j (MCM/mcm_oldstrain.f90:105).
+// Ghosts keep their unshifted positions, as in the reference.
+__global__ void k_strain_prep(StepArgs a) {
+    if (skip_step(a)) return;
+    const double dt = a.time->dt;
+    const double *const *f = a.F.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
+        double x = f[FX][i] - 0.5 * vx * dt;
+        double y = f[FY][i] - 0.5 * vy * dt;
+        double z = f[FZ][i] - 0.5 * vz * dt;
+        a.rec0[i] = make_double4(x, y, z, f[FH][i]);
+        a.rec1[i] = make_double4(vx, vy, vz, f[FMASS][i] / f[FRHO][i]);
+    }
+    if (a.prm.boundary) {
+        const int ngp = *a.ngp;
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngp; g += gridDim.x * blockDim.x) {
+            a.grec0[g] = make_double4(a.gx[g], a.gy[g], a.gz[g], a.gh[g]);
+            a.grec1[g] = make_double4(a.gvx[g], a.gvy[g], a.gvz[g], a.gmass[g] / a.grho[g]);
+        }
+    }
+}
+
+template <int DISC>
+__device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const double4 xi, const double4 vi,
+                                              double gv[3][3]) {
+    const int nn = a.nnbr[i], gn = a.gnnbr[i];
+    const int np = a.npad;
+    if (DISC == 0) {
+        // MCM/mcm_oldstrain.f90:95-115
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, vj;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+            double Volj = vj.w;
+            double havg = 0.5 * (xi.w + xj.w);
+            double d[3];
+            gradw(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, havg, d[0], d[1], d[2]);
+            const double dv[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                double t = Volj * dv[n];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + t * d[m];
+            }
+        }
+    } else {
+        // MCM/mcm_corr_strain.f90:51-134 (three passes, kernel centred at i)
+        double sum_w = 0.0, sg[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, vj;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+            double Volj = vj.w;
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            sum_w = sum_w + Volj * w;
+#pragma unroll
+            for (int l = 0; l < 3; ++l) sg[l] = sg[l] + Volj * d[l];
+        }
+        double B[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double sw2 = sum_w * sum_w;
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, vj;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+            double Volj = vj.w;
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            double cg[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cg[m] = (d[m] * sum_w - w * sg[m]) / sw2;
+            const double xr[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int n = 0; n < 3; ++n) B[n][m] = B[n][m] + Volj * xr[n] * cg[m];
+        }
+        double invB[3][3];
+        inverse3(B, invB);
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, vj;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+            double Volj = vj.w;
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            double cg[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cg[m] = (d[m] * sum_w - w * sg[m]) / sw2;
+            double c2[3];
+#pragma unroll
+            for (int n = 0; n < 3; ++n) c2[n] = invB[n][0] * cg[0] + invB[n][1] * cg[1] + invB[n][2] * cg[2];
+            const double vv[3] = {vj.x, vj.y, vj.z};
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                double t = Volj * vv[n];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + t * c2[m];
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ double block_min(double v, double *sm) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : 1.0e300;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// --------------------------------------------- strain + constitutive update
+// MCM/mcm_strain.f90, mcm_oldstrain.f90 / mcm_corr_strain.f90, mcm_rhoupd.f90,
+// mcm_constitutive.f90:29-83 and mcm_calccritts.f90 for one particle.
+template <int DISC>
+__global__ void __launch_bounds__(kRedThreads) k_strain_const(StepArgs a) {
+    __shared__ double sm[32];
+    if (skip_step(a)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dt = a.time->dt;
+    double crit = 1.0e20;
+    bool bad = false;
+    if (i < a.n) {
+        const double4 xi = a.rec0[i], vi = a.rec1[i];
+        double gv[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        strain_gather<DISC>(a, i, xi, vi, gv);
+        PState<double> P;
+        const DevMaterial &M = a.mats[a.F.mat[i] - 1];
+        load_state(a, i, P, M.model);
+        P.rod[T11] = 0.5 * (gv[0][0] + gv[0][0]);
+        P.rod[T22] = 0.5 * (gv[1][1] + gv[1][1]);
+        P.rod[T33] = 0.5 * (gv[2][2] + gv[2][2]);
+        P.rod[T12] = 0.5 * (gv[0][1] + gv[1][0]);
+        P.rod[T13] = 0.5 * (gv[0][2] + gv[2][0]);
+        P.rod[T23] = 0.5 * (gv[1][2] + gv[2][1]);
+        P.spin[0] = 0.5 * (gv[0][1] - gv[1][0]);
+        P.spin[1] = 0.5 * (gv[0][2] - gv[2][0]);
+        P.spin[2] = 0.5 * (gv[1][2] - gv[2][1]);
+        P.tracerod = P.rod[T11] + P.rod[T22] + P.rod[T33];
+        rhoupd(P, M, dt, 3);
+        bad = !constitutive_particle(P, M, dt);
+        const double vx = a.F.f[FVX][i], vy = a.F.f[FVY][i], vz = a.F.f[FVZ][i];
+        const double mindist = (a.prm.tcrit_opt == 2) ? a.F.f[FMINDIST][i] : 0.0;
+        crit = critts_particle(P, M, a.prm.tcrit_opt, 3, a.F.f[FVABS][i], mindist);
+        store_state(a, i, P, M.model);
+        if (a.prm.diag) a.F.f[FCRITTS][i] = crit;
+        // MCM/mcm_strain.f90:56-60: positions forward again
+        a.F.f[FX][i] = xi.x + 0.5 * vx * dt;
+        a.F.f[FY][i] = xi.y + 0.5 * vy * dt;
+        a.F.f[FZ][i] = xi.z + 0.5 * vz * dt;
+    }
+    if (bad) raise_status(a.status, MCM_ECOMPLEX_C, i);
+    double m = block_min(crit, sm);
+    if (threadIdx.x == 0) a.red[blockIdx.x] = m;
+}
+
+// --------------------------------------------------------- momentum prep
+// Gather records: x, h; (sigma - q)/rho^2 (MCM/mcm_oldacceleration.f90:79-80);
+// mass.  Ghost stresses follow MCM/mcm_update_ghost_stress.f90:272-285 (all
+// off-diagonals negated) with the ghost's own density from its creation.
+__global__ void k_mom_prep(StepArgs a) {
+    if (skip_step(a)) return;
+    const double *const *f = a.F.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double rho = f[FRHO][i];
+        double r2 = rho * rho;
+        double q = f[FQ][i];
+        a.rec0[i] = make_double4(f[FX][i], f[FY][i], f[FZ][i], f[FH][i]);
+        a.rec1[i] = make_double4((f[FS11][i] - q) / r2, (f[FS22][i] - q) / r2, (f[FS33][i] - q) / r2,
+                                 (f[FS12][i] - 0.0) / r2);
+        a.rec2[i] = make_double4((f[FS13][i] - 0.0) / r2, (f[FS23][i] - 0.0) / r2, f[FMASS][i], 0.0);
+    }
+    if (a.prm.boundary) {
+        const int ngp = *a.ngp;
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngp; g += gridDim.x * blockDim.x) {
+            int j = a.gpar[g];
+            double rho = a.grho[g];
+            double r2 = rho * rho;
+            double q = f[FQ][j];
+            a.grec0[g] = make_double4(a.gx[g], a.gy[g], a.gz[g], a.gh[g]);
+            a.grec1[g] = make_double4((f[FS11][j] - q) / r2, (f[FS22][j] - q) / r2, (f[FS33][j] - q) / r2,
+                                      ((-f[FS12][j]) - (-0.0)) / r2);
+            a.grec2[g] = make_double4(((-f[FS13][j]) - (-0.0)) / r2, ((-f[FS23][j]) - (-0.0)) / r2, a.gmass[g], 0.0);
+        }
+    }
+}
+
+__device__ __forceinline__ void sym_from_rec(const double4 &r1, const double4 &r2, double A[3][3]) {
+    A[0][0] = r1.x; A[1][1] = r1.y; A[2][2] = r1.z;
+    A[0][1] = A[1][0] = r1.w;
+    A[0][2] = A[2][0] = r2.x;
+    A[1][2] = A[2][1] = r2.y;
+}
+
+template <int DISC>
+__device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double acc[3]) {
+    const int nn = a.nnbr[i], gn = a.gnnbr[i];
+    const int np = a.npad;
+    const double4 xi = a.rec0[i];
+    double Ai[3][3];
+    sym_from_rec(a.rec1[i], a.rec2[i], Ai);
+    if (DISC == 0) {
+        // MCM/mcm_oldacceleration.f90:66-89
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, r1, r2;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r1 = a.rec1[j]; r2 = a.rec2[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r1 = a.grec1[q]; r2 = a.grec2[q]; }
+            double havg = 0.5 * (xi.w + xj.w);
+            double d[3];
+            gradw(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, havg, d[0], d[1], d[2]);
+            double Aj[3][3];
+            sym_from_rec(r1, r2, Aj);
+            const double massj = r2.z;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                double ds = 0.0;
+#pragma unroll
+                for (int m = 0; m < 3; ++m) ds = ds + (Aj[m][n] + Ai[m][n]) * d[m];
+                acc[n] = acc[n] + massj * ds;
+            }
+        }
+    } else {
+        // MCM/mcm_corr_acceleration.f90:63-161 (kernel centred at j; the self
+        // slot k = nnbr is zeroed; the final sum uses the last neighbour's mass)
+        double sum_w = 0.0, sg[3] = {0.0, 0.0, 0.0};
+        double massj = 0.0;
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, r2;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r2 = a.rec2[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r2 = a.grec2[q]; }
+            // V_j = m_j/rho_j with the current density: rebuilt from the record
+            massj = r2.z;
+            double rhoj = (k < nn) ? a.F.f[FRHO][a.nbr[(size_t)k * np + i]] : a.grho[a.gnbr[(size_t)(k - nn) * np + i]];
+            double Volj = massj / rhoj;
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            sum_w = sum_w + Volj * w;
+#pragma unroll
+            for (int l = 0; l < 3; ++l) sg[l] = sg[l] + Volj * d[l];
+        }
+        double B[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double sw2 = sum_w * sum_w;
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, r2;
+            double rhoj;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r2 = a.rec2[j]; rhoj = a.F.f[FRHO][j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r2 = a.grec2[q]; rhoj = a.grho[q]; }
+            double Volj = r2.z / rhoj;
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            double cg[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cg[m] = (d[m] * sum_w - w * sg[m]) / sw2;
+            const double xr[3] = {dx, dy, dz};
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int n = 0; n < 3; ++n) B[n][m] = B[n][m] + Volj * xr[n] * cg[m];
+        }
+        double invB[3][3];
+        inverse3(B, invB);
+        // deltasig(m,n,l) is symmetric in (m,n): keep 6 x 3 accumulators
+        double ds[6][3];
+#pragma unroll
+        for (int t = 0; t < 6; ++t) ds[t][0] = ds[t][1] = ds[t][2] = 0.0;
+        for (int k = 0; k < nn + gn; ++k) {
+            double4 xj, r1, r2;
+            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r1 = a.rec1[j]; r2 = a.rec2[j]; }
+            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r1 = a.grec1[q]; r2 = a.grec2[q]; }
+            double havg = 0.5 * (xi.w + xj.w);
+            double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double w = kernelw(dx, dy, dz, havg);
+            double d[3];
+            gradw(dx, dy, dz, havg, d[0], d[1], d[2]);
+            double cg[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cg[m] = (d[m] * sum_w - w * sg[m]) / sw2;
+            double Aj[3][3];
+            sym_from_rec(r1, r2, Aj);
+            const bool self_slot = (k == nn - 1);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                const int m = (t < 3) ? t : (t == 5 ? 1 : 0);
+                const int n = (t < 3) ? t : (t == 3 ? 1 : 2);
+                double dsig = Aj[m][n] + Ai[m][n];
+                if (self_slot) dsig = 0.0;
+#pragma unroll
+                for (int l = 0; l < 3; ++l) ds[t][l] = ds[t][l] + dsig * cg[l];
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int l = 0; l < 3; ++l) acc[n] = acc[n] + massj * ds[sym_index(n, m)][l] * invB[l][m];
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sm[k];
+    return r;
+}
+
+__device__ __forceinline__ double block_minmax(double v, double *sm, bool is_max) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double y = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_max ? fmax(v, y) : fmin(v, y);
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = v;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = is_max ? fmax(r, sm[k]) : fmin(r, sm[k]);
+    return r;
+}
+
+// Velocity update (MCM/mcm_update_velocity.f90:29-56) and position update
+// (MCM/mcm_move.f90:32-40) of one particle; check_sym_pen is per particle
+// because the reference's global test "bbox below the plane" selects exactly
+// the particles below it (MCM/mcm_check_sym_pen.f90:27-179).
+__device__ __forceinline__ void integrate_particle(const StepArgs &a, int i, const double acc[3], double dt, double dtold,
+                                                   double x[3]) {
+    double *const *f = a.F.f;
+    double dtn = 0.5 * (dt + dtold);
+    double v[3] = {f[FVX][i], f[FVY][i], f[FVZ][i]};
+    double vabs = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        if (a.prm.drelax) v[j] = a.prm.drelax_scale * v[j] + acc[j] * dtn;
+        else v[j] = v[j] + acc[j] * dtn;
+        vabs = vabs + v[j] * v[j];
+    }
+    vabs = sqrt(vabs);
+    x[0] = f[FX][i]; x[1] = f[FY][i]; x[2] = f[FZ][i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) x[j] = x[j] + v[j] * dt;
+    double xo[3] = {x[0], x[1], x[2]};
+    if (a.prm.boundary) {
+        const DevPlanes &pl = a.prm.planes;
+        for (int d = 0; d < 3; ++d) {
+            if (pl.code[0][d] == 1 && xo[d] < pl.bx[0][d]) { xo[d] = 2.0 * pl.bx[0][d] - xo[d]; v[d] = -v[d]; }
+            if (pl.code[1][d] == 1 && xo[d] > pl.bx[1][d]) { xo[d] = 2.0 * pl.bx[1][d] - xo[d]; v[d] = -v[d]; }
+            if (pl.code[0][d] == 2) {
+                double dx = pl.bx[1][d] - pl.bx[0][d];
+                if (xo[d] < pl.bx[0][d]) xo[d] = xo[d] + dx;
+                if (xo[d] > pl.bx[1][d]) xo[d] = xo[d] - dx;
+            }
+        }
+    }
+    f[FVX][i] = v[0]; f[FVY][i] = v[1]; f[FVZ][i] = v[2];
+    f[FVABS][i] = vabs;
+    f[FX][i] = xo[0]; f[FY][i] = xo[1]; f[FZ][i] = xo[2];
+}
+
+// ----------------------------------------------- momentum + integration
+// Writes a (split path), adds base accelerations and displacement BCs
+// (MCM/mcm_boundcond.f90:23-62), block partial energy sums
+// (MCM/mcm_calctotale.f90:33-51) and, when integrate is set and the run has
+// not terminated, the velocity and position update with block bbox partials.
+template <int DISC>
+__global__ void __launch_bounds__(kRedThreads) k_momentum(StepArgs a, int integrate) {
+    __shared__ double sm[32];
+    if (skip_step(a)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nm = a.nmat;
+    double acc[3] = {0.0, 0.0, 0.0};
+    int mati = 0;
+    double ke = 0.0, ie = 0.0, mo[3] = {0.0, 0.0, 0.0};
+    double x[3] = {1.0e20, 1.0e20, 1.0e20};
+    double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
+    const bool do_int = integrate && !a.time->ended;
+    if (i < a.n) {
+        double *const *f = a.F.f;
+        momentum_gather<DISC>(a, i, acc);
+        if (a.prm.baseaccel)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[j] = acc[j] + a.prm.base_a[j];
+        switch (a.F.dispbc[i]) {
+            case 1: acc[0] = 0.0; break;
+            case 2: acc[1] = 0.0; break;
+            case 3: acc[2] = 0.0; break;
+            case 4: acc[0] = 0.0; acc[1] = 0.0; break;
+            case 5: acc[1] = 0.0; acc[2] = 0.0; break;
+            case 6: acc[0] = 0.0; acc[2] = 0.0; break;
+            case 7: acc[0] = 0.0; acc[1] = 0.0; acc[2] = 0.0; break;
+            default: break;
+        }
+        if (a.split_mode || a.prm.diag) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
+        mati = a.F.mat[i];
+        const double mass = f[FMASS][i], vabs = f[FVABS][i];
+        ke = 0.5 * mass * (vabs * vabs);
+        mo[0] = mass * fabs(f[FVX][i]);
+        mo[1] = mass * fabs(f[FVY][i]);
+        mo[2] = mass * fabs(f[FVZ][i]);
+        ie = f[FE][i];
+        if (do_int) {
+            double xn[3];
+            integrate_particle(a, i, acc, a.time->dt, a.time->dtold, xn);
+            x[0] = xn[0]; x[1] = xn[1]; x[2] = xn[2];
+            xmax[0] = xn[0]; xmax[1] = xn[1]; xmax[2] = xn[2];
+        }
+    }
+    // per-block partials: [5*nmat energies][6 bbox]
+    const int stride = 5 * nm + 6;
+    double *out = a.red + (size_t)blockIdx.x * stride;
+    for (int m = 1; m <= nm; ++m) {
+        bool mine = (mati == m);
+        double v0 = block_sum(mine ? ke : 0.0, sm);
+        double v1 = block_sum(mine ? ie : 0.0, sm);
+        double v2 = block_sum(mine ? mo[0] : 0.0, sm);
+        double v3 = block_sum(mine ? mo[1] : 0.0, sm);
+        double v4 = block_sum(mine ? mo[2] : 0.0, sm);
+        if (threadIdx.x == 0) {
+            out[5 * (m - 1) + 0] = v0; out[5 * (m - 1) + 1] = v1;
+            out[5 * (m - 1) + 2] = v2; out[5 * (m - 1) + 3] = v3; out[5 * (m - 1) + 4] = v4;
+        }
+    }
+    if (do_int) {
+        for (int d = 0; d < 3; ++d) {
+            double lo = block_minmax(x[d], sm, false);
+            double hi = block_minmax(xmax[d], sm, true);
+            if (threadIdx.x == 0) { out[5 * nm + d] = lo; out[5 * nm + 3 + d] = hi; }
+        }
+    }
+}
+
+// Split path: velocity and position update after the host's output phase.
+__global__ void __launch_bounds__(kRedThreads) k_update_move(StepArgs a) {
+    __shared__ double sm[32];
+    if (a.status->code) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double x[3] = {1.0e20, 1.0e20, 1.0e20};
+    double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
+    if (i < a.n) {
+        double acc[3] = {a.F.f[FAX][i], a.F.f[FAY][i], a.F.f[FAZ][i]};
+        double xn[3];
+        integrate_particle(a, i, acc, a.time->dt, a.time->dtold, xn);
+        x[0] = xmax[0] = xn[0]; x[1] = xmax[1] = xn[1]; x[2] = xmax[2] = xn[2];
+    }
+    const int stride = 5 * a.nmat + 6;
+    double *out = a.red + (size_t)blockIdx.x * stride;
+    for (int d = 0; d < 3; ++d) {
+        double lo = block_minmax(x[d], sm, false);
+        double hi = block_minmax(xmax[d], sm, true);
+        if (threadIdx.x == 0) { out[5 * a.nmat + d] = lo; out[5 * a.nmat + 3 + d] = hi; }
+    }
+}
+
+// ------------------------------------------------------- initialisation
+// Per-particle part of mcm_initial (MCM/mcm_initial.f90:33-69):
+// init_boundcond, calcmass (counts in a.red), initvbls, calcrhopc/eoscalc,
+// initsigma, initrod, init_h, and the nodal AV with tracerod = 0.
+__global__ void k_initial(StepArgs a, int massopt, int init_h_opt, int init_rhoe, const int *nppermat) {
+    double *const *f = a.F.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const int mat = a.F.mat[i];
+        const DevMaterial &M = a.mats[mat - 1];
+        // MCM/mcm_init_boundcond.f90:25-54
+        switch (a.F.dispbc[i]) {
+            case 1: f[FVX][i] = 0.0; break;
+            case 2: f[FVY][i] = 0.0; break;
+            case 3: f[FVZ][i] = 0.0; break;
+            case 4: f[FVX][i] = 0.0; f[FVY][i] = 0.0; break;
+            case 5: f[FVY][i] = 0.0; f[FVZ][i] = 0.0; break;
+            case 6: f[FVX][i] = 0.0; f[FVZ][i] = 0.0; break;
+            case 7: f[FVX][i] = 0.0; f[FVY][i] = 0.0; f[FVZ][i] = 0.0; break;
+            default: break;
+        }
+        // MCM/mcm_calcmass.f90:129-137
+        if (massopt == 0) f[FMASS][i] = M.mass / (double)nppermat[mat - 1];
+        // MCM/mcm_initvbls.f90:48-75
+        PState<double> P;
+        P.mat = mat;
+        P.mass = f[FMASS][i];
+        P.efps = 0.0; P.fail = 1.0;
+        switch (M.model) {
+            case 1: case 3: case 4: P.pcut = -9.90E+20; break;
+            case 9: P.pcut = M.strinput[0]; break;
+            case 10: P.pcut = M.strinput[3]; break;
+            default: P.pcut = 0.0;
+        }
+        double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
+        double vabs = 0.0;
+        vabs = vabs + vx * vx; vabs = vabs + vy * vy; vabs = vabs + vz * vz;
+        f[FVABS][i] = sqrt(vabs);
+        // MCM/mcm_calcrhopc.f90:31-95
+        P.rho0 = M.rho;
+        P.tracerod = 0.0;
+        if (init_rhoe == 1) { P.rho = f[FRHO][i]; P.e = f[FE][i]; }
+        else { P.rho = 0.0; P.e = 0.0; }
+        P.p = 0.0; P.c = 0.0;
+        switch (M.model) {
+            case 1: case 3:
+                if (init_rhoe != 1) { P.rho = P.rho0; P.e = 0.0; }
+                P.p = 0.0;
+                P.c = sqrt(M.strinput[1] / P.rho);
+                break;
+            case 9: case 10: {
+                const double *ei = M.eosinput;
+                switch (M.eos) {
+                    case 1:
+                        if (init_rhoe != 1) { P.rho = P.rho0 / ei[8]; P.e = ei[7] * P.mass / P.rho; }
+                        eos1p(P, M); eos1c(P, M); break;
+                    case 4:
+                        if (init_rhoe != 1) { P.rho = P.rho0 / ei[7]; P.e = ei[6] * P.mass / P.rho; }
+                        eos4p(P, M); eos4c(P, M); break;
+                    case 13:
+                        if (init_rhoe != 1) { P.rho = P.rho0 / ei[3]; P.e = ei[2] * P.mass / P.rho; }
+                        eos13p(P, M); eos13c(P, M); break;
+                    case 28:
+                        if (init_rhoe != 1) { P.rho = P.rho0 / ei[3]; P.e = ei[2] * P.mass; }
+                        eos28p(P, M); eos28c(P, M); break;
+                    case 41:
+                        if (init_rhoe != 1) { P.rho = P.rho0 / ei[5]; P.e = ei[2] * ei[3] * P.mass / P.rho; }
+                        eos41p(P, M, 0.0);
+                        if (!eos41c(P, M)) raise_status(a.status, MCM_ECOMPLEX_C, i);
+                        break;
+                }
+                if (M.model == 9) {
+                    double pmax = M.strinput[0];
+                    if (P.p < pmax) P.p = pmax;
+                }
+                break;
+            }
+        }
+        f[FRHO][i] = P.rho; f[FE][i] = P.e; f[FP][i] = P.p; f[FC][i] = P.c;
+        f[FEFPS][i] = 0.0; f[FFAIL][i] = 1.0; f[FPCUT][i] = P.pcut; f[FPCUT2][i] = 0.0;
+        // MCM/mcm_initsigma.f90:26-49
+        f[FS11][i] = -P.p; f[FS22][i] = -P.p; f[FS33][i] = -P.p;
+        f[FS12][i] = 0.0; f[FS13][i] = 0.0; f[FS23][i] = 0.0;
+        for (int t = 0; t < 6; ++t) { f[FD11 + t][i] = 0.0; f[FA11 + t][i] = 0.0; f[FR11 + t][i] = 0.0; }
+        f[FW12][i] = f[FW13][i] = f[FW23][i] = 0.0;
+        // MCM/mcm_init_h.f90:22-48
+        if (init_h_opt == 0) f[FH][i] = M.h;
+        f[FHOLD][i] = f[FH][i];
+        // MCM/mcm_initial.f90:62-69: tracerod = 0 gives q = 0
+        f[FQ][i] = 0.0;
+        f[FTR][i] = 0.0;
+        f[FRHOOLD][i] = P.rho;
+        f[FETRY][i] = 0.0; f[FEINC][i] = 0.0; f[FCAPA][i] = 0.0;
+        f[FAX][i] = f[FAY][i] = f[FAZ][i] = 0.0;
+        f[FCRITTS][i] = 0.0;
+    }
+}
+
+// Critical timestep of the initial state (MCM/mcm_initial.f90:81).
+__global__ void __launch_bounds__(kRedThreads) k_init_critts(StepArgs a) {
+    __shared__ double sm[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double crit = 1.0e20;
+    if (i < a.n) {
+        PState<double> P;
+        const DevMaterial &M = a.mats[a.F.mat[i] - 1];
+        load_state(a, i, P, M.model);
+        P.tracerod = a.F.f[FTR][i];
+        const double mindist = (a.prm.tcrit_opt == 2) ? a.F.f[FMINDIST][i] : 0.0;
+        crit = critts_particle(P, M, a.prm.tcrit_opt, 3, a.F.f[FVABS][i], mindist);
+        a.F.f[FCRITTS][i] = crit;
+    }
+    double m = block_min(crit, sm);
+    if (threadIdx.x == 0) a.red[blockIdx.x] = m;
+}
+
+// ----------------------------------------------------------- launchers
+static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+static inline int gs_blocks(int n) { int b = nblk(n, 256); return b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b); }
+
+int launch_strain_constitutive(const StepArgs &a, cudaStream_t s) {
+    k_strain_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
+    int blocks = nblk(a.n, kRedThreads);
+    if (a.prm.disctype == 0) k_strain_const<0><<<blocks, kRedThreads, 0, s>>>(a);
+    else k_strain_const<1><<<blocks, kRedThreads, 0, s>>>(a);
+    return blocks;
+}
+
+int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
+    k_mom_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
+    int blocks = nblk(a.n, kRedThreads);
+    if (a.prm.disctype == 0) k_momentum<0><<<blocks, kRedThreads, 0, s>>>(a, integrate);
+    else k_momentum<1><<<blocks, kRedThreads, 0, s>>>(a, integrate);
+    return blocks;
+}
+
+int launch_update_move(const StepArgs &a, cudaStream_t s) {
+    int blocks = nblk(a.n, kRedThreads);
+    k_update_move<<<blocks, kRedThreads, 0, s>>>(a);
+    return blocks;
+}
+
+int launch_initial(const StepArgs &a, cudaStream_t s, int massopt, int init_h_opt, int init_rhoe,
+                   const int *nppermat) {
+    k_initial<<<gs_blocks(a.n), 256, 0, s>>>(a, massopt, init_h_opt, init_rhoe, nppermat);
+    return 0;
+}
+
+int launch_init_critts(const StepArgs &a, cudaStream_t s) {
+    int blocks = nblk(a.n, kRedThreads);
+    k_init_critts<<<blocks, kRedThreads, 0, s>>>(a);
+    return blocks;
+}
+
+}  // namespace MCM_FLAVOUR_NS
+}  // namespace mcm

@@ -1,0 +1,193 @@
+"""Synthetic input decks for the MCM explicit step.
+
+A :class:`Deck` holds what MCM's version-2 input file gives the solver: the
+control cards (MCM/mcm_control_v2.f90:88-124), the material cards
+(MCM/mcm_matin.f90:41-148), the node cards (MCM/mcm_nodein.f90:33-43), the
+initial velocities (MCM/mcm_Inputvel.f90), the boundary-plane cards
+(MCM/mcm_inp_symmetry_v2.f90:29-53) and the base accelerations
+(MCM/mcm_baseaccel_in.f90:27).  The reference ships no decks; the generators
+below restate the benchmark configurations as seeded lattices.
+
+Units.  The generators take SI arguments and write the deck in the DYNA3D
+cm-g-microsecond system (length cm, mass g, time us, velocity cm/us, density
+g/cm^3, pressure Mbar), the system MCM decks use.  The reference's Mie-
+Grueneisen energy correction (MCM/mcm_eqos41.f90:81) divides by the initial
+volume where the mass belongs, which multiplies the correction by the density;
+with rho = 8930 in SI units its denominator changes sign after a few steps of
+impact, with rho = 8.93 g/cm^3 the effect is mild.
+"""
+from __future__ import annotations
+
+import dataclasses
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class MaterialCard:
+    """One material as read from its cards (before mcm_sets*)."""
+
+    model: int
+    eos: int
+    rho: float
+    visc_type: int = 0
+    av_l: float = 0.0
+    av_q: float = 0.0
+    mass: float = 0.0
+    h: float = 0.0
+    rho_min: float = 0.0
+    rho_max: float = 0.0
+    strinput: np.ndarray = field(default_factory=lambda: np.zeros(48))
+    eosinput: np.ndarray = field(default_factory=lambda: np.zeros(24))
+
+
+@dataclass
+class Deck:
+    ndim: int = 3
+    disctype: int = 0
+    endtime: float = 1.0
+    tssf: float = 0.8
+    itss: float = 0.0
+    drelax_scale: float = 0.0
+    init_v_opt: int = 1
+    massopt: int = 0
+    init_h_opt: int = 0
+    init_rhoe: int = 0
+    contacttype: int = 0
+    tcrit_opt: int = 0
+    veloc_opt: int = 0
+    mirr_opt: int = 0
+    nthp: tuple = (0, 0, 0)
+    h_opt: int = 0
+    krtype: int = 1
+    maxnbr: int = 0
+    sym_flag: tuple = (0, 0, 0, 0, 0, 0)
+    sym_x: tuple = (0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    base_a: tuple = (0.0, 0.0, 0.0)
+    materials: list = field(default_factory=list)
+    x: np.ndarray = None          # (np, 3)
+    v: np.ndarray = None          # (np, 3)
+    mat: np.ndarray = None        # (np,) 1-based material ids
+    dispbc: np.ndarray = None     # (np,)
+    name: str = "deck"
+
+    @property
+    def np(self) -> int:
+        return int(self.x.shape[0])
+
+    def replace(self, **kw) -> "Deck":
+        return dataclasses.replace(self, **kw)
+
+
+def _jitter(rng: np.random.Generator, shape, amp: float) -> np.ndarray:
+    return rng.uniform(-amp, amp, size=shape)
+
+
+# SI -> cm-g-us conversion factors
+CM = 1.0e2            # m -> cm
+VEL = 1.0e-4          # m/s -> cm/us
+RHO = 1.0e-3          # kg/m^3 -> g/cm^3
+PRESS = 1.0e-11       # Pa -> Mbar
+ACC = 1.0e-10         # m/s^2 -> cm/us^2
+
+
+def copper_model10(h: float, yield_stress: float = 400e6, hardening: float = 100e6, shear: float = 46e9,
+                   gruneisen_s: float = 1.49, rho0: float = 8930.0) -> MaterialCard:
+    """Copper-like elastic-plastic hydrodynamic material (model 10) with the
+    Mie-Grueneisen EOS (41); SI arguments, cm-g-us card values; h in cm.  strinput follows MCM/mcm_f3dm10.f90:29-36
+    (G, yield, plastic modulus, cutoff, a1, a2, spall, failure strain);
+    eosinput follows MCM/mcm_eos41c.f90:240-245 (c0, s, cv, T0, gamma0, v0)."""
+    m = MaterialCard(model=10, eos=41, rho=rho0 * RHO, av_l=0.06, av_q=1.5, h=h)
+    m.strinput[0] = shear * PRESS
+    m.strinput[1] = yield_stress * PRESS
+    m.strinput[2] = hardening * PRESS
+    m.eosinput[0] = 3940.0 * VEL
+    m.eosinput[1] = gruneisen_s
+    m.eosinput[2] = 0.0      # cv * T0 = 0: zero initial internal energy
+    m.eosinput[3] = 0.0
+    m.eosinput[4] = 2.02
+    m.eosinput[5] = 1.0      # v0 = 1 (MCM/mcm_eoscalc.f90:93 divides rho0 by it)
+    return m
+
+
+def taylor_bar(dx: float = 0.4e-3, radius: float = 3.2e-3, length: float = 32.4e-3, velocity: float = 190.0,
+               seed: int = 1234, jitter: float = 0.01, disctype: int = 0, tssf: float = 0.3,
+               endtime: float = 1.0e9, material: MaterialCard | None = None, z0: float = 0.0,
+               tcrit_opt: int = 1) -> Deck:
+    """Taylor impact bar: a cylinder (axis z) of lattice particles at
+    (i+1/2, j+1/2, k+1/2) dx inside r <= R, 0 < z <= L, each displaced by a
+    seeded uniform jitter of +/- jitter*dx per coordinate, moving at -velocity
+    along z onto a rigid wall imposed by a z-min symmetry plane at z = 0.
+    Particle order: z layers, then y rows, then x.  Arguments in SI units; the
+    deck is in cm-g-us."""
+    q = radius / dx
+    n = int(np.ceil(q)) + 1
+    ii = np.arange(-n, n)
+    I, J = np.meshgrid(ii, ii, indexing="xy")
+    inside = (2 * I + 1) ** 2 + (2 * J + 1) ** 2 <= (2.0 * q) ** 2 * (1 + 1e-12)
+    dxc = dx * CM
+    xs = (I[inside] + 0.5) * dxc
+    ys = (J[inside] + 0.5) * dxc
+    order = np.lexsort((xs, ys))
+    xs, ys = xs[order], ys[order]
+    nz = int(round(length / dx))
+    zs = z0 * CM + (np.arange(nz) + 0.5) * dxc
+    x = np.empty((nz * xs.size, 3))
+    x[:, 0] = np.tile(xs, nz)
+    x[:, 1] = np.tile(ys, nz)
+    x[:, 2] = np.repeat(zs, xs.size)
+    rng = np.random.default_rng(seed)
+    x += _jitter(rng, x.shape, jitter * dxc)
+    npart = x.shape[0]
+    v = np.zeros_like(x)
+    v[:, 2] = -velocity * VEL
+    h = 1.3 * dxc
+    mat = material if material is not None else copper_model10(h)
+    mat = dataclasses.replace(mat, strinput=mat.strinput.copy(), eosinput=mat.eosinput.copy(), h=h)
+    mat.mass = mat.rho * npart * dxc ** 3
+    return Deck(ndim=3, disctype=disctype, endtime=endtime, tssf=tssf, tcrit_opt=tcrit_opt, mirr_opt=1,
+                sym_flag=(0, 0, 0, 0, 1, 0), sym_x=(0.0,) * 6, materials=[mat], x=x, v=v,
+                mat=np.ones(npart, dtype=np.int32), dispbc=np.zeros(npart, dtype=np.int32),
+                name=f"taylor_bar_dx{dx * 1e3:g}mm_n{npart}")
+
+
+def water_model9(h: float, c0: float = 40.0, rho0: float = 1000.0, pcut: float = -1.0e4) -> MaterialCard:
+    # h in cm; SI arguments otherwise
+    """Null material (model 9, mu = 0) with a linear polynomial EOS (1):
+    p = rho0 c0^2 mu (MCM/mcm_eqos1.f90:59-62); strinput(1) is the cutoff
+    pressure (MCM/mcm_initvbls.f90:58-59)."""
+    m = MaterialCard(model=9, eos=1, rho=rho0 * RHO, av_l=0.06, av_q=1.5, h=h)
+    m.strinput[0] = pcut * PRESS
+    m.strinput[1] = 0.0
+    m.eosinput[1] = (rho0 * RHO) * (c0 * VEL) ** 2
+    m.eosinput[8] = 1.0      # relative volume (MCM/mcm_eoscalc.f90:35)
+    return m
+
+
+def fluid_column(dx: float = 2.0e-3, block=(0.5, 0.25, 1.0), box=(2.0, 0.25, 1.2), seed: int = 4321,
+                 jitter: float = 0.005, gravity: float = 9.81, tssf: float = 0.3, endtime: float = 1.0e12,
+                 c0: float = 40.0) -> Deck:
+    """Weakly compressible column collapse: a block of lattice particles in
+    the corner of a box whose walls are symmetry planes (x-min, x-max, y-min,
+    y-max, z-min), under gravity along -z (base acceleration).  Arguments in
+    SI units; the deck is in cm-g-us."""
+    nx, ny, nz = (int(round(b / dx)) for b in block)
+    dxc = dx * CM
+    gx = (np.arange(nx) + 0.5) * dxc
+    gy = (np.arange(ny) + 0.5) * dxc
+    gz = (np.arange(nz) + 0.5) * dxc
+    Z, Y, X = np.meshgrid(gz, gy, gx, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    rng = np.random.default_rng(seed)
+    x += _jitter(rng, x.shape, jitter * dxc)
+    npart = x.shape[0]
+    h = 1.3 * dxc
+    mat = water_model9(h, c0=c0)
+    mat.mass = mat.rho * npart * dxc ** 3
+    bx = [b * CM for b in box]
+    return Deck(ndim=3, disctype=0, endtime=endtime, tssf=tssf, tcrit_opt=1, mirr_opt=1, nthp=(0, 0, 1),
+                base_a=(0.0, 0.0, -gravity * ACC), sym_flag=(1, 1, 1, 1, 1, 0),
+                sym_x=(0.0, bx[0], 0.0, bx[1], 0.0, bx[2]), materials=[mat], x=x,
+                v=np.zeros_like(x), mat=np.ones(npart, dtype=np.int32), dispbc=np.zeros(npart, dtype=np.int32),
+                name=f"fluid_column_dx{dx * 1e3:g}mm_n{npart}")

@@ -1,0 +1,226 @@
+"""Host loop mirroring MCM/mcm_solution.f90, driving the GPU step through the
+C ABI of libmcm_gpu.so (include/mcm_gpu.h).
+
+:class:`Solver` owns one device handle.  ``step()`` runs one iteration of the
+reference loop through the split entry points (step_a / host dt update /
+step_b / termination test / step_c), exactly where the Fortran driver would
+call them; ``run(n)`` runs n iterations with the dt update and termination
+test on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+from .deck import Deck
+
+_SYM_FIELDS = ("sigma", "s", "q", "qold", "alfa", "rod", "spin")
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def material_table(deck: Deck) -> "C.Array":
+    """Material structures after the deck defaults and mcm_sets* (done by the library)."""
+    lib = _abi.load()
+    n = len(deck.materials)
+    mats = (_abi.Material * n)()
+    for k, card in enumerate(deck.materials):
+        m = mats[k]
+        m.model, m.eos, m.visc_type = card.model, card.eos, card.visc_type
+        m.rho, m.av_l, m.av_q, m.mass, m.h = card.rho, card.av_l, card.av_q, card.mass, card.h
+        m.rho_min, m.rho_max = card.rho_min, card.rho_max
+        for i in range(48):
+            m.strinput[i] = float(card.strinput[i])
+        for i in range(24):
+            m.eosinput[i] = float(card.eosinput[i])
+        check(lib.mcm_gpu_material_from_deck(C.byref(m)), "mcm_gpu_material_from_deck")
+    return mats
+
+
+def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0) -> _abi.Config:
+    """Control-card processing of MCM/mcm_control_v2.f90:193-243 and the
+    boundary/base-acceleration cards (mcm_inp_symmetry_v2.f90:83-137,
+    mcm_baseaccel_in.f90:23-33)."""
+    c = _abi.Config()
+    c.ndim = deck.ndim
+    c.disctype = deck.disctype
+    c.tcrit_opt = deck.tcrit_opt
+    c.contacttype = deck.contacttype
+    c.h_opt = deck.h_opt
+    c.veloc_opt = deck.veloc_opt
+    c.krtype = deck.krtype if deck.krtype else 1
+    c.drelax = int(0.1 < deck.drelax_scale < 1.0)
+    c.drelax_scale = deck.drelax_scale
+    boundary = deck.mirr_opt == 1 and any(f in (1, 2) for f in deck.sym_flag)
+    c.boundary = int(boundary)
+    for k in range(6):
+        c.boundary_code[k] = int(deck.sym_flag[k]) if boundary else 0
+        c.boundary_x[k] = float(deck.sym_x[k])
+    c.baseaccel = int(any(t == 1 for t in deck.nthp))
+    for k in range(3):
+        c.base_a[k] = float(deck.base_a[k]) if deck.nthp[k] == 1 else 0.0
+    c.tssf = deck.tssf if deck.tssf != 0.0 else 0.8
+    c.hmax = 0.0
+    c.precision = precision
+    c.nbr_stride = nbr_stride
+    return c
+
+
+class Solver:
+    def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0):
+        self.lib = _abi.load()
+        self.deck = deck
+        self.n = deck.np
+        self.nmat = len(deck.materials)
+        self._mats = material_table(deck)
+        self.cfg = config_from_deck(deck, precision, nbr_stride)
+        h = C.c_void_p()
+        check(self.lib.mcm_gpu_create(C.byref(self.cfg), self._mats, self.nmat, self.n, C.byref(h)),
+              "mcm_gpu_create")
+        self.h = h
+        x = np.ascontiguousarray(deck.x, dtype=np.float64)
+        v = np.ascontiguousarray(deck.v if deck.init_v_opt == 1 else np.zeros_like(deck.x), dtype=np.float64)
+        mat = np.ascontiguousarray(deck.mat, dtype=np.int32)
+        disp = np.ascontiguousarray(deck.dispbc if deck.dispbc is not None else np.zeros(self.n), dtype=np.int32)
+        f = _abi.Fields()
+        f.x, f.v, f.mat, f.dispbc = _dptr(x), _dptr(v), _iptr(mat), _iptr(disp)
+        t = _abi.Time(0.0, 0.0, 0.0, deck.endtime)
+        check(self.lib.mcm_gpu_initialise(h, C.byref(f), deck.massopt, deck.init_h_opt, deck.init_rhoe,
+                                          deck.itss, C.byref(t)), "mcm_gpu_initialise", h)
+        self.dt, self.dtold, self.ptime = t.dt, t.dtold, t.ptime
+        self.tssf = self.cfg.tssf
+        self.timestep = 1
+        self.ended = False
+        self.energies = np.zeros(5 * self.nmat + 3)
+        self.bbox = np.zeros(6)
+        self.last_critts = None
+
+    # ------------------------------------------------------------- loop
+    def step_a(self) -> float:
+        crit = C.c_double()
+        check(self.lib.mcm_gpu_step_a(self.h, self.dt, C.byref(crit)), "mcm_gpu_step_a", self.h)
+        self.last_critts = crit.value
+        return crit.value
+
+    def dt_update(self) -> None:
+        # MCM/mcm_solution.f90:58-62
+        self.dtold = self.dt
+        self.dt = self.tssf * self.last_critts
+        self.dt = min(self.dt, 1.1 * self.dtold)
+        self.ptime = self.ptime + self.dt
+
+    def step_b(self) -> np.ndarray:
+        check(self.lib.mcm_gpu_step_b(self.h, _dptr(self.energies)), "mcm_gpu_step_b", self.h)
+        return self.energies
+
+    def step_c(self) -> None:
+        check(self.lib.mcm_gpu_step_c(self.h, self.dt, self.dtold, _dptr(self.bbox)), "mcm_gpu_step_c", self.h)
+        self.timestep += 1
+
+    def step(self) -> bool:
+        """One iteration of MCM/mcm_solution.f90:37-138; False once it terminates."""
+        if self.ended:
+            return False
+        self.step_a()
+        self.dt_update()
+        self.step_b()
+        if self.ptime - self.dt >= self.deck.endtime:   # :101
+            self.ended = True
+            return False
+        self.step_c()
+        return True
+
+    def run(self, nsteps: int) -> int:
+        """nsteps iterations with the time scalars kept on the device."""
+        t = _abi.Time(self.dt, self.dtold, self.ptime, self.deck.endtime)
+        done = C.c_int()
+        check(self.lib.mcm_gpu_run(self.h, nsteps, C.byref(t), C.byref(done)), "mcm_gpu_run", self.h)
+        self.dt, self.dtold, self.ptime = t.dt, t.dtold, t.ptime
+        self.timestep += done.value
+        if done.value < nsteps or self.ptime - self.dt >= self.deck.endtime:
+            self.ended = self.ptime - self.dt >= self.deck.endtime
+        return done.value
+
+    # ------------------------------------------------------- inspection
+    def download(self, names=None) -> dict:
+        if names is None:
+            names = _abi.DOUBLE_FIELDS + _abi.INT_FIELDS
+        f = _abi.Fields()
+        out = {}
+        for nm in names:
+            if nm in _abi.INT_FIELDS:
+                arr = np.zeros(self.n, dtype=np.int32)
+                setattr(f, nm, _iptr(arr))
+            else:
+                w = _abi.FIELD_WIDTH.get(nm, 1)
+                arr = np.zeros(self.n * w, dtype=np.float64)
+                setattr(f, nm, _dptr(arr))
+            out[nm] = arr
+        check(self.lib.mcm_gpu_download(self.h, C.byref(f)), "mcm_gpu_download", self.h)
+        for nm, arr in out.items():
+            w = _abi.FIELD_WIDTH.get(nm, 1)
+            if w == 3:
+                out[nm] = arr.reshape(self.n, 3)
+            elif w == 9:
+                # Fortran (3,3): element (r,c) at r + 3c -> [i, r, c]
+                out[nm] = arr.reshape(self.n, 3, 3).transpose(0, 2, 1)
+        return out
+
+    def neighbours(self):
+        """(nnbr, nbr[np, stride], g_nnbr, g_nbr[np, g_stride]) with 1-based ids."""
+        nn = np.zeros(self.n, dtype=np.int32)
+        gn = np.zeros(self.n, dtype=np.int32)
+        s, gs = C.c_int(0), C.c_int(0)
+        check(self.lib.mcm_gpu_neighbours(self.h, _iptr(nn), None, C.byref(s), _iptr(gn), None, C.byref(gs)),
+              "mcm_gpu_neighbours", self.h)
+        stride, gstride = max(1, s.value), max(1, gs.value)
+        nbr = np.zeros((self.n, stride), dtype=np.int32)
+        gnbr = np.zeros((self.n, gstride), dtype=np.int32)
+        s, gs = C.c_int(stride), C.c_int(gstride)
+        check(self.lib.mcm_gpu_neighbours(self.h, _iptr(nn), _iptr(nbr), C.byref(s), _iptr(gn), _iptr(gnbr),
+                                          C.byref(gs)), "mcm_gpu_neighbours", self.h)
+        return nn, nbr, gn, gnbr
+
+    def ghosts(self):
+        n = C.c_int()
+        check(self.lib.mcm_gpu_ghosts(self.h, C.byref(n), None, None, None, 0), "mcm_gpu_ghosts", self.h)
+        m = n.value
+        par = np.zeros(max(m, 1), dtype=np.int32)
+        x = np.zeros(max(m, 1) * 3)
+        v = np.zeros(max(m, 1) * 3)
+        check(self.lib.mcm_gpu_ghosts(self.h, C.byref(n), _iptr(par), _dptr(x), _dptr(v), m), "mcm_gpu_ghosts", self.h)
+        return par[:m], x[: 3 * m].reshape(m, 3), v[: 3 * m].reshape(m, 3)
+
+    def grid(self):
+        gl = np.zeros(3, dtype=np.int32)
+        gm = np.zeros(3)
+        gs = np.zeros(3)
+        check(self.lib.mcm_gpu_grid(self.h, _iptr(gl), _dptr(gm), _dptr(gs)), "mcm_gpu_grid", self.h)
+        return gl, gm, gs
+
+    def stats(self):
+        mean = C.c_double()
+        mx, st, ngp = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.mcm_gpu_stats(self.h, C.byref(mean), C.byref(mx), C.byref(st), C.byref(ngp)), "mcm_gpu_stats",
+              self.h)
+        return {"mean_nbr": mean.value, "max_nbr": mx.value, "stride": st.value, "ngp": ngp.value}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mcm_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,212 @@
+"""Parity of the CUDA step (through the C ABI) with the CPU oracle.
+
+The FP64-exact flavour evaluates the reference's expressions in the
+reference's order without fused multiply-add, and the neighbour search returns
+the reference's neighbour sequences, so the fields agree to the last few bits
+(transcendental functions such as tan and pow may differ by an ulp between the
+CUDA and host math libraries).  Neighbour lists and ghosts are compared
+exactly.  Tolerances are relative to the field's largest magnitude.
+"""
+import numpy as np
+import pytest
+
+from mcmtop_b200 import _abi
+from mcmtop_b200.deck import fluid_column, taylor_bar
+from mcmtop_b200.solver import Solver
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["x", "v", "mass", "h", "rho", "e", "p", "c", "efps", "pcut", "fail", "vabs", "sigma", "q"]
+DIAG = ["rod", "spin", "tracerod", "rhoold", "etry", "s"]
+
+
+def relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.max(np.abs(b)) if b.size else 0.0
+    if scale == 0.0:
+        return float(np.max(np.abs(a))) if a.size else 0.0
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def compare(sol, orc, fields, tol, label=""):
+    g = sol.download(fields)
+    worst = {}
+    for f in fields:
+        e = relerr(g[f], orc.get(f))
+        worst[f] = e
+    bad = {f: e for f, e in worst.items() if e > tol}
+    assert not bad, f"{label} fields beyond {tol}: {bad}"
+    return worst
+
+
+def compare_neighbours(sol, orc):
+    nn, nbr, gn, gnbr = sol.neighbours()
+    onn = orc.get_int("nnbr")
+    ogn = orc.get_int("g_nnbr")
+    assert np.array_equal(nn, onn), "neighbour counts differ"
+    assert np.array_equal(gn, ogn), "ghost neighbour counts differ"
+    for i in range(sol.n):
+        ref = orc.nbrlist(i + 1)
+        assert np.array_equal(nbr[i, : nn[i]], ref), f"neighbour sequence of particle {i + 1} differs"
+        if gn[i]:
+            gref = orc.g_nbrlist(i + 1)
+            assert np.array_equal(gnbr[i, : gn[i]], gref), f"ghost sequence of particle {i + 1} differs"
+
+
+def small_bar(**kw):
+    return taylor_bar(dx=0.8e-3, **kw)
+
+
+@pytest.fixture(scope="module")
+def lib(gpu_lib):
+    return gpu_lib
+
+
+def test_initial_state(lib):
+    deck = small_bar()
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    compare(sol, orc, STATE, 0.0, "initial")
+    assert sol.dt == orc.scalar("dt")
+    compare_neighbours(sol, orc)
+
+
+def test_grid_and_ghosts(lib):
+    deck = small_bar()
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    gl, gm, gs = sol.grid()
+    ogl, ogm, ogs = orc.grid()
+    assert np.array_equal(gl, ogl) and np.array_equal(gm, ogm) and np.array_equal(gs, ogs)
+    par, x, v = sol.ghosts()
+    opar, ox, ov = orc.ghosts()
+    assert len(par) == len(opar) > 0
+    assert np.array_equal(par, opar)
+    assert np.array_equal(x, ox) and np.array_equal(v, ov)
+
+
+@pytest.mark.parametrize("disctype", [0, 1])
+def test_one_step(lib, disctype):
+    deck = small_bar(disctype=disctype)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    c_gpu = sol.step_a()
+    c_orc = orc.step_a()
+    assert abs(c_gpu - c_orc) <= 1e-15 * abs(c_orc)
+    compare_neighbours(sol, orc)
+    compare(sol, orc, STATE + DIAG, 1e-13, "after step_a")
+    sol.dt_update()
+    orc.dt_update()
+    sol.step_b()
+    orc.step_b()
+    assert relerr(sol.energies, orc.energies()) < 1e-13
+    compare(sol, orc, ["a"], 1e-12, "acceleration")
+    sol.step_c()
+    orc.step_c()
+    compare(sol, orc, STATE, 1e-13, "after step_c")
+
+
+@pytest.mark.parametrize("disctype", [0, 1])
+def test_twenty_steps(lib, disctype):
+    deck = small_bar(disctype=disctype)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    for _ in range(20):
+        sol.step()
+        orc.step()
+    assert abs(sol.ptime - orc.scalar("ptime")) <= 1e-12 * orc.scalar("ptime")
+    compare(sol, orc, STATE, 1e-10, "20 steps")
+    compare_neighbours(sol, orc)
+
+
+def test_fused_run_equals_split(lib):
+    deck = small_bar()
+    a = Solver(deck, _abi.PREC_FP64_EXACT)
+    b = Solver(deck, _abi.PREC_FP64_EXACT)
+    for _ in range(15):
+        a.step()
+    done = b.run(15)
+    assert done == 15
+    assert a.dt == b.dt and a.ptime == b.ptime
+    ga = a.download(STATE)
+    gb = b.download(STATE)
+    for f in STATE:
+        assert np.array_equal(ga[f], gb[f]), f
+
+
+def test_termination(lib):
+    deck = small_bar()
+    orc = Oracle(deck)
+    dt0 = orc.scalar("dt")
+    deck = deck.replace(endtime=5.5 * dt0)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    n_orc = orc.run(100)
+    n_gpu = sol.run(100)
+    assert n_gpu == n_orc
+    compare(sol, orc, STATE, 1e-12, "terminated run")
+
+
+@pytest.mark.parametrize("tcrit", [0, 2])
+def test_timestep_options(lib, tcrit):
+    deck = small_bar(tcrit_opt=tcrit)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    assert abs(sol.dt - orc.scalar("dt")) <= 1e-15 * orc.scalar("dt")
+    for _ in range(3):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-12, f"tcrit {tcrit}")
+
+
+def test_fp64_fast(lib):
+    deck = small_bar()
+    sol = Solver(deck, _abi.PREC_FP64)
+    orc = Oracle(deck)
+    for _ in range(20):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-9, "fp64 fast")
+    compare_neighbours(sol, orc)
+
+
+def test_fluid_column_five_planes(lib):
+    deck = fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    par, x, v = sol.ghosts()
+    opar, ox, ov = orc.ghosts()
+    assert np.array_equal(par, opar) and np.array_equal(x, ox)
+    compare_neighbours(sol, orc)
+    for _ in range(10):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-10, "fluid")
+    compare_neighbours(sol, orc)
+
+
+def test_taylor_bar_16k_steps(lib):
+    """The 16 848-particle Taylor bar (dx = 0.4 mm), first 30 steps."""
+    deck = taylor_bar(dx=0.4e-3)
+    assert deck.np == 16848
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck)
+    for _ in range(30):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-10, "16k bar")
+    compare_neighbours(sol, orc)
+
+
+def test_neighbour_overflow_regrow(lib):
+    """A too narrow initial table is regrown and the step re-run."""
+    deck = small_bar()
+    sol = Solver(deck, _abi.PREC_FP64_EXACT, nbr_stride=8)
+    orc = Oracle(deck)
+    compare_neighbours(sol, orc)
+    sol.step()
+    orc.step()
+    compare(sol, orc, STATE, 1e-12, "after regrow")
+    assert sol.stats()["stride"] >= orc.get_int("nnbr").max()
