@@ -1,0 +1,333 @@
+"""Benchmark of the MCM explicit SPH step on B200.
+
+Workload: the 2 034 720-particle Taylor bar (dx = 0.08 mm, copper, model 10 +
+EOS 41, z-min symmetry wall), the configuration the headline metric is quoted
+on.  One "step" is one iteration of MCM's time loop (neighbour search, strain,
+constitutive update, dt, momentum, boundary conditions, energies, velocity and
+position update) over every particle.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|exact|mixed]
+  python bench.py --impl reference ...   # the CPU restatement on the host cores
+
+value: particle-steps/s of the fused device loop (mcm_gpu_run), device time
+from CUDA events on the library's stream, max over ranks.  e2e: the same
+metric through the split C-ABI entry points a Fortran driver calls
+(mcm_gpu_upload, step_a/b/c per step with host dt logic, mcm_gpu_download),
+host buffers, wall clock.  Each rank owns one independent bar (weak scaling,
+no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (2M Taylor bar), mixed vs FP64 GPU at ≤1e-4 rel err; adj/fwd"
+UNIT = "particle-steps/s"
+DX = 0.08e-3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"])
+    ap.add_argument("--dx", type=float, default=DX)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed oracle work")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- roofline
+def algorithmic_bytes(region: str, kbar: float, precision: str) -> float:
+    """Compulsory bytes per particle of one kernel group (ideal caching of the
+    neighbour gathers): own-state reads and writes plus the neighbour table at
+    4 B per entry.  Field lists per kernel:
+      search:   read x(3) h mat; write count + table            -> 36+4+4K
+      strain:   read x v m h rho e p c efps pcut sigma(6) fail, count, table;
+                write x rho e p c efps h sigma(6) q             -> 168+4+4K+120
+      momentum: read x v m rho h sigma(6) q e vabs, dispbc, count, table;
+                write x v vabs                                 -> 144+8+4K+56
+    The mixed path keeps x and v in FP64 and the rest in FP32."""
+    if precision == "mixed":
+        w = 4
+    else:
+        w = 8
+    if region == "search":
+        return 3 * 8 + w + 4 + 4 + 4 * kbar
+    if region == "strain_constitutive":
+        return 6 * 8 + 15 * w + 4 + 4 * kbar + 3 * 8 + 12 * w
+    if region == "momentum_integrate":
+        return 6 * 8 + 12 * w + 8 + 4 * kbar + 6 * 8 + w
+    return 0.0
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(workload: str, precision: str, region: str):
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    return d.get(workload, {}).get(precision, {}).get(region)
+
+
+# -------------------------------------------------------------- CPU baseline
+def cpu_oracle(deck, budget_s: float, max_steps: int):
+    """Times the OpenMP build of the CPU restatement (oracle/) on the deck:
+    initialisation untimed, then whole steps until max_steps or the budget."""
+    from oracle.pyoracle import Oracle
+
+    orc = Oracle(deck, openmp=True)
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < max_steps:
+        orc.run(1)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    orc.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return deck.np * steps / el, steps, el, cores
+
+
+# ----------------------------------------------------------------- GPU arm
+def gpu_arm(args):
+    import torch
+
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.deck import taylor_bar
+    from mcmtop_b200.solver import Solver
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
+    deck = taylor_bar(dx=args.dx)
+    workload = f"taylor_bar_{deck.np}"
+    sol = Solver(deck, prec, device=local)
+    sol.set_diagnostics(False)
+    sol.run(args.warmup)
+    stats = sol.stats()
+    kbar = stats["mean_nbr"]
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    gpu_index = int(vis.split(",")[local]) if vis else local
+    clocks = ClockSampler(gpu_index)
+    barrier()
+    sol.profile(True)
+    clocks.start()
+    sol.timer_start()
+    done = sol.run(args.steps)
+    ms = sol.timer_stop()
+    clk = clocks.stop()
+    launches = sol.kernel_launches()
+    report = sol.profile_report()
+    sol.profile(False)
+    if done != args.steps:
+        raise RuntimeError(f"run stopped after {done} of {args.steps} steps")
+    ms_max = ms
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ws * deck.np * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel group
+    peak, peak_kind = load_peaks()
+    main = {k: v for k, v in report.items() if k in ("search", "strain_constitutive", "momentum_integrate")}
+    dom = max(main, key=lambda k: main[k][0])
+    dom_ms, dom_n = main[dom]
+    per_launch_s = dom_ms / 1e3 / max(dom_n, 1)
+    bpp = algorithmic_bytes(dom, kbar, args.precision)
+    achieved = bpp * deck.np / per_launch_s / 1e9
+    traffic = load_traffic(workload, args.precision, dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "bytes_per_particle": round(bpp, 1), "mean_neighbours": round(kbar, 2),
+                "launch_ms": round(per_launch_s * 1e3, 4)}
+    kernels = {k: {"ms_per_step": round(v[0] / args.steps, 4), "launches": v[1]} for k, v in report.items() if v[1]}
+
+    # end to end through the split C ABI with host buffers (rank 0 only)
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        names = ["x", "v", "mass", "h", "hold", "rho", "e", "p", "c", "vabs", "efps", "pcut", "fail", "sigma", "q",
+                 "mat", "dispbc"]
+        host = sol.download(names)
+        pinned = {}
+        for k, a in host.items():
+            t = torch.empty(a.shape, dtype=torch.from_numpy(np.ascontiguousarray(a[:1])).dtype, pin_memory=True)
+            arr = t.numpy()
+            arr[...] = a
+            pinned[k] = arr
+        bbox = np.array([host["x"][:, d].min() if j == 0 else host["x"][:, d].max() for d in range(3) for j in range(2)])
+        h2d_bytes = sum(a.nbytes for a in pinned.values())
+        k_e2e = args.steps
+        t0 = time.perf_counter()
+        sol.upload(pinned, bbox)
+        for _ in range(k_e2e):
+            sol.step()
+        out = sol.download(["x", "v", "rho", "e", "p", "sigma", "efps"])
+        el = time.perf_counter() - t0
+        d2h_bytes = sum(a.nbytes for a in out.values())
+        per_step_h2d = 24
+        per_step_d2h = 3 * 96 + 8 * (5 * sol.nmat + 3) + 48
+        e2e = {"value": round(deck.np * k_e2e / el, 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d_bytes / k_e2e + per_step_h2d),
+               "d2h_bytes_per_step": int(d2h_bytes / k_e2e + per_step_d2h),
+               "steps": k_e2e, "path": "mcm_gpu_upload + (step_a, host dt, step_b, step_c) x K + mcm_gpu_download"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, n, el, cores = cpu_oracle(deck, args.cpu_budget, 3)
+        cpu = {"value": round(v, 1), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"oracle (C++ restatement, OpenMP) on the same {deck.np}-particle bar: {n} steps after "
+                         f"initialisation, {el:.1f} s"}
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "exact": "f64", "mixed": "f32+f64"}[args.precision],
+        "data": "synthetic: seeded jittered cubic lattice (Taylor bar, cm-g-us deck), no dataset",
+        "config": {"workload": workload, "particles": deck.np, "dx_mm": args.dx * 1e3, "precision": args.precision,
+                   "material": "copper model 10 + Mie-Grueneisen EOS 41, h = 1.3 dx, CFL 0.3 (tcrit_opt 1)",
+                   "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        "kernels": kernels,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from mcmtop_b200.deck import taylor_bar
+
+    deck = taylor_bar(dx=args.dx)
+    # a bounded sample: the first steps of the same bar, until K steps or ~2 minutes
+    v, n, el, cores = cpu_oracle(deck, 120.0, max(1, args.steps))
+    line = {
+        "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": ws, "steps": n, "warmup": 0,
+        "ms_per_step": round(el * 1e3 / n, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "impl": "reference",
+        "data": "synthetic: seeded jittered cubic lattice (Taylor bar, cm-g-us deck), no dataset",
+        "config": {"workload": f"taylor_bar_{deck.np}", "particles": deck.np, "dx_mm": args.dx * 1e3,
+                   "precision": "fp64", "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"oracle (C++ restatement of the Fortran, the reference cannot be compiled: no "
+                                   f"Fortran compiler) on the {deck.np}-particle bar, {n} steps, {el:.1f} s"},
+        "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

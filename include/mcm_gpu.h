@@ -131,6 +131,10 @@ typedef struct {
 
 /* ---------------------------------------------------------------- set-up */
 
+/* Selects the CUDA device that handles created by this host thread use
+ * (the library links its own CUDA runtime). */
+int mcm_gpu_set_device(int device);
+
 /* Applies the deck defaults and rearrangements of MCM/mcm_matin.f90:46-56,
  * MCM/mcm_sets1.f90, mcm_sets3.f90, mcm_sets10.f90 and mcm_calcg.f90 to a
  * material given as read from its cards.  Replaces those routines for callers
@@ -188,6 +192,27 @@ int mcm_gpu_energies(mcm_gpu_handle *h, double *energies);
 
 /* Mean neighbour count of the last search (for the roofline accounting). */
 int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp);
+
+/* ----------------------------------------------------------- measurement */
+
+/* Diagnostic fields (rod, spin, tracerod, etry, einc, rhoold, critts, s, a)
+ * are refreshed every step when enabled (the default).  The physics state is
+ * computed identically either way; disabling only skips writing outputs that
+ * no later part of the step reads. */
+int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable);
+/* Brackets every kernel group enqueued on the handle's stream with CUDA events
+ * (enable = 1) and resets the launch counter.  The reference has no profiler;
+ * its only timing is the commented-out MCM/mcm_write_timings.f90. */
+int mcm_gpu_profile(mcm_gpu_handle *h, int enable);
+/* Device time and launches of kernel group `region` (0..10) since
+ * mcm_gpu_profile; returns MCM_EINVAL past the last group. */
+int mcm_gpu_profile_report(mcm_gpu_handle *h, int region, char *name, int name_len, double *total_ms,
+                           int *launches);
+/* Kernels launched by this handle since the last mcm_gpu_profile call. */
+long long mcm_gpu_kernel_launches(mcm_gpu_handle *h);
+/* op 0: record a start event on the handle's stream; op 1: record a stop
+ * event, wait for it and return the elapsed device time in *ms. */
+int mcm_gpu_timer(mcm_gpu_handle *h, int op, double *ms);
 
 const char *mcm_gpu_strerror(int status);
 /* Text of the last CUDA error or failed check on this handle. */

@@ -93,6 +93,7 @@ def load() -> C.CDLL:
     H = C.c_void_p
     sig = {
         "mcm_gpu_abi_version": ([], C.c_int),
+        "mcm_gpu_set_device": ([C.c_int], C.c_int),
         "mcm_gpu_strerror": ([C.c_int], C.c_char_p),
         "mcm_gpu_last_error": ([H], C.c_char_p),
         "mcm_gpu_material_from_deck": ([C.POINTER(Material)], C.c_int),
@@ -110,6 +111,11 @@ def load() -> C.CDLL:
         "mcm_gpu_grid": ([H, _IP, _DP, _DP], C.c_int),
         "mcm_gpu_energies": ([H, _DP], C.c_int),
         "mcm_gpu_stats": ([H, _DP, _IP, _IP, _IP], C.c_int),
+        "mcm_gpu_set_diagnostics": ([H, C.c_int], C.c_int),
+        "mcm_gpu_profile": ([H, C.c_int], C.c_int),
+        "mcm_gpu_profile_report": ([H, C.c_int, C.c_char_p, C.c_int, _DP, _IP], C.c_int),
+        "mcm_gpu_kernel_launches": ([H], C.c_longlong),
+        "mcm_gpu_timer": ([H, C.c_int, _DP], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -43,6 +43,12 @@ struct mcm_gpu_handle {
     bool initialised = false;
     int red_cap = 0;
     double mean_nbr = 0.0;
+    // profiling: CUDA events around each kernel group on the handle's stream
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs[16];
+    long long kernel_launches = 0;
+    cudaEvent_t timer[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -69,6 +75,47 @@ int dalloc(mcm_gpu_handle *h, T **p, size_t count) {
 }
 
 inline int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
+
+// Kernel groups that the profiler times separately.
+enum Region {
+    R_CELLS = 0, R_GHOSTS, R_SEARCH, R_STRAIN_PREP, R_STRAIN, R_CRITTS, R_MOM_PREP, R_MOMENTUM, R_REDUCE,
+    R_MOVE, R_MISC, R_NREG
+};
+const char *kRegionName[R_NREG] = {"cell_list", "ghosts", "search", "strain_prep", "strain_constitutive",
+                                   "critts_dt", "momentum_prep", "momentum_integrate", "energy_bbox_reduce",
+                                   "update_move", "misc"};
+
+cudaEvent_t take_event(mcm_gpu_handle *h) {
+    if (h->ev_pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+}
+
+// Counts the kernels of a group and, when profiling, brackets them with events.
+struct Scope {
+    mcm_gpu_handle *h;
+    int r;
+    cudaEvent_t b = nullptr;
+    Scope(mcm_gpu_handle *h_, int r_, int nkernels) : h(h_), r(r_) {
+        h->kernel_launches += nkernels;
+        if (h->prof_on) {
+            b = take_event(h);
+            cudaEventRecord(b, h->stream);
+        }
+    }
+    ~Scope() {
+        if (b) {
+            cudaEvent_t e = take_event(h);
+            cudaEventRecord(e, h->stream);
+            h->prof_pairs[r].push_back({b, e});
+        }
+    }
+};
 
 DevParams make_params(const mcm_gpu_config &c, int nmat) {
     DevParams p;
@@ -226,38 +273,71 @@ int regrow(mcm_gpu_handle *h, int *grew) {
 
 // ---------------------------------------------------------------- dispatch
 int launch_strain(mcm_gpu_handle *h) {
+    {
+        Scope sc(h, R_STRAIN_PREP, 1);
+        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_strain_prep(h->A, h->stream);
+        else fast::launch_strain_prep(h->A, h->stream);
+    }
+    Scope sc(h, R_STRAIN, 1);
     switch (h->cfg.precision) {
         case MCM_PREC_FP64_EXACT: return exact::launch_strain_constitutive(h->A, h->stream);
         default: return fast::launch_strain_constitutive(h->A, h->stream);
     }
 }
 int launch_mom(mcm_gpu_handle *h, int integrate) {
+    {
+        Scope sc(h, R_MOM_PREP, 1);
+        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_mom_prep(h->A, h->stream);
+        else fast::launch_mom_prep(h->A, h->stream);
+    }
+    Scope sc(h, R_MOMENTUM, 1);
     switch (h->cfg.precision) {
         case MCM_PREC_FP64_EXACT: return exact::launch_momentum(h->A, h->stream, integrate);
         default: return fast::launch_momentum(h->A, h->stream, integrate);
     }
 }
 int launch_move(mcm_gpu_handle *h) {
+    Scope sc(h, R_MOVE, 1);
     switch (h->cfg.precision) {
         case MCM_PREC_FP64_EXACT: return exact::launch_update_move(h->A, h->stream);
         default: return fast::launch_update_move(h->A, h->stream);
     }
 }
 
+int active_planes(const mcm_gpu_handle *h) {
+    int n = 0;
+    for (int p = 0; p < 6; ++p) {
+        int c = h->A.prm.planes.code[p & 1][p >> 1];
+        if ((c == 1 || c == 2) && (p >> 1) < h->A.prm.ndim) ++n;
+    }
+    return n;
+}
+
 // neighbours -> strain -> constitutive -> critts (MCM/mcm_solution.f90:41-53)
 void enqueue_part_a(mcm_gpu_handle *h) {
     StepArgs &a = h->A;
-    launch_grid_setup(a, h->stream);
-    launch_cell_build(a, h->stream);
-    if (a.prm.boundary) launch_ghosts(a, h->stream);
-    launch_search(a, h->stream);
+    {
+        Scope sc(h, R_CELLS, 7);
+        launch_grid_setup(a, h->stream);
+        launch_cell_build(a, h->stream);
+    }
+    if (a.prm.boundary) {
+        Scope sc(h, R_GHOSTS, 3 * active_planes(h));
+        launch_ghosts(a, h->stream);
+    }
+    {
+        Scope sc(h, R_SEARCH, 1);
+        launch_search(a, h->stream);
+    }
     int nb = launch_strain(h);
+    Scope sc(h, R_CRITTS, 1);
     launch_critts_reduce(a, h->stream, nb);
 }
 
 // momentum -> boundcond -> calctotale (-> update_velocity -> move)
 void enqueue_part_b(mcm_gpu_handle *h, int integrate) {
     int nb = launch_mom(h, integrate);
+    Scope sc(h, R_REDUCE, 2);
     launch_energy_bbox_reduce(h->A, h->stream, nb, 1, integrate);
 }
 
@@ -302,6 +382,13 @@ int put_scalar(mcm_gpu_handle *h, const double *src, int f) {
 extern "C" {
 
 int mcm_gpu_abi_version(void) { return MCM_GPU_ABI_VERSION; }
+
+int mcm_gpu_set_device(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return MCM_ECUDA;
+    if (device < 0 || device >= n) return MCM_EINVAL;
+    return cudaSetDevice(device) == cudaSuccess ? MCM_OK : MCM_ECUDA;
+}
 
 const char *mcm_gpu_strerror(int status) {
     switch (status) {
@@ -492,6 +579,11 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_time) cudaFreeHost(h->h_time);
+    for (auto &v : h->prof_pairs)
+        for (auto &pr : v) { h->ev_pool.push_back(pr.first); h->ev_pool.push_back(pr.second); }
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->timer)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MCM_OK;
@@ -743,7 +835,10 @@ int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts) {
     int st;
     if ((st = check_handle(h))) return st;
     h->A.split_mode = 1;
-    launch_set_time(h->A, h->stream, dt, 0.0, 0);
+    {
+        Scope sc(h, R_MISC, 1);
+        launch_set_time(h->A, h->stream, dt, 0.0, 0);
+    }
     if ((st = run_part_a(h))) return st;
     if (critts) *critts = h->h_time->critts;
     return MCM_OK;
@@ -770,9 +865,15 @@ int mcm_gpu_step_c(mcm_gpu_handle *h, double dt, double dtold, double *coord_max
     if ((st = check_handle(h))) return st;
     h->A.split_mode = 1;
     if ((st = reset_status(h))) return st;
-    launch_set_time(h->A, h->stream, dt, dtold, 1);
+    {
+        Scope sc(h, R_MISC, 1);
+        launch_set_time(h->A, h->stream, dt, dtold, 1);
+    }
     int nb = launch_move(h);
-    launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
+    {
+        Scope sc(h, R_REDUCE, 1);
+        launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
+    }
     CK(cudaMemcpyAsync(h->h_bbox, h->A.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream));
     if ((st = sync_status(h))) return st;
     if (h->h_status->code) return set_error(h, h->h_status->code, "step_c");
@@ -800,6 +901,7 @@ int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done) {
         for (int k = 0; k < batch; ++k) {
             enqueue_part_a(h);
             enqueue_part_b(h, 1);
+            Scope sc(h, R_MISC, 1);
             launch_finish_step(h->A, h->stream);
         }
         if ((st = sync_status(h))) return st;
@@ -1025,6 +1127,61 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
     }
     if (stride) *stride = h->A.stride;
     if (ngp) CK(cudaMemcpy(ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
+    return MCM_OK;
+}
+
+int mcm_gpu_profile(mcm_gpu_handle *h, int enable) {
+    if (!h) return MCM_EINVAL;
+    CK(cudaStreamSynchronize(h->stream));
+    for (auto &v : h->prof_pairs) {
+        for (auto &pr : v) { h->ev_pool.push_back(pr.first); h->ev_pool.push_back(pr.second); }
+        v.clear();
+    }
+    h->prof_on = enable != 0;
+    h->kernel_launches = 0;
+    return MCM_OK;
+}
+
+int mcm_gpu_profile_report(mcm_gpu_handle *h, int region, char *name, int name_len, double *total_ms, int *launches) {
+    if (!h) return MCM_EINVAL;
+    if (region < 0 || region >= R_NREG) return MCM_EINVAL;
+    CK(cudaStreamSynchronize(h->stream));
+    double ms = 0.0;
+    for (auto &pr : h->prof_pairs[region]) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, pr.first, pr.second));
+        ms += t;
+    }
+    if (name && name_len > 0) {
+        std::strncpy(name, kRegionName[region], (size_t)name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (total_ms) *total_ms = ms;
+    if (launches) *launches = (int)h->prof_pairs[region].size();
+    return MCM_OK;
+}
+
+long long mcm_gpu_kernel_launches(mcm_gpu_handle *h) { return h ? h->kernel_launches : -1; }
+
+int mcm_gpu_timer(mcm_gpu_handle *h, int op, double *ms) {
+    if (!h) return MCM_EINVAL;
+    for (int k = 0; k < 2; ++k)
+        if (!h->timer[k]) CK(cudaEventCreate(&h->timer[k]));
+    if (op == 0) {
+        CK(cudaEventRecord(h->timer[0], h->stream));
+        return MCM_OK;
+    }
+    CK(cudaEventRecord(h->timer[1], h->stream));
+    CK(cudaEventSynchronize(h->timer[1]));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, h->timer[0], h->timer[1]));
+    if (ms) *ms = t;
+    return MCM_OK;
+}
+
+int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable) {
+    if (!h) return MCM_EINVAL;
+    h->A.prm.diag = enable ? 1 : 0;
     return MCM_OK;
 }
 

@@ -66,7 +66,9 @@ void launch_finish_step(const StepArgs &a, cudaStream_t s);
 // step kernels (one namespace per arithmetic flavour)
 #define MCM_DECLARE_STEP(NS)                                                        \
     namespace NS {                                                                  \
+    void launch_strain_prep(const StepArgs &a, cudaStream_t s);                     \
     int launch_strain_constitutive(const StepArgs &a, cudaStream_t s);              \
+    void launch_mom_prep(const StepArgs &a, cudaStream_t s);                        \
     int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);          \
     int launch_update_move(const StepArgs &a, cudaStream_t s);                      \
     int launch_initial(const StepArgs &a, cudaStream_t s, int massopt, int init_h_opt, int init_rhoe, const int *nppermat); \

@@ -763,16 +763,22 @@ __global__ void __launch_bounds__(kRedThreads) k_init_critts(StepArgs a) {
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 static inline int gs_blocks(int n) { int b = nblk(n, 256); return b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b); }
 
-int launch_strain_constitutive(const StepArgs &a, cudaStream_t s) {
+void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
     k_strain_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
+}
+
+int launch_strain_constitutive(const StepArgs &a, cudaStream_t s) {
     int blocks = nblk(a.n, kRedThreads);
     if (a.prm.disctype == 0) k_strain_const<0><<<blocks, kRedThreads, 0, s>>>(a);
     else k_strain_const<1><<<blocks, kRedThreads, 0, s>>>(a);
     return blocks;
 }
 
-int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
+void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
     k_mom_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
+}
+
+int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
     int blocks = nblk(a.n, kRedThreads);
     if (a.prm.disctype == 0) k_momentum<0><<<blocks, kRedThreads, 0, s>>>(a, integrate);
     else k_momentum<1><<<blocks, kRedThreads, 0, s>>>(a, integrate);

@@ -76,8 +76,11 @@ def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0) -> _abi.Co
 
 
 class Solver:
-    def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0):
+    def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0,
+                 device: int | None = None):
         self.lib = _abi.load()
+        if device is not None:
+            check(self.lib.mcm_gpu_set_device(int(device)), "mcm_gpu_set_device")
         self.deck = deck
         self.n = deck.np
         self.nmat = len(deck.materials)
@@ -213,6 +216,61 @@ class Solver:
         check(self.lib.mcm_gpu_stats(self.h, C.byref(mean), C.byref(mx), C.byref(st), C.byref(ngp)), "mcm_gpu_stats",
               self.h)
         return {"mean_nbr": mean.value, "max_nbr": mx.value, "stride": st.value, "ngp": ngp.value}
+
+    # ------------------------------------------------------ measurement
+    def set_diagnostics(self, enable: bool) -> None:
+        check(self.lib.mcm_gpu_set_diagnostics(self.h, int(enable)), "mcm_gpu_set_diagnostics", self.h)
+
+    def profile(self, enable: bool) -> None:
+        check(self.lib.mcm_gpu_profile(self.h, int(enable)), "mcm_gpu_profile", self.h)
+
+    def profile_report(self) -> dict:
+        """{kernel group: (total device ms, launches)} since profile(True)."""
+        out = {}
+        r = 0
+        buf = C.create_string_buffer(64)
+        while True:
+            ms, n = C.c_double(), C.c_int()
+            st = self.lib.mcm_gpu_profile_report(self.h, r, buf, 64, C.byref(ms), C.byref(n))
+            if st == _abi.MCM_EINVAL:
+                break
+            check(st, "mcm_gpu_profile_report", self.h)
+            out[buf.value.decode()] = (ms.value, n.value)
+            r += 1
+        return out
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.mcm_gpu_kernel_launches(self.h))
+
+    def timer_start(self) -> None:
+        check(self.lib.mcm_gpu_timer(self.h, 0, None), "mcm_gpu_timer", self.h)
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        check(self.lib.mcm_gpu_timer(self.h, 1, C.byref(ms)), "mcm_gpu_timer", self.h)
+        return ms.value
+
+    def upload(self, state: dict, bbox=None) -> None:
+        """Uploads a host state (the fields a Fortran driver passes) through mcm_gpu_upload."""
+        f = _abi.Fields()
+        keep = []
+        for nm, arr in state.items():
+            if nm in _abi.INT_FIELDS:
+                a = np.ascontiguousarray(arr, dtype=np.int32)
+                setattr(f, nm, _iptr(a))
+            else:
+                a = np.asarray(arr, dtype=np.float64)
+                if a.ndim == 3:
+                    a = a.transpose(0, 2, 1)
+                a = np.ascontiguousarray(a)
+                setattr(f, nm, _dptr(a))
+            keep.append(a)
+        b = None
+        if bbox is not None:
+            b = np.ascontiguousarray(bbox, dtype=np.float64)
+            keep.append(b)
+        check(self.lib.mcm_gpu_upload(self.h, C.byref(f), _dptr(b) if b is not None else None), "mcm_gpu_upload",
+              self.h)
 
     def close(self) -> None:
         if getattr(self, "h", None):
