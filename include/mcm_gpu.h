@@ -193,6 +193,24 @@ int mcm_gpu_energies(mcm_gpu_handle *h, double *energies);
 /* Mean neighbour count of the last search (for the roofline accounting). */
 int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp);
 
+/* -------------------------------------------------- allocation-free call */
+
+/* No counterpart in the reference.  Per-material energy sums of
+ * MCM/mcm_calctotale.f90's formulas (ke, ie, mom(3) per material, then
+ * kinetice, internale, totale: 5*nmat+3 doubles into `energies`) computed
+ * from DEVICE arrays the caller owns -- mass, vabs, e, mat of length np and v
+ * in the (3,np) layout -- without allocating device memory: for callers that
+ * cannot call cudaMalloc (a host code that gives all device memory to its own
+ * pool, or must keep cudaMalloc/cudaFree and their synchronisation out of the
+ * time step).  Its scratch is a fixed __device__ array of 296 x 5 x 16
+ * doubles (189 440 bytes per GPU, held until exit); nmat above
+ * MCM_GPU_MAX_MATERIALS returns MCM_EINVAL.  The first call on a device looks
+ * up the array's address (make that first call before any stream capture).
+ * Calls share the array, so calls whose kernels overlap on the GPU race.
+ * Runs on `stream` (NULL: the default stream) and waits for it. */
+int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const double *v, const double *e,
+                               const int *mat, int np, int nmat, double *energies, void *stream);
+
 /* ----------------------------------------------------------- measurement */
 
 /* Diagnostic fields (rod, spin, tracerod, etry, einc, rhoold, critts, s, a)

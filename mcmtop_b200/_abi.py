@@ -112,6 +112,7 @@ def load() -> C.CDLL:
         "mcm_gpu_energies": ([H, _DP], C.c_int),
         "mcm_gpu_stats": ([H, _DP, _IP, _IP, _IP], C.c_int),
         "mcm_gpu_set_diagnostics": ([H, C.c_int], C.c_int),
+        "mcm_gpu_calctotale_noalloc": ([C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
         "mcm_gpu_profile": ([H, C.c_int], C.c_int),
         "mcm_gpu_profile_report": ([H, C.c_int, C.c_char_p, C.c_int, _DP, _IP], C.c_int),
         "mcm_gpu_kernel_launches": ([H], C.c_longlong),

@@ -1,0 +1,58 @@
+"""GPU test of mcm_gpu_calctotale_noalloc, the entry point for callers that
+cannot allocate device memory (their device memory belongs to their own pool,
+or they must keep cudaMalloc out of the time step).  It must give the same
+per-material energies as the energy sums of mcm_gpu_step_b, on two calls in a
+row (the calls share one scratch array).  This file sorts last so that a run
+stopping at the first failure has run every other test first."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mcmtop_b200 import _abi
+from mcmtop_b200.deck import taylor_bar
+from mcmtop_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc_energies(lib, state, nmat):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    mass = torch.tensor(state["mass"], dtype=torch.float64, device=dev)
+    vabs = torch.tensor(state["vabs"], dtype=torch.float64, device=dev)
+    v = torch.tensor(np.ascontiguousarray(state["v"]).ravel(), dtype=torch.float64, device=dev)
+    e = torch.tensor(state["e"], dtype=torch.float64, device=dev)
+    mat = torch.tensor(state["mat"], dtype=torch.int32, device=dev)
+    out = torch.full((5 * nmat + 3,), float("nan"), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    st = lib.mcm_gpu_calctotale_noalloc(mass.data_ptr(), vabs.data_ptr(), v.data_ptr(), e.data_ptr(),
+                                        mat.data_ptr(), len(state["mass"]), nmat, out.data_ptr(), None)
+    assert st == _abi.MCM_OK, lib.mcm_gpu_strerror(st)
+    return out.cpu().numpy()
+
+
+def test_noalloc_energies_match_step_b(gpu_lib):
+    lib = gpu_lib
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT, device=0)
+    fields = ["mass", "vabs", "v", "e", "mat"]
+    for call in range(2):
+        for _ in range(3):
+            sol.step()
+        sol.step_a()
+        sol.dt_update()
+        ref = sol.step_b().copy()                      # energies summed inside mcm_gpu_step_b
+        state = sol.download(fields)                   # the arrays that sum read (before step_c)
+        got = _noalloc_energies(lib, state, sol.nmat)
+        scale = np.abs(ref).max()
+        assert np.all(np.isfinite(got))
+        assert np.max(np.abs(got - ref)) <= 1e-13 * scale, (call, got, ref)
+        sol.step_c()
+    sol.close()
+
+
+def test_noalloc_rejects_too_many_materials(gpu_lib):
+    st = gpu_lib.mcm_gpu_calctotale_noalloc(1, 1, 1, 1, 1, 10, _abi.MAX_MATERIALS + 1, 1, None)
+    assert st == _abi.MCM_EINVAL
