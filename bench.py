@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed oracle work")
+    ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
     return ap.parse_args()
 
 
@@ -111,25 +112,27 @@ class ClockSampler:
 
 # --------------------------------------------------------------- roofline
 def algorithmic_bytes(region: str, kbar: float, precision: str) -> float:
-    """Compulsory bytes per particle of one kernel group (ideal caching of the
-    neighbour gathers): own-state reads and writes plus the neighbour table at
-    4 B per entry.  Field lists per kernel:
-      search:   read x(3) h mat; write count + table            -> 36+4+4K
-      strain:   read x v m h rho e p c efps pcut sigma(6) fail, count, table;
-                write x rho e p c efps h sigma(6) q             -> 168+4+4K+120
-      momentum: read x v m rho h sigma(6) q e vabs, dispbc, count, table;
-                write x v vabs                                 -> 144+8+4K+56
-    The mixed path keeps x and v in FP64 and the rest in FP32."""
-    if precision == "mixed":
-        w = 4
-    else:
-        w = 8
+    """Compulsory bytes per particle of one kernel group: the particle's own
+    state read and written plus its neighbour list (16-byte header of per-row
+    counts and one byte per neighbour), with ideal caching of the neighbour
+    gathers (they count zero, as do sorts and intermediates).  Field lists:
+      search:       read x(3) h mat; write header, count, list      36 + 4 + 4 + 16 + K
+      strain:       read x(3) v(3) m rho h, header, list            72 + 16 + K
+      constitutive: read x v (6) m h rho e p c efps pcut fail sigma(6), vabs;
+                    write x(3) h rho e p c efps sigma(6) q          168 + 8 + 120
+      momentum:     read x v (6) m rho h sigma(6) q e vabs dispbc, count, header, list;
+                    write x v (6) vabs                             144 + 8 + 16 + K + 56
+    The mixed path keeps x and v (and the energy/timestep sums) in FP64 and
+    the other fields in FP32."""
+    w = 4 if precision == "mixed" else 8
     if region == "search":
-        return 3 * 8 + w + 4 + 4 + 4 * kbar
-    if region == "strain_constitutive":
-        return 6 * 8 + 15 * w + 4 + 4 * kbar + 3 * 8 + 12 * w
+        return 3 * 8 + w + 4 + 4 + 16 + kbar
+    if region == "strain":
+        return 6 * 8 + 3 * w + 16 + kbar
+    if region == "constitutive":
+        return 6 * 8 + 14 * w + 8 + 3 * 8 + 12 * w
     if region == "momentum_integrate":
-        return 6 * 8 + 12 * w + 8 + 4 * kbar + 6 * 8 + w
+        return 6 * 8 + 12 * w + 4 + 4 + 16 + kbar + 6 * 8 + 8
     return 0.0
 
 
@@ -190,7 +193,7 @@ def gpu_arm(args):
     prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
     deck = taylor_bar(dx=args.dx)
     workload = f"taylor_bar_{deck.np}"
-    sol = Solver(deck, prec, device=local)
+    sol = Solver(deck, prec, device=local, reorder_interval=args.reorder)
     sol.set_diagnostics(False)
     sol.run(args.warmup)
     stats = sol.stats()
@@ -228,7 +231,7 @@ def gpu_arm(args):
 
     # roofline of the dominant kernel group
     peak, peak_kind = load_peaks()
-    main = {k: v for k, v in report.items() if k in ("search", "strain_constitutive", "momentum_integrate")}
+    main = {k: v for k, v in report.items() if k in ("search", "strain", "constitutive", "momentum_integrate")}
     dom = max(main, key=lambda k: main[k][0])
     dom_ms, dom_n = main[dom]
     per_launch_s = dom_ms / 1e3 / max(dom_n, 1)
@@ -284,7 +287,8 @@ def gpu_arm(args):
         "data": "synthetic: seeded jittered cubic lattice (Taylor bar, cm-g-us deck), no dataset",
         "config": {"workload": workload, "particles": deck.np, "dx_mm": args.dx * 1e3, "precision": args.precision,
                    "material": "copper model 10 + Mie-Grueneisen EOS 41, h = 1.3 dx, CFL 0.3 (tcrit_opt 1)",
-                   "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU"},
+                   "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
+                   "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         "kernels": kernels,
     }

@@ -30,7 +30,7 @@ UNITS = [
     ("step_fp64_fast.cu", True),
     ("noalloc.cu", False),
 ]
-HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

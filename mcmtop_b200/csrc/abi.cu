@@ -49,6 +49,8 @@ struct mcm_gpu_handle {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs[16];
     long long kernel_launches = 0;
     cudaEvent_t timer[2] = {nullptr, nullptr};
+    long long steps_enqueued = 0;
+    bool have_cells = false;   // cell_list holds a valid permutation
 };
 
 namespace {
@@ -78,10 +80,10 @@ inline int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
 
 // Kernel groups that the profiler times separately.
 enum Region {
-    R_CELLS = 0, R_GHOSTS, R_SEARCH, R_STRAIN_PREP, R_STRAIN, R_CRITTS, R_MOM_PREP, R_MOMENTUM, R_REDUCE,
-    R_MOVE, R_MISC, R_NREG
+    R_CELLS = 0, R_GHOSTS, R_SEARCH, R_STRAIN_PREP, R_STRAIN, R_CONST, R_CRITTS, R_MOM_PREP, R_MOMENTUM,
+    R_REDUCE, R_MOVE, R_MISC, R_NREG
 };
-const char *kRegionName[R_NREG] = {"cell_list", "ghosts", "search", "strain_prep", "strain_constitutive",
+const char *kRegionName[R_NREG] = {"cell_list", "ghosts", "search", "strain_prep", "strain", "constitutive",
                                    "critts_dt", "momentum_prep", "momentum_integrate", "energy_bbox_reduce",
                                    "update_move", "misc"};
 
@@ -176,6 +178,11 @@ int alloc_particles(mcm_gpu_handle *h) {
     h->A.F.ptype = h->d_ints + 3 * np;
     if ((st = dalloc(h, &h->A.key, np))) return st;
     if ((st = dalloc(h, &h->A.cell_list, np))) return st;
+    if ((st = dalloc(h, &h->A.cpos, np))) return st;
+    if ((st = dalloc(h, &h->A.cmat, np))) return st;
+    if ((st = dalloc(h, &h->A.ckey, np))) return st;
+    if ((st = dalloc(h, &h->A.nhdr, 2 * np))) return st;
+    if ((st = dalloc(h, &h->A.reorder_tmp, np))) return st;
     if ((st = dalloc(h, &h->A.nnbr, np))) return st;
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
     CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
@@ -183,7 +190,7 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.rec0, np))) return st;
     if ((st = dalloc(h, &h->A.rec1, np))) return st;
     if ((st = dalloc(h, &h->A.rec2, np))) return st;
-    h->red_cap = (int)((np + kRedThreads - 1) / kRedThreads) + 8;
+    h->red_cap = (int)((np + 15) / 16) + 8;   // blocks of the cooperative momentum kernel (16 particles each)
     if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
     return MCM_OK;
 }
@@ -217,11 +224,11 @@ int alloc_ghosts(mcm_gpu_handle *h, int cap) {
     return MCM_OK;
 }
 
-int alloc_table(mcm_gpu_handle *h, int stride, int gstride) {
+int alloc_table(mcm_gpu_handle *h, int nwords, int gstride) {
     int st;
-    h->A.stride = stride;
+    h->A.nwords = nwords;
     h->A.gstride = gstride;
-    if ((st = dalloc(h, &h->A.nbr, (size_t)stride * h->npad))) return st;
+    if ((st = dalloc(h, &h->A.nlist, (size_t)nwords * h->npad))) return st;
     if ((st = dalloc(h, &h->A.gnbr, (size_t)gstride * h->npad))) return st;
     return MCM_OK;
 }
@@ -246,10 +253,11 @@ int regrow(mcm_gpu_handle *h, int *grew) {
     int st;
     switch (s.code) {
         case MCM_ENBR_OVERFLOW: {
-            int ns = h->A.stride, ng = h->A.gstride;
-            if (s.req_stride > ns) ns = round_up(s.req_stride + s.req_stride / 8 + 8, 8);
+            if (s.req_stride < 0) break;   // a row with more than 256 candidates or 127 neighbours
+            int nw = h->A.nwords, ng = h->A.gstride;
+            if (s.req_stride > nw * 4) nw = (s.req_stride + s.req_stride / 8 + 8 + 3) / 4;
             if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
-            if ((st = alloc_table(h, ns, ng))) return st;
+            if ((st = alloc_table(h, nw, ng))) return st;
             *grew = 1;
             break;
         }
@@ -278,10 +286,15 @@ int launch_strain(mcm_gpu_handle *h) {
         if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_strain_prep(h->A, h->stream);
         else fast::launch_strain_prep(h->A, h->stream);
     }
-    Scope sc(h, R_STRAIN, 1);
+    {
+        Scope sc(h, R_STRAIN, 1);
+        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_strain(h->A, h->stream);
+        else fast::launch_strain(h->A, h->stream);
+    }
+    Scope sc(h, R_CONST, 1);
     switch (h->cfg.precision) {
-        case MCM_PREC_FP64_EXACT: return exact::launch_strain_constitutive(h->A, h->stream);
-        default: return fast::launch_strain_constitutive(h->A, h->stream);
+        case MCM_PREC_FP64_EXACT: return exact::launch_constitutive(h->A, h->stream);
+        default: return fast::launch_constitutive(h->A, h->stream);
     }
 }
 int launch_mom(mcm_gpu_handle *h, int integrate) {
@@ -316,8 +329,15 @@ int active_planes(const mcm_gpu_handle *h) {
 // neighbours -> strain -> constitutive -> critts (MCM/mcm_solution.f90:41-53)
 void enqueue_part_a(mcm_gpu_handle *h) {
     StepArgs &a = h->A;
+    const int every = h->cfg.reorder_interval;
+    if (every > 0 && h->have_cells && (h->steps_enqueued % every) == 0) {
+        Scope sc(h, R_MISC, 2 * (NFIELD + 4));
+        launch_reorder(a, h->stream);
+    }
+    ++h->steps_enqueued;
+    h->have_cells = true;
     {
-        Scope sc(h, R_CELLS, 7);
+        Scope sc(h, R_CELLS, 8);
         launch_grid_setup(a, h->stream);
         launch_cell_build(a, h->stream);
     }
@@ -546,7 +566,8 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->A.grid = (DevGrid *)p; p += 256;
     h->A.bbox = (double *)p; p += 256;
     h->A.ngp = (int *)p; p += 64;
-    h->A.plane_base = (int *)p; p += 64;
+    h->A.plane_base = (int *)p; p += 32;
+    h->A.n_inside = (int *)p; p += 32;
     h->A.energy = (double *)p;
     cudaMallocHost((void **)&h->h_time, 4096);
     char *q = (char *)h->h_time;
@@ -556,8 +577,8 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->h_ngp = (int *)(q + 1024);
     h->h_energy = (double *)(q + 1088);
     TRY(alloc_particles(h));
-    int stride = cfg->nbr_stride > 0 ? round_up(cfg->nbr_stride, 8) : 96;
-    TRY(alloc_table(h, stride, cfg->boundary ? 48 : 8));
+    int entries = cfg->nbr_stride > 0 ? cfg->nbr_stride : 100;
+    TRY(alloc_table(h, (entries + 3) / 4, cfg->boundary ? 48 : 8));
     TRY(alloc_cells(h, 1 << 16));
     TRY(alloc_ghosts(h, cfg->boundary ? std::max(4096, np / 8) : 32));
     TRY(dalloc(h, &h->d_nppermat, (size_t)nmat));
@@ -572,10 +593,11 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->d_fields, h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
+                    h->A.cpos, h->A.cmat, h->A.ckey, h->A.nhdr, h->A.reorder_tmp, h->A.nlist,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat,
-                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.nbr, h->A.gnbr};
+                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_time) cudaFreeHost(h->h_time);
@@ -689,7 +711,10 @@ int run_search_only(mcm_gpu_handle *h) {
         launch_search(a, h->stream);
         if ((st = sync_status(h))) return st;
         int code = h->h_status->code;
-        if (code == MCM_OK) return MCM_OK;
+        if (code == MCM_OK) {
+            h->have_cells = true;
+            return MCM_OK;
+        }
         int grew = 0;
         if ((st = regrow(h, &grew))) return st;
         if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
@@ -1026,29 +1051,63 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
     if ((st = check_handle(h))) return st;
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np, np = h->npad;
-    std::vector<int> orig(n), cnt(n), gcnt(n);
+    std::vector<int> orig(n), cnt(n), gcnt(n), clist(n), ckey(n);
     CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(cnt.data(), h->A.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(gcnt.data(), h->A.gnnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ckey.data(), h->A.ckey, sizeof(int) * n, cudaMemcpyDeviceToHost));
     int need = 0, gneed = 0;
-    for (int p = 0; p < n; ++p) { need = std::max(need, cnt[p]); gneed = std::max(gneed, gcnt[p]); }
-    if (nnbr) for (int p = 0; p < n; ++p) nnbr[orig[p]] = cnt[p];
-    if (g_nnbr) for (int p = 0; p < n; ++p) g_nnbr[orig[p]] = gcnt[p];
+    for (int t = 0; t < n; ++t) { need = std::max(need, cnt[t]); gneed = std::max(gneed, gcnt[t]); }
+    if (nnbr) for (int t = 0; t < n; ++t) nnbr[orig[clist[t]]] = cnt[t];
+    if (g_nnbr) for (int t = 0; t < n; ++t) g_nnbr[orig[clist[t]]] = gcnt[t];
     bool small = (nbr && stride && *stride < need) || (g_nbr && g_stride && *g_stride < gneed);
     if (stride) { if (small || !nbr) *stride = std::max(*stride, need); }
     if (g_stride) { if (small || !g_nbr) *g_stride = std::max(*g_stride, gneed); }
     if (small) return MCM_EINVAL;
     if (nbr && stride) {
-        std::vector<int> tab((size_t)h->A.stride * np);
-        CK(cudaMemcpy(tab.data(), h->A.nbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
-        for (int p = 0; p < n; ++p)
-            for (int k = 0; k < cnt[p]; ++k) nbr[(size_t)orig[p] * *stride + k] = orig[tab[(size_t)k * np + p]] + 1;
+        DevGrid g;
+        CK(cudaMemcpy(&g, h->A.grid, sizeof(g), cudaMemcpyDeviceToHost));
+        std::vector<int> cstart((size_t)g.ncells + 1);
+        CK(cudaMemcpy(cstart.data(), h->A.cell_start, sizeof(int) * cstart.size(), cudaMemcpyDeviceToHost));
+        std::vector<unsigned long long> hdr(2 * (size_t)np);
+        CK(cudaMemcpy(hdr.data(), h->A.nhdr, sizeof(unsigned long long) * hdr.size(), cudaMemcpyDeviceToHost));
+        std::vector<unsigned int> words((size_t)h->A.nwords * np);
+        CK(cudaMemcpy(words.data(), h->A.nlist, sizeof(unsigned int) * words.size(), cudaMemcpyDeviceToHost));
+        const int *gl = g.gridlim;
+        for (int t = 0; t < n; ++t) {
+            int *row = nbr + (size_t)orig[clist[t]] * *stride;
+            int k = 0;
+            const int key = ckey[t];
+            if (key >= 0) {
+                int bx = key % gl[0] + 1, r0 = key / gl[0], by = r0 % gl[1] + 1, bz = r0 / gl[1] + 1;
+                int lo0 = std::max(bx - 1, 1), hi0 = std::min(bx + 1, gl[0]);
+                int lo1 = std::max(by - 1, 1), hi1 = std::min(by + 1, gl[1]);
+                int lo2 = std::max(bz - 1, 1), hi2 = std::min(bz + 1, gl[2]);
+                int e = 0;
+                for (int pass = 0; pass < (h->nmat > 1 ? 2 : 1); ++pass) {
+                    unsigned long long hh = hdr[(size_t)pass * np + t];
+                    int r = 0;
+                    for (int nz = lo2; nz <= hi2; ++nz)
+                        for (int my = lo1; my <= hi1; ++my, ++r) {
+                            int c = (int)((hh >> (7 * r)) & 127ull);
+                            int rs = cstart[(size_t)cell_key(lo0, my, nz, gl)];
+                            for (int q = 0; q < c; ++q, ++e) {
+                                unsigned int wv = words[(size_t)(e / 4) * np + t];
+                                int off = (int)((wv >> (8 * (e % 4))) & 255u);
+                                row[k++] = orig[clist[rs + off]] + 1;
+                            }
+                        }
+                }
+            }
+            if (h->cfg.disctype == 1) row[k++] = orig[clist[t]] + 1;
+        }
     }
     if (g_nbr && g_stride) {
         std::vector<int> tab((size_t)h->A.gstride * np);
         CK(cudaMemcpy(tab.data(), h->A.gnbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
-        for (int p = 0; p < n; ++p)
-            for (int k = 0; k < gcnt[p]; ++k) g_nbr[(size_t)orig[p] * *g_stride + k] = tab[(size_t)k * np + p] + 1;
+        for (int t = 0; t < n; ++t)
+            for (int k = 0; k < gcnt[t]; ++k) g_nbr[(size_t)orig[clist[t]] * *g_stride + k] = tab[(size_t)k * np + t] + 1;
     }
     return MCM_OK;
 }
@@ -1125,7 +1184,7 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
         CK(cudaMemcpy(&s, h->A.status, sizeof(s), cudaMemcpyDeviceToHost));
         *max_nbr = s.max_nbr;
     }
-    if (stride) *stride = h->A.stride;
+    if (stride) *stride = h->A.nwords * 4;
     if (ngp) CK(cudaMemcpy(ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
     return MCM_OK;
 }

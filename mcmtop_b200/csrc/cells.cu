@@ -13,7 +13,7 @@
 // Compiled without fused multiply-add: the cell index int(gridsize*(x-gridmin))
 // and the predicate d^2 < (h_i+h_j)^2 are evaluated exactly as the reference
 // does in FP64, so borderline pairs resolve identically.
-#include "kernels.h"
+#include "nbr_iter.cuh"
 
 namespace mcm {
 
@@ -81,6 +81,7 @@ __global__ void k_grid_setup(StepArgs a) {
     }
     *a.grid = g;
     *a.ngp = 0;
+    *a.n_inside = 0;
 }
 
 // --------------------------------------------------------------- cell keys
@@ -197,13 +198,31 @@ static void device_exclusive_scan(const int *in, int *out, int *sums, const long
 }
 
 // --------------------------------------------------------------- scatter
+// Particles outside the grid (llpointer = -1 in the reference) take the
+// positions after the last cell; they have no neighbours and are never one.
 __global__ void k_cell_scatter(StepArgs a) {
     if (a.status->code) return;
+    const int base_out = a.cell_start[a.grid->ncells];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         int key = a.key[i];
-        if (key < 0) continue;
+        if (key < 0) {
+            a.cell_list[base_out + atomicAdd(a.n_inside, 1)] = i;
+            continue;
+        }
         int slot = atomicSub(&a.cell_count[key], 1) - 1;
         a.cell_list[a.cell_start[key] + slot] = i;
+    }
+}
+
+// Candidate records in cell order (positions at neighbour time).
+__global__ void k_cell_records(StepArgs a) {
+    if (a.status->code) return;
+    const double *X = a.F.f[FX], *Y = a.F.f[FY], *Z = a.F.f[FZ], *H = a.F.f[FH];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        int i = a.cell_list[p];
+        a.cpos[p] = make_double4(X[i], Y[i], Z[i], H[i]);
+        a.cmat[p] = a.F.mat[i];
+        a.ckey[p] = a.key[i];
     }
 }
 
@@ -244,6 +263,38 @@ void launch_cell_build(const StepArgs &a, cudaStream_t s) {
     device_exclusive_scan(a.cell_count, a.cell_start, a.scan_sums, &a.grid->ncells, a.cell_cap, s);
     k_cell_scatter<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
     k_cell_sort<<<grid_blocks(a.cell_cap, 128), 128, 0, s>>>(a);
+    k_cell_records<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
+}
+
+// ------------------------------------------------------------- re-sorting
+// Permutes the particle state into the cell order of the last step's list,
+// so that the gathers of later steps walk memory nearly in order.  Results do
+// not depend on it: every order used by the step is defined by cell keys and
+// reference indices, not by storage positions.
+__global__ void k_permute_field(const double *src, double *dst, const int *perm, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[perm[p]];
+}
+__global__ void k_permute_int(const int *src, int *dst, const int *perm, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[perm[p]];
+}
+__global__ void k_copy_back(const double *src, double *dst, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[p];
+}
+__global__ void k_copy_back_int(const int *src, int *dst, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[p];
+}
+
+void launch_reorder(const StepArgs &a, cudaStream_t s) {
+    const int b = grid_blocks(a.n, 256);
+    for (int f = 0; f < NFIELD; ++f) {
+        k_permute_field<<<b, 256, 0, s>>>(a.F.f[f], a.reorder_tmp, a.cell_list, a.n);
+        k_copy_back<<<b, 256, 0, s>>>(a.reorder_tmp, a.F.f[f], a.n);
+    }
+    int *ints[4] = {a.F.mat, a.F.dispbc, a.F.orig, a.F.ptype};
+    for (int *p : ints) {
+        k_permute_int<<<b, 256, 0, s>>>(p, (int *)a.reorder_tmp, a.cell_list, a.n);
+        k_copy_back_int<<<b, 256, 0, s>>>((const int *)a.reorder_tmp, p, a.n);
+    }
 }
 
 // ------------------------------------------------------------------ ghosts
@@ -359,7 +410,7 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
                 a.gmass[g] = a.F.f[FMASS][j];
                 a.gh[g] = a.F.f[FH][j];
                 a.ghold[g] = a.F.f[FHOLD][j];
-                a.grho[g] = a.F.f[FRHO][j];
+                a.grho[g] = a.prm.mixed ? (double)a.F.s[FRHO][j] : a.F.f[FRHO][j];
                 a.gx[g] = a.F.f[FX][j] * mult[0] + add[0];
                 a.gy[g] = a.F.f[FY][j] * mult[1] + add[1];
                 a.gz[g] = a.F.f[FZ][j] * mult[2] + add[2];
@@ -401,212 +452,143 @@ void launch_ghosts(const StepArgs &a, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------ search
-// MCM/mcm_ll_neighbours.f90:96-299.  One warp per particle; the candidates of
-// a row of three x-adjacent cells are spread over the lanes and accepted
-// pairs are compacted in lane order with ballots, which keeps the
-// reference's order.  A block handles a tile of 32 consecutive particles and
-// writes its lists column-major with coalesced stores.
+// MCM/mcm_ll_neighbours.f90:96-299.  One thread per cell-order position.  A
+// row of three x-adjacent cells is a contiguous range of positions whose
+// candidate records (cpos) sit next to each other in memory, and the threads
+// of a warp (neighbouring positions, mostly the same cell) read the same rows,
+// so the candidate loads are served by L1.  Accepted neighbours are stored as
+// one byte each (offset inside the row) in row order; the per-row counts go to
+// a 64-bit header.  This reproduces the reference's neighbour sequence: rows
+// in z, y order, cells in x order, each cell in descending reference index.
 
-constexpr int kSearchWarps = 8;
-constexpr int kSearchTile = 32;
-
-size_t search_smem_bytes(const StepArgs &a) {
-    return sizeof(int) * ((size_t)kSearchTile * (a.stride + a.gstride) + (size_t)kSearchWarps * (a.stride + a.gstride) +
-                          2 * kSearchTile);
-}
-
-__device__ __forceinline__ double exact_d2(double xi, double yi, double zi, double xj, double yj, double zj, int ndim) {
-    double d = __dsub_rn(xj, xi);
+__device__ __forceinline__ double exact_d2(double4 a, double4 b) {
+    double d = __dsub_rn(b.x, a.x);
     double s = __dmul_rn(d, d);
-    if (ndim > 1) { d = __dsub_rn(yj, yi); s = __dadd_rn(s, __dmul_rn(d, d)); }
-    if (ndim > 2) { d = __dsub_rn(zj, zi); s = __dadd_rn(s, __dmul_rn(d, d)); }
+    d = __dsub_rn(b.y, a.y);
+    s = __dadd_rn(s, __dmul_rn(d, d));
+    d = __dsub_rn(b.z, a.z);
+    s = __dadd_rn(s, __dmul_rn(d, d));
     return s;
 }
 
-__global__ void __launch_bounds__(kSearchWarps * 32) k_search(StepArgs a) {
-    extern __shared__ int smem[];
+__global__ void __launch_bounds__(256) k_search(StepArgs a) {
     if (a.status->code) return;
-    const int stride = a.stride, gstride = a.gstride;
-    int *s_nbr = smem;                                    // [tile][stride]
-    int *s_gnbr = s_nbr + kSearchTile * stride;           // [tile][gstride]
-    int *s_cont = s_gnbr + kSearchTile * gstride;         // [warps][stride]
-    int *s_gcont = s_cont + kSearchWarps * stride;        // [warps][gstride]
-    int *s_nn = s_gcont + kSearchWarps * gstride;         // [tile]
-    int *s_gn = s_nn + kSearchTile;                       // [tile]
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const DevGrid g = *a.grid;
-    const int ndim = a.prm.ndim;
-    const double *X = a.F.f[FX], *Y = a.F.f[FY], *Z = a.F.f[FZ], *H = a.F.f[FH];
-    const int *MAT = a.F.mat;
-    const int tile0 = blockIdx.x * kSearchTile;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int np = a.npad;
+    const int key = a.ckey[t];
+    const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
-
-    for (int p = warp; p < kSearchTile; p += kSearchWarps) {
-        const int i = tile0 + p;
-        int nn = 0, gn = 0;
-        double mind = 1.0e20;
-        bool inside = false;
-        if (i < a.n && a.key[i] >= 0) {
-            inside = true;
-            const double xi = X[i], yi = Y[i], zi = Z[i], hi = H[i];
-            const int mati = MAT[i];
-            int box[3] = {1, 1, 1}, lo[3] = {1, 1, 1}, hi_[3] = {1, 1, 1};
-            const double xv[3] = {xi, yi, zi};
-            for (int j = 0; j < ndim; ++j) {
-                box[j] = (int)(g.gridsize[j] * (xv[j] - g.gridmin[j])) + 1;
-                lo[j] = box[j] - 1 > 1 ? box[j] - 1 : 1;
-                hi_[j] = box[j] + 1 < g.gridlim[j] ? box[j] + 1 : g.gridlim[j];
-            }
-            int n_same = 0, n_cont = 0, g_same = 0, g_cont = 0;
-            double lmin = 1.0e20, lminc = 1.0e20;
-            int *my_nbr = s_nbr + p * stride;
-            int *my_gnbr = s_gnbr + p * gstride;
-            int *my_cont = s_cont + warp * stride;
-            int *my_gcont = s_gcont + warp * gstride;
-            for (int nz = lo[2]; nz <= hi_[2]; ++nz) {
-                for (int my = lo[1]; my <= hi_[1]; ++my) {
-                    const int k0 = (int)cell_key(lo[0], my, nz, g.gridlim);
-                    const int k1 = k0 + (hi_[0] - lo[0]);
-                    // real particles of the row, in reference chain order
+    int nn = 0, gn = 0;
+    double mind = 1.0e20;
+    bool inside = key >= 0;
+    if (inside) {
+        const DevGrid g = *a.grid;
+        int bx, by, bz;
+        cell_coords(key, g.gridlim, bx, by, bz);
+        const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
+        const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
+        const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
+        const double4 xi = a.cpos[t];
+        const int mati = a.cmat[t];
+        const int cap = a.nwords * 4;
+        unsigned int word = 0;
+        int nb = 0, w = 0;
+        const int passes = a.nmat > 1 ? 2 : 1;
+        for (int pass = 0; pass < passes; ++pass) {
+            unsigned long long hdr = 0ull;
+            int r = 0;
+            for (int nz = lo2; nz <= hi2; ++nz) {
+                for (int my = lo1; my <= hi1; ++my, ++r) {
+                    const int k0 = (int)cell_key(lo0, my, nz, g.gridlim);
+                    const int k1 = k0 + (hi0 - lo0);
                     const int rs = a.cell_start[k0], re = a.cell_start[k1 + 1];
-                    for (int b = rs; b < re; b += 32) {
-                        const int idx = b + lane;
-                        bool acc = false, same = false;
-                        int j = -1;
-                        if (idx < re) {
-                            j = a.cell_list[idx];
-                            if (j != i) {
-                                double d2 = exact_d2(xi, yi, zi, X[j], Y[j], Z[j], ndim);
-                                double hs = __dadd_rn(H[j], hi);
-                                double hsq = __dmul_rn(hs, hs);
-                                if (d2 < hsq) {
-                                    acc = true;
-                                    same = (MAT[j] == mati);
-                                    if (same) lmin = fmin(lmin, d2);
-                                    else lminc = fmin(lminc, d2);
-                                }
+                    if (re - rs > 256) {
+                        a.status->req_stride = -1;
+                        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+                    }
+                    int cnt = 0;
+                    for (int p = rs; p < re; ++p) {
+                        if (p == t) continue;
+                        const double4 c = a.cpos[p];
+                        const double d2 = exact_d2(xi, c);
+                        const double hs = __dadd_rn(c.w, xi.w);
+                        if (d2 < __dmul_rn(hs, hs)) {
+                            const bool same = (a.cmat[p] == mati);
+                            if (same != (pass == 0)) continue;
+                            mind = fmin(mind, d2);
+                            ++cnt;
+                            word |= (unsigned int)(p - rs) << (8 * nb);
+                            if (++nb == 4) {
+                                if (w < a.nwords) a.nlist[(size_t)w * np + t] = word;
+                                ++w;
+                                word = 0u;
+                                nb = 0;
                             }
                         }
-                        unsigned bs = __ballot_sync(0xffffffffu, acc && same);
-                        unsigned bc = __ballot_sync(0xffffffffu, acc && !same);
-                        if (acc && same) {
-                            int pos = n_same + __popc(bs & lt_mask);
-                            if (pos < stride) my_nbr[pos] = j;
-                        } else if (acc) {
-                            int pos = n_cont + __popc(bc & lt_mask);
-                            if (pos < stride) my_cont[pos] = j;
-                        }
-                        n_same += __popc(bs);
-                        n_cont += __popc(bc);
                     }
-                    // ghost cells of the row, one cell at a time (newest ghost first)
-                    if (a.prm.boundary) {
-                        for (int c = k0; c <= k1; ++c) {
-                            const int2 gc = a.gcell[c];
-                            for (int b = 0; b < gc.y; b += 32) {
-                                const int r = b + lane;
-                                bool acc = false, same = false;
-                                int q = -1;
-                                if (r < gc.y) {
-                                    q = gc.x + gc.y - 1 - r;
-                                    double d2 = exact_d2(xi, yi, zi, a.gx[q], a.gy[q], a.gz[q], ndim);
-                                    double hs = __dadd_rn(a.gh[q], hi);
-                                    double hsq = __dmul_rn(hs, hs);
-                                    if (d2 < hsq) {
-                                        acc = true;
-                                        same = (a.gmat[q] == mati);
-                                        if (same) lmin = fmin(lmin, d2);
-                                        else lminc = fmin(lminc, d2);
+                    if (cnt > 127) {
+                        a.status->req_stride = -1;
+                        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+                    }
+                    hdr |= (unsigned long long)(cnt & 127) << (7 * r);
+                    nn += cnt;
+                }
+            }
+            a.nhdr[(size_t)pass * np + t] = hdr;
+        }
+        if (nb > 0 && w < a.nwords) a.nlist[(size_t)w * np + t] = word;
+        if (nn > cap) {
+            atomicMax(&a.status->req_stride, nn);
+            raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+        }
+        // ghosts: only neighbourhoods that reach a ghost layer
+        if (a.prm.boundary) {
+            const DevPlanes &pl = a.prm.planes;
+            const bool near = (lo0 == 1 && pl.code[0][0]) || (hi0 == g.gridlim[0] && pl.code[1][0]) ||
+                              (lo1 == 1 && pl.code[0][1]) || (hi1 == g.gridlim[1] && pl.code[1][1]) ||
+                              (lo2 == 1 && pl.code[0][2]) || (hi2 == g.gridlim[2] && pl.code[1][2]);
+            if (near) {
+                const int gpasses = a.nmat > 1 ? 2 : 1;
+                for (int pass = 0; pass < gpasses; ++pass) {
+                    for (int nz = lo2; nz <= hi2; ++nz)
+                        for (int my = lo1; my <= hi1; ++my)
+                            for (int lx = lo0; lx <= hi0; ++lx) {
+                                const int2 gc = a.gcell[(int)cell_key(lx, my, nz, g.gridlim)];
+                                for (int r = 0; r < gc.y; ++r) {
+                                    const int q = gc.x + gc.y - 1 - r;
+                                    const double4 c = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
+                                    const double d2 = exact_d2(xi, c);
+                                    const double hs = __dadd_rn(c.w, xi.w);
+                                    if (d2 < __dmul_rn(hs, hs)) {
+                                        const bool same = (a.gmat[q] == mati);
+                                        if (same != (pass == 0)) continue;
+                                        mind = fmin(mind, d2);
+                                        if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
+                                        ++gn;
                                     }
                                 }
-                                unsigned bs = __ballot_sync(0xffffffffu, acc && same);
-                                unsigned bc = __ballot_sync(0xffffffffu, acc && !same);
-                                if (acc && same) {
-                                    int pos = g_same + __popc(bs & lt_mask);
-                                    if (pos < gstride) my_gnbr[pos] = q;
-                                } else if (acc) {
-                                    int pos = g_cont + __popc(bc & lt_mask);
-                                    if (pos < gstride) my_gcont[pos] = q;
-                                }
-                                g_same += __popc(bs);
-                                g_cont += __popc(bc);
                             }
-                        }
-                    }
+                }
+                if (gn > a.gstride) {
+                    atomicMax(&a.status->req_gstride, gn);
+                    raise_status(a.status, MCM_ENBR_OVERFLOW, i);
                 }
             }
-            __syncwarp();
-            // kernel contact (contacttype 0): contacts follow the same-material list
-            for (int k = lane; k < n_cont; k += 32) {
-                int pos = n_same + k;
-                if (pos < stride && k < stride) my_nbr[pos] = my_cont[k];
-            }
-            nn = n_same + n_cont;
-            if (a.prm.boundary) {
-                for (int k = lane; k < g_cont; k += 32) {
-                    int pos = g_same + k;
-                    if (pos < gstride && k < gstride) my_gnbr[pos] = my_gcont[k];
-                }
-                gn = g_same + g_cont;
-            } else {
-                gn = g_same;
-            }
-            // mindist (MCM/mcm_ll_neighbours.f90:152,167,252,268)
-            double m = fmin(lmin, lminc);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-            mind = sqrt(m);
-            if (with_self) {
-                // MCM/mcm_ll_neighbours.f90:288-299
-                if (lane == 0 && nn < stride) my_nbr[nn] = i;
-                nn += 1;
-            }
-            __syncwarp();
         }
-        if (lane == 0) {
-            s_nn[p] = nn;
-            s_gn[p] = gn;
-            if (i < a.n) {
-                a.nnbr[i] = nn;
-                a.gnnbr[i] = gn;
-                if (a.prm.tcrit_opt == 2 || a.prm.diag) a.F.f[FMINDIST][i] = inside ? mind : 1.0e20;
-                if (nn > stride) { atomicMax(&a.status->req_stride, nn); raise_status(a.status, MCM_ENBR_OVERFLOW, i); }
-                if (gn > gstride) { atomicMax(&a.status->req_gstride, gn); raise_status(a.status, MCM_ENBR_OVERFLOW, i); }
-                atomicMax(&a.status->max_nbr, nn);
-                atomicMax(&a.status->max_gnbr, gn);
-            }
-        }
+        mind = sqrt(mind);
     }
-    __syncthreads();
-    // coalesced column-major write-out of the tile
-    int maxn = 0, maxg = 0;
-    for (int p = 0; p < kSearchTile; ++p) {
-        maxn = max(maxn, min(s_nn[p], stride));
-        maxg = max(maxg, min(s_gn[p], gstride));
-    }
-    for (int t = threadIdx.x; t < maxn * kSearchTile; t += blockDim.x) {
-        int k = t / kSearchTile, p = t % kSearchTile;
-        int i = tile0 + p;
-        if (i < a.npad) a.nbr[(size_t)k * a.npad + i] = (k < s_nn[p]) ? s_nbr[p * stride + k] : -1;
-    }
-    for (int t = threadIdx.x; t < maxg * kSearchTile; t += blockDim.x) {
-        int k = t / kSearchTile, p = t % kSearchTile;
-        int i = tile0 + p;
-        if (i < a.npad) a.gnbr[(size_t)k * a.npad + i] = (k < s_gn[p]) ? s_gnbr[p * gstride + k] : -1;
-    }
+    if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
+    a.nnbr[t] = nn;
+    a.gnnbr[t] = gn;
+    if (a.prm.tcrit_opt == 2 || a.prm.diag) a.F.f[FMINDIST][i] = mind;
+    atomicMax(&a.status->max_nbr, nn);
+    atomicMax(&a.status->max_gnbr, gn);
 }
 
 void launch_search(const StepArgs &a, cudaStream_t s) {
-    size_t smem = search_smem_bytes(a);
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
-    int blocks = (a.n + kSearchTile - 1) / kSearchTile;
-    k_search<<<blocks, kSearchWarps * 32, smem, s>>>(a);
+    int blocks = (a.n + 255) / 256;
+    k_search<<<blocks, 256, 0, s>>>(a);
 }
 
 }  // namespace mcm

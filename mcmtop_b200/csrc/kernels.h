@@ -10,8 +10,8 @@ struct StepArgs {
     int n;            // particles
     int npad;         // column pitch of per-particle arrays (multiple of 32)
     int nmat;
-    int stride;       // neighbour-table width, real neighbours (incl. contacts and self)
-    int gstride;      // neighbour-table width, ghost neighbours
+    int nwords;       // neighbour-list width in 32-bit words (4 one-byte entries each)
+    int gstride;      // ghost-neighbour table width (int32 entries)
     int ghost_cap;    // ghost storage
     long long cell_cap;   // cell-array storage
     int layer_cap;    // scratch for one boundary layer
@@ -23,11 +23,17 @@ struct StepArgs {
     DevStatus *status;
     DevGrid *grid;
     double *bbox;     // [2][3]: min, max (mcm_coord_maxmin)
-    // cell list
-    int *key;         // per particle cell key or -1
+    // cell list.  "Position" p is a particle's rank in cell order (cells in
+    // key order, each cell in descending reference index, particles outside
+    // the grid last); cell_list[p] is its state index.
+    int *key;         // per state index: cell key or -1
     int *cell_count;  // cell_cap
     int *cell_start;  // cell_cap + 1
-    int *cell_list;   // npad
+    int *cell_list;   // npad: position -> state index
+    int *n_inside;    // particles inside the grid (device counter)
+    double4 *cpos;    // per position: x, y, z, h at neighbour time
+    int *cmat;        // per position: material
+    int *ckey;        // per position: cell key or -1
     int *scan_sums;   // block sums of the scan
     int2 *gcell;      // per cell: first ghost index, ghost count
     // ghosts (SoA, ghost_cap each)
@@ -36,8 +42,16 @@ struct StepArgs {
     int *ngp;         // device ghost counter
     int *plane_base;  // ghost index base of the plane being built
     int *layer_count, *layer_off;
-    // neighbour table (column-major: entry k of particle i at k*npad + i)
-    int *nbr, *gnbr, *nnbr, *gnnbr;
+    // neighbour lists, per position p, in the reference order: one byte per
+    // real neighbour (its offset inside its row of three x-adjacent cells),
+    // word w of p at nlist[w*npad + p]; nhdr[p] packs the per-row counts
+    // (7 bits x 9 rows) of same-material neighbours, nhdr[npad + p] those of
+    // other-material (contact) neighbours.  Ghost neighbours: int32 ghost
+    // indices, entry k of p at gnbr[k*npad + p].
+    unsigned int *nlist;
+    unsigned long long *nhdr;
+    int *gnbr, *nnbr, *gnnbr;
+    double *reorder_tmp;   // npad doubles of scratch for the state permutation
     // gather records
     double4 *rec0, *rec1, *rec2;   // per particle
     double4 *grec0, *grec1, *grec2;  // per ghost
@@ -54,7 +68,7 @@ void launch_grid_setup(const StepArgs &a, cudaStream_t s);
 void launch_cell_build(const StepArgs &a, cudaStream_t s);
 void launch_ghosts(const StepArgs &a, cudaStream_t s);
 void launch_search(const StepArgs &a, cudaStream_t s);
-size_t search_smem_bytes(const StepArgs &a);
+void launch_reorder(const StepArgs &a, cudaStream_t s);
 
 // reduce.cu
 void launch_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks);
@@ -63,11 +77,23 @@ void launch_energy_bbox_reduce(const StepArgs &a, cudaStream_t s, int nblocks, i
 void launch_set_time(const StepArgs &a, cudaStream_t s, double dt, double dtold, int set_dtold);
 void launch_finish_step(const StepArgs &a, cudaStream_t s);
 
+// step_mixed.cu: the mixed-precision path and the FP64 <-> FP32 state copies
+namespace mixed {
+void launch_strain_prep(const StepArgs &a, cudaStream_t s);
+void launch_strain(const StepArgs &a, cudaStream_t s);
+int launch_constitutive(const StepArgs &a, cudaStream_t s);
+void launch_mom_prep(const StepArgs &a, cudaStream_t s);
+int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);
+void launch_to_f32(const StepArgs &a, cudaStream_t s);
+void launch_to_f64(const StepArgs &a, cudaStream_t s);
+}  // namespace mixed
+
 // step kernels (one namespace per arithmetic flavour)
 #define MCM_DECLARE_STEP(NS)                                                        \
     namespace NS {                                                                  \
     void launch_strain_prep(const StepArgs &a, cudaStream_t s);                     \
-    int launch_strain_constitutive(const StepArgs &a, cudaStream_t s);              \
+    void launch_strain(const StepArgs &a, cudaStream_t s);                          \
+    int launch_constitutive(const StepArgs &a, cudaStream_t s);                     \
     void launch_mom_prep(const StepArgs &a, cudaStream_t s);                        \
     int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);          \
     int launch_update_move(const StepArgs &a, cudaStream_t s);                      \

@@ -1,0 +1,427 @@
+// step_coop.cuh -- cooperative gather kernels for the FP64 fast path.
+//
+// L lanes (a sub-warp) work on one particle: they first expand its one-byte
+// neighbour list (see nbr_iter.cuh) into absolute cell-order positions in
+// shared memory, then each lane takes every L-th neighbour, so L independent
+// record loads are in flight per particle, and the partial sums are combined
+// with shuffle reductions (no atomics).  The summation order differs from the
+// reference's sequential order; the FP64-exact path keeps that order.
+#pragma once
+#include "nbr_iter.cuh"
+#include "physics.cuh"
+
+namespace mcm {
+namespace MCM_FLAVOUR_NS {
+
+// Expands the real-neighbour list of position t into spos[0..n); returns n
+// (same-material rows, then contact rows; the self entry of disctype 1 and
+// the ghosts are not included).
+template <int L>
+__device__ __forceinline__ int coop_expand(const StepArgs &a, const DevGrid &g, int t, int lane, int *spos) {
+    const int key = a.ckey[t];
+    if (key < 0) return 0;
+    const int np = a.npad;
+    int bx, by, bz;
+    cell_coords(key, g.gridlim, bx, by, bz);
+    const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
+    const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
+    const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
+    int base = 0;
+    const int passes = a.nmat > 1 ? 2 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+        const unsigned long long hdr = a.nhdr[(size_t)pass * np + t];
+        int r = 0;
+        for (int nz = lo2; nz <= hi2; ++nz) {
+            for (int my = lo1; my <= hi1; ++my, ++r) {
+                const int cnt = (int)((hdr >> (7 * r)) & 127ull);
+                if (cnt == 0) continue;
+                const int rs = a.cell_start[(int)cell_key(lo0, my, nz, g.gridlim)];
+                for (int c = lane; c < cnt; c += L) {
+                    const int k = base + c;
+                    const unsigned int w = a.nlist[(size_t)(k >> 2) * np + t];
+                    spos[k] = rs + (int)((w >> (8 * (k & 3))) & 255u);
+                }
+                base += cnt;
+            }
+        }
+    }
+    return base;
+}
+
+template <int L>
+__device__ __forceinline__ double sub_sum(double v) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, L);
+    return v;
+}
+
+// Cubic B-spline gradient with the reciprocal of havg supplied (FP64).
+__device__ __forceinline__ void gradw_ih(double x0, double x1, double x2, double ih, double &d0, double &d1,
+                                         double &d2) {
+    const double r2 = fma(x0, x0, fma(x1, x1, x2 * x2));
+    if (r2 == 0.0) { d0 = d1 = d2 = 0.0; return; }
+    const double rinv = rsqrt(r2);
+    const double rad = r2 * rinv;
+    const double z = rad * ih;
+    const double const1 = (1.0 / kPi) * ih * ih * ih;
+    double dw;
+    if (z < 1.0) dw = const1 * ((2.25 * z - 3.0) * z);
+    else if (z < 2.0) { const double tt = 2.0 - z; dw = -0.75 * const1 * (tt * tt); }
+    else dw = 0.0;
+    const double f = dw * ih * rinv;
+    d0 = f * x0; d1 = f * x1; d2 = f * x2;
+}
+
+__device__ __forceinline__ double kernelw_ih(double x0, double x1, double x2, double ih) {
+    const double rad = sqrt(fma(x0, x0, fma(x1, x1, x2 * x2)));
+    const double z = rad * ih;
+    const double const1 = (1.0 / kPi) * ih * ih * ih;
+    if (z < 1.0) return const1 * (((0.75 * z - 1.5) * z) * z + 1.0);
+    if (z < 2.0) { const double tt = 2.0 - z; return 0.25 * const1 * (tt * tt * tt); }
+    return 0.0;
+}
+
+// 1/havg with havg = (h_i + h_j)/2; h_i == h_j in all constant-h runs.
+__device__ __forceinline__ double inv_havg(double hi, double hj, double ihi) {
+    return (hi == hj) ? ihi : 1.0 / (0.5 * (hi + hj));
+}
+
+// Visits entry k of position t's full list: real (positions from spos), self
+// (disctype 1), ghosts.  Returns false past the end.
+struct Entry {
+    int kind;   // 0 real position, 1 ghost index
+    int idx;
+    bool self;
+};
+__device__ __forceinline__ Entry entry_at(const StepArgs &a, int t, int k, int nreal, int self, const int *spos) {
+    Entry e;
+    if (k < nreal) { e.kind = 0; e.idx = spos[k]; e.self = false; }
+    else if (k < nreal + self) { e.kind = 0; e.idx = t; e.self = true; }
+    else { e.kind = 1; e.idx = a.gnbr[(size_t)(k - nreal - self) * a.npad + t]; e.self = false; }
+    return e;
+}
+
+template <int L>
+size_t coop_smem(const StepArgs &a, int threads) { return sizeof(int) * (size_t)(threads / L) * (a.nwords * 4); }
+
+// ----------------------------------------------------------- strain rate
+template <int L, int DISC>
+__global__ void __launch_bounds__(256) k_strain_coop(StepArgs a) {
+    extern __shared__ int smem[];
+    if (skip_step(a)) return;
+    const int sub = threadIdx.x / L, lane = threadIdx.x % L;
+    const int per = blockDim.x / L;
+    const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
+    int *spos = smem + sub * (a.nwords * 4);
+    const DevGrid g = *a.grid;
+    for (int round = 0; round < rounds; ++round) {
+    const int t = (round * gridDim.x + blockIdx.x) * per + sub;
+    const bool live = t < a.n;
+    int nreal = 0, gn = 0;
+    double4 xi = make_double4(0, 0, 0, 1), vi = make_double4(0, 0, 0, 0);
+    if (live) {
+        nreal = coop_expand<L>(a, g, t, lane, spos);
+        gn = a.gnnbr[t];
+        xi = a.rec0[t];
+        vi = a.rec1[t];
+    }
+    __syncwarp();
+    const int self = (a.prm.disctype == 1) ? 1 : 0;
+    const int total = live ? nreal + self + gn : 0;
+    const double ihi = 1.0 / xi.w;
+    double gv[9];
+#pragma unroll
+    for (int u = 0; u < 9; ++u) gv[u] = 0.0;
+    if (DISC == 0) {
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 vj = e.kind ? a.grec1[e.idx] : a.rec1[e.idx];
+            double d[3];
+            gradw_ih(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, inv_havg(xi.w, xj.w, ihi), d[0], d[1], d[2]);
+            const double dv[3] = {vj.w * (vj.x - vi.x), vj.w * (vj.y - vi.y), vj.w * (vj.z - vi.z)};
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) gv[3 * n + m] = fma(dv[n], d[m], gv[3 * n + m]);
+        }
+    } else {
+        // MCM/mcm_corr_strain.f90:51-134
+        double sw = 0.0, sg0 = 0.0, sg1 = 0.0, sg2 = 0.0;
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double Volj = e.kind ? a.grec1[e.idx].w : a.rec1[e.idx].w;
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            sw = fma(Volj, kernelw_ih(dx, dy, dz, ih), sw);
+            sg0 = fma(Volj, d[0], sg0); sg1 = fma(Volj, d[1], sg1); sg2 = fma(Volj, d[2], sg2);
+        }
+        sw = sub_sum<L>(sw); sg0 = sub_sum<L>(sg0); sg1 = sub_sum<L>(sg1); sg2 = sub_sum<L>(sg2);
+        const double isw2 = 1.0 / (sw * sw);
+        double B[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) B[u] = 0.0;
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double Volj = e.kind ? a.grec1[e.idx].w : a.rec1[e.idx].w;
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            const double w = kernelw_ih(dx, dy, dz, ih);
+            const double cg[3] = {(d[0] * sw - w * sg0) * isw2, (d[1] * sw - w * sg1) * isw2,
+                                  (d[2] * sw - w * sg2) * isw2};
+            const double xr[3] = {Volj * (xj.x - xi.x), Volj * (xj.y - xi.y), Volj * (xj.z - xi.z)};
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) B[3 * n + m] = fma(xr[n], cg[m], B[3 * n + m]);
+        }
+        double Bm[3][3], invB[3][3];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) Bm[u / 3][u % 3] = sub_sum<L>(B[u]);
+        inverse3(Bm, invB);
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 vj = e.kind ? a.grec1[e.idx] : a.rec1[e.idx];
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            const double w = kernelw_ih(dx, dy, dz, ih);
+            const double cg[3] = {(d[0] * sw - w * sg0) * isw2, (d[1] * sw - w * sg1) * isw2,
+                                  (d[2] * sw - w * sg2) * isw2};
+            double c2[3];
+#pragma unroll
+            for (int n = 0; n < 3; ++n) c2[n] = invB[n][0] * cg[0] + invB[n][1] * cg[1] + invB[n][2] * cg[2];
+            const double vv[3] = {vj.w * vj.x, vj.w * vj.y, vj.w * vj.z};
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) gv[3 * n + m] = fma(vv[n], c2[m], gv[3 * n + m]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 9; ++u) gv[u] = sub_sum<L>(gv[u]);
+    if (live && lane == 0) {
+        const int i = a.cell_list[t];
+        double *const *f = a.F.f;
+        const double r11 = gv[0], r22 = gv[4], r33 = gv[8];
+        f[FR11][i] = r11;
+        f[FR22][i] = r22;
+        f[FR33][i] = r33;
+        f[FR12][i] = 0.5 * (gv[1] + gv[3]);
+        f[FR13][i] = 0.5 * (gv[2] + gv[6]);
+        f[FR23][i] = 0.5 * (gv[5] + gv[7]);
+        f[FW12][i] = 0.5 * (gv[1] - gv[3]);
+        f[FW13][i] = 0.5 * (gv[2] - gv[6]);
+        f[FW23][i] = 0.5 * (gv[5] - gv[7]);
+        f[FTR][i] = r11 + r22 + r33;
+    }
+    __syncwarp();
+    }
+}
+
+// ------------------------------------------------- momentum + integration
+template <int L, int DISC>
+__global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate) {
+    extern __shared__ int smem[];
+    __shared__ double sm[32];
+    if (skip_step(a)) return;
+    const int sub = threadIdx.x / L, lane = threadIdx.x % L;
+    const int per = blockDim.x / L;
+    const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
+    int *spos = smem + sub * (a.nwords * 4);
+    const DevGrid g = *a.grid;
+    const int nm = a.nmat;
+    double ke_m[kMaxMat], ie_m[kMaxMat], mo_m[kMaxMat][3];
+    // per-material sums kept for up to 4 materials in registers, the rest folded below
+    double e_acc[4][5];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) e_acc[m][c] = 0.0;
+    (void)ke_m; (void)ie_m; (void)mo_m;
+    double x[3] = {1.0e20, 1.0e20, 1.0e20};
+    double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
+    const bool do_int = integrate && !a.time->ended;
+    for (int round = 0; round < rounds; ++round) {
+    const int t = (round * gridDim.x + blockIdx.x) * per + sub;
+    const bool live = t < a.n;
+    int nreal = 0, gn = 0;
+    double4 xi = make_double4(0, 0, 0, 1), r1i = make_double4(0, 0, 0, 0), r2i = make_double4(0, 0, 0, 1);
+    if (live) {
+        nreal = coop_expand<L>(a, g, t, lane, spos);
+        gn = a.gnnbr[t];
+        xi = a.rec0[t];
+        r1i = a.rec1[t];
+        r2i = a.rec2[t];
+    }
+    __syncwarp();
+    const int self = (a.prm.disctype == 1) ? 1 : 0;
+    const int total = live ? nreal + self + gn : 0;
+    const double ihi = 1.0 / xi.w;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (DISC == 0) {
+        // MCM/mcm_oldacceleration.f90:66-89
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 r1 = e.kind ? a.grec1[e.idx] : a.rec1[e.idx];
+            const double4 r2 = e.kind ? a.grec2[e.idx] : a.rec2[e.idx];
+            double d[3];
+            gradw_ih(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, inv_havg(xi.w, xj.w, ihi), d[0], d[1], d[2]);
+            const double s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
+            const double s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
+            const double mj = r2.z;
+            acc[0] = fma(mj, s11 * d[0] + s12 * d[1] + s13 * d[2], acc[0]);
+            acc[1] = fma(mj, s12 * d[0] + s22 * d[1] + s23 * d[2], acc[1]);
+            acc[2] = fma(mj, s13 * d[0] + s23 * d[1] + s33 * d[2], acc[2]);
+        }
+    } else {
+        // MCM/mcm_corr_acceleration.f90:63-161
+        double sw = 0.0, sg0 = 0.0, sg1 = 0.0, sg2 = 0.0;
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 r2 = e.kind ? a.grec2[e.idx] : a.rec2[e.idx];
+            const double Volj = r2.z / r2.w;
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            sw = fma(Volj, kernelw_ih(dx, dy, dz, ih), sw);
+            sg0 = fma(Volj, d[0], sg0); sg1 = fma(Volj, d[1], sg1); sg2 = fma(Volj, d[2], sg2);
+        }
+        sw = sub_sum<L>(sw); sg0 = sub_sum<L>(sg0); sg1 = sub_sum<L>(sg1); sg2 = sub_sum<L>(sg2);
+        const double isw2 = 1.0 / (sw * sw);
+        double B[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) B[u] = 0.0;
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 r2 = e.kind ? a.grec2[e.idx] : a.rec2[e.idx];
+            const double Volj = r2.z / r2.w;
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            const double w = kernelw_ih(dx, dy, dz, ih);
+            const double cg[3] = {(d[0] * sw - w * sg0) * isw2, (d[1] * sw - w * sg1) * isw2,
+                                  (d[2] * sw - w * sg2) * isw2};
+            const double xr[3] = {Volj * dx, Volj * dy, Volj * dz};
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) B[3 * n + m] = fma(xr[n], cg[m], B[3 * n + m]);
+        }
+        double Bm[3][3], invB[3][3];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) Bm[u / 3][u % 3] = sub_sum<L>(B[u]);
+        inverse3(Bm, invB);
+        double ds[18];
+#pragma unroll
+        for (int u = 0; u < 18; ++u) ds[u] = 0.0;
+        for (int k = lane; k < total; k += L) {
+            const Entry e = entry_at(a, t, k, nreal, self, spos);
+            const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
+            const double4 r1 = e.kind ? a.grec1[e.idx] : a.rec1[e.idx];
+            const double4 r2 = e.kind ? a.grec2[e.idx] : a.rec2[e.idx];
+            const double ih = inv_havg(xi.w, xj.w, ihi);
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            double d[3];
+            gradw_ih(dx, dy, dz, ih, d[0], d[1], d[2]);
+            const double w = kernelw_ih(dx, dy, dz, ih);
+            const double cg[3] = {(d[0] * sw - w * sg0) * isw2, (d[1] * sw - w * sg1) * isw2,
+                                  (d[2] * sw - w * sg2) * isw2};
+            const double zs = e.self ? 0.0 : 1.0;
+            const double dsg[6] = {zs * (r1.x + r1i.x), zs * (r1.y + r1i.y), zs * (r1.z + r1i.z),
+                                   zs * (r1.w + r1i.w), zs * (r2.x + r2i.x), zs * (r2.y + r2i.y)};
+#pragma unroll
+            for (int u = 0; u < 6; ++u)
+#pragma unroll
+                for (int l = 0; l < 3; ++l) ds[3 * u + l] = fma(dsg[u], cg[l], ds[3 * u + l]);
+        }
+#pragma unroll
+        for (int u = 0; u < 18; ++u) ds[u] = sub_sum<L>(ds[u]);
+        // the mass of the last neighbour of the reference order: the last ghost, else self
+        double massj = r2i.z;
+        if (live && gn > 0) massj = a.grec2[a.gnbr[(size_t)(gn - 1) * a.npad + t]].z;
+        else if (live && !self && nreal > 0) massj = a.rec2[spos[nreal - 1]].z;
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int l = 0; l < 3; ++l) acc[n] = fma(massj * ds[3 * sym_index(n, m) + l], invB[l][m], acc[n]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[c] = sub_sum<L>(acc[c]);
+    // per-particle tail on lane 0 of each sub-warp
+    if (live && lane == 0) {
+        const int i = a.cell_list[t];
+        double *const *f = a.F.f;
+        if (a.prm.baseaccel)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[j] = acc[j] + a.prm.base_a[j];
+        switch (a.F.dispbc[i]) {
+            case 1: acc[0] = 0.0; break;
+            case 2: acc[1] = 0.0; break;
+            case 3: acc[2] = 0.0; break;
+            case 4: acc[0] = 0.0; acc[1] = 0.0; break;
+            case 5: acc[1] = 0.0; acc[2] = 0.0; break;
+            case 6: acc[0] = 0.0; acc[2] = 0.0; break;
+            case 7: acc[0] = 0.0; acc[1] = 0.0; acc[2] = 0.0; break;
+            default: break;
+        }
+        if (a.split_mode || a.prm.diag) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
+        const int mati = a.F.mat[i];
+        const double mass = f[FMASS][i], vabs = f[FVABS][i];
+        const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),
+                                mass * fabs(f[FVY][i]), mass * fabs(f[FVZ][i])};
+        if (mati <= 4) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                if (mati == m + 1)
+#pragma unroll
+                    for (int c = 0; c < 5; ++c) e_acc[m][c] += vals[c];
+        } else {
+            // materials 5..16: rare; accumulated straight into this block's partials
+            for (int c = 0; c < 5; ++c) atomicAdd(&a.red[(size_t)blockIdx.x * (5 * nm + 6) + 5 * (mati - 1) + c], vals[c]);
+        }
+        if (do_int) {
+            double xn[3];
+            integrate_particle(a, i, acc, a.time->dt, a.time->dtold, xn);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { x[d] = fmin(x[d], xn[d]); xmax[d] = fmax(xmax[d], xn[d]); }
+        }
+    }
+    __syncwarp();
+    }
+    const int stride = 5 * nm + 6;
+    double *out = a.red + (size_t)blockIdx.x * stride;
+    for (int m = 1; m <= nm && m <= 4; ++m) {
+        double v[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[c] = block_sum(e_acc[m - 1][c], sm);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int c = 0; c < 5; ++c) out[5 * (m - 1) + c] = v[c];
+    }
+    if (do_int) {
+        for (int d = 0; d < 3; ++d) {
+            double lo = block_minmax(x[d], sm, false);
+            double hi = block_minmax(xmax[d], sm, true);
+            if (threadIdx.x == 0) { out[5 * nm + d] = lo; out[5 * nm + 3 + d] = hi; }
+        }
+    }
+}
+
+}  // namespace MCM_FLAVOUR_NS
+}  // namespace mcm

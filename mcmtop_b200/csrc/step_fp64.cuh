@@ -10,7 +10,7 @@
 // neighbours in the reference order; the sums are sequential, so there are no
 // atomics and the FP64-exact flavour accumulates in the reference's order.
 #pragma once
-#include "kernels.h"
+#include "nbr_iter.cuh"
 #include "physics.cuh"
 
 #ifndef MCM_FLAVOUR_NS
@@ -157,9 +157,8 @@ __device__ __forceinline__ void store_state(const StepArgs &a, int i, const PSta
         for (int t = 0; t < 6; ++t) f[FA11 + t][i] = P.alfa[t];
     }
     if (a.prm.diag) {
-#pragma unroll
-        for (int t = 0; t < 6; ++t) f[FR11 + t][i] = P.rod[t];
-        f[FW12][i] = P.spin[0]; f[FW13][i] = P.spin[1]; f[FW23][i] = P.spin[2];
+        // rhoupd may have changed rod and the trace (MCM/mcm_rhoupd.f90:130-151)
+        f[FR11][i] = P.rod[T11]; f[FR22][i] = P.rod[T22]; f[FR33][i] = P.rod[T33];
         f[FTR][i] = P.tracerod; f[FETRY][i] = P.etry; f[FEINC][i] = P.einc; f[FRHOOLD][i] = P.rhoold;
     }
 }
@@ -172,13 +171,14 @@ __global__ void k_strain_prep(StepArgs a) {
     if (skip_step(a)) return;
     const double dt = a.time->dt;
     const double *const *f = a.F.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
         double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
         double x = f[FX][i] - 0.5 * vx * dt;
         double y = f[FY][i] - 0.5 * vy * dt;
         double z = f[FZ][i] - 0.5 * vz * dt;
-        a.rec0[i] = make_double4(x, y, z, f[FH][i]);
-        a.rec1[i] = make_double4(vx, vy, vz, f[FMASS][i] / f[FRHO][i]);
+        a.rec0[p] = make_double4(x, y, z, f[FH][i]);
+        a.rec1[p] = make_double4(vx, vy, vz, f[FMASS][i] / f[FRHO][i]);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -190,16 +190,11 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 template <int DISC>
-__device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const double4 xi, const double4 vi,
-                                              double gv[3][3]) {
-    const int nn = a.nnbr[i], gn = a.gnnbr[i];
-    const int np = a.npad;
+__device__ __forceinline__ void strain_gather(const StepArgs &a, const DevGrid &g, int t, const double4 xi,
+                                              const double4 vi, double gv[3][3]) {
     if (DISC == 0) {
         // MCM/mcm_oldstrain.f90:95-115
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, vj;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+        auto body = [&](const double4 xj, const double4 vj) {
             double Volj = vj.w;
             double havg = 0.5 * (xi.w + xj.w);
             double d[3];
@@ -207,18 +202,17 @@ __device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const do
             const double dv[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
-                double t = Volj * dv[n];
+                double tt = Volj * dv[n];
 #pragma unroll
-                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + t * d[m];
+                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + tt * d[m];
             }
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { body(a.rec0[p], a.rec1[p]); }, [&](int q) { body(a.grec0[q], a.grec1[q]); });
     } else {
         // MCM/mcm_corr_strain.f90:51-134 (three passes, kernel centred at i)
         double sum_w = 0.0, sg[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, vj;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+        auto pass1 = [&](const double4 xj, const double4 vj) {
             double Volj = vj.w;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -228,13 +222,12 @@ __device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const do
             sum_w = sum_w + Volj * w;
 #pragma unroll
             for (int l = 0; l < 3; ++l) sg[l] = sg[l] + Volj * d[l];
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { pass1(a.rec0[p], a.rec1[p]); }, [&](int q) { pass1(a.grec0[q], a.grec1[q]); });
         double B[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         const double sw2 = sum_w * sum_w;
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, vj;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+        auto pass2 = [&](const double4 xj, const double4 vj) {
             double Volj = vj.w;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -249,13 +242,12 @@ __device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const do
             for (int m = 0; m < 3; ++m)
 #pragma unroll
                 for (int n = 0; n < 3; ++n) B[n][m] = B[n][m] + Volj * xr[n] * cg[m];
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { pass2(a.rec0[p], a.rec1[p]); }, [&](int q) { pass2(a.grec0[q], a.grec1[q]); });
         double invB[3][3];
         inverse3(B, invB);
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, vj;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; vj = a.rec1[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; vj = a.grec1[q]; }
+        auto pass3 = [&](const double4 xj, const double4 vj) {
             double Volj = vj.w;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -271,11 +263,13 @@ __device__ __forceinline__ void strain_gather(const StepArgs &a, int i, const do
             const double vv[3] = {vj.x, vj.y, vj.z};
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
-                double t = Volj * vv[n];
+                double tt = Volj * vv[n];
 #pragma unroll
-                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + t * c2[m];
+                for (int m = 0; m < 3; ++m) gv[n][m] = gv[n][m] + tt * c2[m];
             }
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { pass3(a.rec0[p], a.rec1[p]); }, [&](int q) { pass3(a.grec0[q], a.grec1[q]); });
     }
 }
 
@@ -291,11 +285,42 @@ __device__ __forceinline__ double block_min(double v, double *sm) {
     return v;
 }
 
-// --------------------------------------------- strain + constitutive update
-// MCM/mcm_strain.f90, mcm_oldstrain.f90 / mcm_corr_strain.f90, mcm_rhoupd.f90,
-// mcm_constitutive.f90:29-83 and mcm_calccritts.f90 for one particle.
+// ------------------------------------------------------------ strain rate
+// MCM/mcm_oldstrain.f90 / mcm_corr_strain.f90 for the particle at position t:
+// rod, spin and trace go to the state's diagnostic arrays, which the
+// constitutive kernel reads (this keeps the gather kernel small enough to
+// keep many warps resident).
 template <int DISC>
-__global__ void __launch_bounds__(kRedThreads) k_strain_const(StepArgs a) {
+__global__ void __launch_bounds__(kRedThreads) k_strain(StepArgs a) {
+    if (skip_step(a)) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int i = a.cell_list[t];
+    const DevGrid g = *a.grid;
+    const double4 xi = a.rec0[t], vi = a.rec1[t];
+    double gv[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    strain_gather<DISC>(a, g, t, xi, vi, gv);
+    double *const *f = a.F.f;
+    const double r11 = 0.5 * (gv[0][0] + gv[0][0]);
+    const double r22 = 0.5 * (gv[1][1] + gv[1][1]);
+    const double r33 = 0.5 * (gv[2][2] + gv[2][2]);
+    f[FR11][i] = r11;
+    f[FR22][i] = r22;
+    f[FR33][i] = r33;
+    f[FR12][i] = 0.5 * (gv[0][1] + gv[1][0]);
+    f[FR13][i] = 0.5 * (gv[0][2] + gv[2][0]);
+    f[FR23][i] = 0.5 * (gv[1][2] + gv[2][1]);
+    f[FW12][i] = 0.5 * (gv[0][1] - gv[1][0]);
+    f[FW13][i] = 0.5 * (gv[0][2] - gv[2][0]);
+    f[FW23][i] = 0.5 * (gv[1][2] - gv[2][1]);
+    f[FTR][i] = r11 + r22 + r33;
+}
+
+// ---------------------------------------------------- constitutive update
+// MCM/mcm_rhoupd.f90, mcm_constitutive.f90:29-83 and mcm_calccritts.f90 for
+// the particle with state index i, and the forward half-step shift of
+// MCM/mcm_strain.f90:56-60 (x - v dt/2 recomputed exactly as k_strain_prep).
+__global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
     __shared__ double sm[32];
     if (skip_step(a)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,33 +328,29 @@ __global__ void __launch_bounds__(kRedThreads) k_strain_const(StepArgs a) {
     double crit = 1.0e20;
     bool bad = false;
     if (i < a.n) {
-        const double4 xi = a.rec0[i], vi = a.rec1[i];
-        double gv[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        strain_gather<DISC>(a, i, xi, vi, gv);
-        PState<double> P;
+        double *const *f = a.F.f;
         const DevMaterial &M = a.mats[a.F.mat[i] - 1];
+        PState<double> P;
         load_state(a, i, P, M.model);
-        P.rod[T11] = 0.5 * (gv[0][0] + gv[0][0]);
-        P.rod[T22] = 0.5 * (gv[1][1] + gv[1][1]);
-        P.rod[T33] = 0.5 * (gv[2][2] + gv[2][2]);
-        P.rod[T12] = 0.5 * (gv[0][1] + gv[1][0]);
-        P.rod[T13] = 0.5 * (gv[0][2] + gv[2][0]);
-        P.rod[T23] = 0.5 * (gv[1][2] + gv[2][1]);
-        P.spin[0] = 0.5 * (gv[0][1] - gv[1][0]);
-        P.spin[1] = 0.5 * (gv[0][2] - gv[2][0]);
-        P.spin[2] = 0.5 * (gv[1][2] - gv[2][1]);
-        P.tracerod = P.rod[T11] + P.rod[T22] + P.rod[T33];
+#pragma unroll
+        for (int u = 0; u < 6; ++u) P.rod[u] = f[FR11 + u][i];
+        P.spin[0] = f[FW12][i];
+        P.spin[1] = f[FW13][i];
+        P.spin[2] = f[FW23][i];
+        P.tracerod = f[FTR][i];
         rhoupd(P, M, dt, 3);
         bad = !constitutive_particle(P, M, dt);
-        const double vx = a.F.f[FVX][i], vy = a.F.f[FVY][i], vz = a.F.f[FVZ][i];
-        const double mindist = (a.prm.tcrit_opt == 2) ? a.F.f[FMINDIST][i] : 0.0;
-        crit = critts_particle(P, M, a.prm.tcrit_opt, 3, a.F.f[FVABS][i], mindist);
+        const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
+        const double mindist = (a.prm.tcrit_opt == 2) ? f[FMINDIST][i] : 0.0;
+        crit = critts_particle(P, M, a.prm.tcrit_opt, 3, f[FVABS][i], mindist);
         store_state(a, i, P, M.model);
-        if (a.prm.diag) a.F.f[FCRITTS][i] = crit;
-        // MCM/mcm_strain.f90:56-60: positions forward again
-        a.F.f[FX][i] = xi.x + 0.5 * vx * dt;
-        a.F.f[FY][i] = xi.y + 0.5 * vy * dt;
-        a.F.f[FZ][i] = xi.z + 0.5 * vz * dt;
+        if (a.prm.diag) f[FCRITTS][i] = crit;
+        const double xs = f[FX][i] - 0.5 * vx * dt;
+        const double ys = f[FY][i] - 0.5 * vy * dt;
+        const double zs = f[FZ][i] - 0.5 * vz * dt;
+        f[FX][i] = xs + 0.5 * vx * dt;
+        f[FY][i] = ys + 0.5 * vy * dt;
+        f[FZ][i] = zs + 0.5 * vz * dt;
     }
     if (bad) raise_status(a.status, MCM_ECOMPLEX_C, i);
     double m = block_min(crit, sm);
@@ -343,14 +364,15 @@ __global__ void __launch_bounds__(kRedThreads) k_strain_const(StepArgs a) {
 __global__ void k_mom_prep(StepArgs a) {
     if (skip_step(a)) return;
     const double *const *f = a.F.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
         double rho = f[FRHO][i];
         double r2 = rho * rho;
         double q = f[FQ][i];
-        a.rec0[i] = make_double4(f[FX][i], f[FY][i], f[FZ][i], f[FH][i]);
-        a.rec1[i] = make_double4((f[FS11][i] - q) / r2, (f[FS22][i] - q) / r2, (f[FS33][i] - q) / r2,
+        a.rec0[p] = make_double4(f[FX][i], f[FY][i], f[FZ][i], f[FH][i]);
+        a.rec1[p] = make_double4((f[FS11][i] - q) / r2, (f[FS22][i] - q) / r2, (f[FS33][i] - q) / r2,
                                  (f[FS12][i] - 0.0) / r2);
-        a.rec2[i] = make_double4((f[FS13][i] - 0.0) / r2, (f[FS23][i] - 0.0) / r2, f[FMASS][i], 0.0);
+        a.rec2[p] = make_double4((f[FS13][i] - 0.0) / r2, (f[FS23][i] - 0.0) / r2, f[FMASS][i], rho);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -362,7 +384,7 @@ __global__ void k_mom_prep(StepArgs a) {
             a.grec0[g] = make_double4(a.gx[g], a.gy[g], a.gz[g], a.gh[g]);
             a.grec1[g] = make_double4((f[FS11][j] - q) / r2, (f[FS22][j] - q) / r2, (f[FS33][j] - q) / r2,
                                       ((-f[FS12][j]) - (-0.0)) / r2);
-            a.grec2[g] = make_double4(((-f[FS13][j]) - (-0.0)) / r2, ((-f[FS23][j]) - (-0.0)) / r2, a.gmass[g], 0.0);
+            a.grec2[g] = make_double4(((-f[FS13][j]) - (-0.0)) / r2, ((-f[FS23][j]) - (-0.0)) / r2, a.gmass[g], rho);
         }
     }
 }
@@ -375,18 +397,13 @@ __device__ __forceinline__ void sym_from_rec(const double4 &r1, const double4 &r
 }
 
 template <int DISC>
-__device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double acc[3]) {
-    const int nn = a.nnbr[i], gn = a.gnnbr[i];
-    const int np = a.npad;
-    const double4 xi = a.rec0[i];
+__device__ __forceinline__ void momentum_gather(const StepArgs &a, const DevGrid &g, int t, double acc[3]) {
+    const double4 xi = a.rec0[t];
     double Ai[3][3];
-    sym_from_rec(a.rec1[i], a.rec2[i], Ai);
+    sym_from_rec(a.rec1[t], a.rec2[t], Ai);
     if (DISC == 0) {
         // MCM/mcm_oldacceleration.f90:66-89
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, r1, r2;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r1 = a.rec1[j]; r2 = a.rec2[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r1 = a.grec1[q]; r2 = a.grec2[q]; }
+        auto body = [&](const double4 xj, const double4 r1, const double4 r2) {
             double havg = 0.5 * (xi.w + xj.w);
             double d[3];
             gradw(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, havg, d[0], d[1], d[2]);
@@ -400,20 +417,18 @@ __device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double
                 for (int m = 0; m < 3; ++m) ds = ds + (Aj[m][n] + Ai[m][n]) * d[m];
                 acc[n] = acc[n] + massj * ds;
             }
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { body(a.rec0[p], a.rec1[p], a.rec2[p]); },
+            [&](int q) { body(a.grec0[q], a.grec1[q], a.grec2[q]); });
     } else {
         // MCM/mcm_corr_acceleration.f90:63-161 (kernel centred at j; the self
         // slot k = nnbr is zeroed; the final sum uses the last neighbour's mass)
         double sum_w = 0.0, sg[3] = {0.0, 0.0, 0.0};
         double massj = 0.0;
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, r2;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r2 = a.rec2[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r2 = a.grec2[q]; }
-            // V_j = m_j/rho_j with the current density: rebuilt from the record
+        auto pass1 = [&](const double4 xj, const double4 r2) {
             massj = r2.z;
-            double rhoj = (k < nn) ? a.F.f[FRHO][a.nbr[(size_t)k * np + i]] : a.grho[a.gnbr[(size_t)(k - nn) * np + i]];
-            double Volj = massj / rhoj;
+            double Volj = massj / r2.w;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             double w = kernelw(dx, dy, dz, havg);
@@ -422,15 +437,14 @@ __device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double
             sum_w = sum_w + Volj * w;
 #pragma unroll
             for (int l = 0; l < 3; ++l) sg[l] = sg[l] + Volj * d[l];
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { pass1(a.rec0[p], a.rec2[p]); }, [&](int q) { pass1(a.grec0[q], a.grec2[q]); });
         double B[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         const double sw2 = sum_w * sum_w;
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, r2;
-            double rhoj;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r2 = a.rec2[j]; rhoj = a.F.f[FRHO][j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r2 = a.grec2[q]; rhoj = a.grho[q]; }
-            double Volj = r2.z / rhoj;
+        auto pass2 = [&](const double4 xj, const double4 r2) {
+            massj = r2.z;
+            double Volj = massj / r2.w;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             double w = kernelw(dx, dy, dz, havg);
@@ -444,17 +458,17 @@ __device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double
             for (int m = 0; m < 3; ++m)
 #pragma unroll
                 for (int n = 0; n < 3; ++n) B[n][m] = B[n][m] + Volj * xr[n] * cg[m];
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool) { pass2(a.rec0[p], a.rec2[p]); }, [&](int q) { pass2(a.grec0[q], a.grec2[q]); });
         double invB[3][3];
         inverse3(B, invB);
         // deltasig(m,n,l) is symmetric in (m,n): keep 6 x 3 accumulators
         double ds[6][3];
 #pragma unroll
-        for (int t = 0; t < 6; ++t) ds[t][0] = ds[t][1] = ds[t][2] = 0.0;
-        for (int k = 0; k < nn + gn; ++k) {
-            double4 xj, r1, r2;
-            if (k < nn) { int j = a.nbr[(size_t)k * np + i]; xj = a.rec0[j]; r1 = a.rec1[j]; r2 = a.rec2[j]; }
-            else { int q = a.gnbr[(size_t)(k - nn) * np + i]; xj = a.grec0[q]; r1 = a.grec1[q]; r2 = a.grec2[q]; }
+        for (int u = 0; u < 6; ++u) ds[u][0] = ds[u][1] = ds[u][2] = 0.0;
+        auto pass3 = [&](const double4 xj, const double4 r1, const double4 r2, bool self_slot) {
+            massj = r2.z;
             double havg = 0.5 * (xi.w + xj.w);
             double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             double w = kernelw(dx, dy, dz, havg);
@@ -465,17 +479,19 @@ __device__ __forceinline__ void momentum_gather(const StepArgs &a, int i, double
             for (int m = 0; m < 3; ++m) cg[m] = (d[m] * sum_w - w * sg[m]) / sw2;
             double Aj[3][3];
             sym_from_rec(r1, r2, Aj);
-            const bool self_slot = (k == nn - 1);
 #pragma unroll
-            for (int t = 0; t < 6; ++t) {
-                const int m = (t < 3) ? t : (t == 5 ? 1 : 0);
-                const int n = (t < 3) ? t : (t == 3 ? 1 : 2);
+            for (int u = 0; u < 6; ++u) {
+                const int m = (u < 3) ? u : (u == 5 ? 1 : 0);
+                const int n = (u < 3) ? u : (u == 3 ? 1 : 2);
                 double dsig = Aj[m][n] + Ai[m][n];
                 if (self_slot) dsig = 0.0;
 #pragma unroll
-                for (int l = 0; l < 3; ++l) ds[t][l] = ds[t][l] + dsig * cg[l];
+                for (int l = 0; l < 3; ++l) ds[u][l] = ds[u][l] + dsig * cg[l];
             }
-        }
+        };
+        for_each_neighbour(
+            a, g, t, [&](int p, bool self) { pass3(a.rec0[p], a.rec1[p], a.rec2[p], self); },
+            [&](int q) { pass3(a.grec0[q], a.grec1[q], a.grec2[q], false); });
 #pragma unroll
         for (int n = 0; n < 3; ++n)
 #pragma unroll
@@ -559,7 +575,7 @@ template <int DISC>
 __global__ void __launch_bounds__(kRedThreads) k_momentum(StepArgs a, int integrate) {
     __shared__ double sm[32];
     if (skip_step(a)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nm = a.nmat;
     double acc[3] = {0.0, 0.0, 0.0};
     int mati = 0;
@@ -567,9 +583,11 @@ __global__ void __launch_bounds__(kRedThreads) k_momentum(StepArgs a, int integr
     double x[3] = {1.0e20, 1.0e20, 1.0e20};
     double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
     const bool do_int = integrate && !a.time->ended;
-    if (i < a.n) {
+    if (t < a.n) {
+        const int i = a.cell_list[t];
         double *const *f = a.F.f;
-        momentum_gather<DISC>(a, i, acc);
+        const DevGrid g = *a.grid;
+        momentum_gather<DISC>(a, g, t, acc);
         if (a.prm.baseaccel)
 #pragma unroll
             for (int j = 0; j < 3; ++j) acc[j] = acc[j] + a.prm.base_a[j];
@@ -759,18 +777,48 @@ __global__ void __launch_bounds__(kRedThreads) k_init_critts(StepArgs a) {
     if (threadIdx.x == 0) a.red[blockIdx.x] = m;
 }
 
+}  // namespace MCM_FLAVOUR_NS
+}  // namespace mcm
+
+#if !MCM_EXACT
+#include "step_coop.cuh"
+#endif
+
+namespace mcm {
+namespace MCM_FLAVOUR_NS {
+
 // ----------------------------------------------------------- launchers
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+constexpr int kCoopLanes = 16;   // lanes per particle in the cooperative gathers
+// persistent grid: a few blocks per SM, each looping over particle groups
+static inline int coop_blocks(int n, int per) {
+    int need = nblk(n, per);
+    return need < 148 * 8 ? need : 148 * 8;
+}
 static inline int gs_blocks(int n) { int b = nblk(n, 256); return b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b); }
 
 void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
     k_strain_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
 }
 
-int launch_strain_constitutive(const StepArgs &a, cudaStream_t s) {
+void launch_strain(const StepArgs &a, cudaStream_t s) {
+#if MCM_EXACT
     int blocks = nblk(a.n, kRedThreads);
-    if (a.prm.disctype == 0) k_strain_const<0><<<blocks, kRedThreads, 0, s>>>(a);
-    else k_strain_const<1><<<blocks, kRedThreads, 0, s>>>(a);
+    if (a.prm.disctype == 0) k_strain<0><<<blocks, kRedThreads, 0, s>>>(a);
+    else k_strain<1><<<blocks, kRedThreads, 0, s>>>(a);
+#else
+    constexpr int L = kCoopLanes;
+    const int per = 256 / L;
+    const int blocks = coop_blocks(a.n, per);
+    const size_t smem = coop_smem<L>(a, 256);
+    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, 256, smem, s>>>(a);
+    else k_strain_coop<L, 1><<<blocks, 256, smem, s>>>(a);
+#endif
+}
+
+int launch_constitutive(const StepArgs &a, cudaStream_t s) {
+    int blocks = nblk(a.n, kRedThreads);
+    k_constitutive<<<blocks, kRedThreads, 0, s>>>(a);
     return blocks;
 }
 
@@ -779,10 +827,21 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
+#if MCM_EXACT
     int blocks = nblk(a.n, kRedThreads);
     if (a.prm.disctype == 0) k_momentum<0><<<blocks, kRedThreads, 0, s>>>(a, integrate);
     else k_momentum<1><<<blocks, kRedThreads, 0, s>>>(a, integrate);
     return blocks;
+#else
+    constexpr int L = kCoopLanes;
+    const int per = 256 / L;
+    const int blocks = coop_blocks(a.n, per);
+    const size_t smem = coop_smem<L>(a, 256);
+    if (a.nmat > 4) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
+    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, 256, smem, s>>>(a, integrate);
+    else k_momentum_coop<L, 1><<<blocks, 256, smem, s>>>(a, integrate);
+    return blocks;
+#endif
 }
 
 int launch_update_move(const StepArgs &a, cudaStream_t s) {

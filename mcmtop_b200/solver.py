@@ -46,7 +46,7 @@ def material_table(deck: Deck) -> "C.Array":
     return mats
 
 
-def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0) -> _abi.Config:
+def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_interval: int = 0) -> _abi.Config:
     """Control-card processing of MCM/mcm_control_v2.f90:193-243 and the
     boundary/base-acceleration cards (mcm_inp_symmetry_v2.f90:83-137,
     mcm_baseaccel_in.f90:23-33)."""
@@ -72,12 +72,13 @@ def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0) -> _abi.Co
     c.hmax = 0.0
     c.precision = precision
     c.nbr_stride = nbr_stride
+    c.reorder_interval = reorder_interval
     return c
 
 
 class Solver:
     def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0,
-                 device: int | None = None):
+                 device: int | None = None, reorder_interval: int = 0):
         self.lib = _abi.load()
         if device is not None:
             check(self.lib.mcm_gpu_set_device(int(device)), "mcm_gpu_set_device")
@@ -85,7 +86,7 @@ class Solver:
         self.n = deck.np
         self.nmat = len(deck.materials)
         self._mats = material_table(deck)
-        self.cfg = config_from_deck(deck, precision, nbr_stride)
+        self.cfg = config_from_deck(deck, precision, nbr_stride, reorder_interval)
         h = C.c_void_p()
         check(self.lib.mcm_gpu_create(C.byref(self.cfg), self._mats, self.nmat, self.n, C.byref(h)),
               "mcm_gpu_create")

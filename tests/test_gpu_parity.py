@@ -210,3 +210,21 @@ def test_neighbour_overflow_regrow(lib):
     orc.step()
     compare(sol, orc, STATE, 1e-12, "after regrow")
     assert sol.stats()["stride"] >= orc.get_int("nnbr").max()
+
+
+@pytest.mark.parametrize("disctype", [0, 1])
+def test_reordering_does_not_change_results(lib, disctype):
+    """Re-sorting the particle storage every 3 steps gives bitwise the same state."""
+    deck = small_bar(disctype=disctype)
+    a = Solver(deck, _abi.PREC_FP64_EXACT)
+    b = Solver(deck, _abi.PREC_FP64_EXACT, reorder_interval=3)
+    orc = Oracle(deck)
+    for _ in range(10):
+        a.step()
+        b.step()
+        orc.step()
+    ga = a.download(STATE)
+    gb = b.download(STATE)
+    for f in STATE:
+        assert np.array_equal(ga[f], gb[f]), f
+    compare_neighbours(b, orc)
