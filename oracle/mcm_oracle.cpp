@@ -760,14 +760,14 @@ void Sim::ghost_setup() {
 // MCM/mcm_ll_neighbours.f90:1-311 (storage unbounded; see header)
 void Sim::ll_neighbours(int ip_flag) {
     const real factor = 2.0;
-    int boxcrd[3] = {1, 1, 1};
-    int looplim[2][3] = {{1, 1, 1}, {1, 1, 1}};
     maxnbr = maxnbr + 5 + ip_flag;
     maxcont = maxcont + 5;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
     for (int i = 1; i <= np; ++i) {
+        int boxcrd[3] = {1, 1, 1};                   // per particle: private to the thread
+        int looplim[2][3] = {{1, 1, 1}, {1, 1, 1}};
         Particle &P = par[i];
         P.nnbr = 0; P.ncont = 0; P.g_nnbr = 0; P.g_ncont = 0;
         P.nbr.clear(); P.cont.clear(); P.gnbr.clear(); P.gcont.clear();

@@ -265,3 +265,23 @@ def test_energy_balance_bounded():
     e1 = orc.scalar("totale")
     assert abs(e1 - e0) / e0 < 0.02
     assert orc.scalar("kinetice") < 0.9 * e0
+
+
+@pytest.mark.parametrize("case", ["bar", "fluid"])
+def test_openmp_build_matches_serial(case):
+    """The OpenMP build (the timed CPU baseline) is bitwise the serial one:
+    every parallel loop writes only its own particle."""
+    from mcmtop_b200.deck import fluid_column
+
+    if case == "bar":
+        deck = taylor_bar(dx=0.6e-3)
+    else:
+        deck = fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))
+    a = Oracle(deck)
+    b = Oracle(deck, openmp=True)
+    for _ in range(4):
+        a.step()
+        b.step()
+    for f in ["x", "v", "rho", "e", "p", "sigma", "q", "efps"]:
+        assert np.array_equal(a.get(f), b.get(f)), f
+    assert np.array_equal(a.get_int("nnbr"), b.get_int("nnbr"))
