@@ -28,6 +28,7 @@ UNITS = [
     ("reduce.cu", False),
     ("step_fp64_exact.cu", False),
     ("step_fp64_fast.cu", True),
+    ("step_mixed.cu", True),
     ("noalloc.cu", False),
 ]
 HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh"]

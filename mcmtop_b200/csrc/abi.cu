@@ -192,6 +192,11 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.rec2, np))) return st;
     h->red_cap = (int)((np + 15) / 16) + 8;   // blocks of the cooperative momentum kernel (16 particles each)
     if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
+    if (h->cfg.precision == MCM_PREC_MIXED) {
+        if ((st = dalloc(h, &h->A.frec0, np))) return st;
+        if ((st = dalloc(h, &h->A.frec1, np))) return st;
+        if ((st = dalloc(h, &h->A.frec2, np))) return st;
+    }
     return MCM_OK;
 }
 
@@ -221,6 +226,10 @@ int alloc_ghosts(mcm_gpu_handle *h, int cap) {
     if ((st = dalloc(h, &h->A.grec0, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec1, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec2, (size_t)cap))) return st;
+    if (h->cfg.precision == MCM_PREC_MIXED) {
+        if ((st = dalloc(h, &h->A.gfrec1, (size_t)cap))) return st;
+        if ((st = dalloc(h, &h->A.gfrec2, (size_t)cap))) return st;
+    }
     return MCM_OK;
 }
 
@@ -281,31 +290,37 @@ int regrow(mcm_gpu_handle *h, int *grew) {
 
 // ---------------------------------------------------------------- dispatch
 int launch_strain(mcm_gpu_handle *h) {
+    const int prec = h->cfg.precision;
     {
         Scope sc(h, R_STRAIN_PREP, 1);
-        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_strain_prep(h->A, h->stream);
+        if (prec == MCM_PREC_FP64_EXACT) exact::launch_strain_prep(h->A, h->stream);
+        else if (prec == MCM_PREC_MIXED) mixed::launch_strain_prep(h->A, h->stream);
         else fast::launch_strain_prep(h->A, h->stream);
     }
     {
         Scope sc(h, R_STRAIN, 1);
-        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_strain(h->A, h->stream);
+        if (prec == MCM_PREC_FP64_EXACT) exact::launch_strain(h->A, h->stream);
+        else if (prec == MCM_PREC_MIXED) mixed::launch_strain(h->A, h->stream);
         else fast::launch_strain(h->A, h->stream);
     }
     Scope sc(h, R_CONST, 1);
-    switch (h->cfg.precision) {
+    switch (prec) {
         case MCM_PREC_FP64_EXACT: return exact::launch_constitutive(h->A, h->stream);
         default: return fast::launch_constitutive(h->A, h->stream);
     }
 }
 int launch_mom(mcm_gpu_handle *h, int integrate) {
+    const int prec = h->cfg.precision;
     {
         Scope sc(h, R_MOM_PREP, 1);
-        if (h->cfg.precision == MCM_PREC_FP64_EXACT) exact::launch_mom_prep(h->A, h->stream);
+        if (prec == MCM_PREC_FP64_EXACT) exact::launch_mom_prep(h->A, h->stream);
+        else if (prec == MCM_PREC_MIXED) mixed::launch_mom_prep(h->A, h->stream);
         else fast::launch_mom_prep(h->A, h->stream);
     }
     Scope sc(h, R_MOMENTUM, 1);
-    switch (h->cfg.precision) {
+    switch (prec) {
         case MCM_PREC_FP64_EXACT: return exact::launch_momentum(h->A, h->stream, integrate);
+        case MCM_PREC_MIXED: return mixed::launch_momentum(h->A, h->stream, integrate);
         default: return fast::launch_momentum(h->A, h->stream, integrate);
     }
 }
@@ -520,7 +535,8 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
             if (p0 != p1) return MCM_EINVAL;   // MCM/mcm_inp_symmetry_v2.f90:89-109
         }
     }
-    if (cfg->precision == MCM_PREC_MIXED) return MCM_EUNSUPPORTED;
+    // mixed path: simple SPH sums only; gather entries carry 26-bit positions
+    if (cfg->precision == MCM_PREC_MIXED && (cfg->disctype != 0 || np >= (1 << 26))) return MCM_EUNSUPPORTED;
     mcm_gpu_handle *h = new mcm_gpu_handle();
     h->cfg = *cfg;
     if (h->cfg.tssf == 0.0) h->cfg.tssf = 0.8;   // MCM/mcm_control_v2.f90:193
@@ -591,7 +607,8 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     if (!h) return MCM_EINVAL;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->d_fields, h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
+    void *ptrs[] = {h->d_fields, h->A.frec0, h->A.frec1, h->A.frec2, h->A.gfrec1, h->A.gfrec2,
+                    h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
                     h->A.cpos, h->A.cmat, h->A.ckey, h->A.nhdr, h->A.reorder_tmp, h->A.nlist,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
@@ -673,10 +690,6 @@ __global__ void k_energy_partials(StepArgs a) {
             }
         }
     }
-}
-
-__global__ void k_copy_field(double *dst, const double *src, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
 }
 
 __global__ void k_iota(int *p, int n) {

@@ -410,7 +410,7 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
                 a.gmass[g] = a.F.f[FMASS][j];
                 a.gh[g] = a.F.f[FH][j];
                 a.ghold[g] = a.F.f[FHOLD][j];
-                a.grho[g] = a.prm.mixed ? (double)a.F.s[FRHO][j] : a.F.f[FRHO][j];
+                a.grho[g] = a.F.f[FRHO][j];
                 a.gx[g] = a.F.f[FX][j] * mult[0] + add[0];
                 a.gy[g] = a.F.f[FY][j] * mult[1] + add[1];
                 a.gz[g] = a.F.f[FZ][j] * mult[2] + add[2];

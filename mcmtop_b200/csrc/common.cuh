@@ -61,7 +61,6 @@ struct DevPlanes {
 // Run options used inside kernels.
 struct DevParams {
     int ndim, disctype, tcrit_opt, boundary, baseaccel, drelax, nmat, diag;
-    int mixed;          // FP32 state live (mcm_gpu_precision MCM_PREC_MIXED)
     double drelax_scale, tssf, hmax;
     double base_a[3];
     DevPlanes planes;
@@ -85,17 +84,8 @@ enum Field {
 
 struct Fields {
     double *f[NFIELD];
-    float *s[NFIELD];   // FP32 copies: the live state of the mixed path (all but x, v, |v|, h, hold, mass)
     int *mat, *dispbc, *orig, *ptype;
 };
-
-// Fields that stay FP64 in the mixed path: positions, velocities, |v|
-// (integration) and h, hold, mass (the neighbour predicate and ghost copies
-// must see the reference's FP64 values).
-__host__ __device__ inline bool field_is_fp64_in_mixed(int f) {
-    return f == FX || f == FY || f == FZ || f == FVX || f == FVY || f == FVZ || f == FVABS || f == FH ||
-           f == FHOLD || f == FMASS || f == FMINDIST || f == FAX || f == FAY || f == FAZ;
-}
 
 __host__ __device__ inline long long cell_key(int bx, int by, int bz, const int *gl) {
     return (long long)(bx - 1) + (long long)gl[0] * ((long long)(by - 1) + (long long)gl[1] * (long long)(bz - 1));

@@ -77,15 +77,13 @@ void launch_energy_bbox_reduce(const StepArgs &a, cudaStream_t s, int nblocks, i
 void launch_set_time(const StepArgs &a, cudaStream_t s, double dt, double dtold, int set_dtold);
 void launch_finish_step(const StepArgs &a, cudaStream_t s);
 
-// step_mixed.cu: the mixed-precision path and the FP64 <-> FP32 state copies
+// step_mixed.cu: FP32 pair sums over FP32 gather records (the constitutive
+// update of the mixed path is the FP64 fast one)
 namespace mixed {
 void launch_strain_prep(const StepArgs &a, cudaStream_t s);
 void launch_strain(const StepArgs &a, cudaStream_t s);
-int launch_constitutive(const StepArgs &a, cudaStream_t s);
 void launch_mom_prep(const StepArgs &a, cudaStream_t s);
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);
-void launch_to_f32(const StepArgs &a, cudaStream_t s);
-void launch_to_f64(const StepArgs &a, cudaStream_t s);
 }  // namespace mixed
 
 // step kernels (one namespace per arithmetic flavour)

@@ -1,0 +1,518 @@
+// step_mixed.cu -- the mixed-precision explicit step.
+//
+// The pair sums (strain rate, momentum) run in FP32 over FP32 gather records;
+// every per-particle field stays FP64, and so do the constitutive update (the
+// FP64 fast one), the velocity and position update, the energy sums and the
+// critical-timestep minimum.  An FP32 density could not follow a weakly
+// compressible fluid, whose per-step density change (~1e-9 relative) is below
+// FP32 resolution; FP32 pair terms only carry a relative rounding error.  The
+// neighbour search is the shared FP64-exact one, so neighbour sets are those
+// of the reference.
+//
+// Cell-relative positions: the gather records hold each particle's position
+// relative to the origin of its cell (FP32, |offset| < one cell), and every
+// neighbour entry carries the offset of the neighbour's cell from the
+// particle's (-1, 0, 1 per axis), so x_i - x_j = (r_i - r_j) - db * cell size
+// is formed from small numbers and keeps FP32 relative accuracy at the scale
+// of h.  Ghost neighbours (few, near the planes) use FP64 positions.
+//
+// Compensated sums: each lane accumulates its neighbours with Kahan
+// summation, and the lanes' partial sums are combined with an error-free
+// (TwoSum) shuffle reduction.
+#include "nbr_iter.cuh"
+
+namespace mcm {
+namespace mixed {
+
+constexpr int L = 16;          // lanes per particle
+constexpr float kPiF = 3.14159265358979f;
+
+__device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
+
+// ------------------------------------------------------- compensated sums
+struct KSum {
+    float s, c;
+};
+__device__ __forceinline__ void kadd(KSum &k, float y) {
+    const float yy = y - k.c;
+    const float t = k.s + yy;
+    k.c = (t - k.s) - yy;
+    k.s = t;
+}
+// error-free sum of the L lanes' (s, c) pairs; every lane gets the result
+__device__ __forceinline__ double ksum_reduce(KSum k) {
+    float s = k.s, c = -k.c;
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) {
+        const float s2 = __shfl_xor_sync(0xffffffffu, s, o, L);
+        const float c2 = __shfl_xor_sync(0xffffffffu, c, o, L);
+        const float t = s + s2;
+        const float bp = t - s;
+        const float err = (s - (t - bp)) + (s2 - bp);
+        s = t;
+        c = c + c2 + err;
+    }
+    return (double)s + (double)c;
+}
+
+// ------------------------------------------------------------ geometry
+struct Frame {
+    double gmin[3], cs[3];
+    float csf[3];
+    int gl[3];
+};
+__device__ __forceinline__ Frame make_frame(const DevGrid &g) {
+    Frame fr;
+    for (int d = 0; d < 3; ++d) {
+        fr.gmin[d] = g.gridmin[d];
+        fr.cs[d] = 1.0 / g.gridsize[d];
+        fr.csf[d] = (float)fr.cs[d];
+        fr.gl[d] = g.gridlim[d];
+    }
+    return fr;
+}
+__device__ __forceinline__ void cell_origin(const Frame &fr, int key, double o[3]) {
+    if (key < 0) { o[0] = o[1] = o[2] = 0.0; return; }
+    int b[3];
+    cell_coords(key, fr.gl, b[0], b[1], b[2]);
+    for (int d = 0; d < 3; ++d) o[d] = fr.gmin[d] + (double)(b[d] - 1) * fr.cs[d];
+}
+
+// Expands position t's list into spos: entry = position | (dbx+1)<<26 | (dby+1)<<28 | (dbz+1)<<30.
+__device__ __forceinline__ int expand_cells(const StepArgs &a, const DevGrid &g, int t, int lane, unsigned *spos) {
+    const int key = a.ckey[t];
+    if (key < 0) return 0;
+    const int np = a.npad;
+    int bx, by, bz;
+    cell_coords(key, g.gridlim, bx, by, bz);
+    const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
+    const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
+    const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
+    int base = 0;
+    const int passes = a.nmat > 1 ? 2 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+        const unsigned long long hdr = a.nhdr[(size_t)pass * np + t];
+        int r = 0;
+        for (int nz = lo2; nz <= hi2; ++nz) {
+            for (int my = lo1; my <= hi1; ++my, ++r) {
+                const int cnt = (int)((hdr >> (7 * r)) & 127ull);
+                if (cnt == 0) continue;
+                const int k0 = (int)cell_key(lo0, my, nz, g.gridlim);
+                const int rs = a.cell_start[k0];
+                const int b1 = a.cell_start[k0 + 1];
+                const int b2 = (hi0 - lo0 >= 2) ? a.cell_start[k0 + 2] : 0x7fffffff;
+                const unsigned dyz = ((unsigned)(my - by + 1) << 28) | ((unsigned)(nz - bz + 1) << 30);
+                for (int c = lane; c < cnt; c += L) {
+                    const int k = base + c;
+                    const unsigned w = a.nlist[(size_t)(k >> 2) * np + t];
+                    const int p = rs + (int)((w >> (8 * (k & 3))) & 255u);
+                    const int xoff = (p >= b1) + (p >= b2);
+                    spos[k] = (unsigned)p | ((unsigned)(lo0 + xoff - bx + 1) << 26) | dyz;
+                }
+                base += cnt;
+            }
+        }
+    }
+    return base;
+}
+
+__device__ __forceinline__ void unpack(unsigned e, const Frame &fr, int &p, float &ox, float &oy, float &oz) {
+    p = (int)(e & 0x3ffffffu);
+    ox = (float)((int)((e >> 26) & 3u) - 1) * fr.csf[0];
+    oy = (float)((int)((e >> 28) & 3u) - 1) * fr.csf[1];
+    oz = (float)((int)((e >> 30) & 3u) - 1) * fr.csf[2];
+}
+
+// Cubic B-spline gradient in FP32 (MCM/mcm_gradw.f90:341-381), ih = 1/havg.
+__device__ __forceinline__ void gradw_f(float x0, float x1, float x2, float ih, float &d0, float &d1, float &d2) {
+    const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+    if (r2 == 0.0f) { d0 = d1 = d2 = 0.0f; return; }
+    const float rinv = rsqrtf(r2);
+    const float z = r2 * rinv * ih;
+    const float const1 = (1.0f / kPiF) * ih * ih * ih;
+    float dw;
+    if (z < 1.0f) dw = const1 * ((2.25f * z - 3.0f) * z);
+    else if (z < 2.0f) { const float tt = 2.0f - z; dw = -0.75f * const1 * (tt * tt); }
+    else dw = 0.0f;
+    const float f = dw * ih * rinv;
+    d0 = f * x0; d1 = f * x1; d2 = f * x2;
+}
+
+__device__ __forceinline__ float inv_havg_f(float hi, float hj, float ihi) {
+    return (hi == hj) ? ihi : 2.0f / (hi + hj);
+}
+
+static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+static inline int coop_blocks(int n, int per) {
+    int need = nblk(n, per);
+    return need < 148 * 8 ? need : 148 * 8;
+}
+
+// ------------------------------------------------------------ strain prep
+// MCM/mcm_strain.f90:27-31 (x - v dt/2) and V_j = m_j/rho_j, cell-relative.
+__global__ void k_strain_prep(StepArgs a) {
+    if (skip_step(a)) return;
+    const double dt = a.time->dt;
+    const Frame fr = make_frame(*a.grid);
+    const double *const *f = a.F.f;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
+        double o[3];
+        cell_origin(fr, a.ckey[p], o);
+        const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
+        const double xs = f[FX][i] - 0.5 * vx * dt, ys = f[FY][i] - 0.5 * vy * dt, zs = f[FZ][i] - 0.5 * vz * dt;
+        a.frec0[p] = make_float4((float)(xs - o[0]), (float)(ys - o[1]), (float)(zs - o[2]), (float)f[FH][i]);
+        a.frec1[p] = make_float4((float)vx, (float)vy, (float)vz, (float)(f[FMASS][i] / f[FRHO][i]));
+    }
+    if (a.prm.boundary) {
+        const int ngp = *a.ngp;
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngp; g += gridDim.x * blockDim.x) {
+            a.grec0[g] = make_double4(a.gx[g], a.gy[g], a.gz[g], a.gh[g]);
+            a.gfrec1[g] = make_float4((float)a.gvx[g], (float)a.gvy[g], (float)a.gvz[g], (float)(a.gmass[g] / a.grho[g]));
+        }
+    }
+}
+
+// ----------------------------------------------------------- strain rate
+// MCM/mcm_oldstrain.f90:95-124 with FP32 pair sums (Kahan per lane).
+__global__ void __launch_bounds__(256) k_strain(StepArgs a) {
+    extern __shared__ unsigned smem_u[];
+    if (skip_step(a)) return;
+    const int sub = threadIdx.x / L, lane = threadIdx.x % L;
+    const int per = blockDim.x / L;
+    const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
+    unsigned *spos = smem_u + sub * (a.nwords * 4);
+    const DevGrid g = *a.grid;
+    const Frame fr = make_frame(g);
+    const double dt = a.time->dt;
+    for (int round = 0; round < rounds; ++round) {
+        const int t = (round * gridDim.x + blockIdx.x) * per + sub;
+        const bool live = t < a.n;
+        int nreal = 0, gn = 0, i = 0;
+        float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), vi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (live) {
+            nreal = expand_cells(a, g, t, lane, spos);
+            gn = a.gnnbr[t];
+            xi = a.frec0[t];
+            vi = a.frec1[t];
+            i = a.cell_list[t];
+        }
+        __syncwarp();
+        double xs[3] = {0.0, 0.0, 0.0};
+        if (live && gn > 0) {
+            xs[0] = a.F.f[FX][i] - 0.5 * a.F.f[FVX][i] * dt;
+            xs[1] = a.F.f[FY][i] - 0.5 * a.F.f[FVY][i] * dt;
+            xs[2] = a.F.f[FZ][i] - 0.5 * a.F.f[FVZ][i] * dt;
+        }
+        const int total = live ? nreal + gn : 0;
+        const float ihi = 1.0f / xi.w;
+        KSum gv[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) gv[u] = KSum{0.f, 0.f};
+        for (int k = lane; k < total; k += L) {
+            float dx, dy, dz, hj;
+            float4 vj;
+            if (k < nreal) {
+                int p;
+                float ox, oy, oz;
+                unpack(spos[k], fr, p, ox, oy, oz);
+                const float4 xj = a.frec0[p];
+                vj = a.frec1[p];
+                dx = (xi.x - xj.x) - ox;
+                dy = (xi.y - xj.y) - oy;
+                dz = (xi.z - xj.z) - oz;
+                hj = xj.w;
+            } else {
+                const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
+                const double4 xj = a.grec0[q];
+                vj = a.gfrec1[q];
+                dx = (float)(xs[0] - xj.x);
+                dy = (float)(xs[1] - xj.y);
+                dz = (float)(xs[2] - xj.z);
+                hj = (float)xj.w;
+            }
+            float d0, d1, d2;
+            gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
+            const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
+            kadd(gv[0], t0 * d0); kadd(gv[1], t0 * d1); kadd(gv[2], t0 * d2);
+            kadd(gv[3], t1 * d0); kadd(gv[4], t1 * d1); kadd(gv[5], t1 * d2);
+            kadd(gv[6], t2 * d0); kadd(gv[7], t2 * d1); kadd(gv[8], t2 * d2);
+        }
+        double r[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) r[u] = ksum_reduce(gv[u]);
+        if (live && lane == 0) {
+            // MCM/mcm_oldstrain.f90:117-124
+            double *const *f = a.F.f;
+            f[FR11][i] = r[0];
+            f[FR22][i] = r[4];
+            f[FR33][i] = r[8];
+            f[FR12][i] = 0.5 * (r[1] + r[3]);
+            f[FR13][i] = 0.5 * (r[2] + r[6]);
+            f[FR23][i] = 0.5 * (r[5] + r[7]);
+            f[FW12][i] = 0.5 * (r[1] - r[3]);
+            f[FW13][i] = 0.5 * (r[2] - r[6]);
+            f[FW23][i] = 0.5 * (r[5] - r[7]);
+            f[FTR][i] = r[0] + r[4] + r[8];
+        }
+        __syncwarp();
+    }
+}
+
+// --------------------------------------------------------- momentum prep
+// Records: cell-relative x, h; (sigma - q)/rho^2 (formed in FP64,
+// MCM/mcm_oldacceleration.f90:79-80) and m (FP32).  Ghosts: FP64 positions,
+// stresses with every off-diagonal negated (MCM/mcm_update_ghost_stress.f90:
+// 272-285) over the ghost's own density.
+__global__ void k_mom_prep(StepArgs a) {
+    if (skip_step(a)) return;
+    const Frame fr = make_frame(*a.grid);
+    const double *const *f = a.F.f;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
+        double o[3];
+        cell_origin(fr, a.ckey[p], o);
+        const double rho = f[FRHO][i];
+        const double ir2 = 1.0 / (rho * rho);
+        const double q = f[FQ][i];
+        a.frec0[p] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]),
+                                 (float)f[FH][i]);
+        a.frec1[p] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
+                                 (float)((f[FS33][i] - q) * ir2), (float)(f[FS12][i] * ir2));
+        a.frec2[p] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
+    }
+    if (a.prm.boundary) {
+        const int ngp = *a.ngp;
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngp; g += gridDim.x * blockDim.x) {
+            const int j = a.gpar[g];
+            const double rho = a.grho[g];
+            const double ir2 = 1.0 / (rho * rho);
+            const double q = f[FQ][j];
+            a.grec0[g] = make_double4(a.gx[g], a.gy[g], a.gz[g], a.gh[g]);
+            a.gfrec1[g] = make_float4((float)((f[FS11][j] - q) * ir2), (float)((f[FS22][j] - q) * ir2),
+                                      (float)((f[FS33][j] - q) * ir2), (float)(-f[FS12][j] * ir2));
+            a.gfrec2[g] = make_float4((float)(-f[FS13][j] * ir2), (float)(-f[FS23][j] * ir2), (float)a.gmass[g],
+                                      (float)rho);
+        }
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sm[k];
+    return r;
+}
+
+__device__ __forceinline__ double block_minmax(double v, double *sm, bool is_max) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double y = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_max ? fmax(v, y) : fmin(v, y);
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = v;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = is_max ? fmax(r, sm[k]) : fmin(r, sm[k]);
+    return r;
+}
+
+// FP64 velocity and position update (MCM/mcm_update_velocity.f90:29-56,
+// MCM/mcm_move.f90:32-40, MCM/mcm_check_sym_pen.f90:27-179 per particle).
+__device__ __forceinline__ void integrate(const StepArgs &a, int i, const double acc[3], double dt, double dtold,
+                                          double x[3]) {
+    double *const *f = a.F.f;
+    const double dtn = 0.5 * (dt + dtold);
+    double v[3] = {f[FVX][i], f[FVY][i], f[FVZ][i]};
+    double vabs = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        if (a.prm.drelax) v[j] = a.prm.drelax_scale * v[j] + acc[j] * dtn;
+        else v[j] = v[j] + acc[j] * dtn;
+        vabs = vabs + v[j] * v[j];
+    }
+    vabs = sqrt(vabs);
+    x[0] = f[FX][i] + v[0] * dt;
+    x[1] = f[FY][i] + v[1] * dt;
+    x[2] = f[FZ][i] + v[2] * dt;
+    double xo[3] = {x[0], x[1], x[2]};
+    if (a.prm.boundary) {
+        const DevPlanes &pl = a.prm.planes;
+        for (int d = 0; d < 3; ++d) {
+            if (pl.code[0][d] == 1 && xo[d] < pl.bx[0][d]) { xo[d] = 2.0 * pl.bx[0][d] - xo[d]; v[d] = -v[d]; }
+            if (pl.code[1][d] == 1 && xo[d] > pl.bx[1][d]) { xo[d] = 2.0 * pl.bx[1][d] - xo[d]; v[d] = -v[d]; }
+            if (pl.code[0][d] == 2) {
+                const double span = pl.bx[1][d] - pl.bx[0][d];
+                if (xo[d] < pl.bx[0][d]) xo[d] = xo[d] + span;
+                if (xo[d] > pl.bx[1][d]) xo[d] = xo[d] - span;
+            }
+        }
+    }
+    f[FVX][i] = v[0]; f[FVY][i] = v[1]; f[FVZ][i] = v[2];
+    f[FVABS][i] = vabs;
+    f[FX][i] = xo[0]; f[FY][i] = xo[1]; f[FZ][i] = xo[2];
+}
+
+// ------------------------------------------------- momentum + integration
+// MCM/mcm_oldacceleration.f90:66-89 with FP32 pair sums, then the FP64 tail:
+// base acceleration and displacement BCs (MCM/mcm_boundcond.f90), energy
+// partials (MCM/mcm_calctotale.f90) and, when integrating, the update.
+__global__ void __launch_bounds__(256) k_momentum(StepArgs a, int integrate_flag) {
+    extern __shared__ unsigned smem_u[];
+    __shared__ double sm[32];
+    if (skip_step(a)) return;
+    const int sub = threadIdx.x / L, lane = threadIdx.x % L;
+    const int per = blockDim.x / L;
+    const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
+    unsigned *spos = smem_u + sub * (a.nwords * 4);
+    const DevGrid g = *a.grid;
+    const Frame fr = make_frame(g);
+    const int nm = a.nmat;
+    double e1[5] = {0, 0, 0, 0, 0};   // sums of material 1; others go to the partials directly
+    double xlo[3] = {1.0e20, 1.0e20, 1.0e20}, xhi[3] = {-1.0e20, -1.0e20, -1.0e20};
+    const bool do_int = integrate_flag && !a.time->ended;
+    for (int round = 0; round < rounds; ++round) {
+        const int t = (round * gridDim.x + blockIdx.x) * per + sub;
+        const bool live = t < a.n;
+        int nreal = 0, gn = 0, i = 0;
+        float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), r1i = make_float4(0.f, 0.f, 0.f, 0.f),
+               r2i = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (live) {
+            nreal = expand_cells(a, g, t, lane, spos);
+            gn = a.gnnbr[t];
+            xi = a.frec0[t];
+            r1i = a.frec1[t];
+            r2i = a.frec2[t];
+            i = a.cell_list[t];
+        }
+        __syncwarp();
+        double xa[3] = {0.0, 0.0, 0.0};
+        if (live && gn > 0) { xa[0] = a.F.f[FX][i]; xa[1] = a.F.f[FY][i]; xa[2] = a.F.f[FZ][i]; }
+        const int total = live ? nreal + gn : 0;
+        const float ihi = 1.0f / xi.w;
+        KSum acc[3] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        for (int k = lane; k < total; k += L) {
+            float dx, dy, dz, hj;
+            float4 r1, r2;
+            if (k < nreal) {
+                int p;
+                float ox, oy, oz;
+                unpack(spos[k], fr, p, ox, oy, oz);
+                const float4 xj = a.frec0[p];
+                r1 = a.frec1[p];
+                r2 = a.frec2[p];
+                dx = (xi.x - xj.x) - ox;
+                dy = (xi.y - xj.y) - oy;
+                dz = (xi.z - xj.z) - oz;
+                hj = xj.w;
+            } else {
+                const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
+                const double4 xj = a.grec0[q];
+                r1 = a.gfrec1[q];
+                r2 = a.gfrec2[q];
+                dx = (float)(xa[0] - xj.x);
+                dy = (float)(xa[1] - xj.y);
+                dz = (float)(xa[2] - xj.z);
+                hj = (float)xj.w;
+            }
+            float d0, d1, d2;
+            gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
+            const float s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
+            const float s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
+            const float mj = r2.z;
+            kadd(acc[0], mj * (s11 * d0 + s12 * d1 + s13 * d2));
+            kadd(acc[1], mj * (s12 * d0 + s22 * d1 + s23 * d2));
+            kadd(acc[2], mj * (s13 * d0 + s23 * d1 + s33 * d2));
+        }
+        double ac[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ac[c] = ksum_reduce(acc[c]);
+        if (live && lane == 0) {
+            double *const *f = a.F.f;
+            if (a.prm.baseaccel)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) ac[j] = ac[j] + a.prm.base_a[j];
+            switch (a.F.dispbc[i]) {
+                case 1: ac[0] = 0.0; break;
+                case 2: ac[1] = 0.0; break;
+                case 3: ac[2] = 0.0; break;
+                case 4: ac[0] = 0.0; ac[1] = 0.0; break;
+                case 5: ac[1] = 0.0; ac[2] = 0.0; break;
+                case 6: ac[0] = 0.0; ac[2] = 0.0; break;
+                case 7: ac[0] = 0.0; ac[1] = 0.0; ac[2] = 0.0; break;
+                default: break;
+            }
+            if (a.split_mode || a.prm.diag) { f[FAX][i] = ac[0]; f[FAY][i] = ac[1]; f[FAZ][i] = ac[2]; }
+            const int mati = a.F.mat[i];
+            const double mass = f[FMASS][i], vabs = f[FVABS][i];
+            const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),
+                                    mass * fabs(f[FVY][i]), mass * fabs(f[FVZ][i])};
+            if (mati == 1) {
+#pragma unroll
+                for (int c = 0; c < 5; ++c) e1[c] += vals[c];
+            } else {
+                for (int c = 0; c < 5; ++c)
+                    atomicAdd(&a.red[(size_t)blockIdx.x * (5 * nm + 6) + 5 * (mati - 1) + c], vals[c]);
+            }
+            if (do_int) {
+                double xn[3];
+                integrate(a, i, ac, a.time->dt, a.time->dtold, xn);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) { xlo[d] = fmin(xlo[d], xn[d]); xhi[d] = fmax(xhi[d], xn[d]); }
+            }
+        }
+        __syncwarp();
+    }
+    const int stride = 5 * nm + 6;
+    double *out = a.red + (size_t)blockIdx.x * stride;
+    double v[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) v[c] = block_sum(e1[c], sm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) out[c] = v[c];
+    if (do_int) {
+        for (int d = 0; d < 3; ++d) {
+            const double lo = block_minmax(xlo[d], sm, false);
+            const double hi = block_minmax(xhi[d], sm, true);
+            if (threadIdx.x == 0) { out[5 * nm + d] = lo; out[5 * nm + 3 + d] = hi; }
+        }
+    }
+}
+
+// ------------------------------------------------------------ launchers
+static size_t smem_bytes(const StepArgs &a) { return sizeof(unsigned) * (size_t)(256 / L) * (a.nwords * 4); }
+
+void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
+    int n = a.n > a.ghost_cap ? a.n : a.ghost_cap;
+    int b = nblk(n, 256);
+    k_strain_prep<<<b < 148 * 16 ? b : 148 * 16, 256, 0, s>>>(a);
+}
+
+void launch_strain(const StepArgs &a, cudaStream_t s) {
+    k_strain<<<coop_blocks(a.n, 256 / L), 256, smem_bytes(a), s>>>(a);
+}
+
+void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
+    int n = a.n > a.ghost_cap ? a.n : a.ghost_cap;
+    int b = nblk(n, 256);
+    k_mom_prep<<<b < 148 * 16 ? b : 148 * 16, 256, 0, s>>>(a);
+}
+
+int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
+    const int blocks = coop_blocks(a.n, 256 / L);
+    if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
+    k_momentum<<<blocks, 256, smem_bytes(a), s>>>(a, integrate_flag);
+    return blocks;
+}
+
+
+}  // namespace mixed
+}  // namespace mcm

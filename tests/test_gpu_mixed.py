@@ -1,0 +1,124 @@
+"""Accuracy of the mixed-precision step against the FP64 oracle.
+
+The mixed path computes the strain-rate and momentum pair sums in FP32 with
+compensated summation (cell-relative positions, Kahan sums per lane, TwoSum
+across lanes); every per-particle field, the constitutive update, the
+integration and the energy/timestep reductions stay FP64.  The neighbour
+search is the exact FP64 one, so neighbour sets match the oracle's.  Field
+errors are relative to each field's largest magnitude; the bound 2e-5 after
+20 steps is about 100 FP32 ulps of the largest value.
+"""
+import numpy as np
+import pytest
+
+from mcmtop_b200 import _abi
+from mcmtop_b200.deck import fluid_column, taylor_bar
+from mcmtop_b200.solver import Solver
+from oracle.pyoracle import Oracle
+
+from test_gpu_parity import STATE, compare, compare_neighbours, relerr
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 2e-5
+
+
+@pytest.fixture(scope="module")
+def lib(gpu_lib):
+    return gpu_lib
+
+
+def test_mixed_initial_state(lib):
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_MIXED)
+    orc = Oracle(deck)
+    # initialisation is the FP64 one
+    compare(sol, orc, STATE, 1e-14, "initial")
+    assert abs(sol.dt - orc.scalar("dt")) <= 1e-14 * orc.scalar("dt")
+    compare_neighbours(sol, orc)
+
+
+def test_mixed_one_step_split(lib):
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_MIXED)
+    orc = Oracle(deck)
+    c_gpu = sol.step_a()
+    c_orc = orc.step_a()
+    assert abs(c_gpu - c_orc) <= 1e-6 * abs(c_orc)
+    compare_neighbours(sol, orc)
+    compare(sol, orc, STATE + ["rod", "spin"], MIXED_TOL, "mixed step_a")
+    sol.dt_update()
+    orc.dt_update()
+    sol.step_b()
+    orc.step_b()
+    assert relerr(sol.energies, orc.energies()) < 1e-6
+    compare(sol, orc, ["a"], 1e-4, "mixed acceleration")
+    sol.step_c()
+    orc.step_c()
+    compare(sol, orc, STATE, MIXED_TOL, "mixed step_c")
+
+
+def test_mixed_twenty_steps(lib):
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_MIXED)
+    orc = Oracle(deck)
+    for _ in range(20):
+        sol.step()
+        orc.step()
+    assert abs(sol.ptime - orc.scalar("ptime")) <= 1e-6 * orc.scalar("ptime")
+    compare(sol, orc, STATE, MIXED_TOL, "mixed 20 steps")
+
+
+def test_mixed_fused_run_matches_split(lib):
+    deck = taylor_bar(dx=0.8e-3)
+    a = Solver(deck, _abi.PREC_MIXED)
+    b = Solver(deck, _abi.PREC_MIXED)
+    for _ in range(10):
+        a.step()
+    assert b.run(10) == 10
+    ga = a.download(STATE)
+    gb = b.download(STATE)
+    for f in STATE:
+        assert relerr(gb[f], ga[f]) <= 1e-6, f
+
+
+def test_mixed_reordering(lib):
+    """Re-sorting the storage leaves the mixed results bitwise unchanged (the
+    gather records and the summation order follow the cell order)."""
+    deck = taylor_bar(dx=0.8e-3)
+    a = Solver(deck, _abi.PREC_MIXED)
+    b = Solver(deck, _abi.PREC_MIXED, reorder_interval=3)
+    for _ in range(10):
+        a.step()
+        b.step()
+    ga = a.download(STATE)
+    gb = b.download(STATE)
+    for f in STATE:
+        assert np.array_equal(ga[f], gb[f]), f
+
+
+def test_mixed_fluid_column_ghosts(lib):
+    """Ghost pairs (FP64 positions) in a water column with five planes."""
+    deck = fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))
+    sol = Solver(deck, _abi.PREC_MIXED)
+    orc = Oracle(deck)
+    for _ in range(10):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-4, "mixed fluid")
+
+
+def test_mixed_taylor_bar_16k(lib):
+    deck = taylor_bar(dx=0.4e-3)
+    sol = Solver(deck, _abi.PREC_MIXED)
+    orc = Oracle(deck, openmp=True)
+    for _ in range(30):
+        sol.step()
+        orc.step()
+    compare(sol, orc, STATE, 1e-4, "mixed 16k bar")
+
+
+def test_mixed_rejects_corrected_sph(lib):
+    deck = taylor_bar(dx=0.8e-3, disctype=1)
+    with pytest.raises(_abi.MCMError):
+        Solver(deck, _abi.PREC_MIXED)
