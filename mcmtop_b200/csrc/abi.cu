@@ -179,9 +179,9 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.key, np))) return st;
     if ((st = dalloc(h, &h->A.cell_list, np))) return st;
     if ((st = dalloc(h, &h->A.cpos, np))) return st;
+    if ((st = dalloc(h, &h->A.cposf, np))) return st;
     if ((st = dalloc(h, &h->A.cmat, np))) return st;
     if ((st = dalloc(h, &h->A.ckey, np))) return st;
-    if ((st = dalloc(h, &h->A.nhdr, 2 * np))) return st;
     if ((st = dalloc(h, &h->A.reorder_tmp, np))) return st;
     if ((st = dalloc(h, &h->A.nnbr, np))) return st;
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
@@ -193,9 +193,9 @@ int alloc_particles(mcm_gpu_handle *h) {
     h->red_cap = (int)((np + 15) / 16) + 8;   // blocks of the cooperative momentum kernel (16 particles each)
     if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
     if (h->cfg.precision == MCM_PREC_MIXED) {
-        if ((st = dalloc(h, &h->A.frec0, np))) return st;
-        if ((st = dalloc(h, &h->A.frec1, np))) return st;
-        if ((st = dalloc(h, &h->A.frec2, np))) return st;
+        // one 64-byte slot per particle: strain records use the first 32 bytes
+        // of a 2-float4 stride, momentum records 48 bytes of a 4-float4 stride
+        if ((st = dalloc(h, &h->A.frec0, 4 * np))) return st;
     }
     return MCM_OK;
 }
@@ -233,11 +233,11 @@ int alloc_ghosts(mcm_gpu_handle *h, int cap) {
     return MCM_OK;
 }
 
-int alloc_table(mcm_gpu_handle *h, int nwords, int gstride) {
+int alloc_table(mcm_gpu_handle *h, int nstride, int gstride) {
     int st;
-    h->A.nwords = nwords;
+    h->A.nstride = round_up(nstride, 4);
     h->A.gstride = gstride;
-    if ((st = dalloc(h, &h->A.nlist, (size_t)nwords * h->npad))) return st;
+    if ((st = dalloc(h, &h->A.nidx, (size_t)h->A.nstride * h->npad))) return st;
     if ((st = dalloc(h, &h->A.gnbr, (size_t)gstride * h->npad))) return st;
     return MCM_OK;
 }
@@ -262,11 +262,10 @@ int regrow(mcm_gpu_handle *h, int *grew) {
     int st;
     switch (s.code) {
         case MCM_ENBR_OVERFLOW: {
-            if (s.req_stride < 0) break;   // a row with more than 256 candidates or 127 neighbours
-            int nw = h->A.nwords, ng = h->A.gstride;
-            if (s.req_stride > nw * 4) nw = (s.req_stride + s.req_stride / 8 + 8 + 3) / 4;
+            int ns = h->A.nstride, ng = h->A.gstride;
+            if (s.req_stride > ns) ns = s.req_stride + s.req_stride / 8 + 8;
             if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
-            if ((st = alloc_table(h, nw, ng))) return st;
+            if ((st = alloc_table(h, ns, ng))) return st;
             *grew = 1;
             break;
         }
@@ -536,7 +535,9 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
         }
     }
     // mixed path: simple SPH sums only; gather entries carry 26-bit positions
-    if (cfg->precision == MCM_PREC_MIXED && (cfg->disctype != 0 || np >= (1 << 26))) return MCM_EUNSUPPORTED;
+    // neighbour-list entries carry 26-bit positions; the mixed path has simple SPH sums only
+    if (np >= (1 << 26)) return MCM_EUNSUPPORTED;
+    if (cfg->precision == MCM_PREC_MIXED && cfg->disctype != 0) return MCM_EUNSUPPORTED;
     mcm_gpu_handle *h = new mcm_gpu_handle();
     h->cfg = *cfg;
     if (h->cfg.tssf == 0.0) h->cfg.tssf = 0.8;   // MCM/mcm_control_v2.f90:193
@@ -594,7 +595,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->h_energy = (double *)(q + 1088);
     TRY(alloc_particles(h));
     int entries = cfg->nbr_stride > 0 ? cfg->nbr_stride : 100;
-    TRY(alloc_table(h, (entries + 3) / 4, cfg->boundary ? 48 : 8));
+    TRY(alloc_table(h, entries, cfg->boundary ? 48 : 8));
     TRY(alloc_cells(h, 1 << 16));
     TRY(alloc_ghosts(h, cfg->boundary ? std::max(4096, np / 8) : 32));
     TRY(dalloc(h, &h->d_nppermat, (size_t)nmat));
@@ -607,10 +608,10 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     if (!h) return MCM_EINVAL;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->d_fields, h->A.frec0, h->A.frec1, h->A.frec2, h->A.gfrec1, h->A.gfrec2,
+    void *ptrs[] = {h->d_fields, h->A.frec0, h->A.gfrec1, h->A.gfrec2,
                     h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
-                    h->A.cpos, h->A.cmat, h->A.ckey, h->A.nhdr, h->A.reorder_tmp, h->A.nlist,
+                    h->A.cpos, h->A.cposf, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat,
@@ -1079,41 +1080,15 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
     if (g_stride) { if (small || !g_nbr) *g_stride = std::max(*g_stride, gneed); }
     if (small) return MCM_EINVAL;
     if (nbr && stride) {
-        DevGrid g;
-        CK(cudaMemcpy(&g, h->A.grid, sizeof(g), cudaMemcpyDeviceToHost));
-        std::vector<int> cstart((size_t)g.ncells + 1);
-        CK(cudaMemcpy(cstart.data(), h->A.cell_start, sizeof(int) * cstart.size(), cudaMemcpyDeviceToHost));
-        std::vector<unsigned long long> hdr(2 * (size_t)np);
-        CK(cudaMemcpy(hdr.data(), h->A.nhdr, sizeof(unsigned long long) * hdr.size(), cudaMemcpyDeviceToHost));
-        std::vector<unsigned int> words((size_t)h->A.nwords * np);
-        CK(cudaMemcpy(words.data(), h->A.nlist, sizeof(unsigned int) * words.size(), cudaMemcpyDeviceToHost));
-        const int *gl = g.gridlim;
+        const int ns = h->A.nstride;
+        std::vector<unsigned int> tab((size_t)ns * np);
+        CK(cudaMemcpy(tab.data(), h->A.nidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
+        const int self = h->cfg.disctype == 1 ? 1 : 0;
         for (int t = 0; t < n; ++t) {
             int *row = nbr + (size_t)orig[clist[t]] * *stride;
-            int k = 0;
-            const int key = ckey[t];
-            if (key >= 0) {
-                int bx = key % gl[0] + 1, r0 = key / gl[0], by = r0 % gl[1] + 1, bz = r0 / gl[1] + 1;
-                int lo0 = std::max(bx - 1, 1), hi0 = std::min(bx + 1, gl[0]);
-                int lo1 = std::max(by - 1, 1), hi1 = std::min(by + 1, gl[1]);
-                int lo2 = std::max(bz - 1, 1), hi2 = std::min(bz + 1, gl[2]);
-                int e = 0;
-                for (int pass = 0; pass < (h->nmat > 1 ? 2 : 1); ++pass) {
-                    unsigned long long hh = hdr[(size_t)pass * np + t];
-                    int r = 0;
-                    for (int nz = lo2; nz <= hi2; ++nz)
-                        for (int my = lo1; my <= hi1; ++my, ++r) {
-                            int c = (int)((hh >> (7 * r)) & 127ull);
-                            int rs = cstart[(size_t)cell_key(lo0, my, nz, gl)];
-                            for (int q = 0; q < c; ++q, ++e) {
-                                unsigned int wv = words[(size_t)(e / 4) * np + t];
-                                int off = (int)((wv >> (8 * (e % 4))) & 255u);
-                                row[k++] = orig[clist[rs + off]] + 1;
-                            }
-                        }
-                }
-            }
-            if (h->cfg.disctype == 1) row[k++] = orig[clist[t]] + 1;
+            const int stored = cnt[t] - self;
+            for (int k = 0; k < stored; ++k) row[k] = orig[clist[tab[(size_t)t * ns + k] & 0x3ffffffu]] + 1;
+            if (self) row[stored] = orig[clist[t]] + 1;
         }
     }
     if (g_nbr && g_stride) {
@@ -1197,7 +1172,7 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
         CK(cudaMemcpy(&s, h->A.status, sizeof(s), cudaMemcpyDeviceToHost));
         *max_nbr = s.max_nbr;
     }
-    if (stride) *stride = h->A.nwords * 4;
+    if (stride) *stride = h->A.nstride;
     if (ngp) CK(cudaMemcpy(ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
     return MCM_OK;
 }

@@ -79,6 +79,7 @@ __global__ void k_grid_setup(StepArgs a) {
         a.status->req_cells = g.ncells;
         raise_status(a.status, MCM_EGRID_OVERFLOW);
     }
+    g.hcut = 0.0;   // raised by k_cell_records
     *a.grid = g;
     *a.ngp = 0;
     *a.n_inside = 0;
@@ -215,14 +216,43 @@ __global__ void k_cell_scatter(StepArgs a) {
 }
 
 // Candidate records in cell order (positions at neighbour time).
-__global__ void k_cell_records(StepArgs a) {
+// Candidate records in cell order: FP64 position and h, and an FP32 copy of
+// the position relative to the origin of the particle's own cell, which the
+// search uses to decide all but the near-tie candidates.
+__global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
+    __shared__ unsigned long long smax[8];
     if (a.status->code) return;
     const double *X = a.F.f[FX], *Y = a.F.f[FY], *Z = a.F.f[FZ], *H = a.F.f[FH];
+    const DevGrid g = *a.grid;
+    unsigned long long hbits = 0ull;   // h > 0: the bit pattern orders like the value
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
         int i = a.cell_list[p];
-        a.cpos[p] = make_double4(X[i], Y[i], Z[i], H[i]);
+        const double x = X[i], y = Y[i], z = Z[i], h = H[i];
+        a.cpos[p] = make_double4(x, y, z, h);
         a.cmat[p] = a.F.mat[i];
-        a.ckey[p] = a.key[i];
+        const int key = a.key[i];
+        a.ckey[p] = key;
+        float4 r = make_float4(0.f, 0.f, 0.f, (float)h);
+        if (key >= 0) {
+            int bx, by, bz;
+            cell_coords(key, g.gridlim, bx, by, bz);
+            r.x = (float)(x - cell_origin(g, 0, bx));
+            r.y = (float)(y - cell_origin(g, 1, by));
+            r.z = (float)(z - cell_origin(g, 2, bz));
+            const unsigned long long hb = (unsigned long long)__double_as_longlong(h);
+            hbits = hb > hbits ? hb : hbits;
+        }
+        a.cposf[p] = r;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, hbits, o);
+        hbits = v > hbits ? v : hbits;
+    }
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = hbits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) hbits = smax[w] > hbits ? smax[w] : hbits;
+        atomicMax(reinterpret_cast<unsigned long long *>(&a.grid->hcut), hbits);
     }
 }
 
@@ -263,7 +293,7 @@ void launch_cell_build(const StepArgs &a, cudaStream_t s) {
     device_exclusive_scan(a.cell_count, a.cell_start, a.scan_sums, &a.grid->ncells, a.cell_cap, s);
     k_cell_scatter<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
     k_cell_sort<<<grid_blocks(a.cell_cap, 128), 128, 0, s>>>(a);
-    k_cell_records<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
+    k_cell_records<<<grid_blocks(a.n, 256) < 148 * 8 ? grid_blocks(a.n, 256) : 148 * 8, 256, 0, s>>>(a);
 }
 
 // ------------------------------------------------------------- re-sorting
@@ -452,14 +482,17 @@ void launch_ghosts(const StepArgs &a, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------ search
-// MCM/mcm_ll_neighbours.f90:96-299.  One thread per cell-order position.  A
-// row of three x-adjacent cells is a contiguous range of positions whose
-// candidate records (cpos) sit next to each other in memory, and the threads
-// of a warp (neighbouring positions, mostly the same cell) read the same rows,
-// so the candidate loads are served by L1.  Accepted neighbours are stored as
-// one byte each (offset inside the row) in row order; the per-row counts go to
-// a 64-bit header.  This reproduces the reference's neighbour sequence: rows
-// in z, y order, cells in x order, each cell in descending reference index.
+// MCM/mcm_ll_neighbours.f90:96-299.  One thread per cell-order position t;
+// the threads of a warp (neighbouring positions, mostly one cell) walk the
+// same rows, so their candidate loads hit the same cache lines.  Candidates
+// are visited in the reference order (rows of the 27-cell neighbourhood in
+// z, y order, cells in x order, each cell's contiguous range of positions),
+// and accepted ones are appended to t's list in that order.  The distance
+// test runs first in FP32 on positions relative to cell origins; only
+// candidates within a narrow band around the cutoff (or all accepted ones
+// when the FP64 minimum distance is wanted) are decided by the reference's
+// FP64 expression, so the sets are the reference's.  Cells whose box lies
+// beyond h_i + max h cannot hold a neighbour and are skipped.
 
 __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
     double d = __dsub_rn(b.x, a.x);
@@ -471,18 +504,19 @@ __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
     return s;
 }
 
-__global__ void __launch_bounds__(256) k_search(StepArgs a) {
+__global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     if (a.status->code) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
     const int np = a.npad;
+    const int cap = a.nstride;
     const int key = a.ckey[t];
     const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
+    const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
     int nn = 0, gn = 0;
     double mind = 1.0e20;
-    bool inside = key >= 0;
-    if (inside) {
+    if (key >= 0) {
         const DevGrid g = *a.grid;
         int bx, by, bz;
         cell_coords(key, g.gridlim, bx, by, bz);
@@ -490,54 +524,61 @@ __global__ void __launch_bounds__(256) k_search(StepArgs a) {
         const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
         const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
         const double4 xi = a.cpos[t];
+        const float4 ui = a.cposf[t];
+        const float cs[3] = {(float)(1.0 / g.gridsize[0]), (float)(1.0 / g.gridsize[1]), (float)(1.0 / g.gridsize[2])};
+        const float csm = fmaxf(cs[0], fmaxf(cs[1], cs[2]));
+        // FP32 decision band around the cutoff: the FP32 rounding of d2 and
+        // (h_i + h_j)^2 (a few hundred ulps of csm^2 at most) stays far inside it
+        const float kb = 2.44140625e-4f * csm * csm;
+        const float khi = 1.0f + 2.44140625e-4f, klo = 1.0f - 2.44140625e-4f;
+        const float reach = ui.w + (float)g.hcut;
+        const float reach2 = reach * reach * 1.0009765625f + 9.765625e-4f * csm * csm;
         const int mati = a.cmat[t];
-        const int cap = a.nwords * 4;
-        unsigned int word = 0;
-        int nb = 0, w = 0;
+        unsigned *out = a.nidx + (size_t)t * cap;
         const int passes = a.nmat > 1 ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
-            unsigned long long hdr = 0ull;
-            int r = 0;
             for (int nz = lo2; nz <= hi2; ++nz) {
-                for (int my = lo1; my <= hi1; ++my, ++r) {
+                const float qz = ui.z + (float)(bz - nz) * cs[2];
+                const float gz = fmaxf(nz < bz ? ui.z : (nz > bz ? cs[2] - ui.z : 0.0f), 0.0f);
+                for (int my = lo1; my <= hi1; ++my) {
+                    const float qy = ui.y + (float)(by - my) * cs[1];
+                    const float gy = fmaxf(my < by ? ui.y : (my > by ? cs[1] - ui.y : 0.0f), 0.0f);
+                    const float gyz = gy * gy + gz * gz;
+                    if (gyz > reach2) continue;
                     const int k0 = (int)cell_key(lo0, my, nz, g.gridlim);
-                    const int k1 = k0 + (hi0 - lo0);
-                    const int rs = a.cell_start[k0], re = a.cell_start[k1 + 1];
-                    if (re - rs > 256) {
-                        a.status->req_stride = -1;
-                        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
-                    }
-                    int cnt = 0;
-                    for (int p = rs; p < re; ++p) {
-                        if (p == t) continue;
-                        const double4 c = a.cpos[p];
-                        const double d2 = exact_d2(xi, c);
-                        const double hs = __dadd_rn(c.w, xi.w);
-                        if (d2 < __dmul_rn(hs, hs)) {
-                            const bool same = (a.cmat[p] == mati);
-                            if (same != (pass == 0)) continue;
-                            mind = fmin(mind, d2);
-                            ++cnt;
-                            word |= (unsigned int)(p - rs) << (8 * nb);
-                            if (++nb == 4) {
-                                if (w < a.nwords) a.nlist[(size_t)w * np + t] = word;
-                                ++w;
-                                word = 0u;
-                                nb = 0;
+                    const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
+                    for (int lx = lo0; lx <= hi0; ++lx) {
+                        const float gx = fmaxf(lx < bx ? ui.x : (lx > bx ? cs[0] - ui.x : 0.0f), 0.0f);
+                        if (gyz + gx * gx > reach2) continue;
+                        const int cb = a.cell_start[k0 + (lx - lo0)], ce = a.cell_start[k0 + (lx - lo0) + 1];
+                        // this particle relative to the origin of candidate cell lx
+                        const float qx = ui.x + (float)(bx - lx) * cs[0];
+                        const unsigned code = (code_yz + (unsigned)(lx - bx + 1)) << 26;
+                        for (int p = cb; p < ce; ++p) {
+                            const float4 c = a.cposf[p];
+                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                            const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float hsf = ui.w + c.w;
+                            const float r2f = hsf * hsf;
+                            if (d2f >= fmaf(r2f, khi, kb)) continue;
+                            if (p == t) continue;
+                            double d2 = 0.0;
+                            if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
+                                // near tie (or mindist wanted): the reference's FP64 test
+                                const double4 cd = a.cpos[p];
+                                d2 = exact_d2(xi, cd);
+                                const double hs = __dadd_rn(cd.w, xi.w);
+                                if (!(d2 < __dmul_rn(hs, hs))) continue;
                             }
+                            if ((a.cmat[p] == mati) != (pass == 0)) continue;
+                            if (want_mind) mind = fmin(mind, d2);
+                            if (nn < cap) out[nn] = (unsigned)p | code;
+                            ++nn;
                         }
                     }
-                    if (cnt > 127) {
-                        a.status->req_stride = -1;
-                        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
-                    }
-                    hdr |= (unsigned long long)(cnt & 127) << (7 * r);
-                    nn += cnt;
                 }
             }
-            a.nhdr[(size_t)pass * np + t] = hdr;
         }
-        if (nb > 0 && w < a.nwords) a.nlist[(size_t)w * np + t] = word;
         if (nn > cap) {
             atomicMax(&a.status->req_stride, nn);
             raise_status(a.status, MCM_ENBR_OVERFLOW, i);
@@ -556,13 +597,12 @@ __global__ void __launch_bounds__(256) k_search(StepArgs a) {
                             for (int lx = lo0; lx <= hi0; ++lx) {
                                 const int2 gc = a.gcell[(int)cell_key(lx, my, nz, g.gridlim)];
                                 for (int r = 0; r < gc.y; ++r) {
-                                    const int q = gc.x + gc.y - 1 - r;
+                                    const int q = gc.x + gc.y - 1 - r;   // chain order: newest first
                                     const double4 c = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
                                     const double d2 = exact_d2(xi, c);
                                     const double hs = __dadd_rn(c.w, xi.w);
                                     if (d2 < __dmul_rn(hs, hs)) {
-                                        const bool same = (a.gmat[q] == mati);
-                                        if (same != (pass == 0)) continue;
+                                        if ((a.gmat[q] == mati) != (pass == 0)) continue;
                                         mind = fmin(mind, d2);
                                         if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
                                         ++gn;
@@ -581,7 +621,7 @@ __global__ void __launch_bounds__(256) k_search(StepArgs a) {
     if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
     a.nnbr[t] = nn;
     a.gnnbr[t] = gn;
-    if (a.prm.tcrit_opt == 2 || a.prm.diag) a.F.f[FMINDIST][i] = mind;
+    if (want_mind) a.F.f[FMINDIST][i] = mind;
     atomicMax(&a.status->max_nbr, nn);
     atomicMax(&a.status->max_gnbr, gn);
 }

@@ -47,6 +47,7 @@ struct DevGrid {
     int gridlim[3];
     int pad;
     long long ncells;
+    double hcut;      // largest h of the particles in cells (bounds the search reach)
 };
 
 // Boundary planes (MCM/mcm_init_boundary.f90:28-116).
@@ -89,6 +90,11 @@ struct Fields {
 
 __host__ __device__ inline long long cell_key(int bx, int by, int bz, const int *gl) {
     return (long long)(bx - 1) + (long long)gl[0] * ((long long)(by - 1) + (long long)gl[1] * (long long)(bz - 1));
+}
+
+// Lower corner of cell b (1-based) along axis d of the grid.
+__host__ __device__ inline double cell_origin(const DevGrid &g, int d, int b) {
+    return g.gridmin[d] + (double)(b - 1) * (1.0 / g.gridsize[d]);
 }
 
 __device__ __forceinline__ void raise_status(DevStatus *st, int code, int idx = -1) {

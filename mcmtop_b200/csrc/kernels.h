@@ -10,7 +10,7 @@ struct StepArgs {
     int n;            // particles
     int npad;         // column pitch of per-particle arrays (multiple of 32)
     int nmat;
-    int nwords;       // neighbour-list width in 32-bit words (4 one-byte entries each)
+    int nstride;      // neighbour-list capacity per position (entries, multiple of 4)
     int gstride;      // ghost-neighbour table width (int32 entries)
     int ghost_cap;    // ghost storage
     long long cell_cap;   // cell-array storage
@@ -32,6 +32,7 @@ struct StepArgs {
     int *cell_list;   // npad: position -> state index
     int *n_inside;    // particles inside the grid (device counter)
     double4 *cpos;    // per position: x, y, z, h at neighbour time
+    float4 *cposf;    // per position: x, y, z relative to the cell origin (FP32), h
     int *cmat;        // per position: material
     int *ckey;        // per position: cell key or -1
     int *scan_sums;   // block sums of the scan
@@ -42,21 +43,21 @@ struct StepArgs {
     int *ngp;         // device ghost counter
     int *plane_base;  // ghost index base of the plane being built
     int *layer_count, *layer_off;
-    // neighbour lists, per position p, in the reference order: one byte per
-    // real neighbour (its offset inside its row of three x-adjacent cells),
-    // word w of p at nlist[w*npad + p]; nhdr[p] packs the per-row counts
-    // (7 bits x 9 rows) of same-material neighbours, nhdr[npad + p] those of
-    // other-material (contact) neighbours.  Ghost neighbours: int32 ghost
-    // indices, entry k of p at gnbr[k*npad + p].
-    unsigned int *nlist;
-    unsigned long long *nhdr;
+    // neighbour lists, per position p, in the reference order (same-material
+    // neighbours, then contacts; rows in z, y order, cells in x order, each
+    // cell in descending reference index): entry k of p at
+    // nidx[p*nstride + k] = q | code << 26, q the neighbour's position and
+    // code = (dx+1) + 3(dy+1) + 9(dz+1) the offset of its cell from p's.
+    // The self entry of disctype 1 is not stored.  Ghost neighbours: int32
+    // ghost indices, entry k of p at gnbr[k*npad + p].
+    unsigned int *nidx;
     int *gnbr, *nnbr, *gnnbr;
     double *reorder_tmp;   // npad doubles of scratch for the state permutation
     // gather records
     double4 *rec0, *rec1, *rec2;   // per particle
     double4 *grec0, *grec1, *grec2;  // per ghost
-    float4 *frec0, *frec1, *frec2;   // mixed path
-    float4 *gfrec0, *gfrec1, *gfrec2;
+    float4 *frec0;                   // mixed path: 64 bytes per particle (strain or momentum record)
+    float4 *gfrec1, *gfrec2;         // mixed path, per ghost
     // reductions
     double *red;      // block partials
     int red_blocks;

@@ -1,10 +1,9 @@
 // step_coop.cuh -- cooperative gather kernels for the FP64 fast path.
 //
-// L lanes (a sub-warp) work on one particle: they first expand its one-byte
-// neighbour list (see nbr_iter.cuh) into absolute cell-order positions in
-// shared memory, then each lane takes every L-th neighbour, so L independent
-// record loads are in flight per particle, and the partial sums are combined
-// with shuffle reductions (no atomics).  The summation order differs from the
+// L lanes (a sub-warp) work on one particle: each lane takes every L-th entry
+// of its neighbour list (see nbr_iter.cuh; consecutive lanes read consecutive
+// entries), so L independent record loads are in flight per particle, and
+// the partial sums are combined with shuffle reductions (no atomics).  The summation order differs from the
 // reference's sequential order; the FP64-exact path keeps that order.
 #pragma once
 #include "nbr_iter.cuh"
@@ -12,41 +11,6 @@
 
 namespace mcm {
 namespace MCM_FLAVOUR_NS {
-
-// Expands the real-neighbour list of position t into spos[0..n); returns n
-// (same-material rows, then contact rows; the self entry of disctype 1 and
-// the ghosts are not included).
-template <int L>
-__device__ __forceinline__ int coop_expand(const StepArgs &a, const DevGrid &g, int t, int lane, int *spos) {
-    const int key = a.ckey[t];
-    if (key < 0) return 0;
-    const int np = a.npad;
-    int bx, by, bz;
-    cell_coords(key, g.gridlim, bx, by, bz);
-    const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
-    const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
-    const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
-    int base = 0;
-    const int passes = a.nmat > 1 ? 2 : 1;
-    for (int pass = 0; pass < passes; ++pass) {
-        const unsigned long long hdr = a.nhdr[(size_t)pass * np + t];
-        int r = 0;
-        for (int nz = lo2; nz <= hi2; ++nz) {
-            for (int my = lo1; my <= hi1; ++my, ++r) {
-                const int cnt = (int)((hdr >> (7 * r)) & 127ull);
-                if (cnt == 0) continue;
-                const int rs = a.cell_start[(int)cell_key(lo0, my, nz, g.gridlim)];
-                for (int c = lane; c < cnt; c += L) {
-                    const int k = base + c;
-                    const unsigned int w = a.nlist[(size_t)(k >> 2) * np + t];
-                    spos[k] = rs + (int)((w >> (8 * (k & 3))) & 255u);
-                }
-                base += cnt;
-            }
-        }
-    }
-    return base;
-}
 
 template <int L>
 __device__ __forceinline__ double sub_sum(double v) {
@@ -86,46 +50,42 @@ __device__ __forceinline__ double inv_havg(double hi, double hj, double ihi) {
     return (hi == hj) ? ihi : 1.0 / (0.5 * (hi + hj));
 }
 
-// Visits entry k of position t's full list: real (positions from spos), self
-// (disctype 1), ghosts.  Returns false past the end.
+// Entry k of position t's full list: real neighbours (positions), self
+// (disctype 1), ghosts.
 struct Entry {
     int kind;   // 0 real position, 1 ghost index
     int idx;
     bool self;
 };
-__device__ __forceinline__ Entry entry_at(const StepArgs &a, int t, int k, int nreal, int self, const int *spos) {
+__device__ __forceinline__ Entry entry_at(const StepArgs &a, int t, int k, int nreal, int self, const unsigned *list) {
     Entry e;
-    if (k < nreal) { e.kind = 0; e.idx = spos[k]; e.self = false; }
+    if (k < nreal) { e.kind = 0; e.idx = (int)(list[k] & kPosMask); e.self = false; }
     else if (k < nreal + self) { e.kind = 0; e.idx = t; e.self = true; }
     else { e.kind = 1; e.idx = a.gnbr[(size_t)(k - nreal - self) * a.npad + t]; e.self = false; }
     return e;
 }
 
-template <int L>
-size_t coop_smem(const StepArgs &a, int threads) { return sizeof(int) * (size_t)(threads / L) * (a.nwords * 4); }
-
 // ----------------------------------------------------------- strain rate
 template <int L, int DISC>
-__global__ void __launch_bounds__(256) k_strain_coop(StepArgs a) {
-    extern __shared__ int smem[];
+__global__ void __launch_bounds__(256, DISC == 0 ? 3 : 1) k_strain_coop(StepArgs a) {
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     const int per = blockDim.x / L;
     const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
-    int *spos = smem + sub * (a.nwords * 4);
     const DevGrid g = *a.grid;
+    (void)g;
     for (int round = 0; round < rounds; ++round) {
     const int t = (round * gridDim.x + blockIdx.x) * per + sub;
     const bool live = t < a.n;
     int nreal = 0, gn = 0;
     double4 xi = make_double4(0, 0, 0, 1), vi = make_double4(0, 0, 0, 0);
     if (live) {
-        nreal = coop_expand<L>(a, g, t, lane, spos);
+        nreal = stored_neighbours(a, t);
         gn = a.gnnbr[t];
         xi = a.rec0[t];
         vi = a.rec1[t];
     }
-    __syncwarp();
+    const unsigned *spos = a.nidx + (size_t)t * a.nstride;
     const int self = (a.prm.disctype == 1) ? 1 : 0;
     const int total = live ? nreal + self + gn : 0;
     const double ihi = 1.0 / xi.w;
@@ -229,24 +189,17 @@ __global__ void __launch_bounds__(256) k_strain_coop(StepArgs a) {
 
 // ------------------------------------------------- momentum + integration
 template <int L, int DISC>
-__global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate) {
-    extern __shared__ int smem[];
+__global__ void __launch_bounds__(256, DISC == 0 ? 3 : 1) k_momentum_coop(StepArgs a, int integrate) {
     __shared__ double sm[32];
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     const int per = blockDim.x / L;
     const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
-    int *spos = smem + sub * (a.nwords * 4);
     const DevGrid g = *a.grid;
+    (void)g;
     const int nm = a.nmat;
-    double ke_m[kMaxMat], ie_m[kMaxMat], mo_m[kMaxMat][3];
-    // per-material sums kept for up to 4 materials in registers, the rest folded below
-    double e_acc[4][5];
-#pragma unroll
-    for (int m = 0; m < 4; ++m)
-#pragma unroll
-        for (int c = 0; c < 5; ++c) e_acc[m][c] = 0.0;
-    (void)ke_m; (void)ie_m; (void)mo_m;
+    // sums of material 1 in registers; other materials go to the block's partials
+    double e1[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double x[3] = {1.0e20, 1.0e20, 1.0e20};
     double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
     const bool do_int = integrate && !a.time->ended;
@@ -256,13 +209,13 @@ __global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate
     int nreal = 0, gn = 0;
     double4 xi = make_double4(0, 0, 0, 1), r1i = make_double4(0, 0, 0, 0), r2i = make_double4(0, 0, 0, 1);
     if (live) {
-        nreal = coop_expand<L>(a, g, t, lane, spos);
+        nreal = stored_neighbours(a, t);
         gn = a.gnnbr[t];
         xi = a.rec0[t];
         r1i = a.rec1[t];
         r2i = a.rec2[t];
     }
-    __syncwarp();
+    const unsigned *spos = a.nidx + (size_t)t * a.nstride;
     const int self = (a.prm.disctype == 1) ? 1 : 0;
     const int total = live ? nreal + self + gn : 0;
     const double ihi = 1.0 / xi.w;
@@ -353,7 +306,7 @@ __global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate
         // the mass of the last neighbour of the reference order: the last ghost, else self
         double massj = r2i.z;
         if (live && gn > 0) massj = a.grec2[a.gnbr[(size_t)(gn - 1) * a.npad + t]].z;
-        else if (live && !self && nreal > 0) massj = a.rec2[spos[nreal - 1]].z;
+        else if (live && !self && nreal > 0) massj = a.rec2[spos[nreal - 1] & kPosMask].z;
 #pragma unroll
         for (int n = 0; n < 3; ++n)
 #pragma unroll
@@ -385,14 +338,10 @@ __global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate
         const double mass = f[FMASS][i], vabs = f[FVABS][i];
         const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),
                                 mass * fabs(f[FVY][i]), mass * fabs(f[FVZ][i])};
-        if (mati <= 4) {
+        if (mati == 1) {
 #pragma unroll
-            for (int m = 0; m < 4; ++m)
-                if (mati == m + 1)
-#pragma unroll
-                    for (int c = 0; c < 5; ++c) e_acc[m][c] += vals[c];
+            for (int c = 0; c < 5; ++c) e1[c] += vals[c];
         } else {
-            // materials 5..16: rare; accumulated straight into this block's partials
             for (int c = 0; c < 5; ++c) atomicAdd(&a.red[(size_t)blockIdx.x * (5 * nm + 6) + 5 * (mati - 1) + c], vals[c]);
         }
         if (do_int) {
@@ -406,13 +355,13 @@ __global__ void __launch_bounds__(256) k_momentum_coop(StepArgs a, int integrate
     }
     const int stride = 5 * nm + 6;
     double *out = a.red + (size_t)blockIdx.x * stride;
-    for (int m = 1; m <= nm && m <= 4; ++m) {
+    {
         double v[5];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) v[c] = block_sum(e_acc[m - 1][c], sm);
+        for (int c = 0; c < 5; ++c) v[c] = block_sum(e1[c], sm);
         if (threadIdx.x == 0)
 #pragma unroll
-            for (int c = 0; c < 5; ++c) out[5 * (m - 1) + c] = v[c];
+            for (int c = 0; c < 5; ++c) out[c] = v[c];
     }
     if (do_int) {
         for (int d = 0; d < 3; ++d) {

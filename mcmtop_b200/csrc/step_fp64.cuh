@@ -810,9 +810,8 @@ void launch_strain(const StepArgs &a, cudaStream_t s) {
     constexpr int L = kCoopLanes;
     const int per = 256 / L;
     const int blocks = coop_blocks(a.n, per);
-    const size_t smem = coop_smem<L>(a, 256);
-    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, 256, smem, s>>>(a);
-    else k_strain_coop<L, 1><<<blocks, 256, smem, s>>>(a);
+    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, 256, 0, s>>>(a);
+    else k_strain_coop<L, 1><<<blocks, 256, 0, s>>>(a);
 #endif
 }
 
@@ -836,10 +835,9 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
     constexpr int L = kCoopLanes;
     const int per = 256 / L;
     const int blocks = coop_blocks(a.n, per);
-    const size_t smem = coop_smem<L>(a, 256);
-    if (a.nmat > 4) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
-    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, 256, smem, s>>>(a, integrate);
-    else k_momentum_coop<L, 1><<<blocks, 256, smem, s>>>(a, integrate);
+    if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
+    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, 256, 0, s>>>(a, integrate);
+    else k_momentum_coop<L, 1><<<blocks, 256, 0, s>>>(a, integrate);
     return blocks;
 #endif
 }

@@ -11,14 +11,17 @@
 //
 // Cell-relative positions: the gather records hold each particle's position
 // relative to the origin of its cell (FP32, |offset| < one cell), and every
-// neighbour entry carries the offset of the neighbour's cell from the
-// particle's (-1, 0, 1 per axis), so x_i - x_j = (r_i - r_j) - db * cell size
-// is formed from small numbers and keeps FP32 relative accuracy at the scale
-// of h.  Ghost neighbours (few, near the planes) use FP64 positions.
+// neighbour-list entry carries the offset of the neighbour's cell from the
+// particle's (its 5-bit cell code), so x_i - x_j = (r_i - r_j) - db * cell
+// size is formed from small numbers and keeps FP32 relative accuracy at the
+// scale of h.  Ghost neighbours (few, near the planes) use FP64 positions.
 //
-// Compensated sums: each lane accumulates its neighbours with Kahan
-// summation, and the lanes' partial sums are combined with an error-free
-// (TwoSum) shuffle reduction.
+// Compensated sums: 16 lanes share one particle's neighbours, so a lane
+// adds at most ceil(K/16) terms (about 5) in plain FP32; the 16 partial sums
+// are then combined with an error-free TwoSum shuffle tree that carries the
+// rounding error of every addition, and the result is rounded once to FP64.
+// Per-lane Kahan sums would cost four operations per term for no gain on
+// five-term sums.
 #include "nbr_iter.cuh"
 
 namespace mcm {
@@ -30,18 +33,10 @@ constexpr float kPiF = 3.14159265358979f;
 __device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
 
 // ------------------------------------------------------- compensated sums
-struct KSum {
-    float s, c;
-};
-__device__ __forceinline__ void kadd(KSum &k, float y) {
-    const float yy = y - k.c;
-    const float t = k.s + yy;
-    k.c = (t - k.s) - yy;
-    k.s = t;
-}
-// error-free sum of the L lanes' (s, c) pairs; every lane gets the result
-__device__ __forceinline__ double ksum_reduce(KSum k) {
-    float s = k.s, c = -k.c;
+// Sum of one value per lane over the L lanes of a sub-warp, every addition
+// error-free transformed (TwoSum) and the errors added up; every lane gets it.
+__device__ __forceinline__ double lane_sum(float s) {
+    float c = 0.0f;
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) {
         const float s2 = __shfl_xor_sync(0xffffffffu, s, o, L);
@@ -71,57 +66,38 @@ __device__ __forceinline__ Frame make_frame(const DevGrid &g) {
     }
     return fr;
 }
-__device__ __forceinline__ void cell_origin(const Frame &fr, int key, double o[3]) {
+__device__ __forceinline__ void frame_origin(const Frame &fr, int key, double o[3]) {
     if (key < 0) { o[0] = o[1] = o[2] = 0.0; return; }
     int b[3];
     cell_coords(key, fr.gl, b[0], b[1], b[2]);
     for (int d = 0; d < 3; ++d) o[d] = fr.gmin[d] + (double)(b[d] - 1) * fr.cs[d];
 }
 
-// Expands position t's list into spos: entry = position | (dbx+1)<<26 | (dby+1)<<28 | (dbz+1)<<30.
-__device__ __forceinline__ int expand_cells(const StepArgs &a, const DevGrid &g, int t, int lane, unsigned *spos) {
-    const int key = a.ckey[t];
-    if (key < 0) return 0;
-    const int np = a.npad;
-    int bx, by, bz;
-    cell_coords(key, g.gridlim, bx, by, bz);
-    const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
-    const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
-    const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
-    int base = 0;
-    const int passes = a.nmat > 1 ? 2 : 1;
-    for (int pass = 0; pass < passes; ++pass) {
-        const unsigned long long hdr = a.nhdr[(size_t)pass * np + t];
-        int r = 0;
-        for (int nz = lo2; nz <= hi2; ++nz) {
-            for (int my = lo1; my <= hi1; ++my, ++r) {
-                const int cnt = (int)((hdr >> (7 * r)) & 127ull);
-                if (cnt == 0) continue;
-                const int k0 = (int)cell_key(lo0, my, nz, g.gridlim);
-                const int rs = a.cell_start[k0];
-                const int b1 = a.cell_start[k0 + 1];
-                const int b2 = (hi0 - lo0 >= 2) ? a.cell_start[k0 + 2] : 0x7fffffff;
-                const unsigned dyz = ((unsigned)(my - by + 1) << 28) | ((unsigned)(nz - bz + 1) << 30);
-                for (int c = lane; c < cnt; c += L) {
-                    const int k = base + c;
-                    const unsigned w = a.nlist[(size_t)(k >> 2) * np + t];
-                    const int p = rs + (int)((w >> (8 * (k & 3))) & 255u);
-                    const int xoff = (p >= b1) + (p >= b2);
-                    spos[k] = (unsigned)p | ((unsigned)(lo0 + xoff - bx + 1) << 26) | dyz;
-                }
-                base += cnt;
-            }
-        }
+// Offsets of the 27 neighbour cells (cell size times -1, 0, 1 per axis), by code.
+__device__ __forceinline__ void fill_offsets(float4 *tab, const Frame &fr) {
+    if (threadIdx.x < 27) {
+        const int c = threadIdx.x;
+        tab[c] = make_float4((float)(c % 3 - 1) * fr.csf[0], (float)((c / 3) % 3 - 1) * fr.csf[1],
+                             (float)(c / 9 - 1) * fr.csf[2], 0.0f);
     }
-    return base;
 }
 
-__device__ __forceinline__ void unpack(unsigned e, const Frame &fr, int &p, float &ox, float &oy, float &oz) {
-    p = (int)(e & 0x3ffffffu);
-    ox = (float)((int)((e >> 26) & 3u) - 1) * fr.csf[0];
-    oy = (float)((int)((e >> 28) & 3u) - 1) * fr.csf[1];
-    oz = (float)((int)((e >> 30) & 3u) - 1) * fr.csf[2];
+// Gather records.  A strain record is 32 bytes {x, y, z, h, vx, vy, vz, V}
+// and a momentum record 48 bytes {x, y, z, h, s11, s22, s33, s12 | s13, s23,
+// m, rho} in a 64-byte slot, so that one neighbour costs one (strain) or two
+// (momentum) 32-byte sectors, each fetched by a single 256-bit or 128-bit load.
+struct __align__(32) Rec8 {
+    float4 a, b;
+};
+__device__ __forceinline__ Rec8 ld_rec8(const float4 *p) {
+    Rec8 r;
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w), "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z),
+                   "=f"(r.b.w)
+                 : "l"(p));
+    return r;
 }
+__device__ __forceinline__ float4 ld_rec4(const float4 *p) { return __ldg(p); }
 
 // Cubic B-spline gradient in FP32 (MCM/mcm_gradw.f90:341-381), ih = 1/havg.
 __device__ __forceinline__ void gradw_f(float x0, float x1, float x2, float ih, float &d0, float &d1, float &d2) {
@@ -158,11 +134,11 @@ __global__ void k_strain_prep(StepArgs a) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
         const int i = a.cell_list[p];
         double o[3];
-        cell_origin(fr, a.ckey[p], o);
+        frame_origin(fr, a.ckey[p], o);
         const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
         const double xs = f[FX][i] - 0.5 * vx * dt, ys = f[FY][i] - 0.5 * vy * dt, zs = f[FZ][i] - 0.5 * vz * dt;
-        a.frec0[p] = make_float4((float)(xs - o[0]), (float)(ys - o[1]), (float)(zs - o[2]), (float)f[FH][i]);
-        a.frec1[p] = make_float4((float)vx, (float)vy, (float)vz, (float)(f[FMASS][i] / f[FRHO][i]));
+        a.frec0[2 * (size_t)p] = make_float4((float)(xs - o[0]), (float)(ys - o[1]), (float)(zs - o[2]), (float)f[FH][i]);
+        a.frec0[2 * (size_t)p + 1] = make_float4((float)vx, (float)vy, (float)vz, (float)(f[FMASS][i] / f[FRHO][i]));
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -174,16 +150,17 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 // ----------------------------------------------------------- strain rate
-// MCM/mcm_oldstrain.f90:95-124 with FP32 pair sums (Kahan per lane).
-__global__ void __launch_bounds__(256) k_strain(StepArgs a) {
-    extern __shared__ unsigned smem_u[];
+// MCM/mcm_oldstrain.f90:95-124 with FP32 pair sums.
+__global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
+    __shared__ float4 offs[27];
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     const int per = blockDim.x / L;
     const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
-    unsigned *spos = smem_u + sub * (a.nwords * 4);
     const DevGrid g = *a.grid;
     const Frame fr = make_frame(g);
+    fill_offsets(offs, fr);
+    __syncthreads();
     const double dt = a.time->dt;
     for (int round = 0; round < rounds; ++round) {
         const int t = (round * gridDim.x + blockIdx.x) * per + sub;
@@ -191,13 +168,14 @@ __global__ void __launch_bounds__(256) k_strain(StepArgs a) {
         int nreal = 0, gn = 0, i = 0;
         float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), vi = make_float4(0.f, 0.f, 0.f, 0.f);
         if (live) {
-            nreal = expand_cells(a, g, t, lane, spos);
+            nreal = a.nnbr[t];
             gn = a.gnnbr[t];
-            xi = a.frec0[t];
-            vi = a.frec1[t];
+            const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)t);
+            xi = r.a;
+            vi = r.b;
             i = a.cell_list[t];
         }
-        __syncwarp();
+        const unsigned *spos = a.nidx + (size_t)t * a.nstride;
         double xs[3] = {0.0, 0.0, 0.0};
         if (live && gn > 0) {
             xs[0] = a.F.f[FX][i] - 0.5 * a.F.f[FVX][i] * dt;
@@ -206,21 +184,21 @@ __global__ void __launch_bounds__(256) k_strain(StepArgs a) {
         }
         const int total = live ? nreal + gn : 0;
         const float ihi = 1.0f / xi.w;
-        KSum gv[9];
+        float gv[9];
 #pragma unroll
-        for (int u = 0; u < 9; ++u) gv[u] = KSum{0.f, 0.f};
+        for (int u = 0; u < 9; ++u) gv[u] = 0.0f;
         for (int k = lane; k < total; k += L) {
             float dx, dy, dz, hj;
             float4 vj;
             if (k < nreal) {
-                int p;
-                float ox, oy, oz;
-                unpack(spos[k], fr, p, ox, oy, oz);
-                const float4 xj = a.frec0[p];
-                vj = a.frec1[p];
-                dx = (xi.x - xj.x) - ox;
-                dy = (xi.y - xj.y) - oy;
-                dz = (xi.z - xj.z) - oz;
+                const unsigned e = spos[k];
+                const float4 o = offs[e >> 26];
+                const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)(e & kPosMask));
+                const float4 xj = r.a;
+                vj = r.b;
+                dx = (xi.x - xj.x) - o.x;
+                dy = (xi.y - xj.y) - o.y;
+                dz = (xi.z - xj.z) - o.z;
                 hj = xj.w;
             } else {
                 const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
@@ -234,13 +212,13 @@ __global__ void __launch_bounds__(256) k_strain(StepArgs a) {
             float d0, d1, d2;
             gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
             const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
-            kadd(gv[0], t0 * d0); kadd(gv[1], t0 * d1); kadd(gv[2], t0 * d2);
-            kadd(gv[3], t1 * d0); kadd(gv[4], t1 * d1); kadd(gv[5], t1 * d2);
-            kadd(gv[6], t2 * d0); kadd(gv[7], t2 * d1); kadd(gv[8], t2 * d2);
+            gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
+            gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
+            gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
         }
         double r[9];
 #pragma unroll
-        for (int u = 0; u < 9; ++u) r[u] = ksum_reduce(gv[u]);
+        for (int u = 0; u < 9; ++u) r[u] = lane_sum(gv[u]);
         if (live && lane == 0) {
             // MCM/mcm_oldstrain.f90:117-124
             double *const *f = a.F.f;
@@ -271,15 +249,16 @@ __global__ void k_mom_prep(StepArgs a) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
         const int i = a.cell_list[p];
         double o[3];
-        cell_origin(fr, a.ckey[p], o);
+        frame_origin(fr, a.ckey[p], o);
         const double rho = f[FRHO][i];
         const double ir2 = 1.0 / (rho * rho);
         const double q = f[FQ][i];
-        a.frec0[p] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]),
-                                 (float)f[FH][i]);
-        a.frec1[p] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
+        float4 *rec = a.frec0 + 4 * (size_t)p;
+        rec[0] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]),
+                             (float)f[FH][i]);
+        rec[1] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
                                  (float)((f[FS33][i] - q) * ir2), (float)(f[FS12][i] * ir2));
-        a.frec2[p] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
+        rec[2] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -364,16 +343,17 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // MCM/mcm_oldacceleration.f90:66-89 with FP32 pair sums, then the FP64 tail:
 // base acceleration and displacement BCs (MCM/mcm_boundcond.f90), energy
 // partials (MCM/mcm_calctotale.f90) and, when integrating, the update.
-__global__ void __launch_bounds__(256) k_momentum(StepArgs a, int integrate_flag) {
-    extern __shared__ unsigned smem_u[];
+__global__ void __launch_bounds__(256, 3) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
+    __shared__ float4 offs[27];
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     const int per = blockDim.x / L;
     const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
-    unsigned *spos = smem_u + sub * (a.nwords * 4);
     const DevGrid g = *a.grid;
     const Frame fr = make_frame(g);
+    fill_offsets(offs, fr);
+    __syncthreads();
     const int nm = a.nmat;
     double e1[5] = {0, 0, 0, 0, 0};   // sums of material 1; others go to the partials directly
     double xlo[3] = {1.0e20, 1.0e20, 1.0e20}, xhi[3] = {-1.0e20, -1.0e20, -1.0e20};
@@ -385,32 +365,34 @@ __global__ void __launch_bounds__(256) k_momentum(StepArgs a, int integrate_flag
         float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), r1i = make_float4(0.f, 0.f, 0.f, 0.f),
                r2i = make_float4(0.f, 0.f, 0.f, 1.f);
         if (live) {
-            nreal = expand_cells(a, g, t, lane, spos);
+            nreal = a.nnbr[t];
             gn = a.gnnbr[t];
-            xi = a.frec0[t];
-            r1i = a.frec1[t];
-            r2i = a.frec2[t];
+            const Rec8 r = ld_rec8(a.frec0 + 4 * (size_t)t);
+            xi = r.a;
+            r1i = r.b;
+            r2i = ld_rec4(a.frec0 + 4 * (size_t)t + 2);
             i = a.cell_list[t];
         }
-        __syncwarp();
+        const unsigned *spos = a.nidx + (size_t)t * a.nstride;
         double xa[3] = {0.0, 0.0, 0.0};
         if (live && gn > 0) { xa[0] = a.F.f[FX][i]; xa[1] = a.F.f[FY][i]; xa[2] = a.F.f[FZ][i]; }
         const int total = live ? nreal + gn : 0;
         const float ihi = 1.0f / xi.w;
-        KSum acc[3] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        float acc[3] = {0.0f, 0.0f, 0.0f};
         for (int k = lane; k < total; k += L) {
             float dx, dy, dz, hj;
             float4 r1, r2;
             if (k < nreal) {
-                int p;
-                float ox, oy, oz;
-                unpack(spos[k], fr, p, ox, oy, oz);
-                const float4 xj = a.frec0[p];
-                r1 = a.frec1[p];
-                r2 = a.frec2[p];
-                dx = (xi.x - xj.x) - ox;
-                dy = (xi.y - xj.y) - oy;
-                dz = (xi.z - xj.z) - oz;
+                const unsigned e = spos[k];
+                const float4 o = offs[e >> 26];
+                const size_t p = e & kPosMask;
+                const Rec8 r = ld_rec8(a.frec0 + 4 * p);
+                const float4 xj = r.a;
+                r1 = r.b;
+                r2 = ld_rec4(a.frec0 + 4 * p + 2);
+                dx = (xi.x - xj.x) - o.x;
+                dy = (xi.y - xj.y) - o.y;
+                dz = (xi.z - xj.z) - o.z;
                 hj = xj.w;
             } else {
                 const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
@@ -427,13 +409,14 @@ __global__ void __launch_bounds__(256) k_momentum(StepArgs a, int integrate_flag
             const float s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
             const float s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
             const float mj = r2.z;
-            kadd(acc[0], mj * (s11 * d0 + s12 * d1 + s13 * d2));
-            kadd(acc[1], mj * (s12 * d0 + s22 * d1 + s23 * d2));
-            kadd(acc[2], mj * (s13 * d0 + s23 * d1 + s33 * d2));
+            d0 *= mj; d1 *= mj; d2 *= mj;
+            acc[0] = fmaf(s11, d0, fmaf(s12, d1, fmaf(s13, d2, acc[0])));
+            acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(s23, d2, acc[1])));
+            acc[2] = fmaf(s13, d0, fmaf(s23, d1, fmaf(s33, d2, acc[2])));
         }
         double ac[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ac[c] = ksum_reduce(acc[c]);
+        for (int c = 0; c < 3; ++c) ac[c] = lane_sum(acc[c]);
         if (live && lane == 0) {
             double *const *f = a.F.f;
             if (a.prm.baseaccel)
@@ -488,7 +471,6 @@ __global__ void __launch_bounds__(256) k_momentum(StepArgs a, int integrate_flag
 }
 
 // ------------------------------------------------------------ launchers
-static size_t smem_bytes(const StepArgs &a) { return sizeof(unsigned) * (size_t)(256 / L) * (a.nwords * 4); }
 
 void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
     int n = a.n > a.ghost_cap ? a.n : a.ghost_cap;
@@ -497,7 +479,7 @@ void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 void launch_strain(const StepArgs &a, cudaStream_t s) {
-    k_strain<<<coop_blocks(a.n, 256 / L), 256, smem_bytes(a), s>>>(a);
+    k_strain<<<coop_blocks(a.n, 256 / L), 256, 0, s>>>(a);
 }
 
 void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
@@ -509,7 +491,7 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
     const int blocks = coop_blocks(a.n, 256 / L);
     if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
-    k_momentum<<<blocks, 256, smem_bytes(a), s>>>(a, integrate_flag);
+    k_momentum<<<blocks, 256, 0, s>>>(a, integrate_flag);
     return blocks;
 }
 

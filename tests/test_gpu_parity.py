@@ -228,3 +228,19 @@ def test_reordering_does_not_change_results(lib, disctype):
     for f in STATE:
         assert np.array_equal(ga[f], gb[f]), f
     compare_neighbours(b, orc)
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64_EXACT, _abi.PREC_MIXED])
+def test_search_prefilter_without_diagnostics(lib, precision):
+    """With diagnostics off (and tcrit_opt 1) the search accepts clear
+    neighbours from the FP32 test alone; the sets must still be the oracle's."""
+    deck = taylor_bar(dx=0.4e-3)
+    sol = Solver(deck, precision)
+    sol.set_diagnostics(False)
+    orc = Oracle(deck, openmp=True)
+    for _ in range(5):
+        sol.step()
+        orc.step()
+    if precision == _abi.PREC_FP64_EXACT:
+        compare(sol, orc, STATE, 1e-11, "prefiltered search")
+    compare_neighbours(sol, orc)
