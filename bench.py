@@ -9,12 +9,15 @@ position update) over every particle.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|exact|mixed]
   python bench.py --impl reference ...   # the CPU restatement on the host cores
 
-value: particle-steps/s of the fused device loop (mcm_gpu_run), device time
-from CUDA events on the library's stream, max over ranks.  e2e: the same
-metric through the split C-ABI entry points a Fortran driver calls
-(mcm_gpu_upload, step_a/b/c per step with host dt logic, mcm_gpu_download),
-host buffers, wall clock.  Each rank owns one independent bar (weak scaling,
-no data-path collective).
+value: particle-steps/s of the fused device loop (mcm_gpu_run) in the
+headline precision (mixed: FP32 pair sums, FP64 state), device time from CUDA
+events on the library's stream, max over ranks.  The plain FP64 step is timed
+the same way on the same bar ("fp64"), and the per-field difference between
+the two end states is reported ("accuracy").  e2e: the headline metric
+through the split C-ABI entry points a Fortran driver calls (mcm_gpu_upload,
+step_a/b/c per step with host dt logic, mcm_gpu_download), host buffers,
+wall clock.  Each rank owns one independent bar (weak scaling, no data-path
+collective).
 """
 from __future__ import annotations
 
@@ -43,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "exact", "mixed"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 run next to the mixed one")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -113,26 +117,24 @@ class ClockSampler:
 # --------------------------------------------------------------- roofline
 def algorithmic_bytes(region: str, kbar: float, precision: str) -> float:
     """Compulsory bytes per particle of one kernel group: the particle's own
-    state read and written plus its neighbour list (16-byte header of per-row
-    counts and one byte per neighbour), with ideal caching of the neighbour
-    gathers (they count zero, as do sorts and intermediates).  Field lists:
-      search:       read x(3) h mat; write header, count, list      36 + 4 + 4 + 16 + K
-      strain:       read x(3) v(3) m rho h, header, list            72 + 16 + K
-      constitutive: read x v (6) m h rho e p c efps pcut fail sigma(6), vabs;
-                    write x(3) h rho e p c efps sigma(6) q          168 + 8 + 120
-      momentum:     read x v (6) m rho h sigma(6) q e vabs dispbc, count, header, list;
-                    write x v (6) vabs                             144 + 8 + 16 + K + 56
-    The mixed path keeps x and v (and the energy/timestep sums) in FP64 and
-    the other fields in FP32."""
-    w = 4 if precision == "mixed" else 8
+    state read and written plus its neighbour list (4-byte entries), with
+    ideal caching of the neighbour gathers (they count zero, as do sorts,
+    gather records and other intermediates).  All state is FP64 in both
+    precisions (the mixed path differs in its pair arithmetic).
+      search:       read x(3) h mat; write count, list                 36 + 4 + 4K
+      strain:       read x(3) v(3) m rho h, count, list                 72 + 4 + 4K
+      constitutive: read v(3) m h rho e p c efps pcut fail sigma(6) rod(6) spin(3) tr vabs;
+                    write x(3) rho e p c efps pcut sigma(6) q          224 + 8 + 136
+      momentum:     read x v (6) m rho h sigma(6) q e vabs dispbc, count, list;
+                    write x v (6) vabs                                 136 + 4 + 4 + 4K + 56"""
     if region == "search":
-        return 3 * 8 + w + 4 + 4 + 16 + kbar
+        return 36 + 4 + 4 * kbar
     if region == "strain":
-        return 6 * 8 + 3 * w + 16 + kbar
+        return 72 + 4 + 4 * kbar
     if region == "constitutive":
-        return 6 * 8 + 14 * w + 8 + 3 * 8 + 12 * w
+        return 224 + 8 + 136
     if region == "momentum_integrate":
-        return 6 * 8 + 12 * w + 4 + 4 + 16 + kbar + 6 * 8 + 8
+        return 136 + 4 + 4 + 4 * kbar + 56
     return 0.0
 
 
@@ -244,6 +246,45 @@ def gpu_arm(args):
                 "launch_ms": round(per_launch_s * 1e3, 4)}
     kernels = {k: {"ms_per_step": round(v[0] / args.steps, 4), "launches": v[1]} for k, v in report.items() if v[1]}
 
+    # the plain FP64 step on the same bar, same steps; per-field difference of the end states
+    fp64 = None
+    accuracy = None
+    if args.precision == "mixed" and not args.no_compare:
+        ref = Solver(deck, _abi.PREC_FP64, device=local, reorder_interval=args.reorder)
+        ref.set_diagnostics(False)
+        ref.run(args.warmup)
+        barrier()
+        ref.timer_start()
+        done64 = ref.run(args.steps)
+        ms64 = ref.timer_stop()
+        if ws > 1:
+            import torch.distributed as dist
+
+            t64 = torch.tensor([ms64], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t64, op=dist.ReduceOp.MAX)
+            ms64 = float(t64.item())
+        if done64 != args.steps:
+            raise RuntimeError(f"FP64 run stopped after {done64} of {args.steps} steps")
+        v64 = ws * deck.np * args.steps / (ms64 / 1e3)
+        fp64 = {"value": round(v64, 1), "ms_per_step": round(ms64 / args.steps, 4),
+                "mixed_over_fp64": round(value / v64, 3)}
+        if rank == 0:
+            fields = ["x", "v", "rho", "e", "p", "c", "efps", "sigma", "q", "vabs"]
+            a_ = sol.download(fields)
+            b_ = ref.download(fields)
+            err = {}
+            for f in fields:
+                scale = float(np.max(np.abs(b_[f])))
+                err[f] = float(np.max(np.abs(a_[f] - b_[f])) / scale) if scale > 0 else float(np.max(np.abs(a_[f])))
+            la = a_["x"][:, 2].max() - a_["x"][:, 2].min()
+            lb = b_["x"][:, 2].max() - b_["x"][:, 2].min()
+            accuracy = {"against": "FP64 GPU step (itself within 1e-9 of the FP64 oracle in the parity tests)",
+                        "steps": args.warmup + args.steps, "norm": "max |mixed - fp64| / max |fp64| per field",
+                        "max_rel_err": {k: float(f"{v:.3e}") for k, v in err.items()},
+                        "worst": float(f"{max(err.values()):.3e}"),
+                        "length_rel_diff": float(f"{abs(la - lb) / lb:.3e}")}
+        ref.close()
+
     # end to end through the split C ABI with host buffers (rank 0 only)
     e2e = None
     if rank == 0 and not args.no_e2e:
@@ -290,7 +331,7 @@ def gpu_arm(args):
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
                    "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "kernels": kernels,
+        "fp64": fp64, "accuracy": accuracy, "kernels": kernels,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
