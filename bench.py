@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "exact", "mixed"])
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 run next to the mixed one")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
+    ap.add_argument("--adj-dx", type=float, default=0.2e-3, help="particle spacing of the differentiated bar")
+    ap.add_argument("--adj-steps", type=int, default=400)
+    ap.add_argument("--adj-every", type=int, default=50, help="checkpoint interval")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -174,6 +178,61 @@ def cpu_oracle(deck, budget_s: float, max_steps: int):
     orc.close()
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return deck.np * steps / el, steps, el, cores
+
+
+# ------------------------------------------------------------ adjoint cost
+def adjoint_cost(args, local):
+    """Gradient of a final-state function through the whole run against the
+    forward run: the differentiated Taylor bar (FP64, prescribed dt schedule
+    recorded from a nominal run, checkpoints every --adj-every steps).  All
+    times are wall clock around synchronous ABI calls."""
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.deck import taylor_bar
+    from mcmtop_b200.solver import Solver
+
+    deck = taylor_bar(dx=args.adj_dx)
+    nsteps = args.adj_steps
+    rec = Solver(deck, _abi.PREC_FP64, device=local)
+    rec.set_diagnostics(False)
+    dts = [rec.dt]
+    for _ in range(nsteps):
+        rec.step_a()
+        rec.dt_update()
+        dts.append(rec.dt)
+        rec.step_b()
+        rec.step_c()
+    rec.close()
+    fwd = Solver(deck, _abi.PREC_FP64, device=local)
+    fwd.set_diagnostics(False)
+    fwd.run(3)
+    fwd.close()
+    fwd = Solver(deck, _abi.PREC_FP64, device=local)
+    fwd.set_diagnostics(False)
+    t0 = time.perf_counter()
+    done = fwd.run(nsteps)
+    t_fwd = time.perf_counter() - t0
+    fwd.close()
+    sol = Solver(deck, _abi.PREC_FP64, device=local)
+    t0 = time.perf_counter()
+    sol.adjoint_forward(dts, args.adj_every)
+    t_ckpt = time.perf_counter() - t0
+    x = sol.download(["x"])["x"]
+    xbar = np.zeros_like(x)
+    z = x[:, 2]
+    xbar[int(z.argmax()), 2] += 1.0   # d(final length)
+    xbar[int(z.argmin()), 2] -= 1.0
+    t0 = time.perf_counter()
+    pb, _, _ = sol.adjoint_backward(xbar, None)
+    t_bwd = time.perf_counter() - t0
+    sol.close()
+    return {"workload": f"taylor_bar_{deck.np}", "steps": nsteps, "forward_steps_done": done,
+            "checkpoint_every": args.adj_every, "precision": "fp64",
+            "forward_s": round(t_fwd, 4), "forward_with_checkpoints_s": round(t_ckpt, 4),
+            "backward_s": round(t_bwd, 4), "adj_over_fwd": round((t_ckpt + t_bwd) / t_fwd, 3),
+            "backward_over_fwd": round(t_bwd / t_fwd, 3),
+            "dlength_dparams": {"G": float(pb[0][0]), "yield": float(pb[0][1]), "hardening": float(pb[0][2]),
+                                "eos_s": float(pb[0][3])},
+            "note": "forward = fused mcm_gpu_run; gradient = checkpointed forward + reverse sweep"}
 
 
 # ----------------------------------------------------------------- GPU arm
@@ -314,6 +373,10 @@ def gpu_arm(args):
                "d2h_bytes_per_step": int(d2h_bytes / k_e2e + per_step_d2h),
                "steps": k_e2e, "path": "mcm_gpu_upload + (step_a, host dt, step_b, step_c) x K + mcm_gpu_download"}
 
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        adjoint = adjoint_cost(args, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, n, el, cores = cpu_oracle(deck, args.cpu_budget, 3)
@@ -331,7 +394,7 @@ def gpu_arm(args):
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
                    "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "fp64": fp64, "accuracy": accuracy, "kernels": kernels,
+        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "kernels": kernels,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

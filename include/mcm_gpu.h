@@ -63,9 +63,11 @@ typedef enum {
 typedef enum {
     MCM_PREC_FP64_EXACT = 0,   /* FP64, no fused multiply-add, reference accumulation order */
     MCM_PREC_FP64 = 1,         /* FP64 with fused multiply-add */
-    MCM_PREC_MIXED = 2         /* FP32 pair sums with Kahan compensation and FP32 constitutive
-                                  update on cell-relative positions; FP64 position/velocity
-                                  integration, energy and critical-timestep reductions */
+    MCM_PREC_MIXED = 2         /* FP32 strain-rate and momentum pair sums on cell-relative
+                                  positions, lane sums combined by error-free (TwoSum)
+                                  reduction; FP64 state, constitutive update, position/velocity
+                                  integration, energy and critical-timestep reductions
+                                  (disctype 0) */
 } mcm_gpu_precision;
 
 /* One material, as the reference holds it after mcm_matin, the mcm_sets routines and mcm_calcg:
@@ -211,6 +213,32 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
 int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const double *v, const double *e,
                                const int *mat, int np, int nmat, double *energies, void *stream);
 
+/* ------------------------------------------------------------- adjoint */
+
+/* No counterpart in the reference (it has no differentiation).  Reverse-mode
+ * gradients of a function of the final state with respect to the initial
+ * state and to the material parameters, through the whole step: FP64
+ * precisions, disctype 0, every material model 10 with EOS 41,
+ * reorder_interval 0.  The dt schedule is an input (the critical-timestep
+ * minimum is not differentiated) and each step's neighbour lists are frozen
+ * at their forward values.
+ *
+ * mcm_gpu_adjoint_forward runs nsteps loop iterations from the current state
+ * with step_a(dts[n]), dt update to dts[n+1], step_b, step_c (dts has
+ * nsteps+1 entries; dts[0] is the dt of the first step_a, normally the one
+ * mcm_gpu_initialise returned) and keeps a full-state checkpoint every
+ * checkpoint_every steps.  mcm_gpu_adjoint_backward takes the adjoints of the
+ * final x and v (Fortran (3,np) layout; NULL = zero), recomputes each
+ * checkpoint segment forward and runs the reverse steps backwards, and
+ * returns dL/dx and dL/dv of the initial state (xbar0, vbar0, (3,np)) and, in
+ * param_bar[nmat][4], dL/d(strinput[0] = G, strinput[1] = yield stress,
+ * strinput[2] = hardening modulus, eosinput[1] = Mie-Grueneisen slope s) of
+ * each material, in the card's units.  The device state is left as the
+ * forward run left it. */
+int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, int checkpoint_every);
+int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double *vbar, double *param_bar,
+                             double *xbar0, double *vbar0);
+
 /* ----------------------------------------------------------- measurement */
 
 /* Diagnostic fields (rod, spin, tracerod, etry, einc, rhoold, critts, s, a)
@@ -222,7 +250,7 @@ int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable);
  * (enable = 1) and resets the launch counter.  The reference has no profiler;
  * its only timing is the commented-out MCM/mcm_write_timings.f90. */
 int mcm_gpu_profile(mcm_gpu_handle *h, int enable);
-/* Device time and launches of kernel group `region` (0..10) since
+/* Device time and launches of kernel group `region` (0..14) since
  * mcm_gpu_profile; returns MCM_EINVAL past the last group. */
 int mcm_gpu_profile_report(mcm_gpu_handle *h, int region, char *name, int name_len, double *total_ms,
                            int *launches);

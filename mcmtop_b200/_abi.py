@@ -117,6 +117,8 @@ def load() -> C.CDLL:
         "mcm_gpu_profile_report": ([H, C.c_int, C.c_char_p, C.c_int, _DP, _IP], C.c_int),
         "mcm_gpu_kernel_launches": ([H], C.c_longlong),
         "mcm_gpu_timer": ([H, C.c_int, _DP], C.c_int),
+        "mcm_gpu_adjoint_forward": ([H, C.c_int, _DP, C.c_int], C.c_int),
+        "mcm_gpu_adjoint_backward": ([H, _DP, _DP, _DP, _DP, _DP], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

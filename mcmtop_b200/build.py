@@ -30,8 +30,9 @@ UNITS = [
     ("step_fp64_fast.cu", True),
     ("step_mixed.cu", True),
     ("noalloc.cu", False),
+    ("adjoint.cu", False),
 ]
-HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh", "dual.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -51,6 +51,15 @@ struct mcm_gpu_handle {
     cudaEvent_t timer[2] = {nullptr, nullptr};
     long long steps_enqueued = 0;
     bool have_cells = false;   // cell_list holds a valid permutation
+    // adjoint: prescribed dt schedule, checkpoints (fields + bbox), segment snapshots
+    std::vector<double> adj_dts;
+    int adj_steps = 0, adj_every = 0;
+    std::vector<double *> adj_ckpt;
+    double *adj_seg = nullptr;
+    int adj_seg_cap = 0;
+    double *adj_final = nullptr;
+    double *d_adj = nullptr;     // adjoint arrays (40 x npad)
+    double *d_theta = nullptr;   // parameter adjoints (nmat x 4)
 };
 
 namespace {
@@ -81,11 +90,12 @@ inline int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
 // Kernel groups that the profiler times separately.
 enum Region {
     R_CELLS = 0, R_GHOSTS, R_SEARCH, R_STRAIN_PREP, R_STRAIN, R_CONST, R_CRITTS, R_MOM_PREP, R_MOMENTUM,
-    R_REDUCE, R_MOVE, R_MISC, R_NREG
+    R_REDUCE, R_MOVE, R_MISC, R_ADJ_MOM, R_ADJ_CONST, R_ADJ_STRAIN, R_NREG
 };
 const char *kRegionName[R_NREG] = {"cell_list", "ghosts", "search", "strain_prep", "strain", "constitutive",
                                    "critts_dt", "momentum_prep", "momentum_integrate", "energy_bbox_reduce",
-                                   "update_move", "misc"};
+                                   "update_move", "misc", "adjoint_momentum", "adjoint_constitutive",
+                                   "adjoint_strain"};
 
 cudaEvent_t take_event(mcm_gpu_handle *h) {
     if (h->ev_pool.empty()) {
@@ -223,6 +233,7 @@ int alloc_ghosts(mcm_gpu_handle *h, int cap) {
         if ((st = dalloc(h, p, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.gpar, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.gmat, (size_t)cap))) return st;
+    if ((st = dalloc(h, &h->A.gflip, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec0, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec1, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec2, (size_t)cap))) return st;
@@ -614,10 +625,16 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
                     h->A.cpos, h->A.cposf, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
-                    h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat,
+                    h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,
                     h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (double *p : h->adj_ckpt)
+        if (p) cudaFree(p);
+    if (h->adj_seg) cudaFree(h->adj_seg);
+    if (h->adj_final) cudaFree(h->adj_final);
+    if (h->d_adj) cudaFree(h->d_adj);
+    if (h->d_theta) cudaFree(h->d_theta);
     if (h->h_time) cudaFreeHost(h->h_time);
     for (auto &v : h->prof_pairs)
         for (auto &pr : v) { h->ev_pool.push_back(pr.first); h->ev_pool.push_back(pr.second); }
@@ -1229,6 +1246,177 @@ int mcm_gpu_timer(mcm_gpu_handle *h, int op, double *ms) {
 int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable) {
     if (!h) return MCM_EINVAL;
     h->A.prm.diag = enable ? 1 : 0;
+    return MCM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- adjoint
+namespace {
+
+constexpr int kAdjArrays = 40;
+
+size_t snap_doubles(const mcm_gpu_handle *h) { return (size_t)NFIELD * h->npad + 8; }
+
+int snap_save(mcm_gpu_handle *h, double *buf) {
+    CK(cudaMemcpyAsync(buf, h->d_fields, sizeof(double) * NFIELD * h->npad, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(buf + (size_t)NFIELD * h->npad, h->A.bbox, sizeof(double) * 6, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    return MCM_OK;
+}
+int snap_load(mcm_gpu_handle *h, const double *buf) {
+    CK(cudaMemcpyAsync(h->d_fields, buf, sizeof(double) * NFIELD * h->npad, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->A.bbox, buf + (size_t)NFIELD * h->npad, sizeof(double) * 6, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    return MCM_OK;
+}
+
+// One loop iteration with the prescribed dt schedule: step_a with dts[n],
+// dt update to dts[n+1], step_b, step_c.
+int adj_step(mcm_gpu_handle *h, int n, bool move) {
+    int st;
+    if ((st = mcm_gpu_step_a(h, h->adj_dts[n], nullptr))) return st;
+    if ((st = mcm_gpu_step_b(h, nullptr))) return st;
+    if (move && (st = mcm_gpu_step_c(h, h->adj_dts[n + 1], h->adj_dts[n], nullptr))) return st;
+    return MCM_OK;
+}
+
+int adj_check(mcm_gpu_handle *h) {
+    if (h->cfg.precision == MCM_PREC_MIXED) return set_error(h, MCM_EUNSUPPORTED, "adjoint: FP64 precisions only");
+    if (h->cfg.disctype != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: disctype 0 only");
+    if (h->cfg.reorder_interval != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: reorder_interval must be 0");
+    for (const mcm_gpu_material &m : h->mats)
+        if (m.model != 10 || m.eos != 41) return set_error(h, MCM_EUNSUPPORTED, "adjoint: model 10 with EOS 41 only");
+    return MCM_OK;
+}
+
+struct DiagOff {
+    mcm_gpu_handle *h;
+    int saved;
+    explicit DiagOff(mcm_gpu_handle *hh) : h(hh), saved(hh->A.prm.diag) { h->A.prm.diag = 0; }
+    ~DiagOff() { h->A.prm.diag = saved; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, int checkpoint_every) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (nsteps <= 0 || !dts || checkpoint_every <= 0) return MCM_EINVAL;
+    if ((st = adj_check(h))) return st;
+    DiagOff diag(h);   // the reverse step reads the strain output, which diagnostics overwrite
+    h->adj_dts.assign(dts, dts + nsteps + 1);
+    h->adj_steps = nsteps;
+    h->adj_every = checkpoint_every;
+    const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+    for (double *p : h->adj_ckpt)
+        if (p) cudaFree(p);
+    h->adj_ckpt.assign(nck, nullptr);
+    const size_t sd = snap_doubles(h);
+    for (int c = 0; c < nck; ++c)
+        if ((st = dalloc(h, &h->adj_ckpt[c], sd))) return st;
+    if ((st = dalloc(h, &h->adj_final, sd))) return st;
+    for (int n = 0; n < nsteps; ++n) {
+        if (n % checkpoint_every == 0 && (st = snap_save(h, h->adj_ckpt[n / checkpoint_every]))) return st;
+        if ((st = adj_step(h, n, true))) return st;
+    }
+    if ((st = snap_save(h, h->adj_final))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    return MCM_OK;
+}
+
+int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double *vbar, double *param_bar,
+                             double *xbar0, double *vbar0) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (h->adj_steps <= 0) return set_error(h, MCM_EINVAL, "adjoint: no forward run recorded");
+    if ((st = adj_check(h))) return st;
+    DiagOff diag(h);
+    const int n = h->np;
+    const size_t np = h->npad;
+    if ((st = dalloc(h, &h->d_adj, (size_t)kAdjArrays * np))) return st;
+    CK(cudaMemsetAsync(h->d_adj, 0, sizeof(double) * kAdjArrays * np, h->stream));
+    if ((st = dalloc(h, &h->d_theta, (size_t)h->nmat * adj::kParams))) return st;
+    CK(cudaMemsetAsync(h->d_theta, 0, sizeof(double) * h->nmat * adj::kParams, h->stream));
+    std::vector<int> orig(n);
+    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    adj::AdjArgs b;
+    std::memset(&b, 0, sizeof(b));
+    double *base = h->d_adj;
+    auto arr = [&](int k) { return base + (size_t)k * np; };
+    for (int d = 0; d < 3; ++d) { b.xb[d] = arr(d); b.vb[d] = arr(3 + d); b.ab[d] = arr(16 + d); }
+    b.rhob = arr(6); b.eb = arr(7); b.pb = arr(8); b.efpsb = arr(9);
+    for (int u = 0; u < 6; ++u) { b.sigb[u] = arr(10 + u); b.ysig[u] = arr(23 + u); }
+    b.yrho = arr(19); b.ye = arr(20); b.yp = arr(21); b.yefps = arr(22); b.yq = arr(29); b.rho0b = arr(30);
+    for (int u = 0; u < 9; ++u) b.gb[u] = arr(31 + u);
+    b.theta_b = h->d_theta;
+    // final adjoints, Fortran (3,np) by particle -> state order
+    std::vector<double> tmp(n);
+    for (int d = 0; d < 3; ++d) {
+        if (xbar) {
+            for (int i = 0; i < n; ++i) tmp[i] = xbar[3 * (size_t)orig[i] + d];
+            CK(cudaMemcpy(b.xb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        }
+        if (vbar) {
+            for (int i = 0; i < n; ++i) tmp[i] = vbar[3 * (size_t)orig[i] + d];
+            CK(cudaMemcpy(b.vb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        }
+    }
+    const int every = h->adj_every, nck = (int)h->adj_ckpt.size();
+    const size_t sd = snap_doubles(h);
+    if (h->adj_seg_cap < every) {
+        if ((st = dalloc(h, &h->adj_seg, sd * every))) return st;
+        h->adj_seg_cap = every;
+    }
+    for (int c = nck - 1; c >= 0; --c) {
+        const int n0 = c * every;
+        const int K = std::min(every, h->adj_steps - n0);
+        if ((st = snap_load(h, h->adj_ckpt[c]))) return st;
+        for (int s = 0; s < K; ++s) {
+            if ((st = snap_save(h, h->adj_seg + sd * s))) return st;
+            if (s < K - 1 && (st = adj_step(h, n0 + s, true))) return st;
+        }
+        for (int s = K - 1; s >= 0; --s) {
+            const int m = n0 + s;
+            const double *pre = h->adj_seg + sd * s;
+            if ((st = snap_load(h, pre))) return st;
+            if ((st = adj_step(h, m, false))) return st;   // lists, ghosts, strain, constitutive, momentum
+            for (int f = 0; f < NFIELD; ++f) b.pre[f] = pre + (size_t)f * np;
+            b.dt_prev = h->adj_dts[m];
+            b.dtold = h->adj_dts[m];
+            b.dt = h->adj_dts[m + 1];
+            {
+                Scope sc(h, R_ADJ_MOM, 3);
+                adj::launch_reverse_momentum(h->A, b, h->stream);
+            }
+            {
+                Scope sc(h, R_ADJ_CONST, 1);
+                adj::launch_reverse_constitutive(h->A, b, h->stream);
+            }
+            {
+                Scope sc(h, R_ADJ_STRAIN, 1);
+                adj::launch_reverse_strain(h->A, b, h->stream);
+            }
+            CK(cudaGetLastError());
+        }
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; ++d) {
+        if (xbar0) {
+            CK(cudaMemcpy(tmp.data(), b.xb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; ++i) xbar0[3 * (size_t)orig[i] + d] = tmp[i];
+        }
+        if (vbar0) {
+            CK(cudaMemcpy(tmp.data(), b.vb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; ++i) vbar0[3 * (size_t)orig[i] + d] = tmp[i];
+        }
+    }
+    if (param_bar) CK(cudaMemcpy(param_bar, h->d_theta, sizeof(double) * h->nmat * adj::kParams, cudaMemcpyDeviceToHost));
+    // leave the device state as the forward run left it
+    if ((st = snap_load(h, h->adj_final))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     return MCM_OK;
 }
 

@@ -1,0 +1,470 @@
+// adjoint.cu -- reverse (adjoint) step of the FP64 explicit step.
+//
+// Scope: disctype 0, model 10 with EOS 41 (the Taylor bar), symmetry and
+// periodic planes, fixed smoothing lengths, a prescribed dt schedule (the
+// critical-timestep minimum is not differentiated: dt_n is an input), and the
+// neighbour lists of each step frozen at their forward values.  One reverse
+// step maps the adjoint of the state after step n to the adjoint of the state
+// before it, and adds the step's contribution to the material-parameter
+// adjoints (G, yield stress, hardening modulus, EOS-41 slope s).
+//
+// The forward step n (MCM/mcm_solution.f90:37-138) is, per particle:
+//   xs = x - v dt_prev/2                      (MCM/mcm_strain.f90:25-29)
+//   G_i = sum_j V_j (v_j - v_i) (x) gradW(xs_i - xs_j)   (mcm_oldstrain.f90:95-124)
+//   rod, spin, tr = sym G, skew G, tr G
+//   (rho, e, p, efps, sigma, q)' = C(rho, e, p, efps, sigma, rod, spin, tr; theta)
+//                                             (mcm_rhoupd, mcm_constitutive)
+//   a_i = sum_j m_j (S_i + S_j) gradW(x_i - x_j),  S = (sigma' - q' I)/rho'^2
+//                                             (mcm_oldacceleration.f90:66-89)
+//   v' = v + a (dt + dt_prev)/2,  x' = x + v' dt, plane reflections
+//                                             (mcm_update_velocity, mcm_move, mcm_check_sym_pen)
+// with ghosts g of parent p: x_g = M_g x_p + c_g, v_g = M_g v_p (M_g = +-1 per
+// axis), rho_g = rho_p at neighbour time, S_g = S_p with every off-diagonal
+// negated (mcm_update_ghost_stress.f90:272-285).
+//
+// Reverse kernels (each a gather over the particle's own list; the lists are
+// symmetric, i in N(j) <=> j in N(i), so the terms a particle contributes to
+// its neighbours' sums are collected from the neighbours' adjoints; only the
+// ghost terms, which belong to a parent particle, use atomics):
+//   k_adj_move        x', v' -> x, v, a          (reflections by their branch)
+//   k_adj_momentum    a -> S (post-constitutive sigma', q', rho'), x, ghost parents
+//   k_adj_constitutive  the per-particle vector-Jacobian product of C by forward-
+//                     mode dual numbers through the same templated code the step
+//                     runs (physics.cuh), so the derivative is the one of the
+//                     branch taken (the active branch of the return map)
+//   k_adj_strain      G -> x, v, rho (through V = m/rho), ghost parents
+#include "nbr_iter.cuh"
+#include "physics.cuh"
+
+namespace mcm {
+namespace adj {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kND = 8;          // directions per dual pass
+constexpr int kInputs = 20;     // rho e p efps sigma(6) rod(6) spin(3) tr
+constexpr int kSeeds = kInputs + kParams;
+using D = Dual<kND>;
+
+// Material constants as duals, with the fields the templated physics code
+// reads.  Model 10 reads strinput[0..7] and EOS 41 eosinput[0..5]; the
+// 5-column table accessor of models 1 and 3 (compiled here, never run: the
+// adjoint accepts model 10 only) is kept inside the arrays.
+constexpr int kStr = 8, kEos = 8;
+struct DualMat {
+    int model, eos, visc_type, pad;
+    D rho, g, av_l, av_q, mass, h, rho_min, rho_max;
+    D strinput[kStr];
+    D eosinput[kEos];
+};
+__device__ __forceinline__ D cm5(const DualMat &M, int i, int j) {
+    const int k = (i - 1) + 5 * (j - 1);
+    return M.strinput[k < kStr ? k : kStr - 1];
+}
+
+// gradW and its Hessian (symmetric: 11 22 33 12 13 23) at separation r,
+// MCM/mcm_gradw.f90:41-103 with havg = (h_i + h_j)/2.
+__device__ __forceinline__ void grad_hess(const double r[3], double havg, double g[3], double H[6]) {
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const double rad = sqrt(r2);
+    double F = 0.0, G2 = 0.0;
+    if (rad > 0.0) {
+        const double z = rad / havg;
+        const double c1 = 1.0 / (kPi * havg * havg * havg);
+        double dw = 0.0, dwp = 0.0;
+        if (z < 1.0) { dw = c1 * (2.25 * z - 3.0) * z; dwp = c1 * (4.5 * z - 3.0); }
+        else if (z < 2.0) { const double t = 2.0 - z; dw = -0.75 * c1 * t * t; dwp = 1.5 * c1 * t; }
+        F = dw / (rad * havg);
+        G2 = (dwp * z - dw) / (r2 * rad * havg);
+    }
+    g[0] = F * r[0]; g[1] = F * r[1]; g[2] = F * r[2];
+    H[0] = F + G2 * r[0] * r[0]; H[1] = F + G2 * r[1] * r[1]; H[2] = F + G2 * r[2] * r[2];
+    H[3] = G2 * r[0] * r[1]; H[4] = G2 * r[0] * r[2]; H[5] = G2 * r[1] * r[2];
+}
+
+__device__ __forceinline__ void symv(const double S[6], const double v[3], double o[3]) {
+    o[0] = S[0] * v[0] + S[3] * v[1] + S[4] * v[2];
+    o[1] = S[3] * v[0] + S[1] * v[1] + S[5] * v[2];
+    o[2] = S[4] * v[0] + S[5] * v[1] + S[2] * v[2];
+}
+// d(a . S g)/dS for the 6 stored components of a symmetric S, times w
+__device__ __forceinline__ void add_symouter(double Sb[6], const double a[3], const double g[3], double w) {
+    Sb[0] += w * a[0] * g[0];
+    Sb[1] += w * a[1] * g[1];
+    Sb[2] += w * a[2] * g[2];
+    Sb[3] += w * (a[0] * g[1] + a[1] * g[0]);
+    Sb[4] += w * (a[0] * g[2] + a[2] * g[0]);
+    Sb[5] += w * (a[1] * g[2] + a[2] * g[1]);
+}
+__device__ __forceinline__ double flip(int mask, int d) { return (mask >> d) & 1 ? -1.0 : 1.0; }
+
+// (sigma - q I)/rho^2 of state index i from the post-constitutive fields
+__device__ __forceinline__ void stress_over_rho2(const StepArgs &a, int i, double S[6]) {
+    const double *const *f = a.F.f;
+    const double rho = f[FRHO][i], r2 = rho * rho, q = f[FQ][i];
+    S[0] = (f[FS11][i] - q) / r2; S[1] = (f[FS22][i] - q) / r2; S[2] = (f[FS33][i] - q) / r2;
+    S[3] = f[FS12][i] / r2; S[4] = f[FS13][i] / r2; S[5] = f[FS23][i] / r2;
+}
+
+// ------------------------------------------------------------------ init
+__global__ void k_adj_init(StepArgs a, AdjArgs b) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        b.yrho[i] = b.rhob[i]; b.ye[i] = b.eb[i]; b.yp[i] = b.pb[i]; b.yefps[i] = b.efpsb[i];
+#pragma unroll
+        for (int u = 0; u < 6; ++u) b.ysig[u][i] = b.sigb[u][i];
+        b.yq[i] = 0.0;
+        b.rho0b[i] = 0.0;
+    }
+}
+
+// ------------------------------------------------- velocity update + move
+// MCM/mcm_update_velocity.f90:29-56, MCM/mcm_move.f90:32-40,
+// MCM/mcm_check_sym_pen.f90:27-179 reversed.  The acceleration a and x, v
+// are the step's values (x after the constitutive round trip).
+__global__ void k_adj_move(StepArgs a, AdjArgs b) {
+    const double *const *f = a.F.f;
+    const double dtn = 0.5 * (b.dt + b.dtold);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double acc[3] = {f[FAX][i], f[FAY][i], f[FAZ][i]};
+        double xb[3] = {b.xb[0][i], b.xb[1][i], b.xb[2][i]};
+        double vb[3] = {b.vb[0][i], b.vb[1][i], b.vb[2][i]};
+        double xo[3];
+        const double *pv[3] = {b.pre[FVX], b.pre[FVY], b.pre[FVZ]};
+        const double xc[3] = {f[FX][i], f[FY][i], f[FZ][i]};
+        for (int d = 0; d < 3; ++d) {
+            const double v1 = a.prm.drelax ? a.prm.drelax_scale * pv[d][i] + acc[d] * dtn : pv[d][i] + acc[d] * dtn;
+            xo[d] = xc[d] + v1 * b.dt;
+        }
+        if (a.prm.boundary) {
+            const DevPlanes &pl = a.prm.planes;
+            for (int d = 0; d < 3; ++d) {
+                bool refl = false;
+                double x = xo[d];
+                if (pl.code[0][d] == 1 && x < pl.bx[0][d]) { x = 2.0 * pl.bx[0][d] - x; refl = !refl; }
+                if (pl.code[1][d] == 1 && x > pl.bx[1][d]) { refl = !refl; }
+                if (refl) { xb[d] = -xb[d]; vb[d] = -vb[d]; }
+            }
+        }
+        double ab[3];
+        for (int d = 0; d < 3; ++d) {
+            const double v1b = vb[d] + xb[d] * b.dt;   // x' = x + v' dt
+            ab[d] = v1b * dtn;
+            vb[d] = a.prm.drelax ? a.prm.drelax_scale * v1b : v1b;
+        }
+        // MCM/mcm_boundcond.f90: constrained components of a are zeroed
+        switch (a.F.dispbc[i]) {
+            case 1: ab[0] = 0.0; break;
+            case 2: ab[1] = 0.0; break;
+            case 3: ab[2] = 0.0; break;
+            case 4: ab[0] = 0.0; ab[1] = 0.0; break;
+            case 5: ab[1] = 0.0; ab[2] = 0.0; break;
+            case 6: ab[0] = 0.0; ab[2] = 0.0; break;
+            case 7: ab[0] = 0.0; ab[1] = 0.0; ab[2] = 0.0; break;
+            default: break;
+        }
+        for (int d = 0; d < 3; ++d) { b.ab[d][i] = ab[d]; b.xb[d][i] = xb[d]; b.vb[d][i] = vb[d]; }
+    }
+}
+
+// ----------------------------------------------------------- momentum
+__global__ void __launch_bounds__(128) k_adj_momentum(StepArgs a, AdjArgs b) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const double *const *f = a.F.f;
+    const int i = a.cell_list[t];
+    const double xi[3] = {f[FX][i], f[FY][i], f[FZ][i]};
+    const double hi = f[FH][i], mi = f[FMASS][i];
+    double Si[6];
+    stress_over_rho2(a, i, Si);
+    const double abi[3] = {b.ab[0][i], b.ab[1][i], b.ab[2][i]};
+    double Sb[6] = {0, 0, 0, 0, 0, 0}, xb[3] = {0, 0, 0};
+    const unsigned *list = a.nidx + (size_t)t * a.nstride;
+    const int nreal = stored_neighbours(a, t);
+    for (int k = 0; k < nreal; ++k) {
+        const int j = a.cell_list[list[k] & kPosMask];
+        const double r[3] = {xi[0] - f[FX][j], xi[1] - f[FY][j], xi[2] - f[FZ][j]};
+        double g[3], H[6];
+        grad_hess(r, 0.5 * (hi + f[FH][j]), g, H);
+        double Sj[6], T[6];
+        stress_over_rho2(a, j, Sj);
+        const double mj = f[FMASS][j];
+        const double abj[3] = {b.ab[0][j], b.ab[1][j], b.ab[2][j]};
+        // own sum: a_i += m_j (S_i + S_j) g
+        add_symouter(Sb, abi, g, mj);
+#pragma unroll
+        for (int u = 0; u < 6; ++u) T[u] = mj * (Si[u] + Sj[u]);
+        double Ta[3], HTa[3];
+        symv(T, abi, Ta);
+        symv(H, Ta, HTa);
+        // j's sum: a_j += m_i (S_j + S_i) g(x_j - x_i) = -m_i (S_i + S_j) g
+        add_symouter(Sb, abj, g, -mi);
+#pragma unroll
+        for (int u = 0; u < 6; ++u) T[u] = mi * (Si[u] + Sj[u]);
+        double Tb[3], HTb[3];
+        symv(T, abj, Tb);
+        symv(H, Tb, HTb);
+        for (int d = 0; d < 3; ++d) xb[d] += HTa[d] - HTb[d];
+    }
+    const int gn = a.gnnbr[t];
+    for (int k = 0; k < gn; ++k) {
+        const int q = a.gnbr[(size_t)k * a.npad + t];
+        const int p = a.gpar[q];
+        const int fl = a.gflip[q];
+        const double r[3] = {xi[0] - a.gx[q], xi[1] - a.gy[q], xi[2] - a.gz[q]};
+        double g[3], H[6];
+        grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
+        // S_g: the parent's sigma', q' over the ghost's density, off-diagonals negated
+        const double rg = a.grho[q], r2 = rg * rg, qp = f[FQ][p];
+        const double Sg[6] = {(f[FS11][p] - qp) / r2, (f[FS22][p] - qp) / r2, (f[FS33][p] - qp) / r2,
+                              -f[FS12][p] / r2, -f[FS13][p] / r2, -f[FS23][p] / r2};
+        const double mg = a.gmass[q];
+        add_symouter(Sb, abi, g, mg);
+        double T[6], Ta[3], HTa[3];
+#pragma unroll
+        for (int u = 0; u < 6; ++u) T[u] = mg * (Si[u] + Sg[u]);
+        symv(T, abi, Ta);
+        symv(H, Ta, HTa);
+        for (int d = 0; d < 3; ++d) xb[d] += HTa[d];
+        // ghost side, to the parent: S_g, rho_g (the parent's density at neighbour time), x_g
+        double Sgb[6] = {0, 0, 0, 0, 0, 0};
+        add_symouter(Sgb, abi, g, mg);
+        atomicAdd(&b.ysig[0][p], Sgb[0] / r2);
+        atomicAdd(&b.ysig[1][p], Sgb[1] / r2);
+        atomicAdd(&b.ysig[2][p], Sgb[2] / r2);
+        atomicAdd(&b.ysig[3][p], -Sgb[3] / r2);
+        atomicAdd(&b.ysig[4][p], -Sgb[4] / r2);
+        atomicAdd(&b.ysig[5][p], -Sgb[5] / r2);
+        atomicAdd(&b.yq[p], -(Sgb[0] + Sgb[1] + Sgb[2]) / r2);
+        double dot = 0.0;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) dot += Sgb[u] * Sg[u];
+        atomicAdd(&b.rho0b[p], -2.0 * dot / rg);
+        for (int d = 0; d < 3; ++d) atomicAdd(&b.xb[d][p], -flip(fl, d) * HTa[d]);
+    }
+    // S_i = (sigma' - q' I)/rho'^2 -> sigma', q', rho'
+    const double rho = f[FRHO][i], r2 = rho * rho;
+    atomicAdd(&b.ysig[0][i], Sb[0] / r2);
+    atomicAdd(&b.ysig[1][i], Sb[1] / r2);
+    atomicAdd(&b.ysig[2][i], Sb[2] / r2);
+    atomicAdd(&b.ysig[3][i], Sb[3] / r2);
+    atomicAdd(&b.ysig[4][i], Sb[4] / r2);
+    atomicAdd(&b.ysig[5][i], Sb[5] / r2);
+    atomicAdd(&b.yq[i], -(Sb[0] + Sb[1] + Sb[2]) / r2);
+    double dot = 0.0;
+#pragma unroll
+    for (int u = 0; u < 6; ++u) dot += Sb[u] * Si[u];
+    atomicAdd(&b.yrho[i], -2.0 * dot / rho);
+    for (int d = 0; d < 3; ++d) atomicAdd(&b.xb[d][i], xb[d]);
+}
+
+// ------------------------------------------------------- constitutive
+// Vector-Jacobian product of the per-particle update (rhoupd + model 10 +
+// EOS 41 chain) by forward-mode duals, kND input directions per pass.
+__global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) {
+    __shared__ double sth[kParams][64];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double th[kParams] = {0, 0, 0, 0};
+    if (i < a.n) {
+        const double *const *pre = b.pre;
+        const double *const *f = a.F.f;
+        const int mat = a.F.mat[i];
+        const DevMaterial &M0 = a.mats[mat - 1];
+        double ub[kInputs];
+        for (int u = 0; u < kInputs; ++u) ub[u] = 0.0;
+        const double yb[11] = {b.yrho[i], b.ye[i], b.yp[i], b.yefps[i], b.ysig[0][i], b.ysig[1][i],
+                               b.ysig[2][i], b.ysig[3][i], b.ysig[4][i], b.ysig[5][i], b.yq[i]};
+        for (int pass = 0; pass * kND < kSeeds; ++pass) {
+            DualMat M;
+            M.model = M0.model; M.eos = M0.eos; M.visc_type = M0.visc_type; M.pad = 0;
+            M.rho = D(M0.rho); M.g = D(M0.g); M.av_l = D(M0.av_l); M.av_q = D(M0.av_q);
+            M.mass = D(M0.mass); M.h = D(M0.h); M.rho_min = D(M0.rho_min); M.rho_max = D(M0.rho_max);
+            for (int k = 0; k < kStr; ++k) M.strinput[k] = D(M0.strinput[k]);
+            for (int k = 0; k < kEos; ++k) M.eosinput[k] = D(M0.eosinput[k]);
+            PState<D> P;
+            P.mat = mat;
+            P.mass = D(pre[FMASS][i]); P.h = D(pre[FH][i]); P.hold = D(pre[FHOLD][i]);
+            P.rho = D(pre[FRHO][i]); P.e = D(pre[FE][i]); P.p = D(pre[FP][i]); P.c = D(pre[FC][i]);
+            P.efps = D(pre[FEFPS][i]); P.pcut = D(pre[FPCUT][i]); P.p_cut = D(pre[FPCUT2][i]);
+            P.fail = D(pre[FFAIL][i]); P.capa = D(0.0);
+            P.rho0 = D(M0.rho);
+            for (int u = 0; u < 6; ++u) {
+                P.sig[u] = D(pre[FS11 + u][i]); P.s[u] = D(0.0); P.alfa[u] = D(0.0);
+                P.rod[u] = D(f[FR11 + u][i]);
+            }
+            P.spin[0] = D(f[FW12][i]); P.spin[1] = D(f[FW13][i]); P.spin[2] = D(f[FW23][i]);
+            P.tracerod = D(f[FTR][i]);
+            P.q = D(0.0);
+            // seed directions pass*kND .. pass*kND + kND - 1
+            for (int k = 0; k < kND; ++k) {
+                const int s = pass * kND + k;
+                D *tgt = nullptr;
+                if (s == 0) tgt = &P.rho;
+                else if (s == 1) tgt = &P.e;
+                else if (s == 2) tgt = &P.p;
+                else if (s == 3) tgt = &P.efps;
+                else if (s < 10) tgt = &P.sig[s - 4];
+                else if (s < 16) tgt = &P.rod[s - 10];
+                else if (s < 19) tgt = &P.spin[s - 16];
+                else if (s == 19) tgt = &P.tracerod;
+                if (tgt) tgt->d[k] = 1.0;
+                else if (s == kInputs + 0) { M.strinput[0].d[k] = 1.0; M.g.d[k] = 1.0; }   // G
+                else if (s == kInputs + 1) M.strinput[1].d[k] = 1.0;                        // yield stress
+                else if (s == kInputs + 2) M.strinput[2].d[k] = 1.0;                        // hardening modulus
+                else if (s == kInputs + 3) M.eosinput[1].d[k] = 1.0;                        // EOS-41 slope s
+            }
+            P.etry = D(0.0); P.einc = D(0.0); P.rhoold = P.rho;
+            const D dt = D(b.dt_prev);
+            rhoupd(P, M, dt, 3);
+            constitutive_particle(P, M, dt);
+            const D *out[11] = {&P.rho, &P.e, &P.p, &P.efps, &P.sig[0], &P.sig[1], &P.sig[2],
+                                &P.sig[3], &P.sig[4], &P.sig[5], &P.q};
+            for (int k = 0; k < kND; ++k) {
+                const int s = pass * kND + k;
+                if (s >= kSeeds) break;
+                double acc = 0.0;
+                for (int o = 0; o < 11; ++o) acc += yb[o] * out[o]->d[k];
+                if (s < kInputs) ub[s] = acc;
+                else th[s - kInputs] = acc;
+            }
+        }
+        b.rhob[i] = ub[0] + b.rho0b[i];
+        b.eb[i] = ub[1];
+        b.pb[i] = ub[2];
+        b.efpsb[i] = ub[3];
+        for (int u = 0; u < 6; ++u) b.sigb[u][i] = ub[4 + u];
+        // rod (11 22 33 12 13 23), spin (12 13 23), tr -> G adjoint (row = velocity component)
+        const double *rb = ub + 10, *wb = ub + 16, trb = ub[19];
+        b.gb[0][i] = rb[0] + trb;            // G00
+        b.gb[4][i] = rb[1] + trb;            // G11
+        b.gb[8][i] = rb[2] + trb;            // G22
+        b.gb[1][i] = 0.5 * (rb[3] + wb[0]);  // G01
+        b.gb[3][i] = 0.5 * (rb[3] - wb[0]);  // G10
+        b.gb[2][i] = 0.5 * (rb[4] + wb[1]);  // G02
+        b.gb[6][i] = 0.5 * (rb[4] - wb[1]);  // G20
+        b.gb[5][i] = 0.5 * (rb[5] + wb[2]);  // G12
+        b.gb[7][i] = 0.5 * (rb[5] - wb[2]);  // G21
+    }
+    // parameter adjoints: block sums, one atomic per block and parameter
+    const int mat = i < a.n ? a.F.mat[i] : 0;
+    for (int k = 0; k < kParams; ++k) sth[k][threadIdx.x] = th[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // blocks are small and materials few: sum per material serially
+        for (int m = 1; m <= a.nmat; ++m) {
+            double s[kParams] = {0, 0, 0, 0};
+            bool any = false;
+            for (int l = 0; l < (int)blockDim.x; ++l) {
+                const int il = blockIdx.x * blockDim.x + l;
+                if (il >= a.n || a.F.mat[il] != m) continue;
+                any = true;
+                for (int k = 0; k < kParams; ++k) s[k] += sth[k][l];
+            }
+            if (any)
+                for (int k = 0; k < kParams; ++k) atomicAdd(&b.theta_b[(m - 1) * kParams + k], s[k]);
+        }
+    }
+    (void)mat;
+}
+
+// ----------------------------------------------------------- strain rate
+__device__ __forceinline__ void load_G(const AdjArgs &b, int i, double G[9]) {
+#pragma unroll
+    for (int u = 0; u < 9; ++u) G[u] = b.gb[u][i];
+}
+
+__global__ void __launch_bounds__(128) k_adj_strain(StepArgs a, AdjArgs b) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const double *const *pre = b.pre;
+    const int i = a.cell_list[t];
+    const double hdt = 0.5 * b.dt_prev;
+    const double vi[3] = {pre[FVX][i], pre[FVY][i], pre[FVZ][i]};
+    const double xsi[3] = {pre[FX][i] - hdt * vi[0], pre[FY][i] - hdt * vi[1], pre[FZ][i] - hdt * vi[2]};
+    const double hi = pre[FH][i], Vi = pre[FMASS][i] / pre[FRHO][i];
+    double Gi[9];
+    load_G(b, i, Gi);
+    double vb[3] = {0, 0, 0}, xsb[3] = {0, 0, 0}, Vb = 0.0;
+    const unsigned *list = a.nidx + (size_t)t * a.nstride;
+    const int nreal = stored_neighbours(a, t);
+    for (int k = 0; k < nreal; ++k) {
+        const int j = a.cell_list[list[k] & kPosMask];
+        const double vj[3] = {pre[FVX][j], pre[FVY][j], pre[FVZ][j]};
+        const double r[3] = {xsi[0] - (pre[FX][j] - hdt * vj[0]), xsi[1] - (pre[FY][j] - hdt * vj[1]),
+                             xsi[2] - (pre[FZ][j] - hdt * vj[2])};
+        double g[3], H[6];
+        grad_hess(r, 0.5 * (hi + pre[FH][j]), g, H);
+        const double Vj = pre[FMASS][j] / pre[FRHO][j];
+        const double dv[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+        double Gj[9];
+        load_G(b, j, Gj);
+        // own sum: G_i += V_j dv (x) g
+        double Gig[3], GiTdv[3], Gjg[3], GjTdv[3];
+        for (int n = 0; n < 3; ++n) {
+            Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
+            Gjg[n] = Gj[3 * n] * g[0] + Gj[3 * n + 1] * g[1] + Gj[3 * n + 2] * g[2];
+            GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
+            GjTdv[n] = Gj[n] * dv[0] + Gj[3 + n] * dv[1] + Gj[6 + n] * dv[2];
+        }
+        double HGi[3], HGj[3];
+        symv(H, GiTdv, HGi);
+        symv(H, GjTdv, HGj);
+        for (int d = 0; d < 3; ++d) {
+            vb[d] -= Vj * Gig[d];
+            // j's sum: G_j += V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g
+            vb[d] -= Vi * Gjg[d];
+            xsb[d] += Vj * HGi[d];
+            // d/dxs_i of V_i dv (x) g(xs_j - xs_i): -V_i H (G_j^T (v_i - v_j)) = +V_i H (G_j^T dv)
+            xsb[d] += Vi * HGj[d];
+        }
+        // d/dV_i of G_j's term V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g(r)
+        Vb += dv[0] * Gjg[0] + dv[1] * Gjg[1] + dv[2] * Gjg[2];
+    }
+    const int gn = a.gnnbr[t];
+    for (int k = 0; k < gn; ++k) {
+        const int q = a.gnbr[(size_t)k * a.npad + t];
+        const int p = a.gpar[q];
+        const int fl = a.gflip[q];
+        const double r[3] = {xsi[0] - a.gx[q], xsi[1] - a.gy[q], xsi[2] - a.gz[q]};
+        double g[3], H[6];
+        grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
+        const double rg = a.grho[q], Vg = a.gmass[q] / rg;
+        const double dv[3] = {a.gvx[q] - vi[0], a.gvy[q] - vi[1], a.gvz[q] - vi[2]};
+        double Gig[3], GiTdv[3], HGi[3];
+        for (int n = 0; n < 3; ++n) {
+            Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
+            GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
+        }
+        symv(H, GiTdv, HGi);
+        for (int d = 0; d < 3; ++d) {
+            vb[d] -= Vg * Gig[d];
+            xsb[d] += Vg * HGi[d];
+            // ghost side: v_g = M v_p, x_g = M x_p + c (unshifted, neighbour-time x)
+            atomicAdd(&b.vb[d][p], flip(fl, d) * Vg * Gig[d]);
+            atomicAdd(&b.xb[d][p], -flip(fl, d) * Vg * HGi[d]);
+        }
+        const double Vgb = dv[0] * Gig[0] + dv[1] * Gig[1] + dv[2] * Gig[2];
+        atomicAdd(&b.rhob[p], -Vgb * Vg / rg);
+    }
+    for (int d = 0; d < 3; ++d) {
+        atomicAdd(&b.xb[d][i], xsb[d]);
+        atomicAdd(&b.vb[d][i], vb[d] - hdt * xsb[d]);
+    }
+    atomicAdd(&b.rhob[i], -Vb * Vi / pre[FRHO][i]);
+}
+
+static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+
+void launch_reverse_momentum(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
+    const int gs = nblk(a.n, 256) < 148 * 8 ? nblk(a.n, 256) : 148 * 8;
+    k_adj_init<<<gs, 256, 0, s>>>(a, b);
+    k_adj_move<<<gs, 256, 0, s>>>(a, b);
+    k_adj_momentum<<<nblk(a.n, 128), 128, 0, s>>>(a, b);
+}
+void launch_reverse_constitutive(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
+    k_adj_constitutive<<<nblk(a.n, 64), 64, 0, s>>>(a, b);
+}
+void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
+    k_adj_strain<<<nblk(a.n, 128), 128, 0, s>>>(a, b);
+}
+
+}  // namespace adj
+}  // namespace mcm

@@ -420,6 +420,8 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
     const double *mult = a.prm.planes.mult[plane];
     const double *add = a.prm.planes.add[plane];
     const int base = *a.plane_base;
+    // axes this plane mirrors (bit d: x_d -> -x_d + add_d); composed along ghost chains
+    const int flips = (mult[0] < 0.0 ? 1 : 0) | (mult[1] < 0.0 ? 2 : 0) | (mult[2] < 0.0 ? 4 : 0);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < p.L; t += (long long)gridDim.x * blockDim.x) {
         int cnt = a.layer_count[t];
         if (cnt == 0) continue;
@@ -436,6 +438,7 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
                 // MCM/mcm_ghost_setup.f90:324-355 (create_ghost_from_real)
                 int j = a.cell_list[rs + r];
                 a.gpar[g] = j;
+                a.gflip[g] = flips;
                 a.gmat[g] = a.F.mat[j];
                 a.gmass[g] = a.F.f[FMASS][j];
                 a.gh[g] = a.F.f[FH][j];
@@ -451,6 +454,7 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
                 // MCM/mcm_ghost_setup.f90:392-423 (create_ghost_from_ghost); chain order = newest first
                 int q = src.x + src.y - 1 - r;
                 a.gpar[g] = a.gpar[q];
+                a.gflip[g] = a.gflip[q] ^ flips;
                 a.gmat[g] = a.gmat[q];
                 a.gmass[g] = a.gmass[q];
                 a.gh[g] = a.gh[q];

@@ -40,6 +40,7 @@ struct StepArgs {
     // ghosts (SoA, ghost_cap each)
     double *gx, *gy, *gz, *gvx, *gvy, *gvz, *gmass, *gh, *ghold, *grho;
     int *gpar, *gmat;
+    int *gflip;       // per ghost: bit d set if its position is the parent's mirrored along axis d
     int *ngp;         // device ghost counter
     int *plane_base;  // ghost index base of the plane being built
     int *layer_count, *layer_off;
@@ -86,6 +87,26 @@ void launch_strain(const StepArgs &a, cudaStream_t s);
 void launch_mom_prep(const StepArgs &a, cudaStream_t s);
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);
 }  // namespace mixed
+
+// adjoint.cu: reverse step of the FP64 step (model 10 + EOS 41, disctype 0)
+namespace adj {
+constexpr int kParams = 4;   // per material: G, yield stress, hardening modulus, EOS-41 slope s
+struct AdjArgs {
+    // adjoint of the state (by state index): in = after the step, out = before it
+    double *xb[3], *vb[3], *rhob, *eb, *pb, *efpsb, *sigb[6];
+    double *ab[3];                                   // acceleration
+    double *yrho, *ye, *yp, *yefps, *ysig[6], *yq;   // post-constitutive state
+    double *rho0b;       // the step's initial density, through the ghost copies
+    double *gb[9];       // velocity gradient G (row n = velocity component, column m = derivative)
+    const double *pre[NFIELD];   // the step's initial state (snapshot)
+    double *theta_b;     // [nmat][kParams], accumulated
+    double dt_prev, dt, dtold;   // dt of the strain/constitutive part, of the update, the one before
+};
+// one reverse step = these three, in this order
+void launch_reverse_momentum(const StepArgs &a, const AdjArgs &b, cudaStream_t s);       // move, velocity, momentum
+void launch_reverse_constitutive(const StepArgs &a, const AdjArgs &b, cudaStream_t s);   // per-particle update
+void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s);         // strain rate
+}  // namespace adj
 
 // step kernels (one namespace per arithmetic flavour)
 #define MCM_DECLARE_STEP(NS)                                                        \

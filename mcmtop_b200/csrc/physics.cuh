@@ -7,6 +7,7 @@
 // literals appear as float literals cast to T.
 #pragma once
 #include "common.cuh"
+#include "dual.cuh"
 
 namespace mcm {
 
@@ -43,8 +44,8 @@ __device__ __forceinline__ int sym_index(int k, int l) {
 
 // ---------------------------------------------------------------- density
 // MCM/mcm_rhoupd.f90:119-151
-template <typename T>
-__device__ __forceinline__ void rhoupd(PState<T> &P, const DevMaterial &M, T dt, int ndim) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void rhoupd(PState<T> &P, const Mat &M, T dt, int ndim) {
     P.rhoold = P.rho;
     const T othird = T(1.0) / T(3.0);
     P.rho = P.rho * (T(1.0) - P.tracerod * dt);
@@ -119,9 +120,9 @@ __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
 
 // ------------------------------------------------------------- EOS: sound speed
 // MCM/mcm_eos1c.f90:115-164 (complex c forced to continue)
-template <typename T>
-__device__ __forceinline__ void eos1c(PState<T> &P, const DevMaterial &M) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos1c(PState<T> &P, const Mat &M) {
+    const auto *ei = M.eosinput;
     T c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -138,9 +139,9 @@ __device__ __forceinline__ void eos1c(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eos4c.f90:33-90
-template <typename T>
-__device__ __forceinline__ void eos4c(PState<T> &P, const DevMaterial &M) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos4c(PState<T> &P, const Mat &M) {
+    const auto *ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T e1 = P.e * P.rho0 / P.mass;
     T mu = P.rho / P.rho0 - T(1.0);
@@ -170,24 +171,24 @@ __device__ __forceinline__ void eos4c(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eos13c.f90:219-227
-template <typename T>
-__device__ __forceinline__ void eos13c(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos13c(PState<T> &P, const Mat &M) {
     T gamma = T(M.eosinput[0]);
     T e1 = P.e / P.mass;
     P.c = sqrt((gamma - T(1.0)) * gamma * e1);
 }
 
 // MCM/mcm_eos28c.f90:305-310
-template <typename T>
-__device__ __forceinline__ void eos28c(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos28c(PState<T> &P, const Mat &M) {
     T b = T(M.eosinput[0]), gamma = T(M.eosinput[1]);
     P.c = sqrt(b * gamma / P.rho0);
 }
 
 // MCM/mcm_eos41c.f90:240-294.  Returns false when c^2 < 0 (the reference stops).
-template <typename T>
-__device__ __forceinline__ bool eos41c(PState<T> &P, const DevMaterial &M) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ bool eos41c(PState<T> &P, const Mat &M) {
+    const auto *ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gamma0 = T(ei[4]);
     T e1 = P.e / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -216,8 +217,8 @@ __device__ __forceinline__ bool eos41c(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_sueos.f90:185-207
-template <typename T>
-__device__ __forceinline__ bool sueos(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ bool sueos(PState<T> &P, const Mat &M) {
     switch (M.eos) {
         case 1: eos1c(P, M); return true;
         case 4: eos4c(P, M); return true;
@@ -230,9 +231,9 @@ __device__ __forceinline__ bool sueos(PState<T> &P, const DevMaterial &M) {
 
 // ------------------------------------------------------------ EOS: pressure
 // MCM/mcm_eqos1.f90:32-75
-template <typename T>
-__device__ __forceinline__ void eqos1(PState<T> &P, const DevMaterial &M, T dt) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos1(PState<T> &P, const Mat &M, T dt) {
+    const auto *ei = M.eosinput;
     T c0 = T(ei[0]), c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -251,9 +252,9 @@ __device__ __forceinline__ void eqos1(PState<T> &P, const DevMaterial &M, T dt) 
 }
 
 // MCM/mcm_eqos4.f90:131-183
-template <typename T>
-__device__ __forceinline__ void eqos4(PState<T> &P, const DevMaterial &M, T dt) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos4(PState<T> &P, const Mat &M, T dt) {
+    const auto *ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T mu = P.rho / P.rho0 - T(1.0);
     T dvol = P.mass / P.rho - P.mass / P.rhoold;
@@ -280,8 +281,8 @@ __device__ __forceinline__ void eqos4(PState<T> &P, const DevMaterial &M, T dt) 
 }
 
 // MCM/mcm_eqos13.f90:258-274
-template <typename T>
-__device__ __forceinline__ void eqos13(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos13(PState<T> &P, const Mat &M) {
     T gamma_m1 = T(M.eosinput[0]) - T(1.0);
     T e1try = P.etry / P.mass;
     T dvol = P.mass / P.rho - P.mass / P.rhoold;
@@ -290,8 +291,8 @@ __device__ __forceinline__ void eqos13(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eqos28.f90:343-358
-template <typename T>
-__device__ __forceinline__ void eqos28(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos28(PState<T> &P, const Mat &M) {
     T b = T(M.eosinput[0]), gamma = T(M.eosinput[1]);
     T dvol = P.mass / P.rho - P.mass / P.rhoold;
     P.p = b * (pow(P.rho / P.rho0, gamma) - T(1.0));
@@ -299,9 +300,9 @@ __device__ __forceinline__ void eqos28(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eqos41.f90:32-102
-template <typename T>
-__device__ __forceinline__ void eqos41(PState<T> &P, const DevMaterial &M, T dt) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos41(PState<T> &P, const Mat &M, T dt) {
+    const auto *ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gama0 = T(ei[4]);
     T etry1 = P.etry / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -326,8 +327,8 @@ __device__ __forceinline__ void eqos41(PState<T> &P, const DevMaterial &M, T dt)
 }
 
 // MCM/mcm_eqos.f90:183-214
-template <typename T>
-__device__ __forceinline__ void eqos(PState<T> &P, const DevMaterial &M, T dt) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eqos(PState<T> &P, const Mat &M, T dt) {
     switch (M.eos) {
         case 1: eqos1(P, M, dt); break;
         case 4: eqos4(P, M, dt); break;
@@ -339,9 +340,9 @@ __device__ __forceinline__ void eqos(PState<T> &P, const DevMaterial &M, T dt) {
 
 // --------------------------------------------------------- EOS: initial state
 // MCM/mcm_eos1p.f90:30-47
-template <typename T>
-__device__ __forceinline__ void eos1p(PState<T> &P, const DevMaterial &M) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos1p(PState<T> &P, const Mat &M) {
+    const auto *ei = M.eosinput;
     T c0 = T(ei[0]), c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -350,9 +351,9 @@ __device__ __forceinline__ void eos1p(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eos4p.f90:32-61
-template <typename T>
-__device__ __forceinline__ void eos4p(PState<T> &P, const DevMaterial &M) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos4p(PState<T> &P, const Mat &M) {
+    const auto *ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T e1 = P.e * P.rho0 / P.mass;
     T mu = P.rho / P.rho0 - T(1.0);
@@ -370,24 +371,24 @@ __device__ __forceinline__ void eos4p(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_eos13p.f90:29-35
-template <typename T>
-__device__ __forceinline__ void eos13p(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos13p(PState<T> &P, const Mat &M) {
     T gamma = T(M.eosinput[0]);
     T e1 = P.e / P.mass;
     P.p = P.rho * (gamma - T(1.0)) * e1;
 }
 
 // MCM/mcm_eos28p.f90:28-33
-template <typename T>
-__device__ __forceinline__ void eos28p(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos28p(PState<T> &P, const Mat &M) {
     T B = T(M.eosinput[0]), gamma = T(M.eosinput[1]);
     P.p = B * (pow(P.rho / P.rho0, gamma) - T(1.0));
 }
 
 // MCM/mcm_eos41p.f90:31-76 (tracerod and dt are zero at initialisation)
-template <typename T>
-__device__ __forceinline__ void eos41p(PState<T> &P, const DevMaterial &M, T dt) {
-    const double *ei = M.eosinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void eos41p(PState<T> &P, const Mat &M, T dt) {
+    const auto *ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gamma = T(ei[4]);
     T e1 = P.e / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -409,8 +410,8 @@ __device__ __forceinline__ void eos41p(PState<T> &P, const DevMaterial &M, T dt)
 
 // ------------------------------------------------- artificial viscosity
 // MCM/mcm_nodalav.f90:76-91 (q is isotropic: only the diagonal is stored)
-template <typename T>
-__device__ __forceinline__ void nodalav(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void nodalav(PState<T> &P, const Mat &M) {
     P.q = T(0.0);
     if (P.tracerod < T(0.0)) {
         T ht = P.h * P.tracerod;
@@ -419,8 +420,8 @@ __device__ __forceinline__ void nodalav(PState<T> &P, const DevMaterial &M) {
 }
 
 // MCM/mcm_aviscosity.f90:28-39 (other types print an error and leave q)
-template <typename T>
-__device__ __forceinline__ void aviscosity(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void aviscosity(PState<T> &P, const Mat &M) {
     if (M.visc_type == 1) nodalav(P, M);
 }
 
@@ -480,11 +481,12 @@ __device__ __forceinline__ void stress_up(PState<T> &P) {
 
 // --------------------------------------------------------------- models
 // cm(i,j) of a cm(5,*) view of strinput
-__device__ __forceinline__ double cm5(const DevMaterial &M, int i, int j) { return M.strinput[(i - 1) + 5 * (j - 1)]; }
+template <typename Mat>
+__device__ __forceinline__ auto cm5(const Mat &M, int i, int j) { return M.strinput[(i - 1) + 5 * (j - 1)]; }
 
 // MCM/mcm_f3dm1.f90:27-71
-template <typename T>
-__device__ __forceinline__ void f3dm1(PState<T> &P, const DevMaterial &M, T dt) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void f3dm1(PState<T> &P, const Mat &M, T dt) {
     const T othird = T(1.0) / T(3.0);
     T ym = T(cm5(M, 1, 1)), pr = T(cm5(M, 1, 2)), gg = T(cm5(M, 5, 4));
     T gdt = dt * gg;
@@ -508,15 +510,15 @@ __device__ __forceinline__ void f3dm1(PState<T> &P, const DevMaterial &M, T dt) 
 }
 
 // MCM/mcm_f3dm3.f90:106-233
-template <typename T>
-__device__ __forceinline__ void f3dm3(PState<T> &P, const DevMaterial &M, T dt) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void f3dm3(PState<T> &P, const Mat &M, T dt) {
     const T othird = T(1.0) / T(3.0);
     T qh = T(cm5(M, 2, 4)), qb = T(cm5(M, 1, 5)), qs = T(cm5(M, 1, 3)), ym = T(cm5(M, 1, 1)), pr = T(cm5(M, 1, 2));
     T efps_f = T(cm5(M, 2, 6));
     T gg = T(2.0) * T(cm5(M, 5, 4));
     T gdt = dt * gg;
     T qbqh = qb * qh;
-    int efps_flag = (int)llround(cm5(M, 1, 6));
+    int efps_flag = (int)llround(value_of(cm5(M, 1, 6)));
     T blk = dt * ym / ((T(1.0f) - T(2.0f) * pr));
     T davg = othird * P.tracerod;
     T p_incr = blk * davg;
@@ -565,8 +567,8 @@ __device__ __forceinline__ void f3dm3(PState<T> &P, const DevMaterial &M, T dt) 
 }
 
 // MCM/mcm_f3dm9.f90:261-285 (s(1,2) is never assigned; xmu = cm(2,mat))
-template <typename T>
-__device__ __forceinline__ void f3dm9(PState<T> &P, const DevMaterial &M) {
+template <typename T, typename Mat>
+__device__ __forceinline__ void f3dm9(PState<T> &P, const Mat &M) {
     const T othird = T(1.0) / T(3.0);
     T xmu = T(cm5(M, 2, P.mat));
     if (xmu == T(0.0f)) {
@@ -584,12 +586,12 @@ __device__ __forceinline__ void f3dm9(PState<T> &P, const DevMaterial &M) {
 
 // MCM/mcm_f3dm10.f90:28-157.  `defps` is uninitialised in the reference when
 // fail /= 1; it is 0 here.
-template <typename T>
-__device__ __forceinline__ void f3dm10(PState<T> &P, const DevMaterial &M, T dt) {
-    const double *cm = M.strinput;
+template <typename T, typename Mat>
+__device__ __forceinline__ void f3dm10(PState<T> &P, const Mat &M, T dt) {
+    const auto *cm = M.strinput;
     const T othird = T(1.0) / T(3.0);
     T gg = T(cm[0]), qs = T(cm[1]), qh = T(cm[2]), a1 = T(cm[4]), a2 = T(cm[5]);
-    int ispall = (int)cm[6];
+    int ispall = (int)value_of(cm[6]);
     T epf = T(cm[7]);
     T g2 = T(2.0f) * dt * gg;
     T davg = othird * P.tracerod;
@@ -653,8 +655,8 @@ __device__ __forceinline__ void f3dm10(PState<T> &P, const DevMaterial &M, T dt)
 
 // -------------------------------------------------------- critical timestep
 // MCM/mcm_calccritts.f90:40-78 (per particle)
-template <typename T>
-__device__ __forceinline__ T critts_particle(const PState<T> &P, const DevMaterial &M, int tcrit_opt, int ndim,
+template <typename T, typename Mat>
+__device__ __forceinline__ T critts_particle(const PState<T> &P, const Mat &M, int tcrit_opt, int ndim,
                                              T vabs, T mindist) {
     if (tcrit_opt == 0) {
         T vol = P.mass / P.rho;
@@ -673,8 +675,8 @@ __device__ __forceinline__ T critts_particle(const PState<T> &P, const DevMateri
 // ------------------------------------------------- constitutive driver
 // MCM/mcm_constitutive.f90:29-83 for one particle, after mcm_rhoupd.
 // Returns false if the EOS reported a complex sound speed.
-template <typename T>
-__device__ __forceinline__ bool constitutive_particle(PState<T> &P, const DevMaterial &M, T dt) {
+template <typename T, typename Mat>
+__device__ __forceinline__ bool constitutive_particle(PState<T> &P, const Mat &M, T dt) {
     bool ok = true;
     switch (M.model) {
         case 1:

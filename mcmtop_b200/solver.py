@@ -218,6 +218,34 @@ class Solver:
               self.h)
         return {"mean_nbr": mean.value, "max_nbr": mx.value, "stride": st.value, "ngp": ngp.value}
 
+    # ---------------------------------------------------------- adjoint
+    def adjoint_forward(self, dts, checkpoint_every: int = 50) -> None:
+        """Runs len(dts) - 1 steps with the prescribed dt schedule, keeping
+        checkpoints for adjoint_backward (mcm_gpu_adjoint_forward)."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        check(self.lib.mcm_gpu_adjoint_forward(self.h, len(d) - 1, _dptr(d), int(checkpoint_every)),
+              "mcm_gpu_adjoint_forward", self.h)
+        self.dtold, self.dt = float(d[-2]), float(d[-1])
+
+    def adjoint_backward(self, xbar=None, vbar=None):
+        """Adjoints of the final x, v ((np, 3) arrays) -> (param_bar (nmat, 4):
+        d/d(G, yield, hardening, EOS-41 s) in card units, xbar0, vbar0)."""
+        keep = []
+
+        def arg(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return _dptr(a)
+
+        pb = np.zeros((self.nmat, 4))
+        x0 = np.zeros((self.n, 3))
+        v0 = np.zeros((self.n, 3))
+        check(self.lib.mcm_gpu_adjoint_backward(self.h, arg(xbar), arg(vbar), _dptr(pb), _dptr(x0), _dptr(v0)),
+              "mcm_gpu_adjoint_backward", self.h)
+        return pb, x0, v0
+
     # ------------------------------------------------------ measurement
     def set_diagnostics(self, enable: bool) -> None:
         check(self.lib.mcm_gpu_set_diagnostics(self.h, int(enable)), "mcm_gpu_set_diagnostics", self.h)
