@@ -34,6 +34,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The batched ensemble runs bodies on up to 64 streams; give the CUDA context
+# (created later, on first use) more hardware queues than the default 8.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "particle-steps/s (2M Taylor bar), mixed vs FP64 GPU at ≤1e-4 rel err; adj/fwd"
 UNIT = "particle-steps/s"
@@ -52,6 +55,8 @@ def parse():
     ap.add_argument("--adj-dx", type=float, default=0.2e-3, help="particle spacing of the differentiated bar")
     ap.add_argument("--adj-steps", type=int, default=400)
     ap.add_argument("--adj-every", type=int, default=50, help="checkpoint interval")
+    ap.add_argument("--ens-bodies", type=int, default=256, help="bars of the batched ensemble (0: skip it)")
+    ap.add_argument("--ens-steps", type=int, default=500)
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -212,19 +217,30 @@ def adjoint_cost(args, local):
     done = fwd.run(nsteps)
     t_fwd = time.perf_counter() - t0
     fwd.close()
+    # One untimed gradient on the same handle first: the first call allocates
+    # the checkpoints and step records and loads the reverse kernels.  The
+    # timed call then starts again from the uploaded initial state.
     sol = Solver(deck, _abi.PREC_FP64, device=local)
-    t0 = time.perf_counter()
-    sol.adjoint_forward(dts, args.adj_every)
-    t_ckpt = time.perf_counter() - t0
-    x = sol.download(["x"])["x"]
-    xbar = np.zeros_like(x)
-    z = x[:, 2]
-    xbar[int(z.argmax()), 2] += 1.0   # d(final length)
-    xbar[int(z.argmin()), 2] -= 1.0
-    t0 = time.perf_counter()
-    pb, _, _ = sol.adjoint_backward(xbar, None)
-    t_bwd = time.perf_counter() - t0
+    init = sol.download()
+
+    def gradient():
+        sol.upload(init)
+        t0 = time.perf_counter()
+        sol.adjoint_forward(dts, args.adj_every)
+        t_ckpt = time.perf_counter() - t0
+        x = sol.download(["x"])["x"]
+        xbar = np.zeros_like(x)
+        z = x[:, 2]
+        xbar[int(z.argmax()), 2] += 1.0   # d(final length)
+        xbar[int(z.argmin()), 2] -= 1.0
+        t0 = time.perf_counter()
+        pb, _, _ = sol.adjoint_backward(xbar, None)
+        return pb, t_ckpt, time.perf_counter() - t0
+
+    pb_warm, _, _ = gradient()
+    pb, t_ckpt, t_bwd = gradient()
     sol.close()
+    spread = float(np.max(np.abs(pb - pb_warm) / np.maximum(np.abs(pb), 1e-300)))
     return {"workload": f"taylor_bar_{deck.np}", "steps": nsteps, "forward_steps_done": done,
             "checkpoint_every": args.adj_every, "precision": "fp64",
             "forward_s": round(t_fwd, 4), "forward_with_checkpoints_s": round(t_ckpt, 4),
@@ -232,7 +248,61 @@ def adjoint_cost(args, local):
             "backward_over_fwd": round(t_bwd / t_fwd, 3),
             "dlength_dparams": {"G": float(pb[0][0]), "yield": float(pb[0][1]), "hardening": float(pb[0][2]),
                                 "eos_s": float(pb[0][3])},
-            "note": "forward = fused mcm_gpu_run; gradient = checkpointed forward + reverse sweep"}
+            "repeat_rel_diff": spread,
+            "note": "forward = fused mcm_gpu_run; gradient = checkpointed forward + reverse sweep, timed on the "
+                    "second gradient of the handle (the first allocates its storage); parameter sums use atomics, "
+                    "so repeated gradients differ in the last bits (repeat_rel_diff)"}
+
+
+def ensemble_cost(args, local):
+    """The calibration ensemble: --ens-bodies independent Taylor bars (radius
+    2-4 mm, L/D 6-12, 4k-64k particles log-uniform, yield 200-600 MPa, impact
+    120-250 m/s) advanced --ens-steps iterations in the headline precision,
+    once as a batch (one CUDA-graph launch per iteration of all bodies, lane
+    count from mcm_gpu_batch_autotune) and once body after body through
+    mcm_gpu_run, from the same initial states.  Wall clock around the
+    synchronous calls; the end states of the two runs are compared."""
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.deck import taylor_ensemble
+    from mcmtop_b200.solver import Batch, Solver
+
+    prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
+    decks = taylor_ensemble(nbodies=args.ens_bodies, seed=2024)
+    n_total = sum(d.np for d in decks)
+    t0 = time.perf_counter()
+    batched = [Solver(d, prec, device=local) for d in decks]
+    t_init = time.perf_counter() - t0
+    for s in batched:
+        s.set_diagnostics(False)
+    batch = Batch(batched, lanes=8)
+    lanes, tuned_ms = batch.autotune(2)
+    t0 = time.perf_counter()
+    done = batch.run(args.ens_steps)
+    t_batch = time.perf_counter() - t0
+    batch.close()
+    seq = [Solver(d, prec, device=local) for d in decks]
+    for s in seq:
+        s.set_diagnostics(False)
+    t0 = time.perf_counter()
+    done_seq = [s.run(args.ens_steps) for s in seq]
+    t_seq = time.perf_counter() - t0
+    same = all(np.array_equal(a.download(["x"])["x"], b.download(["x"])["x"]) for a, b in zip(batched, seq))
+    steps = int(np.sum(done))
+    work = sum(d.np * int(k) for d, k in zip(decks, done))
+    for s in batched + seq:
+        s.close()
+    return {"workload": f"taylor_ensemble_{len(decks)}x_{n_total}", "bodies": len(decks), "particles": n_total,
+            "particles_min": min(d.np for d in decks), "particles_max": max(d.np for d in decks),
+            "steps": args.ens_steps, "body_steps_done": steps, "precision": args.precision,
+            "lanes": lanes, "tuned_ms_per_step": round(tuned_ms, 4),
+            "batched_s": round(t_batch, 3), "sequential_s": round(t_seq, 3),
+            "batched_particle_steps_per_s": round(work / t_batch, 1),
+            "sequential_particle_steps_per_s": round(work / t_seq, 1),
+            "speedup": round(t_seq / t_batch, 3), "same_end_positions": bool(same),
+            "sequential_done_equal": bool(list(done_seq) == [int(k) for k in done]),
+            "init_s_per_body": round(t_init / len(decks), 4),
+            "note": "batched = mcm_gpu_batch_run (graph of one iteration of every body over the tuned lanes); "
+                    "sequential = mcm_gpu_run per body, one after the other; wall clock"}
 
 
 # ----------------------------------------------------------------- GPU arm
@@ -377,6 +447,10 @@ def gpu_arm(args):
     if rank == 0 and not args.no_adjoint:
         adjoint = adjoint_cost(args, local)
 
+    ensemble = None
+    if rank == 0 and args.ens_bodies > 0:
+        ensemble = ensemble_cost(args, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, n, el, cores = cpu_oracle(deck, args.cpu_budget, 3)
@@ -394,7 +468,7 @@ def gpu_arm(args):
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
                    "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "kernels": kernels,
+        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "kernels": kernels,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -239,6 +239,54 @@ int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, in
 int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double *vbar, double *param_bar,
                              double *xbar0, double *vbar0);
 
+/* ------------------------------------------------ launch shape, batches */
+
+/* No counterpart in the reference (a serial code).  Launch shape of a handle's
+ * neighbour search and cooperative gathers (the FP64-fast and mixed strain and
+ * momentum kernels; the FP64-exact step keeps one thread per particle).  The
+ * results do not depend on it, except that per-material energy sums are
+ * combined over a different number of block partials.  Zero fields keep the
+ * current value. */
+typedef struct {
+    int search_threads;      /* threads per block of the search: 64, 128 or 256 */
+    int pair_threads;        /* threads per block of the gathers: 64, 128 or 256 */
+    int pair_blocks_per_sm;  /* blocks per SM the gathers' persistent grid is sized for: 1..16 */
+    int nbr_stride;          /* neighbour-table row width in entries (rounded up to 4; still regrown
+                                when a list outgrows it) */
+    double ms_per_step;      /* mcm_gpu_autotune: device time per loop iteration of the chosen shape */
+} mcm_gpu_tuning;
+
+int mcm_gpu_set_tuning(mcm_gpu_handle *h, const mcm_gpu_tuning *t);
+int mcm_gpu_get_tuning(mcm_gpu_handle *h, mcm_gpu_tuning *t);
+/* Times nsteps fused loop iterations (mcm_gpu_run) from the current state for
+ * each candidate shape (search and gather block sizes, persistent-grid size,
+ * and the neighbour-table stride rounded to 16 entries or not), keeps the
+ * fastest, restores the state and time scalars, and returns the choice with
+ * its time in *best (may be NULL).  Needs a copy of the particle state in
+ * device memory for the duration of the call. */
+int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best);
+
+/* No counterpart in the reference.  Many independent bodies (one handle each,
+ * initialised, on the device that is current at create, reorder_interval 0)
+ * advanced together: one loop iteration of every body is one CUDA-graph
+ * launch.  The bodies are spread over `lanes` streams (1..64), largest first
+ * onto the least loaded lane, so bodies of uneven size run concurrently and
+ * fill the GPU; each keeps its own dt, time scalars and termination.  The
+ * handles must not be used through other entry points while a batch run is
+ * in progress; they stay valid after mcm_gpu_batch_destroy. */
+typedef struct mcm_gpu_batch mcm_gpu_batch;
+int mcm_gpu_batch_create(mcm_gpu_handle *const *bodies, int nbodies, int lanes, mcm_gpu_batch **out);
+/* Up to nsteps loop iterations of every body (mcm_gpu_run semantics per
+ * body): times[b] in/out, done[b] = iterations body b completed (may be
+ * NULL).  A body whose neighbour or ghost storage must grow is regrown and
+ * brought level on its own stream; the graph is re-captured after a regrow. */
+int mcm_gpu_batch_run(mcm_gpu_batch *b, int nsteps, mcm_gpu_time *times, int *done);
+/* Times nsteps batched iterations for several lane counts from the current
+ * states, restores every body's state and time scalars, and keeps the fastest
+ * lane count (*lanes, *ms_per_step may be NULL). */
+int mcm_gpu_batch_autotune(mcm_gpu_batch *b, int nsteps, int *lanes, double *ms_per_step);
+int mcm_gpu_batch_destroy(mcm_gpu_batch *b);
+
 /* ----------------------------------------------------------- measurement */
 
 /* Diagnostic fields (rod, spin, tracerod, etry, einc, rhoold, critts, s, a)

@@ -72,6 +72,11 @@ class Time(C.Structure):
     _fields_ = [("dt", C.c_double), ("dtold", C.c_double), ("ptime", C.c_double), ("endtime", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("search_threads", C.c_int), ("pair_threads", C.c_int), ("pair_blocks_per_sm", C.c_int),
+                ("nbr_stride", C.c_int), ("ms_per_step", C.c_double)]
+
+
 # per-particle width of every field in Fields (doubles or ints)
 FIELD_WIDTH = {
     "x": 3, "v": 3, "a": 3, "sigma": 9, "s": 9, "q": 9, "qold": 9, "alfa": 9, "rod": 9, "spin": 9,
@@ -119,6 +124,13 @@ def load() -> C.CDLL:
         "mcm_gpu_timer": ([H, C.c_int, _DP], C.c_int),
         "mcm_gpu_adjoint_forward": ([H, C.c_int, _DP, C.c_int], C.c_int),
         "mcm_gpu_adjoint_backward": ([H, _DP, _DP, _DP, _DP, _DP], C.c_int),
+        "mcm_gpu_set_tuning": ([H, C.POINTER(Tuning)], C.c_int),
+        "mcm_gpu_get_tuning": ([H, C.POINTER(Tuning)], C.c_int),
+        "mcm_gpu_autotune": ([H, C.c_int, C.POINTER(Tuning)], C.c_int),
+        "mcm_gpu_batch_create": ([C.POINTER(H), C.c_int, C.c_int, C.POINTER(H)], C.c_int),
+        "mcm_gpu_batch_run": ([H, C.c_int, C.POINTER(Time), _IP], C.c_int),
+        "mcm_gpu_batch_autotune": ([H, C.c_int, _IP, _DP], C.c_int),
+        "mcm_gpu_batch_destroy": ([H], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

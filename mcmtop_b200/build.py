@@ -31,8 +31,9 @@ UNITS = [
     ("step_mixed.cu", True),
     ("noalloc.cu", False),
     ("adjoint.cu", False),
+    ("batch.cu", False),
 ]
-HEADERS = ["common.cuh", "kernels.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh", "dual.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "handle.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh", "dual.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -15,119 +15,17 @@
 #include <string>
 #include <vector>
 
-#include "kernels.h"
+#include "handle.h"
 
 using namespace mcm;
+using namespace mcm_host;
 
-struct mcm_gpu_handle {
-    mcm_gpu_config cfg;
-    int np = 0, npad = 0, nmat = 0;
-    std::vector<mcm_gpu_material> mats;
-    cudaStream_t stream = nullptr;
-    int device = 0;
-    StepArgs A;
-    // owned allocations
-    double *d_fields = nullptr;
-    int *d_ints = nullptr;
-    DevMaterial *d_mats = nullptr;
-    void *d_scalars = nullptr;     // DevTime, DevStatus, DevGrid, bbox, energy, counters
-    int *d_nppermat = nullptr;
-    // host mirrors (pinned)
-    DevTime *h_time = nullptr;
-    DevStatus *h_status = nullptr;
-    DevGrid *h_grid = nullptr;
-    double *h_bbox = nullptr;
-    double *h_energy = nullptr;
-    int *h_ngp = nullptr;
-    std::string last_error;
-    bool initialised = false;
-    int red_cap = 0;
-    double mean_nbr = 0.0;
-    // profiling: CUDA events around each kernel group on the handle's stream
-    bool prof_on = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs[16];
-    long long kernel_launches = 0;
-    cudaEvent_t timer[2] = {nullptr, nullptr};
-    long long steps_enqueued = 0;
-    bool have_cells = false;   // cell_list holds a valid permutation
-    // adjoint: prescribed dt schedule, checkpoints (fields + bbox), segment snapshots
-    std::vector<double> adj_dts;
-    int adj_steps = 0, adj_every = 0;
-    std::vector<double *> adj_ckpt;
-    double *adj_seg = nullptr;
-    int adj_seg_cap = 0;
-    double *adj_final = nullptr;
-    double *d_adj = nullptr;     // adjoint arrays (40 x npad)
-    double *d_theta = nullptr;   // parameter adjoints (nmat x 4)
-};
+namespace mcm_host {
 
-namespace {
-
-int set_error(mcm_gpu_handle *h, int code, const std::string &msg) {
-    if (h) h->last_error = msg;
-    return code;
-}
-
-#define CK(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
-            return set_error(h, e_ == cudaErrorMemoryAllocation ? MCM_ENOMEM : MCM_ECUDA,          \
-                             std::string(#call) + ": " + cudaGetErrorString(e_));                  \
-    } while (0)
-
-template <typename T>
-int dalloc(mcm_gpu_handle *h, T **p, size_t count) {
-    if (*p) { cudaFree(*p); *p = nullptr; }
-    if (count == 0) count = 1;
-    CK(cudaMalloc((void **)p, sizeof(T) * count));
-    return MCM_OK;
-}
-
-inline int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
-
-// Kernel groups that the profiler times separately.
-enum Region {
-    R_CELLS = 0, R_GHOSTS, R_SEARCH, R_STRAIN_PREP, R_STRAIN, R_CONST, R_CRITTS, R_MOM_PREP, R_MOMENTUM,
-    R_REDUCE, R_MOVE, R_MISC, R_ADJ_MOM, R_ADJ_CONST, R_ADJ_STRAIN, R_NREG
-};
 const char *kRegionName[R_NREG] = {"cell_list", "ghosts", "search", "strain_prep", "strain", "constitutive",
                                    "critts_dt", "momentum_prep", "momentum_integrate", "energy_bbox_reduce",
                                    "update_move", "misc", "adjoint_momentum", "adjoint_constitutive",
                                    "adjoint_strain"};
-
-cudaEvent_t take_event(mcm_gpu_handle *h) {
-    if (h->ev_pool.empty()) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        return e;
-    }
-    cudaEvent_t e = h->ev_pool.back();
-    h->ev_pool.pop_back();
-    return e;
-}
-
-// Counts the kernels of a group and, when profiling, brackets them with events.
-struct Scope {
-    mcm_gpu_handle *h;
-    int r;
-    cudaEvent_t b = nullptr;
-    Scope(mcm_gpu_handle *h_, int r_, int nkernels) : h(h_), r(r_) {
-        h->kernel_launches += nkernels;
-        if (h->prof_on) {
-            b = take_event(h);
-            cudaEventRecord(b, h->stream);
-        }
-    }
-    ~Scope() {
-        if (b) {
-            cudaEvent_t e = take_event(h);
-            cudaEventRecord(e, h->stream);
-            h->prof_pairs[r].push_back({b, e});
-        }
-    }
-};
 
 DevParams make_params(const mcm_gpu_config &c, int nmat) {
     DevParams p;
@@ -200,7 +98,11 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.rec0, np))) return st;
     if ((st = dalloc(h, &h->A.rec1, np))) return st;
     if ((st = dalloc(h, &h->A.rec2, np))) return st;
-    h->red_cap = (int)((np + 15) / 16) + 8;   // blocks of the cooperative momentum kernel (16 particles each)
+    // partial vectors: one per block of the cooperative momentum kernel (at
+    // least 16 particles per block of 256 threads, at most 148 x 16 blocks
+    // for narrower blocks) or of the per-particle kernels (256 threads)
+    h->red_cap = (int)std::max<size_t>((np + 15) / 16, 148 * 16) + 8;
+    h->A.red_blocks = h->red_cap;
     if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
     if (h->cfg.precision == MCM_PREC_MIXED) {
         // one 64-byte slot per particle: strain records use the first 32 bytes
@@ -632,6 +534,8 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     for (double *p : h->adj_ckpt)
         if (p) cudaFree(p);
     if (h->adj_seg) cudaFree(h->adj_seg);
+    for (auto &r : h->adj_rec)
+        if (r.buf) cudaFree(r.buf);
     if (h->adj_final) cudaFree(h->adj_final);
     if (h->d_adj) cudaFree(h->d_adj);
     if (h->d_theta) cudaFree(h->d_theta);
@@ -648,7 +552,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
 
 }  // extern "C"
 
-namespace {
+namespace mcm_host {
 
 // bbox from x (MCM/mcm_initvbls.f90:81-91) when none is supplied
 __global__ void k_bbox_partials(StepArgs a) {
@@ -896,6 +800,7 @@ int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts) {
         launch_set_time(h->A, h->stream, dt, 0.0, 0);
     }
     if ((st = run_part_a(h))) return st;
+    h->last_max_gnbr = h->h_status->max_gnbr;
     if (critts) *critts = h->h_time->critts;
     return MCM_OK;
 }
@@ -1252,7 +1157,7 @@ int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable) {
 }  // extern "C"
 
 // ---------------------------------------------------------------- adjoint
-namespace {
+namespace mcm_host {
 
 constexpr int kAdjArrays = 40;
 
@@ -1296,6 +1201,133 @@ struct DiagOff {
     explicit DiagOff(mcm_gpu_handle *hh) : h(hh), saved(hh->A.prm.diag) { h->A.prm.diag = 0; }
     ~DiagOff() { h->A.prm.diag = saved; }
 };
+
+// Step records: what the reverse kernels read of a step's forward pass (the
+// state after momentum, the neighbour table, the ghosts), copied once while
+// the segment is recomputed, so that the reverse sweep does not run the
+// forward part of each step a second time.
+constexpr int kGhostD = 9;   // ghost doubles kept: x y z vx vy vz mass h rho (and the int parent and mirror mask)
+// Post-step fields the reverse kernels read, as contiguous runs of the field
+// enumeration: x | h mass rho | sigma q | rod spin tr | a.  (Material ids and
+// displacement conditions do not change: the adjoint runs without re-sorting.)
+constexpr int kRecRuns = 5;
+constexpr int kRecRun[kRecRuns][2] = {{FX, 3}, {FH, 3}, {FS11, 7}, {FR11, 10}, {FAX, 3}};
+constexpr int rec_fields() {
+    int n = 0;
+    for (int r = 0; r < kRecRuns; ++r) n += kRecRun[r][1];
+    return n;
+}
+static_assert(FMASS == FH + 1 && FRHO == FH + 2 && FQ == FS11 + 6 && FW12 == FR11 + 6 && FTR == FR11 + 9 &&
+                  FAZ == FAX + 2,
+              "recorded field runs");
+
+// Carves a record buffer into its arrays (256-byte aligned pieces).  With a
+// null base it only measures: the returned size is the buffer a record of
+// these widths needs.
+struct RecordView {
+    double *fields, *g[kGhostD];
+    unsigned *nidx;
+    int *gnbr, *nnbr, *gnnbr, *cell_list, *gpar, *gflip;
+};
+size_t record_layout(const mcm_gpu_handle *h, char *base, int nstride, int gstride, int ghost_cap, RecordView *v) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char *q = base ? base + off : nullptr; off += (bytes + 255) / 256 * 256; return q; };
+    const size_t np = h->npad, gc = (size_t)ghost_cap;
+    RecordView t;
+    t.fields = (double *)take(sizeof(double) * rec_fields() * np);
+    t.nidx = (unsigned *)take(sizeof(unsigned) * (size_t)nstride * np);
+    t.gnbr = (int *)take(sizeof(int) * (size_t)gstride * np);
+    t.nnbr = (int *)take(sizeof(int) * np);
+    t.gnnbr = (int *)take(sizeof(int) * np);
+    t.cell_list = (int *)take(sizeof(int) * np);
+    for (int k = 0; k < kGhostD; ++k) t.g[k] = (double *)take(sizeof(double) * gc);
+    t.gpar = (int *)take(sizeof(int) * gc);
+    t.gflip = (int *)take(sizeof(int) * gc);
+    if (v) *v = t;
+    return off;
+}
+size_t record_bytes(const mcm_gpu_handle *h) {
+    return record_layout(h, nullptr, h->A.nstride, h->A.gstride, h->A.ghost_cap, nullptr);
+}
+RecordView record_view(const mcm_gpu_handle *h, const mcm_gpu_handle::StepRecord &r) {
+    RecordView v;
+    record_layout(h, r.buf, r.nstride, r.gstride, r.ghost_cap, &v);
+    return v;
+}
+
+double *ghost_arrays(StepArgs &a, int k) {
+    double *const g[kGhostD] = {a.gx, a.gy, a.gz, a.gvx, a.gvy, a.gvz, a.gmass, a.gh, a.grho};
+    return g[k];
+}
+
+int record_save(mcm_gpu_handle *h, mcm_gpu_handle::StepRecord &r) {
+    const size_t need = record_bytes(h);
+    if (r.bytes < need) {
+        if (r.buf) cudaFree(r.buf);
+        r.buf = nullptr;
+        r.bytes = 0;
+        CK(cudaMalloc((void **)&r.buf, need));
+        r.bytes = need;
+    }
+    r.nstride = h->A.nstride;
+    r.gstride = h->A.gstride;
+    r.ghost_cap = h->A.ghost_cap;
+    const RecordView v = record_view(h, r);
+    const size_t np = h->npad, gc = (size_t)r.ghost_cap;
+    StepArgs &a = h->A;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream);
+    };
+    for (int r = 0, o = 0; r < kRecRuns; o += kRecRun[r][1], ++r)
+        CK(cp(v.fields + (size_t)o * np, h->A.F.f[kRecRun[r][0]], sizeof(double) * kRecRun[r][1] * np));
+    CK(cp(v.nidx, a.nidx, sizeof(unsigned) * (size_t)r.nstride * np));
+    // ghost lists are column-major (entry k of every position in row k): only
+    // the rows that hold entries are copied
+    const int grows = std::min(h->last_max_gnbr, r.gstride);
+    if (grows > 0) CK(cp(v.gnbr, a.gnbr, sizeof(int) * (size_t)grows * np));
+    CK(cp(v.nnbr, a.nnbr, sizeof(int) * np));
+    CK(cp(v.gnnbr, a.gnnbr, sizeof(int) * np));
+    CK(cp(v.cell_list, a.cell_list, sizeof(int) * np));
+    for (int k = 0; k < kGhostD; ++k) CK(cp(v.g[k], ghost_arrays(a, k), sizeof(double) * gc));
+    CK(cp(v.gpar, a.gpar, sizeof(int) * gc));
+    CK(cp(v.gflip, a.gflip, sizeof(int) * gc));
+    return MCM_OK;
+}
+
+// The step arguments of a recorded step: the live arguments with every array
+// the reverse kernels read pointed into the record.
+StepArgs record_args(const mcm_gpu_handle *h, const mcm_gpu_handle::StepRecord &r) {
+    StepArgs a = h->A;
+    const RecordView v = record_view(h, r);
+    // fields outside the runs keep pointing at the live state, which the
+    // reverse kernels do not read
+    for (int r = 0, o = 0; r < kRecRuns; o += kRecRun[r][1], ++r)
+        for (int k = 0; k < kRecRun[r][1]; ++k) a.F.f[kRecRun[r][0] + k] = v.fields + (size_t)(o + k) * h->npad;
+    a.nstride = r.nstride;
+    a.gstride = r.gstride;
+    a.ghost_cap = r.ghost_cap;
+    a.nidx = v.nidx;
+    a.gnbr = v.gnbr;
+    a.nnbr = v.nnbr;
+    a.gnnbr = v.gnnbr;
+    a.cell_list = v.cell_list;
+    a.gx = v.g[0]; a.gy = v.g[1]; a.gz = v.g[2];
+    a.gvx = v.g[3]; a.gvy = v.g[4]; a.gvz = v.g[5];
+    a.gmass = v.g[6]; a.gh = v.g[7]; a.grho = v.g[8];
+    a.gpar = v.gpar;
+    a.gflip = v.gflip;
+    return a;
+}
+
+// Records are kept when a segment's worth fits in half of the free memory.
+bool records_fit(mcm_gpu_handle *h, int every) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    size_t held = 0;
+    for (auto &r : h->adj_rec) held += r.bytes;
+    const size_t need = (size_t)every * (record_bytes(h) + record_bytes(h) / 8);
+    return need <= (fr + held) / 2;
+}
 
 }  // namespace
 
@@ -1370,34 +1402,52 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
         if ((st = dalloc(h, &h->adj_seg, sd * every))) return st;
         h->adj_seg_cap = every;
     }
+    // With step records, each step of a segment runs forward once (its record
+    // is taken after momentum, before the move); without them the reverse
+    // sweep re-runs the forward part of each step from its snapshot.
+    const bool keep = records_fit(h, every);
+    if (keep && (int)h->adj_rec.size() < every) h->adj_rec.resize(every);
     for (int c = nck - 1; c >= 0; --c) {
         const int n0 = c * every;
         const int K = std::min(every, h->adj_steps - n0);
         if ((st = snap_load(h, h->adj_ckpt[c]))) return st;
         for (int s = 0; s < K; ++s) {
             if ((st = snap_save(h, h->adj_seg + sd * s))) return st;
-            if (s < K - 1 && (st = adj_step(h, n0 + s, true))) return st;
+            if (keep) {
+                if ((st = adj_step(h, n0 + s, false))) return st;
+                if ((st = record_save(h, h->adj_rec[s]))) return st;
+                if (s < K - 1 && (st = mcm_gpu_step_c(h, h->adj_dts[n0 + s + 1], h->adj_dts[n0 + s], nullptr)))
+                    return st;
+            } else if (s < K - 1 && (st = adj_step(h, n0 + s, true))) {
+                return st;
+            }
         }
         for (int s = K - 1; s >= 0; --s) {
             const int m = n0 + s;
             const double *pre = h->adj_seg + sd * s;
-            if ((st = snap_load(h, pre))) return st;
-            if ((st = adj_step(h, m, false))) return st;   // lists, ghosts, strain, constitutive, momentum
+            StepArgs as;
+            if (keep) {
+                as = record_args(h, h->adj_rec[s]);
+            } else {
+                if ((st = snap_load(h, pre))) return st;
+                if ((st = adj_step(h, m, false))) return st;   // lists, ghosts, strain, constitutive, momentum
+                as = h->A;
+            }
             for (int f = 0; f < NFIELD; ++f) b.pre[f] = pre + (size_t)f * np;
             b.dt_prev = h->adj_dts[m];
             b.dtold = h->adj_dts[m];
             b.dt = h->adj_dts[m + 1];
             {
                 Scope sc(h, R_ADJ_MOM, 3);
-                adj::launch_reverse_momentum(h->A, b, h->stream);
+                adj::launch_reverse_momentum(as, b, h->stream);
             }
             {
                 Scope sc(h, R_ADJ_CONST, 1);
-                adj::launch_reverse_constitutive(h->A, b, h->stream);
+                adj::launch_reverse_constitutive(as, b, h->stream);
             }
             {
                 Scope sc(h, R_ADJ_STRAIN, 1);
-                adj::launch_reverse_strain(h->A, b, h->stream);
+                adj::launch_reverse_strain(as, b, h->stream);
             }
             CK(cudaGetLastError());
         }

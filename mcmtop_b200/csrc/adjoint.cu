@@ -40,26 +40,43 @@ namespace mcm {
 namespace adj {
 
 constexpr double kPi = 3.14159265358979323846;
-constexpr int kND = 8;          // directions per dual pass
+#ifndef MCM_ADJ_DIRECTIONS
+#define MCM_ADJ_DIRECTIONS 8
+#endif
+constexpr int kND = MCM_ADJ_DIRECTIONS;   // directions per dual pass
 constexpr int kInputs = 20;     // rho e p efps sigma(6) rod(6) spin(3) tr
 constexpr int kSeeds = kInputs + kParams;
+constexpr int kPasses = (kSeeds + kND - 1) / kND;
 using D = Dual<kND>;
 
-// Material constants as duals, with the fields the templated physics code
-// reads.  Model 10 reads strinput[0..7] and EOS 41 eosinput[0..5]; the
-// 5-column table accessor of models 1 and 3 (compiled here, never run: the
-// adjoint accepts model 10 only) is kept inside the arrays.
+// Material constants for the dual passes.  Only the four differentiated
+// parameters carry derivatives (strinput(1..3) = G, yield stress, hardening
+// modulus of model 10; eosinput(2) = the EOS-41 slope s; the shear modulus g
+// that EOS 1 and 4 read is G as well); every other card value is a plain
+// double, so that the dual state of a pass stays in registers.  Model 10
+// reads strinput[0..7] and EOS 41 eosinput[0..5]; indices beyond the stored
+// ones (the 5-row table of models 1 and 3, compiled here but never run: the
+// adjoint accepts model 10 only) read the last stored value.
 constexpr int kStr = 8, kEos = 8;
+struct StrCards {
+    double v[kStr];
+    D gmod, yield, hard;
+    __device__ __forceinline__ D operator[](int k) const {
+        return k == 0 ? gmod : (k == 1 ? yield : (k == 2 ? hard : D(v[k < kStr ? k : kStr - 1])));
+    }
+};
+struct EosCards {
+    double v[kEos];
+    D slope;
+    __device__ __forceinline__ D operator[](int k) const { return k == 1 ? slope : D(v[k < kEos ? k : kEos - 1]); }
+};
 struct DualMat {
     int model, eos, visc_type, pad;
-    D rho, g, av_l, av_q, mass, h, rho_min, rho_max;
-    D strinput[kStr];
-    D eosinput[kEos];
+    double rho, av_l, av_q, mass, h, rho_min, rho_max;
+    D g;
+    StrCards strinput;
+    EosCards eosinput;
 };
-__device__ __forceinline__ D cm5(const DualMat &M, int i, int j) {
-    const int k = (i - 1) + 5 * (j - 1);
-    return M.strinput[k < kStr ? k : kStr - 1];
-}
 
 // gradW and its Hessian (symmetric: 11 22 33 12 13 23) at separation r,
 // MCM/mcm_gradw.f90:41-103 with havg = (h_i + h_j)/2.
@@ -258,74 +275,110 @@ __global__ void __launch_bounds__(128) k_adj_momentum(StepArgs a, AdjArgs b) {
 
 // ------------------------------------------------------- constitutive
 // Vector-Jacobian product of the per-particle update (rhoupd + model 10 +
-// EOS 41 chain) by forward-mode duals, kND input directions per pass.
+// EOS 41 chain) by forward-mode duals, kND input directions per pass.  The
+// passes and their seed directions are compile-time constants, so that no
+// part of the dual state is addressed through a runtime index (which would
+// put it in local memory).
+
+// Sets derivative slot k of seed direction s (inputs, then parameters).
+// Every case names its field with a constant index, so a runtime s selects a
+// register and does not index the dual state.
+__device__ __forceinline__ void seed(PState<D> &P, DualMat &M, int s, int k) {
+    switch (s) {
+        case 0: P.rho.d[k] = 1.0; break;
+        case 1: P.e.d[k] = 1.0; break;
+        case 2: P.p.d[k] = 1.0; break;
+        case 3: P.efps.d[k] = 1.0; break;
+        case 4: P.sig[0].d[k] = 1.0; break;
+        case 5: P.sig[1].d[k] = 1.0; break;
+        case 6: P.sig[2].d[k] = 1.0; break;
+        case 7: P.sig[3].d[k] = 1.0; break;
+        case 8: P.sig[4].d[k] = 1.0; break;
+        case 9: P.sig[5].d[k] = 1.0; break;
+        case 10: P.rod[0].d[k] = 1.0; break;
+        case 11: P.rod[1].d[k] = 1.0; break;
+        case 12: P.rod[2].d[k] = 1.0; break;
+        case 13: P.rod[3].d[k] = 1.0; break;
+        case 14: P.rod[4].d[k] = 1.0; break;
+        case 15: P.rod[5].d[k] = 1.0; break;
+        case 16: P.spin[0].d[k] = 1.0; break;
+        case 17: P.spin[1].d[k] = 1.0; break;
+        case 18: P.spin[2].d[k] = 1.0; break;
+        case 19: P.tracerod.d[k] = 1.0; break;
+        case kInputs + 0: M.strinput.gmod.d[k] = 1.0; M.g.d[k] = 1.0; break;   // G
+        case kInputs + 1: M.strinput.yield.d[k] = 1.0; break;                 // yield stress
+        case kInputs + 2: M.strinput.hard.d[k] = 1.0; break;                  // hardening modulus
+        case kInputs + 3: M.eosinput.slope.d[k] = 1.0; break;                 // EOS-41 slope s
+        default: break;
+    }
+}
+
+__device__ __forceinline__ void constitutive_pass(int pass, const StepArgs &a, const AdjArgs &b, int i, int mat,
+                                                  const DevMaterial &M0, const double (&yb)[11],
+                                                  double (&ub)[kInputs], double (&th)[kParams]) {
+    const double *const *pre = b.pre;
+    const double *const *f = a.F.f;
+    DualMat M;
+    M.model = M0.model; M.eos = M0.eos; M.visc_type = M0.visc_type; M.pad = 0;
+    M.rho = M0.rho; M.av_l = M0.av_l; M.av_q = M0.av_q;
+    M.mass = M0.mass; M.h = M0.h; M.rho_min = M0.rho_min; M.rho_max = M0.rho_max;
+    M.g = D(M0.g);
+#pragma unroll
+    for (int k = 0; k < kStr; ++k) M.strinput.v[k] = M0.strinput[k];
+#pragma unroll
+    for (int k = 0; k < kEos; ++k) M.eosinput.v[k] = M0.eosinput[k];
+    M.strinput.gmod = D(M0.strinput[0]);
+    M.strinput.yield = D(M0.strinput[1]);
+    M.strinput.hard = D(M0.strinput[2]);
+    M.eosinput.slope = D(M0.eosinput[1]);
+    PState<D> P;
+    P.mat = mat;
+    P.mass = D(pre[FMASS][i]); P.h = D(pre[FH][i]); P.hold = D(pre[FHOLD][i]);
+    P.rho = D(pre[FRHO][i]); P.e = D(pre[FE][i]); P.p = D(pre[FP][i]); P.c = D(pre[FC][i]);
+    P.efps = D(pre[FEFPS][i]); P.pcut = D(pre[FPCUT][i]); P.p_cut = D(pre[FPCUT2][i]);
+    P.fail = D(pre[FFAIL][i]); P.capa = D(0.0);
+    P.rho0 = D(M0.rho);
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+        P.sig[u] = D(pre[FS11 + u][i]); P.s[u] = D(0.0); P.alfa[u] = D(0.0);
+        P.rod[u] = D(f[FR11 + u][i]);
+    }
+    P.spin[0] = D(f[FW12][i]); P.spin[1] = D(f[FW13][i]); P.spin[2] = D(f[FW23][i]);
+    P.tracerod = D(f[FTR][i]);
+    P.q = D(0.0);
+#pragma unroll
+    for (int k = 0; k < kND; ++k) seed(P, M, pass * kND + k, k);
+    P.etry = D(0.0); P.einc = D(0.0); P.rhoold = P.rho;
+    const D dt = D(b.dt_prev);
+    rhoupd(P, M, dt, 3);
+    constitutive_particle(P, M, dt);
+#pragma unroll
+    for (int k = 0; k < kND; ++k) {
+        const int s = pass * kND + k;
+        if (s >= kSeeds) break;
+        const double acc = yb[0] * P.rho.d[k] + yb[1] * P.e.d[k] + yb[2] * P.p.d[k] + yb[3] * P.efps.d[k] +
+                           yb[4] * P.sig[0].d[k] + yb[5] * P.sig[1].d[k] + yb[6] * P.sig[2].d[k] +
+                           yb[7] * P.sig[3].d[k] + yb[8] * P.sig[4].d[k] + yb[9] * P.sig[5].d[k] +
+                           yb[10] * P.q.d[k];
+        if (s < kInputs) ub[s] = acc;
+        else th[s - kInputs] = acc;
+    }
+}
+
 __global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) {
     __shared__ double sth[kParams][64];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double th[kParams] = {0, 0, 0, 0};
     if (i < a.n) {
-        const double *const *pre = b.pre;
-        const double *const *f = a.F.f;
         const int mat = a.F.mat[i];
         const DevMaterial &M0 = a.mats[mat - 1];
         double ub[kInputs];
+#pragma unroll
         for (int u = 0; u < kInputs; ++u) ub[u] = 0.0;
         const double yb[11] = {b.yrho[i], b.ye[i], b.yp[i], b.yefps[i], b.ysig[0][i], b.ysig[1][i],
                                b.ysig[2][i], b.ysig[3][i], b.ysig[4][i], b.ysig[5][i], b.yq[i]};
-        for (int pass = 0; pass * kND < kSeeds; ++pass) {
-            DualMat M;
-            M.model = M0.model; M.eos = M0.eos; M.visc_type = M0.visc_type; M.pad = 0;
-            M.rho = D(M0.rho); M.g = D(M0.g); M.av_l = D(M0.av_l); M.av_q = D(M0.av_q);
-            M.mass = D(M0.mass); M.h = D(M0.h); M.rho_min = D(M0.rho_min); M.rho_max = D(M0.rho_max);
-            for (int k = 0; k < kStr; ++k) M.strinput[k] = D(M0.strinput[k]);
-            for (int k = 0; k < kEos; ++k) M.eosinput[k] = D(M0.eosinput[k]);
-            PState<D> P;
-            P.mat = mat;
-            P.mass = D(pre[FMASS][i]); P.h = D(pre[FH][i]); P.hold = D(pre[FHOLD][i]);
-            P.rho = D(pre[FRHO][i]); P.e = D(pre[FE][i]); P.p = D(pre[FP][i]); P.c = D(pre[FC][i]);
-            P.efps = D(pre[FEFPS][i]); P.pcut = D(pre[FPCUT][i]); P.p_cut = D(pre[FPCUT2][i]);
-            P.fail = D(pre[FFAIL][i]); P.capa = D(0.0);
-            P.rho0 = D(M0.rho);
-            for (int u = 0; u < 6; ++u) {
-                P.sig[u] = D(pre[FS11 + u][i]); P.s[u] = D(0.0); P.alfa[u] = D(0.0);
-                P.rod[u] = D(f[FR11 + u][i]);
-            }
-            P.spin[0] = D(f[FW12][i]); P.spin[1] = D(f[FW13][i]); P.spin[2] = D(f[FW23][i]);
-            P.tracerod = D(f[FTR][i]);
-            P.q = D(0.0);
-            // seed directions pass*kND .. pass*kND + kND - 1
-            for (int k = 0; k < kND; ++k) {
-                const int s = pass * kND + k;
-                D *tgt = nullptr;
-                if (s == 0) tgt = &P.rho;
-                else if (s == 1) tgt = &P.e;
-                else if (s == 2) tgt = &P.p;
-                else if (s == 3) tgt = &P.efps;
-                else if (s < 10) tgt = &P.sig[s - 4];
-                else if (s < 16) tgt = &P.rod[s - 10];
-                else if (s < 19) tgt = &P.spin[s - 16];
-                else if (s == 19) tgt = &P.tracerod;
-                if (tgt) tgt->d[k] = 1.0;
-                else if (s == kInputs + 0) { M.strinput[0].d[k] = 1.0; M.g.d[k] = 1.0; }   // G
-                else if (s == kInputs + 1) M.strinput[1].d[k] = 1.0;                        // yield stress
-                else if (s == kInputs + 2) M.strinput[2].d[k] = 1.0;                        // hardening modulus
-                else if (s == kInputs + 3) M.eosinput[1].d[k] = 1.0;                        // EOS-41 slope s
-            }
-            P.etry = D(0.0); P.einc = D(0.0); P.rhoold = P.rho;
-            const D dt = D(b.dt_prev);
-            rhoupd(P, M, dt, 3);
-            constitutive_particle(P, M, dt);
-            const D *out[11] = {&P.rho, &P.e, &P.p, &P.efps, &P.sig[0], &P.sig[1], &P.sig[2],
-                                &P.sig[3], &P.sig[4], &P.sig[5], &P.q};
-            for (int k = 0; k < kND; ++k) {
-                const int s = pass * kND + k;
-                if (s >= kSeeds) break;
-                double acc = 0.0;
-                for (int o = 0; o < 11; ++o) acc += yb[o] * out[o]->d[k];
-                if (s < kInputs) ub[s] = acc;
-                else th[s - kInputs] = acc;
-            }
-        }
+#pragma unroll 1
+        for (int pass = 0; pass < kPasses; ++pass) constitutive_pass(pass, a, b, i, mat, M0, yb, ub, th);
         b.rhob[i] = ub[0] + b.rho0b[i];
         b.eb[i] = ub[1];
         b.pb[i] = ub[2];

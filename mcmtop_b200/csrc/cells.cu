@@ -631,8 +631,8 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
 }
 
 void launch_search(const StepArgs &a, cudaStream_t s) {
-    int blocks = (a.n + 255) / 256;
-    k_search<<<blocks, 256, 0, s>>>(a);
+    const int threads = search_threads_of(a);
+    k_search<<<(a.n + threads - 1) / threads, threads, 0, s>>>(a);
 }
 
 }  // namespace mcm

@@ -61,7 +61,11 @@ struct StepArgs {
     float4 *gfrec1, *gfrec2;         // mixed path, per ghost
     // reductions
     double *red;      // block partials
-    int red_blocks;
+    int red_blocks;   // capacity of red in blocks (partial vectors)
+    // launch shape, chosen by mcm_gpu_set_tuning or mcm_gpu_autotune (0: default)
+    int search_threads;   // threads per block of the neighbour search
+    int pair_threads;     // threads per block of the cooperative strain and momentum gathers
+    int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for
     double *energy;   // 5*nmat + 3
 };
 
@@ -125,5 +129,20 @@ MCM_DECLARE_STEP(fast)
 #undef MCM_DECLARE_STEP
 
 constexpr int kRedThreads = 256;
+
+// Launch shape of the cooperative gathers: per block, pair_threads / lanes
+// particles; the persistent grid covers every particle group once or
+// 148 * pair_bps blocks, whichever is fewer, and never more blocks than the
+// partials buffer holds.
+inline int pair_threads_of(const StepArgs &a) { return a.pair_threads > 0 ? a.pair_threads : 256; }
+inline int pair_blocks_of(const StepArgs &a, int lanes) {
+    const int per = pair_threads_of(a) / lanes;
+    int b = (a.n + per - 1) / per;
+    const int cap = 148 * (a.pair_bps > 0 ? a.pair_bps : 8);
+    if (b > cap) b = cap;
+    if (a.red_blocks > 0 && b > a.red_blocks) b = a.red_blocks;
+    return b < 1 ? 1 : b;
+}
+inline int search_threads_of(const StepArgs &a) { return a.search_threads > 0 ? a.search_threads : 256; }
 
 }  // namespace mcm

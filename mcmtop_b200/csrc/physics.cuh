@@ -122,7 +122,7 @@ __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
 // MCM/mcm_eos1c.f90:115-164 (complex c forced to continue)
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos1c(PState<T> &P, const Mat &M) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -141,7 +141,7 @@ __device__ __forceinline__ void eos1c(PState<T> &P, const Mat &M) {
 // MCM/mcm_eos4c.f90:33-90
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos4c(PState<T> &P, const Mat &M) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T e1 = P.e * P.rho0 / P.mass;
     T mu = P.rho / P.rho0 - T(1.0);
@@ -188,7 +188,7 @@ __device__ __forceinline__ void eos28c(PState<T> &P, const Mat &M) {
 // MCM/mcm_eos41c.f90:240-294.  Returns false when c^2 < 0 (the reference stops).
 template <typename T, typename Mat>
 __device__ __forceinline__ bool eos41c(PState<T> &P, const Mat &M) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gamma0 = T(ei[4]);
     T e1 = P.e / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -233,7 +233,7 @@ __device__ __forceinline__ bool sueos(PState<T> &P, const Mat &M) {
 // MCM/mcm_eqos1.f90:32-75
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos1(PState<T> &P, const Mat &M, T dt) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c0 = T(ei[0]), c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -254,7 +254,7 @@ __device__ __forceinline__ void eqos1(PState<T> &P, const Mat &M, T dt) {
 // MCM/mcm_eqos4.f90:131-183
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos4(PState<T> &P, const Mat &M, T dt) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T mu = P.rho / P.rho0 - T(1.0);
     T dvol = P.mass / P.rho - P.mass / P.rhoold;
@@ -302,7 +302,7 @@ __device__ __forceinline__ void eqos28(PState<T> &P, const Mat &M) {
 // MCM/mcm_eqos41.f90:32-102
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos41(PState<T> &P, const Mat &M, T dt) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gama0 = T(ei[4]);
     T etry1 = P.etry / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -342,7 +342,7 @@ __device__ __forceinline__ void eqos(PState<T> &P, const Mat &M, T dt) {
 // MCM/mcm_eos1p.f90:30-47
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos1p(PState<T> &P, const Mat &M) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c0 = T(ei[0]), c1 = T(ei[1]), c2 = T(ei[2]), c3 = T(ei[3]), c4 = T(ei[4]), c5 = T(ei[5]), c6 = T(ei[6]);
     T mu = P.rho / P.rho0 - T(1.0);
     T mu_t = tmax(mu, T(0.0));
@@ -353,7 +353,7 @@ __device__ __forceinline__ void eos1p(PState<T> &P, const Mat &M) {
 // MCM/mcm_eos4p.f90:32-61
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos4p(PState<T> &P, const Mat &M) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T c1 = T(ei[0]), s1 = T(ei[1]), s2 = T(ei[2]), s3 = T(ei[3]), gamma = T(ei[4]), a1 = T(ei[5]);
     T e1 = P.e * P.rho0 / P.mass;
     T mu = P.rho / P.rho0 - T(1.0);
@@ -388,7 +388,7 @@ __device__ __forceinline__ void eos28p(PState<T> &P, const Mat &M) {
 // MCM/mcm_eos41p.f90:31-76 (tracerod and dt are zero at initialisation)
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos41p(PState<T> &P, const Mat &M, T dt) {
-    const auto *ei = M.eosinput;
+    const auto &ei = M.eosinput;
     T cc = T(ei[0]), sl = T(ei[1]), gamma = T(ei[4]);
     T e1 = P.e / P.mass;
     T ao = P.rho0 * (cc * cc);
@@ -588,7 +588,7 @@ __device__ __forceinline__ void f3dm9(PState<T> &P, const Mat &M) {
 // fail /= 1; it is 0 here.
 template <typename T, typename Mat>
 __device__ __forceinline__ void f3dm10(PState<T> &P, const Mat &M, T dt) {
-    const auto *cm = M.strinput;
+    const auto &cm = M.strinput;
     const T othird = T(1.0) / T(3.0);
     T gg = T(cm[0]), qs = T(cm[1]), qh = T(cm[2]), a1 = T(cm[4]), a2 = T(cm[5]);
     int ispall = (int)value_of(cm[6]);

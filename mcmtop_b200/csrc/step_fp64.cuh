@@ -790,11 +790,6 @@ namespace MCM_FLAVOUR_NS {
 // ----------------------------------------------------------- launchers
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 constexpr int kCoopLanes = 16;   // lanes per particle in the cooperative gathers
-// persistent grid: a few blocks per SM, each looping over particle groups
-static inline int coop_blocks(int n, int per) {
-    int need = nblk(n, per);
-    return need < 148 * 8 ? need : 148 * 8;
-}
 static inline int gs_blocks(int n) { int b = nblk(n, 256); return b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b); }
 
 void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
@@ -808,10 +803,9 @@ void launch_strain(const StepArgs &a, cudaStream_t s) {
     else k_strain<1><<<blocks, kRedThreads, 0, s>>>(a);
 #else
     constexpr int L = kCoopLanes;
-    const int per = 256 / L;
-    const int blocks = coop_blocks(a.n, per);
-    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, 256, 0, s>>>(a);
-    else k_strain_coop<L, 1><<<blocks, 256, 0, s>>>(a);
+    const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
+    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, threads, 0, s>>>(a);
+    else k_strain_coop<L, 1><<<blocks, threads, 0, s>>>(a);
 #endif
 }
 
@@ -833,11 +827,10 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
     return blocks;
 #else
     constexpr int L = kCoopLanes;
-    const int per = 256 / L;
-    const int blocks = coop_blocks(a.n, per);
+    const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
     if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
-    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, 256, 0, s>>>(a, integrate);
-    else k_momentum_coop<L, 1><<<blocks, 256, 0, s>>>(a, integrate);
+    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, threads, 0, s>>>(a, integrate);
+    else k_momentum_coop<L, 1><<<blocks, threads, 0, s>>>(a, integrate);
     return blocks;
 #endif
 }

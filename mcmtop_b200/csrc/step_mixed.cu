@@ -119,10 +119,6 @@ __device__ __forceinline__ float inv_havg_f(float hi, float hj, float ihi) {
 }
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
-static inline int coop_blocks(int n, int per) {
-    int need = nblk(n, per);
-    return need < 148 * 8 ? need : 148 * 8;
-}
 
 // ------------------------------------------------------------ strain prep
 // MCM/mcm_strain.f90:27-31 (x - v dt/2) and V_j = m_j/rho_j, cell-relative.
@@ -479,7 +475,7 @@ void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 void launch_strain(const StepArgs &a, cudaStream_t s) {
-    k_strain<<<coop_blocks(a.n, 256 / L), 256, 0, s>>>(a);
+    k_strain<<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
 }
 
 void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
@@ -489,9 +485,9 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
-    const int blocks = coop_blocks(a.n, 256 / L);
+    const int blocks = pair_blocks_of(a, L);
     if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
-    k_momentum<<<blocks, 256, 0, s>>>(a, integrate_flag);
+    k_momentum<<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
     return blocks;
 }
 

@@ -191,3 +191,27 @@ def fluid_column(dx: float = 2.0e-3, block=(0.5, 0.25, 1.0), box=(2.0, 0.25, 1.2
                 sym_x=(0.0, bx[0], 0.0, bx[1], 0.0, bx[2]), materials=[mat], x=x,
                 v=np.zeros_like(x), mat=np.ones(npart, dtype=np.int32), dispbc=np.zeros(npart, dtype=np.int32),
                 name=f"fluid_column_dx{dx * 1e3:g}mm_n{npart}")
+
+
+def taylor_ensemble(nbodies: int = 256, seed: int = 2024, nmin: int = 4000, nmax: int = 64000,
+                    radius=(2.0e-3, 4.0e-3), aspect=(6.0, 12.0), yield_stress=(200e6, 600e6),
+                    velocity=(120.0, 250.0), tcrit_opt: int = 1) -> list:
+    """A calibration ensemble of independent Taylor bars: radius uniform in
+    `radius`, length/diameter uniform in `aspect`, particle count log-uniform
+    in [nmin, nmax] (the spacing dx = (pi R^2 L / N)^(1/3) that gives it),
+    yield stress and impact velocity uniform in their ranges; everything else
+    as taylor_bar.  SI arguments; one seeded generator for the whole set."""
+    rng = np.random.default_rng(seed)
+    decks = []
+    for b in range(nbodies):
+        r = rng.uniform(*radius)
+        length = 2.0 * r * rng.uniform(*aspect)
+        n = np.exp(rng.uniform(np.log(nmin), np.log(nmax)))
+        dx = (np.pi * r * r * length / n) ** (1.0 / 3.0)
+        ys = rng.uniform(*yield_stress)
+        v = rng.uniform(*velocity)
+        mat = copper_model10(1.3 * dx * CM, yield_stress=ys)
+        d = taylor_bar(dx=dx, radius=r, length=length, velocity=v, seed=seed + 1 + b, material=mat,
+                       tcrit_opt=tcrit_opt)
+        decks.append(d.replace(name=f"ensemble{b}_{d.name}"))
+    return decks

@@ -246,6 +246,24 @@ class Solver:
               "mcm_gpu_adjoint_backward", self.h)
         return pb, x0, v0
 
+    # ------------------------------------------------------ launch shape
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        check(self.lib.mcm_gpu_get_tuning(self.h, C.byref(t)), "mcm_gpu_get_tuning", self.h)
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
+
+    def set_tuning(self, search_threads: int = 0, pair_threads: int = 0, pair_blocks_per_sm: int = 0,
+                   nbr_stride: int = 0) -> None:
+        t = _abi.Tuning(search_threads, pair_threads, pair_blocks_per_sm, nbr_stride, 0.0)
+        check(self.lib.mcm_gpu_set_tuning(self.h, C.byref(t)), "mcm_gpu_set_tuning", self.h)
+
+    def autotune(self, nsteps: int = 5) -> dict:
+        """Times candidate launch shapes over nsteps iterations from the
+        current state (which is restored) and keeps the fastest."""
+        t = _abi.Tuning()
+        check(self.lib.mcm_gpu_autotune(self.h, int(nsteps), C.byref(t)), "mcm_gpu_autotune", self.h)
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
+
     # ------------------------------------------------------ measurement
     def set_diagnostics(self, enable: bool) -> None:
         check(self.lib.mcm_gpu_set_diagnostics(self.h, int(enable)), "mcm_gpu_set_diagnostics", self.h)
@@ -305,6 +323,55 @@ class Solver:
         if getattr(self, "h", None):
             self.lib.mcm_gpu_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent bodies advanced together (mcm_gpu_batch_*): one loop
+    iteration of every body per CUDA-graph launch, bodies spread over `lanes`
+    streams.  The solvers keep their own time scalars; run() updates them."""
+
+    def __init__(self, solvers, lanes: int = 8):
+        self.lib = _abi.load()
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        b = C.c_void_p()
+        check(self.lib.mcm_gpu_batch_create(arr, len(self.solvers), int(lanes), C.byref(b)), "mcm_gpu_batch_create",
+              self.solvers[0].h)
+        self.b = b
+
+    def _times(self):
+        return (_abi.Time * len(self.solvers))(*[_abi.Time(s.dt, s.dtold, s.ptime, s.deck.endtime)
+                                                  for s in self.solvers])
+
+    def run(self, nsteps: int) -> np.ndarray:
+        """nsteps iterations of every body; returns the iterations each completed."""
+        t = self._times()
+        done = np.zeros(len(self.solvers), dtype=np.int32)
+        check(self.lib.mcm_gpu_batch_run(self.b, int(nsteps), t, _iptr(done)), "mcm_gpu_batch_run",
+              self.solvers[0].h)
+        for s, tk, d in zip(self.solvers, t, done):
+            s.dt, s.dtold, s.ptime = tk.dt, tk.dtold, tk.ptime
+            s.timestep += int(d)
+            if d < nsteps or s.ptime - s.dt >= s.deck.endtime:
+                s.ended = s.ptime - s.dt >= s.deck.endtime
+        return done
+
+    def autotune(self, nsteps: int = 3):
+        lanes, ms = C.c_int(), C.c_double()
+        check(self.lib.mcm_gpu_batch_autotune(self.b, int(nsteps), C.byref(lanes), C.byref(ms)),
+              "mcm_gpu_batch_autotune", self.solvers[0].h)
+        return lanes.value, ms.value
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            self.lib.mcm_gpu_batch_destroy(self.b)
+            self.b = None
 
     def __del__(self):
         try:
