@@ -57,10 +57,13 @@ def parse():
     ap.add_argument("--adj-every", type=int, default=50, help="checkpoint interval")
     ap.add_argument("--ens-bodies", type=int, default=256, help="bars of the batched ensemble (0: skip it)")
     ap.add_argument("--ens-steps", type=int, default=500)
+    ap.add_argument("--fluid-steps", type=int, default=20, help="iterations of the 15.6M fluid column (0: skip)")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed oracle work")
+    ap.add_argument("--cpu-budget", type=float, default=30.0, help="seconds of timed oracle work")
+    ap.add_argument("--oracle-steps", type=int, default=20,
+                    help="oracle steps on the full bar (CPU baseline sample and GPU spot check)")
     ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
     return ap.parse_args()
 
@@ -168,7 +171,8 @@ def load_traffic(workload: str, precision: str, region: str):
 # -------------------------------------------------------------- CPU baseline
 def cpu_oracle(deck, budget_s: float, max_steps: int):
     """Times the OpenMP build of the CPU restatement (oracle/) on the deck:
-    initialisation untimed, then whole steps until max_steps or the budget."""
+    initialisation untimed, then whole steps until max_steps or the budget.
+    Returns the oracle as well, for the comparison with the GPU runs."""
     from oracle.pyoracle import Oracle
 
     orc = Oracle(deck, openmp=True)
@@ -180,12 +184,38 @@ def cpu_oracle(deck, budget_s: float, max_steps: int):
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    orc.close()
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return deck.np * steps / el, steps, el, cores
+    return deck.np * steps / el, steps, el, cores, orc
 
 
-# ------------------------------------------------------------ adjoint cost
+ORACLE_FIELDS = ["x", "v", "rho", "e", "p", "c", "efps", "sigma", "q", "vabs"]
+
+
+def oracle_spot_check(deck, orc, nsteps: int, local: int, reorder: int):
+    """Per-field error of the mixed and the FP64 GPU steps against the FP64
+    CPU oracle on the full bar after the oracle's first nsteps steps:
+    max |gpu - oracle| / max |oracle| per field."""
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.solver import Solver
+
+    ref = {f: orc.get(f) for f in ORACLE_FIELDS}
+    out = {"against": "FP64 CPU oracle (OpenMP build), same deck, first steps after initialisation",
+           "steps": nsteps, "norm": "max |gpu - oracle| / max |oracle| per field"}
+    for name, prec in (("mixed", _abi.PREC_MIXED), ("fp64", _abi.PREC_FP64)):
+        s = Solver(deck, prec, device=local, reorder_interval=reorder)
+        s.set_diagnostics(False)
+        s.run(nsteps)
+        g = s.download(ORACLE_FIELDS)
+        s.close()
+        err = {}
+        for f in ORACLE_FIELDS:
+            scale = float(np.max(np.abs(ref[f])))
+            err[f] = float(np.max(np.abs(g[f] - ref[f])) / scale) if scale > 0 else float(np.max(np.abs(g[f])))
+        out[name] = {"max_rel_err": {k: float(f"{v:.3e}") for k, v in err.items()},
+                     "worst": float(f"{max(err.values()):.3e}")}
+    return out
+
+
 def adjoint_cost(args, local):
     """Gradient of a final-state function through the whole run against the
     forward run: the differentiated Taylor bar (FP64, prescribed dt schedule
@@ -252,6 +282,33 @@ def adjoint_cost(args, local):
             "note": "forward = fused mcm_gpu_run; gradient = checkpointed forward + reverse sweep, timed on the "
                     "second gradient of the handle (the first allocates its storage); parameter sums use atomics, "
                     "so repeated gradients differ in the last bits (repeat_rel_diff)"}
+
+
+def fluid_column_cost(args, local):
+    """The weakly compressible column collapse at full size: a 0.5 x 0.25 x 1.0 m
+    block of water-like null material (linear polynomial EOS, c0 = 40 m/s) at
+    dx = 2 mm (15.6 M particles) in a 2.0 x 0.25 x 1.2 m box of five ghost-
+    particle walls, under gravity; headline precision, device time of
+    --fluid-steps fused iterations after 3 warm-up iterations."""
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.deck import fluid_column
+    from mcmtop_b200.solver import Solver
+
+    prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
+    deck = fluid_column(dx=2.0e-3)
+    s = Solver(deck, prec, device=local, reorder_interval=args.reorder)
+    s.set_diagnostics(False)
+    s.run(3)
+    s.timer_start()
+    done = s.run(args.fluid_steps)
+    ms = s.timer_stop()
+    st = s.stats()
+    s.close()
+    return {"workload": f"fluid_column_{deck.np}", "particles": deck.np, "steps": done, "precision": args.precision,
+            "value": round(deck.np * done / (ms / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms / max(done, 1), 3),
+            "mean_neighbours": round(st["mean_nbr"], 2), "ghosts": st["ngp"],
+            "note": "null material + EOS 1, five symmetry-plane walls of ghost particles, gravity; lists rebuilt "
+                    "every step; device time (CUDA events on the library stream)"}
 
 
 def ensemble_cost(args, local):
@@ -451,12 +508,19 @@ def gpu_arm(args):
     if rank == 0 and args.ens_bodies > 0:
         ensemble = ensemble_cost(args, local)
 
+    fluid = None
+    if rank == 0 and args.fluid_steps > 0:
+        fluid = fluid_column_cost(args, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, n, el, cores = cpu_oracle(deck, args.cpu_budget, 3)
+        v, n, el, cores, orc = cpu_oracle(deck, args.cpu_budget, args.oracle_steps)
         cpu = {"value": round(v, 1), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"oracle (C++ restatement, OpenMP) on the same {deck.np}-particle bar: {n} steps after "
                          f"initialisation, {el:.1f} s"}
+        if accuracy is not None:
+            accuracy["vs_oracle"] = oracle_spot_check(deck, orc, n, local, args.reorder)
+        orc.close()
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -468,7 +532,8 @@ def gpu_arm(args):
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
                    "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "kernels": kernels,
+        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "fluid_column": fluid,
+        "kernels": kernels,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -487,7 +552,8 @@ def reference_arm(args):
 
     deck = taylor_bar(dx=args.dx)
     # a bounded sample: the first steps of the same bar, until K steps or ~2 minutes
-    v, n, el, cores = cpu_oracle(deck, 120.0, max(1, args.steps))
+    v, n, el, cores, orc = cpu_oracle(deck, 120.0, max(1, args.steps))
+    orc.close()
     line = {
         "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": ws, "steps": n, "warmup": 0,
         "ms_per_step": round(el * 1e3 / n, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -1159,7 +1159,7 @@ int mcm_gpu_set_diagnostics(mcm_gpu_handle *h, int enable) {
 // ---------------------------------------------------------------- adjoint
 namespace mcm_host {
 
-constexpr int kAdjArrays = 40;
+constexpr int kAdjArrays = 40 + 4 * adj::kRecSlots;   // 40 adjoint arrays, then the gather records
 
 size_t snap_doubles(const mcm_gpu_handle *h) { return (size_t)NFIELD * h->npad + 8; }
 
@@ -1329,6 +1329,59 @@ bool records_fit(mcm_gpu_handle *h, int every) {
     return need <= (fr + held) / 2;
 }
 
+// The same iteration, enqueued without waiting: storage overflows are found
+// from the status after a whole segment (adj_segment).  `record` (may be
+// null) receives the step's record between momentum and the move.
+int adj_enqueue_step(mcm_gpu_handle *h, int n, bool move, mcm_gpu_handle::StepRecord *record) {
+    StepArgs &a = h->A;
+    a.split_mode = 1;
+    launch_set_time(a, h->stream, h->adj_dts[n], 0.0, 0);
+    enqueue_part_a(h);
+    enqueue_part_b(h, 0);
+    int st;
+    if (record && (st = record_save(h, *record))) return st;
+    if (move) {
+        launch_set_time(a, h->stream, h->adj_dts[n + 1], h->adj_dts[n], 1);
+        const int nb = launch_move(h);
+        launch_energy_bbox_reduce(a, h->stream, nb, 0, 1);
+    }
+    CK(cudaGetLastError());
+    return MCM_OK;
+}
+
+// Steps n0 .. n0+K-1 from the handle's state, which equals the snapshot
+// `start`: seg (may be null) receives the state before each step; with
+// records, each step's record is kept and the last step stops before its move;
+// without them the last step is not run (only its snapshot is taken) unless
+// `move_last`.  One status check per segment: after a storage overflow the
+// storage is regrown, the state reloaded from `start` and the segment re-run.
+int adj_segment(mcm_gpu_handle *h, int n0, int K, const double *start, double *seg, bool records, bool move_last) {
+    const size_t sd = snap_doubles(h);
+    // records copy every ghost-list row: the longest list is not known before the status is read
+    h->last_max_gnbr = 1 << 30;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int st;
+        if ((st = reset_status(h))) return st;
+        for (int s = 0; s < K; ++s) {
+            if (seg && (st = snap_save(h, seg + sd * s))) return st;
+            const bool last = (s == K - 1);
+            if (records) {
+                if ((st = adj_enqueue_step(h, n0 + s, !last || move_last, &h->adj_rec[s]))) return st;
+            } else if (!last || move_last) {
+                if ((st = adj_enqueue_step(h, n0 + s, true, nullptr))) return st;
+            }
+        }
+        if ((st = sync_status(h))) return st;
+        const int code = h->h_status->code;
+        if (code == MCM_OK) return MCM_OK;
+        int grew = 0;
+        if ((st = regrow(h, &grew))) return st;
+        if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
+        if ((st = snap_load(h, start))) return st;
+    }
+    return set_error(h, MCM_ENBR_OVERFLOW, "adjoint: storage did not converge");
+}
+
 }  // namespace
 
 extern "C" {
@@ -1350,9 +1403,11 @@ int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, in
     for (int c = 0; c < nck; ++c)
         if ((st = dalloc(h, &h->adj_ckpt[c], sd))) return st;
     if ((st = dalloc(h, &h->adj_final, sd))) return st;
-    for (int n = 0; n < nsteps; ++n) {
-        if (n % checkpoint_every == 0 && (st = snap_save(h, h->adj_ckpt[n / checkpoint_every]))) return st;
-        if ((st = adj_step(h, n, true))) return st;
+    for (int c = 0; c < nck; ++c) {
+        const int n0 = c * checkpoint_every;
+        if ((st = snap_save(h, h->adj_ckpt[c]))) return st;
+        if ((st = adj_segment(h, n0, std::min(checkpoint_every, nsteps - n0), h->adj_ckpt[c], nullptr, false, true)))
+            return st;
     }
     if ((st = snap_save(h, h->adj_final))) return st;
     CK(cudaStreamSynchronize(h->stream));
@@ -1383,6 +1438,7 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     for (int u = 0; u < 6; ++u) { b.sigb[u] = arr(10 + u); b.ysig[u] = arr(23 + u); }
     b.yrho = arr(19); b.ye = arr(20); b.yp = arr(21); b.yefps = arr(22); b.yq = arr(29); b.rho0b = arr(30);
     for (int u = 0; u < 9; ++u) b.gb[u] = arr(31 + u);
+    b.rec = reinterpret_cast<double4 *>(arr(40));   // 4 * kRecSlots doubles per position
     b.theta_b = h->d_theta;
     // final adjoints, Fortran (3,np) by particle -> state order
     std::vector<double> tmp(n);
@@ -1411,17 +1467,7 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
         const int n0 = c * every;
         const int K = std::min(every, h->adj_steps - n0);
         if ((st = snap_load(h, h->adj_ckpt[c]))) return st;
-        for (int s = 0; s < K; ++s) {
-            if ((st = snap_save(h, h->adj_seg + sd * s))) return st;
-            if (keep) {
-                if ((st = adj_step(h, n0 + s, false))) return st;
-                if ((st = record_save(h, h->adj_rec[s]))) return st;
-                if (s < K - 1 && (st = mcm_gpu_step_c(h, h->adj_dts[n0 + s + 1], h->adj_dts[n0 + s], nullptr)))
-                    return st;
-            } else if (s < K - 1 && (st = adj_step(h, n0 + s, true))) {
-                return st;
-            }
-        }
+        if ((st = adj_segment(h, n0, K, h->adj_ckpt[c], h->adj_seg, keep, false))) return st;
         for (int s = K - 1; s >= 0; --s) {
             const int m = n0 + s;
             const double *pre = h->adj_seg + sd * s;

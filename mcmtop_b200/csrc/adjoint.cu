@@ -182,81 +182,135 @@ __global__ void k_adj_move(StepArgs a, AdjArgs b) {
     }
 }
 
-// ----------------------------------------------------------- momentum
-__global__ void __launch_bounds__(128) k_adj_momentum(StepArgs a, AdjArgs b) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+// ------------------------------------------------------- gather records
+// One record per cell-order position holds what a reverse gather reads of a
+// neighbour, so that a neighbour costs 4-5 sectors of one or two lines
+// instead of one sector in each of 16-18 field arrays.
+// momentum: {x y z h} {S11 S22 S33 S12} {S13 S23 m -} {ab_x ab_y ab_z -}
+__global__ void k_adj_pack_momentum(StepArgs a, AdjArgs b) {
     const double *const *f = a.F.f;
-    const int i = a.cell_list[t];
-    const double xi[3] = {f[FX][i], f[FY][i], f[FZ][i]};
-    const double hi = f[FH][i], mi = f[FMASS][i];
-    double Si[6];
-    stress_over_rho2(a, i, Si);
-    const double abi[3] = {b.ab[0][i], b.ab[1][i], b.ab[2][i]};
-    double Sb[6] = {0, 0, 0, 0, 0, 0}, xb[3] = {0, 0, 0};
-    const unsigned *list = a.nidx + (size_t)t * a.nstride;
-    const int nreal = stored_neighbours(a, t);
-    for (int k = 0; k < nreal; ++k) {
-        const int j = a.cell_list[list[k] & kPosMask];
-        const double r[3] = {xi[0] - f[FX][j], xi[1] - f[FY][j], xi[2] - f[FZ][j]};
-        double g[3], H[6];
-        grad_hess(r, 0.5 * (hi + f[FH][j]), g, H);
-        double Sj[6], T[6];
-        stress_over_rho2(a, j, Sj);
-        const double mj = f[FMASS][j];
-        const double abj[3] = {b.ab[0][j], b.ab[1][j], b.ab[2][j]};
-        // own sum: a_i += m_j (S_i + S_j) g
-        add_symouter(Sb, abi, g, mj);
-#pragma unroll
-        for (int u = 0; u < 6; ++u) T[u] = mj * (Si[u] + Sj[u]);
-        double Ta[3], HTa[3];
-        symv(T, abi, Ta);
-        symv(H, Ta, HTa);
-        // j's sum: a_j += m_i (S_j + S_i) g(x_j - x_i) = -m_i (S_i + S_j) g
-        add_symouter(Sb, abj, g, -mi);
-#pragma unroll
-        for (int u = 0; u < 6; ++u) T[u] = mi * (Si[u] + Sj[u]);
-        double Tb[3], HTb[3];
-        symv(T, abj, Tb);
-        symv(H, Tb, HTb);
-        for (int d = 0; d < 3; ++d) xb[d] += HTa[d] - HTb[d];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
+        double S[6];
+        stress_over_rho2(a, i, S);
+        double4 *r = b.rec + (size_t)p * kRecSlots;
+        r[0] = make_double4(f[FX][i], f[FY][i], f[FZ][i], f[FH][i]);
+        r[1] = make_double4(S[0], S[1], S[2], S[3]);
+        r[2] = make_double4(S[4], S[5], f[FMASS][i], 0.0);
+        r[3] = make_double4(b.ab[0][i], b.ab[1][i], b.ab[2][i], 0.0);
     }
-    const int gn = a.gnnbr[t];
-    for (int k = 0; k < gn; ++k) {
-        const int q = a.gnbr[(size_t)k * a.npad + t];
-        const int p = a.gpar[q];
-        const int fl = a.gflip[q];
-        const double r[3] = {xi[0] - a.gx[q], xi[1] - a.gy[q], xi[2] - a.gz[q]};
-        double g[3], H[6];
-        grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
-        // S_g: the parent's sigma', q' over the ghost's density, off-diagonals negated
-        const double rg = a.grho[q], r2 = rg * rg, qp = f[FQ][p];
-        const double Sg[6] = {(f[FS11][p] - qp) / r2, (f[FS22][p] - qp) / r2, (f[FS33][p] - qp) / r2,
-                              -f[FS12][p] / r2, -f[FS13][p] / r2, -f[FS23][p] / r2};
-        const double mg = a.gmass[q];
-        add_symouter(Sb, abi, g, mg);
-        double T[6], Ta[3], HTa[3];
-#pragma unroll
-        for (int u = 0; u < 6; ++u) T[u] = mg * (Si[u] + Sg[u]);
-        symv(T, abi, Ta);
-        symv(H, Ta, HTa);
-        for (int d = 0; d < 3; ++d) xb[d] += HTa[d];
-        // ghost side, to the parent: S_g, rho_g (the parent's density at neighbour time), x_g
-        double Sgb[6] = {0, 0, 0, 0, 0, 0};
-        add_symouter(Sgb, abi, g, mg);
-        atomicAdd(&b.ysig[0][p], Sgb[0] / r2);
-        atomicAdd(&b.ysig[1][p], Sgb[1] / r2);
-        atomicAdd(&b.ysig[2][p], Sgb[2] / r2);
-        atomicAdd(&b.ysig[3][p], -Sgb[3] / r2);
-        atomicAdd(&b.ysig[4][p], -Sgb[4] / r2);
-        atomicAdd(&b.ysig[5][p], -Sgb[5] / r2);
-        atomicAdd(&b.yq[p], -(Sgb[0] + Sgb[1] + Sgb[2]) / r2);
-        double dot = 0.0;
-#pragma unroll
-        for (int u = 0; u < 6; ++u) dot += Sgb[u] * Sg[u];
-        atomicAdd(&b.rho0b[p], -2.0 * dot / rg);
-        for (int d = 0; d < 3; ++d) atomicAdd(&b.xb[d][p], -flip(fl, d) * HTa[d]);
+}
+// strain: {xs_x xs_y xs_z h} {v_x v_y v_z V} {G00 G01 G02 G10} {G11 G12 G20 G21} {G22 - - -}
+__global__ void k_adj_pack_strain(StepArgs a, AdjArgs b) {
+    const double *const *pre = b.pre;
+    const double hdt = 0.5 * b.dt_prev;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[p];
+        const double v[3] = {pre[FVX][i], pre[FVY][i], pre[FVZ][i]};
+        double4 *r = b.rec + (size_t)p * kRecSlots;
+        r[0] = make_double4(pre[FX][i] - hdt * v[0], pre[FY][i] - hdt * v[1], pre[FZ][i] - hdt * v[2], pre[FH][i]);
+        r[1] = make_double4(v[0], v[1], v[2], pre[FMASS][i] / pre[FRHO][i]);
+        r[2] = make_double4(b.gb[0][i], b.gb[1][i], b.gb[2][i], b.gb[3][i]);
+        r[3] = make_double4(b.gb[4][i], b.gb[5][i], b.gb[6][i], b.gb[7][i]);
+        r[4] = make_double4(b.gb[8][i], 0.0, 0.0, 0.0);
     }
+}
+
+// ----------------------------------------------------------- momentum
+// kLanes lanes share a particle: lane l takes neighbours l, l + kLanes, ...;
+// the per-particle sums are combined by shuffles and one lane writes them.
+constexpr int kLanes = 16;
+
+template <int N>
+__device__ __forceinline__ void lane_sum(double (&v)[N]) {
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int u = 0; u < N; ++u) v[u] += __shfl_xor_sync(0xffffffffu, v[u], o);
+}
+
+__global__ void __launch_bounds__(128) k_adj_momentum(StepArgs a, AdjArgs b) {
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+    const int lane = threadIdx.x % kLanes;
+    const bool live = t < a.n;
+    const double *const *f = a.F.f;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // Sb[6], xb[3]
+    double *Sb = acc, *xb = acc + 6;
+    int i = 0;
+    double Si[6] = {0, 0, 0, 0, 0, 0};
+    if (live) {
+        i = a.cell_list[t];
+        const double xi[3] = {f[FX][i], f[FY][i], f[FZ][i]};
+        const double hi = f[FH][i], mi = f[FMASS][i];
+        stress_over_rho2(a, i, Si);
+        const double abi[3] = {b.ab[0][i], b.ab[1][i], b.ab[2][i]};
+        const unsigned *list = a.nidx + (size_t)t * a.nstride;
+        const int nreal = stored_neighbours(a, t);
+        for (int k = lane; k < nreal; k += kLanes) {
+            const double4 *rj = b.rec + (size_t)(list[k] & kPosMask) * kRecSlots;
+            const double4 q0 = rj[0], q1 = rj[1], q2 = rj[2], q3 = rj[3];
+            const double r[3] = {xi[0] - q0.x, xi[1] - q0.y, xi[2] - q0.z};
+            double g[3], H[6];
+            grad_hess(r, 0.5 * (hi + q0.w), g, H);
+            const double Sj[6] = {q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+            double T[6];
+            const double mj = q2.z;
+            const double abj[3] = {q3.x, q3.y, q3.z};
+            // own sum: a_i += m_j (S_i + S_j) g
+            add_symouter(Sb, abi, g, mj);
+#pragma unroll
+            for (int u = 0; u < 6; ++u) T[u] = mj * (Si[u] + Sj[u]);
+            double Ta[3], HTa[3];
+            symv(T, abi, Ta);
+            symv(H, Ta, HTa);
+            // j's sum: a_j += m_i (S_j + S_i) g(x_j - x_i) = -m_i (S_i + S_j) g
+            add_symouter(Sb, abj, g, -mi);
+#pragma unroll
+            for (int u = 0; u < 6; ++u) T[u] = mi * (Si[u] + Sj[u]);
+            double Tb[3], HTb[3];
+            symv(T, abj, Tb);
+            symv(H, Tb, HTb);
+            for (int d = 0; d < 3; ++d) xb[d] += HTa[d] - HTb[d];
+        }
+        const int gn = a.gnnbr[t];
+        for (int k = lane; k < gn; k += kLanes) {
+            const int q = a.gnbr[(size_t)k * a.npad + t];
+            const int p = a.gpar[q];
+            const int fl = a.gflip[q];
+            const double r[3] = {xi[0] - a.gx[q], xi[1] - a.gy[q], xi[2] - a.gz[q]};
+            double g[3], H[6];
+            grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
+            // S_g: the parent's sigma', q' over the ghost's density, off-diagonals negated
+            const double rg = a.grho[q], r2 = rg * rg, qp = f[FQ][p];
+            const double Sg[6] = {(f[FS11][p] - qp) / r2, (f[FS22][p] - qp) / r2, (f[FS33][p] - qp) / r2,
+                                  -f[FS12][p] / r2, -f[FS13][p] / r2, -f[FS23][p] / r2};
+            const double mg = a.gmass[q];
+            add_symouter(Sb, abi, g, mg);
+            double T[6], Ta[3], HTa[3];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) T[u] = mg * (Si[u] + Sg[u]);
+            symv(T, abi, Ta);
+            symv(H, Ta, HTa);
+            for (int d = 0; d < 3; ++d) xb[d] += HTa[d];
+            // ghost side, to the parent: S_g, rho_g (the parent's density at neighbour time), x_g
+            double Sgb[6] = {0, 0, 0, 0, 0, 0};
+            add_symouter(Sgb, abi, g, mg);
+            atomicAdd(&b.ysig[0][p], Sgb[0] / r2);
+            atomicAdd(&b.ysig[1][p], Sgb[1] / r2);
+            atomicAdd(&b.ysig[2][p], Sgb[2] / r2);
+            atomicAdd(&b.ysig[3][p], -Sgb[3] / r2);
+            atomicAdd(&b.ysig[4][p], -Sgb[4] / r2);
+            atomicAdd(&b.ysig[5][p], -Sgb[5] / r2);
+            atomicAdd(&b.yq[p], -(Sgb[0] + Sgb[1] + Sgb[2]) / r2);
+            double dot = 0.0;
+#pragma unroll
+            for (int u = 0; u < 6; ++u) dot += Sgb[u] * Sg[u];
+            atomicAdd(&b.rho0b[p], -2.0 * dot / rg);
+            for (int d = 0; d < 3; ++d) atomicAdd(&b.xb[d][p], -flip(fl, d) * HTa[d]);
+        }
+    }
+    lane_sum(acc);
+    if (!live || lane != 0) return;
     // S_i = (sigma' - q' I)/rho'^2 -> sigma', q', rho'
     const double rho = f[FRHO][i], r2 = rho * rho;
     atomicAdd(&b.ysig[0][i], Sb[0] / r2);
@@ -425,83 +479,91 @@ __device__ __forceinline__ void load_G(const AdjArgs &b, int i, double G[9]) {
 }
 
 __global__ void __launch_bounds__(128) k_adj_strain(StepArgs a, AdjArgs b) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+    const int lane = threadIdx.x % kLanes;
+    const bool live = t < a.n;
     const double *const *pre = b.pre;
-    const int i = a.cell_list[t];
     const double hdt = 0.5 * b.dt_prev;
-    const double vi[3] = {pre[FVX][i], pre[FVY][i], pre[FVZ][i]};
-    const double xsi[3] = {pre[FX][i] - hdt * vi[0], pre[FY][i] - hdt * vi[1], pre[FZ][i] - hdt * vi[2]};
-    const double hi = pre[FH][i], Vi = pre[FMASS][i] / pre[FRHO][i];
-    double Gi[9];
-    load_G(b, i, Gi);
-    double vb[3] = {0, 0, 0}, xsb[3] = {0, 0, 0}, Vb = 0.0;
-    const unsigned *list = a.nidx + (size_t)t * a.nstride;
-    const int nreal = stored_neighbours(a, t);
-    for (int k = 0; k < nreal; ++k) {
-        const int j = a.cell_list[list[k] & kPosMask];
-        const double vj[3] = {pre[FVX][j], pre[FVY][j], pre[FVZ][j]};
-        const double r[3] = {xsi[0] - (pre[FX][j] - hdt * vj[0]), xsi[1] - (pre[FY][j] - hdt * vj[1]),
-                             xsi[2] - (pre[FZ][j] - hdt * vj[2])};
-        double g[3], H[6];
-        grad_hess(r, 0.5 * (hi + pre[FH][j]), g, H);
-        const double Vj = pre[FMASS][j] / pre[FRHO][j];
-        const double dv[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
-        double Gj[9];
-        load_G(b, j, Gj);
-        // own sum: G_i += V_j dv (x) g
-        double Gig[3], GiTdv[3], Gjg[3], GjTdv[3];
-        for (int n = 0; n < 3; ++n) {
-            Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
-            Gjg[n] = Gj[3 * n] * g[0] + Gj[3 * n + 1] * g[1] + Gj[3 * n + 2] * g[2];
-            GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
-            GjTdv[n] = Gj[n] * dv[0] + Gj[3 + n] * dv[1] + Gj[6 + n] * dv[2];
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};   // vb[3], xsb[3], Vb
+    double *vb = acc, *xsb = acc + 3;
+    int i = 0;
+    double Vi = 0.0;
+    if (live) {
+        i = a.cell_list[t];
+        const double vi[3] = {pre[FVX][i], pre[FVY][i], pre[FVZ][i]};
+        const double xsi[3] = {pre[FX][i] - hdt * vi[0], pre[FY][i] - hdt * vi[1], pre[FZ][i] - hdt * vi[2]};
+        const double hi = pre[FH][i];
+        Vi = pre[FMASS][i] / pre[FRHO][i];
+        double Gi[9];
+        load_G(b, i, Gi);
+        const unsigned *list = a.nidx + (size_t)t * a.nstride;
+        const int nreal = stored_neighbours(a, t);
+        for (int k = lane; k < nreal; k += kLanes) {
+            const double4 *rj = b.rec + (size_t)(list[k] & kPosMask) * kRecSlots;
+            const double4 q0 = rj[0], q1 = rj[1], q2 = rj[2], q3 = rj[3], q4 = rj[4];
+            const double vj[3] = {q1.x, q1.y, q1.z};
+            const double r[3] = {xsi[0] - q0.x, xsi[1] - q0.y, xsi[2] - q0.z};
+            double g[3], H[6];
+            grad_hess(r, 0.5 * (hi + q0.w), g, H);
+            const double Vj = q1.w;
+            const double dv[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+            const double Gj[9] = {q2.x, q2.y, q2.z, q2.w, q3.x, q3.y, q3.z, q3.w, q4.x};
+            // own sum: G_i += V_j dv (x) g
+            double Gig[3], GiTdv[3], Gjg[3], GjTdv[3];
+            for (int n = 0; n < 3; ++n) {
+                Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
+                Gjg[n] = Gj[3 * n] * g[0] + Gj[3 * n + 1] * g[1] + Gj[3 * n + 2] * g[2];
+                GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
+                GjTdv[n] = Gj[n] * dv[0] + Gj[3 + n] * dv[1] + Gj[6 + n] * dv[2];
+            }
+            double HGi[3], HGj[3];
+            symv(H, GiTdv, HGi);
+            symv(H, GjTdv, HGj);
+            for (int d = 0; d < 3; ++d) {
+                vb[d] -= Vj * Gig[d];
+                // j's sum: G_j += V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g
+                vb[d] -= Vi * Gjg[d];
+                xsb[d] += Vj * HGi[d];
+                // d/dxs_i of V_i dv (x) g(xs_j - xs_i): -V_i H (G_j^T (v_i - v_j)) = +V_i H (G_j^T dv)
+                xsb[d] += Vi * HGj[d];
+            }
+            // d/dV_i of G_j's term V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g(r)
+            acc[6] += dv[0] * Gjg[0] + dv[1] * Gjg[1] + dv[2] * Gjg[2];
         }
-        double HGi[3], HGj[3];
-        symv(H, GiTdv, HGi);
-        symv(H, GjTdv, HGj);
-        for (int d = 0; d < 3; ++d) {
-            vb[d] -= Vj * Gig[d];
-            // j's sum: G_j += V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g
-            vb[d] -= Vi * Gjg[d];
-            xsb[d] += Vj * HGi[d];
-            // d/dxs_i of V_i dv (x) g(xs_j - xs_i): -V_i H (G_j^T (v_i - v_j)) = +V_i H (G_j^T dv)
-            xsb[d] += Vi * HGj[d];
+        const int gn = a.gnnbr[t];
+        for (int k = lane; k < gn; k += kLanes) {
+            const int q = a.gnbr[(size_t)k * a.npad + t];
+            const int p = a.gpar[q];
+            const int fl = a.gflip[q];
+            const double r[3] = {xsi[0] - a.gx[q], xsi[1] - a.gy[q], xsi[2] - a.gz[q]};
+            double g[3], H[6];
+            grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
+            const double rg = a.grho[q], Vg = a.gmass[q] / rg;
+            const double dv[3] = {a.gvx[q] - vi[0], a.gvy[q] - vi[1], a.gvz[q] - vi[2]};
+            double Gig[3], GiTdv[3], HGi[3];
+            for (int n = 0; n < 3; ++n) {
+                Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
+                GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
+            }
+            symv(H, GiTdv, HGi);
+            for (int d = 0; d < 3; ++d) {
+                vb[d] -= Vg * Gig[d];
+                xsb[d] += Vg * HGi[d];
+                // ghost side: v_g = M v_p, x_g = M x_p + c (unshifted, neighbour-time x)
+                atomicAdd(&b.vb[d][p], flip(fl, d) * Vg * Gig[d]);
+                atomicAdd(&b.xb[d][p], -flip(fl, d) * Vg * HGi[d]);
+            }
+            const double Vgb = dv[0] * Gig[0] + dv[1] * Gig[1] + dv[2] * Gig[2];
+            atomicAdd(&b.rhob[p], -Vgb * Vg / rg);
         }
-        // d/dV_i of G_j's term V_i (v_i - v_j) (x) g(xs_j - xs_i) = V_i dv (x) g(r)
-        Vb += dv[0] * Gjg[0] + dv[1] * Gjg[1] + dv[2] * Gjg[2];
     }
-    const int gn = a.gnnbr[t];
-    for (int k = 0; k < gn; ++k) {
-        const int q = a.gnbr[(size_t)k * a.npad + t];
-        const int p = a.gpar[q];
-        const int fl = a.gflip[q];
-        const double r[3] = {xsi[0] - a.gx[q], xsi[1] - a.gy[q], xsi[2] - a.gz[q]};
-        double g[3], H[6];
-        grad_hess(r, 0.5 * (hi + a.gh[q]), g, H);
-        const double rg = a.grho[q], Vg = a.gmass[q] / rg;
-        const double dv[3] = {a.gvx[q] - vi[0], a.gvy[q] - vi[1], a.gvz[q] - vi[2]};
-        double Gig[3], GiTdv[3], HGi[3];
-        for (int n = 0; n < 3; ++n) {
-            Gig[n] = Gi[3 * n] * g[0] + Gi[3 * n + 1] * g[1] + Gi[3 * n + 2] * g[2];
-            GiTdv[n] = Gi[n] * dv[0] + Gi[3 + n] * dv[1] + Gi[6 + n] * dv[2];
-        }
-        symv(H, GiTdv, HGi);
-        for (int d = 0; d < 3; ++d) {
-            vb[d] -= Vg * Gig[d];
-            xsb[d] += Vg * HGi[d];
-            // ghost side: v_g = M v_p, x_g = M x_p + c (unshifted, neighbour-time x)
-            atomicAdd(&b.vb[d][p], flip(fl, d) * Vg * Gig[d]);
-            atomicAdd(&b.xb[d][p], -flip(fl, d) * Vg * HGi[d]);
-        }
-        const double Vgb = dv[0] * Gig[0] + dv[1] * Gig[1] + dv[2] * Gig[2];
-        atomicAdd(&b.rhob[p], -Vgb * Vg / rg);
-    }
+    lane_sum(acc);
+    if (!live || lane != 0) return;
     for (int d = 0; d < 3; ++d) {
         atomicAdd(&b.xb[d][i], xsb[d]);
         atomicAdd(&b.vb[d][i], vb[d] - hdt * xsb[d]);
     }
-    atomicAdd(&b.rhob[i], -Vb * Vi / pre[FRHO][i]);
+    atomicAdd(&b.rhob[i], -acc[6] * Vi / pre[FRHO][i]);
 }
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
@@ -510,13 +572,16 @@ void launch_reverse_momentum(const StepArgs &a, const AdjArgs &b, cudaStream_t s
     const int gs = nblk(a.n, 256) < 148 * 8 ? nblk(a.n, 256) : 148 * 8;
     k_adj_init<<<gs, 256, 0, s>>>(a, b);
     k_adj_move<<<gs, 256, 0, s>>>(a, b);
-    k_adj_momentum<<<nblk(a.n, 128), 128, 0, s>>>(a, b);
+    k_adj_pack_momentum<<<gs, 256, 0, s>>>(a, b);
+    k_adj_momentum<<<nblk(a.n, 128 / kLanes), 128, 0, s>>>(a, b);
 }
 void launch_reverse_constitutive(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
     k_adj_constitutive<<<nblk(a.n, 64), 64, 0, s>>>(a, b);
 }
 void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
-    k_adj_strain<<<nblk(a.n, 128), 128, 0, s>>>(a, b);
+    const int gs = nblk(a.n, 256) < 148 * 8 ? nblk(a.n, 256) : 148 * 8;
+    k_adj_pack_strain<<<gs, 256, 0, s>>>(a, b);
+    k_adj_strain<<<nblk(a.n, 128 / kLanes), 128, 0, s>>>(a, b);
 }
 
 }  // namespace adj

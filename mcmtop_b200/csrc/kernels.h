@@ -104,8 +104,10 @@ struct AdjArgs {
     double *gb[9];       // velocity gradient G (row n = velocity component, column m = derivative)
     const double *pre[NFIELD];   // the step's initial state (snapshot)
     double *theta_b;     // [nmat][kParams], accumulated
+    double4 *rec;        // per cell-order position, kRecSlots double4: what the reverse gathers read of a neighbour
     double dt_prev, dt, dtold;   // dt of the strain/constitutive part, of the update, the one before
 };
+constexpr int kRecSlots = 5;   // double4 slots per position in AdjArgs::rec
 // one reverse step = these three, in this order
 void launch_reverse_momentum(const StepArgs &a, const AdjArgs &b, cudaStream_t s);       // move, velocity, momentum
 void launch_reverse_constitutive(const StepArgs &a, const AdjArgs &b, cudaStream_t s);   // per-particle update

@@ -201,3 +201,24 @@ def test_adjoint_rejects_unsupported(lib):
     with pytest.raises(_abi.MCMError):
         s.adjoint_forward(np.full(3, s.dt), 2)
     s.close()
+
+
+def test_adjoint_regrows_storage_within_a_segment(lib, dts):
+    """A segment whose neighbour table overflows is re-run from its checkpoint
+    after the table has grown: same forward end state, same gradient."""
+    theta = nominal_theta()
+    rng = np.random.default_rng(3)
+    s1, x1, v1 = run(theta, V0, dts)
+    W = rng.standard_normal(x1.shape)
+    pb1, x01, _ = s1.adjoint_backward(W, None)
+    s1.close()
+    s2 = Solver(deck_with(theta, V0), PREC)
+    s2.set_tuning(nbr_stride=8)
+    s2.adjoint_forward(dts, EVERY)
+    st = s2.download(["x", "v"])
+    assert np.array_equal(st["x"], x1) and np.array_equal(st["v"], v1)
+    s2.set_tuning(nbr_stride=8)   # and once more for the backward's recomputation
+    pb2, x02, _ = s2.adjoint_backward(W, None)
+    s2.close()
+    assert np.allclose(pb2, pb1, rtol=1e-12, atol=0.0)
+    assert np.allclose(x02, x01, rtol=1e-9, atol=1e-12 * np.max(np.abs(x01)))
