@@ -116,6 +116,7 @@ struct Sim {
     void sets1(Material &M);
     void sets3(Material &M);
     void sets10(Material &M);
+    int sets4(Material &M);
     // ------------------------------------------------------------- init path
     void initial();
     void init_boundcond();
@@ -161,6 +162,7 @@ struct Sim {
     void f3dm3(Material &M, int i);
     void f3dm9(Material &M, int i);
     void f3dm10(Material &M, int i);
+    int f3dm25(Material &M, int i);
     int sueos(int i);
     int eos1c(int i); int eos4c(int i); int eos13c(int i); int eos28c(int i); int eos41c(int i);
     void aviscosity(int i);
@@ -224,6 +226,52 @@ void Sim::sets3(Material &M) {
     M.cm(2, 6) = prop7;
 }
 
+// MCM/mcm_sets4.f90:21-41 and its initel (:43-98).  Both routines are
+// `implicit double precision (a-h,o-z)`: everything is FP64 except the
+// integer ltype and the single-precision literals (tol = 1.0e-3, 1.e10,
+// 1.e-15 assigned to doubles keep their float values).  initel's Newton loops
+// only print a message past maxit = 200 iterations and keep going; here they
+// stop after 100000 and the material is rejected.
+int Sim::sets4(Material &M) {
+    real alpha = M.cm(1, 3), theta = M.cm(1, 4), gama = M.cm(1, 5), beta = M.cm(1, 6), r = M.cm(2, 1);
+    real xint = M.cm(2, 5);
+    real tempE = (9.0 * M.cm(1, 1) * M.cm(1, 2)) / (3.0 * M.cm(1, 1) + M.cm(1, 2));
+    real tempNi = (3.0 * M.cm(1, 1) - tempE) / (6.0 * M.cm(1, 1));
+    real q1 = tempE * tempNi / ((1.0 + tempNi) * (1.0 - 2.0 * tempNi));
+    real q2 = tempE * 0.5 / (1.0 + tempNi);
+    real q3 = q1 + 2.0 * q2;
+    M.cm(5, 2) = q3;
+    // initel: initial cap kappa0 from X0 = kappa + R Fe(kappa), then the
+    // tension cut-off Fe(fcut) = 0
+    const real tol = F32(1.0e-3f);
+    real capint = 0.0, delcap = F32(1.e10f), delf = F32(1.e10f), fcut = 0.0;
+    for (int it = 0;; ++it) {
+        real fe = alpha - gama * std::exp(-beta * capint) + theta * capint;
+        real psik = xint - capint - r * fe;
+        real err1 = std::fabs(psik);
+        real err2 = std::fabs(delcap) / (std::fabs(capint) + F32(1.e-15f));
+        if (!((err1 > tol) && (err2 > tol))) break;
+        if (it > 100000) return MCMO_EINVAL;
+        real fep = beta * gama * std::exp(-beta * capint) + theta;
+        real dpsik = -1.0 - r * fep;
+        delcap = psik / dpsik;
+        capint = capint - delcap;
+    }
+    for (int it = 0;; ++it) {
+        real fe = alpha - gama * std::exp(-beta * fcut) + theta * fcut;
+        real err1 = std::fabs(fe);
+        real err2 = std::fabs(delf) / (std::fabs(fcut) + F32(1.e-15f));
+        if (!((err1 > tol) && (err2 > tol))) break;
+        if (it > 100000) return MCMO_EINVAL;
+        real fep = gama * beta * std::exp(-beta * fcut) + theta;
+        delf = fe / fep;
+        fcut = fcut - delf;
+    }
+    M.cm(3, 3) = capint;
+    M.cm(3, 4) = fcut;
+    return MCMO_OK;
+}
+
 // MCM/mcm_sets10.f90:21-35
 void Sim::sets10(Material &M) {
     real prop[48];
@@ -282,7 +330,8 @@ int Sim::setup(const mcmo_deck *d, const mcmo_material *m, const double *x, cons
                 if (M.eos != 0) return MCMO_EINVAL;
                 break;
             case 4:
-                return MCMO_EUNSUPPORTED;
+                if (M.eos != 0) return MCMO_EINVAL;
+                break;
             case 9: case 10:
                 if (!(M.eos == 1 || M.eos == 4 || M.eos == 13 || M.eos == 28 || M.eos == 41)) return MCMO_EINVAL;
                 break;
@@ -290,6 +339,7 @@ int Sim::setup(const mcmo_deck *d, const mcmo_material *m, const double *x, cons
         }
         if (M.model == 1) sets1(M);
         else if (M.model == 3) sets3(M);
+        else if (M.model == 4) { if (sets4(M) != MCMO_OK) return MCMO_EINVAL; }
         else if (M.model == 10) sets10(M);
     }
     // symmetry planes: MCM/mcm_inp_symmetry_v2.f90:83-137
@@ -440,6 +490,11 @@ void Sim::calcrhopc() {
                 if (init_rhoe != 1) { P.rho = P.rho0; P.e = 0.0; }
                 P.p = 0.0;
                 P.c = std::sqrt(mat[P.mat].strinput[1] / P.rho);
+                break;
+            case 4:   // MCM/mcm_calcrhopc.f90:57-67: strinput(10) = cm(5,2), set by mcm_sets4
+                if (init_rhoe != 1) { P.rho = P.rho0; P.e = 0.0; }
+                P.p = 0.0;
+                P.c = std::sqrt(mat[P.mat].strinput[9] / P.rho);
                 break;
             case 9: {
                 eoscalc(i);
@@ -1072,17 +1127,22 @@ int Sim::constitutive() {
     rhoupd();
     for (int m = 1; m <= nummat; ++m) {
         int md = mat[m].model;
-        if (md != 1 && md != 3 && md != 9 && md != 10) return MCMO_EUNSUPPORTED;
+        if (md != 1 && md != 3 && md != 4 && md != 9 && md != 10) return MCMO_EUNSUPPORTED;
     }
-    int bad = 0;
+    int bad = 0, cap_bad = 0;
 #ifdef _OPENMP
-#pragma omp parallel for schedule(static) reduction(max : bad)
+#pragma omp parallel for schedule(static) reduction(max : bad, cap_bad)
 #endif
     for (int nn = ssp; nn <= esp; ++nn) {
         Material &M = mat[par[nn].mat];
         switch (M.model) {
             case 1: stress_rot1(nn); f3dm1(M, nn); aviscosity(nn); lieupd(nn); break;
             case 3: stress_rot1(nn); f3dm3(M, nn); aviscosity(nn); lieupd(nn); break;
+            case 4:
+                stress_rot1(nn);
+                if (f3dm25(M, nn) != MCMO_OK) cap_bad = 1;
+                aviscosity(nn); lieupd(nn);
+                break;
             case 9: {
                 stress_rot1(nn); f3dm9(M, nn);
                 if (sueos(nn) != MCMO_OK) bad = 1;
@@ -1099,6 +1159,7 @@ int Sim::constitutive() {
         }
     }
     calccritts();
+    if (cap_bad) return MCMO_ECAP_NOCONV;
     return bad ? MCMO_ECOMPLEX_C : MCMO_OK;
 }
 
@@ -1676,6 +1737,352 @@ void Sim::lieupd(int nn) {
     for (int l = 0; l < 3; ++l)
         for (int k = 0; k < 3; ++k) qpm = qpm + P.q[k][l] * P.rod[k][l];
     P.e = P.e + (P.einc - dt * qpm) * P.mass / P.rho;
+}
+
+// ------------------------------------------------------------ cap model
+// Model 4: the generalised cap model of MCM/mcm_f3dm25.f90 (f3dm25a :37-827,
+// feit :906-966, fcit :968-1038).  f3dm25a has no `implicit none`: every local
+// it does not declare is default REAL (single precision; names i-n INTEGER).
+// Those locals are float here, the declared ones (sig*, dd*, p, bulk, capan,
+// davgm, gdt, gd2, ...) double, and mixed expressions are evaluated in the
+// wider kind, left to right.  Single-precision exp is taken as the correctly
+// rounded float of a double exp (fexp); sqrt and the four operations are IEEE
+// in both kinds.  Quirks kept:
+//  * the local `capa` (not par%capa) is never assigned: static and zero under
+//    /Qsave, so the first Fe of :197 is Fe(0);
+//  * only the upper triangle of sigma is written back (:813-815): the lower
+//    triangle keeps the rotated stress of mcm_stress_rot1, which the next
+//    rotation (sigma(3,1)) and the momentum sum read;
+//  * `nplot = cm(2,5)` and `xint = cm(2,5)` (mcm_sets4.f90:28) share a slot,
+//    while f3dm25 reads X0 for the hardening law from cm(2,4) (`z`).
+// A return-map iteration that does not converge (feit/fcit, 100 iterations)
+// stops the reference; here it returns MCMO_ECAP_NOCONV.
+
+inline float fexp(float x) { return (float)std::exp((double)x); }
+
+struct CapConst {
+    float shear, alpha, theta, gama, beta, r, dDyna, w, z, tcut, fcut;
+    double bulk;
+    int ltype, ivec;
+};
+
+// One iteration of the failure-surface return (feit :923-960 and the
+// unrolled copies of f3dm25a :491-596).  capa is par%capa (double).
+static void cap_fail_iter(const CapConst &C, double &capa, double sig[6], float s[6], float &x1, float &x2d) {
+    float xk = (float)(capa + C.r * (C.alpha - C.gama * std::exp(-C.beta * capa) + C.theta * capa));
+    float dhdk = (float)((C.w * C.dDyna * fexp(-C.dDyna * xk)) *
+                         (1.0 + C.r * (C.theta + C.gama * C.beta * std::exp(-C.beta * capa))));
+    float omega = C.theta + C.gama * C.beta * fexp(-C.beta * x1);
+    float dcd = (float)(C.shear + 9.0 * C.bulk * (double)(omega * omega));
+    float f = x2d - (C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1);
+    float delcap = -(3.0f * omega * f / (dcd * dhdk));
+    float delam = -(dhdk * delcap / (3.0f * omega));
+    capa = capa + delcap;
+    (void)xk;
+    float fac1 = C.shear / x2d;
+    float fac2 = (float)(3.0 * C.bulk * omega);
+    sig[0] = sig[0] - delam * (fac1 * s[0] - fac2);
+    sig[1] = sig[1] - delam * (fac1 * s[1] - fac2);
+    sig[2] = sig[2] - delam * (fac1 * s[2] - fac2);
+    sig[3] = sig[3] - delam * fac1 * s[3];
+    sig[4] = sig[4] - delam * fac1 * s[4];
+    sig[5] = sig[5] - delam * fac1 * s[5];
+    x1 = (float)(sig[0] + sig[1] + sig[2]);
+    s[0] = (float)(sig[0] - x1 / 3.0f);
+    s[1] = (float)(sig[1] - x1 / 3.0f);
+    s[2] = (float)(sig[2] - x1 / 3.0f);
+    s[3] = (float)sig[3];
+    s[4] = (float)sig[4];
+    s[5] = (float)sig[5];
+    x2d = std::sqrt(0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+}
+
+// One iteration of the cap return (fcit :986-1022 and f3dm25a :652-800).
+// Returns the cap function value of the convergence test of fcit (:1023) and
+// the elcap of the iteration (before the capa update).
+static float cap_cap_iter(const CapConst &C, double &capa, double sig[6], float s[6], float &x1, float &x2d,
+                          float &elcap_out) {
+    const float unit = 1.0f;
+    float xk = (float)(capa + C.r * (C.alpha - C.gama * std::exp(-C.beta * capa) + C.theta * capa));
+    float dhdk = (float)((C.w * C.dDyna * fexp(-C.dDyna * xk)) *
+                         (1.0 + C.r * (C.theta + C.gama * C.beta * std::exp(-C.beta * capa))));
+    float dfdk;
+    if (capa >= 0.0) {
+        dfdk = (float)(-(2.0f * (std::fabs((double)x1 - capa) / (double)(C.r * C.r) +
+                                 (C.alpha - C.gama * std::exp(-C.beta * capa) + C.theta * capa) *
+                                     (C.theta + C.gama * C.beta * std::exp(-C.beta * capa)))));
+    } else {
+        dfdk = (float)(-(((2.0f * xk) * (1.0 + C.r * (C.theta + C.gama * C.beta * std::exp(-C.beta * capa)))) /
+                         (double)(C.r * C.r)));
+    }
+    float elcap = (float)std::max(capa, (double)(0.0f * unit));
+    float omega = std::min(-(2.0f * std::fabs(x1 - elcap) / (C.r * C.r)), -1.e-15f * unit);
+    float dcd = (float)((4.0f * C.shear * (x2d * x2d)) +
+                        9.0 * C.bulk * (double)((2.0f * (x1 - elcap) / (C.r * C.r)) * (2.0f * (x1 - elcap) / (C.r * C.r))));
+    float f = x2d * x2d + (x1 - elcap) * (x1 - elcap) / (C.r * C.r) - (xk - elcap) * (xk - elcap) / (C.r * C.r);
+    float delcap = -(f / (dfdk + (dcd * dhdk) / (3.0f * omega)));
+    float delam = -(dhdk * delcap / (3.0f * omega));
+    capa = capa + delcap;
+    xk = (float)(capa + C.r * (C.alpha - C.gama * std::exp(-C.beta * capa) + C.theta * capa));
+    float fac1 = 2.0f * C.shear;
+    float fac2 = (float)(6.0 * C.bulk * (double)std::fabs(x1 - elcap) / (double)(C.r * C.r));
+    sig[0] = sig[0] - delam * (fac1 * s[0] + fac2);
+    sig[1] = sig[1] - delam * (fac1 * s[1] + fac2);
+    sig[2] = sig[2] - delam * (fac1 * s[2] + fac2);
+    sig[3] = sig[3] - delam * fac1 * s[3];
+    sig[4] = sig[4] - delam * fac1 * s[4];
+    sig[5] = sig[5] - delam * fac1 * s[5];
+    x1 = (float)(sig[0] + sig[1] + sig[2]);
+    s[0] = (float)(sig[0] - x1 / 3.0f);
+    s[1] = (float)(sig[1] - x1 / 3.0f);
+    s[2] = (float)(sig[2] - x1 / 3.0f);
+    s[3] = (float)sig[3];
+    s[4] = (float)sig[4];
+    s[5] = (float)sig[5];
+    x2d = std::sqrt(0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+    elcap_out = elcap;
+    return x2d * x2d + (x1 - elcap) * (x1 - elcap) / (C.r * C.r) - (xk - elcap) * (xk - elcap) / (C.r * C.r);
+}
+
+int Sim::f3dm25(Material &M, int i) {
+    Particle &P = par[i];
+    const float unit = 1.0f, third = 1.0f / 3.0f, geop = 0.0f, tol = 1.0e-7f;
+    CapConst C;
+    C.bulk = M.cm(1, 1);
+    C.shear = (float)M.cm(1, 2);
+    C.alpha = (float)M.cm(1, 3);
+    C.theta = (float)M.cm(1, 4);
+    C.gama = (float)M.cm(1, 5);
+    C.beta = (float)M.cm(1, 6);
+    C.r = (float)M.cm(2, 1);
+    C.dDyna = (float)M.cm(2, 2);
+    C.w = (float)M.cm(2, 3);
+    const float falfac = (float)M.cm(4, 1);
+    C.alpha = C.alpha - falfac;
+    C.z = (float)M.cm(2, 4);
+    C.ivec = (M.cm(3, 5) != 0.0) ? 0 : 1;
+    C.ltype = (int)M.cm(2, 6);
+    C.tcut = (float)M.cm(3, 1);
+    C.fcut = (float)M.cm(3, 4);
+    const float t = std::max(C.fcut, C.tcut + 3.0f * geop);
+    const float fet = C.alpha - C.gama * fexp(-C.beta * t) + C.theta * t;
+    const float fept = C.gama * C.beta * fexp(-C.beta * t) + C.theta;
+    P.capa = std::max(P.capa, M.cm(3, 3));
+    double sig[6] = {-P.sigma[0][0], -P.sigma[1][1], -P.sigma[2][2], -P.sigma[0][1], -P.sigma[0][2], -P.sigma[1][2]};
+    const double dd1 = -P.rod[0][0], dd2 = -P.rod[1][1], dd3 = -P.rod[2][2];
+    const double dd4 = -P.rod[0][1] / 2.0, dd5 = -P.rod[0][2] / 2.0, dd6 = -P.rod[1][2] / 2.0;
+    const double dd = (dd1 + dd2 + dd3);
+    const double davgm = (double)(1.0f / 3.0f) * dd;
+    const float dt1 = (float)dt;
+    double p = 3.0 * C.bulk * (double)dt1 * davgm;
+    const double gdt = dt * (double)C.shear;
+    const double gd2 = 2.0 * gdt;
+    const float gtr11 = (float)(sig[0] + p + gd2 * (dd1 - davgm));
+    const float gtr22 = (float)(sig[1] + p + gd2 * (dd2 - davgm));
+    const float gtr33 = (float)(sig[2] + p + gd2 * (dd3 - davgm));
+    const float gtr12 = (float)(sig[3] + gd2 * dd4);
+    const float gtr23 = (float)(sig[4] + gd2 * dd5);
+    const float gtr31 = (float)(sig[5] + gd2 * dd6);
+    const float x1tr = gtr11 + gtr22 + gtr33;
+    float s[6];
+    s[0] = gtr11 - (1.0f / 3.0f) * x1tr;
+    s[1] = gtr22 - (1.0f / 3.0f) * x1tr;
+    s[2] = gtr33 - (1.0f / 3.0f) * x1tr;
+    const float sdtr11 = s[0], sdtr22 = s[1], sdtr33 = s[2];
+    float x2dtr = 0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + 2.0f * (gtr12 * gtr12 + gtr23 * gtr23 + gtr31 * gtr31));
+    x2dtr = std::sqrt(x2dtr);
+    const float capa_local = 0.0f;   // never assigned in f3dm25a (see above)
+    float fe = C.alpha - C.gama * fexp(-C.beta * capa_local) + C.theta * capa_local;
+    const float xkn = capa_local + C.r * fe;
+    const float elcapn = (float)std::max(P.capa, (double)(0.0f * unit));
+    const float tmises = std::fabs(xkn - elcapn) / C.r;
+    fe = C.alpha - C.gama * fexp(-C.beta * x1tr) + C.theta * x1tr;
+    const float f1tr = x2dtr - std::min(fe, tmises);
+    const float tcrit = (float)((double)t - 9.0 * C.bulk / (double)C.shear * (double)(x2dtr - fet) * (double)fept);
+    fe = C.alpha - C.gama * fexp(-C.beta * elcapn) + C.theta * elcapn;
+    const float fep = C.beta * C.gama * fexp(-C.beta * elcapn) + C.theta;
+    const float fc2tr = ((xkn - elcapn) * (xkn - elcapn) - (x1tr - elcapn) * (x1tr - elcapn)) / (C.r * C.r);
+    const float f2tr = x2dtr * x2dtr - fc2tr;
+    const float x1crt = (float)((double)elcapn - ((double)((x2dtr - fe) * 9.0f) * C.bulk) * (double)fep / (double)C.shear);
+    fe = (float)(C.alpha - C.gama * std::exp(-C.beta * P.capa) + C.theta * P.capa);
+    const float capal = (float)std::min((double)(0.0f * unit), P.capa - (double)(tol * fe));
+    fe = C.alpha - C.gama * fexp(-C.beta * capal) + C.theta * capal;
+    const float xk0 = capal + C.r * fe;
+    const float evpn = C.w * (1.0f - fexp(C.dDyna * (C.z - xkn)));
+    const float devpb = C.w * (1.0f - fexp(C.dDyna * (C.z - xk0))) - evpn;
+    const double capan = P.capa;
+    const int ltype = C.ltype;
+    // mode selection (:219-253)
+    int imode = 0;
+    if ((x1tr <= t) && (x2dtr <= fet) && (ltype == 1) && (capan > 0.0) && (devpb >= 0.0f)) imode = 2;
+    else if ((x1tr <= t) && (x2dtr <= fet) && (ltype == 1) && (capan > 0.0) && (devpb < 0.0f)) imode = 7;
+    else if ((x1tr <= t) && (x2dtr <= fet) && ((ltype == 2) || (capan <= 0.0))) imode = 3;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && (ltype == 1) && (capan > 0.0) && (devpb >= 0.0f)) imode = 4;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && (ltype == 1) && (capan > 0.0) && (devpb < 0.0f)) imode = 6;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && ((ltype == 2) || (capan <= 0.0))) imode = 5;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr > tcrit) && (capan >= 0.0)) imode = 10;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr > tcrit) && (capan < 0.0)) imode = 8;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr <= tol)) imode = 1;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr >= x1crt)) imode = 9;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr < x1crt) && (capan >= 0.0)) imode = 10;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr < x1crt) && (capan < 0.0)) imode = 8;
+    else if ((x1tr > t) && (x1tr > elcapn) && (f2tr < tol)) imode = 1;
+    else if ((x1tr > t) && (x1tr > elcapn) && (f2tr >= tol)) imode = 11;
+    P.ptype = imode;
+    float x1 = 0.0f, x2d = 0.0f, ratio = 0.0f;
+    auto set_scaled = [&](const float *sd, float rat) {   // sig = s*ratio + p, off-diagonals gtr*ratio
+        sig[0] = (double)(sd[0] * rat) + p;
+        sig[1] = (double)(sd[1] * rat) + p;
+        sig[2] = (double)(sd[2] * rat) + p;
+        sig[3] = (double)(gtr12 * rat);
+        sig[4] = (double)(gtr23 * rat);
+        sig[5] = (double)(gtr31 * rat);
+    };
+    auto set_plain = [&]() {   // sig = s + p, off-diagonals gtr
+        sig[0] = (double)s[0] + p;
+        sig[1] = (double)s[1] + p;
+        sig[2] = (double)s[2] + p;
+        sig[3] = (double)gtr12;
+        sig[4] = (double)gtr23;
+        sig[5] = (double)gtr31;
+    };
+    auto move_cap = [&]() {   // modes 6 and 7 (:359-364, :381-386)
+        const float x1old = (float)(sig[0] + sig[1] + sig[2]);
+        const float devp = (float)(dd - (double)(x1 - x1old) / (3.0 * C.bulk));
+        const float xhat = std::min(devpb, devp);
+        P.capa = P.capa + (double)devp * ((double)capal - capan) / (double)xhat;
+        P.capa = std::max(P.capa, (double)(0.0f * unit));
+    };
+    switch (imode) {
+        case 1:
+            x1 = x1tr; x2d = x2dtr; P.capa = capan;
+            p = (double)(third * x1 + geop);
+            set_plain();
+            break;
+        case 2:
+            x1 = t; x2d = x2dtr; P.capa = 0.0;
+            p = (double)(third * x1 + geop);
+            set_plain();
+            break;
+        case 3:
+            x1 = t; x2d = x2dtr; P.capa = capan;
+            p = (double)(third * x1 + geop);
+            set_plain();
+            break;
+        case 4:
+            x1 = t; x2d = fet; P.capa = 0.0;
+            p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr;
+            set_scaled(s, ratio);
+            break;
+        case 5:
+            x1 = t; x2d = fet; P.capa = capan;
+            p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr;
+            set_scaled(s, ratio);
+            break;
+        case 6:
+            x1 = t; x2d = fet;
+            move_cap();
+            p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr;
+            set_scaled(s, ratio);
+            break;
+        case 7:
+            x1 = t; x2d = x2dtr;
+            move_cap();
+            p = (double)(third * x1 + geop);
+            set_plain();
+            break;
+        case 8:
+            x1 = x1tr;
+            fe = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            x2d = std::min(fe, tmises);
+            P.capa = capan;
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            set_scaled(s, ratio);
+            break;
+        case 9:
+            x1 = elcapn;
+            x2d = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            P.capa = capan;
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            set_scaled(s, ratio);
+            break;
+        case 10: {
+            double sg[6] = {gtr11, gtr22, gtr33, gtr12, gtr23, gtr31};
+            P.capa = capan;
+            x1 = x1tr;
+            x2d = x2dtr;
+            float si[6];
+            for (int k = 0; k < 3; ++k) si[k] = (float)(sg[k] - x1tr / 3.0f);
+            for (int k = 3; k < 6; ++k) si[k] = (float)sg[k];
+            if (C.ivec == 0) {
+                // feit: iterate to |f| <= 1e-8 (at most 100 iterations)
+                bool conv = false;
+                for (int it = 1; it <= 100; ++it) {
+                    cap_fail_iter(C, P.capa, sg, si, x1, x2d);
+                    const float f = x2d - (C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1);
+                    if (std::fabs(f) <= 1.0e-8f) { conv = true; break; }
+                }
+                if (!conv) return MCMO_ECAP_NOCONV;
+            } else {
+                for (int it = 0; it < 4; ++it) cap_fail_iter(C, P.capa, sg, si, x1, x2d);
+            }
+            if (x1 > elcapn) x1 = elcapn;
+            if ((ltype == 2) || (capan == 0.0)) P.capa = capan;
+            if ((double)x1 > P.capa) P.capa = x1;
+            if ((ltype == 1) && (capan >= 0.0)) P.capa = std::max(P.capa, (double)(0.0f * unit));
+            fe = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            x2d = std::min(fe, tmises);
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            if (C.ivec == 0) {
+                set_scaled(s, ratio);
+            } else {
+                const float sd[3] = {sdtr11, sdtr22, sdtr33};
+                set_scaled(sd, ratio);
+            }
+            break;
+        }
+        case 11: {
+            double sg[6] = {gtr11, gtr22, gtr33, gtr12, gtr23, gtr31};
+            P.capa = capan;
+            x1 = x1tr;
+            x2d = x2dtr;
+            float si[6];
+            for (int k = 0; k < 3; ++k) si[k] = (float)(sg[k] - x1tr / 3.0f);
+            for (int k = 3; k < 6; ++k) si[k] = (float)sg[k];
+            float elcap = 0.0f;
+            bool done = false;
+            const int nit = (C.ivec == 0) ? 100 : 4;
+            for (int it = 1; it <= nit; ++it) {
+                const float f = cap_cap_iter(C, P.capa, sg, si, x1, x2d, elcap);
+                if (C.ivec == 0 && std::fabs(f) <= 1.0e-8f) { done = true; break; }
+            }
+            if (C.ivec == 0 && !done) return MCMO_ECAP_NOCONV;
+            if (x1 < elcap) {
+                x1 = elcap + std::fabs(x1 - elcap);
+                sg[0] = (double)(si[0] + x1 / 3.0f);
+                sg[1] = (double)(si[1] + x1 / 3.0f);
+                sg[2] = (double)(si[2] + x1 / 3.0f);
+            }
+            for (int k = 0; k < 6; ++k) sig[k] = sg[k];
+            break;
+        }
+        default: break;
+    }
+    // write-back (:813-827): the upper triangle only
+    P.sigma[0][0] = -sig[0];
+    P.sigma[1][1] = -sig[1];
+    P.sigma[2][2] = -sig[2];
+    P.sigma[0][1] = -sig[3];
+    P.sigma[0][2] = -sig[4];
+    P.sigma[1][2] = -sig[5];
+    P.p = -(1.0 / 3.0) * (P.sigma[0][0] + P.sigma[1][1] + P.sigma[2][2]);
+    return MCMO_OK;
 }
 
 // MCM/mcm_calccritts.f90:32-87
