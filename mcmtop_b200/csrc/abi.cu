@@ -98,6 +98,7 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.rec0, np))) return st;
     if ((st = dalloc(h, &h->A.rec1, np))) return st;
     if ((st = dalloc(h, &h->A.rec2, np))) return st;
+    if (h->A.prm.asym && (st = dalloc(h, &h->A.rec3, np))) return st;
     // partial vectors: one per block of the cooperative momentum kernel (at
     // least 16 particles per block of 256 threads, at most 148 x 16 blocks
     // for narrower blocks) or of the per-particle kernels (256 threads)
@@ -139,6 +140,7 @@ int alloc_ghosts(mcm_gpu_handle *h, int cap) {
     if ((st = dalloc(h, &h->A.grec0, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec1, (size_t)cap))) return st;
     if ((st = dalloc(h, &h->A.grec2, (size_t)cap))) return st;
+    if (h->A.prm.asym && (st = dalloc(h, &h->A.grec3, (size_t)cap))) return st;
     if (h->cfg.precision == MCM_PREC_MIXED) {
         if ((st = dalloc(h, &h->A.gfrec1, (size_t)cap))) return st;
         if ((st = dalloc(h, &h->A.gfrec2, (size_t)cap))) return st;
@@ -317,6 +319,17 @@ int put_sym(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &t
     return MCM_OK;
 }
 
+// the lower triangle (2,1), (3,1), (3,2) of a Fortran (3,3,np) tensor
+int put_lower(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
+    static const int rc[3][2] = {{1, 0}, {2, 0}, {2, 1}};
+    const int n = h->np;
+    for (int t = 0; t < 3; ++t) {
+        for (int i = 0; i < n; ++i) tmp[i] = src[9 * (size_t)i + rc[t][0] + 3 * rc[t][1]];
+        CK(cudaMemcpy(h->A.F.f[f0 + t], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    return MCM_OK;
+}
+
 int put_scalar(mcm_gpu_handle *h, const double *src, int f) {
     CK(cudaMemcpy(h->A.F.f[f], src, sizeof(double) * h->np, cudaMemcpyHostToDevice));
     return MCM_OK;
@@ -418,8 +431,49 @@ int mcm_gpu_material_from_deck(mcm_gpu_material *m) {
             if (!(m->eos == 1 || m->eos == 4 || m->eos == 13 || m->eos == 28 || m->eos == 41)) return MCM_EINVAL;
             break;
         }
-        case 4:
-            return MCM_EUNSUPPORTED;
+        case 4: {
+            // MCM/mcm_sets4.f90:21-41: the elastic modulus cm(5,2) = lambda + 2 mu
+            // from K and G, then initel (:43-98, implicit double precision,
+            // single-precision literals kept): the initial cap kappa0 with
+            // X0 = kappa0 + R Fe(kappa0), X0 = cm(2,5), and the tension cut-off
+            // Fe(fcut) = 0, by Newton iterations to an absolute/relative
+            // tolerance of 1e-3.  The reference only prints a warning past 200
+            // iterations and keeps going; here a material that needs more
+            // than 100000 is rejected.
+            if (m->eos != 0) return MCM_EINVAL;
+            const double alpha = C(1, 3), theta = C(1, 4), gama = C(1, 5), beta = C(1, 6), r = C(2, 1);
+            const double xint = C(2, 5);
+            const double tempE = (9.0 * C(1, 1) * C(1, 2)) / (3.0 * C(1, 1) + C(1, 2));
+            const double tempNi = (3.0 * C(1, 1) - tempE) / (6.0 * C(1, 1));
+            const double q1 = tempE * tempNi / ((1.0 + tempNi) * (1.0 - 2.0 * tempNi));
+            const double q2 = tempE * 0.5 / (1.0 + tempNi);
+            C(5, 2) = q1 + 2.0 * q2;
+            const double tol = (double)1.0e-3f, tiny = (double)1.e-15f;
+            double capint = 0.0, delcap = (double)1.e10f, delf = (double)1.e10f, fcut = 0.0;
+            for (int it = 0;; ++it) {
+                const double fe = alpha - gama * std::exp(-beta * capint) + theta * capint;
+                const double psik = xint - capint - r * fe;
+                if (!((std::fabs(psik) > tol) && (std::fabs(delcap) / (std::fabs(capint) + tiny) > tol))) break;
+                if (it > 100000) return MCM_EINVAL;
+                const double fep = beta * gama * std::exp(-beta * capint) + theta;
+                delcap = psik / (-1.0 - r * fep);
+                capint = capint - delcap;
+            }
+            for (int it = 0;; ++it) {
+                const double fe = alpha - gama * std::exp(-beta * fcut) + theta * fcut;
+                if (!((std::fabs(fe) > tol) && (std::fabs(delf) / (std::fabs(fcut) + tiny) > tol))) break;
+                if (it > 100000) return MCM_EINVAL;
+                const double fep = gama * beta * std::exp(-beta * fcut) + theta;
+                delf = fe / fep;
+                fcut = fcut - delf;
+            }
+            C(3, 3) = capint;
+            C(3, 4) = fcut;
+            const int ltype = (int)C(2, 6);
+            if (ltype != 1 && ltype != 2) return MCM_EINVAL;   // the mode table of f3dm25 covers soil and rock
+            m->g = cm[5];   // MCM/mcm_calcg.f90:43-45: cm(1,2), the shear modulus
+            break;
+        }
         default:
             return MCM_EINVAL;
     }
@@ -436,11 +490,15 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     if (cfg->disctype != 0 && cfg->disctype != 1) return MCM_EINVAL;
     if (cfg->tcrit_opt < 0 || cfg->tcrit_opt > 2) return MCM_EINVAL;
     if (cfg->precision < 0 || cfg->precision > 2) return MCM_EINVAL;
+    bool cap_model = false;
     for (int m = 0; m < nmat; ++m) {
         int md = mats[m].model;
-        if (md == 4) return MCM_EUNSUPPORTED;
-        if (md != 1 && md != 3 && md != 9 && md != 10) return MCM_EINVAL;
+        if (md != 1 && md != 3 && md != 4 && md != 9 && md != 10) return MCM_EINVAL;
+        cap_model = cap_model || md == 4;
     }
+    // the cap model leaves sigma asymmetric, which only the FP64-exact simple-SPH
+    // momentum sum reads (both triangles); the other gathers carry 6 components
+    if (cap_model && (cfg->precision != MCM_PREC_FP64_EXACT || cfg->disctype != 0)) return MCM_EUNSUPPORTED;
     if (cfg->boundary) {
         for (int d = 0; d < 3; ++d) {
             bool p0 = cfg->boundary_code[2 * d] == 2, p1 = cfg->boundary_code[2 * d + 1] == 2;
@@ -469,6 +527,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->A.nmat = nmat;
     h->A.split_mode = 1;
     h->A.prm = make_params(h->cfg, nmat);
+    h->A.prm.asym = cap_model ? 1 : 0;
     // materials
     std::vector<DevMaterial> dm(nmat);
     for (int m = 0; m < nmat; ++m) {
@@ -528,7 +587,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,
-                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr};
+                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr, h->A.rec3, h->A.grec3};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (double *p : h->adj_ckpt)
@@ -710,6 +769,7 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     for (auto &s : sc)
         if (s.p && (st = put_scalar(h, s.p, s.f))) return st;
     if (f->sigma && (st = put_sym(h, f->sigma, FS11, tmp))) return st;
+    if (f->sigma && (st = put_lower(h, f->sigma, FL21, tmp))) return st;
     if (f->s && (st = put_sym(h, f->s, FD11, tmp))) return st;
     if (f->alfa && (st = put_sym(h, f->alfa, FA11, tmp))) return st;
     if (f->rod && (st = put_sym(h, f->rod, FR11, tmp))) return st;
@@ -938,6 +998,14 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     for (auto &s : sc)
         if (s.p && (st = scal(s.p, s.f))) return st;
     if (f->sigma && (st = sym(f->sigma, FS11))) return st;
+    if (f->sigma) {
+        // the lower triangle as stored (it differs from the upper one for the cap model)
+        static const int rc[3][2] = {{1, 0}, {2, 0}, {2, 1}};
+        for (int t = 0; t < 3; ++t) {
+            int s2 = get(FL21 + t); if (s2) return s2;
+            for (int p = 0; p < n; ++p) f->sigma[9 * (size_t)orig[p] + rc[t][0] + 3 * rc[t][1]] = tmp[p];
+        }
+    }
     if (f->s && (st = sym(f->s, FD11))) return st;
     if (f->alfa && (st = sym(f->alfa, FA11))) return st;
     if (f->rod && (st = sym(f->rod, FR11))) return st;

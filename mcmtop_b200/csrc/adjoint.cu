@@ -402,6 +402,7 @@ __device__ __forceinline__ void constitutive_pass(int pass, const StepArgs &a, c
     P.q = D(0.0);
 #pragma unroll
     for (int k = 0; k < kND; ++k) seed(P, M, pass * kND + k, k);
+    sym_lower(P);   // model 10: the lower triangle is the (seeded) upper one
     P.etry = D(0.0); P.einc = D(0.0); P.rhoold = P.rho;
     const D dt = D(b.dt_prev);
     rhoupd(P, M, dt, 3);

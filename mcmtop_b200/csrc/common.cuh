@@ -62,6 +62,8 @@ struct DevPlanes {
 // Run options used inside kernels.
 struct DevParams {
     int ndim, disctype, tcrit_opt, boundary, baseaccel, drelax, nmat, diag;
+    int asym;         // a material of the cap model is present: the momentum sum reads both triangles of sigma
+    int pad_;
     double drelax_scale, tssf, hmax;
     double base_a[3];
     DevPlanes planes;
@@ -80,6 +82,9 @@ enum Field {
     FR11, FR22, FR33, FR12, FR13, FR23,      // rod
     FW12, FW13, FW23,                        // spin
     FTR, FETRY, FEINC, FRHOOLD, FMINDIST, FCRITTS, FAX, FAY, FAZ,
+    // lower triangle of sigma (21, 31, 32): equal to the upper one except for
+    // the cap model, whose return map writes the upper triangle only
+    FL21, FL31, FL32,
     NFIELD
 };
 

@@ -6,6 +6,8 @@
 // multiply-add reproduces the reference arithmetic; single-precision Fortran
 // literals appear as float literals cast to T.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "dual.cuh"
 
@@ -20,6 +22,8 @@ struct PState {
     T mass, h, hold, rho, rho0, rhoold, e, etry, einc, p, c;
     T efps, pcut, p_cut, fail, capa;
     T sig[6], s[6], alfa[6];
+    T sigl[3];     // lower triangle of sigma: (2,1), (3,1), (3,2)
+    int ptype;     // cap model mode (MCM/mcm_f3dm25.f90:257)
     T rod[6];      // rate of deformation (symmetric)
     T spin[3];     // spin(1,2), spin(1,3), spin(2,3)
     T tracerod;
@@ -69,7 +73,9 @@ __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
     const T etol = T(1.0e-3f);
     const T z1 = T(1.0) / T(3.0), z2 = T(2.0) / T(15.0), z3 = T(17.0) / T(315.0), z4 = T(62.0) / T(2835.0);
     const T s11 = P.sig[T11], s22 = P.sig[T22], s33 = P.sig[T33];
-    const T s12 = P.sig[T12], s23 = P.sig[T23], s31 = P.sig[T13];
+    // the reference reads sigma(1,2), sigma(2,3) and sigma(3,1): the upper
+    // triangle except for (3,1) (MCM/mcm_stress_rot1.f90:40-48, 243-259)
+    const T s12 = P.sig[T12], s23 = P.sig[T23], s31 = P.sigl[1];
     T dt2 = T(0.5f) * dt;
     T wzz = -dt2 * P.spin[0];
     T wyy = dt2 * P.spin[1];
@@ -116,6 +122,18 @@ __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
     P.sig[T12] = qs11 * q21 + qs12 * q22 + qs13 * q23;
     P.sig[T23] = qs21 * q31 + qs22 * q32 + qs23 * q33;
     P.sig[T13] = qs11 * q31 + qs12 * q32 + qs13 * q33;
+    P.sigl[0] = P.sig[T12];
+    P.sigl[1] = P.sig[T13];
+    P.sigl[2] = P.sig[T23];
+}
+
+// The symmetric writes of the other models (MCM/mcm_f3dm1.f90:58-60,
+// mcm_f3dm3.f90:69-71, mcm_stress_up.f90:35-37): lower triangle = upper.
+template <typename T>
+__device__ __forceinline__ void sym_lower(PState<T> &P) {
+    P.sigl[0] = P.sig[T12];
+    P.sigl[1] = P.sig[T13];
+    P.sigl[2] = P.sig[T23];
 }
 
 // ------------------------------------------------------------- EOS: sound speed
@@ -653,6 +671,323 @@ __device__ __forceinline__ void f3dm10(PState<T> &P, const Mat &M, T dt) {
     }
 }
 
+// ---------------------------------------------------------------- cap model
+// Model 4, the generalised cap model of MCM/mcm_f3dm25.f90 (f3dm25a :37-827,
+// feit :906-966, fcit :968-1038).  f3dm25a has no `implicit none`: its
+// undeclared locals are single precision, so they are float here, the
+// declared ones double, and mixed expressions are evaluated in the wider kind,
+// left to right (this translation unit has no fused multiply-add).  Single-
+// precision exp is the correctly rounded float of a double exp.  Quirks kept:
+// the local `capa` of :197 is never assigned (static zero), only the upper
+// triangle of sigma is written back (:813-815), X0 of the hardening law is
+// cm(2,4) while the initial cap used cm(2,5).  The iterated returns (vector
+// flag cm(3,5) /= 0) stop the reference when unconverged after 100
+// iterations; here the particle reports MCM_ECAP_NOCONV.
+namespace cap {
+
+__device__ __forceinline__ float fexp(float x) { return (float)exp((double)x); }
+template <typename U> __device__ __forceinline__ U vmin(U a, U b) { return (b < a) ? b : a; }
+template <typename U> __device__ __forceinline__ U vmax(U a, U b) { return (a < b) ? b : a; }
+
+struct Const {
+    float shear, alpha, theta, gama, beta, r, dDyna, w, z, tcut, fcut;
+    double bulk;
+    int ltype, ivec;
+};
+
+// one failure-surface iteration (feit :923-960)
+__device__ __forceinline__ void fail_iter(const Const &C, double &capa, double sig[6], float s[6], float &x1,
+                                          float &x2d) {
+    float xk = (float)(capa + C.r * (C.alpha - C.gama * exp(-C.beta * capa) + C.theta * capa));
+    float dhdk = (float)((C.w * C.dDyna * fexp(-C.dDyna * xk)) *
+                         (1.0 + C.r * (C.theta + C.gama * C.beta * exp(-C.beta * capa))));
+    float omega = C.theta + C.gama * C.beta * fexp(-C.beta * x1);
+    float dcd = (float)(C.shear + 9.0 * C.bulk * (double)(omega * omega));
+    float f = x2d - (C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1);
+    float delcap = -(3.0f * omega * f / (dcd * dhdk));
+    float delam = -(dhdk * delcap / (3.0f * omega));
+    capa = capa + delcap;
+    float fac1 = C.shear / x2d;
+    float fac2 = (float)(3.0 * C.bulk * omega);
+    sig[0] = sig[0] - delam * (fac1 * s[0] - fac2);
+    sig[1] = sig[1] - delam * (fac1 * s[1] - fac2);
+    sig[2] = sig[2] - delam * (fac1 * s[2] - fac2);
+    sig[3] = sig[3] - delam * fac1 * s[3];
+    sig[4] = sig[4] - delam * fac1 * s[4];
+    sig[5] = sig[5] - delam * fac1 * s[5];
+    x1 = (float)(sig[0] + sig[1] + sig[2]);
+    s[0] = (float)(sig[0] - x1 / 3.0f);
+    s[1] = (float)(sig[1] - x1 / 3.0f);
+    s[2] = (float)(sig[2] - x1 / 3.0f);
+    s[3] = (float)sig[3];
+    s[4] = (float)sig[4];
+    s[5] = (float)sig[5];
+    x2d = sqrtf(0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+}
+
+// one cap iteration (fcit :986-1022); returns the convergence function of :1023
+__device__ __forceinline__ float cap_iter(const Const &C, double &capa, double sig[6], float s[6], float &x1, float &x2d,
+                                          float &elcap_out) {
+    const float unit = 1.0f;
+    float xk = (float)(capa + C.r * (C.alpha - C.gama * exp(-C.beta * capa) + C.theta * capa));
+    float dhdk = (float)((C.w * C.dDyna * fexp(-C.dDyna * xk)) *
+                         (1.0 + C.r * (C.theta + C.gama * C.beta * exp(-C.beta * capa))));
+    float dfdk;
+    if (capa >= 0.0) {
+        dfdk = (float)(-(2.0f * (fabs((double)x1 - capa) / (double)(C.r * C.r) +
+                                 (C.alpha - C.gama * exp(-C.beta * capa) + C.theta * capa) *
+                                     (C.theta + C.gama * C.beta * exp(-C.beta * capa)))));
+    } else {
+        dfdk = (float)(-(((2.0f * xk) * (1.0 + C.r * (C.theta + C.gama * C.beta * exp(-C.beta * capa)))) /
+                         (double)(C.r * C.r)));
+    }
+    float elcap = (float)vmax(capa, (double)(0.0f * unit));
+    float omega = vmin(-(2.0f * fabsf(x1 - elcap) / (C.r * C.r)), -1.e-15f * unit);
+    float dcd = (float)((4.0f * C.shear * (x2d * x2d)) +
+                        9.0 * C.bulk * (double)((2.0f * (x1 - elcap) / (C.r * C.r)) * (2.0f * (x1 - elcap) / (C.r * C.r))));
+    float f = x2d * x2d + (x1 - elcap) * (x1 - elcap) / (C.r * C.r) - (xk - elcap) * (xk - elcap) / (C.r * C.r);
+    float delcap = -(f / (dfdk + (dcd * dhdk) / (3.0f * omega)));
+    float delam = -(dhdk * delcap / (3.0f * omega));
+    capa = capa + delcap;
+    xk = (float)(capa + C.r * (C.alpha - C.gama * exp(-C.beta * capa) + C.theta * capa));
+    float fac1 = 2.0f * C.shear;
+    float fac2 = (float)(6.0 * C.bulk * (double)fabsf(x1 - elcap) / (double)(C.r * C.r));
+    sig[0] = sig[0] - delam * (fac1 * s[0] + fac2);
+    sig[1] = sig[1] - delam * (fac1 * s[1] + fac2);
+    sig[2] = sig[2] - delam * (fac1 * s[2] + fac2);
+    sig[3] = sig[3] - delam * fac1 * s[3];
+    sig[4] = sig[4] - delam * fac1 * s[4];
+    sig[5] = sig[5] - delam * fac1 * s[5];
+    x1 = (float)(sig[0] + sig[1] + sig[2]);
+    s[0] = (float)(sig[0] - x1 / 3.0f);
+    s[1] = (float)(sig[1] - x1 / 3.0f);
+    s[2] = (float)(sig[2] - x1 / 3.0f);
+    s[3] = (float)sig[3];
+    s[4] = (float)sig[4];
+    s[5] = (float)sig[5];
+    x2d = sqrtf(0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+    elcap_out = elcap;
+    return x2d * x2d + (x1 - elcap) * (x1 - elcap) / (C.r * C.r) - (xk - elcap) * (xk - elcap) / (C.r * C.r);
+}
+
+}  // namespace cap
+
+// sigma (state convention) <-> the reference's compression-positive
+// sig1..sig6 = -(11 22 33 12 13 23); returns 0 or MCM_ECAP_NOCONV
+template <typename Mat>
+__device__ __noinline__ int f3dm25(PState<double> &P, const Mat &M, double dt) {
+    using namespace cap;
+    const float unit = 1.0f, third = 1.0f / 3.0f, geop = 0.0f, tol = 1.0e-7f;
+    Const C;
+    C.bulk = cm5(M, 1, 1);
+    C.shear = (float)cm5(M, 1, 2);
+    C.alpha = (float)cm5(M, 1, 3);
+    C.theta = (float)cm5(M, 1, 4);
+    C.gama = (float)cm5(M, 1, 5);
+    C.beta = (float)cm5(M, 1, 6);
+    C.r = (float)cm5(M, 2, 1);
+    C.dDyna = (float)cm5(M, 2, 2);
+    C.w = (float)cm5(M, 2, 3);
+    const float falfac = (float)cm5(M, 4, 1);
+    C.alpha = C.alpha - falfac;
+    C.z = (float)cm5(M, 2, 4);
+    C.ivec = (cm5(M, 3, 5) != 0.0) ? 0 : 1;
+    C.ltype = (int)cm5(M, 2, 6);
+    C.tcut = (float)cm5(M, 3, 1);
+    C.fcut = (float)cm5(M, 3, 4);
+    const float t = vmax(C.fcut, C.tcut + 3.0f * geop);
+    const float fet = C.alpha - C.gama * fexp(-C.beta * t) + C.theta * t;
+    const float fept = C.gama * C.beta * fexp(-C.beta * t) + C.theta;
+    P.capa = vmax(P.capa, (double)cm5(M, 3, 3));
+    double sig[6] = {-P.sig[T11], -P.sig[T22], -P.sig[T33], -P.sig[T12], -P.sig[T13], -P.sig[T23]};
+    const double dd1 = -P.rod[T11], dd2 = -P.rod[T22], dd3 = -P.rod[T33];
+    const double dd4 = -P.rod[T12] / 2.0, dd5 = -P.rod[T13] / 2.0, dd6 = -P.rod[T23] / 2.0;
+    const double dd = (dd1 + dd2 + dd3);
+    const double davgm = (double)(1.0f / 3.0f) * dd;
+    const float dt1 = (float)dt;
+    double p = 3.0 * C.bulk * (double)dt1 * davgm;
+    const double gdt = dt * (double)C.shear;
+    const double gd2 = 2.0 * gdt;
+    const float gtr11 = (float)(sig[0] + p + gd2 * (dd1 - davgm));
+    const float gtr22 = (float)(sig[1] + p + gd2 * (dd2 - davgm));
+    const float gtr33 = (float)(sig[2] + p + gd2 * (dd3 - davgm));
+    const float gtr12 = (float)(sig[3] + gd2 * dd4);
+    const float gtr23 = (float)(sig[4] + gd2 * dd5);
+    const float gtr31 = (float)(sig[5] + gd2 * dd6);
+    const float x1tr = gtr11 + gtr22 + gtr33;
+    float s[6];
+    s[0] = gtr11 - (1.0f / 3.0f) * x1tr;
+    s[1] = gtr22 - (1.0f / 3.0f) * x1tr;
+    s[2] = gtr33 - (1.0f / 3.0f) * x1tr;
+    float x2dtr = 0.5f * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + 2.0f * (gtr12 * gtr12 + gtr23 * gtr23 + gtr31 * gtr31));
+    x2dtr = sqrtf(x2dtr);
+    const float capa_local = 0.0f;
+    float fe = C.alpha - C.gama * fexp(-C.beta * capa_local) + C.theta * capa_local;
+    const float xkn = capa_local + C.r * fe;
+    const float elcapn = (float)vmax(P.capa, (double)(0.0f * unit));
+    const float tmises = fabsf(xkn - elcapn) / C.r;
+    fe = C.alpha - C.gama * fexp(-C.beta * x1tr) + C.theta * x1tr;
+    const float f1tr = x2dtr - vmin(fe, tmises);
+    const float tcrit = (float)((double)t - 9.0 * C.bulk / (double)C.shear * (double)(x2dtr - fet) * (double)fept);
+    fe = C.alpha - C.gama * fexp(-C.beta * elcapn) + C.theta * elcapn;
+    const float fep = C.beta * C.gama * fexp(-C.beta * elcapn) + C.theta;
+    const float fc2tr = ((xkn - elcapn) * (xkn - elcapn) - (x1tr - elcapn) * (x1tr - elcapn)) / (C.r * C.r);
+    const float f2tr = x2dtr * x2dtr - fc2tr;
+    const float x1crt = (float)((double)elcapn - ((double)((x2dtr - fe) * 9.0f) * C.bulk) * (double)fep / (double)C.shear);
+    fe = (float)(C.alpha - C.gama * exp(-C.beta * P.capa) + C.theta * P.capa);
+    const float capal = (float)vmin((double)(0.0f * unit), P.capa - (double)(tol * fe));
+    fe = C.alpha - C.gama * fexp(-C.beta * capal) + C.theta * capal;
+    const float xk0 = capal + C.r * fe;
+    const float evpn = C.w * (1.0f - fexp(C.dDyna * (C.z - xkn)));
+    const float devpb = C.w * (1.0f - fexp(C.dDyna * (C.z - xk0))) - evpn;
+    const double capan = P.capa;
+    const int ltype = C.ltype;
+    int imode = 0;
+    if ((x1tr <= t) && (x2dtr <= fet) && (ltype == 1) && (capan > 0.0) && (devpb >= 0.0f)) imode = 2;
+    else if ((x1tr <= t) && (x2dtr <= fet) && (ltype == 1) && (capan > 0.0) && (devpb < 0.0f)) imode = 7;
+    else if ((x1tr <= t) && (x2dtr <= fet) && ((ltype == 2) || (capan <= 0.0))) imode = 3;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && (ltype == 1) && (capan > 0.0) && (devpb >= 0.0f)) imode = 4;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && (ltype == 1) && (capan > 0.0) && (devpb < 0.0f)) imode = 6;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr <= tcrit) && ((ltype == 2) || (capan <= 0.0))) imode = 5;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr > tcrit) && (capan >= 0.0)) imode = 10;
+    else if ((x1tr <= t) && (x2dtr > fet) && (x1tr > tcrit) && (capan < 0.0)) imode = 8;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr <= tol)) imode = 1;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr >= x1crt)) imode = 9;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr < x1crt) && (capan >= 0.0)) imode = 10;
+    else if ((x1tr > t) && (x1tr <= elcapn) && (f1tr > tol) && (x1tr < x1crt) && (capan < 0.0)) imode = 8;
+    else if ((x1tr > t) && (x1tr > elcapn) && (f2tr < tol)) imode = 1;
+    else if ((x1tr > t) && (x1tr > elcapn) && (f2tr >= tol)) imode = 11;
+    P.ptype = imode;
+    float x1 = 0.0f, x2d = 0.0f, ratio = 0.0f;
+    const float sdtr[3] = {s[0], s[1], s[2]};
+    auto set_scaled = [&](float rat) {
+        sig[0] = (double)(sdtr[0] * rat) + p;
+        sig[1] = (double)(sdtr[1] * rat) + p;
+        sig[2] = (double)(sdtr[2] * rat) + p;
+        sig[3] = (double)(gtr12 * rat);
+        sig[4] = (double)(gtr23 * rat);
+        sig[5] = (double)(gtr31 * rat);
+    };
+    auto set_plain = [&]() {
+        sig[0] = (double)s[0] + p;
+        sig[1] = (double)s[1] + p;
+        sig[2] = (double)s[2] + p;
+        sig[3] = (double)gtr12;
+        sig[4] = (double)gtr23;
+        sig[5] = (double)gtr31;
+    };
+    auto move_cap = [&]() {
+        const float x1old = (float)(sig[0] + sig[1] + sig[2]);
+        const float devp = (float)(dd - (double)(x1 - x1old) / (3.0 * C.bulk));
+        const float xhat = vmin(devpb, devp);
+        P.capa = P.capa + (double)devp * ((double)capal - capan) / (double)xhat;
+        P.capa = vmax(P.capa, (double)(0.0f * unit));
+    };
+    int code = 0;
+    switch (imode) {
+        case 1: x1 = x1tr; x2d = x2dtr; P.capa = capan; p = (double)(third * x1 + geop); set_plain(); break;
+        case 2: x1 = t; x2d = x2dtr; P.capa = 0.0; p = (double)(third * x1 + geop); set_plain(); break;
+        case 3: x1 = t; x2d = x2dtr; P.capa = capan; p = (double)(third * x1 + geop); set_plain(); break;
+        case 4:
+            x1 = t; x2d = fet; P.capa = 0.0; p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr; set_scaled(ratio);
+            break;
+        case 5:
+            x1 = t; x2d = fet; P.capa = capan; p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr; set_scaled(ratio);
+            break;
+        case 6:
+            x1 = t; x2d = fet; move_cap(); p = (double)(third * x1 + geop);
+            ratio = x2d / x2dtr; set_scaled(ratio);
+            break;
+        case 7:
+            x1 = t; x2d = x2dtr; move_cap(); p = (double)(third * x1 + geop); set_plain();
+            break;
+        case 8:
+            x1 = x1tr;
+            fe = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            x2d = vmin(fe, tmises);
+            P.capa = capan;
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            set_scaled(ratio);
+            break;
+        case 9:
+            x1 = elcapn;
+            x2d = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            P.capa = capan;
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            set_scaled(ratio);
+            break;
+        case 10: {
+            double sg[6] = {gtr11, gtr22, gtr33, gtr12, gtr23, gtr31};
+            P.capa = capan;
+            x1 = x1tr;
+            x2d = x2dtr;
+            float si[6];
+            for (int k = 0; k < 3; ++k) si[k] = (float)(sg[k] - x1tr / 3.0f);
+            for (int k = 3; k < 6; ++k) si[k] = (float)sg[k];
+            if (C.ivec == 0) {
+                bool conv = false;
+                for (int it = 1; it <= 100; ++it) {
+                    fail_iter(C, P.capa, sg, si, x1, x2d);
+                    const float f = x2d - (C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1);
+                    if (fabsf(f) <= 1.0e-8f) { conv = true; break; }
+                }
+                if (!conv) code = MCM_ECAP_NOCONV;
+            } else {
+                for (int it = 0; it < 4; ++it) fail_iter(C, P.capa, sg, si, x1, x2d);
+            }
+            if (x1 > elcapn) x1 = elcapn;
+            if ((ltype == 2) || (capan == 0.0)) P.capa = capan;
+            if ((double)x1 > P.capa) P.capa = x1;
+            if ((ltype == 1) && (capan >= 0.0)) P.capa = vmax(P.capa, (double)(0.0f * unit));
+            fe = C.alpha - C.gama * fexp(-C.beta * x1) + C.theta * x1;
+            x2d = vmin(fe, tmises);
+            ratio = x2d / x2dtr;
+            p = (double)(third * x1 + geop);
+            set_scaled(ratio);
+            break;
+        }
+        case 11: {
+            double sg[6] = {gtr11, gtr22, gtr33, gtr12, gtr23, gtr31};
+            P.capa = capan;
+            x1 = x1tr;
+            x2d = x2dtr;
+            float si[6];
+            for (int k = 0; k < 3; ++k) si[k] = (float)(sg[k] - x1tr / 3.0f);
+            for (int k = 3; k < 6; ++k) si[k] = (float)sg[k];
+            float elcap = 0.0f;
+            bool done = false;
+            const int nit = (C.ivec == 0) ? 100 : 4;
+            for (int it = 1; it <= nit; ++it) {
+                const float f = cap_iter(C, P.capa, sg, si, x1, x2d, elcap);
+                if (C.ivec == 0 && fabsf(f) <= 1.0e-8f) { done = true; break; }
+            }
+            if (C.ivec == 0 && !done) code = MCM_ECAP_NOCONV;
+            if (x1 < elcap) {
+                x1 = elcap + fabsf(x1 - elcap);
+                sg[0] = (double)(si[0] + x1 / 3.0f);
+                sg[1] = (double)(si[1] + x1 / 3.0f);
+                sg[2] = (double)(si[2] + x1 / 3.0f);
+            }
+            for (int k = 0; k < 6; ++k) sig[k] = sg[k];
+            break;
+        }
+        default: break;
+    }
+    // write-back (:813-827): the upper triangle only; the lower keeps the rotated stress
+    P.sig[T11] = -sig[0];
+    P.sig[T22] = -sig[1];
+    P.sig[T33] = -sig[2];
+    P.sig[T12] = -sig[3];
+    P.sig[T13] = -sig[4];
+    P.sig[T23] = -sig[5];
+    P.p = -(1.0 / 3.0) * (P.sig[T11] + P.sig[T22] + P.sig[T33]);
+    return code;
+}
+
 // -------------------------------------------------------- critical timestep
 // MCM/mcm_calccritts.f90:40-78 (per particle)
 template <typename T, typename Mat>
@@ -674,28 +1009,38 @@ __device__ __forceinline__ T critts_particle(const PState<T> &P, const Mat &M, i
 
 // ------------------------------------------------- constitutive driver
 // MCM/mcm_constitutive.f90:29-83 for one particle, after mcm_rhoupd.
-// Returns false if the EOS reported a complex sound speed.
+// Returns 0, MCM_ECOMPLEX_C (the EOS reported a complex sound speed) or
+// MCM_ECAP_NOCONV (the cap model's iterated return did not converge).
 template <typename T, typename Mat>
-__device__ __forceinline__ bool constitutive_particle(PState<T> &P, const Mat &M, T dt) {
-    bool ok = true;
+__device__ __forceinline__ int constitutive_particle(PState<T> &P, const Mat &M, T dt) {
+    int code = 0;
     switch (M.model) {
         case 1:
-            stress_rot1(P, dt); f3dm1(P, M, dt); aviscosity(P, M); lieupd(P, dt);
+            stress_rot1(P, dt); f3dm1(P, M, dt); sym_lower(P); aviscosity(P, M); lieupd(P, dt);
             break;
         case 3:
-            stress_rot1(P, dt); f3dm3(P, M, dt); aviscosity(P, M); lieupd(P, dt);
+            stress_rot1(P, dt); f3dm3(P, M, dt); sym_lower(P); aviscosity(P, M); lieupd(P, dt);
+            break;
+        case 4:
+            if constexpr (std::is_same<T, double>::value) {
+                stress_rot1(P, dt); code = f3dm25(P, M, dt); aviscosity(P, M); lieupd(P, dt);
+            }
             break;
         case 9:
-            stress_rot1(P, dt); f3dm9(P, M); ok = sueos(P, M); aviscosity(P, M); hieupd(P, dt); eqos(P, M, dt);
-            stress_up(P);
+            stress_rot1(P, dt); f3dm9(P, M);
+            if (!sueos(P, M)) code = MCM_ECOMPLEX_C;
+            aviscosity(P, M); hieupd(P, dt); eqos(P, M, dt);
+            stress_up(P); sym_lower(P);
             break;
         case 10:
-            stress_rot1(P, dt); f3dm10(P, M, dt); ok = sueos(P, M); aviscosity(P, M); hieupd(P, dt); eqos(P, M, dt);
-            stress_up(P);
+            stress_rot1(P, dt); f3dm10(P, M, dt);
+            if (!sueos(P, M)) code = MCM_ECOMPLEX_C;
+            aviscosity(P, M); hieupd(P, dt); eqos(P, M, dt);
+            stress_up(P); sym_lower(P);
             break;
         default: break;
     }
-    return ok;
+    return code;
 }
 
 }  // namespace mcm

@@ -124,10 +124,13 @@ __device__ __forceinline__ void load_state(const StepArgs &a, int i, PState<doub
     P.mass = f[FMASS][i]; P.h = f[FH][i]; P.hold = f[FHOLD][i];
     P.rho = f[FRHO][i]; P.e = f[FE][i]; P.p = f[FP][i]; P.c = f[FC][i];
     P.efps = f[FEFPS][i]; P.pcut = f[FPCUT][i]; P.p_cut = f[FPCUT2][i]; P.fail = f[FFAIL][i];
-    P.capa = 0.0;
+    P.capa = (model == 4) ? f[FCAPA][i] : 0.0;
+    P.ptype = 0;
     P.rho0 = a.mats[P.mat - 1].rho;
 #pragma unroll
     for (int t = 0; t < 6; ++t) { P.sig[t] = f[FS11 + t][i]; P.s[t] = 0.0; P.alfa[t] = 0.0; }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) P.sigl[t] = f[FL21 + t][i];
     if (model == 9) {
 #pragma unroll
         for (int t = 0; t < 6; ++t) P.s[t] = f[FD11 + t][i];
@@ -147,7 +150,13 @@ __device__ __forceinline__ void store_state(const StepArgs &a, int i, const PSta
     f[FEFPS][i] = P.efps; f[FPCUT][i] = P.pcut; f[FPCUT2][i] = P.p_cut; f[FFAIL][i] = P.fail;
 #pragma unroll
     for (int t = 0; t < 6; ++t) f[FS11 + t][i] = P.sig[t];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) f[FL21 + t][i] = P.sigl[t];
     f[FQ][i] = P.q;
+    if (model == 4) {
+        f[FCAPA][i] = P.capa;
+        a.F.ptype[i] = P.ptype;
+    }
     if (a.prm.diag || model == 9) {
 #pragma unroll
         for (int t = 0; t < 6; ++t) f[FD11 + t][i] = P.s[t];
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double dt = a.time->dt;
     double crit = 1.0e20;
-    bool bad = false;
+    int bad = 0;
     if (i < a.n) {
         double *const *f = a.F.f;
         const DevMaterial &M = a.mats[a.F.mat[i] - 1];
@@ -339,7 +348,7 @@ __global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
         P.spin[2] = f[FW23][i];
         P.tracerod = f[FTR][i];
         rhoupd(P, M, dt, 3);
-        bad = !constitutive_particle(P, M, dt);
+        bad = constitutive_particle(P, M, dt);
         const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
         const double mindist = (a.prm.tcrit_opt == 2) ? f[FMINDIST][i] : 0.0;
         crit = critts_particle(P, M, a.prm.tcrit_opt, 3, f[FVABS][i], mindist);
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
         f[FY][i] = ys + 0.5 * vy * dt;
         f[FZ][i] = zs + 0.5 * vz * dt;
     }
-    if (bad) raise_status(a.status, MCM_ECOMPLEX_C, i);
+    if (bad) raise_status(a.status, bad, i);
     double m = block_min(crit, sm);
     if (threadIdx.x == 0) a.red[blockIdx.x] = m;
 }
@@ -373,6 +382,8 @@ __global__ void k_mom_prep(StepArgs a) {
         a.rec1[p] = make_double4((f[FS11][i] - q) / r2, (f[FS22][i] - q) / r2, (f[FS33][i] - q) / r2,
                                  (f[FS12][i] - 0.0) / r2);
         a.rec2[p] = make_double4((f[FS13][i] - 0.0) / r2, (f[FS23][i] - 0.0) / r2, f[FMASS][i], rho);
+        if (a.prm.asym)
+            a.rec3[p] = make_double4((f[FL21][i] - 0.0) / r2, (f[FL31][i] - 0.0) / r2, (f[FL32][i] - 0.0) / r2, 0.0);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -385,6 +396,9 @@ __global__ void k_mom_prep(StepArgs a) {
             a.grec1[g] = make_double4((f[FS11][j] - q) / r2, (f[FS22][j] - q) / r2, (f[FS33][j] - q) / r2,
                                       ((-f[FS12][j]) - (-0.0)) / r2);
             a.grec2[g] = make_double4(((-f[FS13][j]) - (-0.0)) / r2, ((-f[FS23][j]) - (-0.0)) / r2, a.gmass[g], rho);
+            if (a.prm.asym)
+                a.grec3[g] = make_double4(((-f[FL21][j]) - (-0.0)) / r2, ((-f[FL31][j]) - (-0.0)) / r2,
+                                          ((-f[FL32][j]) - (-0.0)) / r2, 0.0);
         }
     }
 }
@@ -396,19 +410,30 @@ __device__ __forceinline__ void sym_from_rec(const double4 &r1, const double4 &r
     A[1][2] = A[2][1] = r2.y;
 }
 
+// The lower triangle from the asymmetric record (cap model, prm.asym).
+__device__ __forceinline__ void lower_from_rec(const double4 &r3, double A[3][3]) {
+    A[1][0] = r3.x;
+    A[2][0] = r3.y;
+    A[2][1] = r3.z;
+}
+
 template <int DISC>
 __device__ __forceinline__ void momentum_gather(const StepArgs &a, const DevGrid &g, int t, double acc[3]) {
     const double4 xi = a.rec0[t];
     double Ai[3][3];
     sym_from_rec(a.rec1[t], a.rec2[t], Ai);
+    const bool asym = a.prm.asym != 0;
+    if (asym) lower_from_rec(a.rec3[t], Ai);
     if (DISC == 0) {
-        // MCM/mcm_oldacceleration.f90:66-89
-        auto body = [&](const double4 xj, const double4 r1, const double4 r2) {
+        // MCM/mcm_oldacceleration.f90:66-89; sigma(m,n) is read as stored,
+        // both triangles (they differ for the cap model)
+        auto body = [&](const double4 xj, const double4 r1, const double4 r2, const double4 *r3) {
             double havg = 0.5 * (xi.w + xj.w);
             double d[3];
             gradw(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, havg, d[0], d[1], d[2]);
             double Aj[3][3];
             sym_from_rec(r1, r2, Aj);
+            if (r3) lower_from_rec(*r3, Aj);
             const double massj = r2.z;
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
@@ -419,8 +444,8 @@ __device__ __forceinline__ void momentum_gather(const StepArgs &a, const DevGrid
             }
         };
         for_each_neighbour(
-            a, g, t, [&](int p, bool) { body(a.rec0[p], a.rec1[p], a.rec2[p]); },
-            [&](int q) { body(a.grec0[q], a.grec1[q], a.grec2[q]); });
+            a, g, t, [&](int p, bool) { body(a.rec0[p], a.rec1[p], a.rec2[p], asym ? &a.rec3[p] : nullptr); },
+            [&](int q) { body(a.grec0[q], a.grec1[q], a.grec2[q], asym ? &a.grec3[q] : nullptr); });
     } else {
         // MCM/mcm_corr_acceleration.f90:63-161 (kernel centred at j; the self
         // slot k = nnbr is zeroed; the final sum uses the last neighbour's mass)
@@ -711,6 +736,11 @@ __global__ void k_initial(StepArgs a, int massopt, int init_h_opt, int init_rhoe
                 P.p = 0.0;
                 P.c = sqrt(M.strinput[1] / P.rho);
                 break;
+            case 4:   // MCM/mcm_calcrhopc.f90:57-67: strinput(10) = cm(5,2), set by mcm_sets4
+                if (init_rhoe != 1) { P.rho = P.rho0; P.e = 0.0; }
+                P.p = 0.0;
+                P.c = sqrt(M.strinput[9] / P.rho);
+                break;
             case 9: case 10: {
                 const double *ei = M.eosinput;
                 switch (M.eos) {
@@ -744,6 +774,7 @@ __global__ void k_initial(StepArgs a, int massopt, int init_h_opt, int init_rhoe
         // MCM/mcm_initsigma.f90:26-49
         f[FS11][i] = -P.p; f[FS22][i] = -P.p; f[FS33][i] = -P.p;
         f[FS12][i] = 0.0; f[FS13][i] = 0.0; f[FS23][i] = 0.0;
+        f[FL21][i] = 0.0; f[FL31][i] = 0.0; f[FL32][i] = 0.0;
         for (int t = 0; t < 6; ++t) { f[FD11 + t][i] = 0.0; f[FA11 + t][i] = 0.0; f[FR11 + t][i] = 0.0; }
         f[FW12][i] = f[FW13][i] = f[FW23][i] = 0.0;
         // MCM/mcm_init_h.f90:22-48

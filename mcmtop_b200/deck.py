@@ -92,6 +92,19 @@ PRESS = 1.0e-11       # Pa -> Mbar
 ACC = 1.0e-10         # m/s^2 -> cm/us^2
 
 
+@dataclass(frozen=True)
+class Units:
+    """SI -> deck unit factors for length, velocity, density and pressure."""
+    length: float
+    velocity: float
+    density: float
+    pressure: float
+
+
+CGUS = Units(CM, VEL, RHO, PRESS)          # cm, g, us: pressure in Mbar (the metal decks)
+MMMSG = Units(1.0e3, 1.0, 1.0e-6, 1.0e-6)  # mm, ms, g: pressure in MPa, velocity in m/s (the soil deck)
+
+
 def copper_model10(h: float, yield_stress: float = 400e6, hardening: float = 100e6, shear: float = 46e9,
                    gruneisen_s: float = 1.49, rho0: float = 8930.0) -> MaterialCard:
     """Copper-like elastic-plastic hydrodynamic material (model 10) with the
@@ -114,25 +127,26 @@ def copper_model10(h: float, yield_stress: float = 400e6, hardening: float = 100
 def taylor_bar(dx: float = 0.4e-3, radius: float = 3.2e-3, length: float = 32.4e-3, velocity: float = 190.0,
                seed: int = 1234, jitter: float = 0.01, disctype: int = 0, tssf: float = 0.3,
                endtime: float = 1.0e9, material: MaterialCard | None = None, z0: float = 0.0,
-               tcrit_opt: int = 1) -> Deck:
+               tcrit_opt: int = 1, units: Units = CGUS) -> Deck:
     """Taylor impact bar: a cylinder (axis z) of lattice particles at
     (i+1/2, j+1/2, k+1/2) dx inside r <= R, 0 < z <= L, each displaced by a
     seeded uniform jitter of +/- jitter*dx per coordinate, moving at -velocity
     along z onto a rigid wall imposed by a z-min symmetry plane at z = 0.
     Particle order: z layers, then y rows, then x.  Arguments in SI units; the
-    deck is in cm-g-us."""
+    deck is in `units` (cm-g-us by default; a given material must be in the
+    same units)."""
     q = radius / dx
     n = int(np.ceil(q)) + 1
     ii = np.arange(-n, n)
     I, J = np.meshgrid(ii, ii, indexing="xy")
     inside = (2 * I + 1) ** 2 + (2 * J + 1) ** 2 <= (2.0 * q) ** 2 * (1 + 1e-12)
-    dxc = dx * CM
+    dxc = dx * units.length
     xs = (I[inside] + 0.5) * dxc
     ys = (J[inside] + 0.5) * dxc
     order = np.lexsort((xs, ys))
     xs, ys = xs[order], ys[order]
     nz = int(round(length / dx))
-    zs = z0 * CM + (np.arange(nz) + 0.5) * dxc
+    zs = z0 * units.length + (np.arange(nz) + 0.5) * dxc
     x = np.empty((nz * xs.size, 3))
     x[:, 0] = np.tile(xs, nz)
     x[:, 1] = np.tile(ys, nz)
@@ -141,7 +155,7 @@ def taylor_bar(dx: float = 0.4e-3, radius: float = 3.2e-3, length: float = 32.4e
     x += _jitter(rng, x.shape, jitter * dxc)
     npart = x.shape[0]
     v = np.zeros_like(x)
-    v[:, 2] = -velocity * VEL
+    v[:, 2] = -velocity * units.velocity
     h = 1.3 * dxc
     mat = material if material is not None else copper_model10(h)
     mat = dataclasses.replace(mat, strinput=mat.strinput.copy(), eosinput=mat.eosinput.copy(), h=h)
@@ -150,6 +164,41 @@ def taylor_bar(dx: float = 0.4e-3, radius: float = 3.2e-3, length: float = 32.4e
                 sym_flag=(0, 0, 0, 0, 1, 0), sym_x=(0.0,) * 6, materials=[mat], x=x, v=v,
                 mat=np.ones(npart, dtype=np.int32), dispbc=np.zeros(npart, dtype=np.int32),
                 name=f"taylor_bar_dx{dx * 1e3:g}mm_n{npart}")
+
+
+def sand_model4(h: float, bulk: float = 1.0e9, shear: float = 0.6e9, alpha: float = 10e6, theta: float = 0.1,
+                gamma: float = 8e6, beta: float = 0.1e-6, r: float = 2.5, d: float = 0.002e-6, w: float = 0.05,
+                x0: float = 30e6, tcut: float = -1e6, rho0: float = 1800.0, iterate: bool = False,
+                units: Units = MMMSG) -> MaterialCard:
+    """Granular material for the cap model (model 4, MCM/mcm_f3dm25.f90):
+    failure surface Fe(J1) = alpha - gamma exp(-beta J1) + theta J1, cap
+    ratio R, hardening law W (1 - exp(-D (X - X0))), tension cut-off, soil
+    (ltype 1).  SI arguments (Pa, 1/Pa); card values in `units`, by default
+    mm-ms-g (MPa): the model's absolute tolerances (1e-3 in the initial-cap
+    iteration of MCM/mcm_sets4.f90:61, 1e-7 and 1e-8 in MCM/mcm_f3dm25.f90)
+    assume stresses of order 1-100, as in MPa or psi decks.  The cards
+    fill the 5-row table cm(i, j) = strinput(i + 5(j-1)) as MCM/mcm_matin.f90
+    reads 6 cards of 5 values: K, R, tcut, falfac | G, D | alpha, W | theta,
+    X0 (hardening) | gamma, X0 (initial cap, MCM/mcm_sets4.f90:28), vector
+    flag | beta, ltype.  iterate = True selects the iterated return
+    (feit/fcit, cm(3,5) /= 0) instead of four fixed iterations."""
+    m = MaterialCard(model=4, eos=0, rho=rho0 * units.density, av_l=0.06, av_q=1.5, h=h)
+    cm = lambda i, j: (i - 1) + 5 * (j - 1)   # noqa: E731
+    m.strinput[cm(1, 1)] = bulk * units.pressure
+    m.strinput[cm(2, 1)] = r
+    m.strinput[cm(3, 1)] = tcut * units.pressure
+    m.strinput[cm(1, 2)] = shear * units.pressure
+    m.strinput[cm(2, 2)] = d / units.pressure
+    m.strinput[cm(1, 3)] = alpha * units.pressure
+    m.strinput[cm(2, 3)] = w
+    m.strinput[cm(1, 4)] = theta
+    m.strinput[cm(2, 4)] = x0 * units.pressure
+    m.strinput[cm(1, 5)] = gamma * units.pressure
+    m.strinput[cm(2, 5)] = x0 * units.pressure
+    m.strinput[cm(3, 5)] = 1.0 if iterate else 0.0
+    m.strinput[cm(1, 6)] = beta / units.pressure
+    m.strinput[cm(2, 6)] = 1.0
+    return m
 
 
 def water_model9(h: float, c0: float = 40.0, rho0: float = 1000.0, pcut: float = -1.0e4) -> MaterialCard:

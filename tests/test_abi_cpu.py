@@ -110,7 +110,9 @@ def test_material_rejects_eos_on_solid(lib):
     assert st == _abi.MCM_EINVAL
 
 
-def test_cap_model_is_reported_unsupported(lib):
+def test_cap_model_card_without_soil_type_is_rejected(lib):
+    """Model 4 is set up by the library (mcm_sets4); a card whose ltype is
+    neither soil (1) nor rock (2) has no mode in the cap model's table."""
     card = MaterialCard(model=4, eos=0, rho=2.0)
     st, _ = _lib_material(lib, card)
-    assert st == _abi.MCM_EUNSUPPORTED
+    assert st == _abi.MCM_EINVAL
