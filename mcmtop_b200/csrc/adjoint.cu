@@ -219,7 +219,7 @@ __global__ void k_adj_pack_strain(StepArgs a, AdjArgs b) {
 // ----------------------------------------------------------- momentum
 // kLanes lanes share a particle: lane l takes neighbours l, l + kLanes, ...;
 // the per-particle sums are combined by shuffles and one lane writes them.
-constexpr int kLanes = 16;
+constexpr int kLanes = 4;
 
 template <int N>
 __device__ __forceinline__ void lane_sum(double (&v)[N]) {

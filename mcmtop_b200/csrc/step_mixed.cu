@@ -16,18 +16,22 @@
 // size is formed from small numbers and keeps FP32 relative accuracy at the
 // scale of h.  Ghost neighbours (few, near the planes) use FP64 positions.
 //
-// Compensated sums: 16 lanes share one particle's neighbours, so a lane
-// adds at most ceil(K/16) terms (about 5) in plain FP32; the 16 partial sums
-// are then combined with an error-free TwoSum shuffle tree that carries the
-// rounding error of every addition, and the result is rounded once to FP64.
-// Per-lane Kahan sums would cost four operations per term for no gain on
-// five-term sums.
+// Compensated sums: 4 lanes share one particle's neighbours, so a lane adds
+// about K/4 terms (20) in plain FP32; the 4 partial sums are then combined
+// with an error-free TwoSum shuffle tree that carries the rounding error of
+// every addition, and the result is rounded once to FP64.  Measured on the
+// 2M bar after 205 steps against the FP64 step: worst field 1.25e-5 of its
+// range with plain lane sums, 1.05e-5 with per-lane Kahan sums; the error is
+// that of the FP32 pair terms, not of their sum, and the Kahan registers cost
+// 9 % of the step.  Four lanes (about 20 neighbours in flight per lane) hide
+// the record-gather latency better than 8 or 16: 0.92/1.19 ms for strain/
+// momentum against 0.96/1.33 (8 lanes) and 1.33/1.70 ms (16).
 #include "nbr_iter.cuh"
 
 namespace mcm {
 namespace mixed {
 
-constexpr int L = 16;          // lanes per particle
+constexpr int L = 4;           // lanes per particle
 constexpr float kPiF = 3.14159265358979f;
 
 __device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
@@ -339,9 +343,9 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // MCM/mcm_oldacceleration.f90:66-89 with FP32 pair sums, then the FP64 tail:
 // base acceleration and displacement BCs (MCM/mcm_boundcond.f90), energy
 // partials (MCM/mcm_calctotale.f90) and, when integrating, the update.
-// Four resident blocks (64 registers, a 64-byte spill) hide the record
-// gathers' latency better than three at 80 registers: 1.70 against 2.19 ms
-// per step on the 2M bar.
+// Four resident blocks (64 registers) hide the record gathers' latency
+// better than three at 80 registers (measured with 16 lanes per particle:
+// 1.70 against 2.19 ms per step on the 2M bar).
 __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
