@@ -63,7 +63,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=30.0, help="seconds of timed oracle work")
     ap.add_argument("--oracle-steps", type=int, default=20,
-                    help="oracle steps on the full bar (CPU baseline sample and GPU spot check)")
+                    help="timed oracle steps on the full bar (the CPU baseline sample)")
+    ap.add_argument("--oracle-check-steps", type=int, default=50,
+                    help="oracle steps on the full bar for the GPU accuracy spot check")
     ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
     return ap.parse_args()
 
@@ -186,6 +188,16 @@ def cpu_oracle(deck, budget_s: float, max_steps: int):
     el = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return deck.np * steps / el, steps, el, cores, orc
+
+
+def advance_oracle(orc, done: int, target: int, budget_s: float) -> int:
+    """Runs the oracle on from step `done` towards `target` steps (untimed,
+    bounded by budget_s); returns the steps it has then run."""
+    t0 = time.perf_counter()
+    while done < target and time.perf_counter() - t0 < budget_s:
+        orc.run(1)
+        done += 1
+    return done
 
 
 ORACLE_FIELDS = ["x", "v", "rho", "e", "p", "c", "efps", "sigma", "q", "vabs"]
@@ -519,7 +531,9 @@ def gpu_arm(args):
                "sample": f"oracle (C++ restatement, OpenMP) on the same {deck.np}-particle bar: {n} steps after "
                          f"initialisation, {el:.1f} s"}
         if accuracy is not None:
-            accuracy["vs_oracle"] = oracle_spot_check(deck, orc, n, local, args.reorder)
+            # the spot check runs the oracle on to --oracle-check-steps (the first 50)
+            m = advance_oracle(orc, n, args.oracle_check_steps, 150.0)
+            accuracy["vs_oracle"] = oracle_spot_check(deck, orc, m, local, args.reorder)
         orc.close()
 
     line = {

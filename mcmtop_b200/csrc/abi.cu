@@ -1464,13 +1464,15 @@ int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, in
     h->adj_steps = nsteps;
     h->adj_every = checkpoint_every;
     const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
-    for (double *p : h->adj_ckpt)
-        if (p) cudaFree(p);
-    h->adj_ckpt.assign(nck, nullptr);
+    // checkpoints are kept between calls (a snapshot's size is fixed per
+    // handle): only missing ones are allocated, surplus ones freed
     const size_t sd = snap_doubles(h);
+    for (size_t c = nck; c < h->adj_ckpt.size(); ++c)
+        if (h->adj_ckpt[c]) cudaFree(h->adj_ckpt[c]);
+    h->adj_ckpt.resize(nck, nullptr);
     for (int c = 0; c < nck; ++c)
-        if ((st = dalloc(h, &h->adj_ckpt[c], sd))) return st;
-    if ((st = dalloc(h, &h->adj_final, sd))) return st;
+        if (!h->adj_ckpt[c] && (st = dalloc(h, &h->adj_ckpt[c], sd))) return st;
+    if (!h->adj_final && (st = dalloc(h, &h->adj_final, sd))) return st;
     for (int c = 0; c < nck; ++c) {
         const int n0 = c * checkpoint_every;
         if ((st = snap_save(h, h->adj_ckpt[c]))) return st;
@@ -1491,9 +1493,9 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     DiagOff diag(h);
     const int n = h->np;
     const size_t np = h->npad;
-    if ((st = dalloc(h, &h->d_adj, (size_t)kAdjArrays * np))) return st;
+    if (!h->d_adj && (st = dalloc(h, &h->d_adj, (size_t)kAdjArrays * np))) return st;
     CK(cudaMemsetAsync(h->d_adj, 0, sizeof(double) * kAdjArrays * np, h->stream));
-    if ((st = dalloc(h, &h->d_theta, (size_t)h->nmat * adj::kParams))) return st;
+    if (!h->d_theta && (st = dalloc(h, &h->d_theta, (size_t)h->nmat * adj::kParams))) return st;
     CK(cudaMemsetAsync(h->d_theta, 0, sizeof(double) * h->nmat * adj::kParams, h->stream));
     std::vector<int> orig(n);
     CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));

@@ -187,17 +187,34 @@ def test_fluid_column_five_planes(lib):
     compare_neighbours(sol, orc)
 
 
-def test_taylor_bar_16k_steps(lib):
-    """The 16 848-particle Taylor bar (dx = 0.4 mm), first 30 steps."""
-    deck = taylor_bar(dx=0.4e-3)
+@pytest.mark.parametrize("disctype", [0, 1])
+def test_taylor_bar_16k_steps(lib, disctype):
+    """The 16 848-particle Taylor bar (dx = 0.4 mm), first 30 steps, simple and
+    corrected SPH."""
+    deck = taylor_bar(dx=0.4e-3, disctype=disctype)
     assert deck.np == 16848
     sol = Solver(deck, _abi.PREC_FP64_EXACT)
-    orc = Oracle(deck)
+    orc = Oracle(deck, openmp=True)
     for _ in range(30):
         sol.step()
         orc.step()
     compare(sol, orc, STATE, 1e-10, "16k bar")
     compare_neighbours(sol, orc)
+
+
+def test_taylor_bar_16k_thousand_steps(lib):
+    """The 16 848-particle bar for the 1000 steps of its configuration: the
+    FP64-exact step against the oracle (OpenMP build) at the end, through the
+    fused device loop.  The per-step differences (transcendentals an ulp
+    apart) grow over the run; the bound is 1e-8 of each field's range."""
+    deck = taylor_bar(dx=0.4e-3)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT)
+    orc = Oracle(deck, openmp=True)
+    assert sol.run(1000) == 1000
+    assert orc.run(1000) == 1000
+    errs = compare(sol, orc, STATE, 1e-8, "16k bar, 1000 steps")
+    print("max relative error per field after 1000 steps:", errs)
+    assert abs(sol.ptime - orc.scalar("ptime")) <= 1e-10 * orc.scalar("ptime")
 
 
 def test_neighbour_overflow_regrow(lib):
