@@ -283,6 +283,16 @@ def adjoint_cost(args, local):
     pb, t_ckpt, t_bwd = gradient()
     sol.close()
     spread = float(np.max(np.abs(pb - pb_warm) / np.maximum(np.abs(pb), 1e-300)))
+    # the same gradient along the mixed-precision (FP32 pair sum) forward
+    mixed = Solver(deck, _abi.PREC_MIXED, device=local)
+    mixed.adjoint_forward(dts, args.adj_every)
+    xm = mixed.download(["x"])["x"]
+    xbar_m = np.zeros_like(xm)
+    xbar_m[int(xm[:, 2].argmax()), 2] += 1.0
+    xbar_m[int(xm[:, 2].argmin()), 2] -= 1.0
+    pb32, _, _ = mixed.adjoint_backward(xbar_m, None)
+    mixed.close()
+    diff32 = float(np.max(np.abs(pb32 - pb) / np.maximum(np.abs(pb), 1e-300)))
     return {"workload": f"taylor_bar_{deck.np}", "steps": nsteps, "forward_steps_done": done,
             "checkpoint_every": args.adj_every, "precision": "fp64",
             "forward_s": round(t_fwd, 4), "forward_with_checkpoints_s": round(t_ckpt, 4),
@@ -291,6 +301,10 @@ def adjoint_cost(args, local):
             "dlength_dparams": {"G": float(pb[0][0]), "yield": float(pb[0][1]), "hardening": float(pb[0][2]),
                                 "eos_s": float(pb[0][3])},
             "repeat_rel_diff": spread,
+            "fp32_forward": {"dlength_dparams": {"G": float(pb32[0][0]), "yield": float(pb32[0][1]),
+                                                  "hardening": float(pb32[0][2]), "eos_s": float(pb32[0][3])},
+                             "max_rel_diff_vs_fp64": diff32,
+                             "note": "the same reverse kernels along the mixed-precision forward trajectory"},
             "note": "forward = fused mcm_gpu_run; gradient = checkpointed forward + reverse sweep, timed on the "
                     "second gradient of the handle (the first allocates its storage); parameter sums use atomics, "
                     "so repeated gradients differ in the last bits (repeat_rel_diff)"}

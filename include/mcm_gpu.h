@@ -73,7 +73,7 @@ typedef enum {
 /* One material, as the reference holds it after mcm_matin, the mcm_sets routines and mcm_calcg:
  * `type material` of MCM/mcm_database.f90:235-257. */
 typedef struct {
-    int model;                 /* 1, 3, 9, 10 (4: cap model) */
+    int model;                 /* 1, 3, 4 (cap model: FP64-exact precision, disctype 0), 9, 10 */
     int eos;                   /* 1, 4, 13, 28, 41 (models 9, 10) */
     int visc_type;             /* 1: nodal artificial viscosity */
     double rho;                /* reference density (rho0 of every particle of this material) */
@@ -138,7 +138,8 @@ typedef struct {
 int mcm_gpu_set_device(int device);
 
 /* Applies the deck defaults and rearrangements of MCM/mcm_matin.f90:46-56,
- * MCM/mcm_sets1.f90, mcm_sets3.f90, mcm_sets10.f90 and mcm_calcg.f90 to a
+ * MCM/mcm_sets1.f90, mcm_sets3.f90, mcm_sets4.f90 (with its initial-cap and
+ * tension cut-off iterations), mcm_sets10.f90 and mcm_calcg.f90 to a
  * material given as read from its cards.  Replaces those routines for callers
  * that do not run the Fortran input phase. */
 int mcm_gpu_material_from_deck(mcm_gpu_material *m);
@@ -217,9 +218,11 @@ int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const dou
 
 /* No counterpart in the reference (it has no differentiation).  Reverse-mode
  * gradients of a function of the final state with respect to the initial
- * state and to the material parameters, through the whole step: FP64
- * precisions, disctype 0, every material model 10 with EOS 41,
- * reorder_interval 0.  The dt schedule is an input (the critical-timestep
+ * state and to the material parameters, through the whole step: disctype 0,
+ * every material model 10 with EOS 41, reorder_interval 0.  The forward runs
+ * in the handle's precision; the reverse kernels are FP64 and differentiate
+ * the FP64 step along that forward trajectory (with MCM_PREC_MIXED: the
+ * gradient of the step along the FP32-pair-sum trajectory).  The dt schedule is an input (the critical-timestep
  * minimum is not differentiated) and each step's neighbour lists are frozen
  * at their forward values.
  *

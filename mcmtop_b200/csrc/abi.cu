@@ -1255,7 +1255,6 @@ int adj_step(mcm_gpu_handle *h, int n, bool move) {
 }
 
 int adj_check(mcm_gpu_handle *h) {
-    if (h->cfg.precision == MCM_PREC_MIXED) return set_error(h, MCM_EUNSUPPORTED, "adjoint: FP64 precisions only");
     if (h->cfg.disctype != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: disctype 0 only");
     if (h->cfg.reorder_interval != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: reorder_interval must be 0");
     for (const mcm_gpu_material &m : h->mats)

@@ -191,12 +191,29 @@ def test_autograd_bar_shape_loss_matches_fd(lib, dts):
     assert np.all(rel < 1e-3), (grad, ref, rel)
 
 
+def test_fp32_forward_adjoint_agrees_with_fp64(lib, dts):
+    """The gradient along the mixed-precision forward (FP32 pair sums) against
+    the one along the FP64 forward: the trajectories differ by the mixed
+    step's error (about 1e-5 of each field), and so do the gradients."""
+    theta = nominal_theta()
+    rng = np.random.default_rng(21)
+    grads = {}
+    for name, prec in (("fp64", PREC), ("mixed", _abi.PREC_MIXED)):
+        s = Solver(deck_with(theta, V0), prec)
+        s.adjoint_forward(dts, EVERY)
+        x = s.download(["x"])["x"]
+        if name == "fp64":
+            W = rng.standard_normal(x.shape)
+        pb, _, v0b = s.adjoint_backward(W, None)
+        s.close()
+        grads[name] = np.concatenate([pb[0], [-VEL * v0b[:, 2].sum()]])
+    rel = np.abs(grads["mixed"] - grads["fp64"]) / np.abs(grads["fp64"])
+    print("fp64", grads["fp64"], "mixed", grads["mixed"], "rel", rel)
+    assert np.all(rel < 1e-3), rel
+
+
 def test_adjoint_rejects_unsupported(lib):
     d = taylor_bar(dx=DX)
-    s = Solver(d, _abi.PREC_MIXED)
-    with pytest.raises(_abi.MCMError):
-        s.adjoint_forward(np.full(3, s.dt), 2)
-    s.close()
     s = Solver(d, PREC, reorder_interval=5)
     with pytest.raises(_abi.MCMError):
         s.adjoint_forward(np.full(3, s.dt), 2)
