@@ -16,22 +16,24 @@
 // size is formed from small numbers and keeps FP32 relative accuracy at the
 // scale of h.  Ghost neighbours (few, near the planes) use FP64 positions.
 //
-// Compensated sums: 4 lanes share one particle's neighbours, so a lane adds
-// about K/4 terms (20) in plain FP32; the 4 partial sums are then combined
-// with an error-free TwoSum shuffle tree that carries the rounding error of
-// every addition, and the result is rounded once to FP64.  Measured on the
-// 2M bar after 205 steps against the FP64 step: worst field 1.25e-5 of its
-// range with plain lane sums, 1.05e-5 with per-lane Kahan sums; the error is
-// that of the FP32 pair terms, not of their sum, and the Kahan registers cost
-// 9 % of the step.  Four lanes (about 20 neighbours in flight per lane) hide
-// the record-gather latency better than 8 or 16: 0.92/1.19 ms for strain/
-// momentum against 0.96/1.33 (8 lanes) and 1.33/1.70 ms (16).
+// Compensated sums: 2 lanes share one particle's neighbours, so a lane adds
+// about K/2 terms (40) in plain FP32; the two partial sums are combined with
+// an error-free TwoSum shuffle step that carries the rounding error of the
+// addition, and the result is rounded once to FP64.  Measured on the 2M bar
+// (worst field's error against the FP64 step after 205 steps; mixed step
+// throughput): 2 lanes plain 1.20e-5, 402 M particle-steps/s; 2 lanes with
+// per-lane Kahan sums 1.00e-5, 374 M; 1 lane plain 1.57e-5, 377 M; 1 lane
+// Kahan 1.33e-5, 358 M; 4 lanes plain 1.25e-5, 385 M; 16 lanes 6.3e-6, 328 M.
+// The error is that of the FP32 pair terms rather than of their sum, and the
+// Kahan registers cost occupancy, so the lanes sum plainly.  Two lanes (about
+// 40 neighbours in flight per lane, one shuffle level) hide the record-gather
+// latency best: strain/momentum 0.78/1.11 ms per step.
 #include "nbr_iter.cuh"
 
 namespace mcm {
 namespace mixed {
 
-constexpr int L = 4;           // lanes per particle
+constexpr int L = 2;           // lanes per particle
 constexpr float kPiF = 3.14159265358979f;
 
 __device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
