@@ -40,6 +40,10 @@ class MaterialCard:
     rho_max: float = 0.0
     strinput: np.ndarray = field(default_factory=lambda: np.zeros(48))
     eosinput: np.ndarray = field(default_factory=lambda: np.zeros(24))
+    head: str = ""           # material heading card (12a6)
+    eos_head: str = ""       # EOS heading card (12a6)
+    ihq: int = 0             # hourglass type and coefficient: read, not used
+    qh: float = 0.0
 
 
 @dataclass
@@ -71,6 +75,26 @@ class Deck:
     mat: np.ndarray = None        # (np,) 1-based material ids
     dispbc: np.ndarray = None     # (np,)
     name: str = "deck"
+    # cards that select output and bookkeeping (MCM/mcm_control_v2.f90:92-115)
+    title: str = ""
+    max_np: int = 0
+    nstressp: int = 0
+    nvelocp: int = 0
+    stpltime: float = 0.0
+    state_opt: int = 0
+    thpltime: float = 0.0
+    status_interval: int = 0
+    restart_interval: int = 0
+    run_restart: int = 0
+    keep_files: int = 0
+    nlcur: int = 0
+    thnodes: tuple = ()           # time-history particle ids (1-based)
+    transducers: tuple = ()       # ((x, y, z), mat) per pressure transducer
+    pardata: np.ndarray = None    # (np, 4): mass, h, rho, e when massopt/init_h_opt/init_rhoe is 1
+    ncontmats: int = 0            # contact cards (MCM/mcm_contactype.f90)
+    cont_opt: int = 0
+    k_cont: tuple = ()
+    n_cont: tuple = ()
 
     @property
     def np(self) -> int:

@@ -1,0 +1,282 @@
+"""MCM's output files, written from the state downloaded at output times.
+
+The GPU step leaves the Fortran-side writers unchanged; this module is the
+same set of writers for a host program driving the step from Python:
+
+* state files of output option 4 (legacy VTK): MCM/mcm_VTK.f90 ``WriteVTK``
+  (all particles, ``<out><n>.vtk``) and ``WriteVTKmat`` (materials 1 and 2,
+  ``<m><out><n>.vtk``, with the cap-model point type), called by
+  MCM/mcm_init_state_output.f90:61-66 and MCM/mcm_state_output.f90:89-93;
+* time histories: MCM/mcm_inittimehist.f90 (file headers) and
+  MCM/mcm_timehist.f90 (``<out>_thist.csv``: per-material energies and
+  contact forces; ``<out>_th<id>.csv``: one particle's state);
+* pressure transducers: MCM/mcm_transducer_nbr.f90 (particles of the
+  transducer's material within 2h) and MCM/mcm_pressure_transducer.f90
+  (SPH interpolation of pressure and velocity, ``<out>_ptrn.csv``,
+  ``<out>_vtrn.csv``).
+
+Record layouts, number formats (fortio.fmt_e / fmt_f / fmt_i) and the
+values zeroed below 1e-50 (1e-40 for transducers) follow those routines.
+Deliberate differences: where the reference's integer fields overflow
+(``I5`` point counts from 100 000 particles, ``I6`` cell ids from 1 000 000,
+``I3`` state numbers from 1 000) it writes asterisks that no reader accepts;
+these writers widen the field instead.  The state writers of options 1-3
+(EnSight, LS-DYNA d3plot) and the 1D/2D ASCII state plots of option 0 are
+not provided: option 0 has no writer for 3D problems in the reference
+either (MCM/mcm_Stateplot.f90:40-47).
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+from .fortio import fmt_e, fmt_f, fmt_i
+
+# fields a state or time-history record reads
+VTK_FIELDS = ("x", "v", "p", "sigma", "mat", "ptype")
+TH_FIELDS = ("x", "v", "rho", "p", "sigma", "efps", "e", "mass", "c", "critts")
+TR_FIELDS = ("x", "v", "mass", "rho", "p", "h", "mat")
+
+_TH_HEAD_3D = (",Time,x coordinate,y coordinate,z coordinate,x velocity,y velocity,z velocity,"
+               "Density,Pressure,11 Stress,22 Stress,33 Stress,12 Stress,13 Stress,23 Stress,"
+               " Eff. Plastic Strain,Total Internal Energy,Speed of Sound,Critical timestep,Temperature")
+
+
+def _count(n: int) -> str:
+    """charParNumb of MCM/mcm_VTK.f90:45-56: the count left-aligned in 25
+    characters (I1..I5 by magnitude), widened past 99 999."""
+    return f"{n:<25d}"
+
+
+def _vm_stress(sig: np.ndarray) -> np.ndarray:
+    """VMStress of MCM/mcm_VTK.f90:153-158: the FP64 expression in the
+    reference's order, stored in a default REAL (FP32) variable."""
+    s11, s22, s33 = sig[:, 0, 0], sig[:, 1, 1], sig[:, 2, 2]
+    s12, s23, s13 = sig[:, 0, 1], sig[:, 1, 2], sig[:, 0, 2]
+    a = (s11 - s22) * (s11 - s22) + (s22 - s33) * (s22 - s33)
+    a = a + (s33 - s11) * (s33 - s11)
+    b = s12 * s12 + s23 * s23
+    b = b + s13 * s13
+    return np.sqrt(0.5 * (a + 6.0 * b)).astype(np.float32)
+
+
+def vtk_text(state: dict, sel: np.ndarray | None = None, with_ptype: bool = False) -> str:
+    """One legacy-VTK state file: WriteVTK (sel None, all particles) or
+    WriteVTKmat (sel = the particles of one material, with_ptype True)."""
+    x, v, p, sig = state["x"], state["v"], state["p"], state["sigma"]
+    if sel is not None:
+        x, v, p, sig = x[sel], v[sel], p[sel], sig[sel]
+    n = x.shape[0]
+    out = ["# vtk DataFile Version 3.0\n", "TEST\n", "ASCII\n", "DATASET UNSTRUCTURED_GRID\n",
+           f" POINTS {_count(n)} double\n"]
+    out.extend(fmt_f(a, 15, 8) + fmt_f(b, 15, 8) + fmt_f(c, 15, 8) + "\n" for a, b, c in x.tolist())
+    out.append(f" CELLS {_count(n)} {_count(2 * n)}\n")
+    out.extend(f"1 {k:6d}\n" for k in range(n))
+    out.append(f"CELL_TYPES {n:5d}\n")
+    out.append("1\n" * n)
+    out.append(f"POINT_DATA {n:5d}\n")
+    out.append(" VECTORS Velocities double\n")
+    out.extend(fmt_f(a, 15, 8) + fmt_f(b, 15, 8) + fmt_f(c, 15, 8) + "\n" for a, b, c in v.tolist())
+
+    def scalars(name, vals):
+        out.append(f"SCALARS {name} double 1\n")
+        out.append("LOOKUP_TABLE default\n")
+        out.extend(fmt_e(a, 24, 5) + "\n" for a in vals.tolist())
+
+    scalars("Pressure", p)
+    scalars("Stress_X", sig[:, 0, 0])
+    scalars("Stress_Y", sig[:, 1, 1])
+    scalars("Stress_Z", sig[:, 2, 2])
+    scalars("Shear_Stress_XY", sig[:, 0, 1])
+    scalars("Shear_Stress_XZ", sig[:, 0, 2])
+    scalars("Shear_Stress_YZ", sig[:, 1, 2])
+    scalars("VM_Stress", _vm_stress(sig).astype(np.float64))
+    if with_ptype:
+        pt = state["ptype"] if sel is None else state["ptype"][sel]
+        out.append("SCALARS PTYPE double 1\n")
+        out.append("LOOKUP_TABLE default\n")
+        out.extend(f"{int(a):5d}\n" for a in pt.tolist())
+    return "".join(out)
+
+
+def read_vtk(path: str) -> dict:
+    """Parses a file written by vtk_text back into arrays (for checks)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    out, i = {}, 0
+    while i < len(lines):
+        t = lines[i].split()
+        if not t:
+            i += 1
+            continue
+        if t[0] == "POINTS":
+            n = int(t[1])
+            out["x"] = np.array([[float(s) for s in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 3)
+            i += n + 1
+        elif t[0] == "VECTORS":
+            n = out["x"].shape[0]
+            out["v"] = np.array([[float(s) for s in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 3)
+            i += n + 1
+        elif t[0] == "SCALARS":
+            n = out["x"].shape[0]
+            out[t[1]] = np.array([float(lines[i + 2 + k]) for k in range(n)])
+            i += n + 2
+        else:
+            i += 1
+    return out
+
+
+class Outputs:
+    """Output cadence and files of MCM/mcm_initial.f90:109-115 and
+    MCM/mcm_solution.f90:81-92 for one problem.
+
+    ``fileout`` is the output base name (MCM's ``o=`` argument), ``directory``
+    where the files go."""
+
+    def __init__(self, deck, fileout: str, directory: str = "."):
+        self.deck = deck
+        self.base = os.path.join(directory, fileout)
+        self.title = (deck.title or deck.name)[:78]
+        self.nummat = len(deck.materials)
+        self.istate = 0
+        self.nextsttime = 0.0
+        self.nextthtime = 0.0
+        self.files = []
+
+    # --------------------------------------------------------- cadence
+    def fields(self, state_due: bool, th_due: bool) -> tuple:
+        need = set()
+        if state_due and self.deck.state_opt == 4:
+            need.update(VTK_FIELDS)
+        if th_due:
+            if self.deck.thnodes:
+                need.update(TH_FIELDS)
+            if self.deck.transducers:
+                need.update(TR_FIELDS)
+        return tuple(sorted(need))
+
+    def due(self, ptime: float) -> tuple:
+        end = self.deck.endtime
+        return ptime >= self.nextsttime or ptime >= end, ptime >= self.nextthtime or ptime >= end
+
+    def next_time(self) -> float:
+        return min(self.nextsttime, self.nextthtime, self.deck.endtime)
+
+    def initial(self, ptime: float, state: dict, energies: np.ndarray) -> None:
+        """mcm_init_state_output + mcm_state_output, mcm_inittimehist + mcm_timehist."""
+        self.nextsttime = ptime + self.deck.stpltime
+        if self.deck.state_opt == 4:
+            self._write_vtk(state)          # MCM/mcm_init_state_output.f90:61-64 (no increment)
+        self.state_output(state)
+        self.nextthtime = ptime + self.deck.thpltime
+        self._init_timehist()
+        self.timehist(ptime, state, energies)
+
+    def after_energies(self, ptime: float, state: dict, energies: np.ndarray) -> None:
+        """MCM/mcm_solution.f90:81-92, called after mcm_calctotale."""
+        st, th = self.due(ptime)
+        if st:
+            self.state_output(state)
+            self.nextsttime += self.deck.stpltime
+        if th:
+            self.timehist(ptime, state, energies)
+            self.nextthtime += self.deck.thpltime
+
+    # ---------------------------------------------------------- states
+    def state_output(self, state: dict) -> None:
+        """MCM/mcm_state_output.f90: option 4 writes the VTK files and counts."""
+        if self.deck.state_opt == 4:
+            self._write_vtk(state)
+            self.istate += 1
+
+    def _write_vtk(self, state: dict) -> None:
+        d, name = os.path.split(self.base)
+        tag = f"{self.istate:d}.vtk"
+        path = os.path.join(d, name + tag)
+        self._put(path, vtk_text(state))
+        for m in (1, 2):                     # MCM/mcm_state_output.f90:91-92
+            sel = np.flatnonzero(state["mat"] == m)
+            self._put(os.path.join(d, f"{m:d}{name}{tag}"), vtk_text(state, sel, with_ptype=True))
+
+    def _put(self, path: str, text: str, mode: str = "w") -> None:
+        with open(path, mode) as f:
+            f.write(text)
+        if path not in self.files:
+            self.files.append(path)
+
+    # ---------------------------------------------------- time history
+    def _th_path(self, pid: int) -> str:
+        # MCM/mcm_inittimehist.f90:62-65: '_th' // I<digits> // '.csv'
+        return f"{self.base}_th{pid:d}.csv"
+
+    def _init_timehist(self) -> None:
+        title = f"{self.title:<78}\n"
+        self._put(self.base + "_thist.csv", title + "Global time history data\n")
+        for pid in self.deck.thnodes:
+            if pid <= 0:
+                raise ValueError(f"time-history particle id {pid} is not positive")
+            self._put(self._th_path(pid), title + f"Time history data for particle {pid:6d}\n"
+                      + _TH_HEAD_3D + "\n")
+        if self.deck.transducers:
+            self._put(self.base + "_ptrn.csv", title + "Time,Pressure transducer time histories\n")
+            self._put(self.base + "_vtrn.csv", title + "Time,Velocity transducer time histories\n")
+
+    def timehist(self, ptime: float, state: dict, energies: np.ndarray) -> None:
+        """MCM/mcm_timehist.f90:41-64 and the 3D rows of :112-140."""
+        row = [ptime]
+        for m in range(self.nummat):
+            ke, ie = energies[5 * m], energies[5 * m + 1]
+            row += [ke, ie, 0.0, 0.0, 0.0]       # contact forces: no contact in this step
+        self._put(self.base + "_thist.csv", "".join("," + fmt_e(a, 14, 6) for a in row) + "\n", "a")
+        if self.deck.transducers:
+            self._transducers(ptime, state)
+        for pid in self.deck.thnodes:
+            i = pid - 1
+            s = state["sigma"][i]
+            cols = [*state["x"][i], *state["v"][i], state["rho"][i], state["p"][i], s[0, 0], s[1, 1], s[2, 2],
+                    s[0, 1], s[0, 2], s[1, 2], state["efps"][i], state["e"][i] / state["mass"][i],
+                    state["c"][i], state["critts"][i], 0.0]
+            cols = [0.0 if abs(c) < 1.0e-50 else float(c) for c in cols]
+            self._put(self._th_path(pid), "," + "".join(fmt_e(a, 14, 6) + "," for a in [ptime] + cols) + "\n",
+                      "a")
+
+    def _transducers(self, ptime: float, state: dict) -> None:
+        """MCM/mcm_transducer_nbr.f90:46-86 and MCM/mcm_pressure_transducer.f90:28-80:
+        particles of the transducer's material closer than 2h, summed only when
+        more than one is found.  (The reference keeps at most maxnbr+10 of
+        them and then reads past its list; all are summed here.)"""
+        x, h = state["x"], state["h"]
+        vol = state["mass"] / state["rho"]
+        pres, vel = [], []
+        for pos, mat in self.deck.transducers:
+            r2 = ((x - np.asarray(pos)) ** 2).sum(axis=1)
+            (idx,) = np.nonzero((r2 < (2.0 * h) ** 2) & (state["mat"] == mat))
+            pi, vi = 0.0, np.zeros(3)
+            if idx.size > 1:
+                for j in idx:
+                    w = _kernel_w(math.sqrt(r2[j]), h[j])
+                    pi += vol[j] * state["p"][j] * w
+                    vi += vol[j] * state["v"][j] * w
+            pres.append(0.0 if abs(pi) < 1.0e-40 else pi)
+            vel.extend(0.0 if abs(c) < 1.0e-40 else float(c) for c in vi)
+        self._put(self.base + "_ptrn.csv", "".join(fmt_e(a, 14, 6) + "," for a in [ptime] + pres) + "\n", "a")
+        self._put(self.base + "_vtrn.csv", "".join(fmt_e(a, 14, 6) + "," for a in [ptime] + vel) + "\n", "a")
+
+
+def _kernel_w(r: float, h: float) -> float:
+    """Cubic spline of MCM/mcm_kernel.f90:60-93 in 3D (c1 = 1/(pi h^3))."""
+    c1 = 1.0 / (math.acos(-1.0) * h * h * h)
+    z = r / h
+    if z < 1.0:
+        return c1 * ((0.75 * z - 1.5) * z * z + 1.0)
+    if z < 2.0:
+        return 0.25 * c1 * (2.0 - z) ** 3
+    return 0.0
+
+
+def status_line(timestep: int, ptime: float, dt: float) -> str:
+    """Format 1000 of MCM/mcm_solution.f90:143-144."""
+    return (f"\n     Problem status for time-step {fmt_i(timestep, 6)}\n"
+            f"     Time: {fmt_e(ptime, 10, 4)}     dt: {fmt_e(dt, 10, 4)}")

@@ -97,6 +97,13 @@ class Solver:
         disp = np.ascontiguousarray(deck.dispbc if deck.dispbc is not None else np.zeros(self.n), dtype=np.int32)
         f = _abi.Fields()
         f.x, f.v, f.mat, f.dispbc = _dptr(x), _dptr(v), _iptr(mat), _iptr(disp)
+        keep = []
+        if deck.pardata is not None:
+            # additional particle cards (MCM/mcm_nodein.f90:76-112): mass, h, rho, e
+            for col, nm in enumerate(("mass", "h", "rho", "e")):
+                a = np.ascontiguousarray(np.asarray(deck.pardata, dtype=np.float64)[:, col])
+                keep.append(a)
+                setattr(f, nm, _dptr(a))
         t = _abi.Time(0.0, 0.0, 0.0, deck.endtime)
         check(self.lib.mcm_gpu_initialise(h, C.byref(f), deck.massopt, deck.init_h_opt, deck.init_rhoe,
                                           deck.itss, C.byref(t)), "mcm_gpu_initialise", h)
@@ -125,6 +132,12 @@ class Solver:
     def step_b(self) -> np.ndarray:
         check(self.lib.mcm_gpu_step_b(self.h, _dptr(self.energies)), "mcm_gpu_step_b", self.h)
         return self.energies
+
+    def energies_now(self) -> np.ndarray:
+        """The energies of the last mcm_calctotale (step_b or initialisation)."""
+        e = np.zeros(5 * self.nmat + 3)
+        check(self.lib.mcm_gpu_energies(self.h, _dptr(e)), "mcm_gpu_energies", self.h)
+        return e
 
     def step_c(self) -> None:
         check(self.lib.mcm_gpu_step_c(self.h, self.dt, self.dtold, _dptr(self.bbox)), "mcm_gpu_step_c", self.h)

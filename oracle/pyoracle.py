@@ -129,7 +129,11 @@ class Oracle:
         mat = np.ascontiguousarray(deck.mat, dtype=np.int32)
         disp = np.ascontiguousarray(deck.dispbc, dtype=np.int32)
         st = C.c_int()
-        self.sim = self.lib.mcmo_create(C.byref(d), mats, _dp(x), _dp(v), _ip(mat), _ip(disp), None, C.byref(st))
+        pd = None
+        if getattr(deck, "pardata", None) is not None:
+            pd = np.ascontiguousarray(deck.pardata, dtype=np.float64)
+        self.sim = self.lib.mcmo_create(C.byref(d), mats, _dp(x), _dp(v), _ip(mat), _ip(disp),
+                                        _dp(pd) if pd is not None else None, C.byref(st))
         if not self.sim:
             raise RuntimeError(f"oracle create failed: status {st.value}")
 
