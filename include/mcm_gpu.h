@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MCM_GPU_ABI_VERSION 1
+#define MCM_GPU_ABI_VERSION 2
 #define MCM_GPU_MAX_MATERIALS 16
 
 /* Status codes.  The reference's fatal paths call mcm_shutdown(2)
@@ -93,8 +93,9 @@ typedef struct {
     int disctype;              /* 0 basic SPH, 1 Bonet mixed-corrected SPH */
     int tcrit_opt;             /* 0 DYNA formula, 1 h/(c+|v|), 2 mindist/(c+|v|) */
     int contacttype;           /* must be 0 (kernel contact) */
-    int h_opt;                 /* must be 0 (constant h) */
-    int veloc_opt;             /* must be 0 (no XSPH) */
+    int h_opt;                 /* smoothing length: 0 constant, 1 from the volumetric strain rate,
+                                  2 from the density (MCM/mcm_update_h.f90) */
+    int veloc_opt;             /* 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87) */
     int krtype;                /* 1: cubic B-spline */
     int drelax;                /* dynamic relaxation active */
     double drelax_scale;
@@ -122,6 +123,7 @@ typedef struct {
     double *etry, *einc, *capa;
     double *sigma, *s, *q, *qold, *alfa, *rod, *spin;   /* (3,3,np) */
     int *mat, *dispbc, *nnbr, *g_nnbr, *ptype;
+    double *h0;                                /* initial h (h_opt 2); upload: NULL takes h */
 } mcm_gpu_fields;
 
 typedef struct mcm_gpu_handle mcm_gpu_handle;

@@ -65,6 +65,7 @@ class Fields(C.Structure):
         ("etry", _DP), ("einc", _DP), ("capa", _DP),
         ("sigma", _DP), ("s", _DP), ("q", _DP), ("qold", _DP), ("alfa", _DP), ("rod", _DP), ("spin", _DP),
         ("mat", _IP), ("dispbc", _IP), ("nnbr", _IP), ("g_nnbr", _IP), ("ptype", _IP),
+        ("h0", _DP),
     ]
 
 

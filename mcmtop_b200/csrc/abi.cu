@@ -41,6 +41,8 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.drelax_scale = c.drelax_scale;
     p.tssf = c.tssf;
     p.hmax = c.hmax;
+    p.h_opt = c.h_opt;
+    p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;
     for (int d = 0; d < 3; ++d) {
@@ -239,6 +241,11 @@ int launch_mom(mcm_gpu_handle *h, int integrate) {
     }
 }
 int launch_move(mcm_gpu_handle *h) {
+    if (h->A.prm.veloc_opt) {
+        Scope sc(h, R_MOVE, 3);
+        if (h->cfg.precision == MCM_PREC_FP64_EXACT) return exact::launch_xsph_move(h->A, h->stream);
+        return fast::launch_xsph_move(h->A, h->stream);
+    }
     Scope sc(h, R_MOVE, 1);
     switch (h->cfg.precision) {
         case MCM_PREC_FP64_EXACT: return exact::launch_update_move(h->A, h->stream);
@@ -285,6 +292,18 @@ void enqueue_part_a(mcm_gpu_handle *h) {
 
 // momentum -> boundcond -> calctotale (-> update_velocity -> move)
 void enqueue_part_b(mcm_gpu_handle *h, int integrate) {
+    if (h->A.prm.veloc_opt && integrate) {
+        // XSPH needs every updated velocity before any particle moves
+        int nb = launch_mom(h, 0);
+        {
+            Scope sc(h, R_REDUCE, 2);
+            launch_energy_bbox_reduce(h->A, h->stream, nb, 1, 0);
+        }
+        nb = launch_move(h);
+        Scope sc(h, R_REDUCE, 1);
+        launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
+        return;
+    }
     int nb = launch_mom(h, integrate);
     Scope sc(h, R_REDUCE, 2);
     launch_energy_bbox_reduce(h->A, h->stream, nb, 1, integrate);
@@ -485,7 +504,8 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     if (!cfg || !mats || !out || np <= 0 || nmat <= 0 || nmat > MCM_GPU_MAX_MATERIALS) return MCM_EINVAL;
     *out = nullptr;
     if (cfg->ndim != 3) return MCM_EUNSUPPORTED;
-    if (cfg->contacttype != 0 || cfg->h_opt != 0 || cfg->veloc_opt != 0) return MCM_EUNSUPPORTED;
+    if (cfg->contacttype != 0) return MCM_EUNSUPPORTED;
+    if (cfg->h_opt < 0 || cfg->h_opt > 2 || cfg->veloc_opt < 0 || cfg->veloc_opt > 1) return MCM_EINVAL;
     if (cfg->krtype != 0 && cfg->krtype != 1) return MCM_EUNSUPPORTED;
     if (cfg->disctype != 0 && cfg->disctype != 1) return MCM_EINVAL;
     if (cfg->tcrit_opt < 0 || cfg->tcrit_opt > 2) return MCM_EINVAL;
@@ -557,6 +577,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->A.ngp = (int *)p; p += 64;
     h->A.plane_base = (int *)p; p += 32;
     h->A.n_inside = (int *)p; p += 32;
+    h->A.hmax = (double *)p; p += 32;
     h->A.energy = (double *)p;
     cudaMallocHost((void **)&h->h_time, 4096);
     char *q = (char *)h->h_time;
@@ -735,6 +756,8 @@ int run_part_a(mcm_gpu_handle *h) {
 int finish_upload(mcm_gpu_handle *h, const double *coord_maxmin) {
     int st;
     k_iota<<<256, 256, 0, h->stream>>>(h->A.F.orig, h->np);
+    const double hm[2] = {h->A.prm.hmax, 0.0};
+    CK(cudaMemcpyAsync(h->A.hmax, hm, sizeof(hm), cudaMemcpyHostToDevice, h->stream));
     if (coord_maxmin) {
         double b[6];
         for (int d = 0; d < 3; ++d) { b[d] = coord_maxmin[2 * d]; b[3 + d] = coord_maxmin[2 * d + 1]; }
@@ -768,6 +791,9 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
         {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}};
     for (auto &s : sc)
         if (s.p && (st = put_scalar(h, s.p, s.f))) return st;
+    if (f->h0 || f->h) {
+        if ((st = put_scalar(h, f->h0 ? f->h0 : f->h, FH0))) return st;
+    }
     if (f->sigma && (st = put_sym(h, f->sigma, FS11, tmp))) return st;
     if (f->sigma && (st = put_lower(h, f->sigma, FL21, tmp))) return st;
     if (f->s && (st = put_sym(h, f->s, FD11, tmp))) return st;
@@ -994,7 +1020,7 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
         {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
         {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
         {f->fail, FFAIL}, {f->mindist, FMINDIST}, {f->critts, FCRITTS}, {f->tracerod, FTR},
-        {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}};
+        {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}, {f->h0, FH0}};
     for (auto &s : sc)
         if (s.p && (st = scal(s.p, s.f))) return st;
     if (f->sigma && (st = sym(f->sigma, FS11))) return st;
@@ -1235,11 +1261,15 @@ int snap_save(mcm_gpu_handle *h, double *buf) {
     CK(cudaMemcpyAsync(buf, h->d_fields, sizeof(double) * NFIELD * h->npad, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(buf + (size_t)NFIELD * h->npad, h->A.bbox, sizeof(double) * 6, cudaMemcpyDeviceToDevice,
                        h->stream));
+    CK(cudaMemcpyAsync(buf + (size_t)NFIELD * h->npad + 6, h->A.hmax, sizeof(double) * 2, cudaMemcpyDeviceToDevice,
+                       h->stream));
     return MCM_OK;
 }
 int snap_load(mcm_gpu_handle *h, const double *buf) {
     CK(cudaMemcpyAsync(h->d_fields, buf, sizeof(double) * NFIELD * h->npad, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(h->A.bbox, buf + (size_t)NFIELD * h->npad, sizeof(double) * 6, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    CK(cudaMemcpyAsync(h->A.hmax, buf + (size_t)NFIELD * h->npad + 6, sizeof(double) * 2, cudaMemcpyDeviceToDevice,
                        h->stream));
     return MCM_OK;
 }
@@ -1257,6 +1287,8 @@ int adj_step(mcm_gpu_handle *h, int n, bool move) {
 int adj_check(mcm_gpu_handle *h) {
     if (h->cfg.disctype != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: disctype 0 only");
     if (h->cfg.reorder_interval != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: reorder_interval must be 0");
+    if (h->cfg.h_opt != 0 || h->cfg.veloc_opt != 0)
+        return set_error(h, MCM_EUNSUPPORTED, "adjoint: constant smoothing length without XSPH only");
     for (const mcm_gpu_material &m : h->mats)
         if (m.model != 10 || m.eos != 41) return set_error(h, MCM_EUNSUPPORTED, "adjoint: model 10 with EOS 41 only");
     return MCM_OK;

@@ -24,18 +24,19 @@ __global__ void k_grid_setup(StepArgs a) {
     if (a.status->code) return;
     const DevParams &P = a.prm;
     const double factor = 2.0;
+    const double hmax = a.hmax[0];   // fixed, or the last mcm_update_h's maximum
     DevGrid g;
     for (int i = 0; i < 3; ++i) {
         g.gridmin[i] = 0.0;
         g.gridlim[i] = 1;
-        g.gridsize[i] = 1.0 / (factor * P.hmax);
+        g.gridsize[i] = 1.0 / (factor * hmax);
     }
     bool bad = false;
     for (int i = 0; i < P.ndim; ++i) {
         double span = 0.0;
         switch (P.planes.type[i]) {
             case 1:
-                g.gridmin[i] = a.bbox[i] - 0.01 * P.hmax;
+                g.gridmin[i] = a.bbox[i] - 0.01 * hmax;
                 span = g.gridsize[i] * (a.bbox[3 + i] - g.gridmin[i]);
                 if (!(span < 1.0e9)) { bad = true; span = 0; }
                 g.gridlim[i] = (int)span + 1;
@@ -50,7 +51,7 @@ __global__ void k_grid_setup(StepArgs a) {
                 span = g.gridsize[i] * (P.planes.bx[1][i] - a.bbox[i]);
                 if (!(span < 1.0e9)) { bad = true; span = 0; }
                 g.gridlim[i] = (int)span + 1;
-                g.gridmin[i] = P.planes.bx[1][i] - g.gridlim[i] * factor * P.hmax;
+                g.gridmin[i] = P.planes.bx[1][i] - g.gridlim[i] * factor * hmax;
                 break;
             case 4:
                 g.gridmin[i] = P.planes.bx[0][i];

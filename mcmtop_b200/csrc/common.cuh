@@ -63,6 +63,8 @@ struct DevPlanes {
 struct DevParams {
     int ndim, disctype, tcrit_opt, boundary, baseaccel, drelax, nmat, diag;
     int asym;         // a material of the cap model is present: the momentum sum reads both triangles of sigma
+    int h_opt;        // variable smoothing length (MCM/mcm_update_h.f90): 0 fixed, 1 strain rate, 2 density
+    int veloc_opt;    // 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87)
     int pad_;
     double drelax_scale, tssf, hmax;
     double base_a[3];
@@ -85,6 +87,8 @@ enum Field {
     // lower triangle of sigma (21, 31, 32): equal to the upper one except for
     // the cap model, whose return map writes the upper triangle only
     FL21, FL31, FL32,
+    FH0,                                     // initial smoothing length (h_opt 2)
+    FXS0, FXS1, FXS2,                        // XSPH velocity sums of the step
     NFIELD
 };
 

@@ -23,6 +23,7 @@ struct StepArgs {
     DevStatus *status;
     DevGrid *grid;
     double *bbox;     // [2][3]: min, max (mcm_coord_maxmin)
+    double *hmax;     // [0]: mcm_hmax, the grid's cell half-size; [1]: bits of the step's new maximum (h_opt > 0)
     // cell list.  "Position" p is a particle's rank in cell order (cells in
     // key order, each cell in descending reference index, particles outside
     // the grid last); cell_list[p] is its state index.
@@ -124,6 +125,7 @@ void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s);
     void launch_mom_prep(const StepArgs &a, cudaStream_t s);                        \
     int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);          \
     int launch_update_move(const StepArgs &a, cudaStream_t s);                      \
+    int launch_xsph_move(const StepArgs &a, cudaStream_t s);                        \
     int launch_initial(const StepArgs &a, cudaStream_t s, int massopt, int init_h_opt, int init_rhoe, const int *nppermat); \
     int launch_init_critts(const StepArgs &a, cudaStream_t s);                      \
     }

@@ -26,6 +26,14 @@ __global__ void k_critts_reduce(StepArgs a, int nblocks, int fused, int init) {
         DevTime *t = a.time;
         t->critts = m;
         if (init) return;
+        if (a.prm.h_opt) {
+            // the largest h of this step's mcm_update_h becomes the next grid's hmax
+            // (kept when no particle was at or above its cut-off pressure)
+            unsigned long long *bid = reinterpret_cast<unsigned long long *>(a.hmax + 1);
+            const unsigned long long b = *bid;
+            if (b) a.hmax[0] = __longlong_as_double(static_cast<long long>(b));
+            *bid = 0ull;
+        }
         if (fused) {
             t->dtold = t->dt;
             double dt = a.prm.tssf * m;

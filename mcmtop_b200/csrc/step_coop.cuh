@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
             case 7: acc[0] = 0.0; acc[1] = 0.0; acc[2] = 0.0; break;
             default: break;
         }
-        if (a.split_mode || a.prm.diag) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
+        if (a.split_mode || a.prm.diag || a.prm.veloc_opt) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
         const int mati = a.F.mat[i];
         const double mass = f[FMASS][i], vabs = f[FVABS][i];
         const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),

@@ -146,6 +146,7 @@ __device__ __forceinline__ void load_state(const StepArgs &a, int i, PState<doub
 __device__ __forceinline__ void store_state(const StepArgs &a, int i, const PState<double> &P, int model) {
     double *const *f = a.F.f;
     f[FH][i] = P.h;
+    if (a.prm.h_opt) f[FHOLD][i] = P.hold;
     f[FRHO][i] = P.rho; f[FE][i] = P.e; f[FP][i] = P.p; f[FC][i] = P.c;
     f[FEFPS][i] = P.efps; f[FPCUT][i] = P.pcut; f[FPCUT2][i] = P.p_cut; f[FFAIL][i] = P.fail;
 #pragma unroll
@@ -325,6 +326,20 @@ __global__ void __launch_bounds__(kRedThreads) k_strain(StepArgs a) {
     f[FTR][i] = r11 + r22 + r33;
 }
 
+// ------------------------------------------------- variable smoothing length
+// MCM/mcm_update_h.f90:25-55 (after mcm_strain, before the constitutive
+// update): particles at or above their cut-off pressure take a new h and
+// bid it for the next grid's hmax.  h >= 0, so the bit patterns of the
+// doubles order like the values and an integer maximum picks the largest.
+__device__ __forceinline__ void update_h(const StepArgs &a, int i, PState<double> &P, double dt) {
+    if (!(P.p >= P.pcut)) return;
+    P.hold = P.h;
+    if (a.prm.h_opt == 1) P.h = P.hold * (1.0 + P.tracerod * dt / 3.0);
+    else P.h = a.F.f[FH0][i] * pow(P.rho0 / P.rho, 1.0 / 3.0);
+    atomicMax(reinterpret_cast<unsigned long long *>(a.hmax + 1),
+              static_cast<unsigned long long>(__double_as_longlong(P.h)));
+}
+
 // ---------------------------------------------------- constitutive update
 // MCM/mcm_rhoupd.f90, mcm_constitutive.f90:29-83 and mcm_calccritts.f90 for
 // the particle with state index i, and the forward half-step shift of
@@ -347,6 +362,7 @@ __global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
         P.spin[1] = f[FW13][i];
         P.spin[2] = f[FW23][i];
         P.tracerod = f[FTR][i];
+        if (a.prm.h_opt) update_h(a, i, P, dt);
         rhoupd(P, M, dt, 3);
         bad = constitutive_particle(P, M, dt);
         const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
@@ -626,7 +642,7 @@ __global__ void __launch_bounds__(kRedThreads) k_momentum(StepArgs a, int integr
             case 7: acc[0] = 0.0; acc[1] = 0.0; acc[2] = 0.0; break;
             default: break;
         }
-        if (a.split_mode || a.prm.diag) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
+        if (a.split_mode || a.prm.diag || a.prm.veloc_opt) { f[FAX][i] = acc[0]; f[FAY][i] = acc[1]; f[FAZ][i] = acc[2]; }
         mati = a.F.mat[i];
         const double mass = f[FMASS][i], vabs = f[FVABS][i];
         ke = 0.5 * mass * (vabs * vabs);
@@ -677,6 +693,106 @@ __global__ void __launch_bounds__(kRedThreads) k_update_move(StepArgs a) {
         double xn[3];
         integrate_particle(a, i, acc, a.time->dt, a.time->dtold, xn);
         x[0] = xmax[0] = xn[0]; x[1] = xmax[1] = xn[1]; x[2] = xmax[2] = xn[2];
+    }
+    const int stride = 5 * a.nmat + 6;
+    double *out = a.red + (size_t)blockIdx.x * stride;
+    for (int d = 0; d < 3; ++d) {
+        double lo = block_minmax(x[d], sm, false);
+        double hi = block_minmax(xmax[d], sm, true);
+        if (threadIdx.x == 0) { out[5 * a.nmat + d] = lo; out[5 * a.nmat + 3 + d] = hi; }
+    }
+}
+
+// ----------------------------------------------------------------- XSPH
+// MCM/mcm_update_velocity.f90:29-87 with veloc_opt 1, as three passes over
+// the particles: the velocity update, the XSPH sums (which read every
+// particle's updated velocity), then the smoothed velocity and the move.
+// In a fused run the step that terminates skips all three, like the fused
+// momentum kernel.
+__global__ void k_velocity(StepArgs a) {
+    if (skip_step(a) || a.time->ended) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    double *const *f = a.F.f;
+    const double dtn = 0.5 * (a.time->dt + a.time->dtold);
+    double vabs = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        double v = f[FVX + j][i];
+        if (a.prm.drelax) v = a.prm.drelax_scale * v + f[FAX + j][i] * dtn;
+        else v = v + f[FAX + j][i] * dtn;
+        f[FVX + j][i] = v;
+        vabs = vabs + v * v;
+    }
+    f[FVABS][i] = sqrt(vabs);
+}
+
+// Sum over the step's neighbours in reference order: real ones read the
+// updated state, ghosts their copies from the start of the step; W takes the
+// neighbour's h and V_j = m_j / ((rho_j + rho_i) / 2).
+__global__ void k_xsph_sum(StepArgs a) {
+    if (skip_step(a) || a.time->ended) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const double *const *f = a.F.f;
+    const int i = a.cell_list[t];
+    const double xi[3] = {f[FX][i], f[FY][i], f[FZ][i]};
+    const double vi[3] = {f[FVX][i], f[FVY][i], f[FVZ][i]};
+    const double rhoi = f[FRHO][i];
+    double sv[3] = {0.0, 0.0, 0.0};
+    auto body = [&](double xj0, double xj1, double xj2, double vj0, double vj1, double vj2, double massj,
+                    double rhoj, double hj) {
+        const double w = kernelw(xi[0] - xj0, xi[1] - xj1, xi[2] - xj2, hj);
+        const double volj = massj / (0.5 * (rhoj + rhoi));
+        sv[0] = sv[0] + volj * (vj0 - vi[0]) * w;
+        sv[1] = sv[1] + volj * (vj1 - vi[1]) * w;
+        sv[2] = sv[2] + volj * (vj2 - vi[2]) * w;
+    };
+    for_each_neighbour(
+        a, *a.grid, t,
+        [&](int p, bool) {
+            const int j = a.cell_list[p];
+            body(f[FX][j], f[FY][j], f[FZ][j], f[FVX][j], f[FVY][j], f[FVZ][j], f[FMASS][j], f[FRHO][j], f[FH][j]);
+        },
+        [&](int q) { body(a.gx[q], a.gy[q], a.gz[q], a.gvx[q], a.gvy[q], a.gvz[q], a.gmass[q], a.grho[q], a.gh[q]); });
+    double *const *fw = a.F.f;
+    fw[FXS0][i] = sv[0];
+    fw[FXS1][i] = sv[1];
+    fw[FXS2][i] = sv[2];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_xsph_move(StepArgs a) {
+    __shared__ double sm[32];
+    if (skip_step(a) || a.time->ended) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double x[3] = {1.0e20, 1.0e20, 1.0e20};
+    double xmax[3] = {-1.0e20, -1.0e20, -1.0e20};
+    if (i < a.n) {
+        double *const *f = a.F.f;
+        const double epsilon = 0.100;
+        const double dt = a.time->dt;
+        double v[3], xo[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            v[j] = f[FVX + j][i] + epsilon * f[FXS0 + j][i];
+            x[j] = f[FX + j][i] + v[j] * dt;
+            xmax[j] = x[j];
+            xo[j] = x[j];
+        }
+        if (a.prm.boundary) {
+            const DevPlanes &pl = a.prm.planes;
+            for (int d = 0; d < 3; ++d) {
+                if (pl.code[0][d] == 1 && xo[d] < pl.bx[0][d]) { xo[d] = 2.0 * pl.bx[0][d] - xo[d]; v[d] = -v[d]; }
+                if (pl.code[1][d] == 1 && xo[d] > pl.bx[1][d]) { xo[d] = 2.0 * pl.bx[1][d] - xo[d]; v[d] = -v[d]; }
+                if (pl.code[0][d] == 2) {
+                    double dx = pl.bx[1][d] - pl.bx[0][d];
+                    if (xo[d] < pl.bx[0][d]) xo[d] = xo[d] + dx;
+                    if (xo[d] > pl.bx[1][d]) xo[d] = xo[d] - dx;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { f[FVX + j][i] = v[j]; f[FX + j][i] = xo[j]; }
     }
     const int stride = 5 * a.nmat + 6;
     double *out = a.red + (size_t)blockIdx.x * stride;
@@ -780,6 +896,7 @@ __global__ void k_initial(StepArgs a, int massopt, int init_h_opt, int init_rhoe
         // MCM/mcm_init_h.f90:22-48
         if (init_h_opt == 0) f[FH][i] = M.h;
         f[FHOLD][i] = f[FH][i];
+        f[FH0][i] = f[FH][i];
         // MCM/mcm_initial.f90:62-69: tracerod = 0 gives q = 0
         f[FQ][i] = 0.0;
         f[FTR][i] = 0.0;
@@ -872,6 +989,14 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
 int launch_update_move(const StepArgs &a, cudaStream_t s) {
     int blocks = nblk(a.n, kRedThreads);
     k_update_move<<<blocks, kRedThreads, 0, s>>>(a);
+    return blocks;
+}
+
+int launch_xsph_move(const StepArgs &a, cudaStream_t s) {
+    const int blocks = nblk(a.n, kRedThreads);
+    k_velocity<<<blocks, kRedThreads, 0, s>>>(a);
+    k_xsph_sum<<<blocks, kRedThreads, 0, s>>>(a);
+    k_xsph_move<<<blocks, kRedThreads, 0, s>>>(a);
     return blocks;
 }
 

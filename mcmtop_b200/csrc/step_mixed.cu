@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
                 case 7: ac[0] = 0.0; ac[1] = 0.0; ac[2] = 0.0; break;
                 default: break;
             }
-            if (a.split_mode || a.prm.diag) { f[FAX][i] = ac[0]; f[FAY][i] = ac[1]; f[FAZ][i] = ac[2]; }
+            if (a.split_mode || a.prm.diag || a.prm.veloc_opt) { f[FAX][i] = ac[0]; f[FAY][i] = ac[1]; f[FAZ][i] = ac[2]; }
             const int mati = a.F.mat[i];
             const double mass = f[FMASS][i], vabs = f[FVABS][i];
             const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),

@@ -150,6 +150,8 @@ struct Sim {
     void grad1(real *dwdx, real &dwdr, const real *xi, const real *xj, real havg) const;
     // strain
     void strain();
+    void update_h();
+    void xsph();
     void oldstrain();
     void corr_strain();
     void get_j_strain_info(int i, int k, real *x, real *v, real &mass, real &rho, real &h, real &hold);
@@ -297,7 +299,7 @@ int Sim::setup(const mcmo_deck *d, const mcmo_material *m, const double *x, cons
     contacttype = d->contacttype; tcrit_opt = d->tcrit_opt; veloc_opt = d->veloc_opt;
     h_opt = d->h_opt; krtype = d->krtype; maxnbr = d->maxnbr;
     for (int k = 0; k < 3; ++k) nthp[k] = d->nthp[k];
-    if (contacttype != 0 || h_opt != 0 || veloc_opt != 0) return MCMO_EUNSUPPORTED;
+    if (contacttype != 0 || h_opt < 0 || h_opt > 2 || veloc_opt < 0 || veloc_opt > 1) return MCMO_EUNSUPPORTED;
     // MCM/mcm_control_v2.f90:193-243
     if (tssf == 0.0) tssf = 0.8;
     if (krtype == 0) krtype = 1;
@@ -2288,7 +2290,62 @@ void Sim::calctotale() {
     totale = kinetice + internale;
 }
 
-// MCM/mcm_update_velocity.f90:29-56 (XSPH is not restated: veloc_opt 0)
+// MCM/mcm_update_h.f90:25-55: h follows the volumetric strain rate (h_opt 1)
+// or the density (h_opt 2) for particles at or above their cut-off pressure,
+// and hmax, the next grid's cell size, is their largest h.  With no such
+// particle the reference would set hmax to 0 (a zero division in the grid);
+// the previous hmax is kept instead.
+void Sim::update_h() {
+    real hm = 0.0;
+    if (h_opt == 1) {
+        for (int i = ssp; i <= esp; ++i) {
+            Particle &P = par[i];
+            if (P.p >= P.pcut) {
+                P.hold = P.h;
+                P.h = P.hold * (1.0 + P.tracerod * dt / (real)(float)ndim);
+                hm = std::max(hm, P.h);
+            }
+        }
+    } else if (h_opt == 2) {
+        const real power = 1.0 / (real)(float)ndim;
+        for (int i = ssp; i <= esp; ++i) {
+            Particle &P = par[i];
+            if (P.p >= P.pcut) {
+                P.hold = P.h;
+                P.h = P.h0 * std::pow(P.rho0 / P.rho, power);
+                hm = std::max(hm, P.h);
+            }
+        }
+    }
+    if (hm > 0.0) hmax = hm;
+}
+
+// MCM/mcm_update_velocity.f90:61-87: XSPH.  The neighbours' velocities are
+// the updated ones for real particles and the ghosts' copies from the start of
+// the step; W uses the neighbour's h; the sums are applied after all are done.
+void Sim::xsph() {
+    const real epsilon = 0.100;
+    std::vector<real> sv(3 * (size_t)(np + 1), 0.0);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int i = 1; i <= np; ++i) {
+        Particle &P = par[i];
+        real s[3] = {0.0, 0.0, 0.0};
+        for (int j = 1; j <= P.nnbr + P.g_nnbr; ++j) {
+            real xj[3], vj[3], massj, rhoj, hj, holdj;
+            get_j_strain_info(i, j, xj, vj, massj, rhoj, hj, holdj);
+            real w = kernel1(P.x, xj, hj);
+            real volj = massj / (0.5 * (rhoj + P.rho));
+            for (int k = 0; k < ndim; ++k) s[k] = s[k] + volj * (vj[k] - P.v[k]) * w;
+        }
+        for (int k = 0; k < 3; ++k) sv[3 * (size_t)i + k] = s[k];
+    }
+    for (int i = 1; i <= np; ++i)
+        for (int j = 0; j < ndim; ++j) par[i].v[j] = par[i].v[j] + epsilon * sv[3 * (size_t)i + j];
+}
+
+// MCM/mcm_update_velocity.f90:29-56, then XSPH (veloc_opt 1)
 void Sim::update_velocity() {
     real dtn = 0.5 * (dt + dtold);
 #ifdef _OPENMP
@@ -2304,6 +2361,7 @@ void Sim::update_velocity() {
         }
         P.vabs = std::sqrt(P.vabs);
     }
+    if (veloc_opt == 1) xsph();
 }
 
 // MCM/mcm_move.f90:25-55
@@ -2346,6 +2404,7 @@ void Sim::check_sym_pen() {
 int Sim::step_a(real *critts_out) {
     neighbours();
     strain();
+    if (h_opt > 0) update_h();
     int st = constitutive();
     if (critts_out) *critts_out = critts;
     return st;

@@ -1,0 +1,102 @@
+"""Variable smoothing length (h_opt 1 and 2, MCM/mcm_update_h.f90) and XSPH
+velocity smoothing (veloc_opt 1, MCM/mcm_update_velocity.f90:61-87) on the
+GPU against the oracle."""
+import numpy as np
+import pytest
+
+from mcmtop_b200 import _abi
+from mcmtop_b200.deck import fluid_column, taylor_bar
+from mcmtop_b200.solver import Solver
+from oracle.pyoracle import Oracle
+from test_gpu_parity import STATE, compare, compare_neighbours
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "h_strain_rate": dict(h_opt=1),
+    "h_density": dict(h_opt=2),
+    "xsph": dict(veloc_opt=1),
+    "h_density_xsph": dict(h_opt=2, veloc_opt=1),
+    "h_strain_rate_corrected": dict(h_opt=1, disctype=1),
+}
+
+
+def _pair(deck, prec=_abi.PREC_FP64_EXACT):
+    return Solver(deck, prec), Oracle(deck)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_exact_matches_oracle(name, gpu_lib, oracle_lib):
+    deck = taylor_bar(dx=0.8e-3).replace(**CASES[name])
+    sol, orc = _pair(deck)
+    try:
+        for step in range(40):
+            sol.step()
+            orc.step()
+            if step % 10 == 9:
+                gl, gm, gs = sol.grid()
+                ogl, ogm, ogs = orc.grid()
+                assert np.array_equal(gl, ogl) and np.array_equal(gs, ogs) and np.array_equal(gm, ogm), step
+        assert sol.dt == orc.scalar("dt")
+        compare(sol, orc, STATE + ["hold"], 1e-12, name)
+        compare_neighbours(sol, orc)
+        h = sol.download(["h"])["h"]
+        if deck.h_opt:
+            assert h.max() > h.min()          # h now differs between particles
+    finally:
+        sol.close()
+        orc.close()
+
+
+def test_xsph_with_ghost_planes(gpu_lib, oracle_lib):
+    # five symmetry planes: the ghosts carry their velocities from the start of the step
+    deck = fluid_column(dx=40e-3).replace(veloc_opt=1, h_opt=2)
+    sol, orc = _pair(deck)
+    try:
+        for _ in range(30):
+            sol.step()
+            orc.step()
+        compare(sol, orc, STATE, 1e-12, "fluid column")
+    finally:
+        sol.close()
+        orc.close()
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64_EXACT, _abi.PREC_FP64, _abi.PREC_MIXED])
+def test_fused_run_equals_split_steps(prec, gpu_lib):
+    deck = taylor_bar(dx=0.8e-3).replace(h_opt=1, veloc_opt=1)
+    a, b = Solver(deck, prec), Solver(deck, prec)
+    try:
+        for _ in range(25):
+            a.step()
+        assert b.run(25) == 25
+        sa, sb = a.download(STATE + ["hold"]), b.download(STATE + ["hold"])
+        for f in sa:
+            assert np.array_equal(sa[f], sb[f]), f
+        assert a.ptime == b.ptime and a.dt == b.dt
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(_abi.PREC_FP64, 1e-9), (_abi.PREC_MIXED, 2e-4)])
+def test_fast_paths_follow_the_oracle(prec, tol, gpu_lib, oracle_lib):
+    deck = taylor_bar(dx=0.8e-3).replace(h_opt=2, veloc_opt=1)
+    sol, orc = _pair(deck, prec)
+    try:
+        for _ in range(20):
+            sol.step()
+            orc.step()
+        compare(sol, orc, ["x", "v", "h", "rho", "p", "sigma"], tol, "fast")
+    finally:
+        sol.close()
+        orc.close()
+
+
+def test_adjoint_rejects_variable_h(gpu_lib):
+    sol = Solver(taylor_bar(dx=0.8e-3).replace(h_opt=1), _abi.PREC_FP64)
+    try:
+        with pytest.raises(RuntimeError):
+            sol.adjoint_forward(np.full(3, 1e-3))
+    finally:
+        sol.close()
