@@ -266,6 +266,23 @@ def fluid_column(dx: float = 2.0e-3, block=(0.5, 0.25, 1.0), box=(2.0, 0.25, 1.2
                 name=f"fluid_column_dx{dx * 1e3:g}mm_n{npart}")
 
 
+def periodic_layer(dx: float = 40e-3, size=(2.0, 0.24, 0.4), seed: int = 77, jitter: float = 0.005,
+                   noise: float = 1.0, gravity: float = 9.81, tssf: float = 0.3, endtime: float = 1.0e12,
+                   c0: float = 40.0) -> Deck:
+    """A water layer filling a box that is periodic in x and y
+    (MCM/mcm_inp_symmetry_v2.f90 flag 2 on both sides) on a z-min symmetry
+    floor, under gravity, with a seeded random velocity of amplitude `noise`
+    (m/s) so that particles cross the periodic planes.  SI arguments; the deck
+    is in cm-g-us."""
+    d = fluid_column(dx=dx, block=size, box=(size[0], size[1], 3.0 * size[2]), seed=seed, jitter=jitter,
+                     gravity=gravity, tssf=tssf, endtime=endtime, c0=c0)
+    rng = np.random.default_rng(seed + 1)
+    v = rng.uniform(-noise, noise, size=d.x.shape) * VEL
+    bx = [b * CM for b in size]
+    return d.replace(v=v, sym_flag=(2, 2, 2, 2, 1, 0), sym_x=(0.0, bx[0], 0.0, bx[1], 0.0, 3.0 * bx[2]),
+                     name=f"periodic_layer_dx{dx * 1e3:g}mm_n{d.np}")
+
+
 def taylor_ensemble(nbodies: int = 256, seed: int = 2024, nmin: int = 4000, nmax: int = 64000,
                     radius=(2.0e-3, 4.0e-3), aspect=(6.0, 12.0), yield_stress=(200e6, 600e6),
                     velocity=(120.0, 250.0), tcrit_opt: int = 1) -> list:

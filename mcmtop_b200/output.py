@@ -13,7 +13,9 @@ same set of writers for a host program driving the step from Python:
 * pressure transducers: MCM/mcm_transducer_nbr.f90 (particles of the
   transducer's material within 2h) and MCM/mcm_pressure_transducer.f90
   (SPH interpolation of pressure and velocity, ``<out>_ptrn.csv``,
-  ``<out>_vtrn.csv``).
+  ``<out>_vtrn.csv``);
+* the relaxed state after a dynamic-relaxation run: MCM/mcm_write_drelax.f90
+  (``<out>.drlx``).
 
 Record layouts, number formats (fortio.fmt_e / fmt_f / fmt_i) and the
 values zeroed below 1e-50 (1e-40 for transducers) follow those routines.
@@ -200,6 +202,12 @@ class Outputs:
             sel = np.flatnonzero(state["mat"] == m)
             self._put(os.path.join(d, f"{m:d}{name}{tag}"), vtk_text(state, sel, with_ptype=True))
 
+    def drelax(self, state: dict) -> None:
+        """MCM/mcm_write_drelax.f90: written once, after the loop, when
+        dynamic relaxation is active (0.1 < drelax_scale < 1)."""
+        if 0.1 < self.deck.drelax_scale < 1.0:
+            self._put(self.base + ".drlx", drelax_text(state))
+
     def _put(self, path: str, text: str, mode: str = "w") -> None:
         with open(path, mode) as f:
             f.write(text)
@@ -274,6 +282,25 @@ def _kernel_w(r: float, h: float) -> float:
     if z < 2.0:
         return 0.25 * c1 * (2.0 - z) ** 3
     return 0.0
+
+
+DRELAX_FIELDS = ("x", "dispbc", "mat", "mass", "h", "rho", "e")
+
+
+def drelax_text(state: dict) -> str:
+    """The relaxed state file of MCM/mcm_write_drelax.f90:36-72 (3D): node
+    cards (i8,i5,3e20.13,i7) and additional particle cards (i8,4e20.13), the
+    layouts of MCM/mcm_nodein.f90 so that the lines can be pasted into a deck.
+    (The second layout spans 88 columns; a deck reader that keeps 80 of them,
+    as MCM's does, loses the energy's exponent.)"""
+    x, disp, mat = state["x"], state["dispbc"], state["mat"]
+    out = ["*\n* Node Coordinates and Materials\n*\n"]
+    out.extend(f"{i + 1:8d}{int(disp[i]):5d}" + "".join(fmt_e(c, 20, 13) for c in x[i]) + f"{int(mat[i]):7d}\n"
+               for i in range(x.shape[0]))
+    out.append("*\n* Node Data\n*     ID  Mass                Smoothing Length    Density             Internal Energy\n")
+    cols = np.stack([state["mass"], state["h"], state["rho"], state["e"]], axis=1)
+    out.extend(f"{i + 1:8d}" + "".join(fmt_e(c, 20, 13) for c in cols[i]) + "\n" for i in range(x.shape[0]))
+    return "".join(out)
 
 
 def status_line(timestep: int, ptime: float, dt: float) -> str:

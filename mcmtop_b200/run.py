@@ -105,6 +105,12 @@ class Program:
                 break
         return self.solver.timestep - start
 
+    def finish(self) -> None:
+        """MCM/main.f90: mcm_write_drelax after the loop has terminated."""
+        if self.solver.ended:
+            from .output import DRELAX_FIELDS
+            self.out.drelax(self._state(DRELAX_FIELDS))
+
     def close(self) -> None:
         self.solver.close()
 
@@ -138,6 +144,7 @@ def main(argv=None) -> int:
     try:
         prog.initial()
         n = prog.run(int(args["steps"]) if "steps" in args else None)
+        prog.finish()
         print(f"\n     {n} time steps, time {prog.solver.ptime:.6e}; "
               f"{prog.fused_steps} fused on the device, {prog.sync_steps} with host output checks")
     finally:

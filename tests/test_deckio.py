@@ -393,3 +393,18 @@ def test_vtk_record_layout():
     assert m[-3:] == ["SCALARS PTYPE double 1", "LOOKUP_TABLE default", "    3"]
     assert status_line(100, 1.5e-5, 2.5e-8).splitlines()[1:] == [
         "     Problem status for time-step    100", "     Time: 0.1500E-04     dt: 0.2500E-07"]
+
+
+def test_relaxed_state_layout():
+    from mcmtop_b200.output import drelax_text
+    st = {"x": np.array([[0.5, -1.25e-3, 3.0]]), "dispbc": np.array([7]), "mat": np.array([2]),
+          "mass": np.array([1e-3]), "h": np.array([0.052]), "rho": np.array([8.93]), "e": np.array([12.5])}
+    t = drelax_text(st).splitlines()
+    assert t[:3] == ["*", "* Node Coordinates and Materials", "*"]
+    assert t[3] == "       1    7 0.5000000000000E+00-0.1250000000000E-02 0.3000000000000E+01      2"
+    assert len(t[3]) == 80
+    assert t[7] == "       1 0.1000000000000E-02 0.5200000000000E-01 0.8930000000000E+01 0.1250000000000E+02"
+    # the node card reads back with the deck's node format; the data card is
+    # 88 columns wide, and an 80-column reader loses the energy's exponent
+    assert read_record(t[3], "(i8,i5,3e20.0,i7)") == [1, 7, 0.5, -1.25e-3, 3.0, 2]
+    assert read_record(t[7], "(i8,4e20.0)")[4] == 0.125
