@@ -92,7 +92,9 @@ typedef struct {
     int ndim;                  /* 3 (1-D and 2-D return MCM_EUNSUPPORTED) */
     int disctype;              /* 0 basic SPH, 1 Bonet mixed-corrected SPH */
     int tcrit_opt;             /* 0 DYNA formula, 1 h/(c+|v|), 2 mindist/(c+|v|) */
-    int contacttype;           /* must be 0 (kernel contact) */
+    int contacttype;           /* 0: kernel contact (other materials are neighbours); > 0: they are not.
+                                  The reference's repulsive force (MCM/mcm_rep_contact.f90) has no call
+                                  site, so no contact force is added either way. */
     int h_opt;                 /* smoothing length: 0 constant, 1 from the volumetric strain rate,
                                   2 from the density (MCM/mcm_update_h.f90) */
     int veloc_opt;             /* 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87) */

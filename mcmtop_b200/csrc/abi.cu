@@ -42,6 +42,7 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.tssf = c.tssf;
     p.hmax = c.hmax;
     p.h_opt = c.h_opt;
+    p.contacttype = c.contacttype;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;
@@ -504,7 +505,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     if (!cfg || !mats || !out || np <= 0 || nmat <= 0 || nmat > MCM_GPU_MAX_MATERIALS) return MCM_EINVAL;
     *out = nullptr;
     if (cfg->ndim != 3) return MCM_EUNSUPPORTED;
-    if (cfg->contacttype != 0) return MCM_EUNSUPPORTED;
+    if (cfg->contacttype < 0) return MCM_EINVAL;
     if (cfg->h_opt < 0 || cfg->h_opt > 2 || cfg->veloc_opt < 0 || cfg->veloc_opt > 1) return MCM_EINVAL;
     if (cfg->krtype != 0 && cfg->krtype != 1) return MCM_EUNSUPPORTED;
     if (cfg->disctype != 0 && cfg->disctype != 1) return MCM_EINVAL;

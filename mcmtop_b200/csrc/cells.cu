@@ -540,7 +540,9 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         const float reach2 = reach * reach * 1.0009765625f + 9.765625e-4f * csm * csm;
         const int mati = a.cmat[t];
         unsigned *out = a.nidx + (size_t)t * cap;
-        const int passes = a.nmat > 1 ? 2 : 1;
+        // MCM/mcm_ll_neighbours.f90:238-267: other materials' particles are
+        // appended after the own material's only with kernel contact
+        const int passes = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
                 const float qz = ui.z + (float)(bz - nz) * cs[2];
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                               (lo1 == 1 && pl.code[0][1]) || (hi1 == g.gridlim[1] && pl.code[1][1]) ||
                               (lo2 == 1 && pl.code[0][2]) || (hi2 == g.gridlim[2] && pl.code[1][2]);
             if (near) {
-                const int gpasses = a.nmat > 1 ? 2 : 1;
+                const int gpasses = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
                 for (int pass = 0; pass < gpasses; ++pass) {
                     for (int nz = lo2; nz <= hi2; ++nz)
                         for (int my = lo1; my <= hi1; ++my)

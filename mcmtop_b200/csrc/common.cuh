@@ -65,7 +65,7 @@ struct DevParams {
     int asym;         // a material of the cap model is present: the momentum sum reads both triangles of sigma
     int h_opt;        // variable smoothing length (MCM/mcm_update_h.f90): 0 fixed, 1 strain rate, 2 density
     int veloc_opt;    // 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87)
-    int pad_;
+    int contacttype;  // 0: particles of other materials are neighbours (kernel contact); > 0: they are not
     double drelax_scale, tssf, hmax;
     double base_a[3];
     DevPlanes planes;

@@ -299,7 +299,7 @@ int Sim::setup(const mcmo_deck *d, const mcmo_material *m, const double *x, cons
     contacttype = d->contacttype; tcrit_opt = d->tcrit_opt; veloc_opt = d->veloc_opt;
     h_opt = d->h_opt; krtype = d->krtype; maxnbr = d->maxnbr;
     for (int k = 0; k < 3; ++k) nthp[k] = d->nthp[k];
-    if (contacttype != 0 || h_opt < 0 || h_opt > 2 || veloc_opt < 0 || veloc_opt > 1) return MCMO_EUNSUPPORTED;
+    if (contacttype < 0 || h_opt < 0 || h_opt > 2 || veloc_opt < 0 || veloc_opt > 1) return MCMO_EUNSUPPORTED;
     // MCM/mcm_control_v2.f90:193-243
     if (tssf == 0.0) tssf = 0.8;
     if (krtype == 0) krtype = 1;
@@ -2155,7 +2155,9 @@ void Sim::get_j_moment_info(int i, int k, real *x, real &mass, real &rho, real &
     }
 }
 
-// MCM/mcm_oldacceleration.f90:36-90 (contacttype 0)
+// MCM/mcm_oldacceleration.f90:36-90.  With contacttype > 0 the reference adds
+// par%repulsion (:44-56), which stays 0: mcm_rep_cont (MCM/mcm_rep_contact.f90)
+// has no call site, so the sum is the same.
 void Sim::oldacceleration() {
     for (int i = 1; i <= nummat; ++i) { mat[i].xcf = 0.0; mat[i].ycf = 0.0; mat[i].zcf = 0.0; }
 #ifdef _OPENMP
