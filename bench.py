@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--oracle-check-steps", type=int, default=50,
                     help="oracle steps on the full bar for the GPU accuracy spot check")
     ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
+    ap.add_argument("--search-kind", type=int, default=0, choices=[0, 1, 2],
+                    help="neighbour search: 1 one thread per particle, 2 one warp per particle (0: default)")
     return ap.parse_args()
 
 
@@ -409,6 +411,8 @@ def gpu_arm(args):
     workload = f"taylor_bar_{deck.np}"
     sol = Solver(deck, prec, device=local, reorder_interval=args.reorder)
     sol.set_diagnostics(False)
+    if args.search_kind:
+        sol.set_tuning(search_kind=args.search_kind)
     sol.run(args.warmup)
     stats = sol.stats()
     kbar = stats["mean_nbr"]

@@ -260,6 +260,7 @@ typedef struct {
     int pair_blocks_per_sm;  /* blocks per SM the gathers' persistent grid is sized for: 1..16 */
     int nbr_stride;          /* neighbour-table row width in entries (rounded up to 4; still regrown
                                 when a list outgrows it) */
+    int search_kind;         /* 1: one thread per particle (the default), 2: one warp per particle */
     double ms_per_step;      /* mcm_gpu_autotune: device time per loop iteration of the chosen shape */
 } mcm_gpu_tuning;
 

@@ -47,10 +47,13 @@ void enqueue_iteration(mcm_gpu_handle *h) {
 
 // ------------------------------------------------------------------ tuning
 struct Shape {
-    int search, pair, bps, stride;
+    int search, pair, bps, stride, kind;
 };
 
+int search_kind_of(const mcm_gpu_handle *h) { return h->A.search_kind == 2 ? 2 : 1; }
+
 void apply_shape(mcm_gpu_handle *h, const Shape &s) {
+    h->A.search_kind = s.kind;
     h->A.search_threads = s.search;
     h->A.pair_threads = s.pair;
     h->A.pair_bps = s.bps;
@@ -205,9 +208,11 @@ int mcm_gpu_set_tuning(mcm_gpu_handle *h, const mcm_gpu_tuning *t) {
     if (!h || !t) return MCM_EINVAL;
     if (!valid_block(t->search_threads) || !valid_block(t->pair_threads)) return MCM_EINVAL;
     if (t->pair_blocks_per_sm < 0 || t->pair_blocks_per_sm > 16 || t->nbr_stride < 0) return MCM_EINVAL;
+    if (t->search_kind < 0 || t->search_kind > 2) return MCM_EINVAL;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (t->search_threads) h->A.search_threads = t->search_threads;
+    if (t->search_kind) h->A.search_kind = t->search_kind;
     if (t->pair_threads) h->A.pair_threads = t->pair_threads;
     if (t->pair_blocks_per_sm) h->A.pair_bps = t->pair_blocks_per_sm;
     if (t->nbr_stride && t->nbr_stride != h->A.nstride) {
@@ -223,6 +228,7 @@ int mcm_gpu_get_tuning(mcm_gpu_handle *h, mcm_gpu_tuning *t) {
     t->pair_threads = pair_threads_of(h->A);
     t->pair_blocks_per_sm = h->A.pair_bps > 0 ? h->A.pair_bps : 8;
     t->nbr_stride = h->A.nstride;
+    t->search_kind = search_kind_of(h);
     t->ms_per_step = h->tuned_ms;
     return MCM_OK;
 }
@@ -238,7 +244,7 @@ int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best) {
     if ((st = save_body(h, saved))) { h->cfg.reorder_interval = every; return st; }
     cudaEvent_t e0 = take_event(h), e1 = take_event(h);
     const Shape cur = {search_threads_of(h->A), pair_threads_of(h->A), h->A.pair_bps > 0 ? h->A.pair_bps : 8,
-                       h->A.nstride};
+                       h->A.nstride, search_kind_of(h)};
     auto timed = [&](const Shape &s, double *ms) -> int {
         int r;
         apply_shape(h, s);
@@ -267,11 +273,19 @@ int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best) {
         for (int pb : blocks)
             for (int g : bpss) {
                 if (sb == 64 && pb != 64) continue;   // narrow searches only with narrow gathers
-                const Shape s = {sb, pb, g, cur.stride};
+                const Shape s = {sb, pb, g, cur.stride, cur.kind};
                 double ms = 0.0;
                 if ((st = timed(s, &ms))) goto out;
                 if (ms < bestMs) { bestMs = ms; bestS = s; }
             }
+    // the other search kind with the best block sizes
+    {
+        Shape s = bestS;
+        s.kind = (cur.kind == 1) ? 2 : 1;
+        double ms = 0.0;
+        if ((st = timed(s, &ms))) goto out;
+        if (ms < bestMs) { bestMs = ms; bestS = s; }
+    }
     // stage 2: neighbour-table stride, tight or rounded to 64-byte rows
     {
         const int need = std::max(h->h_status->max_nbr, 1);

@@ -66,6 +66,7 @@ struct StepArgs {
     int red_blocks;   // capacity of red in blocks (partial vectors)
     // launch shape, chosen by mcm_gpu_set_tuning or mcm_gpu_autotune (0: default)
     int search_threads;   // threads per block of the neighbour search
+    int search_kind;      // 0 or 1: one thread per particle (k_search); 2: one warp per particle (k_search_warp)
     int pair_threads;     // threads per block of the cooperative strain and momentum gathers
     int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for
     double *energy;   // 5*nmat + 3

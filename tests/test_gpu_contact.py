@@ -61,3 +61,27 @@ def test_separate_materials_do_not_interact(gpu_lib):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("contacttype", [0, 1])
+def test_search_kinds_build_the_same_lists(contacttype, gpu_lib):
+    # one thread per particle and one warp per particle: same lists, same order,
+    # same ghosts and minimum distances (FP64 exact path, two materials, a plane)
+    deck = two_material_bar(contacttype).replace(tcrit_opt=2)
+    a, b = Solver(deck, _abi.PREC_FP64_EXACT), Solver(deck, _abi.PREC_FP64_EXACT)
+    try:
+        a.set_tuning(search_kind=1)
+        b.set_tuning(search_kind=2)
+        assert a.tuning()["search_kind"] == 1 and b.tuning()["search_kind"] == 2
+        for _ in range(5):
+            a.step()
+            b.step()
+            la, lb = a.neighbours(), b.neighbours()
+            for u, v in zip(la, lb):
+                assert np.array_equal(u, v)
+        sa, sb = a.download(STATE + ["mindist"]), b.download(STATE + ["mindist"])
+        for f in sa:
+            assert np.array_equal(sa[f], sb[f]), f
+    finally:
+        a.close()
+        b.close()
