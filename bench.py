@@ -518,17 +518,22 @@ def gpu_arm(args):
         k_e2e = args.steps
         t0 = time.perf_counter()
         sol.upload(pinned, bbox)
+        t1 = time.perf_counter()
         for _ in range(k_e2e):
             sol.step()
+        t2 = time.perf_counter()
         out = sol.download(["x", "v", "rho", "e", "p", "sigma", "efps"])
         el = time.perf_counter() - t0
+        split_ms = {"upload": round((t1 - t0) * 1e3, 2), "steps": round((t2 - t1) * 1e3, 2),
+                    "download": round((time.perf_counter() - t2) * 1e3, 2)}
         d2h_bytes = sum(a.nbytes for a in out.values())
         per_step_h2d = 24
-        per_step_d2h = 3 * 96 + 8 * (5 * sol.nmat + 3) + 48
+        per_step_d2h = 2 * 96 + 8 * (5 * sol.nmat + 3)   # status + time at step_a and step_b, energies
         e2e = {"value": round(deck.np * k_e2e / el, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d_bytes / k_e2e + per_step_h2d),
                "d2h_bytes_per_step": int(d2h_bytes / k_e2e + per_step_d2h),
-               "steps": k_e2e, "path": "mcm_gpu_upload + (step_a, host dt, step_b, step_c) x K + mcm_gpu_download"}
+               "steps": k_e2e, "wall_ms": split_ms,
+               "path": "mcm_gpu_upload + (step_a -> critts, host dt, step_b -> energies, step_c) x K + mcm_gpu_download"}
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:

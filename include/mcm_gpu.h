@@ -173,7 +173,11 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f);
 
 int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts);
 /* energies: per material ke, ie, mom(3) -> 5*nmat doubles (mcm_mat%ke, %ie, %mom),
- * then kinetice, internale, totale.  May be NULL. */
+ * then kinetice, internale, totale.  May be NULL.
+ * step_b with energies NULL and step_c with coord_maxmin NULL (the next grid
+ * reads the box on the device) only enqueue their work and return without
+ * waiting; a device error they meet is returned by the next call that waits
+ * (step_a, or step_b/step_c with an output, download). */
 int mcm_gpu_step_b(mcm_gpu_handle *h, double *energies);
 int mcm_gpu_step_c(mcm_gpu_handle *h, double dt, double dtold, double *coord_maxmin);
 

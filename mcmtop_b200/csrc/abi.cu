@@ -898,13 +898,12 @@ int mcm_gpu_step_b(mcm_gpu_handle *h, double *energies) {
     h->A.split_mode = 1;
     if ((st = reset_status(h))) return st;
     enqueue_part_b(h, 0);
-    if (energies) {
-        CK(cudaMemcpyAsync(h->h_energy, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost,
-                           h->stream));
-    }
+    if (!energies) return MCM_OK;   // nothing to wait for: errors surface at the next waiting call
+    CK(cudaMemcpyAsync(h->h_energy, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost,
+                       h->stream));
     if ((st = sync_status(h))) return st;
     if (h->h_status->code) return set_error(h, h->h_status->code, "step_b");
-    if (energies) std::memcpy(energies, h->h_energy, sizeof(double) * (5 * h->nmat + 3));
+    std::memcpy(energies, h->h_energy, sizeof(double) * (5 * h->nmat + 3));
     return MCM_OK;
 }
 
@@ -922,11 +921,11 @@ int mcm_gpu_step_c(mcm_gpu_handle *h, double dt, double dtold, double *coord_max
         Scope sc(h, R_REDUCE, 1);
         launch_energy_bbox_reduce(h->A, h->stream, nb, 0, 1);
     }
+    if (!coord_maxmin) return MCM_OK;   // the next grid reads the box on the device
     CK(cudaMemcpyAsync(h->h_bbox, h->A.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream));
     if ((st = sync_status(h))) return st;
     if (h->h_status->code) return set_error(h, h->h_status->code, "step_c");
-    if (coord_maxmin)
-        for (int d = 0; d < 3; ++d) { coord_maxmin[2 * d] = h->h_bbox[d]; coord_maxmin[2 * d + 1] = h->h_bbox[3 + d]; }
+    for (int d = 0; d < 3; ++d) { coord_maxmin[2 * d] = h->h_bbox[d]; coord_maxmin[2 * d + 1] = h->h_bbox[3 + d]; }
     return MCM_OK;
 }
 

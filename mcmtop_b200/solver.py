@@ -139,8 +139,11 @@ class Solver:
         check(self.lib.mcm_gpu_energies(self.h, _dptr(e)), "mcm_gpu_energies", self.h)
         return e
 
-    def step_c(self) -> None:
-        check(self.lib.mcm_gpu_step_c(self.h, self.dt, self.dtold, _dptr(self.bbox)), "mcm_gpu_step_c", self.h)
+    def step_c(self, bbox: bool = False) -> None:
+        """Velocity and position update; bbox=True also reads mcm_coord_maxmin
+        into self.bbox (a wait), otherwise the call returns without waiting."""
+        check(self.lib.mcm_gpu_step_c(self.h, self.dt, self.dtold, _dptr(self.bbox) if bbox else None),
+              "mcm_gpu_step_c", self.h)
         self.timestep += 1
 
     def step(self) -> bool:

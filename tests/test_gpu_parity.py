@@ -103,9 +103,13 @@ def test_one_step(lib, disctype):
     orc.step_b()
     assert relerr(sol.energies, orc.energies()) < 1e-13
     compare(sol, orc, ["a"], 1e-12, "acceleration")
-    sol.step_c()
+    sol.step_c(bbox=True)
     orc.step_c()
     compare(sol, orc, STATE, 1e-13, "after step_c")
+    # mcm_coord_maxmin of MCM/mcm_move.f90:26-39 (before the plane checks)
+    x = orc.get("x")
+    assert np.allclose(sol.bbox[0::2], x.min(axis=0), rtol=0, atol=1e-9)
+    assert np.allclose(sol.bbox[1::2], x.max(axis=0), rtol=0, atol=1e-9)
 
 
 @pytest.mark.parametrize("disctype", [0, 1])
