@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 if (!(d2 < __dmul_rn(hs, hs))) continue;
                             }
-                            if ((a.cmat[p] == mati) != (pass == 0)) continue;
+                            if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) continue;
                             if (want_mind) mind = fmin(mind, d2);
                             if (nn < cap) out[nn] = (unsigned)p | code;
                             ++nn;
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                     const double d2 = exact_d2(xi, c);
                                     const double hs = __dadd_rn(c.w, xi.w);
                                     if (d2 < __dmul_rn(hs, hs)) {
-                                        if ((a.gmat[q] == mati) != (pass == 0)) continue;
+                                        if (a.nmat > 1 && (a.gmat[q] == mati) != (pass == 0)) continue;
                                         mind = fmin(mind, d2);
                                         if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
                                         ++gn;
@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 acc = d2 < __dmul_rn(hs, hs);
                             }
-                            if (acc) acc = ((a.cmat[p] == mati) == (pass == 0));
+                            if (acc && a.nmat > 1) acc = ((a.cmat[p] == mati) == (pass == 0));
                         }
                         const unsigned bal = __ballot_sync(0xffffffffu, acc);
                         if (acc) {
@@ -753,7 +753,8 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                         const double4 c = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
                                         d2 = exact_d2(xi, c);
                                         const double hs = __dadd_rn(c.w, xi.w);
-                                        acc = (d2 < __dmul_rn(hs, hs)) && ((a.gmat[q] == mati) == (pass == 0));
+                                        acc = (d2 < __dmul_rn(hs, hs)) &&
+                                              (a.nmat == 1 || (a.gmat[q] == mati) == (pass == 0));
                                     }
                                     const unsigned bal = __ballot_sync(0xffffffffu, acc);
                                     if (acc) {
