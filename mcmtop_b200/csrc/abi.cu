@@ -38,7 +38,6 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.drelax = c.drelax;
     p.nmat = nmat;
     p.diag = 1;
-    p.subcells = (c.precision != MCM_PREC_FP64_EXACT) ? 1 : 0;
     p.drelax_scale = c.drelax_scale;
     p.tssf = c.tssf;
     p.hmax = c.hmax;
@@ -89,7 +88,6 @@ int alloc_particles(mcm_gpu_handle *h) {
     h->A.F.orig = h->d_ints + 2 * np;
     h->A.F.ptype = h->d_ints + 3 * np;
     if ((st = dalloc(h, &h->A.key, np))) return st;
-    if ((st = dalloc(h, &h->A.oct, np))) return st;
     if ((st = dalloc(h, &h->A.cell_list, np))) return st;
     if ((st = dalloc(h, &h->A.cpos, np))) return st;
     if ((st = dalloc(h, &h->A.cposf, np))) return st;
@@ -126,7 +124,6 @@ int alloc_cells(mcm_gpu_handle *h, long long cap) {
     long long nsum = (cap + 4095) / 4096 + 2;
     if ((st = dalloc(h, &h->A.scan_sums, (size_t)nsum))) return st;
     if ((st = dalloc(h, &h->A.gcell, (size_t)cap))) return st;
-    if ((st = dalloc(h, &h->A.csub, (size_t)cap))) return st;
     h->A.layer_cap = (int)std::min<long long>(cap, 1LL << 30);
     if ((st = dalloc(h, &h->A.layer_count, (size_t)h->A.layer_cap))) return st;
     if ((st = dalloc(h, &h->A.layer_off, (size_t)h->A.layer_cap))) return st;

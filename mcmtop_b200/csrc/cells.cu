@@ -106,14 +106,6 @@ __global__ void k_cell_keys(StepArgs a) {
         int key = in ? (int)cell_key(box[0], box[1], box[2], g.gridlim) : kNoCell;
         a.key[i] = key;
         if (key >= 0) atomicAdd(&a.cell_count[key], 1);
-        if (a.prm.subcells) {
-            // octant: bit d set when the particle lies in the upper half of its cell along axis d
-            unsigned o = 0;
-            if (key >= 0)
-                for (int j = 0; j < ndim; ++j)
-                    if (X[j][i] - cell_origin(g, j, box[j]) >= 0.5 / g.gridsize[j]) o |= 1u << j;
-            a.oct[i] = (unsigned char)o;
-        }
     }
 }
 
@@ -266,41 +258,23 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
 }
 
 // Per-cell order: descending reference index (head insertion in
-// MCM/mcm_setuplist.f90:336-340 over i = 1..np ascending).  With subcells
-// the octant comes first (then descending reference index) and the octants'
-// first positions are recorded for the search.
-__device__ __forceinline__ bool cell_before(const StepArgs &a, int u, int v, bool sub) {
-    if (sub && a.oct[u] != a.oct[v]) return a.oct[u] < a.oct[v];
-    return a.F.orig[u] > a.F.orig[v];
-}
-
+// MCM/mcm_setuplist.f90:336-340 over i = 1..np ascending).
 __global__ void k_cell_sort(StepArgs a) {
     if (a.status->code) return;
     const long long ncells = a.grid->ncells;
-    const bool sub = a.prm.subcells != 0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
          c += (long long)gridDim.x * blockDim.x) {
         int s = a.cell_start[c], e = a.cell_start[c + 1];
+        if (e - s < 2) continue;
         for (int k = s + 1; k < e; ++k) {
             int v = a.cell_list[k];
+            int ov = a.F.orig[v];
             int m = k - 1;
-            while (m >= s && cell_before(a, v, a.cell_list[m], sub)) {
+            while (m >= s && a.F.orig[a.cell_list[m]] < ov) {
                 a.cell_list[m + 1] = a.cell_list[m];
                 --m;
             }
             a.cell_list[m + 1] = v;
-        }
-        if (sub) {
-            unsigned long long packed = ~0ull;
-            if (e - s < 256) {
-                packed = 0ull;
-                int k = s;
-                for (int o = 1; o < 8; ++o) {
-                    while (k < e && a.oct[a.cell_list[k]] < o) ++k;
-                    packed |= (unsigned long long)(k - s) << (8 * (o - 1));
-                }
-            }
-            a.csub[c] = make_uint2((unsigned)packed, (unsigned)(packed >> 32));
         }
     }
 }
@@ -535,17 +509,6 @@ __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
     return s;
 }
 
-// Distances from a coordinate q (in a cell's frame, cell edge w) to the
-// cell's lower half [0, w/2] and upper half [w/2, w].
-__device__ __forceinline__ void half_gaps(float q, float w, float g[2]) {
-    const float h = 0.5f * w;
-    g[0] = fmaxf(fmaxf(-q, q - h), 0.0f);
-    g[1] = fmaxf(fmaxf(h - q, q - w), 0.0f);
-}
-
-// Cells with fewer particles are scanned whole even with subcells.
-constexpr int kSubMin = 8;
-
 __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     if (a.status->code) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -594,56 +557,31 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     for (int lx = lo0; lx <= hi0; ++lx) {
                         const float gx = fmaxf(lx < bx ? ui.x : (lx > bx ? cs[0] - ui.x : 0.0f), 0.0f);
                         if (gyz + gx * gx > reach2) continue;
-                        const int kc = k0 + (lx - lo0);
-                        const int cb = a.cell_start[kc], ce = a.cell_start[kc + 1];
+                        const int cb = a.cell_start[k0 + (lx - lo0)], ce = a.cell_start[k0 + (lx - lo0) + 1];
                         // this particle relative to the origin of candidate cell lx
                         const float qx = ui.x + (float)(bx - lx) * cs[0];
                         const unsigned code = (code_yz + (unsigned)(lx - bx + 1)) << 26;
-                        auto candidates = [&](int pb, int pe) {
-                            for (int p = pb; p < pe; ++p) {
-                                const float4 c = a.cposf[p];
-                                const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
-                                const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                                const float hsf = ui.w + c.w;
-                                const float r2f = hsf * hsf;
-                                if (d2f >= fmaf(r2f, khi, kb)) continue;
-                                if (p == t) continue;
-                                double d2 = 0.0;
-                                if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
-                                    // near tie (or mindist wanted): the reference's FP64 test
-                                    const double4 cd = a.cpos[p];
-                                    d2 = exact_d2(xi, cd);
-                                    const double hs = __dadd_rn(cd.w, xi.w);
-                                    if (!(d2 < __dmul_rn(hs, hs))) continue;
-                                }
-                                if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) continue;
-                                if (want_mind) mind = fmin(mind, d2);
-                                if (nn < cap) out[nn] = (unsigned)p | code;
-                                ++nn;
+                        for (int p = cb; p < ce; ++p) {
+                            const float4 c = a.cposf[p];
+                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                            const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float hsf = ui.w + c.w;
+                            const float r2f = hsf * hsf;
+                            if (d2f >= fmaf(r2f, khi, kb)) continue;
+                            if (p == t) continue;
+                            double d2 = 0.0;
+                            if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
+                                // near tie (or mindist wanted): the reference's FP64 test
+                                const double4 cd = a.cpos[p];
+                                d2 = exact_d2(xi, cd);
+                                const double hs = __dadd_rn(cd.w, xi.w);
+                                if (!(d2 < __dmul_rn(hs, hs))) continue;
                             }
-                        };
-                        if (a.prm.subcells && ce - cb >= kSubMin) {
-                            const uint2 so = a.csub[kc];
-                            if (so.x != 0xffffffffu || so.y != 0xffffffffu) {
-                                // distances from this particle to the lower and upper half of the
-                                // candidate cell along each axis (the cell frame of qx, qy, qz)
-                                float hx[2], hy[2], hz[2];
-                                half_gaps(qx, cs[0], hx);
-                                half_gaps(qy, cs[1], hy);
-                                half_gaps(qz, cs[2], hz);
-                                const unsigned long long packed =
-                                    (unsigned long long)so.x | ((unsigned long long)so.y << 32);
-                                int ob = cb;
-                                for (int o = 0; o < 8; ++o) {
-                                    const int oe = (o < 7) ? cb + (int)((packed >> (8 * o)) & 0xffu) : ce;
-                                    const float gx2 = hx[o & 1], gy2 = hy[(o >> 1) & 1], gz2 = hz[o >> 2];
-                                    if (oe > ob && gx2 * gx2 + gy2 * gy2 + gz2 * gz2 <= reach2) candidates(ob, oe);
-                                    ob = oe;
-                                }
-                                continue;
-                            }
+                            if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) continue;
+                            if (want_mind) mind = fmin(mind, d2);
+                            if (nn < cap) out[nn] = (unsigned)p | code;
+                            ++nn;
                         }
-                        candidates(cb, ce);
                     }
                 }
             }

@@ -66,9 +66,6 @@ struct DevParams {
     int h_opt;        // variable smoothing length (MCM/mcm_update_h.f90): 0 fixed, 1 strain rate, 2 density
     int veloc_opt;    // 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87)
     int contacttype;  // 0: particles of other materials are neighbours (kernel contact); > 0: they are not
-    int subcells;     // 1: each cell ordered by octant, the search skips octants beyond reach (lists in
-                      //    another order than the reference's: the FP64-fast and mixed steps)
-    int pad_;
     double drelax_scale, tssf, hmax;
     double base_a[3];
     DevPlanes planes;

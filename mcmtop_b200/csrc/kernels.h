@@ -28,11 +28,8 @@ struct StepArgs {
     // key order, each cell in descending reference index, particles outside
     // the grid last); cell_list[p] is its state index.
     int *key;         // per state index: cell key or -1
-    unsigned char *oct;   // per state index: octant of the particle in its cell (subcells)
     int *cell_count;  // cell_cap
     int *cell_start;  // cell_cap + 1
-    uint2 *csub;      // per cell (subcells): first position of octants 1..7 relative to the cell's
-                      // start, one byte each; all bytes 0xff for a cell of 256 or more particles
     int *cell_list;   // npad: position -> state index
     int *n_inside;    // particles inside the grid (device counter)
     double4 *cpos;    // per position: x, y, z, h at neighbour time

@@ -42,10 +42,6 @@ def compare(sol, orc, fields, tol, label=""):
 
 
 def compare_neighbours(sol, orc):
-    """The FP64-exact step keeps the reference's neighbour sequences; the
-    FP64-fast and mixed steps order each cell by octant, so their lists hold
-    the reference's sets in another order."""
-    ordered = sol.cfg.precision == _abi.PREC_FP64_EXACT
     nn, nbr, gn, gnbr = sol.neighbours()
     onn = orc.get_int("nnbr")
     ogn = orc.get_int("g_nnbr")
@@ -53,28 +49,10 @@ def compare_neighbours(sol, orc):
     assert np.array_equal(gn, ogn), "ghost neighbour counts differ"
     for i in range(sol.n):
         ref = orc.nbrlist(i + 1)
-        got = nbr[i, : nn[i]]
-        if ordered:
-            assert np.array_equal(got, ref), f"neighbour sequence of particle {i + 1} differs"
-        else:
-            assert np.array_equal(np.sort(got), np.sort(ref)), f"neighbour set of particle {i + 1} differs"
-    if not ordered and gn.any():
-        # ghosts are numbered in creation order, which follows the cell order:
-        # compare them by parent and by the axes along which they are mirrored
-        gp, gx, _ = sol.ghosts()
-        ogp, ogx, _ = orc.ghosts()
-        px, opx = sol.download(["x"])["x"], orc.get("x")
-        gkey = [(int(gp[q]), *np.sign(gx[q] - px[gp[q] - 1]).astype(int)) for q in range(len(gp))]
-        ogkey = [(int(ogp[q]), *np.sign(ogx[q] - opx[ogp[q] - 1]).astype(int)) for q in range(len(ogp))]
-    for i in range(sol.n):
+        assert np.array_equal(nbr[i, : nn[i]], ref), f"neighbour sequence of particle {i + 1} differs"
         if gn[i]:
             gref = orc.g_nbrlist(i + 1)
-            gg = gnbr[i, : gn[i]]
-            if ordered:
-                assert np.array_equal(gg, gref), f"ghost sequence of particle {i + 1} differs"
-            else:
-                assert sorted(gkey[q - 1] for q in gg) == sorted(ogkey[q - 1] for q in gref), \
-                    f"ghost set of particle {i + 1} differs"
+            assert np.array_equal(gnbr[i, : gn[i]], gref), f"ghost sequence of particle {i + 1} differs"
 
 
 def small_bar(**kw):
