@@ -507,17 +507,20 @@ def gpu_arm(args):
         names = ["x", "v", "mass", "h", "hold", "rho", "e", "p", "c", "vabs", "efps", "pcut", "fail", "sigma", "q",
                  "mat", "dispbc"]
         host = sol.download(names)
+        # the host buffers a Fortran driver holds: pinned, in the ABI's layout
+        # ((3,np) vectors, (3,3,np) column-major tensors), filled before the clock starts
         pinned = {}
         for k, a in host.items():
-            t = torch.empty(a.shape, dtype=torch.from_numpy(np.ascontiguousarray(a[:1])).dtype, pin_memory=True)
+            src = np.ascontiguousarray(a.transpose(0, 2, 1) if a.ndim == 3 else a)
+            t = torch.empty(src.shape, dtype=torch.from_numpy(src[:1].copy()).dtype, pin_memory=True)
             arr = t.numpy()
-            arr[...] = a
+            arr[...] = src
             pinned[k] = arr
         bbox = np.array([host["x"][:, d].min() if j == 0 else host["x"][:, d].max() for d in range(3) for j in range(2)])
         h2d_bytes = sum(a.nbytes for a in pinned.values())
         k_e2e = args.steps
         t0 = time.perf_counter()
-        sol.upload(pinned, bbox)
+        sol.upload(pinned, bbox, fortran_layout=True)
         t1 = time.perf_counter()
         for _ in range(k_e2e):
             sol.step()

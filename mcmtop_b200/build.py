@@ -32,6 +32,7 @@ UNITS = [
     ("noalloc.cu", False),
     ("adjoint.cu", False),
     ("batch.cu", False),
+    ("transfer.cu", False),
 ]
 HEADERS = ["common.cuh", "kernels.h", "handle.h", "physics.cuh", "step_fp64.cuh", "step_coop.cuh", "nbr_iter.cuh", "dual.cuh"]
 

@@ -319,39 +319,85 @@ int check_handle(mcm_gpu_handle *h) {
 
 // ------------------------------------------------------------- transfers
 // Fortran (3,np) vector -> three device arrays
-int put_vec3(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
-    const int n = h->np;
-    for (int k = 0; k < 3; ++k) {
-        for (int i = 0; i < n; ++i) tmp[i] = src[3 * (size_t)i + k];
-        CK(cudaMemcpy(h->A.F.f[f0 + k], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    }
-    return MCM_OK;
+// Host arrays cross PCIe as one contiguous copy each, into a device staging
+// buffer (9 doubles per particle, allocated on first use), and kernels
+// convert between the Fortran record layout and the per-field arrays.
+PackSpec spec_none(int width) {
+    PackSpec s;
+    s.width = width;
+    for (int k = 0; k < 9; ++k) { s.field[k] = -1; s.sign[k] = 1.0; }
+    return s;
 }
-
-// Fortran (3,3,np) symmetric tensor -> six device arrays (11 22 33 12 13 23)
-int put_sym(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
-    static const int rc[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
-    const int n = h->np;
+// Fortran (3,np) vector
+PackSpec spec_vec3(int f0) {
+    PackSpec s = spec_none(3);
+    for (int k = 0; k < 3; ++k) s.field[k] = f0 + k;
+    return s;
+}
+// entry (r, c) of a Fortran (3,3) record is r + 3c; a symmetric tensor keeps
+// 11 22 33 12 13 23 in fields f0..f0+5
+constexpr int kSymIdx[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+PackSpec spec_sym(int f0, bool both) {
+    PackSpec s = spec_none(9);
     for (int t = 0; t < 6; ++t) {
-        for (int i = 0; i < n; ++i) tmp[i] = src[9 * (size_t)i + rc[t][0] + 3 * rc[t][1]];
-        CK(cudaMemcpy(h->A.F.f[f0 + t], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        s.field[kSymIdx[t][0] + 3 * kSymIdx[t][1]] = f0 + t;
+        if (both) s.field[kSymIdx[t][1] + 3 * kSymIdx[t][0]] = f0 + t;
     }
+    return s;
+}
+// sigma: upper triangle from 11..23, lower triangle (21, 31, 32) from its own fields
+PackSpec spec_sigma() {
+    PackSpec s = spec_sym(FS11, false);
+    s.field[1] = FL21; s.field[2] = FL31; s.field[5] = FL32;
+    return s;
+}
+PackSpec spec_spin() {
+    PackSpec s = spec_none(9);
+    const int fl[3] = {FW12, FW13, FW23};
+    const int rc[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    for (int t = 0; t < 3; ++t) {
+        s.field[rc[t][0] + 3 * rc[t][1]] = fl[t];
+        s.field[rc[t][1] + 3 * rc[t][0]] = fl[t];
+        s.sign[rc[t][1] + 3 * rc[t][0]] = -1.0;
+    }
+    return s;
+}
+PackSpec spec_iso(int f, bool full) {   // q: the isotropic value on the diagonal
+    PackSpec s = spec_none(9);
+    s.field[0] = f;
+    if (full) { s.field[4] = f; s.field[8] = f; }
+    return s;
+}
+
+int stage_ready(mcm_gpu_handle *h) {
+    if (h->d_stage) return MCM_OK;
+    return dalloc(h, &h->d_stage, 9 * (size_t)h->npad);
+}
+
+int put_rec(mcm_gpu_handle *h, const double *src, const PackSpec &s) {
+    int st;
+    if ((st = stage_ready(h))) return st;
+    CK(cudaMemcpyAsync(h->d_stage, src, sizeof(double) * s.width * (size_t)h->np, cudaMemcpyHostToDevice,
+                       h->stream));
+    launch_unpack(h->A, s, h->d_stage, h->stream);
+    CK(cudaGetLastError());
     return MCM_OK;
 }
 
-// the lower triangle (2,1), (3,1), (3,2) of a Fortran (3,3,np) tensor
-int put_lower(mcm_gpu_handle *h, const double *src, int f0, std::vector<double> &tmp) {
-    static const int rc[3][2] = {{1, 0}, {2, 0}, {2, 1}};
-    const int n = h->np;
-    for (int t = 0; t < 3; ++t) {
-        for (int i = 0; i < n; ++i) tmp[i] = src[9 * (size_t)i + rc[t][0] + 3 * rc[t][1]];
-        CK(cudaMemcpy(h->A.F.f[f0 + t], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    }
+int get_rec(mcm_gpu_handle *h, double *dst, const PackSpec &s) {
+    int st;
+    if ((st = stage_ready(h))) return st;
+    launch_pack(h->A, s, h->d_stage, h->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, h->d_stage, sizeof(double) * s.width * (size_t)h->np, cudaMemcpyDeviceToHost,
+                       h->stream));
     return MCM_OK;
 }
+
+int put_vec3(mcm_gpu_handle *h, const double *src, int f0) { return put_rec(h, src, spec_vec3(f0)); }
 
 int put_scalar(mcm_gpu_handle *h, const double *src, int f) {
-    CK(cudaMemcpy(h->A.F.f[f], src, sizeof(double) * h->np, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->A.F.f[f], src, sizeof(double) * h->np, cudaMemcpyHostToDevice, h->stream));
     return MCM_OK;
 }
 
@@ -602,7 +648,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     if (!h) return MCM_EINVAL;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->d_fields, h->A.frec0, h->A.gfrec1, h->A.gfrec2,
+    void *ptrs[] = {h->d_fields, h->d_stage, h->A.frec0, h->A.gfrec1, h->A.gfrec2,
                     h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
                     h->A.cpos, h->A.cposf, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
@@ -780,11 +826,11 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np;
-    std::vector<double> tmp(n);
     int st;
-    if ((st = put_vec3(h, f->x, FX, tmp))) return st;
-    if (f->v && (st = put_vec3(h, f->v, FVX, tmp))) return st;
-    if (f->a && (st = put_vec3(h, f->a, FAX, tmp))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    if ((st = put_vec3(h, f->x, FX))) return st;
+    if (f->v && (st = put_vec3(h, f->v, FVX))) return st;
+    if (f->a && (st = put_vec3(h, f->a, FAX))) return st;
     struct { const double *p; int f; } sc[] = {
         {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
         {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
@@ -795,15 +841,11 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     if (f->h0 || f->h) {
         if ((st = put_scalar(h, f->h0 ? f->h0 : f->h, FH0))) return st;
     }
-    if (f->sigma && (st = put_sym(h, f->sigma, FS11, tmp))) return st;
-    if (f->sigma && (st = put_lower(h, f->sigma, FL21, tmp))) return st;
-    if (f->s && (st = put_sym(h, f->s, FD11, tmp))) return st;
-    if (f->alfa && (st = put_sym(h, f->alfa, FA11, tmp))) return st;
-    if (f->rod && (st = put_sym(h, f->rod, FR11, tmp))) return st;
-    if (f->q) {
-        for (int i = 0; i < n; ++i) tmp[i] = f->q[9 * (size_t)i];
-        CK(cudaMemcpy(h->A.F.f[FQ], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    }
+    if (f->sigma && (st = put_rec(h, f->sigma, spec_sigma()))) return st;
+    if (f->s && (st = put_rec(h, f->s, spec_sym(FD11, false)))) return st;
+    if (f->alfa && (st = put_rec(h, f->alfa, spec_sym(FA11, false)))) return st;
+    if (f->rod && (st = put_rec(h, f->rod, spec_sym(FR11, false)))) return st;
+    if (f->q && (st = put_rec(h, f->q, spec_iso(FQ, false)))) return st;
     for (int i = 0; i < n; ++i)
         if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
     CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
@@ -820,8 +862,8 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
     const int n = h->np;
     std::vector<double> tmp(n);
     int st;
-    if ((st = put_vec3(h, f->x, FX, tmp))) return st;
-    if (f->v) { if ((st = put_vec3(h, f->v, FVX, tmp))) return st; }
+    if ((st = put_vec3(h, f->x, FX))) return st;
+    if (f->v) { if ((st = put_vec3(h, f->v, FVX))) return st; }
     else {
         for (int k = 0; k < 3; ++k) CK(cudaMemset(h->A.F.f[FVX + k], 0, sizeof(double) * n));
     }
@@ -984,84 +1026,28 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     const int n = h->np;
     std::vector<int> orig(n);
     CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    std::vector<double> tmp(n);
-    auto get = [&](int fld) -> int {
-        CK(cudaMemcpy(tmp.data(), h->A.F.f[fld], sizeof(double) * n, cudaMemcpyDeviceToHost));
-        return MCM_OK;
-    };
-    auto vec3 = [&](double *dst, int f0) -> int {
-        for (int k = 0; k < 3; ++k) {
-            int s = get(f0 + k); if (s) return s;
-            for (int p = 0; p < n; ++p) dst[3 * (size_t)orig[p] + k] = tmp[p];
-        }
-        return MCM_OK;
-    };
-    auto sym = [&](double *dst, int f0) -> int {
-        static const int rc[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
-        for (int t = 0; t < 6; ++t) {
-            int s = get(f0 + t); if (s) return s;
-            for (int p = 0; p < n; ++p) {
-                size_t b = 9 * (size_t)orig[p];
-                dst[b + rc[t][0] + 3 * rc[t][1]] = tmp[p];
-                dst[b + rc[t][1] + 3 * rc[t][0]] = tmp[p];
-            }
-        }
-        return MCM_OK;
-    };
-    auto scal = [&](double *dst, int fld) -> int {
-        int s = get(fld); if (s) return s;
-        for (int p = 0; p < n; ++p) dst[orig[p]] = tmp[p];
-        return MCM_OK;
-    };
-    if (f->x && (st = vec3(f->x, FX))) return st;
-    if (f->v && (st = vec3(f->v, FVX))) return st;
-    if (f->a && (st = vec3(f->a, FAX))) return st;
+    if (f->x && (st = get_rec(h, f->x, spec_vec3(FX)))) return st;
+    if (f->v && (st = get_rec(h, f->v, spec_vec3(FVX)))) return st;
+    if (f->a && (st = get_rec(h, f->a, spec_vec3(FAX)))) return st;
     struct { double *p; int f; } sc[] = {
         {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
         {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
         {f->fail, FFAIL}, {f->mindist, FMINDIST}, {f->critts, FCRITTS}, {f->tracerod, FTR},
         {f->etry, FETRY}, {f->einc, FEINC}, {f->capa, FCAPA}, {f->h0, FH0}};
-    for (auto &s : sc)
-        if (s.p && (st = scal(s.p, s.f))) return st;
-    if (f->sigma && (st = sym(f->sigma, FS11))) return st;
-    if (f->sigma) {
-        // the lower triangle as stored (it differs from the upper one for the cap model)
-        static const int rc[3][2] = {{1, 0}, {2, 0}, {2, 1}};
-        for (int t = 0; t < 3; ++t) {
-            int s2 = get(FL21 + t); if (s2) return s2;
-            for (int p = 0; p < n; ++p) f->sigma[9 * (size_t)orig[p] + rc[t][0] + 3 * rc[t][1]] = tmp[p];
-        }
+    for (auto &s : sc) {
+        if (!s.p) continue;
+        PackSpec one = spec_none(1);
+        one.field[0] = s.f;
+        if ((st = get_rec(h, s.p, one))) return st;
     }
-    if (f->s && (st = sym(f->s, FD11))) return st;
-    if (f->alfa && (st = sym(f->alfa, FA11))) return st;
-    if (f->rod && (st = sym(f->rod, FR11))) return st;
-    if (f->spin) {
-        // spin(n,m) = -spin(m,n), zero diagonal
-        static const int fl[3] = {FW12, FW13, FW23};
-        static const int rc[3][2] = {{0, 1}, {0, 2}, {1, 2}};
-        for (int p = 0; p < n; ++p)
-            for (int k = 0; k < 9; ++k) f->spin[9 * (size_t)orig[p] + k] = 0.0;
-        for (int t = 0; t < 3; ++t) {
-            if ((st = get(fl[t]))) return st;
-            for (int p = 0; p < n; ++p) {
-                size_t b = 9 * (size_t)orig[p];
-                f->spin[b + rc[t][0] + 3 * rc[t][1]] = tmp[p];
-                f->spin[b + rc[t][1] + 3 * rc[t][0]] = -tmp[p];
-            }
-        }
-    }
-    if (f->q || f->qold) {
-        if ((st = get(FQ))) return st;
-        double *dsts[2] = {f->q, f->qold};
-        for (double *dst : dsts) {
-            if (!dst) continue;
-            for (int p = 0; p < n; ++p) {
-                size_t b = 9 * (size_t)orig[p];
-                for (int k = 0; k < 9; ++k) dst[b + k] = 0.0;
-                dst[b] = dst[b + 4] = dst[b + 8] = tmp[p];
-            }
-        }
-    }
+    if (f->sigma && (st = get_rec(h, f->sigma, spec_sigma()))) return st;
+    if (f->s && (st = get_rec(h, f->s, spec_sym(FD11, true)))) return st;
+    if (f->alfa && (st = get_rec(h, f->alfa, spec_sym(FA11, true)))) return st;
+    if (f->rod && (st = get_rec(h, f->rod, spec_sym(FR11, true)))) return st;
+    if (f->spin && (st = get_rec(h, f->spin, spec_spin()))) return st;
+    if (f->q && (st = get_rec(h, f->q, spec_iso(FQ, true)))) return st;
+    if (f->qold && (st = get_rec(h, f->qold, spec_iso(FQ, true)))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     std::vector<int> itmp(n);
     auto geti = [&](int *dst, const int *src) -> int {
         CK(cudaMemcpy(itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));

@@ -18,6 +18,7 @@ struct mcm_gpu_handle {
     mcm::StepArgs A;
     // owned allocations
     double *d_fields = nullptr;
+    double *d_stage = nullptr;   // host-array staging for upload/download (9 x npad), on first use
     int *d_ints = nullptr;
     mcm::DevMaterial *d_mats = nullptr;
     void *d_scalars = nullptr;     // DevTime, DevStatus, DevGrid, bbox, energy, counters

@@ -134,6 +134,17 @@ MCM_DECLARE_STEP(exact)
 MCM_DECLARE_STEP(fast)
 #undef MCM_DECLARE_STEP
 
+// Layout of one particle's record in a host array of the C ABI: entry k of
+// the record comes from (goes to) field[k], times sign[k] on download; a
+// negative field is zero on download and skipped on upload.
+struct PackSpec {
+    int width;
+    int field[9];
+    double sign[9];
+};
+void launch_unpack(const StepArgs &a, const PackSpec &s, const double *stage, cudaStream_t st);
+void launch_pack(const StepArgs &a, const PackSpec &s, double *stage, cudaStream_t st);
+
 constexpr int kRedThreads = 256;
 
 // Launch shape of the cooperative gathers: per block, pair_threads / lanes

@@ -314,19 +314,30 @@ class Solver:
         check(self.lib.mcm_gpu_timer(self.h, 1, C.byref(ms)), "mcm_gpu_timer", self.h)
         return ms.value
 
-    def upload(self, state: dict, bbox=None) -> None:
-        """Uploads a host state (the fields a Fortran driver passes) through mcm_gpu_upload."""
+    def upload(self, state: dict, bbox=None, fortran_layout: bool = False) -> None:
+        """Uploads a host state (the fields a Fortran driver passes) through
+        mcm_gpu_upload.  Arrays are [particle, ...] as download returns them;
+        with fortran_layout=True they are already the ABI's buffers (vectors
+        (3,np), tensors (3,3,np) column-major, C-contiguous float64/int32) and
+        are passed as they are, without a host copy."""
         f = _abi.Fields()
         keep = []
         for nm, arr in state.items():
             if nm in _abi.INT_FIELDS:
-                a = np.ascontiguousarray(arr, dtype=np.int32)
+                a = arr if fortran_layout else np.ascontiguousarray(arr, dtype=np.int32)
+                if a.dtype != np.int32 or not a.flags.c_contiguous:
+                    raise ValueError(f"{nm}: C-contiguous int32 expected")
                 setattr(f, nm, _iptr(a))
             else:
-                a = np.asarray(arr, dtype=np.float64)
-                if a.ndim == 3:
-                    a = a.transpose(0, 2, 1)
-                a = np.ascontiguousarray(a)
+                if fortran_layout:
+                    a = arr
+                    if a.dtype != np.float64 or not a.flags.c_contiguous:
+                        raise ValueError(f"{nm}: C-contiguous float64 expected")
+                else:
+                    a = np.asarray(arr, dtype=np.float64)
+                    if a.ndim == 3:
+                        a = a.transpose(0, 2, 1)
+                    a = np.ascontiguousarray(a)
                 setattr(f, nm, _dptr(a))
             keep.append(a)
         b = None
