@@ -850,7 +850,7 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
         if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
     CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
     if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
-    else CK(cudaMemset(h->A.F.dispbc, 0, sizeof(int) * n));
+    else CK(cudaMemsetAsync(h->A.F.dispbc, 0, sizeof(int) * n, h->stream));
     if (f->ptype) CK(cudaMemcpy(h->A.F.ptype, f->ptype, sizeof(int) * n, cudaMemcpyHostToDevice));
     return finish_upload(h, coord_maxmin);
 }
@@ -860,12 +860,11 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
     if (!h || !f || !f->x || !f->mat || !t) return MCM_EINVAL;
     CK(cudaSetDevice(h->device));
     const int n = h->np;
-    std::vector<double> tmp(n);
     int st;
     if ((st = put_vec3(h, f->x, FX))) return st;
     if (f->v) { if ((st = put_vec3(h, f->v, FVX))) return st; }
     else {
-        for (int k = 0; k < 3; ++k) CK(cudaMemset(h->A.F.f[FVX + k], 0, sizeof(double) * n));
+        for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(h->A.F.f[FVX + k], 0, sizeof(double) * n, h->stream));
     }
     if (massopt == 1) { if (!f->mass) return MCM_EINVAL; if ((st = put_scalar(h, f->mass, FMASS))) return st; }
     if (init_h_opt == 1) { if (!f->h) return MCM_EINVAL; if ((st = put_scalar(h, f->h, FH))) return st; }
@@ -881,7 +880,7 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
     }
     CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
     if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
-    else CK(cudaMemset(h->A.F.dispbc, 0, sizeof(int) * n));
+    else CK(cudaMemsetAsync(h->A.F.dispbc, 0, sizeof(int) * n, h->stream));
     CK(cudaMemcpy(h->d_nppermat, cnt.data(), sizeof(int) * h->nmat, cudaMemcpyHostToDevice));
     // hmax (MCM/mcm_init_h.f90:22-37; the material loop indexes particles 1..nummat)
     double hmax = 0.0;
