@@ -2447,6 +2447,7 @@ bool field_ptr(Particle &P, const std::string &f, real *&ptr, int &n) {
     else if (f == "mass") ptr = &P.mass;
     else if (f == "h") ptr = &P.h;
     else if (f == "hold") ptr = &P.hold;
+    else if (f == "h0") ptr = &P.h0;
     else if (f == "rho") ptr = &P.rho;
     else if (f == "rho0") ptr = &P.rho0;
     else if (f == "rhoold") ptr = &P.rhoold;

@@ -285,3 +285,93 @@ def test_openmp_build_matches_serial(case):
     for f in ["x", "v", "rho", "e", "p", "sigma", "q", "efps"]:
         assert np.array_equal(a.get(f), b.get(f)), f
     assert np.array_equal(a.get_int("nnbr"), b.get_int("nnbr"))
+
+
+# ------------------------------------------- variable h and XSPH, restated
+def _bar(**kw):
+    return taylor_bar(dx=0.8e-3, length=8e-3).replace(**kw)
+
+
+def test_variable_h_from_strain_rate(oracle_lib):
+    # MCM/mcm_update_h.f90:27-36: h = hold (1 + tr dt / ndim) for p >= pcut; hmax their largest h
+    orc = Oracle(_bar(h_opt=1))
+    for _ in range(3):
+        orc.step()
+    h0, p0, pc0 = orc.get("h").copy(), orc.get("p").copy(), orc.get("pcut").copy()
+    dt = orc.scalar("dt")
+    orc.step_a()
+    tr = orc.get("tracerod")
+    on = p0 >= pc0
+    want = np.where(on, h0 * (1.0 + tr * dt / 3.0), h0)
+    assert np.array_equal(orc.get("h"), want)
+    assert np.array_equal(orc.get("hold")[on], h0[on])
+    assert orc.scalar("hmax") == want[on].max()
+    assert not np.all(want == h0)
+
+
+def test_variable_h_from_density(oracle_lib):
+    # MCM/mcm_update_h.f90:38-49: h = h0 (rho0 / rho)^(1/ndim) with the density before mcm_rhoupd
+    orc = Oracle(_bar(h_opt=2))
+    for _ in range(3):
+        orc.step()
+    orc.step_a()
+    rho_prev = orc.get("rhoold")            # mcm_rhoupd saves the density it starts from
+    want = orc.get("h0") * np.power(orc.get("rho0") / rho_prev, 1.0 / 3.0)
+    np.testing.assert_allclose(orc.get("h"), want, rtol=2e-16, atol=0)
+
+
+def _w(r, h):
+    c1 = 1.0 / (math.acos(-1.0) * h * h * h)
+    z = r / h
+    return np.where(z < 1.0, c1 * (((0.75 * z - 1.5) * z) * z + 1.0),
+                    np.where(z < 2.0, (c1 / 4.0) * (2.0 - z) ** 3, 0.0))
+
+
+def test_xsph_restated(oracle_lib):
+    # MCM/mcm_update_velocity.f90:61-87 restated on the oracle's state: updated
+    # velocities of real neighbours, ghost velocities from the ghosts' creation,
+    # W with the neighbour's h, V_j = m_j / ((rho_j + rho_i) / 2), epsilon 0.1
+    orc = Oracle(_bar(veloc_opt=1))
+    for _ in range(3):
+        orc.step()
+    orc.step_a()
+    orc.dt_update()
+    orc.step_b()
+    x, v, a = orc.get("x").copy(), orc.get("v").copy(), orc.get("a").copy()
+    m, rho, h, rhoold = orc.get("mass"), orc.get("rho"), orc.get("h"), orc.get("rhoold")
+    dt, dtold = orc.scalar("dt"), orc.scalar("dtold")
+    gpar, gx, gv = orc.ghosts()
+    vu = v + a * (0.5 * (dt + dtold))
+    sv = np.zeros_like(v)
+    nghost = 0
+    for i in range(len(x)):
+        js = orc.nbrlist(i + 1) - 1
+        r = np.sqrt(((x[i] - x[js]) ** 2).sum(axis=1))
+        vol = m[js] / (0.5 * (rho[js] + rho[i]))
+        sv[i] = ((vol * _w(r, h[js]))[:, None] * (vu[js] - vu[i])).sum(axis=0)
+        gq = orc.g_nbrlist(i + 1) - 1
+        if len(gq):
+            nghost += len(gq)
+            pj = gpar[gq] - 1                 # a ghost carries its parent's mass, h and start-of-step rho
+            r = np.sqrt(((x[i] - gx[gq]) ** 2).sum(axis=1))
+            vol = m[pj] / (0.5 * (rhoold[pj] + rho[i]))
+            sv[i] += ((vol * _w(r, h[pj]))[:, None] * (gv[gq] - vu[i])).sum(axis=0)
+    orc.step_c()
+    assert nghost > 0
+    want = vu + 0.1 * sv
+    np.testing.assert_allclose(orc.get("v"), want, rtol=0, atol=1e-12 * np.abs(want).max())
+    assert np.abs(0.1 * sv).max() > 1e-6 * np.abs(want).max()     # the smoothing is not negligible
+
+
+def test_dynamic_relaxation_restated(oracle_lib):
+    # MCM/mcm_update_velocity.f90:33-44: v = drelax_scale v + a (dt + dtold) / 2
+    orc = Oracle(_bar(drelax_scale=0.5))
+    for _ in range(3):
+        orc.step()
+    orc.step_a()
+    orc.dt_update()
+    orc.step_b()
+    v, a = orc.get("v").copy(), orc.get("a").copy()
+    dtn = 0.5 * (orc.scalar("dt") + orc.scalar("dtold"))
+    orc.step_c()
+    assert np.array_equal(orc.get("v"), 0.5 * v + a * dtn)
