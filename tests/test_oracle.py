@@ -320,7 +320,7 @@ def test_variable_h_from_density(oracle_lib):
     np.testing.assert_allclose(orc.get("h"), want, rtol=2e-16, atol=0)
 
 
-def _w(r, h):
+def _w_kernel(r, h):
     c1 = 1.0 / (math.acos(-1.0) * h * h * h)
     z = r / h
     return np.where(z < 1.0, c1 * (((0.75 * z - 1.5) * z) * z + 1.0),
@@ -348,14 +348,14 @@ def test_xsph_restated(oracle_lib):
         js = orc.nbrlist(i + 1) - 1
         r = np.sqrt(((x[i] - x[js]) ** 2).sum(axis=1))
         vol = m[js] / (0.5 * (rho[js] + rho[i]))
-        sv[i] = ((vol * _w(r, h[js]))[:, None] * (vu[js] - vu[i])).sum(axis=0)
+        sv[i] = ((vol * _w_kernel(r, h[js]))[:, None] * (vu[js] - vu[i])).sum(axis=0)
         gq = orc.g_nbrlist(i + 1) - 1
         if len(gq):
             nghost += len(gq)
             pj = gpar[gq] - 1                 # a ghost carries its parent's mass, h and start-of-step rho
             r = np.sqrt(((x[i] - gx[gq]) ** 2).sum(axis=1))
             vol = m[pj] / (0.5 * (rhoold[pj] + rho[i]))
-            sv[i] += ((vol * _w(r, h[pj]))[:, None] * (gv[gq] - vu[i])).sum(axis=0)
+            sv[i] += ((vol * _w_kernel(r, h[pj]))[:, None] * (gv[gq] - vu[i])).sum(axis=0)
     orc.step_c()
     assert nghost > 0
     want = vu + 0.1 * sv
