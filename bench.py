@@ -34,6 +34,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+from mcmtop_b200 import ranks  # noqa: E402  (no CUDA work at import)
+from mcmtop_b200.ranks import job_rate, max_over_ranks  # noqa: E402
 # The batched ensemble runs bodies on up to 64 streams; give the CUDA context
 # (created later, on first use) more hardware queues than the default 8.
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
@@ -73,10 +75,7 @@ def parse():
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return ranks.dist_env()
 
 
 # ------------------------------------------------------------------ clocks
@@ -438,14 +437,8 @@ def gpu_arm(args):
     sol.profile(False)
     if done != args.steps:
         raise RuntimeError(f"run stopped after {done} of {args.steps} steps")
-    ms_max = ms
-    if ws > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = ws * deck.np * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, f"cuda:{local}")
+    value = job_rate(deck.np * args.steps, ws, ms_max)
 
     # roofline of the dominant kernel group
     peak, peak_kind = load_peaks()
@@ -473,15 +466,10 @@ def gpu_arm(args):
         ref.timer_start()
         done64 = ref.run(args.steps)
         ms64 = ref.timer_stop()
-        if ws > 1:
-            import torch.distributed as dist
-
-            t64 = torch.tensor([ms64], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t64, op=dist.ReduceOp.MAX)
-            ms64 = float(t64.item())
+        ms64 = max_over_ranks(ms64, f"cuda:{local}")
         if done64 != args.steps:
             raise RuntimeError(f"FP64 run stopped after {done64} of {args.steps} steps")
-        v64 = ws * deck.np * args.steps / (ms64 / 1e3)
+        v64 = job_rate(deck.np * args.steps, ws, ms64)
         fp64 = {"value": round(v64, 1), "ms_per_step": round(ms64 / args.steps, 4),
                 "mixed_over_fp64": round(value / v64, 3)}
         if rank == 0:
