@@ -1055,8 +1055,18 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     };
     if (f->mat && (st = geti(f->mat, h->A.F.mat))) return st;
     if (f->dispbc && (st = geti(f->dispbc, h->A.F.dispbc))) return st;
-    if (f->nnbr && (st = geti(f->nnbr, h->A.nnbr))) return st;
-    if (f->g_nnbr && (st = geti(f->g_nnbr, h->A.gnnbr))) return st;
+    if (f->nnbr || f->g_nnbr) {
+        // the counts are per cell-order position: position t holds state index cell_list[t]
+        std::vector<int> clist(n);
+        CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        auto getc = [&](int *dst, const int *src) -> int {
+            CK(cudaMemcpy(itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            for (int t = 0; t < n; ++t) dst[orig[clist[t]]] = itmp[t];
+            return MCM_OK;
+        };
+        if (f->nnbr && (st = getc(f->nnbr, h->A.nnbr))) return st;
+        if (f->g_nnbr && (st = getc(f->g_nnbr, h->A.gnnbr))) return st;
+    }
     if (f->ptype && (st = geti(f->ptype, h->A.F.ptype))) return st;
     return MCM_OK;
 }

@@ -22,10 +22,14 @@ values zeroed below 1e-50 (1e-40 for transducers) follow those routines.
 Deliberate differences: where the reference's integer fields overflow
 (``I5`` point counts from 100 000 particles, ``I6`` cell ids from 1 000 000,
 ``I3`` state numbers from 1 000) it writes asterisks that no reader accepts;
-these writers widen the field instead.  The state writers of options 1-3
-(EnSight, LS-DYNA d3plot) and the 1D/2D ASCII state plots of option 0 are
+these writers widen the field instead.  The state writers of options 2-3
+(EnSight case, LS-DYNA d3plot) and the 1D/2D ASCII state plots of option 0 are
 not provided: option 0 has no writer for 3D problems in the reference
-either (MCM/mcm_Stateplot.f90:40-47).
+either (MCM/mcm_Stateplot.f90:40-47).  Option 1 (EnSight: geometry at the
+start, 21 variable files per state, results file, time file) follows
+MCM/mcm_geometry.f90, MCM/mcm_write_ensight_3d.f90 with
+MCM/mcm_write_scalar.f90 / mcm_write_vector.f90 / mcm_write_tensor.f90, and
+MCM/mcm_write_res.f90.
 """
 from __future__ import annotations
 
@@ -34,7 +38,7 @@ import os
 
 import numpy as np
 
-from .fortio import fmt_e, fmt_f, fmt_i
+from .fortio import fmt_e, fmt_f, fmt_i, read_real
 
 # fields a state or time-history record reads
 VTK_FIELDS = ("x", "v", "p", "sigma", "mat", "ptype")
@@ -152,6 +156,8 @@ class Outputs:
         need = set()
         if state_due and self.deck.state_opt == 4:
             need.update(VTK_FIELDS)
+        if state_due and self.deck.state_opt == 1:
+            need.update(ENSIGHT_FIELDS)
         if th_due:
             if self.deck.thnodes:
                 need.update(TH_FIELDS)
@@ -169,8 +175,16 @@ class Outputs:
     def initial(self, ptime: float, state: dict, energies: np.ndarray) -> None:
         """mcm_init_state_output + mcm_state_output, mcm_inittimehist + mcm_timehist."""
         self.nextsttime = ptime + self.deck.stpltime
+        self.ptime = ptime
         if self.deck.state_opt == 4:
             self._write_vtk(state)          # MCM/mcm_init_state_output.f90:61-64 (no increment)
+        if self.deck.state_opt == 1:
+            # MCM/mcm_init_state_output.f90:28-32: the counter starts at 1, mcm_geometry
+            # writes the initial coordinates and clears the time file
+            self.istate = 1
+            self.times = []
+            self._put(self.base + ".geo", ensight_geometry_text(state["x"], state["mat"], self.nummat))
+            self._put(self.base + "_time.txt", "")
         self.state_output(state)
         self.nextthtime = ptime + self.deck.thpltime
         self._init_timehist()
@@ -179,6 +193,7 @@ class Outputs:
     def after_energies(self, ptime: float, state: dict, energies: np.ndarray) -> None:
         """MCM/mcm_solution.f90:81-92, called after mcm_calctotale."""
         st, th = self.due(ptime)
+        self.ptime = ptime
         if st:
             self.state_output(state)
             self.nextsttime += self.deck.stpltime
@@ -188,10 +203,27 @@ class Outputs:
 
     # ---------------------------------------------------------- states
     def state_output(self, state: dict) -> None:
-        """MCM/mcm_state_output.f90: option 4 writes the VTK files and counts."""
+        """MCM/mcm_state_output.f90: option 4 writes the VTK files, option 1
+        the EnSight variable files and the results file; both count."""
         if self.deck.state_opt == 4:
             self._write_vtk(state)
             self.istate += 1
+        elif self.deck.state_opt == 1:
+            self._write_ensight(state)
+            self.istate += 1
+
+    def _write_ensight(self, state: dict) -> None:
+        """MCM/mcm_write_ensight_3d.f90 then MCM/mcm_write_res.f90."""
+        t = fmt_e(self.ptime, 13, 6)
+        self.times.append(t)
+        self._put(self.base + "_time.txt", t + "\n", "a")
+        ext = f"{self.istate:03d}" if self.istate < 1000 else str(self.istate)
+        x0 = np.asarray(self.deck.x, dtype=np.float64)   # xzero: the deck's coordinates (MCM/mcm_initvbls.f90:32)
+        for suf, head, kind, vals in _ensight_variables(state, x0):
+            body = _ens_vector(vals) if kind == "v" else _ens_scalar(vals)
+            self._put(self.base + suf + ext, " " + head + "\n" + "".join(body))
+        name = os.path.basename(self.base)
+        self._put(self.base + ".res", ensight_res_text(name, self.istate, self.times))
 
     def _write_vtk(self, state: dict) -> None:
         d, name = os.path.split(self.base)
@@ -282,6 +314,107 @@ def _kernel_w(r: float, h: float) -> float:
     if z < 2.0:
         return 0.25 * c1 * (2.0 - z) ** 3
     return 0.0
+
+
+# ----------------------------------------------------- EnSight (option 1)
+ENSIGHT_FIELDS = ("x", "v", "a", "p", "rho", "mass", "sigma", "efps", "e", "c", "critts", "h", "nnbr", "mat")
+
+
+def _e12(vals) -> str:
+    return "".join(fmt_e(v, 12, 5) for v in vals)
+
+
+def _zeroed(a: np.ndarray) -> np.ndarray:
+    return np.where(np.abs(a) < 1.0e-50, 0.0, a)
+
+
+def _ens_scalar(values: np.ndarray) -> list:
+    """MCM/mcm_write_scalar.f90: six values per record (6(e12.5)), the last
+    record holding what is left."""
+    v = _zeroed(np.asarray(values, dtype=np.float64)).tolist()
+    return [_e12(v[k:k + 6]) + "\n" for k in range(0, len(v), 6)]
+
+
+def _ens_vector(values: np.ndarray) -> list:
+    """MCM/mcm_write_vector.f90: two particles (six values) per record; the
+    particles go in groups of six, the last group holding what is left."""
+    v = _zeroed(np.asarray(values, dtype=np.float64))
+    out = []
+    for g in range(0, v.shape[0], 6):
+        blk = v[g:g + 6]
+        for k in range(0, blk.shape[0], 2):
+            out.append(_e12(blk[k:k + 2].ravel().tolist()) + "\n")
+    return out
+
+
+def ensight_geometry_text(x: np.ndarray, mat: np.ndarray, nummat: int) -> str:
+    """MCM/mcm_geometry.f90 (3D): coordinates, then per material the point
+    numbers ind .. ind + count - 1 (consecutive, as if the particles were
+    ordered by material)."""
+    out = [" frame geometry\n", " node id assign\n", " element id assign\n", " coordinates\n", f"{len(x):7d}\n"]
+    out.extend(_e12(r) + "\n" for r in x.tolist())
+    ind = 1
+    for j in range(1, nummat + 1):
+        cnt = int((mat == j).sum())
+        out.append(f"part {fmt_i(j, 1)}\n")
+        out.append(f"points list of part {fmt_i(j, 1)}\n")
+        out.append(" point\n")
+        out.append(f"{cnt:8d}\n")
+        out.extend(f"{k:8d}\n" for k in range(ind, ind + cnt))
+        ind += cnt
+    return "".join(out)
+
+
+# (file suffix, header, value) of MCM/mcm_write_ensight_3d.f90, in the order the files are written
+def _ensight_variables(st: dict, x0: np.ndarray) -> list:
+    sig = st["sigma"]
+    z = np.zeros(len(st["x"]))
+    return [
+        ("_displace", "displacement", "v", st["x"] - x0),
+        ("_pressure", "pressure", "s", st["p"]),
+        ("_velocity", "velocity", "v", st["v"]),
+        ("_accelera", "acceleration", "v", st["a"]),
+        ("_density", "density", "s", st["rho"]),
+        ("_mass", "mass", "s", st["mass"]),
+        ("_sigma11", "sigma11", "s", sig[:, 0, 0]),
+        ("_sigma22", "sigma22", "s", sig[:, 1, 1]),
+        ("_sigma33", "sigma33", "s", sig[:, 2, 2]),
+        ("_sigma12", "sigma12", "s", sig[:, 0, 1]),
+        ("_sigma13", "sigma13", "s", sig[:, 0, 2]),
+        ("_sigma23", "sigma23", "s", sig[:, 1, 2]),
+        ("_strain", "Effective plastic strain", "s", st["efps"]),
+        ("_energy", "energy", "s", st["e"] / st["mass"]),
+        ("_C", "C", "s", st["c"]),
+        ("_PCT", "Partical_Critical_Timestep", "s", st["critts"]),
+        ("_Temp", "Temperature", "s", z),                      # temper: not computed
+        ("_Bound", "Boundary_Particles", "s", z),               # mcm_id_boundary is never called
+        ("_Smooth", "Smoothing_length", "s", st["h"]),
+        ("_Neigh", "Number_of_Neighbours", "s", st["nnbr"].astype(np.float64)),
+        ("_material", "Material", "s", st["mat"].astype(np.float64)),
+    ]
+
+
+_RES_NAMES = [("_density", " density"), ("_pressure", " pressure"), ("_material", " material"), ("_mass", " mass"),
+              ("_sigma11", " sigma11"), ("_sigma22", " sigma22"), ("_sigma12", " sigma12"), ("_sigma33", " sigma33"),
+              ("_sigma13", " sigma13"), ("_sigma23", " sigma23"), ("_energy", " Internal_Energy"),
+              ("_strain", " Eff_Plastic_Strain"), ("_C", " Sound Speed"), ("_PCT", " Part_Crit_Timestep"),
+              ("_Temp", " Temperature"), ("_Bound", " Boundary_Particles"), ("_Smooth", " Smoothing_length"),
+              ("_Neigh", " Nber_of_Neigbours"), ("_displace", " displacement"), ("_velocity", " velocity"),
+              ("_accelera", " acceleration")]
+
+
+def ensight_res_text(name: str, istate: int, times: list) -> str:
+    """MCM/mcm_write_res.f90 (3D) before the state counter moves on: it lists
+    istate - 1 times (the ones before the state just written), read back from
+    the time file (so rounded to its e13.6) and written six per record with
+    e10.3."""
+    out = [" 18 3 0\n", f"{fmt_i(istate - 1, 3)}\n"]
+    vals = [read_real(t) for t in times[:max(istate - 1, 0)]]
+    for k in range(0, len(vals), 6):
+        out.append("".join(fmt_e(v, 10, 3) for v in vals[k:k + 6]) + "\n")
+    out.append(" 1 1\n")
+    out.extend(f" {name}{suf}***{label}\n" for suf, label in _RES_NAMES)
+    return "".join(out)
 
 
 DRELAX_FIELDS = ("x", "dispbc", "mat", "mass", "h", "rho", "e")

@@ -291,7 +291,7 @@ def test_deck_text_drives_the_same_simulation(oracle_lib):
 def oracle_state(orc, fields):
     out = {}
     for f in fields:
-        out[f] = orc.get_int(f) if f in ("mat", "ptype") else orc.get(f)
+        out[f] = orc.get_int(f) if f in ("mat", "ptype", "nnbr") else orc.get(f)
     return out
 
 
@@ -408,3 +408,48 @@ def test_relaxed_state_layout():
     # 88 columns wide, and an 80-column reader loses the energy's exponent
     assert read_record(t[3], "(i8,i5,3e20.0,i7)") == [1, 7, 0.5, -1.25e-3, 3.0, 2]
     assert read_record(t[7], "(i8,4e20.0)")[4] == 0.125
+
+
+def test_ensight_records():
+    from mcmtop_b200.output import _ens_scalar, _ens_vector, ensight_geometry_text, ensight_res_text
+    # six scalars per record, the rest on the last one; |v| < 1e-50 written as zero
+    assert _ens_scalar(np.array([1.0, -2.0, 3.0, 4.0, 5.0, 6.0, 1e-60])) == [
+        " 0.10000E+01-0.20000E+01 0.30000E+01 0.40000E+01 0.50000E+01 0.60000E+01\n", " 0.00000E+00\n"]
+    # vectors: two particles per record, in groups of six particles
+    v = np.arange(21, dtype=float).reshape(7, 3)
+    rec = _ens_vector(v)
+    assert len(rec) == 4 and rec[3] == " 0.18000E+02 0.19000E+02 0.20000E+02\n"
+    g = ensight_geometry_text(np.array([[0.5, -0.25, 1.0], [1.0, 2.0, 3.0]]), np.array([1, 1]), 1).splitlines()
+    assert g[:5] == [" frame geometry", " node id assign", " element id assign", " coordinates", "      2"]
+    assert g[5] == " 0.50000E+00-0.25000E+00 0.10000E+01"
+    assert g[7:] == ["part 1", "points list of part 1", " point", "       2", "       1", "       2"]
+    # the results file lists the times before the state just written
+    r = ensight_res_text("bar", 3, ["  0.000000E+00", "  0.123456E+01", "  0.250000E+01"]).splitlines()
+    assert r[:4] == [" 18 3 0", "  2", " 0.000E+00 0.123E+01", " 1 1"]
+    assert r[4] == " bar_density*** density" and r[-1] == " bar_accelera*** acceleration" and len(r) == 25
+
+
+def test_ensight_outputs_follow_the_state(tmp_path, oracle_lib):
+    d = _grid_bar().replace(state_opt=1, stpltime=0.1, thpltime=1e9)
+    orc, out = oracle_program(d, "bar", str(tmp_path), 8)
+    try:
+        names = set(os.listdir(tmp_path))
+        assert {"bar.geo", "bar.res", "bar_time.txt", "bar_density001", "bar_displace001", "bar_material001"} <= names
+        last = out.istate - 1
+        assert last >= 2 and f"bar_sigma23{last:03d}" in names
+        st = out.last_state
+        def fields12(path):     # e12.5 fields, which touch when a value is negative
+            lines = path.read_text().splitlines()
+            return lines[0], np.array([float(ln[k:k + 12]) for ln in lines[1:] for k in range(0, len(ln), 12)])
+
+        head, dens = fields12(tmp_path / f"bar_density{last:03d}")
+        assert head == " density" and len(dens) == d.np
+        np.testing.assert_allclose(dens, st["rho"], rtol=5e-5)
+        _, disp = fields12(tmp_path / f"bar_displace{last:03d}")
+        np.testing.assert_allclose(disp.reshape(-1, 3), st["x"] - d.x, rtol=5e-5, atol=1e-9)
+        times = (tmp_path / "bar_time.txt").read_text().splitlines()
+        assert len(times) == last
+        res = (tmp_path / "bar.res").read_text().splitlines()
+        assert int(res[1]) == last - 1
+    finally:
+        orc.close()

@@ -72,3 +72,18 @@ def test_download_after_resorting(gpu_lib):
     finally:
         a.close()
         b.close()
+
+
+def test_downloaded_neighbour_counts_follow_the_reference_order(gpu_lib):
+    # the counts live per cell-order position on the device
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_FP64_EXACT, reorder_interval=2)
+    try:
+        sol.run(5)
+        nn, _, gn, _ = sol.neighbours()
+        got = sol.download(["nnbr", "g_nnbr"])
+        assert np.array_equal(got["nnbr"], nn) and np.array_equal(got["g_nnbr"], gn)
+        assert gn.any()
+    finally:
+        sol.close()
+
