@@ -828,6 +828,9 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     const int n = h->np;
     int st;
     CK(cudaStreamSynchronize(h->stream));
+    // checked before any copy starts, so that no copy is left reading the caller's buffers
+    for (int i = 0; i < n; ++i)
+        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
     if ((st = put_vec3(h, f->x, FX))) return st;
     if (f->v && (st = put_vec3(h, f->v, FVX))) return st;
     if (f->a && (st = put_vec3(h, f->a, FAX))) return st;
@@ -846,8 +849,6 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     if (f->alfa && (st = put_rec(h, f->alfa, spec_sym(FA11, false)))) return st;
     if (f->rod && (st = put_rec(h, f->rod, spec_sym(FR11, false)))) return st;
     if (f->q && (st = put_rec(h, f->q, spec_iso(FQ, false)))) return st;
-    for (int i = 0; i < n; ++i)
-        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
     CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
     if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
     else CK(cudaMemsetAsync(h->A.F.dispbc, 0, sizeof(int) * n, h->stream));
@@ -861,22 +862,25 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
     CK(cudaSetDevice(h->device));
     const int n = h->np;
     int st;
+    // every check before the first copy, so that no copy is left reading the caller's buffers
+    if ((massopt == 1 && !f->mass) || (init_h_opt == 1 && !f->h) || (init_rhoe == 1 && (!f->rho || !f->e)))
+        return MCM_EINVAL;
+    std::vector<int> cnt(h->nmat, 0);
+    for (int i = 0; i < n; ++i) {
+        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
+        cnt[f->mat[i] - 1] += 1;
+    }
+    CK(cudaStreamSynchronize(h->stream));
     if ((st = put_vec3(h, f->x, FX))) return st;
     if (f->v) { if ((st = put_vec3(h, f->v, FVX))) return st; }
     else {
         for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(h->A.F.f[FVX + k], 0, sizeof(double) * n, h->stream));
     }
-    if (massopt == 1) { if (!f->mass) return MCM_EINVAL; if ((st = put_scalar(h, f->mass, FMASS))) return st; }
-    if (init_h_opt == 1) { if (!f->h) return MCM_EINVAL; if ((st = put_scalar(h, f->h, FH))) return st; }
+    if (massopt == 1 && (st = put_scalar(h, f->mass, FMASS))) return st;
+    if (init_h_opt == 1 && (st = put_scalar(h, f->h, FH))) return st;
     if (init_rhoe == 1) {
-        if (!f->rho || !f->e) return MCM_EINVAL;
         if ((st = put_scalar(h, f->rho, FRHO))) return st;
         if ((st = put_scalar(h, f->e, FE))) return st;
-    }
-    std::vector<int> cnt(h->nmat, 0);
-    for (int i = 0; i < n; ++i) {
-        if (f->mat[i] < 1 || f->mat[i] > h->nmat) return set_error(h, MCM_EINVAL, "material id out of range");
-        cnt[f->mat[i] - 1] += 1;
     }
     CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
     if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
