@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from mcmtop_b200 import _abi
-from mcmtop_b200.deck import copper_model10, fluid_column, taylor_bar, MaterialCard
+from mcmtop_b200.deck import fluid_column, taylor_bar, MaterialCard
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

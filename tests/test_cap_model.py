@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 from mcmtop_b200 import _abi
-from mcmtop_b200.deck import MMMSG, MaterialCard, sand_model4, taylor_bar
+from mcmtop_b200.deck import MMMSG, sand_model4, taylor_bar
 from oracle.pyoracle import Oracle
 
 NSTEPS = 20

@@ -2,8 +2,6 @@
 MCM/mcm_check_sym_pen.f90) and dynamic relaxation
 (MCM/mcm_update_velocity.f90:33-44, MCM/mcm_write_drelax.f90) on the GPU
 against the oracle."""
-import os
-
 import numpy as np
 import pytest
 

@@ -4,8 +4,6 @@ or they must keep cudaMalloc out of the time step).  It must give the same
 per-material energies as the energy sums of mcm_gpu_step_b, on two calls in a
 row (the calls share one scratch array).  This file sorts last so that a run
 stopping at the first failure has run every other test first."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
