@@ -171,6 +171,19 @@ class Solver:
         return done.value
 
     # ------------------------------------------------------- inspection
+    def download_into(self, buffers: dict) -> None:
+        """mcm_gpu_download into the caller's buffers in the ABI's layout
+        (C-contiguous: vectors (np, 3) = Fortran (3,np), tensors (np, 3, 3)
+        holding Fortran (3,3,np) column-major records, ints int32), e.g.
+        page-locked arrays that the copies fill at the link's speed."""
+        f = _abi.Fields()
+        for nm, a in buffers.items():
+            want = np.int32 if nm in _abi.INT_FIELDS else np.float64
+            if a.dtype != want or not a.flags.c_contiguous or a.size != self.n * _abi.FIELD_WIDTH.get(nm, 1):
+                raise ValueError(f"{nm}: C-contiguous {np.dtype(want).name} of {self.n} records expected")
+            setattr(f, nm, _iptr(a) if want is np.int32 else _dptr(a))
+        check(self.lib.mcm_gpu_download(self.h, C.byref(f)), "mcm_gpu_download", self.h)
+
     def download(self, names=None) -> dict:
         if names is None:
             names = _abi.DOUBLE_FIELDS + _abi.INT_FIELDS

@@ -87,3 +87,21 @@ def test_downloaded_neighbour_counts_follow_the_reference_order(gpu_lib):
     finally:
         sol.close()
 
+
+
+def test_download_into_caller_buffers(gpu_lib):
+    deck = taylor_bar(dx=0.8e-3)
+    sol = Solver(deck, _abi.PREC_MIXED)
+    try:
+        sol.run(3)
+        ref = sol.download(["x", "sigma", "rho", "mat"])
+        buf = {"x": np.empty((sol.n, 3)), "sigma": np.empty((sol.n, 9)), "rho": np.empty(sol.n),
+               "mat": np.empty(sol.n, np.int32)}
+        sol.download_into(buf)
+        assert np.array_equal(buf["x"], ref["x"]) and np.array_equal(buf["rho"], ref["rho"])
+        assert np.array_equal(buf["sigma"].reshape(-1, 3, 3).transpose(0, 2, 1), ref["sigma"])
+        assert np.array_equal(buf["mat"], ref["mat"])
+        with pytest.raises(ValueError):
+            sol.download_into({"x": np.empty((sol.n, 2))})
+    finally:
+        sol.close()
