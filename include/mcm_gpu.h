@@ -167,6 +167,11 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
 int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, int init_h_opt,
                        int init_rhoe, double itss, mcm_gpu_time *t);
 
+/* Copies the non-NULL members of f back in the reference's particle order
+ * (whatever order the device keeps its storage in).  Upload, initialise and
+ * download move each host array in one copy through a device staging buffer
+ * of 72 bytes per particle, allocated by the first of them, and convert the
+ * layout on the device: page-locked host buffers move at the link's speed. */
 int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f);
 
 /* ------------------------------------------------------------------ step */
