@@ -86,6 +86,48 @@ class _Cards:
     def fail(self, msg: str):
         raise DeckError(msg, self.line, self.text)
 
+    def block(self, n: int) -> tuple:
+        """The next n cards and their line numbers (for a bulk parse)."""
+        texts, lines = [], []
+        while len(texts) < n and self.pos < len(self.lines):
+            t = self.lines[self.pos]
+            self.pos += 1
+            if t[:1] in ("*", "$"):
+                continue
+            texts.append(t)
+            lines.append(self.pos)
+        return texts, lines
+
+
+def _bulk_columns(texts: list, fmt: str):
+    """Columns of many cards of one fixed format, converted by numpy; None when
+    any field needs the full Fortran rules (blank or embedded-blank fields,
+    D or bare-sign exponents, or what numpy reads that a Fortran READ would
+    not), in which case the cards are read one by one."""
+    from .fortio import parse_format, RECORD
+    spec = parse_format(fmt)
+    rec = np.array([t.rstrip("\r\n")[:RECORD].ljust(RECORD) for t in texts])
+    cols, pos = [], 0
+    try:
+        for kind, w, d in spec:
+            sub = np.array([r[pos:pos + w] for r in rec.tolist()])
+            pos += w
+            # numpy also takes forms a Fortran READ does not ("1_0", "nan"): keep to the plain ones
+            if (np.char.find(sub, "_") >= 0).any():
+                return None
+            if kind == "i":
+                col = sub.astype(np.int64)
+            else:
+                if d:
+                    return None
+                col = sub.astype(np.float64)
+                if not np.all(np.isfinite(col)):
+                    return None
+            cols.append(col)
+    except ValueError:
+        return None
+    return cols
+
 
 # ------------------------------------------------------------------ reading
 def read_deck(source) -> Deck:
@@ -244,20 +286,42 @@ def _nodes(cards: _Cards, d: dict) -> None:
     mat = np.zeros(n, dtype=np.int32)
     disp = np.zeros(n, dtype=np.int32)
     fmt = f"(i8,i5,{ndim}e20.0,i7)"
-    for j in range(1, n + 1):
-        v = cards.read("Error in nodal poistion cards", fmt)
-        if v[0] != j:
-            cards.fail(f"Card for node {v[0]} is out of order. Should be {j}")
-        disp[j - 1] = v[1]
-        x[j - 1, :ndim] = v[2:2 + ndim]
-        mat[j - 1] = v[2 + ndim]
-        if mat[j - 1] == 0:
-            cards.fail(f"Node {j} has zero material type")
-        if not 0 < mat[j - 1] <= d["nummat"]:
-            cards.fail(f"Node {j} has material {mat[j - 1]}, beyond the {d['nummat']} materials")
+    # all cards at once when every field is a plain number and the cards are in
+    # order; otherwise card by card, which applies the full rules and reports
+    # the first bad card
+    start = cards.pos
+    texts, _ = cards.block(n)
+    cols = _bulk_columns(texts, fmt) if len(texts) == n else None
+    ok = (cols is not None and np.array_equal(cols[0], np.arange(1, n + 1))
+          and bool(((cols[2 + ndim] > 0) & (cols[2 + ndim] <= d["nummat"])).all()))
+    if ok:
+        x[:, :ndim] = np.stack(cols[2:2 + ndim], axis=1)
+        mat[:] = cols[2 + ndim]
+        disp[:] = cols[1]
+    else:
+        cards.pos = start
+        for j in range(1, n + 1):
+            v = cards.read("Error in nodal poistion cards", fmt)
+            if v[0] != j:
+                cards.fail(f"Card for node {v[0]} is out of order. Should be {j}")
+            disp[j - 1] = v[1]
+            x[j - 1, :ndim] = v[2:2 + ndim]
+            mat[j - 1] = v[2 + ndim]
+            if mat[j - 1] == 0:
+                cards.fail(f"Node {j} has zero material type")
+            if not 0 < mat[j - 1] <= d["nummat"]:
+                cards.fail(f"Node {j} has material {mat[j - 1]}, beyond the {d['nummat']} materials")
     d["x"], d["mat"], d["dispbc"] = x, mat, disp
     if d["massopt"] == 1 or d["init_h_opt"] == 1 or d["init_rhoe"] == 1:
         pd = np.zeros((n, 4))
+        start = cards.pos
+        texts, _ = cards.block(n)
+        cols = _bulk_columns(texts, "(i8,4e20.0)") if len(texts) == n else None
+        if cols is not None and np.array_equal(cols[0], np.arange(1, n + 1)):
+            pd[:] = np.stack(cols[1:], axis=1)
+            d["pardata"] = pd
+            return
+        cards.pos = start
         for j in range(1, n + 1):
             v = cards.read("Error in additional particle information cards", "(i8,4e20.0)")
             if v[0] != j:

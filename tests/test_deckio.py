@@ -453,3 +453,21 @@ def test_ensight_outputs_follow_the_state(tmp_path, oracle_lib):
         assert int(res[1]) == last - 1
     finally:
         orc.close()
+
+
+def test_node_cards_bulk_and_card_by_card_agree():
+    # plain numbers are read in bulk; a card with a D exponent or a blank
+    # field sends the block through the card-by-card Fortran rules
+    d = _grid_bar()
+    text = deck_text(d)
+    plain = read_deck(text)
+    lines = text.splitlines()
+    k = next(i for i, ln in enumerate(lines) if ln.startswith("       7    0"))
+    rec = lines[k]
+    lines[k] = rec[:8] + "     " + f"{'-1.25d-1':>20}" + rec[33:]
+    odd = read_deck("\n".join(lines) + "\n")
+    assert odd.x[6, 0] == -0.125 and odd.dispbc[6] == 0
+    same = np.ones(d.np, bool)
+    same[6] = False
+    assert np.array_equal(odd.x[same], plain.x[same]) and np.array_equal(odd.x[6, 1:], plain.x[6, 1:])
+    assert np.array_equal(odd.mat, plain.mat)
