@@ -521,20 +521,28 @@ def _heading(text: str, default: str) -> str:
 
 
 def _velocity_cards(v: np.ndarray, ndim: int) -> list:
-    """Runs of equal velocities become a first card and a generation card."""
+    """Runs of equal velocities become a first card and a generation card.
+    What is equal is the text a velocity has in the deck: runs of equal
+    doubles are found first, then neighbouring runs whose text is the same
+    are joined."""
     n = v.shape[0]
-    # the text each particle's velocity has in the deck decides what is equal
-    txt = ["".join(_r(v[i, k], 10) for k in range(ndim)) for i in range(n)]
+    if n == 0:
+        return []
+    vv = v[:, :ndim]
+    starts = np.flatnonzero(np.concatenate([[True], np.any(vv[1:] != vv[:-1], axis=1)]))
+    ends = np.concatenate([starts[1:], [n]]) - 1
+    runs = []                      # (first, last, text)
+    for a, b in zip(starts.tolist(), ends.tolist()):
+        txt = "".join(_r(vv[a, k], 10) for k in range(ndim))
+        if runs and runs[-1][2] == txt:
+            runs[-1] = (runs[-1][0], b, txt)
+        else:
+            runs.append((a, b, txt))
     cards = []
-    i = 0
-    while i < n:
-        j = i
-        while j + 1 < n and txt[j + 1] == txt[i]:
-            j += 1
-        cards.append(_i(i + 1, 8) + txt[i] + "\n")
-        if j > i:
-            cards.append(_i(j + 1, 8) + txt[i] + "\n")
-        i = j + 1
+    for a, b, txt in runs:
+        cards.append(_i(a + 1, 8) + txt + "\n")
+        if b > a:
+            cards.append(_i(b + 1, 8) + txt + "\n")
     return cards
 
 

@@ -193,6 +193,12 @@ def real_field(x: float, w: int) -> str:
         return "0.0".rjust(w)
     if x != x or x in (float("inf"), float("-inf")):
         raise ValueError(f"{x!r} has no deck representation")
+    r = repr(x)
+    if "e" not in r:
+        # the first rendering without building a Decimal: repr's positional digits
+        f = r.rstrip("0") if "." in r else r + "."
+        if len(f) <= room:
+            return f.rjust(w)
     for t in _renderings(x):
         if len(t) <= room:
             return t.rjust(w)
