@@ -436,6 +436,11 @@ def drelax_text(state: dict) -> str:
     return "".join(out)
 
 
+def state_line(ptime: float) -> str:
+    """Format 1200 of MCM/mcm_solution.f90:145, printed after each state output."""
+    return f"\n     State plot written at time {fmt_e(ptime, 10, 4)}"
+
+
 def status_line(timestep: int, ptime: float, dt: float) -> str:
     """Format 1000 of MCM/mcm_solution.f90:143-144."""
     return (f"\n     Problem status for time-step {fmt_i(timestep, 6)}\n"

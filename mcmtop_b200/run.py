@@ -18,7 +18,7 @@ import sys
 
 from . import _abi
 from .deckio import read_deck
-from .output import Outputs, status_line
+from .output import Outputs, state_line, status_line
 from .solver import Solver
 
 PRECISIONS = {"fp64": _abi.PREC_FP64_EXACT, "exact": _abi.PREC_FP64_EXACT, "fast": _abi.PREC_FP64,
@@ -39,6 +39,14 @@ class Program:
         self.status_interval = deck.status_interval if deck.status_interval >= 1 else 100
         self.fused_steps = 0
         self.sync_steps = 0
+        self.log = None
+
+    def _say(self, text: str) -> None:
+        """A message for the screen and the log file (MCM writes both, units * and 13)."""
+        if self.echo:
+            self.echo(text)
+        if self.log is not None:
+            self.log.write(text + "\n")
 
     def _state(self, fields) -> dict:
         return self.solver.download(list(fields)) if fields else {}
@@ -87,8 +95,10 @@ class Program:
         fields = self.out.fields(st, th)
         if st or th:
             self.out.after_energies(s.ptime, self._state(fields), s.energies)
-        if s.timestep % self.status_interval == 0 and self.echo:
-            self.echo(status_line(s.timestep, s.ptime, s.dt))
+        if st:
+            self._say(state_line(s.ptime))
+        if s.timestep % self.status_interval == 0:
+            self._say(status_line(s.timestep, s.ptime, s.dt))
         if s.ptime - s.dt >= self.deck.endtime:       # MCM/mcm_solution.f90:101
             s.ended = True
             return False
@@ -111,7 +121,16 @@ class Program:
             from .output import DRELAX_FIELDS
             self.out.drelax(self._state(DRELAX_FIELDS))
 
+    def open_log(self) -> None:
+        """<out>.log with the status and state-output messages (the reference's
+        log also echoes the input cards, which this one does not)."""
+        self.log = open(self.out.base + ".log", "w")
+        self.log.write(f"{(self.deck.title or self.deck.name)[:78]}\n")
+
     def close(self) -> None:
+        if self.log is not None:
+            self.log.close()
+            self.log = None
         self.solver.close()
 
 
@@ -142,6 +161,7 @@ def main(argv=None) -> int:
     prec = PRECISIONS[args.get("precision", "fp64")]
     prog = Program(deck, fileout, directory, prec, echo=print)
     try:
+        prog.open_log()
         prog.initial()
         n = prog.run(int(args["steps"]) if "steps" in args else None)
         prog.finish()

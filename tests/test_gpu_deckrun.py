@@ -125,4 +125,7 @@ def test_command_line(tmp_path, gpu_lib):
                        cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "Problem status for time-step     25" in r.stdout
+    assert "State plot written at time" in r.stdout
     assert os.path.exists(tmp_path / "cli0.vtk") and os.path.exists(tmp_path / "cli_th16848.csv")
+    log = (tmp_path / "cli.log").read_text()
+    assert log.startswith("taylor bar") and "Problem status for time-step     25" in log
