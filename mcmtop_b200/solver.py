@@ -352,10 +352,14 @@ class Solver:
                         a = a.transpose(0, 2, 1)
                     a = np.ascontiguousarray(a)
                 setattr(f, nm, _dptr(a))
+            if a.size != self.n * _abi.FIELD_WIDTH.get(nm, 1):
+                raise ValueError(f"{nm}: {self.n} records of {_abi.FIELD_WIDTH.get(nm, 1)} expected, got {a.size} values")
             keep.append(a)
         b = None
         if bbox is not None:
             b = np.ascontiguousarray(bbox, dtype=np.float64)
+            if b.size != 6:
+                raise ValueError("bbox: xmin xmax ymin ymax zmin zmax expected")
             keep.append(b)
         check(self.lib.mcm_gpu_upload(self.h, C.byref(f), _dptr(b) if b is not None else None), "mcm_gpu_upload",
               self.h)
