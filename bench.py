@@ -69,8 +69,8 @@ def parse():
     ap.add_argument("--oracle-check-steps", type=int, default=50,
                     help="oracle steps on the full bar for the GPU accuracy spot check")
     ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
-    ap.add_argument("--search-kind", type=int, default=0, choices=[0, 1, 2],
-                    help="neighbour search: 1 one thread per particle, 2 one warp per particle (0: default)")
+    ap.add_argument("--search-kind", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="neighbour search: 1 one thread per particle, 2 one warp per particle, 3 one warp per cell (0: default)")
     return ap.parse_args()
 
 

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MCM_GPU_ABI_VERSION 2
+#define MCM_GPU_ABI_VERSION 3
 #define MCM_GPU_MAX_MATERIALS 16
 
 /* Status codes.  The reference's fatal paths call mcm_shutdown(2)
@@ -46,17 +46,18 @@ typedef enum {
                                   (MCM/mcm_ll_neighbours.f90:44,301-309) */
     MCM_EGHOST_OVERFLOW = 2,   /* ghost storage too small; regrown and retried internally
                                   (MCM/mcm_ghost_setup.f90:269-282) */
-    MCM_ECOMPLEX_C = 3,        /* eos41 c^2 < 0 (MCM/mcm_eos41c.f90:282-288) */
+    MCM_ECOMPLEX_C = 3,        /* eos41 c^2 < 0 (MCM/mcm_eos41c.f90:73-79) */
     MCM_ECAP_NOCONV = 4,       /* cap model Newton loop did not converge (MCM/mcm_f3dm25.f90) */
     MCM_ETIMEOUT = 5,          /* a bounded device wait ran out */
     MCM_ECUDA = 6,             /* CUDA runtime error (see mcm_gpu_last_error) */
     MCM_ENOMEM = 7,            /* device allocation failed */
     MCM_EINVAL = 8,            /* bad argument */
-    MCM_EUNSUPPORTED = 9,      /* option outside the ported path (e.g. contacttype > 0) */
+    MCM_EUNSUPPORTED = 9,      /* option outside the ported path (e.g. 1-D and 2-D problems) */
     MCM_EGRID_OVERFLOW = 10,   /* cell grid larger than its storage; regrown and retried internally */
     MCM_EGHOST_LAYER = 11,     /* a real particle lies in a ghost-layer cell (undefined in the reference) */
     MCM_EGRID_TOO_LARGE = 12   /* the linked-list grid would exceed 2^31 cells
-                                  (MCM/mcm_setuplist.f90:295-302 shuts down) */
+                                  (MCM/mcm_setuplist.f90:85-92 shuts down when
+                                  the grid cannot be allocated) */
 } mcm_gpu_status;
 
 /* Arithmetic of the step. */
@@ -84,6 +85,8 @@ typedef struct {
     double rho_min, rho_max;   /* density limits */
     double strinput[48];       /* constitutive constants after mcm_sets* */
     double eosinput[24];       /* EOS constants */
+    double k_cont, n_cont;     /* repulsive-contact strength K and exponent n (contact cards,
+                                  MCM/mcm_contactype.f90:35; read when contacttype > 0) */
 } mcm_gpu_material;
 
 /* Run options: control cards (MCM/mcm_control_v2.f90:88-124), boundary planes
@@ -92,9 +95,10 @@ typedef struct {
     int ndim;                  /* 3 (1-D and 2-D return MCM_EUNSUPPORTED) */
     int disctype;              /* 0 basic SPH, 1 Bonet mixed-corrected SPH */
     int tcrit_opt;             /* 0 DYNA formula, 1 h/(c+|v|), 2 mindist/(c+|v|) */
-    int contacttype;           /* 0: kernel contact (other materials are neighbours); > 0: they are not.
-                                  The reference's repulsive force (MCM/mcm_rep_contact.f90) has no call
-                                  site, so no contact force is added either way. */
+    int contacttype;           /* 0: kernel contact (other materials are neighbours); > 0: they are
+                                  contacts instead, and Monaghan's repulsive acceleration over them
+                                  (MCM/mcm_rep_contact.f90:37-94, called at mcm_solution.f90:64)
+                                  starts each particle's momentum sum (mcm_oldacceleration.f90:49-56) */
     int h_opt;                 /* smoothing length: 0 constant, 1 from the volumetric strain rate,
                                   2 from the density (MCM/mcm_update_h.f90) */
     int veloc_opt;             /* 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87) */
@@ -126,6 +130,8 @@ typedef struct {
     double *sigma, *s, *q, *qold, *alfa, *rod, *spin;   /* (3,3,np) */
     int *mat, *dispbc, *nnbr, *g_nnbr, *ptype;
     double *h0;                                /* initial h (h_opt 2); upload: NULL takes h */
+    double *repulsion;                         /* (3,np) contact acceleration par%repulsion
+                                                  (contacttype > 0); download only */
 } mcm_gpu_fields;
 
 typedef struct mcm_gpu_handle mcm_gpu_handle;
@@ -149,7 +155,7 @@ int mcm_gpu_set_device(int device);
 int mcm_gpu_material_from_deck(mcm_gpu_material *m);
 
 /* Allocates device storage for np particles.  Replaces the allocation part of
- * MCM/mcm_database.f90:mcm_allocate_memory and MCM/mcm_init_neighb.f90:364-384. */
+ * MCM/mcm_database.f90:mcm_allocate_memory and MCM/mcm_init_neighb.f90:25-46. */
 int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int nmat,
                    int np, mcm_gpu_handle **out);
 int mcm_gpu_destroy(mcm_gpu_handle *h);
@@ -200,6 +206,18 @@ int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done);
  * is too small (the required strides are written to *stride / *g_stride). */
 int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride,
                        int *g_nnbr, int *g_nbr, int *g_stride);
+/* Contact lists of the last search (contacttype > 0): particles of other
+ * materials within reach, in the order mcm_ll_neighbours.f90:150-174 fills
+ * mcm_contlist (1-based ids), and ghost contacts like mcm_g_contlist.  Same
+ * conventions as mcm_gpu_neighbours; with contacttype 0 every count is 0. */
+int mcm_gpu_contacts(mcm_gpu_handle *h, int *ncont, int *cont, int *stride,
+                     int *g_ncont, int *g_cont, int *g_stride);
+/* Per-material contact forces of the last step_b (mcm_mat%xcf, %ycf, %zcf:
+ * the sums of mass x repulsion of MCM/mcm_oldacceleration.f90:52-55, written
+ * to the time-history file by MCM/mcm_timehist.f90:46): 3*nmat doubles,
+ * x y z per material.  Zero with contacttype 0 and with disctype 1, whose
+ * momentum routine (MCM/mcm_corr_acceleration.f90) does not sum them. */
+int mcm_gpu_contact_forces(mcm_gpu_handle *h, double *xyz);
 /* Ghosts of the last mcm_ghost_setup: *ngp, source particle (1-based), x (3,ngp), v (3,ngp). */
 int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, int cap);
 /* Linked-list grid of the last search: gridlim(3), gridmin(3), gridsize(3). */
@@ -269,7 +287,8 @@ typedef struct {
     int pair_blocks_per_sm;  /* blocks per SM the gathers' persistent grid is sized for: 1..16 */
     int nbr_stride;          /* neighbour-table row width in entries (rounded up to 4; still regrown
                                 when a list outgrows it) */
-    int search_kind;         /* 1: one thread per particle (the default), 2: one warp per particle */
+    int search_kind;         /* 1: one thread per particle (the default), 2: one warp per particle,
+                                3: one warp per cell (candidates staged in shared memory) */
     double ms_per_step;      /* mcm_gpu_autotune: device time per loop iteration of the chosen shape */
 } mcm_gpu_tuning;
 

@@ -37,6 +37,7 @@ class Material(C.Structure):
         ("rho", C.c_double), ("g", C.c_double), ("av_l", C.c_double), ("av_q", C.c_double),
         ("mass", C.c_double), ("h", C.c_double), ("rho_min", C.c_double), ("rho_max", C.c_double),
         ("strinput", C.c_double * 48), ("eosinput", C.c_double * 24),
+        ("k_cont", C.c_double), ("n_cont", C.c_double),
     ]
 
 
@@ -65,7 +66,7 @@ class Fields(C.Structure):
         ("etry", _DP), ("einc", _DP), ("capa", _DP),
         ("sigma", _DP), ("s", _DP), ("q", _DP), ("qold", _DP), ("alfa", _DP), ("rod", _DP), ("spin", _DP),
         ("mat", _IP), ("dispbc", _IP), ("nnbr", _IP), ("g_nnbr", _IP), ("ptype", _IP),
-        ("h0", _DP),
+        ("h0", _DP), ("repulsion", _DP),
     ]
 
 
@@ -80,7 +81,7 @@ class Tuning(C.Structure):
 
 # per-particle width of every field in Fields (doubles or ints)
 FIELD_WIDTH = {
-    "x": 3, "v": 3, "a": 3, "sigma": 9, "s": 9, "q": 9, "qold": 9, "alfa": 9, "rod": 9, "spin": 9,
+    "x": 3, "v": 3, "a": 3, "repulsion": 3, "sigma": 9, "s": 9, "q": 9, "qold": 9, "alfa": 9, "rod": 9, "spin": 9,
 }
 DOUBLE_FIELDS = [f for f, t in Fields._fields_ if t is _DP]
 INT_FIELDS = [f for f, t in Fields._fields_ if t is _IP]
@@ -114,6 +115,8 @@ def load() -> C.CDLL:
         "mcm_gpu_run": ([H, C.c_int, C.POINTER(Time), _IP], C.c_int),
         "mcm_gpu_neighbours": ([H, _IP, _IP, _IP, _IP, _IP, _IP], C.c_int),
         "mcm_gpu_ghosts": ([H, _IP, _IP, _DP, _DP, C.c_int], C.c_int),
+        "mcm_gpu_contacts": ([H, _IP, _IP, _IP, _IP, _IP, _IP], C.c_int),
+        "mcm_gpu_contact_forces": ([H, _DP], C.c_int),
         "mcm_gpu_grid": ([H, _IP, _DP, _DP], C.c_int),
         "mcm_gpu_energies": ([H, _DP], C.c_int),
         "mcm_gpu_stats": ([H, _DP, _IP, _IP, _IP], C.c_int),

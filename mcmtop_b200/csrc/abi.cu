@@ -43,6 +43,7 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.hmax = c.hmax;
     p.h_opt = c.h_opt;
     p.contacttype = c.contacttype;
+    p.contact = (c.contacttype > 0 && nmat > 1) ? 1 : 0;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;
@@ -98,6 +99,12 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
     CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
     CK(cudaMemsetAsync(h->A.gnnbr, 0, sizeof(int) * np, h->stream));
+    if (h->A.prm.contact) {
+        if ((st = dalloc(h, &h->A.ncont, np))) return st;
+        if ((st = dalloc(h, &h->A.gncont, np))) return st;
+        CK(cudaMemsetAsync(h->A.ncont, 0, sizeof(int) * np, h->stream));
+        CK(cudaMemsetAsync(h->A.gncont, 0, sizeof(int) * np, h->stream));
+    }
     if ((st = dalloc(h, &h->A.rec0, np))) return st;
     if ((st = dalloc(h, &h->A.rec1, np))) return st;
     if ((st = dalloc(h, &h->A.rec2, np))) return st;
@@ -160,6 +167,17 @@ int alloc_table(mcm_gpu_handle *h, int nstride, int gstride) {
     return MCM_OK;
 }
 
+// Contact lists (contacttype > 0 with several materials): particles of other
+// materials within reach, the lists mcm_rep_cont reads.
+int alloc_contacts(mcm_gpu_handle *h, int cstride, int gcstride) {
+    int st;
+    h->A.cstride = round_up(cstride, 4);
+    h->A.gcstride = gcstride;
+    if ((st = dalloc(h, &h->A.cidx, (size_t)h->A.cstride * h->npad))) return st;
+    if ((st = dalloc(h, &h->A.gcont, (size_t)gcstride * h->npad))) return st;
+    return MCM_OK;
+}
+
 int reset_status(mcm_gpu_handle *h) {
     CK(cudaMemsetAsync(h->A.status, 0, sizeof(DevStatus), h->stream));
     return MCM_OK;
@@ -181,10 +199,19 @@ int regrow(mcm_gpu_handle *h, int *grew) {
     switch (s.code) {
         case MCM_ENBR_OVERFLOW: {
             int ns = h->A.nstride, ng = h->A.gstride;
-            if (s.req_stride > ns) ns = s.req_stride + s.req_stride / 8 + 8;
-            if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
-            if ((st = alloc_table(h, ns, ng))) return st;
-            *grew = 1;
+            if (s.req_stride > ns || s.req_gstride > ng) {
+                if (s.req_stride > ns) ns = s.req_stride + s.req_stride / 8 + 8;
+                if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
+                if ((st = alloc_table(h, ns, ng))) return st;
+                *grew = 1;
+            }
+            int cs = h->A.cstride, gcs = h->A.gcstride;
+            if (h->A.prm.contact && (s.req_cstride > cs || s.req_gcstride > gcs)) {
+                if (s.req_cstride > cs) cs = s.req_cstride + s.req_cstride / 8 + 8;
+                if (s.req_gcstride > gcs) gcs = round_up(s.req_gcstride + s.req_gcstride / 8 + 8, 8);
+                if ((st = alloc_contacts(h, cs, gcs))) return st;
+                *grew = 1;
+            }
             break;
         }
         case MCM_EGHOST_OVERFLOW: {
@@ -228,13 +255,20 @@ int launch_strain(mcm_gpu_handle *h) {
 }
 int launch_mom(mcm_gpu_handle *h, int integrate) {
     const int prec = h->cfg.precision;
+    if (h->A.prm.contact) {
+        // MCM/mcm_solution.f90:64: repulsive contact before the momentum sum
+        Scope sc(h, R_MOM_PREP, 1);
+        if (prec == MCM_PREC_FP64_EXACT) exact::launch_rep_cont(h->A, h->stream);
+        else fast::launch_rep_cont(h->A, h->stream);
+    }
     {
         Scope sc(h, R_MOM_PREP, 1);
         if (prec == MCM_PREC_FP64_EXACT) exact::launch_mom_prep(h->A, h->stream);
         else if (prec == MCM_PREC_MIXED) mixed::launch_mom_prep(h->A, h->stream);
         else fast::launch_mom_prep(h->A, h->stream);
     }
-    Scope sc(h, R_MOMENTUM, 1);
+    // the cooperative gathers of several materials add a fixed-order energy-partials kernel
+    Scope sc(h, R_MOMENTUM, (prec != MCM_PREC_FP64_EXACT && h->nmat > 1) ? 2 : 1);
     switch (prec) {
         case MCM_PREC_FP64_EXACT: return exact::launch_momentum(h->A, h->stream, integrate);
         case MCM_PREC_MIXED: return mixed::launch_momentum(h->A, h->stream, integrate);
@@ -437,8 +471,8 @@ const char *mcm_gpu_strerror(int status) {
 
 const char *mcm_gpu_last_error(mcm_gpu_handle *h) { return h ? h->last_error.c_str() : "no handle"; }
 
-// MCM/mcm_matin.f90:46-56, MCM/mcm_sets1.f90:23-51, mcm_sets3.f90:78-96,
-// mcm_sets10.f90:121-134, MCM/mcm_calcg.f90:31-59.
+// MCM/mcm_matin.f90:46-56, MCM/mcm_sets1.f90:23-51, mcm_sets3.f90:25-43,
+// mcm_sets10.f90:23-36, MCM/mcm_calcg.f90:31-59.
 int mcm_gpu_material_from_deck(mcm_gpu_material *m) {
     if (!m) return MCM_EINVAL;
     if (m->visc_type == 0) m->visc_type = 1;
@@ -603,6 +637,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
         d.model = mats[m].model; d.eos = mats[m].eos; d.visc_type = mats[m].visc_type;
         d.rho = mats[m].rho; d.g = mats[m].g; d.av_l = mats[m].av_l; d.av_q = mats[m].av_q;
         d.mass = mats[m].mass; d.h = mats[m].h; d.rho_min = mats[m].rho_min; d.rho_max = mats[m].rho_max;
+        d.k_cont = mats[m].k_cont; d.n_cont = mats[m].n_cont;
         std::memcpy(d.strinput, mats[m].strinput, sizeof(d.strinput));
         std::memcpy(d.eosinput, mats[m].eosinput, sizeof(d.eosinput));
     }
@@ -636,6 +671,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     TRY(alloc_particles(h));
     int entries = cfg->nbr_stride > 0 ? cfg->nbr_stride : 100;
     TRY(alloc_table(h, entries, cfg->boundary ? 48 : 8));
+    if (h->A.prm.contact) TRY(alloc_contacts(h, 16, 8));
     TRY(alloc_cells(h, 1 << 16));
     TRY(alloc_ghosts(h, cfg->boundary ? std::max(4096, np / 8) : 32));
     TRY(dalloc(h, &h->d_nppermat, (size_t)nmat));
@@ -655,7 +691,8 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,
-                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr, h->A.rec3, h->A.grec3};
+                    h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr, h->A.rec3, h->A.grec3,
+                    h->A.cidx, h->A.gcont, h->A.ncont, h->A.gncont};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (double *p : h->adj_ckpt)
@@ -1032,6 +1069,7 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     if (f->x && (st = get_rec(h, f->x, spec_vec3(FX)))) return st;
     if (f->v && (st = get_rec(h, f->v, spec_vec3(FVX)))) return st;
     if (f->a && (st = get_rec(h, f->a, spec_vec3(FAX)))) return st;
+    if (f->repulsion && (st = get_rec(h, f->repulsion, spec_vec3(FRPX)))) return st;
     struct { double *p; int f; } sc[] = {
         {f->mass, FMASS}, {f->h, FH}, {f->hold, FHOLD}, {f->rho, FRHO}, {f->rhoold, FRHOOLD}, {f->e, FE},
         {f->p, FP}, {f->c, FC}, {f->vabs, FVABS}, {f->efps, FEFPS}, {f->pcut, FPCUT}, {f->p_cut, FPCUT2},
@@ -1112,6 +1150,65 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
         for (int t = 0; t < n; ++t)
             for (int k = 0; k < gcnt[t]; ++k) g_nbr[(size_t)orig[clist[t]] * *g_stride + k] = tab[(size_t)k * np + t] + 1;
     }
+    return MCM_OK;
+}
+
+int mcm_gpu_contacts(mcm_gpu_handle *h, int *ncont, int *cont, int *stride, int *g_ncont, int *g_cont,
+                     int *g_stride) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    const int n = h->np, np = h->npad;
+    std::vector<int> orig(n), cnt(n, 0), gcnt(n, 0), clist(n);
+    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    const bool on = h->A.prm.contact != 0;
+    if (on) {
+        CK(cudaMemcpy(cnt.data(), h->A.ncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gcnt.data(), h->A.gncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    int need = 0, gneed = 0;
+    for (int t = 0; t < n; ++t) { need = std::max(need, cnt[t]); gneed = std::max(gneed, gcnt[t]); }
+    if (ncont) for (int t = 0; t < n; ++t) ncont[orig[clist[t]]] = cnt[t];
+    if (g_ncont) for (int t = 0; t < n; ++t) g_ncont[orig[clist[t]]] = gcnt[t];
+    bool small = (cont && stride && *stride < need) || (g_cont && g_stride && *g_stride < gneed);
+    if (stride) { if (small || !cont) *stride = std::max(*stride, need); }
+    if (g_stride) { if (small || !g_cont) *g_stride = std::max(*g_stride, gneed); }
+    if (small) return MCM_EINVAL;
+    if (!on) return MCM_OK;
+    if (cont && stride) {
+        const int cs = h->A.cstride;
+        std::vector<unsigned int> tab((size_t)cs * np);
+        CK(cudaMemcpy(tab.data(), h->A.cidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
+        for (int t = 0; t < n; ++t) {
+            int *row = cont + (size_t)orig[clist[t]] * *stride;
+            for (int k = 0; k < cnt[t]; ++k) row[k] = orig[clist[tab[(size_t)t * cs + k] & 0x3ffffffu]] + 1;
+        }
+    }
+    if (g_cont && g_stride) {
+        std::vector<int> tab((size_t)h->A.gcstride * np);
+        CK(cudaMemcpy(tab.data(), h->A.gcont, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
+        for (int t = 0; t < n; ++t)
+            for (int k = 0; k < gcnt[t]; ++k)
+                g_cont[(size_t)orig[clist[t]] * *g_stride + k] = tab[(size_t)k * np + t] + 1;
+    }
+    return MCM_OK;
+}
+
+int mcm_gpu_contact_forces(mcm_gpu_handle *h, double *xyz) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (!xyz) return MCM_EINVAL;
+    const int nv = 3 * h->nmat;
+    if (!h->A.prm.contact || h->cfg.disctype != 0) {
+        for (int k = 0; k < nv; ++k) xyz[k] = 0.0;
+        return MCM_OK;
+    }
+    // the rows of the block partials are free between steps
+    launch_contact_forces(h->A, h->stream, h->A.red);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(xyz, h->A.red, sizeof(double) * nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return MCM_OK;
 }
 
@@ -1288,6 +1385,7 @@ int adj_check(mcm_gpu_handle *h) {
     if (h->cfg.reorder_interval != 0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: reorder_interval must be 0");
     if (h->cfg.h_opt != 0 || h->cfg.veloc_opt != 0)
         return set_error(h, MCM_EUNSUPPORTED, "adjoint: constant smoothing length without XSPH only");
+    if (h->A.prm.contact) return set_error(h, MCM_EUNSUPPORTED, "adjoint: no repulsive contact (contacttype > 0)");
     for (const mcm_gpu_material &m : h->mats)
         if (m.model != 10 || m.eos != 41) return set_error(h, MCM_EUNSUPPORTED, "adjoint: model 10 with EOS 41 only");
     return MCM_OK;

@@ -10,7 +10,7 @@
 //
 // The forward step n (MCM/mcm_solution.f90:37-138) is, per particle:
 //   xs = x - v dt_prev/2                      (MCM/mcm_strain.f90:25-29)
-//   G_i = sum_j V_j (v_j - v_i) (x) gradW(xs_i - xs_j)   (mcm_oldstrain.f90:95-124)
+//   G_i = sum_j V_j (v_j - v_i) (x) gradW(xs_i - xs_j)   (mcm_oldstrain.f90:34-64)
 //   rod, spin, tr = sym G, skew G, tr G
 //   (rho, e, p, efps, sigma, q)' = C(rho, e, p, efps, sigma, rod, spin, tr; theta)
 //                                             (mcm_rhoupd, mcm_constitutive)
@@ -20,7 +20,7 @@
 //                                             (mcm_update_velocity, mcm_move, mcm_check_sym_pen)
 // with ghosts g of parent p: x_g = M_g x_p + c_g, v_g = M_g v_p (M_g = +-1 per
 // axis), rho_g = rho_p at neighbour time, S_g = S_p with every off-diagonal
-// negated (mcm_update_ghost_stress.f90:272-285).
+// negated (mcm_update_ghost_stress.f90:28-41).
 //
 // Reverse kernels (each a gather over the particle's own list; the lists are
 // symmetric, i in N(j) <=> j in N(i), so the terms a particle contributes to

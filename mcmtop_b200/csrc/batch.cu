@@ -50,7 +50,7 @@ struct Shape {
     int search, pair, bps, stride, kind;
 };
 
-int search_kind_of(const mcm_gpu_handle *h) { return h->A.search_kind == 2 ? 2 : 1; }
+int search_kind_of(const mcm_gpu_handle *h) { return (h->A.search_kind == 2 || h->A.search_kind == 3) ? h->A.search_kind : 1; }
 
 void apply_shape(mcm_gpu_handle *h, const Shape &s) {
     h->A.search_kind = s.kind;
@@ -208,7 +208,7 @@ int mcm_gpu_set_tuning(mcm_gpu_handle *h, const mcm_gpu_tuning *t) {
     if (!h || !t) return MCM_EINVAL;
     if (!valid_block(t->search_threads) || !valid_block(t->pair_threads)) return MCM_EINVAL;
     if (t->pair_blocks_per_sm < 0 || t->pair_blocks_per_sm > 16 || t->nbr_stride < 0) return MCM_EINVAL;
-    if (t->search_kind < 0 || t->search_kind > 2) return MCM_EINVAL;
+    if (t->search_kind < 0 || t->search_kind > 3) return MCM_EINVAL;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (t->search_threads) h->A.search_threads = t->search_threads;
@@ -278,10 +278,11 @@ int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best) {
                 if ((st = timed(s, &ms))) goto out;
                 if (ms < bestMs) { bestMs = ms; bestS = s; }
             }
-    // the other search kind with the best block sizes
-    {
+    // the other search kinds with the best block sizes
+    for (int kind = 1; kind <= 3; ++kind) {
+        if (kind == cur.kind) continue;
         Shape s = bestS;
-        s.kind = (cur.kind == 1) ? 2 : 1;
+        s.kind = kind;
         double ms = 0.0;
         if ((st = timed(s, &ms))) goto out;
         if (ms < bestMs) { bestMs = ms; bestS = s; }

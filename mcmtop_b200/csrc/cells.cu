@@ -18,7 +18,7 @@
 namespace mcm {
 
 // ------------------------------------------------------------- grid set-up
-// MCM/mcm_setuplist.f90:240-291 (one thread).
+// MCM/mcm_setuplist.f90:30-81 (one thread).
 __global__ void k_grid_setup(StepArgs a) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (a.status->code) return;
@@ -87,7 +87,7 @@ __global__ void k_grid_setup(StepArgs a) {
 }
 
 // --------------------------------------------------------------- cell keys
-// MCM/mcm_setuplist.f90:316-345: particles outside the grid get no cell.
+// MCM/mcm_setuplist.f90:110-135: particles outside the grid get no cell.
 __global__ void k_cell_keys(StepArgs a) {
     if (a.status->code) return;
     const DevGrid g = *a.grid;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
 }
 
 // Per-cell order: descending reference index (head insertion in
-// MCM/mcm_setuplist.f90:336-340 over i = 1..np ascending).
+// MCM/mcm_setuplist.f90:126-130 over i = 1..np ascending).
 __global__ void k_cell_sort(StepArgs a) {
     if (a.status->code) return;
     const long long ncells = a.grid->ncells;
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
     const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
-    int nn = 0, gn = 0;
+    int nn = 0, gn = 0, nc = 0, gcn = 0;
     double mind = 1.0e20;
     if (key >= 0) {
         const DevGrid g = *a.grid;
@@ -540,8 +540,12 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         const float reach2 = reach * reach * 1.0009765625f + 9.765625e-4f * csm * csm;
         const int mati = a.cmat[t];
         unsigned *out = a.nidx + (size_t)t * cap;
-        // MCM/mcm_ll_neighbours.f90:238-267: other materials' particles are
-        // appended after the own material's only with kernel contact
+        // MCM/mcm_ll_neighbours.f90:150-174, 238-267: other materials'
+        // particles are appended after the own material's with kernel contact
+        // (a second walk), and form the contact list otherwise (the same walk,
+        // each list in walk order)
+        const bool contact = a.prm.contact != 0;
+        unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
         const int passes = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
@@ -577,7 +581,15 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 if (!(d2 < __dmul_rn(hs, hs))) continue;
                             }
-                            if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) continue;
+                            if (contact) {
+                                if (a.cmat[p] != mati) {
+                                    if (nc < a.cstride) cout[nc] = (unsigned)p | code;
+                                    ++nc;
+                                    continue;
+                                }
+                            } else if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) {
+                                continue;
+                            }
                             if (want_mind) mind = fmin(mind, d2);
                             if (nn < cap) out[nn] = (unsigned)p | code;
                             ++nn;
@@ -588,6 +600,10 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         }
         if (nn > cap) {
             atomicMax(&a.status->req_stride, nn);
+            raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+        }
+        if (contact && nc > a.cstride) {
+            atomicMax(&a.status->req_cstride, nc);
             raise_status(a.status, MCM_ENBR_OVERFLOW, i);
         }
         // ghosts: only neighbourhoods that reach a ghost layer
@@ -609,7 +625,15 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                     const double d2 = exact_d2(xi, c);
                                     const double hs = __dadd_rn(c.w, xi.w);
                                     if (d2 < __dmul_rn(hs, hs)) {
-                                        if (a.nmat > 1 && (a.gmat[q] == mati) != (pass == 0)) continue;
+                                        if (contact) {
+                                            if (a.gmat[q] != mati) {
+                                                if (gcn < a.gcstride) a.gcont[(size_t)gcn * np + t] = q;
+                                                ++gcn;
+                                                continue;
+                                            }
+                                        } else if (a.nmat > 1 && (a.gmat[q] == mati) != (pass == 0)) {
+                                            continue;
+                                        }
                                         mind = fmin(mind, d2);
                                         if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
                                         ++gn;
@@ -621,6 +645,10 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     atomicMax(&a.status->req_gstride, gn);
                     raise_status(a.status, MCM_ENBR_OVERFLOW, i);
                 }
+                if (gcn > a.gcstride) {
+                    atomicMax(&a.status->req_gcstride, gcn);
+                    raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+                }
             }
         }
         mind = sqrt(mind);
@@ -628,6 +656,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
     a.nnbr[t] = nn;
     a.gnnbr[t] = gn;
+    if (a.prm.contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
     if (want_mind) a.F.f[FMINDIST][i] = mind;
     atomicMax(&a.status->max_nbr, nn);
     atomicMax(&a.status->max_gnbr, gn);
@@ -655,8 +684,9 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
     const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
     const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
-    int nn = 0, gn = 0;
+    int nn = 0, gn = 0, nc = 0, gcn = 0;
     double mind = 1.0e20;
+    const bool contact = a.prm.contact != 0;
     if (key >= 0) {
         const DevGrid g = *a.grid;
         int bx, by, bz;
@@ -677,6 +707,7 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
         // x extent of the rows: the own column always, a side column when its
         // box can hold a neighbour (the test of k_search's cell loop)
         const float gxl = ui.x, gxr = fmaxf(cs[0] - ui.x, 0.0f);
+        unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
         const int passes = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
@@ -698,7 +729,7 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                     const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
                     for (int base = cb; base < ce; base += 32) {
                         const int p = base + lane;
-                        bool acc = false;
+                        bool acc = false, accc = false;
                         double d2 = 0.0;
                         int lx = lf;
                         if (p < ce) {
@@ -716,7 +747,12 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 acc = d2 < __dmul_rn(hs, hs);
                             }
-                            if (acc && a.nmat > 1) acc = ((a.cmat[p] == mati) == (pass == 0));
+                            if (acc && contact) {
+                                accc = (a.cmat[p] != mati);
+                                acc = !accc;
+                            } else if (acc && a.nmat > 1) {
+                                acc = ((a.cmat[p] == mati) == (pass == 0));
+                            }
                         }
                         const unsigned bal = __ballot_sync(0xffffffffu, acc);
                         if (acc) {
@@ -725,6 +761,14 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                             if (pos < cap) out[pos] = (unsigned)p | ((code_yz + (unsigned)(lx - bx + 1)) << 26);
                         }
                         nn += __popc(bal);
+                        if (contact) {
+                            const unsigned cbal = __ballot_sync(0xffffffffu, accc);
+                            if (accc) {
+                                const int pos = nc + __popc(cbal & below);
+                                if (pos < a.cstride) cout[pos] = (unsigned)p | ((code_yz + (unsigned)(lx - bx + 1)) << 26);
+                            }
+                            nc += __popc(cbal);
+                        }
                     }
                 }
             }
@@ -745,7 +789,7 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                 const int2 gc = a.gcell[(int)cell_key(lx, my, nz, g.gridlim)];
                                 for (int base = 0; base < gc.y; base += 32) {
                                     const int r = base + lane;
-                                    bool acc = false;
+                                    bool acc = false, accc = false;
                                     double d2 = 0.0;
                                     int q = 0;
                                     if (r < gc.y) {
@@ -753,8 +797,13 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                         const double4 c = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
                                         d2 = exact_d2(xi, c);
                                         const double hs = __dadd_rn(c.w, xi.w);
-                                        acc = (d2 < __dmul_rn(hs, hs)) &&
-                                              (a.nmat == 1 || (a.gmat[q] == mati) == (pass == 0));
+                                        acc = d2 < __dmul_rn(hs, hs);
+                                        if (acc && contact) {
+                                            accc = (a.gmat[q] != mati);
+                                            acc = !accc;
+                                        } else if (acc && a.nmat > 1) {
+                                            acc = ((a.gmat[q] == mati) == (pass == 0));
+                                        }
                                     }
                                     const unsigned bal = __ballot_sync(0xffffffffu, acc);
                                     if (acc) {
@@ -763,6 +812,14 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
                                         if (pos < a.gstride) a.gnbr[(size_t)pos * np + t] = q;
                                     }
                                     gn += __popc(bal);
+                                    if (contact) {
+                                        const unsigned cbal = __ballot_sync(0xffffffffu, accc);
+                                        if (accc) {
+                                            const int pos = gcn + __popc(cbal & below);
+                                            if (pos < a.gcstride) a.gcont[(size_t)pos * np + t] = q;
+                                        }
+                                        gcn += __popc(cbal);
+                                    }
                                 }
                             }
                 }
@@ -780,17 +837,237 @@ __global__ void __launch_bounds__(256) k_search_warp(StepArgs a) {
         atomicMax(&a.status->req_gstride, gn);
         raise_status(a.status, MCM_ENBR_OVERFLOW, i);
     }
+    if (contact && nc > a.cstride) {
+        atomicMax(&a.status->req_cstride, nc);
+        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+    }
+    if (contact && gcn > a.gcstride) {
+        atomicMax(&a.status->req_gcstride, gcn);
+        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+    }
     if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
     a.nnbr[t] = nn;
     a.gnnbr[t] = gn;
+    if (contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
     if (want_mind) a.F.f[FMINDIST][i] = mind;
     atomicMax(&a.status->max_nbr, nn);
     atomicMax(&a.status->max_gnbr, gn);
 }
 
+// The same search with one warp per cell (search_kind 3): the lanes are the
+// particles of one cell (32 at a time), so every lane walks the same rows of
+// the same 27-cell neighbourhood and the loop control is warp-uniform.  Each
+// row's contiguous candidate range is staged 32 records at a time in shared
+// memory by one coalesced load per lane and then read by every lane as a
+// broadcast, so the inner loop has no global load.  Candidates are visited in
+// k_search's order and tested with its FP32 decision and FP64 tie test, so
+// the lists are k_search's, entry for entry.
+constexpr int kCellWarps = 8;
+__global__ void __launch_bounds__(kCellWarps * 32, 3) k_search_cell(StepArgs a) {
+    __shared__ float4 stage[kCellWarps][32];
+    __shared__ int stage_mat[kCellWarps][32];
+    if (a.status->code) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long ncells = a.grid->ncells;
+    const int gl0 = a.grid->gridlim[0], gl1 = a.grid->gridlim[1], gl2 = a.grid->gridlim[2];
+    // cell keys from scalars (an array passed by pointer would live in local memory)
+    auto key_of = [gl0, gl1](int x, int y, int z) { return (x - 1) + gl0 * ((y - 1) + gl1 * (z - 1)); };
+    const float hcut = (float)a.grid->hcut;
+    const int np = a.npad;
+    const int cap = a.nstride;
+    const bool with_self = (a.prm.disctype == 1);
+    const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
+    const bool contact = a.prm.contact != 0;
+    const bool multi = a.nmat > 1;
+    const float cs[3] = {(float)(1.0 / a.grid->gridsize[0]), (float)(1.0 / a.grid->gridsize[1]),
+                         (float)(1.0 / a.grid->gridsize[2])};
+    const float csm = fmaxf(cs[0], fmaxf(cs[1], cs[2]));
+    const float kb = 2.44140625e-4f * csm * csm;
+    const float khi = 1.0f + 2.44140625e-4f, klo = 1.0f - 2.44140625e-4f;
+    float4 *st = stage[w];
+    int *stm = stage_mat[w];
+    const long long nwarps = (long long)gridDim.x * kCellWarps;
+    for (long long c = (long long)blockIdx.x * kCellWarps + w; c < ncells; c += nwarps) {
+        const int c0 = a.cell_start[c], c1 = a.cell_start[c + 1];
+        if (c0 == c1) continue;   // warp-uniform
+        const int bx = (int)(c % gl0) + 1;
+        const int by = (int)((c / gl0) % gl1) + 1;
+        const int bz = (int)(c / ((long long)gl0 * gl1)) + 1;
+        const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < gl0 ? bx + 1 : gl0;
+        const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < gl1 ? by + 1 : gl1;
+        const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < gl2 ? bz + 1 : gl2;
+        for (int base = c0; base < c1; base += 32) {
+            const int t = base + lane;
+            const bool live = t < c1;
+            double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+            float4 ui = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            int mati = 0, i = 0;
+            if (live) {
+                xi = a.cpos[t];
+                ui = a.cposf[t];
+                mati = a.cmat[t];
+                i = a.cell_list[t];
+            }
+            const float reach = ui.w + hcut;
+            const float reach2 = reach * reach * 1.0009765625f + 9.765625e-4f * csm * csm;
+            unsigned *out = a.nidx + (size_t)(live ? t : 0) * cap;
+            unsigned *cout = contact ? a.cidx + (size_t)(live ? t : 0) * a.cstride : nullptr;
+            int nn = 0, gn = 0, nc = 0, gcn = 0;
+            double mind = 1.0e20;
+            // x extent of the own cell's neighbours: distance to the side columns
+            const float gxl = fmaxf(ui.x, 0.0f), gxr = fmaxf(cs[0] - ui.x, 0.0f);
+            const int passes = (multi && a.prm.contacttype == 0) ? 2 : 1;
+            for (int pass = 0; pass < passes; ++pass) {
+                for (int nz = lo2; nz <= hi2; ++nz) {
+                    const float qz = ui.z + (float)(bz - nz) * cs[2];
+                    const float gz = fmaxf(nz < bz ? ui.z : (nz > bz ? cs[2] - ui.z : 0.0f), 0.0f);
+                    for (int my = lo1; my <= hi1; ++my) {
+                        const float qy = ui.y + (float)(by - my) * cs[1];
+                        const float gy = fmaxf(my < by ? ui.y : (my > by ? cs[1] - ui.y : 0.0f), 0.0f);
+                        const float gyz = gy * gy + gz * gz;
+                        const bool rowok = live && !(gyz > reach2);
+                        if (!__any_sync(0xffffffffu, rowok)) continue;
+                        // per lane: which of the row's cells can hold a neighbour
+                        const bool okl = rowok && !(gyz + gxl * gxl > reach2);
+                        const bool okr = rowok && !(gyz + gxr * gxr > reach2);
+                        const int k0 = key_of(lo0, my, nz);
+                        const int rb = a.cell_start[k0];
+                        const int re = a.cell_start[k0 + (hi0 - lo0) + 1];
+                        const int s1 = a.cell_start[k0 + 1];
+                        const int s2 = (hi0 - lo0 >= 2) ? a.cell_start[k0 + 2] : re;
+                        const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
+                        for (int chunk = rb; chunk < re; chunk += 32) {
+                            const int pc = chunk + lane;
+                            if (pc < re) {
+                                st[lane] = a.cposf[pc];
+                                if (multi) stm[lane] = a.cmat[pc];
+                            }
+                            __syncwarp();
+                            const int m = (re - chunk) < 32 ? (re - chunk) : 32;
+                            if (rowok) {
+                                for (int k = 0; k < m; ++k) {
+                                    const int p = chunk + k;
+                                    const int lx = lo0 + (p >= s1 ? 1 : 0) + (p >= s2 ? 1 : 0);
+                                    if (lx < bx ? !okl : (lx > bx ? !okr : false)) continue;
+                                    const float4 cd4 = st[k];
+                                    const float qx = ui.x + (float)(bx - lx) * cs[0];
+                                    const float dx = qx - cd4.x, dy = qy - cd4.y, dz = qz - cd4.z;
+                                    const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                                    const float hsf = ui.w + cd4.w;
+                                    const float r2f = hsf * hsf;
+                                    if (d2f >= fmaf(r2f, khi, kb)) continue;
+                                    if (p == t) continue;
+                                    double d2 = 0.0;
+                                    if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
+                                        const double4 cd = a.cpos[p];
+                                        d2 = exact_d2(xi, cd);
+                                        const double hs = __dadd_rn(cd.w, xi.w);
+                                        if (!(d2 < __dmul_rn(hs, hs))) continue;
+                                    }
+                                    const unsigned code = (code_yz + (unsigned)(lx - bx + 1)) << 26;
+                                    if (contact) {
+                                        if (stm[k] != mati) {
+                                            if (nc < a.cstride) cout[nc] = (unsigned)p | code;
+                                            ++nc;
+                                            continue;
+                                        }
+                                    } else if (multi && (stm[k] == mati) != (pass == 0)) {
+                                        continue;
+                                    }
+                                    if (want_mind) mind = fmin(mind, d2);
+                                    if (nn < cap) out[nn] = (unsigned)p | code;
+                                    ++nn;
+                                }
+                            }
+                            __syncwarp();
+                        }
+                    }
+                }
+            }
+            // ghosts: only neighbourhoods that reach a ghost layer (warp-uniform test)
+            if (a.prm.boundary && live) {
+                const DevPlanes &pl = a.prm.planes;
+                const bool near = (lo0 == 1 && pl.code[0][0]) || (hi0 == gl0 && pl.code[1][0]) ||
+                                  (lo1 == 1 && pl.code[0][1]) || (hi1 == gl1 && pl.code[1][1]) ||
+                                  (lo2 == 1 && pl.code[0][2]) || (hi2 == gl2 && pl.code[1][2]);
+                if (near) {
+                    const int gpasses = (multi && a.prm.contacttype == 0) ? 2 : 1;
+                    for (int pass = 0; pass < gpasses; ++pass) {
+                        for (int nz = lo2; nz <= hi2; ++nz)
+                            for (int my = lo1; my <= hi1; ++my)
+                                for (int lx = lo0; lx <= hi0; ++lx) {
+                                    const int2 gcl = a.gcell[key_of(lx, my, nz)];
+                                    for (int r = 0; r < gcl.y; ++r) {
+                                        const int q = gcl.x + gcl.y - 1 - r;   // chain order: newest first
+                                        const double4 gq = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
+                                        const double d2 = exact_d2(xi, gq);
+                                        const double hs = __dadd_rn(gq.w, xi.w);
+                                        if (d2 < __dmul_rn(hs, hs)) {
+                                            if (contact) {
+                                                if (a.gmat[q] != mati) {
+                                                    if (gcn < a.gcstride) a.gcont[(size_t)gcn * np + t] = q;
+                                                    ++gcn;
+                                                    continue;
+                                                }
+                                            } else if (multi && (a.gmat[q] == mati) != (pass == 0)) {
+                                                continue;
+                                            }
+                                            mind = fmin(mind, d2);
+                                            if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
+                                            ++gn;
+                                        }
+                                    }
+                                }
+                    }
+                }
+            }
+            if (!live) continue;
+            if (nn > cap) {
+                atomicMax(&a.status->req_stride, nn);
+                raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+            }
+            if (gn > a.gstride) {
+                atomicMax(&a.status->req_gstride, gn);
+                raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+            }
+            if (contact && nc > a.cstride) {
+                atomicMax(&a.status->req_cstride, nc);
+                raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+            }
+            if (contact && gcn > a.gcstride) {
+                atomicMax(&a.status->req_gcstride, gcn);
+                raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+            }
+            mind = sqrt(mind);
+            if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
+            a.nnbr[t] = nn;
+            a.gnnbr[t] = gn;
+            if (contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
+            if (want_mind) a.F.f[FMINDIST][i] = mind;
+            atomicMax(&a.status->max_nbr, nn);
+            atomicMax(&a.status->max_gnbr, gn);
+        }
+    }
+    // particles outside the grid (the last positions) have no neighbours
+    const int first_out = a.cell_start[ncells];
+    for (int t = first_out + blockIdx.x * blockDim.x + threadIdx.x; t < a.n; t += gridDim.x * blockDim.x) {
+        const int nn = with_self ? 1 : 0;
+        a.nnbr[t] = nn;
+        a.gnnbr[t] = 0;
+        if (contact) { a.ncont[t] = 0; a.gncont[t] = 0; }
+        if (want_mind) a.F.f[FMINDIST][a.cell_list[t]] = 1.0e20;
+        atomicMax(&a.status->max_nbr, nn);
+    }
+}
+
 void launch_search(const StepArgs &a, cudaStream_t s) {
     const int threads = search_threads_of(a);
-    if (a.search_kind == 2) {
+    if (a.search_kind == 3) {
+        // grid-stride over the cells (ncells is on the device): up to 16 blocks per SM
+        long long b = (a.cell_cap + kCellWarps - 1) / kCellWarps;
+        if (b > 148LL * 16) b = 148LL * 16;
+        k_search_cell<<<(unsigned)(b < 1 ? 1 : b), kCellWarps * 32, 0, s>>>(a);
+    } else if (a.search_kind == 2) {
         const long long lanes = 32LL * a.n;
         k_search_warp<<<(unsigned)((lanes + threads - 1) / threads), threads, 0, s>>>(a);
     } else {

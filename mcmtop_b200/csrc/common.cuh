@@ -17,6 +17,7 @@ struct DevMaterial {
     double rho, g, av_l, av_q, mass, h, rho_min, rho_max;
     double strinput[48];
     double eosinput[24];
+    double k_cont, n_cont;   // repulsive contact (contacttype > 0)
 };
 
 // Scalars of the time loop kept on the device so that whole steps can be
@@ -34,6 +35,8 @@ struct DevStatus {
     int req_stride;   // neighbour-list entries needed (real part); -1: a row is too long
     int req_gstride;  // neighbour-table width needed (ghost part)
     int req_ngp;      // ghost storage needed
+    int req_cstride;  // contact-list entries needed (real contacts)
+    int req_gcstride; // contact-list entries needed (ghost contacts)
     long long req_cells;
     int bad_index;
     int max_nbr, max_gnbr;
@@ -65,7 +68,8 @@ struct DevParams {
     int asym;         // a material of the cap model is present: the momentum sum reads both triangles of sigma
     int h_opt;        // variable smoothing length (MCM/mcm_update_h.f90): 0 fixed, 1 strain rate, 2 density
     int veloc_opt;    // 1: XSPH velocity smoothing (MCM/mcm_update_velocity.f90:61-87)
-    int contacttype;  // 0: particles of other materials are neighbours (kernel contact); > 0: they are not
+    int contacttype;  // 0: particles of other materials are neighbours (kernel contact); > 0: contacts
+    int contact;      // contacttype > 0 with more than one material: contact lists and repulsion are built
     double drelax_scale, tssf, hmax;
     double base_a[3];
     DevPlanes planes;
@@ -89,6 +93,7 @@ enum Field {
     FL21, FL31, FL32,
     FH0,                                     // initial smoothing length (h_opt 2)
     FXS0, FXS1, FXS2,                        // XSPH velocity sums of the step
+    FRPX, FRPY, FRPZ,                        // repulsive contact acceleration (contacttype > 0)
     NFIELD
 };
 

@@ -54,6 +54,12 @@ struct StepArgs {
     // ghost indices, entry k of p at gnbr[k*npad + p].
     unsigned int *nidx;
     int *gnbr, *nnbr, *gnnbr;
+    // contact lists (prm.contact): particles of other materials, entry k of
+    // position p at cidx[p*cstride + k] (same encoding as nidx), ghost
+    // contacts at gcont[k*npad + p]; counts per position
+    unsigned int *cidx;
+    int *gcont, *ncont, *gncont;
+    int cstride, gcstride;
     double *reorder_tmp;   // npad doubles of scratch for the state permutation
     // gather records
     double4 *rec0, *rec1, *rec2;   // per particle
@@ -66,7 +72,8 @@ struct StepArgs {
     int red_blocks;   // capacity of red in blocks (partial vectors)
     // launch shape, chosen by mcm_gpu_set_tuning or mcm_gpu_autotune (0: default)
     int search_threads;   // threads per block of the neighbour search
-    int search_kind;      // 0 or 1: one thread per particle (k_search); 2: one warp per particle (k_search_warp)
+    int search_kind;      // 0 or 1: one thread per particle (k_search); 2: one warp per particle (k_search_warp);
+                          // 3: one warp per cell (k_search_cell)
     int pair_threads;     // threads per block of the cooperative strain and momentum gathers
     int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for
     double *energy;   // 5*nmat + 3
@@ -84,6 +91,10 @@ void launch_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks);
 void launch_init_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks);
 void launch_energy_bbox_reduce(const StepArgs &a, cudaStream_t s, int nblocks, int energy, int bbox);
 void launch_set_time(const StepArgs &a, cudaStream_t s, double dt, double dtold, int set_dtold);
+// energy partials of several materials in the rows of the momentum kernel's nblocks blocks
+void launch_energy_step_partials(const StepArgs &a, cudaStream_t s, int nblocks);
+// per-material sums of mass x repulsion into out[3*nmat] (device memory)
+void launch_contact_forces(const StepArgs &a, cudaStream_t s, double *out);
 void launch_finish_step(const StepArgs &a, cudaStream_t s);
 
 // step_mixed.cu: FP32 pair sums over FP32 gather records (the constitutive
@@ -124,6 +135,7 @@ void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s);
     void launch_strain(const StepArgs &a, cudaStream_t s);                          \
     int launch_constitutive(const StepArgs &a, cudaStream_t s);                     \
     void launch_mom_prep(const StepArgs &a, cudaStream_t s);                        \
+    void launch_rep_cont(const StepArgs &a, cudaStream_t s);                        \
     int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate);          \
     int launch_update_move(const StepArgs &a, cudaStream_t s);                      \
     int launch_xsph_move(const StepArgs &a, cudaStream_t s);                        \

@@ -47,7 +47,7 @@ __device__ __forceinline__ int sym_index(int k, int l) {
 }
 
 // ---------------------------------------------------------------- density
-// MCM/mcm_rhoupd.f90:119-151
+// MCM/mcm_rhoupd.f90:24-56
 template <typename T, typename Mat>
 __device__ __forceinline__ void rhoupd(PState<T> &P, const Mat &M, T dt, int ndim) {
     P.rhoold = P.rho;
@@ -67,14 +67,14 @@ __device__ __forceinline__ void rhoupd(PState<T> &P, const Mat &M, T dt, int ndi
 }
 
 // --------------------------------------------------------- Jaumann rotation
-// MCM/mcm_stress_rot1.f90:193-355 (iorder = 3, exponential map)
+// MCM/mcm_stress_rot1.f90:35-199 (iorder = 3: the exponential map of :115-184)
 template <typename T>
 __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
     const T etol = T(1.0e-3f);
     const T z1 = T(1.0) / T(3.0), z2 = T(2.0) / T(15.0), z3 = T(17.0) / T(315.0), z4 = T(62.0) / T(2835.0);
     const T s11 = P.sig[T11], s22 = P.sig[T22], s33 = P.sig[T33];
     // the reference reads sigma(1,2), sigma(2,3) and sigma(3,1): the upper
-    // triangle except for (3,1) (MCM/mcm_stress_rot1.f90:40-48, 243-259)
+    // triangle except for (3,1) (MCM/mcm_stress_rot1.f90:40-48, 164-172)
     const T s12 = P.sig[T12], s23 = P.sig[T23], s31 = P.sigl[1];
     T dt2 = T(0.5f) * dt;
     T wzz = -dt2 * P.spin[0];
@@ -137,7 +137,7 @@ __device__ __forceinline__ void sym_lower(PState<T> &P) {
 }
 
 // ------------------------------------------------------------- EOS: sound speed
-// MCM/mcm_eos1c.f90:115-164 (complex c forced to continue)
+// MCM/mcm_eos1c.f90:32-81 (complex c forced to continue)
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos1c(PState<T> &P, const Mat &M) {
     const auto &ei = M.eosinput;
@@ -188,7 +188,7 @@ __device__ __forceinline__ void eos4c(PState<T> &P, const Mat &M) {
     else P.c = sqrt(fabs(c_sq));
 }
 
-// MCM/mcm_eos13c.f90:219-227
+// MCM/mcm_eos13c.f90:29-37
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos13c(PState<T> &P, const Mat &M) {
     T gamma = T(M.eosinput[0]);
@@ -196,14 +196,14 @@ __device__ __forceinline__ void eos13c(PState<T> &P, const Mat &M) {
     P.c = sqrt((gamma - T(1.0)) * gamma * e1);
 }
 
-// MCM/mcm_eos28c.f90:305-310
+// MCM/mcm_eos28c.f90:28-33
 template <typename T, typename Mat>
 __device__ __forceinline__ void eos28c(PState<T> &P, const Mat &M) {
     T b = T(M.eosinput[0]), gamma = T(M.eosinput[1]);
     P.c = sqrt(b * gamma / P.rho0);
 }
 
-// MCM/mcm_eos41c.f90:240-294.  Returns false when c^2 < 0 (the reference stops).
+// MCM/mcm_eos41c.f90:31-85.  Returns false when c^2 < 0 (the reference stops).
 template <typename T, typename Mat>
 __device__ __forceinline__ bool eos41c(PState<T> &P, const Mat &M) {
     const auto &ei = M.eosinput;
@@ -234,7 +234,7 @@ __device__ __forceinline__ bool eos41c(PState<T> &P, const Mat &M) {
     return !(c2 < T(0.0));
 }
 
-// MCM/mcm_sueos.f90:185-207
+// MCM/mcm_sueos.f90:24-46
 template <typename T, typename Mat>
 __device__ __forceinline__ bool sueos(PState<T> &P, const Mat &M) {
     switch (M.eos) {
@@ -269,7 +269,7 @@ __device__ __forceinline__ void eqos1(PState<T> &P, const Mat &M, T dt) {
     }
 }
 
-// MCM/mcm_eqos4.f90:131-183
+// MCM/mcm_eqos4.f90:30-82
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos4(PState<T> &P, const Mat &M, T dt) {
     const auto &ei = M.eosinput;
@@ -298,7 +298,7 @@ __device__ __forceinline__ void eqos4(PState<T> &P, const Mat &M, T dt) {
     }
 }
 
-// MCM/mcm_eqos13.f90:258-274
+// MCM/mcm_eqos13.f90:30-46
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos13(PState<T> &P, const Mat &M) {
     T gamma_m1 = T(M.eosinput[0]) - T(1.0);
@@ -308,7 +308,7 @@ __device__ __forceinline__ void eqos13(PState<T> &P, const Mat &M) {
     P.e = P.etry - T(0.5) * dvol * P.p;
 }
 
-// MCM/mcm_eqos28.f90:343-358
+// MCM/mcm_eqos28.f90:30-45
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos28(PState<T> &P, const Mat &M) {
     T b = T(M.eosinput[0]), gamma = T(M.eosinput[1]);
@@ -344,7 +344,7 @@ __device__ __forceinline__ void eqos41(PState<T> &P, const Mat &M, T dt) {
     P.p = pn;
 }
 
-// MCM/mcm_eqos.f90:183-214
+// MCM/mcm_eqos.f90:24-55
 template <typename T, typename Mat>
 __device__ __forceinline__ void eqos(PState<T> &P, const Mat &M, T dt) {
     switch (M.eos) {
@@ -427,7 +427,7 @@ __device__ __forceinline__ void eos41p(PState<T> &P, const Mat &M, T dt) {
 }
 
 // ------------------------------------------------- artificial viscosity
-// MCM/mcm_nodalav.f90:76-91 (q is isotropic: only the diagonal is stored)
+// MCM/mcm_nodalav.f90:32-47 (q is isotropic: only the diagonal is stored)
 template <typename T, typename Mat>
 __device__ __forceinline__ void nodalav(PState<T> &P, const Mat &M) {
     P.q = T(0.0);
@@ -444,7 +444,7 @@ __device__ __forceinline__ void aviscosity(PState<T> &P, const Mat &M) {
 }
 
 // ---------------------------------------------------------- energy updates
-// MCM/mcm_hieupd.f90:119-156; de(k,l) summed in column-major order
+// MCM/mcm_hieupd.f90:27-64; de(k,l) summed in column-major order
 template <typename T>
 __device__ __forceinline__ void hieupd(PState<T> &P, T dt) {
     const T othird = T(1.0) / T(3.0);
@@ -472,7 +472,7 @@ __device__ __forceinline__ void hieupd(PState<T> &P, T dt) {
     P.etry = P.e + dt * eincr - mean_incr;
 }
 
-// MCM/mcm_lieupd.f90:283-290 (dot product in column-major order)
+// MCM/mcm_lieupd.f90:26-33 (dot product in column-major order)
 template <typename T>
 __device__ __forceinline__ void lieupd(PState<T> &P, T dt) {
     T qpm = T(0.0);
@@ -486,7 +486,7 @@ __device__ __forceinline__ void lieupd(PState<T> &P, T dt) {
     P.e = P.e + (P.einc - dt * qpm) * P.mass / P.rho;
 }
 
-// MCM/mcm_stress_up.f90:245-253
+// MCM/mcm_stress_up.f90:28-36
 template <typename T>
 __device__ __forceinline__ void stress_up(PState<T> &P) {
     P.sig[T11] = P.s[T11] - P.p;
@@ -527,7 +527,7 @@ __device__ __forceinline__ void f3dm1(PState<T> &P, const Mat &M, T dt) {
     P.p = -othird * (s[T11] + s[T22] + s[T33]);
 }
 
-// MCM/mcm_f3dm3.f90:106-233
+// MCM/mcm_f3dm3.f90:31-156
 template <typename T, typename Mat>
 __device__ __forceinline__ void f3dm3(PState<T> &P, const Mat &M, T dt) {
     const T othird = T(1.0) / T(3.0);
@@ -584,7 +584,7 @@ __device__ __forceinline__ void f3dm3(PState<T> &P, const Mat &M, T dt) {
                          T(2.0f) * (r[T12] * sg[T12] + r[T13] * sg[T13] + r[T23] * sg[T23])) * dt + P.einc);
 }
 
-// MCM/mcm_f3dm9.f90:261-285 (s(1,2) is never assigned; xmu = cm(2,mat))
+// MCM/mcm_f3dm9.f90:26-48 (s(1,2) is never assigned; xmu = cm(2,mat))
 template <typename T, typename Mat>
 __device__ __forceinline__ void f3dm9(PState<T> &P, const Mat &M) {
     const T othird = T(1.0) / T(3.0);

@@ -81,6 +81,73 @@ __global__ void k_energy_bbox_reduce(StepArgs a, int nblocks, int energy, int bb
     }
 }
 
+// Per-material block partials of the energy sums (MCM/mcm_calctotale.f90:
+// 33-51) for bodies of several materials, enqueued before the cooperative
+// momentum kernels, which then move particles and write only the bounding-box
+// partials of the same rows.  Block b sums, material by material, particles
+// b*T + tid + k*nblocks*T (T threads) and combines its threads in a fixed
+// order, so the sums do not depend on scheduling.
+__global__ void k_energy_step_partials(StepArgs a) {
+    __shared__ double sm[32];
+    if (a.status->code || a.time->ended >= 2) return;
+    const int nv = 5 * a.nmat + 6;
+    double *out = a.red + (size_t)blockIdx.x * nv;
+    const double *const *f = a.F.f;
+    for (int m = 1; m <= a.nmat; ++m) {
+        double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+            if (a.F.mat[i] != m) continue;
+            const double mass = f[FMASS][i], vabs = f[FVABS][i];
+            acc[0] += 0.5 * mass * (vabs * vabs);
+            acc[1] += f[FE][i];
+            acc[2] += mass * fabs(f[FVX][i]);
+            acc[3] += mass * fabs(f[FVY][i]);
+            acc[4] += mass * fabs(f[FVZ][i]);
+        }
+        for (int c = 0; c < 5; ++c) {
+            double x = acc[c];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = x;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double r = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sm[w];
+                out[5 * (m - 1) + c] = r;
+            }
+        }
+    }
+}
+
+// Per-material contact forces xcf, ycf, zcf (MCM/mcm_oldacceleration.f90:
+// 52-55): one block per material sums mass x repulsion over the particles in
+// state order, threads combined in a fixed order.
+__global__ void k_contact_forces(StepArgs a, double *out) {
+    __shared__ double sm[32];
+    const int m = blockIdx.x + 1;
+    const double *const *f = a.F.f;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
+        if (a.F.mat[i] != m) continue;
+        const double mass = f[FMASS][i];
+        acc[0] += mass * f[FRPX][i];
+        acc[1] += mass * f[FRPY][i];
+        acc[2] += mass * f[FRPZ][i];
+    }
+    for (int c = 0; c < 3; ++c) {
+        double x = acc[c];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sm[w];
+            out[3 * (m - 1) + c] = r;
+        }
+    }
+}
+
 // Totals after the per-material sums (MCM/mcm_calctotale.f90:53-60).
 __global__ void k_energy_totals(StepArgs a) {
     if (a.status->code || a.time->ended >= 2) return;
@@ -117,6 +184,14 @@ void launch_init_critts_reduce(const StepArgs &a, cudaStream_t s, int nblocks) {
 void launch_energy_bbox_reduce(const StepArgs &a, cudaStream_t s, int nblocks, int energy, int bbox) {
     k_energy_bbox_reduce<<<5 * a.nmat + 6, 256, 0, s>>>(a, nblocks, energy, bbox);
     if (energy) k_energy_totals<<<1, 1, 0, s>>>(a);
+}
+
+void launch_energy_step_partials(const StepArgs &a, cudaStream_t s, int nblocks) {
+    k_energy_step_partials<<<nblocks, 256, 0, s>>>(a);
+}
+
+void launch_contact_forces(const StepArgs &a, cudaStream_t s, double *out) {
+    k_contact_forces<<<a.nmat, 256, 0, s>>>(a, out);
 }
 
 void launch_set_time(const StepArgs &a, cudaStream_t s, double dt, double dtold, int set_dtold) {

@@ -323,6 +323,9 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
     if (live && lane == 0) {
         const int i = a.cell_list[t];
         double *const *f = a.F.f;
+        if (a.prm.contact)   // repulsive contact (MCM/mcm_oldacceleration.f90:49-51)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[j] = acc[j] + f[FRPX + j][i];
         if (a.prm.baseaccel)
 #pragma unroll
             for (int j = 0; j < 3; ++j) acc[j] = acc[j] + a.prm.base_a[j];
@@ -341,11 +344,11 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
         const double mass = f[FMASS][i], vabs = f[FVABS][i];
         const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),
                                 mass * fabs(f[FVY][i]), mass * fabs(f[FVZ][i])};
-        if (mati == 1) {
+        // one material: sums in registers; several: k_energy_step_partials
+        // summed them in a fixed order before this kernel moved anything
+        if (nm == 1) {
 #pragma unroll
             for (int c = 0; c < 5; ++c) e1[c] += vals[c];
-        } else {
-            for (int c = 0; c < 5; ++c) atomicAdd(&a.red[(size_t)blockIdx.x * (5 * nm + 6) + 5 * (mati - 1) + c], vals[c]);
         }
         if (do_int) {
             double xn[3];
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
     }
     const int stride = 5 * nm + 6;
     double *out = a.red + (size_t)blockIdx.x * stride;
-    {
+    if (nm == 1) {
         double v[5];
 #pragma unroll
         for (int c = 0; c < 5; ++c) v[c] = block_sum(e1[c], sm);

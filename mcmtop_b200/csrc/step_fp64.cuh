@@ -27,7 +27,7 @@ constexpr double kPi = 3.141592653589793;   // acos(-1) (MCM/mcm_startup.f90:33)
 // momentum and energy part, as MCM/mcm_solution.f90:69-101 does.
 __device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->code || a.time->ended >= 2; }
 
-// Cubic B-spline gradient, 3-D (MCM/mcm_gradw.f90:321-383), xij = xi - xj.
+// Cubic B-spline gradient, 3-D (MCM/mcm_gradw.f90:41-103), xij = xi - xj.
 __device__ __forceinline__ void gradw(double x0, double x1, double x2, double havg, double &d0, double &d1,
                                       double &d2) {
 #if MCM_EXACT
@@ -67,7 +67,7 @@ __device__ __forceinline__ void gradw(double x0, double x1, double x2, double ha
 #endif
 }
 
-// Cubic B-spline kernel, 3-D (MCM/mcm_kernel.f90:227-280).
+// Cubic B-spline kernel, 3-D (MCM/mcm_kernel.f90:42-95).
 __device__ __forceinline__ double kernelw(double x0, double x1, double x2, double havg) {
 #if MCM_EXACT
     double const1 = 1.0 / (kPi * havg * havg * havg);
@@ -91,7 +91,7 @@ __device__ __forceinline__ double kernelw(double x0, double x1, double x2, doubl
 #endif
 }
 
-// 3x3 inverse with the reference's singular fallback (MCM/mcm_math_func.f90:199-228).
+// 3x3 inverse with the reference's singular fallback (MCM/mcm_math_func.f90:50-79).
 __device__ __forceinline__ void inverse3(const double M[3][3], double inv[3][3]) {
     double sd00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
     double sd01 = M[1][0] * M[2][2] - M[1][2] * M[2][0];
@@ -167,7 +167,7 @@ __device__ __forceinline__ void store_state(const StepArgs &a, int i, const PSta
         for (int t = 0; t < 6; ++t) f[FA11 + t][i] = P.alfa[t];
     }
     if (a.prm.diag) {
-        // rhoupd may have changed rod and the trace (MCM/mcm_rhoupd.f90:130-151)
+        // rhoupd may have changed rod and the trace (MCM/mcm_rhoupd.f90:35-56)
         f[FR11][i] = P.rod[T11]; f[FR22][i] = P.rod[T22]; f[FR33][i] = P.rod[T33];
         f[FTR][i] = P.tracerod; f[FETRY][i] = P.etry; f[FEINC][i] = P.einc; f[FRHOOLD][i] = P.rhoold;
     }
@@ -175,7 +175,7 @@ __device__ __forceinline__ void store_state(const StepArgs &a, int i, const PSta
 
 // ------------------------------------------------------------ strain prep
 // Gather records for the strain loop: positions shifted back half a step
-// (MCM/mcm_strain.f90:27-31) and V_j = m_j/rho_j (MCM/mcm_oldstrain.f90:105).
+// (MCM/mcm_strain.f90:27-31) and V_j = m_j/rho_j (MCM/mcm_oldstrain.f90:44).
 // Ghosts keep their unshifted positions, as in the reference.
 __global__ void k_strain_prep(StepArgs a) {
     if (skip_step(a)) return;
@@ -203,7 +203,7 @@ template <int DISC>
 __device__ __forceinline__ void strain_gather(const StepArgs &a, const DevGrid &g, int t, const double4 xi,
                                               const double4 vi, double gv[3][3]) {
     if (DISC == 0) {
-        // MCM/mcm_oldstrain.f90:95-115
+        // MCM/mcm_oldstrain.f90:34-54
         auto body = [&](const double4 xj, const double4 vj) {
             double Volj = vj.w;
             double havg = 0.5 * (xi.w + xj.w);
@@ -382,9 +382,76 @@ __global__ void __launch_bounds__(kRedThreads) k_constitutive(StepArgs a) {
     if (threadIdx.x == 0) a.red[blockIdx.x] = m;
 }
 
+// ------------------------------------------------------ repulsive contact
+// MCM/mcm_rep_contact.f90:37-161 with MCM/mcm_get_j_cont_info.f90:31-58
+// (contacttype > 0, called by MCM/mcm_solution.f90:64 before mcm_momentum):
+// Monaghan's repulsive acceleration -sum_j m_j (K_i + K_j) f_ij^n grad W_ij
+// over the particle's real contacts and then its ghost contacts, for
+// particles with at least one real contact (:41); zero for the others.
+// Positions are the state's after the strain half-step round trip, ghosts'
+// from their creation, as in the reference.  Ghost contacts come from the
+// ghost contact list (the reference reads their ids from the real contact
+// list past ncont, :48 of mcm_get_j_cont_info.f90, entries no search wrote).
+__global__ void k_rep_cont(StepArgs a) {
+    if (skip_step(a)) return;
+    double *const *f = a.F.f;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.n; t += gridDim.x * blockDim.x) {
+        const int i = a.cell_list[t];
+        double r[3] = {0.0, 0.0, 0.0};
+        const int nc = a.ncont[t];
+        if (nc > 0) {
+            const DevMaterial &M = a.mats[a.F.mat[i] - 1];
+            const double ki = M.k_cont, n = M.n_cont;
+            const double xi0 = f[FX][i], xi1 = f[FY][i], xi2 = f[FZ][i], hi = f[FH][i];
+            const unsigned *list = a.cidx + (size_t)t * a.cstride;
+            const int total = nc + a.gncont[t];
+            for (int k = 0; k < total; ++k) {
+                double xj0, xj1, xj2, hj, mj, kj;
+                if (k < nc) {
+                    const int j = a.cell_list[list[k] & kPosMask];
+                    xj0 = f[FX][j]; xj1 = f[FY][j]; xj2 = f[FZ][j];
+                    hj = f[FH][j]; mj = f[FMASS][j];
+                    kj = a.mats[a.F.mat[j] - 1].k_cont;
+                } else {
+                    const int q = a.gcont[(size_t)(k - nc) * a.npad + t];
+                    xj0 = a.gx[q]; xj1 = a.gy[q]; xj2 = a.gz[q];
+                    hj = a.gh[q]; mj = a.gmass[q];
+                    kj = a.mats[a.gmat[q] - 1].k_cont;
+                }
+                const double havg = 0.5 * (hi + hj);
+                // inverse of W at the particle spacing, cubic B-spline (:55-68)
+                const double ratio = hj / havg;
+                double inv_w;
+                if (ratio < 1.0) inv_w = 1.0 / (((0.75 * ratio - 1.5) * ratio) * ratio + 1.0);
+                else { const double u = 2.0 - ratio; inv_w = 1.0 / (u * u * u); }
+                const double d0 = xi0 - xj0, d1 = xi1 - xj1, d2 = xi2 - xj2;
+                double g0, g1, g2;
+                gradw(d0, d1, d2, havg, g0, g1, g2);
+                // mcm_calc_fij (:129-154); its velocity term is unused
+                double rad = d0 * d0;
+                rad = rad + d1 * d1;
+                rad = rad + d2 * d2;
+                rad = sqrt(rad);
+                const double z = rad / havg;
+                double fij;
+                if (z < 1.0) fij = inv_w * (((0.75 * z - 1.5) * z) * z + 1.0);
+                else if (z < 2.0) { const double u = 2.0 - z; fij = 0.25 * inv_w * (u * u * u); }
+                else fij = 0.0;
+                const double mk = mj * ((ki + kj) * pow(fij, n));
+                r[0] = r[0] - mk * g0;
+                r[1] = r[1] - mk * g1;
+                r[2] = r[2] - mk * g2;
+            }
+        }
+        f[FRPX][i] = r[0];
+        f[FRPY][i] = r[1];
+        f[FRPZ][i] = r[2];
+    }
+}
+
 // --------------------------------------------------------- momentum prep
 // Gather records: x, h; (sigma - q)/rho^2 (MCM/mcm_oldacceleration.f90:79-80);
-// mass.  Ghost stresses follow MCM/mcm_update_ghost_stress.f90:272-285 (all
+// mass.  Ghost stresses follow MCM/mcm_update_ghost_stress.f90:28-41 (all
 // off-diagonals negated) with the ghost's own density from its creation.
 __global__ void k_mom_prep(StepArgs a) {
     if (skip_step(a)) return;
@@ -628,6 +695,10 @@ __global__ void __launch_bounds__(kRedThreads) k_momentum(StepArgs a, int integr
         const int i = a.cell_list[t];
         double *const *f = a.F.f;
         const DevGrid g = *a.grid;
+        // MCM/mcm_oldacceleration.f90:49-51, mcm_corr_acceleration.f90:45-49
+        if (a.prm.contact)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[j] = acc[j] + f[FRPX + j][i];
         momentum_gather<DISC>(a, g, t, acc);
         if (a.prm.baseaccel)
 #pragma unroll
@@ -970,6 +1041,8 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
     k_mom_prep<<<gs_blocks(a.n > a.ghost_cap ? a.n : a.ghost_cap), 256, 0, s>>>(a);
 }
 
+void launch_rep_cont(const StepArgs &a, cudaStream_t s) { k_rep_cont<<<gs_blocks(a.n), 256, 0, s>>>(a); }
+
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
 #if MCM_EXACT
     int blocks = nblk(a.n, kRedThreads);
@@ -979,7 +1052,7 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
 #else
     constexpr int L = kCoopLanes;
     const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
-    if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
+    if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
     if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, threads, 0, s>>>(a, integrate);
     else k_momentum_coop<L, 1><<<blocks, threads, 0, s>>>(a, integrate);
     return blocks;

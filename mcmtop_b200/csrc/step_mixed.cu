@@ -105,7 +105,7 @@ __device__ __forceinline__ Rec8 ld_rec8(const float4 *p) {
 }
 __device__ __forceinline__ float4 ld_rec4(const float4 *p) { return __ldg(p); }
 
-// Cubic B-spline gradient in FP32 (MCM/mcm_gradw.f90:341-381), ih = 1/havg.
+// Cubic B-spline gradient in FP32 (MCM/mcm_gradw.f90:64-101), ih = 1/havg.
 __device__ __forceinline__ void gradw_f(float x0, float x1, float x2, float ih, float &d0, float &d1, float &d2) {
     const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
     if (r2 == 0.0f) { d0 = d1 = d2 = 0.0f; return; }
@@ -152,7 +152,7 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 // ----------------------------------------------------------- strain rate
-// MCM/mcm_oldstrain.f90:95-124 with FP32 pair sums.
+// MCM/mcm_oldstrain.f90:34-64 with FP32 pair sums.
 __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
     __shared__ float4 offs[27];
     if (skip_step(a)) return;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
 #pragma unroll
         for (int u = 0; u < 9; ++u) r[u] = lane_sum(gv[u]);
         if (live && lane == 0) {
-            // MCM/mcm_oldstrain.f90:117-124
+            // MCM/mcm_oldstrain.f90:56-63
             double *const *f = a.F.f;
             f[FR11][i] = r[0];
             f[FR22][i] = r[4];
@@ -424,6 +424,9 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
         for (int c = 0; c < 3; ++c) ac[c] = lane_sum(acc[c]);
         if (live && lane == 0) {
             double *const *f = a.F.f;
+            if (a.prm.contact)   // repulsive contact (MCM/mcm_oldacceleration.f90:49-51)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) ac[j] = ac[j] + f[FRPX + j][i];
             if (a.prm.baseaccel)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) ac[j] = ac[j] + a.prm.base_a[j];
@@ -442,12 +445,11 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
             const double mass = f[FMASS][i], vabs = f[FVABS][i];
             const double vals[5] = {0.5 * mass * (vabs * vabs), f[FE][i], mass * fabs(f[FVX][i]),
                                     mass * fabs(f[FVY][i]), mass * fabs(f[FVZ][i])};
-            if (mati == 1) {
+            // one material: sums in registers; several: k_energy_step_partials
+            // summed them in a fixed order before this kernel moved anything
+            if (nm == 1) {
 #pragma unroll
                 for (int c = 0; c < 5; ++c) e1[c] += vals[c];
-            } else {
-                for (int c = 0; c < 5; ++c)
-                    atomicAdd(&a.red[(size_t)blockIdx.x * (5 * nm + 6) + 5 * (mati - 1) + c], vals[c]);
             }
             if (do_int) {
                 double xn[3];
@@ -460,12 +462,14 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
     }
     const int stride = 5 * nm + 6;
     double *out = a.red + (size_t)blockIdx.x * stride;
-    double v[5];
+    if (nm == 1) {
+        double v[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) v[c] = block_sum(e1[c], sm);
-    if (threadIdx.x == 0)
+        for (int c = 0; c < 5; ++c) v[c] = block_sum(e1[c], sm);
+        if (threadIdx.x == 0)
 #pragma unroll
-        for (int c = 0; c < 5; ++c) out[c] = v[c];
+            for (int c = 0; c < 5; ++c) out[c] = v[c];
+    }
     if (do_int) {
         for (int d = 0; d < 3; ++d) {
             const double lo = block_minmax(xlo[d], sm, false);
@@ -495,7 +499,7 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
     const int blocks = pair_blocks_of(a, L);
-    if (a.nmat > 1) cudaMemsetAsync(a.red, 0, sizeof(double) * blocks * (5 * a.nmat + 6), s);
+    if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
     k_momentum<<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
     return blocks;
 }

@@ -134,7 +134,7 @@ def copper_model10(h: float, yield_stress: float = 400e6, hardening: float = 100
     """Copper-like elastic-plastic hydrodynamic material (model 10) with the
     Mie-Grueneisen EOS (41); SI arguments, cm-g-us card values; h in cm.  strinput follows MCM/mcm_f3dm10.f90:29-36
     (G, yield, plastic modulus, cutoff, a1, a2, spall, failure strain);
-    eosinput follows MCM/mcm_eos41c.f90:240-245 (c0, s, cv, T0, gamma0, v0)."""
+    eosinput follows MCM/mcm_eos41c.f90:31-36 (c0, s, cv, T0, gamma0, v0)."""
     m = MaterialCard(model=10, eos=41, rho=rho0 * RHO, av_l=0.06, av_q=1.5, h=h)
     m.strinput[0] = shear * PRESS
     m.strinput[1] = yield_stress * PRESS
@@ -188,6 +188,33 @@ def taylor_bar(dx: float = 0.4e-3, radius: float = 3.2e-3, length: float = 32.4e
                 sym_flag=(0, 0, 0, 0, 1, 0), sym_x=(0.0,) * 6, materials=[mat], x=x, v=v,
                 mat=np.ones(npart, dtype=np.int32), dispbc=np.zeros(npart, dtype=np.int32),
                 name=f"taylor_bar_dx{dx * 1e3:g}mm_n{npart}")
+
+
+def two_material_bar(dx: float = 0.8e-3, contacttype: int = 0, k_cont: float = 1.0e-3, n_cont: float = 4.0,
+                     yields=(400e6, 250e6), **kw) -> Deck:
+    """A Taylor bar whose lower half is material 1 and upper half material 2
+    (the same copper-like model 10 + EOS 41 with the yield stresses `yields`).
+    With contacttype 0 the halves are each other's neighbours (kernel
+    contact); with contacttype > 0 they interact only through Monaghan's
+    repulsive force, with the contact cards' strength K and exponent n for
+    both materials (MCM/mcm_contactype.f90:32-39, cm-g-us units: K in
+    (cm/us)^2).  Other arguments as taylor_bar."""
+    d = taylor_bar(dx=dx, **kw)
+    upper = d.x[:, 2] > 0.5 * (d.x[:, 2].min() + d.x[:, 2].max())
+    mat = np.where(upper, 2, 1).astype(np.int32)
+    dxc = dx * CM
+    mats = []
+    for k, ys in ((1, yields[0]), (2, yields[1])):
+        m1 = d.materials[0]
+        m = dataclasses.replace(m1, strinput=m1.strinput.copy(), eosinput=m1.eosinput.copy())
+        m.strinput[1] = ys * PRESS
+        m.mass = m.rho * int((mat == k).sum()) * dxc ** 3
+        mats.append(m)
+    extra = {}
+    if contacttype > 0:
+        extra = dict(ncontmats=-1, cont_opt=0, k_cont=(k_cont, k_cont), n_cont=(n_cont, n_cont))
+    return d.replace(materials=mats, mat=mat, contacttype=contacttype,
+                     name=f"two_material_bar_dx{dx * 1e3:g}mm_n{d.np}_ct{contacttype}", **extra)
 
 
 def sand_model4(h: float, bulk: float = 1.0e9, shear: float = 0.6e9, alpha: float = 10e6, theta: float = 0.1,

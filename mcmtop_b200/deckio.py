@@ -15,7 +15,7 @@ defaults left to the solver set-up, order checks and error conditions:
                                    boundary planes
 * MCM/mcm_contactype.f90:27-47     contact cards
 * MCM/mcm_baseaccel_in.f90:23-33   base accelerations
-* MCM/mcm_gttxsg.f90:20-37         card reader: lines whose first column is
+* MCM/mcm_gttxsg.f90:22-31         card reader: lines whose first column is
                                    ``*`` or ``$`` are comments
 
 The writer produces version-2 decks that the reference reads back: every

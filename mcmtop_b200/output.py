@@ -190,15 +190,16 @@ class Outputs:
         self._init_timehist()
         self.timehist(ptime, state, energies)
 
-    def after_energies(self, ptime: float, state: dict, energies: np.ndarray) -> None:
-        """MCM/mcm_solution.f90:81-92, called after mcm_calctotale."""
+    def after_energies(self, ptime: float, state: dict, energies: np.ndarray, contact_forces=None) -> None:
+        """MCM/mcm_solution.f90:81-92, called after mcm_calctotale; contact_forces
+        (nmat, 3) are the step's mcm_mat%xcf, %ycf, %zcf (zero when omitted)."""
         st, th = self.due(ptime)
         self.ptime = ptime
         if st:
             self.state_output(state)
             self.nextsttime += self.deck.stpltime
         if th:
-            self.timehist(ptime, state, energies)
+            self.timehist(ptime, state, energies, contact_forces)
             self.nextthtime += self.deck.thpltime
 
     # ---------------------------------------------------------- states
@@ -263,12 +264,15 @@ class Outputs:
             self._put(self.base + "_ptrn.csv", title + "Time,Pressure transducer time histories\n")
             self._put(self.base + "_vtrn.csv", title + "Time,Velocity transducer time histories\n")
 
-    def timehist(self, ptime: float, state: dict, energies: np.ndarray) -> None:
-        """MCM/mcm_timehist.f90:41-64 and the 3D rows of :112-140."""
+    def timehist(self, ptime: float, state: dict, energies: np.ndarray, contact_forces=None) -> None:
+        """MCM/mcm_timehist.f90:41-64 and the 3D rows of :112-140.  The contact
+        forces of each material (xcf, ycf, zcf) are zero before the first
+        momentum sum and without repulsive contact."""
         row = [ptime]
+        cf = np.zeros((self.nummat, 3)) if contact_forces is None else np.asarray(contact_forces)
         for m in range(self.nummat):
             ke, ie = energies[5 * m], energies[5 * m + 1]
-            row += [ke, ie, 0.0, 0.0, 0.0]       # contact forces: no contact in this step
+            row += [ke, ie, float(cf[m, 0]), float(cf[m, 1]), float(cf[m, 2])]
         self._put(self.base + "_thist.csv", "".join("," + fmt_e(a, 14, 6) for a in row) + "\n", "a")
         if self.deck.transducers:
             self._transducers(ptime, state)

@@ -94,7 +94,8 @@ class Program:
         st, th = self.out.due(s.ptime)
         fields = self.out.fields(st, th)
         if st or th:
-            self.out.after_energies(s.ptime, self._state(fields), s.energies)
+            cf = s.contact_forces() if (th and self.deck.contacttype > 0) else None
+            self.out.after_energies(s.ptime, self._state(fields), s.energies, cf)
         if st:
             self._say(state_line(s.ptime))
         if s.timestep % self.status_interval == 0:

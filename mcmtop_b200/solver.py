@@ -43,6 +43,9 @@ def material_table(deck: Deck) -> "C.Array":
         for i in range(24):
             m.eosinput[i] = float(card.eosinput[i])
         check(lib.mcm_gpu_material_from_deck(C.byref(m)), "mcm_gpu_material_from_deck")
+        # contact cards (MCM/mcm_contactype.f90:32-39): K and n per material
+        if deck.contacttype > 0 and k < len(deck.k_cont):
+            m.k_cont, m.n_cont = float(deck.k_cont[k]), float(deck.n_cont[k])
     return mats
 
 
@@ -223,6 +226,28 @@ class Solver:
                                           C.byref(gs)), "mcm_gpu_neighbours", self.h)
         return nn, nbr, gn, gnbr
 
+    def contacts(self):
+        """(ncont, cont[np, stride], g_ncont, g_cont[np, g_stride]) with 1-based ids:
+        the contact lists of the last search (contacttype > 0)."""
+        nc = np.zeros(self.n, dtype=np.int32)
+        gc = np.zeros(self.n, dtype=np.int32)
+        s, gs = C.c_int(0), C.c_int(0)
+        check(self.lib.mcm_gpu_contacts(self.h, _iptr(nc), None, C.byref(s), _iptr(gc), None, C.byref(gs)),
+              "mcm_gpu_contacts", self.h)
+        stride, gstride = max(1, s.value), max(1, gs.value)
+        cont = np.zeros((self.n, stride), dtype=np.int32)
+        gcont = np.zeros((self.n, gstride), dtype=np.int32)
+        s, gs = C.c_int(stride), C.c_int(gstride)
+        check(self.lib.mcm_gpu_contacts(self.h, _iptr(nc), _iptr(cont), C.byref(s), _iptr(gc), _iptr(gcont),
+                                        C.byref(gs)), "mcm_gpu_contacts", self.h)
+        return nc, cont, gc, gcont
+
+    def contact_forces(self) -> np.ndarray:
+        """Per-material contact forces (xcf, ycf, zcf) of the last step_b, shape (nmat, 3)."""
+        out = np.zeros(3 * self.nmat)
+        check(self.lib.mcm_gpu_contact_forces(self.h, _dptr(out)), "mcm_gpu_contact_forces", self.h)
+        return out.reshape(self.nmat, 3)
+
     def ghosts(self):
         n = C.c_int()
         check(self.lib.mcm_gpu_ghosts(self.h, C.byref(n), None, None, None, 0), "mcm_gpu_ghosts", self.h)
@@ -283,7 +308,7 @@ class Solver:
 
     def set_tuning(self, search_threads: int = 0, pair_threads: int = 0, pair_blocks_per_sm: int = 0,
                    nbr_stride: int = 0, search_kind: int = 0) -> None:
-        """search_kind 1: one thread per particle, 2: one warp per particle."""
+        """search_kind 1: one thread per particle, 2: one warp per particle, 3: one warp per cell."""
         t = _abi.Tuning(search_threads, pair_threads, pair_blocks_per_sm, nbr_stride, search_kind, 0.0)
         check(self.lib.mcm_gpu_set_tuning(self.h, C.byref(t)), "mcm_gpu_set_tuning", self.h)
 

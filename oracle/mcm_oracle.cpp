@@ -47,6 +47,7 @@ struct Material {
     real rho = 0, g = 0, av_l = 0, av_q = 0, mass = 0, h = 0, rho_min = 0, rho_max = 0;
     real ke = 0, ie = 0, xcf = 0, ycf = 0, zcf = 0;
     real mom[3] = {0, 0, 0};
+    real k_cont = 0, n_cont = 0;   // contact cards (MCM/mcm_contactype.f90:35)
     real strinput[48];
     real strinput2[48];
     real eosinput[24];
@@ -64,6 +65,7 @@ struct Particle {
     real epx[6] = {0, 0, 0, 0, 0, 0};
     real alfa[3][3] = {};
     real x[3] = {0, 0, 0}, xzero[3] = {0, 0, 0}, v[3] = {0, 0, 0}, a[3] = {0, 0, 0};
+    real repulsion[3] = {0, 0, 0};   // contact acceleration (MCM/mcm_database.f90:206)
     real rod[3][3] = {}, spin[3][3] = {}, sigma[3][3] = {}, s[3][3] = {}, q[3][3] = {},
          qold[3][3] = {}, qq[3][3] = {};
     std::vector<int> nbr, cont, gnbr, gcont;
@@ -175,6 +177,10 @@ struct Sim {
     void stress_up(int i);
     void lieupd(int i);
     void calccritts();
+    // repulsive contact (contacttype > 0)
+    void rep_cont();
+    real calc_fij(const real *xi, const real *xj, real havg, real inv_w_deltap) const;
+    void get_j_cont_info(int i, int k, real *x, real &mass, real &rho, real &h, real &kj) const;
     // momentum
     void momentum();
     void update_ghost_stress();
@@ -320,6 +326,7 @@ int Sim::setup(const mcmo_deck *d, const mcmo_material *m, const double *x, cons
         M.model = s.model; M.eos = s.eos; M.visc_type = s.visc_type;
         M.rho = s.rho; M.av_l = s.av_l; M.av_q = s.av_q; M.mass = s.mass; M.h = s.h;
         M.rho_min = s.rho_min; M.rho_max = s.rho_max;
+        M.k_cont = s.k_cont; M.n_cont = s.n_cont;
         for (int k = 0; k < 48; ++k) { M.strinput[k] = s.strinput[k]; M.strinput2[k] = 0; }
         for (int k = 0; k < 24; ++k) M.eosinput[k] = s.eosinput[k];
         if (M.visc_type == 0) M.visc_type = 1;
@@ -633,7 +640,7 @@ void Sim::init_h() {
     for (int i = 1; i <= np; ++i) { par[i].h0 = par[i].h; par[i].hold = par[i].h; }
 }
 
-// MCM/mcm_init_neighb.f90:364-422
+// MCM/mcm_init_neighb.f90:25-84
 void Sim::init_neighb() {
     for (int i = 1; i <= np; ++i) { par[i].nnbr = 0; par[i].g_nnbr = 0; }
     setuplist();
@@ -1028,7 +1035,7 @@ void Sim::oldstrain() {
     }
 }
 
-// MCM/mcm_math_func.f90:165-231 (3-D branch)
+// MCM/mcm_math_func.f90:16-82 (3-D branch, :50-79)
 void Sim::inverse(const real M[3][3], real inv[3][3]) const {
     real sd[3][3];
     sd[0][0] = M[1][1] * M[2][2] - M[1][2] * M[2][1];
@@ -1284,7 +1291,7 @@ void Sim::f3dm1(Material &M, int i) {
     P.p = -othird * (s[0][0] + s[1][1] + s[2][2]);
 }
 
-// MCM/mcm_f3dm3.f90:106-233
+// MCM/mcm_f3dm3.f90:31-156
 void Sim::f3dm3(Material &M, int i) {
     Particle &P = par[i];
     real othird = 1.0 / 3.0;
@@ -1536,7 +1543,7 @@ int Sim::eos28c(int i) {
     return MCMO_OK;
 }
 
-// MCM/mcm_eos41c.f90:40-94 (c2 < 0 stops the reference; a status here)
+// MCM/mcm_eos41c.f90:31-85 (c2 < 0 stops the reference; a status here)
 int Sim::eos41c(int i) {
     Particle &P = par[i];
     const real *ei = mat[P.mat].eosinput;
@@ -1574,7 +1581,7 @@ void Sim::aviscosity(int i) {
     if (mat[par[i].mat].visc_type == 1) nodalav(i);
 }
 
-// MCM/mcm_nodalav.f90:76-91
+// MCM/mcm_nodalav.f90:32-47
 void Sim::nodalav(int i) {
     Particle &P = par[i];
     const Material &M = mat[P.mat];
@@ -1587,7 +1594,7 @@ void Sim::nodalav(int i) {
     }
 }
 
-// MCM/mcm_hieupd.f90:119-156
+// MCM/mcm_hieupd.f90:27-64
 void Sim::hieupd(int i) {
     Particle &P = par[i];
     real othird = 1.0 / 3.0;
@@ -1612,7 +1619,7 @@ void Sim::hieupd(int i) {
     std::memcpy(P.qold, P.q, sizeof(P.q));
 }
 
-// MCM/mcm_eqos.f90:183-214
+// MCM/mcm_eqos.f90:24-55
 void Sim::eqos(int i) {
     switch (mat[par[i].mat].eos) {
         case 1: eqos1(i); break;
@@ -1644,7 +1651,7 @@ void Sim::eqos1(int i) {
     }
 }
 
-// MCM/mcm_eqos4.f90:131-183
+// MCM/mcm_eqos4.f90:30-82
 void Sim::eqos4(int i) {
     Particle &P = par[i];
     const real *ei = mat[P.mat].eosinput;
@@ -1672,7 +1679,7 @@ void Sim::eqos4(int i) {
     }
 }
 
-// MCM/mcm_eqos13.f90:258-274
+// MCM/mcm_eqos13.f90:30-46
 void Sim::eqos13(int i) {
     Particle &P = par[i];
     real gamma_m1 = mat[P.mat].eosinput[0] - 1.0;
@@ -1682,7 +1689,7 @@ void Sim::eqos13(int i) {
     P.e = P.etry - 0.5 * dvol * P.p;
 }
 
-// MCM/mcm_eqos28.f90:343-358
+// MCM/mcm_eqos28.f90:30-45
 void Sim::eqos28(int i) {
     Particle &P = par[i];
     real b = mat[P.mat].eosinput[0], gamma = mat[P.mat].eosinput[1];
@@ -1718,7 +1725,7 @@ void Sim::eqos41(int i) {
     P.p = pn;
 }
 
-// MCM/mcm_stress_up.f90:245-253
+// MCM/mcm_stress_up.f90:28-36
 void Sim::stress_up(int i) {
     Particle &P = par[i];
     P.sigma[0][0] = P.s[0][0] - P.p;
@@ -1732,7 +1739,7 @@ void Sim::stress_up(int i) {
     P.sigma[2][1] = P.sigma[1][2];
 }
 
-// MCM/mcm_lieupd.f90:283-290
+// MCM/mcm_lieupd.f90:26-33
 void Sim::lieupd(int nn) {
     Particle &P = par[nn];
     real qpm = 0.0;
@@ -2123,7 +2130,7 @@ void Sim::momentum() {
     else corr_acceleration();
 }
 
-// MCM/mcm_update_ghost_stress.f90:272-285 (all off-diagonals flipped)
+// MCM/mcm_update_ghost_stress.f90:28-41 (all off-diagonals flipped)
 void Sim::update_ghost_stress() {
     for (int g = 1; g <= ngp; ++g) {
         int id = gpar[g].par;
@@ -2155,17 +2162,105 @@ void Sim::get_j_moment_info(int i, int k, real *x, real &mass, real &rho, real &
     }
 }
 
-// MCM/mcm_oldacceleration.f90:36-90.  With contacttype > 0 the reference adds
-// par%repulsion (:44-56), which stays 0: mcm_rep_cont (MCM/mcm_rep_contact.f90)
-// has no call site, so the sum is the same.
+// =========================================================================
+// Repulsive contact (MCM/mcm_rep_contact.f90, mcm_get_j_cont_info.f90),
+// called by MCM/mcm_solution.f90:64 when contacttype > 0, after the dt update
+// and before mcm_momentum.  It reads the contact lists that
+// mcm_ll_neighbours builds from particles of other materials (:150-174).
+// =========================================================================
+
+// MCM/mcm_get_j_cont_info.f90:31-58.  For k > ncont the reference reads the
+// ghost index from the REAL contact list (mcm_contlist(k,i), :48), whose
+// entries past ncont are left over from earlier searches or never written;
+// the ghost contact list the search builds for that purpose (mcm_g_contlist)
+// is read here instead.
+void Sim::get_j_cont_info(int i, int k, real *x, real &mass, real &rho, real &h, real &kj) const {
+    const Particle &P = par[i];
+    if (k <= P.ncont) {
+        const Particle &J = par[P.cont[k - 1]];
+        kj = mat[J.mat].k_cont;
+        for (int m = 0; m < 3; ++m) x[m] = J.x[m];
+        mass = J.mass; rho = J.rho; h = J.h;
+    } else {
+        const Ghost &J = gpar[P.gcont[k - P.ncont - 1]];
+        kj = mat[J.mat].k_cont;
+        for (int m = 0; m < 3; ++m) x[m] = J.x[m];
+        mass = J.mass; rho = J.rho; h = J.h;
+    }
+}
+
+// MCM/mcm_rep_contact.f90:102-161 (mcm_calc_fij).  The velocity difference of
+// :133-134 reads the uninitialised locals vi, vj and feeds only xijdotvij,
+// which nothing uses (:156-157 are commented out), so it is not restated.
+real Sim::calc_fij(const real *xi, const real *xj, real havg, real inv_w_deltap) const {
+    real rad = 0.0;
+    for (int n = 0; n < ndim; ++n) {
+        real xij = xi[n] - xj[n];
+        rad = rad + xij * xij;
+    }
+    rad = std::sqrt(rad);
+    real z = rad / havg;
+    if (z < 1.0) return inv_w_deltap * (((0.75 * z - 1.5) * z) * z + 1.0);
+    if (z < 2.0) {
+        real t = 2.0 - z;
+        return 0.25 * inv_w_deltap * (t * t * t);
+    }
+    return 0.0;
+}
+
+// MCM/mcm_rep_contact.f90:37-94: Monaghan's repulsive acceleration
+// -sum_j m_j (K_i + K_j) f_ij^n grad W_ij over the real and ghost contacts,
+// only for particles with at least one real contact (:41).
+void Sim::rep_cont() {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int i = svp; i <= evp; ++i) {
+        Particle &P = par[i];
+        for (int l = 0; l < ndim; ++l) P.repulsion[l] = 0.0;
+        if (P.ncont > 0) {
+            const real ki = mat[P.mat].k_cont;
+            const real n = mat[P.mat].n_cont;
+            for (int j = 1; j <= P.ncont + P.g_ncont; ++j) {
+                real xj[3] = {0, 0, 0}, massj, rhoj, hj, kj;
+                get_j_cont_info(i, j, xj, massj, rhoj, hj, kj);
+                real havg = 0.5 * (P.h + hj);
+                // inverse of W(delta p) for the cubic B-spline (:55-68)
+                real ratio = hj / havg;
+                real inv_w_deltap;
+                if (ratio < 1.0) inv_w_deltap = 1.0 / (((0.75 * ratio - 1.5) * ratio) * ratio + 1.0);
+                else { real t = 2.0 - ratio; inv_w_deltap = 1.0 / (t * t * t); }
+                real dwdx[3] = {0, 0, 0}, dwdr = 0;
+                grad1(dwdx, dwdr, P.x, xj, havg);
+                real fij = calc_fij(P.x, xj, havg, inv_w_deltap);
+                real kij = ki + kj;
+                for (int l = 0; l < ndim; ++l)
+                    P.repulsion[l] = P.repulsion[l] - (massj * (kij * std::pow(fij, n)) * dwdx[l]);
+            }
+        }
+    }
+}
+
+// MCM/mcm_oldacceleration.f90:36-90.  With contacttype > 0 the acceleration
+// starts from par%repulsion and the per-material contact forces xcf, ycf, zcf
+// (written to the time-history file) sum mass x repulsion (:44-56).
 void Sim::oldacceleration() {
     for (int i = 1; i <= nummat; ++i) { mat[i].xcf = 0.0; mat[i].ycf = 0.0; mat[i].zcf = 0.0; }
+    if (contacttype > 0)
+        for (int i = svp; i <= evp; ++i) {
+            const Particle &P = par[i];
+            mat[P.mat].xcf = mat[P.mat].xcf + P.mass * P.repulsion[0];
+            mat[P.mat].ycf = mat[P.mat].ycf + P.mass * P.repulsion[1];
+            mat[P.mat].zcf = mat[P.mat].zcf + P.mass * P.repulsion[2];
+        }
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
     for (int i = svp; i <= evp; ++i) {
         Particle &P = par[i];
         P.a[0] = P.a[1] = P.a[2] = 0.0;
+        if (contacttype > 0)
+            for (int l = 0; l < ndim; ++l) P.a[l] = P.a[l] + P.repulsion[l];
         real rhoi = P.rho;
         real sigmai[3][3], qi[3][3];
         std::memcpy(sigmai, P.sigma, sizeof(sigmai));
@@ -2188,7 +2283,9 @@ void Sim::oldacceleration() {
 }
 
 // MCM/mcm_corr_acceleration.f90:37-163 (kernel centred at j; self slot zeroed;
-// the final sum uses the mass of the last neighbour visited)
+// the final sum uses the mass of the last neighbour visited).  With
+// contacttype > 0 the acceleration starts from par%repulsion (:45-49); this
+// routine does not touch the per-material contact forces.
 void Sim::corr_acceleration() {
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
@@ -2196,6 +2293,8 @@ void Sim::corr_acceleration() {
     for (int i = svp; i <= evp; ++i) {
         Particle &P = par[i];
         P.a[0] = P.a[1] = P.a[2] = 0.0;
+        if (contacttype > 0)
+            for (int l = 0; l < ndim; ++l) P.a[l] = P.a[l] + P.repulsion[l];
         real rhoi = P.rho;
         real sigmai[3][3], qi[3][3];
         std::memcpy(sigmai, P.sigma, sizeof(sigmai));
@@ -2420,6 +2519,7 @@ void Sim::dt_update() {
 }
 
 void Sim::step_b() {
+    if (contacttype > 0) rep_cont();   // MCM/mcm_solution.f90:64
     momentum();
     boundcond();
     calctotale();
@@ -2437,6 +2537,7 @@ bool field_ptr(Particle &P, const std::string &f, real *&ptr, int &n) {
     else if (f == "xzero") { ptr = P.xzero; n = 3; }
     else if (f == "v") { ptr = P.v; n = 3; }
     else if (f == "a") { ptr = P.a; n = 3; }
+    else if (f == "repulsion") { ptr = P.repulsion; n = 3; }
     else if (f == "rod") { ptr = &P.rod[0][0]; n = 9; }
     else if (f == "spin") { ptr = &P.spin[0][0]; n = 9; }
     else if (f == "sigma") { ptr = &P.sigma[0][0]; n = 9; }
@@ -2555,6 +2656,7 @@ int mcmo_get_int(void *sim, const char *field, int *out) {
         if (f == "nnbr") v = P.nnbr;
         else if (f == "g_nnbr") v = P.g_nnbr;
         else if (f == "ncont") v = P.ncont;
+        else if (f == "g_ncont") v = P.g_ncont;
         else if (f == "mat") v = P.mat;
         else if (f == "dispbc") v = P.dispbc;
         else if (f == "llpointer") v = P.llpointer;
@@ -2615,6 +2717,32 @@ int mcmo_g_nbrlist(void *sim, int i, int *out, int cap) {
     int n = (int)P.gnbr.size();
     for (int k = 0; k < n && k < cap; ++k) out[k] = P.gnbr[k];
     return n;
+}
+
+int mcmo_contlist(void *sim, int i, int *out, int cap) {
+    Sim *s = static_cast<Sim *>(sim);
+    const Particle &P = s->par[i];
+    int n = (int)P.cont.size();
+    for (int k = 0; k < n && k < cap; ++k) out[k] = P.cont[k];
+    return n;
+}
+
+int mcmo_g_contlist(void *sim, int i, int *out, int cap) {
+    Sim *s = static_cast<Sim *>(sim);
+    const Particle &P = s->par[i];
+    int n = (int)P.gcont.size();
+    for (int k = 0; k < n && k < cap; ++k) out[k] = P.gcont[k];
+    return n;
+}
+
+int mcmo_contact_forces(void *sim, double *xyz) {
+    Sim *s = static_cast<Sim *>(sim);
+    for (int m = 1; m <= s->nummat; ++m) {
+        xyz[3 * (m - 1) + 0] = s->mat[m].xcf;
+        xyz[3 * (m - 1) + 1] = s->mat[m].ycf;
+        xyz[3 * (m - 1) + 2] = s->mat[m].zcf;
+    }
+    return MCMO_OK;
 }
 
 int mcmo_ghosts(void *sim, int *par_out, double *x_out, double *v_out, int cap) {

@@ -32,6 +32,7 @@ typedef struct {
     double rho_min, rho_max;
     double strinput[48];
     double eosinput[24];
+    double k_cont, n_cont;  /* contact cards (MCM/mcm_contactype.f90:35), contacttype > 0 */
 } mcmo_material;
 
 /* Control cards (MCM/mcm_control_v2.f90:88-124), the symmetry cards
@@ -85,6 +86,11 @@ int mcmo_set_scalar(void *sim, const char *name, double value);
 /* Neighbour lists: returns count; 1-based ids as in mcm_nbrlist. */
 int mcmo_nbrlist(void *sim, int i, int *out, int cap);
 int mcmo_g_nbrlist(void *sim, int i, int *out, int cap);
+/* Contact lists (other materials' particles, contacttype > 0) and the
+ * per-material contact forces xcf, ycf, zcf of the last mcm_oldacceleration. */
+int mcmo_contlist(void *sim, int i, int *out, int cap);
+int mcmo_g_contlist(void *sim, int i, int *out, int cap);
+int mcmo_contact_forces(void *sim, double *xyz);
 /* Ghosts created by the last mcm_ghost_setup: source particle id and x. */
 int mcmo_ghosts(void *sim, int *par_out, double *x_out, double *v_out, int cap);
 int mcmo_grid(void *sim, int *gridlim, double *gridmin, double *gridsize);

@@ -20,6 +20,7 @@ class OMaterial(C.Structure):
         ("rho", C.c_double), ("av_l", C.c_double), ("av_q", C.c_double), ("mass", C.c_double),
         ("h", C.c_double), ("rho_min", C.c_double), ("rho_max", C.c_double),
         ("strinput", C.c_double * 48), ("eosinput", C.c_double * 24),
+        ("k_cont", C.c_double), ("n_cont", C.c_double),
     ]
 
 
@@ -69,6 +70,9 @@ def load(openmp: bool = False) -> C.CDLL:
         "mcmo_set_scalar": ([V, C.c_char_p, C.c_double], C.c_int),
         "mcmo_nbrlist": ([V, C.c_int, IP, C.c_int], C.c_int),
         "mcmo_g_nbrlist": ([V, C.c_int, IP, C.c_int], C.c_int),
+        "mcmo_contlist": ([V, C.c_int, IP, C.c_int], C.c_int),
+        "mcmo_g_contlist": ([V, C.c_int, IP, C.c_int], C.c_int),
+        "mcmo_contact_forces": ([V, DP], C.c_int),
         "mcmo_ghosts": ([V, IP, DP, DP, C.c_int], C.c_int),
         "mcmo_grid": ([V, IP, DP, DP], C.c_int),
         "mcmo_material_energy": ([V, DP, DP, DP], C.c_int),
@@ -84,7 +88,7 @@ def load(openmp: bool = False) -> C.CDLL:
     return lib
 
 
-WIDTH = {"x": 3, "xzero": 3, "v": 3, "a": 3, "rod": 9, "spin": 9, "sigma": 9, "s": 9, "q": 9, "qold": 9, "alfa": 9}
+WIDTH = {"x": 3, "xzero": 3, "v": 3, "a": 3, "repulsion": 3, "rod": 9, "spin": 9, "sigma": 9, "s": 9, "q": 9, "qold": 9, "alfa": 9}
 
 
 def _dp(a):
@@ -122,6 +126,8 @@ class Oracle:
                 m.strinput[i] = float(c.strinput[i])
             for i in range(24):
                 m.eosinput[i] = float(c.eosinput[i])
+            if deck.contacttype > 0 and k < len(deck.k_cont):
+                m.k_cont, m.n_cont = float(deck.k_cont[k]), float(deck.n_cont[k])
         self.n = deck.np
         self.nmat = len(deck.materials)
         x = np.ascontiguousarray(deck.x, dtype=np.float64)
@@ -223,6 +229,22 @@ class Oracle:
         buf = np.zeros(1024, dtype=np.int32)
         n = self.lib.mcmo_g_nbrlist(self.sim, i, _ip(buf), 1024)
         return buf[:n].copy()
+
+    def contlist(self, i: int) -> np.ndarray:
+        buf = np.zeros(1024, dtype=np.int32)
+        n = self.lib.mcmo_contlist(self.sim, i, _ip(buf), 1024)
+        return buf[:n].copy()
+
+    def g_contlist(self, i: int) -> np.ndarray:
+        buf = np.zeros(1024, dtype=np.int32)
+        n = self.lib.mcmo_g_contlist(self.sim, i, _ip(buf), 1024)
+        return buf[:n].copy()
+
+    def contact_forces(self) -> np.ndarray:
+        """Per material xcf, ycf, zcf of the last momentum sum, shape (nmat, 3)."""
+        out = np.zeros(3 * self.nmat)
+        self.lib.mcmo_contact_forces(self.sim, _dp(out))
+        return out.reshape(self.nmat, 3)
 
     def ghosts(self):
         n = self.lib.mcmo_ghosts(self.sim, None, None, None, 0)

@@ -36,7 +36,7 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version_and_strerror(lib):
-    assert lib.mcm_gpu_abi_version() == 2
+    assert lib.mcm_gpu_abi_version() == 3
     assert lib.mcm_gpu_strerror(_abi.MCM_ENBR_OVERFLOW) == b"neighbour table overflow"
     assert lib.mcm_gpu_strerror(12345) == b"unknown status"
 

@@ -22,7 +22,7 @@ def test_read_real_fields(field, d, value):
 
 
 def test_read_record_columns():
-    # (2i5,e10.0,2i5,e10.0,i5,2e10.0): the material card of MCM/mcm_matin.f90:250
+    # (2i5,e10.0,2i5,e10.0,i5,2e10.0): the material card, format 250 of MCM/mcm_matin.f90:224
     rec = "    2   10      8.93   41                   0       1.5      0.06"
     assert read_record(rec, "(2i5,e10.0,2i5,e10.0,i5,2e10.0)") == [2, 10, 8.93, 41, 0, 0.0, 0, 1.5, 0.06]
     # beyond column 80 nothing is read; short records read blanks
@@ -304,9 +304,9 @@ def oracle_program(deck, base, directory, steps):
             self.last_state = state
             super().state_output(state)
 
-        def timehist(self, ptime, state, energies):
+        def timehist(self, ptime, state, energies, contact_forces=None):
             self.last_th = (ptime, state, energies.copy())
-            super().timehist(ptime, state, energies)
+            super().timehist(ptime, state, energies, contact_forces)
 
     orc = Oracle(deck)
     out = Recording(deck, base, directory)
@@ -319,7 +319,8 @@ def oracle_program(deck, base, directory, steps):
         t = orc.scalar("ptime")
         st, th = out.due(t)
         if st or th:
-            out.after_energies(t, oracle_state(orc, out.fields(st, th)), orc.energies())
+            cf = orc.contact_forces() if (th and deck.contacttype > 0) else None
+            out.after_energies(t, oracle_state(orc, out.fields(st, th)), orc.energies(), cf)
         if orc.ended():
             break
         orc.step_c()

@@ -114,7 +114,7 @@ def test_autotune_keeps_state_and_results(lib):
 
 @pytest.mark.parametrize("shape", [dict(search_threads=64, pair_threads=64, pair_blocks_per_sm=16),
                                    dict(search_threads=128, pair_threads=128, pair_blocks_per_sm=1),
-                                   dict(search_threads=256, search_kind=2)])
+                                   dict(search_threads=256, search_kind=2), dict(search_kind=3)])
 def test_launch_shape_does_not_change_results(lib, shape):
     deck = bodies()[2]
     for precision in (_abi.PREC_FP64, _abi.PREC_MIXED):
@@ -128,7 +128,7 @@ def test_launch_shape_does_not_change_results(lib, shape):
 
 def test_set_tuning_rejects_bad_shapes(lib):
     s = Solver(bodies()[0], _abi.PREC_MIXED)
-    for bad in (dict(search_threads=96), dict(pair_threads=512), dict(pair_blocks_per_sm=17), dict(search_kind=3)):
+    for bad in (dict(search_threads=96), dict(pair_threads=512), dict(pair_blocks_per_sm=17), dict(search_kind=4)):
         with pytest.raises(_abi.MCMError):
             s.set_tuning(**bad)
 

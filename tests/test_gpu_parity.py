@@ -214,11 +214,47 @@ def test_taylor_bar_16k_thousand_steps(lib):
     deck = taylor_bar(dx=0.4e-3)
     sol = Solver(deck, _abi.PREC_FP64_EXACT)
     orc = Oracle(deck, openmp=True)
-    assert sol.run(1000) == 1000
-    assert orc.run(1000) == 1000
+    # the total-energy balance of mcm_calctotale (MCM/mcm_calctotale.f90:53-60)
+    # along the run: the GPU's drift follows the oracle's every 100 steps
+    e0, o0 = sol.energies_now()[-1], orc.scalar("totale")
+    assert abs(e0 - o0) <= 1e-13 * abs(o0)
+    for _ in range(10):
+        assert sol.run(100) == 100
+        assert orc.run(100) == 100
+        drift_gpu = (sol.energies_now()[-1] - e0) / e0
+        drift_orc = (orc.scalar("totale") - o0) / o0
+        assert abs(drift_gpu - drift_orc) <= 1e-9, (drift_gpu, drift_orc)
     errs = compare(sol, orc, STATE, 1e-8, "16k bar, 1000 steps")
-    print("max relative error per field after 1000 steps:", errs)
+    print("max relative error per field after 1000 steps:", errs, "energy drift", drift_orc)
     assert abs(sol.ptime - orc.scalar("ptime")) <= 1e-10 * orc.scalar("ptime")
+
+
+def test_displacement_bcs(lib, oracle_lib):
+    """Displacement codes 1-7 (MCM/mcm_boundcond.f90:30-61 zero the
+    constrained acceleration components; MCM/mcm_init_boundcond.f90:25-54
+    zero the constrained initial velocity components) on a bar whose
+    particles carry seeded random codes, against the oracle in all three
+    precisions; constrained velocity components stay zero."""
+    deck = small_bar()
+    rng = np.random.default_rng(11)
+    deck = deck.replace(dispbc=rng.integers(0, 8, size=deck.np).astype(np.int32))
+    masks = {1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (1, 1, 0), 5: (0, 1, 1), 6: (1, 0, 1), 7: (1, 1, 1)}
+    for prec, tol in ((_abi.PREC_FP64_EXACT, 1e-12), (_abi.PREC_FP64, 1e-9), (_abi.PREC_MIXED, 5e-5)):
+        sol, orc = Solver(deck, prec), Oracle(deck)
+        try:
+            for _ in range(25):
+                sol.step()
+                orc.step()
+            compare(sol, orc, STATE + ["a"], tol, f"dispbc, precision {prec}")
+            v = sol.download(["v"])["v"]
+            for code, m in masks.items():
+                sel = deck.dispbc == code
+                for d in range(3):
+                    if m[d]:
+                        assert not v[sel, d].any(), (code, d)
+        finally:
+            sol.close()
+            orc.close()
 
 
 def test_neighbour_overflow_regrow(lib):
@@ -265,3 +301,24 @@ def test_search_prefilter_without_diagnostics(lib, precision):
     if precision == _abi.PREC_FP64_EXACT:
         compare(sol, orc, STATE, 1e-11, "prefiltered search")
     compare_neighbours(sol, orc)
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_search_kinds_match_oracle(lib, kind):
+    """The warp-per-particle and warp-per-cell searches build the reference's
+    neighbour sequences on the fluid column (five ghost planes, ghosts of
+    ghosts) and the 16 848-particle bar, with diagnostics off (FP32 decisions
+    with FP64 ties only) and on (FP64 minimum distances)."""
+    for deck in (fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3)), taylor_bar(dx=0.4e-3)):
+        for diag in (False, True):
+            sol = Solver(deck, _abi.PREC_FP64_EXACT)
+            sol.set_tuning(search_kind=kind)
+            sol.set_diagnostics(diag)
+            orc = Oracle(deck, openmp=True)
+            for _ in range(3):
+                sol.step()
+                orc.step()
+            compare_neighbours(sol, orc)
+            compare(sol, orc, STATE + (["mindist"] if diag else []), 1e-12, f"search kind {kind}")
+            sol.close()
+            orc.close()

@@ -145,7 +145,7 @@ def test_rigid_rotation_preserves_stress_invariants():
     out = orc.get("sigma")[inner]
     S = S[inner]
     assert np.max(np.abs(orc.get("rod")[inner])) < 1e-4
-    # Q sigma Q^T (MCM/mcm_stress_rot1.f90:286-355) keeps trace and norm
+    # Q sigma Q^T (MCM/mcm_stress_rot1.f90:164-182) keeps trace and norm
     assert np.allclose(np.trace(out, axis1=1, axis2=2), np.trace(S, axis1=1, axis2=2), rtol=1e-7, atol=1e-7)
     assert np.allclose(np.linalg.norm(out, axis=(1, 2)), np.linalg.norm(S, axis=(1, 2)), rtol=1e-7)
     assert np.max(np.abs(out - S)) > 1e-5
@@ -375,3 +375,81 @@ def test_dynamic_relaxation_restated(oracle_lib):
     dtn = 0.5 * (orc.scalar("dt") + orc.scalar("dtold"))
     orc.step_c()
     assert np.array_equal(orc.get("v"), 0.5 * v + a * dtn)
+
+
+def _rep_restated(orc, deck):
+    """Monaghan's repulsive acceleration of MCM/mcm_rep_contact.f90:37-161,
+    restated in numpy on the oracle's state (positions after the strain
+    half-step round trip, the contact lists of the step's search)."""
+    x, h, mass = orc.get("x"), orc.get("h"), orc.get("mass")
+    mat = orc.get_int("mat")
+    kc = np.asarray(deck.k_cont, dtype=np.float64)
+    nc = np.asarray(deck.n_cont, dtype=np.float64)
+    gpar, gx, _ = orc.ghosts()
+    rep = np.zeros((deck.np, 3))
+    for i in range(deck.np):
+        cont = orc.contlist(i + 1)
+        if cont.size == 0:
+            continue
+        gcont = orc.g_contlist(i + 1)
+        xs = [x[j - 1] for j in cont] + [gx[g - 1] for g in gcont]
+        hs = [h[j - 1] for j in cont] + [h[gpar[g - 1] - 1] for g in gcont]
+        ms = [mass[j - 1] for j in cont] + [mass[gpar[g - 1] - 1] for g in gcont]
+        ks = [kc[mat[j - 1] - 1] for j in cont] + [kc[mat[gpar[g - 1] - 1] - 1] for g in gcont]
+        for xj, hj, mj, kj in zip(xs, hs, ms, ks):
+            havg = 0.5 * (h[i] + hj)
+            ratio = hj / havg
+            inv_w = 1.0 / ((0.75 * ratio - 1.5) * ratio * ratio + 1.0) if ratio < 1 else 1.0 / (2.0 - ratio) ** 3
+            d = x[i] - xj
+            r = np.sqrt(d @ d)
+            z = r / havg
+            c1 = 1.0 / (np.pi * havg ** 3)
+            if z < 1:
+                dw = c1 * (2.25 * z - 3.0) * z
+                fij = inv_w * ((0.75 * z - 1.5) * z * z + 1.0)
+            elif z < 2:
+                dw = -0.75 * c1 * (2.0 - z) ** 2
+                fij = 0.25 * inv_w * (2.0 - z) ** 3
+            else:
+                dw, fij = 0.0, 0.0
+            grad = dw * d / (r * havg) if r > 0 else np.zeros(3)
+            rep[i] -= mj * (kc[mat[i] - 1] + kj) * fij ** nc[mat[i] - 1] * grad
+    return rep
+
+
+@pytest.mark.parametrize("disctype", [0, 1])
+def test_repulsive_contact_restated(disctype, oracle_lib):
+    # a two-material bar with contacttype 1: contact lists hold exactly the
+    # other material's particles within reach, the repulsion follows the
+    # formulas of mcm_rep_contact.f90, the acceleration starts from it and the
+    # per-material contact forces sum mass x repulsion (disctype 0 only)
+    from mcmtop_b200.deck import two_material_bar
+
+    deck = two_material_bar(contacttype=1, disctype=disctype)
+    orc = Oracle(deck)
+    for _ in range(15):
+        orc.step()
+    orc.step_a()
+    orc.dt_update()
+    orc.step_b()
+    x, h, mat = orc.get("x"), orc.get("h"), orc.get_int("mat")
+    ncont = orc.get_int("ncont")
+    assert ncont.sum() > 0
+    for i in range(0, deck.np, 37):
+        d2 = ((x - x[i]) ** 2).sum(axis=1)
+        near = np.flatnonzero((d2 < (h + h[i]) ** 2) & (mat != mat[i])) + 1
+        assert np.array_equal(np.sort(orc.contlist(i + 1)), near)
+        assert not np.isin(orc.nbrlist(i + 1), near).any()
+    rep = orc.get("repulsion")
+    ref = _rep_restated(orc, deck)
+    assert np.max(np.abs(rep - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert np.max(np.abs(ref)) > 0
+    cf = orc.contact_forces()
+    if disctype == 0:
+        mass = orc.get("mass")
+        for m in (1, 2):
+            want = (mass[mat == m, None] * rep[mat == m]).sum(axis=0)
+            assert np.allclose(cf[m - 1], want, rtol=1e-12, atol=0)
+        assert cf[0, 2] < 0 < cf[1, 2]          # the halves push each other apart
+    else:
+        assert not cf.any()                      # mcm_corr_acceleration does not sum them
