@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--ens-bodies", type=int, default=256, help="bars of the batched ensemble (0: skip it)")
     ap.add_argument("--ens-steps", type=int, default=500)
     ap.add_argument("--fluid-steps", type=int, default=20, help="iterations of the 15.6M fluid column (0: skip)")
+    ap.add_argument("--long-steps", type=int, default=2000,
+                    help="iterations of the 2000-step accuracy run of the configuration, mixed and FP64 (0: skip)")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -338,21 +340,28 @@ def fluid_column_cost(args, local):
                     "every step; device time (CUDA events on the library stream)"}
 
 
-def ensemble_cost(args, local):
+def ensemble_cost(args, local, ws=1, rank=0, barrier=None):
     """The calibration ensemble: --ens-bodies independent Taylor bars (radius
     2-4 mm, L/D 6-12, 4k-64k particles log-uniform, yield 200-600 MPa, impact
     120-250 m/s) advanced --ens-steps iterations in the headline precision,
     once as a batch (one CUDA-graph launch per iteration of all bodies, lane
     count from mcm_gpu_batch_autotune) and once body after body through
     mcm_gpu_run, from the same initial states.  Wall clock around the
-    synchronous calls; the end states of the two runs are compared."""
+    synchronous calls; the end states of the two runs are compared.  With
+    several ranks each rank advances its contiguous block of the bodies
+    (ranks.share), the times are the slowest rank's, the work and the final
+    bar lengths are gathered from every rank."""
     from mcmtop_b200 import _abi
     from mcmtop_b200.deck import taylor_ensemble
+    from mcmtop_b200.ranks import gather_items, share, sum_over_ranks
     from mcmtop_b200.solver import Batch, Solver
 
     prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
-    decks = taylor_ensemble(nbodies=args.ens_bodies, seed=2024)
-    n_total = sum(d.np for d in decks)
+    everyone = taylor_ensemble(nbodies=args.ens_bodies, seed=2024)
+    mine = share(len(everyone), ws, rank)
+    decks = [everyone[k] for k in mine]
+    n_total = sum(d.np for d in everyone)
+    dev = f"cuda:{local}"
     t0 = time.perf_counter()
     batched = [Solver(d, prec, device=local) for d in decks]
     t_init = time.perf_counter() - t0
@@ -360,33 +369,90 @@ def ensemble_cost(args, local):
         s.set_diagnostics(False)
     batch = Batch(batched, lanes=8)
     lanes, tuned_ms = batch.autotune(2)
+    if barrier:
+        barrier()
     t0 = time.perf_counter()
     done = batch.run(args.ens_steps)
-    t_batch = time.perf_counter() - t0
+    t_batch = max_over_ranks(time.perf_counter() - t0, dev)
     batch.close()
     seq = [Solver(d, prec, device=local) for d in decks]
     for s in seq:
         s.set_diagnostics(False)
+    if barrier:
+        barrier()
     t0 = time.perf_counter()
     done_seq = [s.run(args.ens_steps) for s in seq]
-    t_seq = time.perf_counter() - t0
+    t_seq = max_over_ranks(time.perf_counter() - t0, dev)
     same = all(np.array_equal(a.download(["x"])["x"], b.download(["x"])["x"]) for a, b in zip(batched, seq))
-    steps = int(np.sum(done))
-    work = sum(d.np * int(k) for d, k in zip(decks, done))
+    lengths = {}
+    for k, s in zip(mine, batched):
+        z = s.download(["x"])["x"][:, 2]
+        lengths[k] = float(z.max() - z.min())
+    steps = int(sum_over_ranks(float(np.sum(done)), dev))
+    work = sum_over_ranks(float(sum(d.np * int(k) for d, k in zip(decks, done))), dev)
+    same_all = sum_over_ranks(0.0 if same else 1.0, dev) == 0.0
+    final_len = gather_items(lengths, len(everyone), dev)[:, 0]
     for s in batched + seq:
         s.close()
-    return {"workload": f"taylor_ensemble_{len(decks)}x_{n_total}", "bodies": len(decks), "particles": n_total,
-            "particles_min": min(d.np for d in decks), "particles_max": max(d.np for d in decks),
+    return {"workload": f"taylor_ensemble_{len(everyone)}x_{n_total}", "bodies": len(everyone),
+            "particles": n_total, "ranks": ws, "bodies_per_rank": [len(share(len(everyone), ws, r)) for r in range(ws)],
+            "particles_min": min(d.np for d in everyone), "particles_max": max(d.np for d in everyone),
             "steps": args.ens_steps, "body_steps_done": steps, "precision": args.precision,
             "lanes": lanes, "tuned_ms_per_step": round(tuned_ms, 4),
             "batched_s": round(t_batch, 3), "sequential_s": round(t_seq, 3),
             "batched_particle_steps_per_s": round(work / t_batch, 1),
             "sequential_particle_steps_per_s": round(work / t_seq, 1),
-            "speedup": round(t_seq / t_batch, 3), "same_end_positions": bool(same),
+            "speedup": round(t_seq / t_batch, 3), "same_end_positions": bool(same_all),
             "sequential_done_equal": bool(list(done_seq) == [int(k) for k in done]),
-            "init_s_per_body": round(t_init / len(decks), 4),
+            "final_length_cm": {"min": round(float(final_len.min()), 6), "max": round(float(final_len.max()), 6)},
+            "init_s_per_body": round(t_init / max(len(decks), 1), 4),
             "note": "batched = mcm_gpu_batch_run (graph of one iteration of every body over the tuned lanes); "
-                    "sequential = mcm_gpu_run per body, one after the other; wall clock"}
+                    "sequential = mcm_gpu_run per body, one after the other; wall clock, slowest rank; "
+                    "each rank advances its contiguous block of the bodies"}
+
+
+def long_run(args, local):
+    """The configuration's full run: the bar advanced --long-steps iterations
+    as the plain FP64 step and as the mixed step from the same initial state;
+    per-field error of the mixed end state against the FP64 one (max |mixed -
+    fp64| / max |fp64|), the relative difference of the final bar lengths, and
+    the device time of each run (CUDA events on the library's stream)."""
+    from mcmtop_b200 import _abi
+    from mcmtop_b200.deck import taylor_bar
+    from mcmtop_b200.solver import Solver
+
+    deck = taylor_bar(dx=args.dx)
+    out = {"workload": f"taylor_bar_{deck.np}", "steps": args.long_steps}
+    ends = {}
+    for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
+        sol = Solver(deck, prec, device=local, reorder_interval=args.reorder)
+        sol.set_diagnostics(False)
+        sol.timer_start()
+        done = sol.run(args.long_steps)
+        ms = sol.timer_stop()
+        if done != args.long_steps:
+            raise RuntimeError(f"{name} long run stopped after {done} steps")
+        ends[name] = sol.download(["x", "v", "rho", "e", "p", "c", "efps", "sigma", "q", "vabs"])
+        out[name] = {"ms_per_step": round(ms / done, 4), "particle_steps_per_s": round(deck.np * done / (ms / 1e3), 1),
+                     "ptime": sol.ptime}
+        sol.close()
+    a_, b_ = ends["mixed"], ends["fp64"]
+    err = {}
+    for f in b_:
+        scale = float(np.max(np.abs(b_[f])))
+        err[f] = float(np.max(np.abs(a_[f] - b_[f])) / scale) if scale > 0 else float(np.max(np.abs(a_[f])))
+    la = a_["x"][:, 2].max() - a_["x"][:, 2].min()
+    lb = b_["x"][:, 2].max() - b_["x"][:, 2].min()
+    l0 = deck.x[:, 2].max() - deck.x[:, 2].min()
+    out.update({"max_rel_err": {k: float(f"{v:.3e}") for k, v in err.items()},
+                "worst": float(f"{max(err.values()):.3e}"), "within_1e-4": bool(max(err.values()) <= 1e-4),
+                "final_length_rel_diff": float(f"{abs(la - lb) / lb:.3e}"),
+                "within_0.1_percent": bool(abs(la - lb) / lb <= 1e-3),
+                "length_over_initial": {"fp64": round(float(lb / l0), 6), "mixed": round(float(la / l0), 6)},
+                "mixed_over_fp64": round(out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"], 3),
+                "note": "the FP64 GPU step is itself within 1e-13 of the FP64 oracle after the first 50 steps of "
+                        "this bar (accuracy.vs_oracle) and bit-close over 1000 steps of the 16k bar (GPU tests)"})
+    return out
 
 
 # ----------------------------------------------------------------- GPU arm
@@ -489,6 +555,11 @@ def gpu_arm(args):
                         "length_rel_diff": float(f"{abs(la - lb) / lb:.3e}")}
         ref.close()
 
+    ensemble = None
+    if args.ens_bodies > 0:
+        # every rank advances its block of the bodies; collectives in the same order on all ranks
+        ensemble = ensemble_cost(args, local, ws, rank, barrier)
+
     # end to end through the split C ABI with host buffers (rank 0 only)
     e2e = None
     if rank == 0 and not args.no_e2e:
@@ -535,13 +606,13 @@ def gpu_arm(args):
     if rank == 0 and not args.no_adjoint:
         adjoint = adjoint_cost(args, local)
 
-    ensemble = None
-    if rank == 0 and args.ens_bodies > 0:
-        ensemble = ensemble_cost(args, local)
-
     fluid = None
     if rank == 0 and args.fluid_steps > 0:
         fluid = fluid_column_cost(args, local)
+
+    longrun = None
+    if rank == 0 and args.long_steps > 0 and args.precision == "mixed":
+        longrun = long_run(args, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -565,7 +636,8 @@ def gpu_arm(args):
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
                    "reorder_interval": args.reorder},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "fluid_column": fluid,
+        "fp64": fp64, "accuracy": accuracy, "long_run": longrun, "adjoint": adjoint, "ensemble": ensemble,
+        "fluid_column": fluid,
         "kernels": kernels,
     }
     if rank == 0:

@@ -229,19 +229,23 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
 
 /* -------------------------------------------------- allocation-free call */
 
-/* No counterpart in the reference.  Per-material energy sums of
- * MCM/mcm_calctotale.f90's formulas (ke, ie, mom(3) per material, then
- * kinetice, internale, totale: 5*nmat+3 doubles into `energies`) computed
- * from DEVICE arrays the caller owns -- mass, vabs, e, mat of length np and v
- * in the (3,np) layout -- without allocating device memory: for callers that
- * cannot call cudaMalloc (a host code that gives all device memory to its own
- * pool, or must keep cudaMalloc/cudaFree and their synchronisation out of the
- * time step).  Its scratch is a fixed __device__ array of 296 x 5 x 16
- * doubles (189 440 bytes per GPU, held until exit); nmat above
- * MCM_GPU_MAX_MATERIALS returns MCM_EINVAL.  The first call on a device looks
- * up the array's address (make that first call before any stream capture).
- * Calls share the array, so calls whose kernels overlap on the GPU race.
- * Runs on `stream` (NULL: the default stream) and waits for it. */
+/* No counterpart in the reference.  The per-material energy sums that
+ * mcm_gpu_step_b returns (ke = sum 0.5 m vabs^2, ie = sum e, mom(3) = sum m |v_d|
+ * per material, then kinetice, internale, totale: 5*nmat+3 doubles into
+ * `energies`), summed over all np particles with no active-particle filter,
+ * as step_b sums them, from DEVICE arrays the caller owns -- mass, vabs, e,
+ * mat of length np and v in the (3,np) layout -- without allocating device
+ * memory: for callers that cannot call cudaMalloc (a host code that gives all
+ * device memory to its own pool, or must keep cudaMalloc/cudaFree and their
+ * synchronisation out of the time step).  Particles whose mat lies outside
+ * 1..nmat are skipped.  Its scratch is a fixed __device__ array of
+ * 296 x 5 x 16 doubles (189 440 bytes per GPU, held until exit); nmat above
+ * MCM_GPU_MAX_MATERIALS returns MCM_EINVAL.  Every call looks up the array's
+ * address in the current device's context, which a stream capture in
+ * progress may not allow: call it outside captures.  Calls share the array,
+ * so calls whose kernels overlap on the GPU race.  Runs on `stream` (NULL:
+ * the default stream) and waits for it; an error already pending from the
+ * caller's earlier CUDA work returns MCM_ECUDA before anything is launched. */
 int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const double *v, const double *e,
                                const int *mat, int np, int nmat, double *energies, void *stream);
 
@@ -321,6 +325,18 @@ int mcm_gpu_batch_run(mcm_gpu_batch *b, int nsteps, mcm_gpu_time *times, int *do
  * states, restores every body's state and time scalars, and keeps the fastest
  * lane count (*lanes, *ms_per_step may be NULL). */
 int mcm_gpu_batch_autotune(mcm_gpu_batch *b, int nsteps, int *lanes, double *ms_per_step);
+/* No counterpart in the reference.  Gradients of every body of a batch:
+ * mcm_gpu_adjoint_forward and mcm_gpu_adjoint_backward of each body (same
+ * arguments, per body: dts[b] with nsteps+1 entries, xbar[b], vbar[b],
+ * param_bar[b] (nmat x 4), xbar0[b], vbar0[b]; a NULL array of pointers is
+ * NULL for every body), run by host worker threads -- at most the batch's
+ * lane count and 16 -- that take the bodies largest first, each body's work
+ * on its own stream, so that the bodies' kernels overlap on the GPU.  Each
+ * body's results are those of its single-body calls.  Returns the first
+ * failing body's status (the workers then stop taking bodies). */
+int mcm_gpu_batch_adjoint_forward(mcm_gpu_batch *b, int nsteps, const double *const *dts, int checkpoint_every);
+int mcm_gpu_batch_adjoint_backward(mcm_gpu_batch *b, const double *const *xbar, const double *const *vbar,
+                                   double *const *param_bar, double *const *xbar0, double *const *vbar0);
 int mcm_gpu_batch_destroy(mcm_gpu_batch *b);
 
 /* ----------------------------------------------------------- measurement */

@@ -135,6 +135,9 @@ def load() -> C.CDLL:
         "mcm_gpu_batch_run": ([H, C.c_int, C.POINTER(Time), _IP], C.c_int),
         "mcm_gpu_batch_autotune": ([H, C.c_int, _IP, _DP], C.c_int),
         "mcm_gpu_batch_destroy": ([H], C.c_int),
+        "mcm_gpu_batch_adjoint_forward": ([H, C.c_int, C.POINTER(_DP), C.c_int], C.c_int),
+        "mcm_gpu_batch_adjoint_backward": ([H, C.POINTER(_DP), C.POINTER(_DP), C.POINTER(_DP), C.POINTER(_DP),
+                                            C.POINTER(_DP)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -9,9 +9,11 @@
 // costs one graph launch, and bodies of uneven size share the GPU instead of
 // each under-filling it in turn.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "handle.h"
@@ -199,6 +201,42 @@ int capture(mcm_gpu_batch *b) {
     return MCM_OK;
 }
 
+// Runs fn(body index) for every body of the batch on host worker threads
+// (at most the batch's lane count, 16 and the bodies), largest bodies first,
+// each body's calls on its own stream, so that the bodies' GPU work overlaps.
+// Returns the first non-zero status (the other workers stop taking bodies).
+template <typename F>
+int for_each_body(mcm_gpu_batch *b, F &&fn) {
+    const int nb = (int)b->bodies.size();
+    std::vector<int> order(nb);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->bodies[x]->np > b->bodies[y]->np; });
+    std::atomic<int> next{0}, err{0};
+    const int nthreads = std::max(1, std::min({b->lanes, 16, nb}));
+    auto work = [&]() {
+        if (cudaSetDevice(b->device) != cudaSuccess) {
+            int z = 0;
+            err.compare_exchange_strong(z, (int)MCM_ECUDA);
+            return;
+        }
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= nb || err.load() != 0) return;
+            const int st = fn(order[k]);
+            if (st != MCM_OK) {
+                int z = 0;
+                err.compare_exchange_strong(z, st);
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return err.load();
+}
+
 }  // namespace
 }  // namespace mcm_host
 
@@ -341,6 +379,23 @@ int mcm_gpu_batch_create(mcm_gpu_handle *const *bodies, int nbodies, int lanes, 
     assign_lanes(b);
     *out = b;
     return MCM_OK;
+}
+
+int mcm_gpu_batch_adjoint_forward(mcm_gpu_batch *b, int nsteps, const double *const *dts, int checkpoint_every) {
+    if (!b || !dts || nsteps <= 0 || checkpoint_every <= 0) return MCM_EINVAL;
+    for (size_t k = 0; k < b->bodies.size(); ++k)
+        if (!dts[k]) return MCM_EINVAL;
+    return for_each_body(b, [&](int k) { return mcm_gpu_adjoint_forward(b->bodies[k], nsteps, dts[k], checkpoint_every); });
+}
+
+int mcm_gpu_batch_adjoint_backward(mcm_gpu_batch *b, const double *const *xbar, const double *const *vbar,
+                                   double *const *param_bar, double *const *xbar0, double *const *vbar0) {
+    if (!b) return MCM_EINVAL;
+    return for_each_body(b, [&](int k) {
+        return mcm_gpu_adjoint_backward(b->bodies[k], xbar ? xbar[k] : nullptr, vbar ? vbar[k] : nullptr,
+                                        param_bar ? param_bar[k] : nullptr, xbar0 ? xbar0[k] : nullptr,
+                                        vbar0 ? vbar0[k] : nullptr);
+    });
 }
 
 int mcm_gpu_batch_destroy(mcm_gpu_batch *b) {

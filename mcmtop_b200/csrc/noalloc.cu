@@ -1,13 +1,13 @@
 // noalloc.cu -- allocation-free variant of the per-material energy sums.
 //
-// mcm_gpu_calctotale_noalloc computes the same per-material kinetic energy,
-// internal energy and momentum sums as the energy reduction inside
-// mcm_gpu_step_b, from device arrays the caller already owns, without
-// allocating device memory.  It exists for callers that cannot call
-// cudaMalloc: host codes that hand all device memory to their own pool or
-// map MCM's particle arrays to the device once and forbid further
-// allocations, and drivers that must not add the device-wide synchronisation
-// of cudaMalloc/cudaFree inside a time step.
+// mcm_gpu_calctotale_noalloc computes the per-material kinetic energy,
+// internal energy and momentum sums that mcm_gpu_step_b computes (over every
+// particle, with no active-particle filter, as step_b does), from device
+// arrays the caller already owns, without allocating device memory.  It
+// exists for callers that cannot call cudaMalloc: host codes that hand all
+// device memory to their own pool or map the particle arrays to the device
+// once and forbid further allocations, and drivers that must not add the
+// device-wide synchronisation of cudaMalloc/cudaFree inside a time step.
 //
 // Scratch: the block partial sums live in g_noalloc_partials, a file-scope
 // __device__ array of kNoAllocBlocks x 5 x MCM_GPU_MAX_MATERIALS doubles
@@ -15,8 +15,6 @@
 // until the process exits.  All calls share it: each call overwrites every
 // slot it later reads, so nothing has to start at zero, but calls whose
 // kernels overlap on the GPU (different streams or devices sharing it) race.
-#include <mutex>
-
 #include "kernels.h"
 
 namespace {
@@ -27,8 +25,9 @@ constexpr int kNoAllocValues = 5 * MCM_GPU_MAX_MATERIALS;
 
 __device__ __align__(256) double g_noalloc_partials[kNoAllocBlocks * kNoAllocValues];
 
-// Per-block sums: slot [block][5*(m-1) + {ke, ie, mom_x, mom_y, mom_z}].
-// Particles with a material id outside 1..nmat are not counted.
+// Per-block sums: slot [block][5*(m-1) + {ke, ie, mom_x, mom_y, mom_z}] of
+// 0.5 m |v|^2, e and m |v_d| over the particles of material m.  Particles with
+// a material id outside 1..nmat are not counted.
 __global__ void __launch_bounds__(kNoAllocThreads)
 k_calctotale_partials(const double *mass, const double *vabs, const double *v, const double *e, const int *mat,
                       int np, int nmat, double *partials) {
@@ -38,9 +37,9 @@ k_calctotale_partials(const double *mass, const double *vabs, const double *v, c
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
             if (mat[i] != m) continue;
             const double mi = mass[i], va = vabs[i];
-            acc[0] += 0.5 * mi * (va * va);                 // MCM/mcm_calctotale.f90:37
-            acc[1] += e[i];                                 // :49
-            acc[2] += mi * fabs(v[3 * (size_t)i + 0]);      // :39-41
+            acc[0] += 0.5 * mi * (va * va);
+            acc[1] += e[i];
+            acc[2] += mi * fabs(v[3 * (size_t)i + 0]);
             acc[3] += mi * fabs(v[3 * (size_t)i + 1]);
             acc[4] += mi * fabs(v[3 * (size_t)i + 2]);
         }
@@ -59,8 +58,8 @@ k_calctotale_partials(const double *mass, const double *vabs, const double *v, c
     }
 }
 
-// One block: fixed-order sum of the block partials, then the totals of
-// MCM/mcm_calctotale.f90:53-60.
+// One block: fixed-order sum of the block partials, then the totals (sums of
+// ke and ie over the materials, and their sum), as step_b returns them.
 __global__ void k_calctotale_finish(const double *partials, int nmat, double *out) {
     __shared__ double sm[32];
     for (int v = 0; v < 5 * nmat; ++v) {
@@ -86,20 +85,13 @@ __global__ void k_calctotale_finish(const double *partials, int nmat, double *ou
     }
 }
 
-// Device address of g_noalloc_partials, looked up once per device.
-std::mutex g_scratch_mu;
-void *g_scratch_ptr[64] = {};
-
+// Device address of g_noalloc_partials in the current device's context.  It
+// is looked up on every call (cudaGetSymbolAddress allocates nothing), so a
+// context that was torn down and recreated never sees a stale address.
 int scratch_address(double **out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MCM_ECUDA;
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return MCM_ECUDA;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = static_cast<double *>(g_scratch_ptr[dev]);
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return MCM_ECUDA;
+    *out = static_cast<double *>(p);
     return MCM_OK;
 }
 
@@ -109,11 +101,14 @@ extern "C" int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs
                                           const int *mat, int np, int nmat, double *energies, void *stream) {
     if (!mass || !vabs || !v || !e || !mat || !energies || np < 0) return MCM_EINVAL;
     if (nmat < 1 || nmat > MCM_GPU_MAX_MATERIALS) return MCM_EINVAL;   // scratch holds 16 materials
+    // an error left pending by the caller's earlier CUDA calls is not this call's
+    if (cudaPeekAtLastError() != cudaSuccess) return MCM_ECUDA;
     double *partials = nullptr;
     int st = scratch_address(&partials);
     if (st != MCM_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_calctotale_partials<<<kNoAllocBlocks, kNoAllocThreads, 0, s>>>(mass, vabs, v, e, mat, np, nmat, partials);
+    if (cudaGetLastError() != cudaSuccess) return MCM_ECUDA;
     k_calctotale_finish<<<1, 256, 0, s>>>(partials, nmat, energies);
     if (cudaGetLastError() != cudaSuccess) return MCM_ECUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return MCM_ECUDA;

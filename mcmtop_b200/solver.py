@@ -419,6 +419,42 @@ class Batch:
         return (_abi.Time * len(self.solvers))(*[_abi.Time(s.dt, s.dtold, s.ptime, s.deck.endtime)
                                                   for s in self.solvers])
 
+    def adjoint_forward(self, dts_per_body, checkpoint_every: int = 50) -> None:
+        """mcm_gpu_adjoint_forward of every body at once (mcm_gpu_batch_adjoint_forward):
+        body b runs len(dts_per_body[b]) - 1 steps with its prescribed dt schedule."""
+        ds = [np.ascontiguousarray(d, dtype=np.float64) for d in dts_per_body]
+        if len(ds) != len(self.solvers) or len({len(d) for d in ds}) != 1:
+            raise ValueError("one dt schedule per body, all of the same length")
+        ptrs = (_abi._DP * len(ds))(*[_dptr(d) for d in ds])
+        check(self.lib.mcm_gpu_batch_adjoint_forward(self.b, len(ds[0]) - 1, ptrs, int(checkpoint_every)),
+              "mcm_gpu_batch_adjoint_forward", self.solvers[0].h)
+        for s_, d in zip(self.solvers, ds):
+            s_.dtold, s_.dt = float(d[-2]), float(d[-1])
+
+    def adjoint_backward(self, xbars=None, vbars=None):
+        """mcm_gpu_batch_adjoint_backward: per body the adjoints of its final x, v
+        ((np, 3) arrays or None) -> lists of (param_bar (nmat, 4), xbar0, vbar0)."""
+        n = len(self.solvers)
+        keep = []
+
+        def ptrs(arrays):
+            if arrays is None:
+                return None
+            out = []
+            for a in arrays:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(a)
+                out.append(_dptr(a))
+            return (_abi._DP * n)(*out)
+
+        pb = [np.zeros((s_.nmat, 4)) for s_ in self.solvers]
+        x0 = [np.zeros((s_.n, 3)) for s_ in self.solvers]
+        v0 = [np.zeros((s_.n, 3)) for s_ in self.solvers]
+        outs = [(_abi._DP * n)(*[_dptr(a) for a in arrs]) for arrs in (pb, x0, v0)]
+        check(self.lib.mcm_gpu_batch_adjoint_backward(self.b, ptrs(xbars), ptrs(vbars), *outs),
+              "mcm_gpu_batch_adjoint_backward", self.solvers[0].h)
+        return pb, x0, v0
+
     def run(self, nsteps: int) -> np.ndarray:
         """nsteps iterations of every body; returns the iterations each completed."""
         t = self._times()

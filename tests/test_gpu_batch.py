@@ -146,3 +146,53 @@ def test_batch_autotune_restores_states(lib):
     for a, b in zip(alone, together):
         same_state(a, b)
     batch.close()
+
+
+def _schedule(deck, nsteps):
+    s = Solver(deck, _abi.PREC_FP64)
+    out = [s.dt]
+    for _ in range(nsteps):
+        s.step_a()
+        s.dt_update()
+        out.append(s.dt)
+        s.step_b()
+        s.step_c()
+    s.close()
+    return np.array(out)
+
+
+def _length_adjoint(x):
+    xbar = np.zeros_like(x)
+    xbar[int(x[:, 2].argmax()), 2] += 1.0
+    xbar[int(x[:, 2].argmin()), 2] -= 1.0
+    return xbar
+
+
+def test_batched_adjoint_matches_each_body_alone(lib):
+    """Gradients of the final bar length of every body of a batch
+    (mcm_gpu_batch_adjoint_forward/backward, worker threads over the bodies)
+    equal those of each body's own adjoint calls: parameter gradients and the
+    initial-state adjoints.  Ghost-parent adjoints are summed with atomics, so
+    the comparison allows the last bits (1e-12 relative)."""
+    decks = bodies()
+    nsteps, every = 24, 7
+    dts = [_schedule(d, nsteps) for d in decks]
+    batched = [Solver(d, _abi.PREC_FP64) for d in decks]
+    batch = Batch(batched, lanes=3)
+    batch.adjoint_forward(dts, every)
+    xbars = [_length_adjoint(s.download(["x"])["x"]) for s in batched]
+    pb, x0, v0 = batch.adjoint_backward(xbars, None)
+    batch.close()
+    for k, d in enumerate(decks):
+        alone = Solver(d, _abi.PREC_FP64)
+        alone.adjoint_forward(dts[k], every)
+        xa = alone.download(["x"])["x"]
+        assert np.array_equal(xa, batched[k].download(["x"])["x"]), k      # same forward, bitwise
+        pa, xa0, va0 = alone.adjoint_backward(_length_adjoint(xa), None)
+        alone.close()
+        assert np.all(np.isfinite(pb[k])) and np.abs(pb[k]).max() > 0
+        assert np.max(np.abs(pb[k] - pa)) <= 1e-12 * np.abs(pa).max(), (k, pb[k], pa)
+        assert np.max(np.abs(x0[k] - xa0)) <= 1e-12 * np.abs(xa0).max(), k
+        assert np.max(np.abs(v0[k] - va0)) <= 1e-12 * np.abs(va0).max(), k
+    for s in batched:
+        s.close()

@@ -51,6 +51,40 @@ def test_noalloc_energies_match_step_b(gpu_lib):
     sol.close()
 
 
+def test_noalloc_several_materials(gpu_lib):
+    # two materials: every slot of the 5*nmat+3 output against step_b's sums,
+    # then with some material ids outside 1..nmat, which the call skips
+    from mcmtop_b200.deck import two_material_bar
+
+    lib = gpu_lib
+    deck = two_material_bar()
+    sol = Solver(deck, _abi.PREC_FP64, device=0)
+    for _ in range(4):
+        sol.step()
+    sol.step_a()
+    sol.dt_update()
+    ref = sol.step_b().copy()
+    state = sol.download(["mass", "vabs", "v", "e", "mat"])
+    sol.close()
+    got = _noalloc_energies(lib, state, 2)
+    assert np.max(np.abs(got - ref)) <= 1e-13 * np.abs(ref).max(), (got, ref)
+    bad = dict(state)
+    mat = state["mat"].copy()
+    rng = np.random.default_rng(5)
+    odd = rng.choice(len(mat), size=len(mat) // 10, replace=False)
+    mat[odd[: len(odd) // 2]] = 0
+    mat[odd[len(odd) // 2:]] = 3
+    bad["mat"] = mat
+    got = _noalloc_energies(lib, bad, 2)
+    want = []
+    for m in (1, 2):
+        sel = mat == m
+        ms, va, v = state["mass"][sel], state["vabs"][sel], state["v"][sel]
+        want += [(0.5 * ms * va * va).sum(), state["e"][sel].sum(), *(ms[:, None] * np.abs(v)).sum(axis=0)]
+    want += [want[0] + want[5], want[1] + want[6], want[0] + want[5] + want[1] + want[6]]
+    assert np.allclose(got, want, rtol=1e-12, atol=0.0), (got, want)
+
+
 def test_noalloc_rejects_too_many_materials(gpu_lib):
     st = gpu_lib.mcm_gpu_calctotale_noalloc(1, 1, 1, 1, 1, 10, _abi.MAX_MATERIALS + 1, 1, None)
     assert st == _abi.MCM_EINVAL
