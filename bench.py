@@ -527,6 +527,8 @@ def gpu_arm(args):
     if args.precision == "mixed" and not args.no_compare:
         ref = Solver(deck, _abi.PREC_FP64, device=local, reorder_interval=args.reorder)
         ref.set_diagnostics(False)
+        if args.search_kind:
+            ref.set_tuning(search_kind=args.search_kind)
         ref.run(args.warmup)
         barrier()
         ref.timer_start()
@@ -537,7 +539,8 @@ def gpu_arm(args):
             raise RuntimeError(f"FP64 run stopped after {done64} of {args.steps} steps")
         v64 = job_rate(deck.np * args.steps, ws, ms64)
         fp64 = {"value": round(v64, 1), "ms_per_step": round(ms64 / args.steps, 4),
-                "mixed_over_fp64": round(value / v64, 3)}
+                "mixed_over_fp64": round(value / v64, 3),
+                "note": "FP64 with fused multiply-add and cooperative gathers (the optimised FP64 step)"}
         if rank == 0:
             fields = ["x", "v", "rho", "e", "p", "c", "efps", "sigma", "q", "vabs"]
             a_ = sol.download(fields)
@@ -554,6 +557,25 @@ def gpu_arm(args):
                         "worst": float(f"{max(err.values()):.3e}"),
                         "length_rel_diff": float(f"{abs(la - lb) / lb:.3e}")}
         ref.close()
+        # the plain FP64 step: the reference's expressions and summation order,
+        # no fused multiply-add, one thread per particle (MCM_PREC_FP64_EXACT)
+        ex = Solver(deck, _abi.PREC_FP64_EXACT, device=local, reorder_interval=args.reorder)
+        ex.set_diagnostics(False)
+        if args.search_kind:
+            ex.set_tuning(search_kind=args.search_kind)
+        ex.run(args.warmup)
+        barrier()
+        ex.timer_start()
+        done_ex = ex.run(args.steps)
+        ms_ex = max_over_ranks(ex.timer_stop(), f"cuda:{local}")
+        ex.close()
+        if done_ex != args.steps:
+            raise RuntimeError(f"FP64-exact run stopped after {done_ex} of {args.steps} steps")
+        v_ex = job_rate(deck.np * args.steps, ws, ms_ex)
+        fp64["exact"] = {"value": round(v_ex, 1), "ms_per_step": round(ms_ex / args.steps, 4),
+                         "mixed_over_fp64_exact": round(value / v_ex, 3),
+                         "note": "the plain FP64 step: reference expressions and summation order, no fused "
+                                 "multiply-add, one thread per particle"}
 
     ensemble = None
     if args.ens_bodies > 0:

@@ -117,6 +117,12 @@ typedef struct {
     int nbr_stride;            /* initial neighbour-table stride (0: automatic) */
     int reorder_interval;      /* steps between particle re-sorts (0: never) */
     int block_size;            /* threads per block for the pair kernels (0: tuned default) */
+    double nbr_skin;           /* 0: neighbour lists rebuilt from the cell list every step (the
+                                  reference).  > 0 (FP64 and mixed precision, constant h): a skin
+                                  list per particle of the particles within h_i + h_j + nbr_skin*hmax,
+                                  rebuilt only when some particle has moved nbr_skin*hmax/2 since the
+                                  last build, filtered every step to the reference's neighbour sets
+                                  (not its order).  No counterpart in the reference. */
 } mcm_gpu_config;
 
 /* Host views of the particle arrays (Fortran layout, np particles).  NULL
@@ -224,6 +230,8 @@ int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, 
 int mcm_gpu_grid(mcm_gpu_handle *h, int *gridlim, double *gridmin, double *gridsize);
 int mcm_gpu_energies(mcm_gpu_handle *h, double *energies);
 
+/* Skin-list builds since mcm_gpu_create (nbr_skin > 0; 0 otherwise). */
+int mcm_gpu_skin_builds(mcm_gpu_handle *h, long long *builds);
 /* Mean neighbour count of the last search (for the roofline accounting). */
 int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp);
 

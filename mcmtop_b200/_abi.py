@@ -48,7 +48,7 @@ class Config(C.Structure):
         ("drelax_scale", C.c_double), ("boundary", C.c_int), ("boundary_code", C.c_int * 6),
         ("boundary_x", C.c_double * 6), ("baseaccel", C.c_int), ("base_a", C.c_double * 3),
         ("tssf", C.c_double), ("hmax", C.c_double), ("precision", C.c_int), ("nbr_stride", C.c_int),
-        ("reorder_interval", C.c_int), ("block_size", C.c_int),
+        ("reorder_interval", C.c_int), ("block_size", C.c_int), ("nbr_skin", C.c_double),
     ]
 
 
@@ -120,6 +120,7 @@ def load() -> C.CDLL:
         "mcm_gpu_grid": ([H, _IP, _DP, _DP], C.c_int),
         "mcm_gpu_energies": ([H, _DP], C.c_int),
         "mcm_gpu_stats": ([H, _DP, _IP, _IP, _IP], C.c_int),
+        "mcm_gpu_skin_builds": ([H, C.POINTER(C.c_longlong)], C.c_int),
         "mcm_gpu_set_diagnostics": ([H, C.c_int], C.c_int),
         "mcm_gpu_calctotale_noalloc": ([C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
         "mcm_gpu_profile": ([H, C.c_int], C.c_int),

@@ -44,6 +44,7 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.h_opt = c.h_opt;
     p.contacttype = c.contacttype;
     p.contact = (c.contacttype > 0 && nmat > 1) ? 1 : 0;
+    p.skin = c.nbr_skin > 0.0 ? c.nbr_skin : 0.0;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;
@@ -99,6 +100,11 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
     CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
     CK(cudaMemsetAsync(h->A.gnnbr, 0, sizeof(int) * np, h->stream));
+    if (h->A.prm.skin > 0.0) {
+        if ((st = dalloc(h, &h->A.pos_of, np))) return st;
+        if ((st = dalloc(h, &h->A.supn, np))) return st;
+        if ((st = dalloc(h, &h->A.xref, 3 * np))) return st;
+    }
     if (h->A.prm.contact) {
         if ((st = dalloc(h, &h->A.ncont, np))) return st;
         if ((st = dalloc(h, &h->A.gncont, np))) return st;
@@ -178,6 +184,17 @@ int alloc_contacts(mcm_gpu_handle *h, int cstride, int gcstride) {
     return MCM_OK;
 }
 
+// Skin lists (nbr_skin > 0): sstride entries per particle; a new table holds
+// no lists, so the next step builds them.
+int alloc_skin(mcm_gpu_handle *h, int sstride) {
+    int st;
+    h->A.sstride = round_up(sstride, 4);
+    if ((st = dalloc(h, &h->A.sup, (size_t)h->A.sstride * h->npad))) return st;
+    launch_skin_force(h->A, h->stream);
+    CK(cudaGetLastError());
+    return MCM_OK;
+}
+
 int reset_status(mcm_gpu_handle *h) {
     CK(cudaMemsetAsync(h->A.status, 0, sizeof(DevStatus), h->stream));
     return MCM_OK;
@@ -203,6 +220,10 @@ int regrow(mcm_gpu_handle *h, int *grew) {
                 if (s.req_stride > ns) ns = s.req_stride + s.req_stride / 8 + 8;
                 if (s.req_gstride > ng) ng = round_up(s.req_gstride + s.req_gstride / 8 + 8, 8);
                 if ((st = alloc_table(h, ns, ng))) return st;
+                *grew = 1;
+            }
+            if (h->A.prm.skin > 0.0 && s.req_sstride > h->A.sstride) {
+                if ((st = alloc_skin(h, s.req_sstride + s.req_sstride / 8 + 8))) return st;
                 *grew = 1;
             }
             int cs = h->A.cstride, gcs = h->A.gcstride;
@@ -302,8 +323,10 @@ void enqueue_part_a(mcm_gpu_handle *h) {
     StepArgs &a = h->A;
     const int every = h->cfg.reorder_interval;
     if (every > 0 && h->have_cells && (h->steps_enqueued % every) == 0) {
-        Scope sc(h, R_MISC, 2 * (NFIELD + 4));
+        Scope sc(h, R_MISC, 2 * (NFIELD + 4) + (a.prm.skin > 0.0 ? 1 : 0));
         launch_reorder(a, h->stream);
+        // the skin lists hold state indices, which the re-sort permutes
+        if (a.prm.skin > 0.0) launch_skin_force(a, h->stream);
     }
     ++h->steps_enqueued;
     h->have_cells = true;
@@ -316,7 +339,10 @@ void enqueue_part_a(mcm_gpu_handle *h) {
         Scope sc(h, R_GHOSTS, 3 * active_planes(h));
         launch_ghosts(a, h->stream);
     }
-    {
+    if (a.prm.skin > 0.0) {
+        Scope sc(h, R_SEARCH, 4);
+        launch_skin_search(a, h->stream);
+    } else {
         Scope sc(h, R_SEARCH, 1);
         launch_search(a, h->stream);
     }
@@ -586,6 +612,10 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     *out = nullptr;
     if (cfg->ndim != 3) return MCM_EUNSUPPORTED;
     if (cfg->contacttype < 0) return MCM_EINVAL;
+    if (!(cfg->nbr_skin >= 0.0)) return MCM_EINVAL;
+    // skin lists: the reference's neighbour order is not kept, and the skin
+    // bound assumes smoothing lengths that do not change between builds
+    if (cfg->nbr_skin > 0.0 && (cfg->precision == MCM_PREC_FP64_EXACT || cfg->h_opt != 0)) return MCM_EUNSUPPORTED;
     if (cfg->h_opt < 0 || cfg->h_opt > 2 || cfg->veloc_opt < 0 || cfg->veloc_opt > 1) return MCM_EINVAL;
     if (cfg->krtype != 0 && cfg->krtype != 1) return MCM_EUNSUPPORTED;
     if (cfg->disctype != 0 && cfg->disctype != 1) return MCM_EINVAL;
@@ -660,6 +690,8 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     h->A.plane_base = (int *)p; p += 32;
     h->A.n_inside = (int *)p; p += 32;
     h->A.hmax = (double *)p; p += 32;
+    h->A.skin_d2 = (unsigned long long *)p; p += 32;
+    h->A.skin_flags = (int *)p; p += 32;
     h->A.energy = (double *)p;
     cudaMallocHost((void **)&h->h_time, 4096);
     char *q = (char *)h->h_time;
@@ -672,6 +704,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     int entries = cfg->nbr_stride > 0 ? cfg->nbr_stride : 100;
     TRY(alloc_table(h, entries, cfg->boundary ? 48 : 8));
     if (h->A.prm.contact) TRY(alloc_contacts(h, 16, 8));
+    if (h->A.prm.skin > 0.0) TRY(alloc_skin(h, entries + entries / 2));
     TRY(alloc_cells(h, 1 << 16));
     TRY(alloc_ghosts(h, cfg->boundary ? std::max(4096, np / 8) : 32));
     TRY(dalloc(h, &h->d_nppermat, (size_t)nmat));
@@ -692,7 +725,8 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,
                     h->A.grec0, h->A.grec1, h->A.grec2, h->A.gnbr, h->A.rec3, h->A.grec3,
-                    h->A.cidx, h->A.gcont, h->A.ncont, h->A.gncont};
+                    h->A.cidx, h->A.gcont, h->A.ncont, h->A.gncont,
+                    h->A.sup, h->A.supn, h->A.pos_of, h->A.xref};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (double *p : h->adj_ckpt)
@@ -849,6 +883,8 @@ int finish_upload(mcm_gpu_handle *h, const double *coord_maxmin) {
     } else {
         if ((st = compute_bbox(h))) return st;
     }
+    // new positions and smoothing lengths: the next step builds the skin lists
+    if (h->A.prm.skin > 0.0) launch_skin_force(h->A, h->stream);
     CK(cudaStreamSynchronize(h->stream));
     h->initialised = true;
     return MCM_OK;
@@ -1267,6 +1303,19 @@ int mcm_gpu_energies(mcm_gpu_handle *h, double *energies) {
     return MCM_OK;
 }
 
+int mcm_gpu_skin_builds(mcm_gpu_handle *h, long long *builds) {
+    int st;
+    if ((st = check_handle(h))) return st;
+    if (!builds) return MCM_EINVAL;
+    *builds = 0;
+    if (h->A.prm.skin <= 0.0) return MCM_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    int flags[3] = {0, 0, 0};
+    CK(cudaMemcpy(flags, h->A.skin_flags, sizeof(flags), cudaMemcpyDeviceToHost));
+    *builds = flags[2];
+    return MCM_OK;
+}
+
 int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride, int *ngp) {
     int st;
     if ((st = check_handle(h))) return st;
@@ -1386,6 +1435,7 @@ int adj_check(mcm_gpu_handle *h) {
     if (h->cfg.h_opt != 0 || h->cfg.veloc_opt != 0)
         return set_error(h, MCM_EUNSUPPORTED, "adjoint: constant smoothing length without XSPH only");
     if (h->A.prm.contact) return set_error(h, MCM_EUNSUPPORTED, "adjoint: no repulsive contact (contacttype > 0)");
+    if (h->A.prm.skin > 0.0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: neighbour lists rebuilt every step (nbr_skin 0)");
     for (const mcm_gpu_material &m : h->mats)
         if (m.model != 10 || m.eos != 41) return set_error(h, MCM_EUNSUPPORTED, "adjoint: model 10 with EOS 41 only");
     return MCM_OK;

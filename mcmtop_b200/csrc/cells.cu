@@ -230,6 +230,7 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
         int i = a.cell_list[p];
         const double x = X[i], y = Y[i], z = Z[i], h = H[i];
         a.cpos[p] = make_double4(x, y, z, h);
+        if (a.pos_of) a.pos_of[i] = p;
         a.cmat[p] = a.F.mat[i];
         const int key = a.key[i];
         a.ckey[p] = key;
@@ -1058,6 +1059,269 @@ __global__ void __launch_bounds__(kCellWarps * 32, 3) k_search_cell(StepArgs a) 
         if (want_mind) a.F.f[FMINDIST][a.cell_list[t]] = 1.0e20;
         atomicMax(&a.status->max_nbr, nn);
     }
+}
+
+// ------------------------------------------------------------- skin lists
+// For the FP64-fast and mixed steps, whose sums do not follow the reference's
+// neighbour order: the neighbour lists of a step are filtered from a skin
+// list, a superset of each particle's neighbours kept from the last build.
+// A pair (i, j) missing from the skin list was at least h_i + h_j + skin apart
+// at the build; while every particle has moved less than skin/2 since then,
+// it is still at least h_i + h_j apart, so it cannot be a neighbour.  The
+// step rebuilds the skin lists when the largest displacement reaches skin/2
+// (or on request), and filters them every step with k_search's FP32 decision
+// and FP64 tie test, among the candidates in the 27 cells around the
+// particle's cell of the current grid (the only ones the reference examines),
+// so the neighbour sets are the reference's; their order is the skin list's.
+
+// Largest squared displacement since the last build (state order).
+__global__ void __launch_bounds__(256) k_skin_disp(StepArgs a) {
+    __shared__ unsigned long long sm[8];
+    if (a.status->code) return;
+    unsigned long long best = 0ull;
+    const double *X = a.F.f[FX], *Y = a.F.f[FY], *Z = a.F.f[FZ];
+    const size_t np = a.npad;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double dx = X[i] - a.xref[i], dy = Y[i] - a.xref[np + i], dz = Z[i] - a.xref[2 * np + i];
+        const double d2 = dx * dx + dy * dy + dz * dz;   // >= 0: the bit pattern orders like the value
+        const unsigned long long b = (unsigned long long)__double_as_longlong(d2);
+        best = b > best ? b : best;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+        best = v > best ? v : best;
+    }
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = sm[w] > best ? sm[w] : best;
+        atomicMax(a.skin_d2, best);
+    }
+}
+
+// One thread: build when asked to, or when 2 * max displacement >= skin.
+__global__ void k_skin_decide(StepArgs a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (a.status->code) return;
+    const double dmax = sqrt(__longlong_as_double((long long)*a.skin_d2));
+    const double skin = a.prm.skin * a.hmax[0];
+    const int need = (a.skin_flags[0] != 0 || !(2.0 * dmax < skin)) ? 1 : 0;
+    a.skin_flags[1] = need;
+    a.skin_flags[0] = 0;
+    if (need) a.skin_flags[2] += 1;
+    *a.skin_d2 = 0ull;
+}
+
+// The skin lists: one thread per cell-order position, candidates in the
+// cells within reach (up to two cells away), accepted when their FP32
+// distance lies below h_i + h_j + skin with a margin (a superset needs no
+// exact test).  Positions outside the grid keep an empty list.
+__global__ void __launch_bounds__(256) k_skin_build(StepArgs a) {
+    if (a.status->code || !a.skin_flags[1]) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int i = a.cell_list[t];
+    const size_t np = a.npad;
+    const double4 xi = a.cpos[t];
+    a.xref[i] = xi.x;
+    a.xref[np + i] = xi.y;
+    a.xref[2 * np + i] = xi.z;
+    const int key = a.ckey[t];
+    int nn = 0;
+    if (key >= 0) {
+        const int gl0 = a.grid->gridlim[0], gl1 = a.grid->gridlim[1], gl2 = a.grid->gridlim[2];
+        const int bx = key % gl0 + 1, by = (key / gl0) % gl1 + 1, bz = key / (gl0 * gl1) + 1;
+        const float cs[3] = {(float)(1.0 / a.grid->gridsize[0]), (float)(1.0 / a.grid->gridsize[1]),
+                             (float)(1.0 / a.grid->gridsize[2])};
+        const float skin = (float)(a.prm.skin * a.hmax[0]);
+        const float4 ui = a.cposf[t];
+        const float reach = ui.w + (float)a.grid->hcut + skin;
+        const float reach2 = reach * reach * 1.001f + 1.0e-3f * cs[0] * cs[0];
+        int *out = a.sup + (size_t)i * a.sstride;
+        for (int nz = max(bz - 2, 1); nz <= min(bz + 2, gl2); ++nz) {
+            const float qz = ui.z + (float)(bz - nz) * cs[2];
+            const float gz = nz < bz ? ui.z + (float)(bz - nz - 1) * cs[2] : (nz > bz ? (float)(nz - bz) * cs[2] - ui.z : 0.0f);
+            for (int my = max(by - 2, 1); my <= min(by + 2, gl1); ++my) {
+                const float qy = ui.y + (float)(by - my) * cs[1];
+                const float gy = my < by ? ui.y + (float)(by - my - 1) * cs[1] : (my > by ? (float)(my - by) * cs[1] - ui.y : 0.0f);
+                const float gyz = fmaxf(gy, 0.0f) * fmaxf(gy, 0.0f) + fmaxf(gz, 0.0f) * fmaxf(gz, 0.0f);
+                if (gyz > reach2) continue;
+                for (int lx = max(bx - 2, 1); lx <= min(bx + 2, gl0); ++lx) {
+                    const float gx = lx < bx ? ui.x + (float)(bx - lx - 1) * cs[0] : (lx > bx ? (float)(lx - bx) * cs[0] - ui.x : 0.0f);
+                    if (gyz + fmaxf(gx, 0.0f) * fmaxf(gx, 0.0f) > reach2) continue;
+                    const int k = (lx - 1) + gl0 * ((my - 1) + gl1 * (nz - 1));
+                    const int cb = a.cell_start[k], ce = a.cell_start[k + 1];
+                    const float qx = ui.x + (float)(bx - lx) * cs[0];
+                    for (int p = cb; p < ce; ++p) {
+                        if (p == t) continue;
+                        const float4 c = a.cposf[p];
+                        const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                        const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float r = ui.w + c.w + skin;
+                        if (d2f >= r * r * 1.001f + 1.0e-3f * cs[0] * cs[0]) continue;
+                        if (nn < a.sstride) out[nn] = a.cell_list[p];
+                        ++nn;
+                    }
+                }
+            }
+        }
+    }
+    a.supn[i] = nn;
+    if (nn > a.sstride) {
+        atomicMax(&a.status->req_sstride, nn);
+        raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+    }
+}
+
+// The step's neighbour lists from the skin lists: k_search's decisions on
+// the candidates that lie in the 27 cells around the particle's cell, in
+// skin-list order; ghosts, contacts, minimum distances and counts as k_search.
+__global__ void __launch_bounds__(256, 4) k_skin_filter(StepArgs a) {
+    if (a.status->code) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int np = a.npad;
+    const int cap = a.nstride;
+    const int key = a.ckey[t];
+    const int i = a.cell_list[t];
+    const bool with_self = (a.prm.disctype == 1);
+    const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
+    const bool contact = a.prm.contact != 0;
+    int nn = 0, gn = 0, nc = 0, gcn = 0;
+    double mind = 1.0e20;
+    if (key >= 0) {
+        const int gl0 = a.grid->gridlim[0], gl1 = a.grid->gridlim[1], gl2 = a.grid->gridlim[2];
+        const int bx = key % gl0 + 1, by = (key / gl0) % gl1 + 1, bz = key / (gl0 * gl1) + 1;
+        const double4 xi = a.cpos[t];
+        const float4 ui = a.cposf[t];
+        const float cs[3] = {(float)(1.0 / a.grid->gridsize[0]), (float)(1.0 / a.grid->gridsize[1]),
+                             (float)(1.0 / a.grid->gridsize[2])};
+        const float csm = fmaxf(cs[0], fmaxf(cs[1], cs[2]));
+        const float kb = 2.44140625e-4f * csm * csm;
+        const float khi = 1.0f + 2.44140625e-4f, klo = 1.0f - 2.44140625e-4f;
+        const int mati = a.cmat[t];
+        unsigned *out = a.nidx + (size_t)t * cap;
+        unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
+        const int *cand = a.sup + (size_t)i * a.sstride;
+        const int ns = a.supn[i];
+        // with kernel contact the other materials follow the own material's neighbours
+        const int passes = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
+        for (int pass = 0; pass < passes; ++pass) {
+            for (int k = 0; k < ns; ++k) {
+                const int p = a.pos_of[cand[k]];
+                const int kp = a.ckey[p];
+                if (kp < 0) continue;
+                const int ex = kp % gl0 + 1 - bx, ey = (kp / gl0) % gl1 + 1 - by, ez = kp / (gl0 * gl1) + 1 - bz;
+                if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) continue;
+                const float4 c = a.cposf[p];
+                const float dx = (ui.x - (float)ex * cs[0]) - c.x;
+                const float dy = (ui.y - (float)ey * cs[1]) - c.y;
+                const float dz = (ui.z - (float)ez * cs[2]) - c.z;
+                const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float hsf = ui.w + c.w;
+                const float r2f = hsf * hsf;
+                if (d2f >= fmaf(r2f, khi, kb)) continue;
+                double d2 = 0.0;
+                if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
+                    const double4 cd = a.cpos[p];
+                    d2 = exact_d2(xi, cd);
+                    const double hs = __dadd_rn(cd.w, xi.w);
+                    if (!(d2 < __dmul_rn(hs, hs))) continue;
+                }
+                const unsigned code = (unsigned)((ex + 1) + 3 * (ey + 1) + 9 * (ez + 1)) << 26;
+                if (contact) {
+                    if (a.cmat[p] != mati) {
+                        if (nc < a.cstride) cout[nc] = (unsigned)p | code;
+                        ++nc;
+                        continue;
+                    }
+                } else if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) {
+                    continue;
+                }
+                if (want_mind) mind = fmin(mind, d2);
+                if (nn < cap) out[nn] = (unsigned)p | code;
+                ++nn;
+            }
+        }
+        if (nn > cap) {
+            atomicMax(&a.status->req_stride, nn);
+            raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+        }
+        if (contact && nc > a.cstride) {
+            atomicMax(&a.status->req_cstride, nc);
+            raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+        }
+        // ghosts: as k_search, from the current grid's ghost cells
+        if (a.prm.boundary) {
+            const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < gl0 ? bx + 1 : gl0;
+            const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < gl1 ? by + 1 : gl1;
+            const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < gl2 ? bz + 1 : gl2;
+            const DevPlanes &pl = a.prm.planes;
+            const bool near = (lo0 == 1 && pl.code[0][0]) || (hi0 == gl0 && pl.code[1][0]) ||
+                              (lo1 == 1 && pl.code[0][1]) || (hi1 == gl1 && pl.code[1][1]) ||
+                              (lo2 == 1 && pl.code[0][2]) || (hi2 == gl2 && pl.code[1][2]);
+            if (near) {
+                const int gpasses = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
+                for (int pass = 0; pass < gpasses; ++pass) {
+                    for (int nz = lo2; nz <= hi2; ++nz)
+                        for (int my = lo1; my <= hi1; ++my)
+                            for (int lx = lo0; lx <= hi0; ++lx) {
+                                const int2 gcl = a.gcell[(lx - 1) + gl0 * ((my - 1) + gl1 * (nz - 1))];
+                                for (int r = 0; r < gcl.y; ++r) {
+                                    const int q = gcl.x + gcl.y - 1 - r;
+                                    const double4 gq = make_double4(a.gx[q], a.gy[q], a.gz[q], a.gh[q]);
+                                    const double d2 = exact_d2(xi, gq);
+                                    const double hs = __dadd_rn(gq.w, xi.w);
+                                    if (d2 < __dmul_rn(hs, hs)) {
+                                        if (contact) {
+                                            if (a.gmat[q] != mati) {
+                                                if (gcn < a.gcstride) a.gcont[(size_t)gcn * np + t] = q;
+                                                ++gcn;
+                                                continue;
+                                            }
+                                        } else if (a.nmat > 1 && (a.gmat[q] == mati) != (pass == 0)) {
+                                            continue;
+                                        }
+                                        mind = fmin(mind, d2);
+                                        if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
+                                        ++gn;
+                                    }
+                                }
+                            }
+                }
+                if (gn > a.gstride) {
+                    atomicMax(&a.status->req_gstride, gn);
+                    raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+                }
+                if (gcn > a.gcstride) {
+                    atomicMax(&a.status->req_gcstride, gcn);
+                    raise_status(a.status, MCM_ENBR_OVERFLOW, i);
+                }
+            }
+        }
+        mind = sqrt(mind);
+    }
+    if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
+    a.nnbr[t] = nn;
+    a.gnnbr[t] = gn;
+    if (contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
+    if (want_mind) a.F.f[FMINDIST][i] = mind;
+    atomicMax(&a.status->max_nbr, nn);
+    atomicMax(&a.status->max_gnbr, gn);
+}
+
+__global__ void k_skin_force(StepArgs a) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) a.skin_flags[0] = 1;
+}
+
+void launch_skin_force(const StepArgs &a, cudaStream_t s) { k_skin_force<<<1, 32, 0, s>>>(a); }
+
+void launch_skin_search(const StepArgs &a, cudaStream_t s) {
+    const int nb = (a.n + 255) / 256;
+    k_skin_disp<<<nb < 148 * 8 ? nb : 148 * 8, 256, 0, s>>>(a);
+    k_skin_decide<<<1, 32, 0, s>>>(a);
+    k_skin_build<<<nb, 256, 0, s>>>(a);
+    k_skin_filter<<<nb, 256, 0, s>>>(a);
 }
 
 void launch_search(const StepArgs &a, cudaStream_t s) {

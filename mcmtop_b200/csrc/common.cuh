@@ -35,6 +35,7 @@ struct DevStatus {
     int req_stride;   // neighbour-list entries needed (real part); -1: a row is too long
     int req_gstride;  // neighbour-table width needed (ghost part)
     int req_ngp;      // ghost storage needed
+    int req_sstride;  // skin-list entries needed
     int req_cstride;  // contact-list entries needed (real contacts)
     int req_gcstride; // contact-list entries needed (ghost contacts)
     long long req_cells;
@@ -71,6 +72,7 @@ struct DevParams {
     int contacttype;  // 0: particles of other materials are neighbours (kernel contact); > 0: contacts
     int contact;      // contacttype > 0 with more than one material: contact lists and repulsion are built
     double drelax_scale, tssf, hmax;
+    double skin;      // > 0: neighbour lists filtered from skin lists kept within h_i + h_j + skin * hmax
     double base_a[3];
     DevPlanes planes;
 };

@@ -60,6 +60,15 @@ struct StepArgs {
     unsigned int *cidx;
     int *gcont, *ncont, *gncont;
     int cstride, gcstride;
+    // skin lists (prm.skin > 0): per STATE index i, the state indices of the
+    // particles within h_i + h_j + skin at the last build, sup[i*sstride + k],
+    // supn[i] of them; the positions x at that build (xref, 3 x npad); pos_of[i]
+    // the cell-order position of state index i in the current cell list
+    int *sup, *supn, *pos_of;
+    int sstride;
+    double *xref;
+    int *skin_flags;                 // [0] force a build, [1] this step builds, [2] builds so far
+    unsigned long long *skin_d2;     // bits of the largest squared displacement since the build
     double *reorder_tmp;   // npad doubles of scratch for the state permutation
     // gather records
     double4 *rec0, *rec1, *rec2;   // per particle
@@ -84,6 +93,9 @@ void launch_grid_setup(const StepArgs &a, cudaStream_t s);
 void launch_cell_build(const StepArgs &a, cudaStream_t s);
 void launch_ghosts(const StepArgs &a, cudaStream_t s);
 void launch_search(const StepArgs &a, cudaStream_t s);
+// skin lists: displacement check, conditional skin-list build, per-step filter
+void launch_skin_search(const StepArgs &a, cudaStream_t s);
+void launch_skin_force(const StepArgs &a, cudaStream_t s);   // the next step rebuilds the skin lists
 void launch_reorder(const StepArgs &a, cudaStream_t s);
 
 // reduce.cu

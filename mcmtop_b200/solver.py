@@ -49,7 +49,8 @@ def material_table(deck: Deck) -> "C.Array":
     return mats
 
 
-def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_interval: int = 0) -> _abi.Config:
+def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_interval: int = 0,
+                     nbr_skin: float = 0.0) -> _abi.Config:
     """Control-card processing of MCM/mcm_control_v2.f90:193-243 and the
     boundary/base-acceleration cards (mcm_inp_symmetry_v2.f90:83-137,
     mcm_baseaccel_in.f90:23-33)."""
@@ -76,12 +77,13 @@ def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_in
     c.precision = precision
     c.nbr_stride = nbr_stride
     c.reorder_interval = reorder_interval
+    c.nbr_skin = nbr_skin
     return c
 
 
 class Solver:
     def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0,
-                 device: int | None = None, reorder_interval: int = 0):
+                 device: int | None = None, reorder_interval: int = 0, nbr_skin: float = 0.0):
         self.lib = _abi.load()
         if device is not None:
             check(self.lib.mcm_gpu_set_device(int(device)), "mcm_gpu_set_device")
@@ -89,7 +91,7 @@ class Solver:
         self.n = deck.np
         self.nmat = len(deck.materials)
         self._mats = material_table(deck)
-        self.cfg = config_from_deck(deck, precision, nbr_stride, reorder_interval)
+        self.cfg = config_from_deck(deck, precision, nbr_stride, reorder_interval, nbr_skin)
         h = C.c_void_p()
         check(self.lib.mcm_gpu_create(C.byref(self.cfg), self._mats, self.nmat, self.n, C.byref(h)),
               "mcm_gpu_create")
@@ -225,6 +227,12 @@ class Solver:
         check(self.lib.mcm_gpu_neighbours(self.h, _iptr(nn), _iptr(nbr), C.byref(s), _iptr(gn), _iptr(gnbr),
                                           C.byref(gs)), "mcm_gpu_neighbours", self.h)
         return nn, nbr, gn, gnbr
+
+    def skin_builds(self) -> int:
+        """Skin-list builds since the handle was created (nbr_skin > 0)."""
+        n = C.c_longlong()
+        check(self.lib.mcm_gpu_skin_builds(self.h, C.byref(n)), "mcm_gpu_skin_builds", self.h)
+        return n.value
 
     def contacts(self):
         """(ncont, cont[np, stride], g_ncont, g_cont[np, g_stride]) with 1-based ids:
