@@ -59,9 +59,15 @@ def parse():
     ap.add_argument("--adj-every", type=int, default=50, help="checkpoint interval")
     ap.add_argument("--ens-bodies", type=int, default=256, help="bars of the batched ensemble (0: skip it)")
     ap.add_argument("--ens-steps", type=int, default=500)
+    ap.add_argument("--ens-adj-steps", type=int, default=40,
+                    help="steps of the ensemble's per-body gradients, batched and body after body (0: skip)")
+    ap.add_argument("--ens-adj-every", type=int, default=10, help="checkpoint interval of the ensemble gradients")
     ap.add_argument("--fluid-steps", type=int, default=20, help="iterations of the 15.6M fluid column (0: skip)")
     ap.add_argument("--long-steps", type=int, default=2000,
                     help="iterations of the 2000-step accuracy run of the configuration, mixed and FP64 (0: skip)")
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="neighbour-list skin as a fraction of hmax for the FP64-fast and mixed runs (0: rebuild "
+                         "the lists every step)")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -132,7 +138,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- roofline
-def algorithmic_bytes(region: str, kbar: float, precision: str) -> float:
+def algorithmic_bytes(region: str, kbar: float, precision: str, skin: bool = False) -> float:
     """Compulsory bytes per particle of one kernel group: the particle's own
     state read and written plus its neighbour list (4-byte entries), with
     ideal caching of the neighbour gathers (they count zero, as do sorts,
@@ -143,9 +149,11 @@ def algorithmic_bytes(region: str, kbar: float, precision: str) -> float:
       constitutive: read v(3) m h rho e p c efps pcut fail sigma(6) rod(6) spin(3) tr vabs;
                     write x(3) rho e p c efps pcut sigma(6) q          224 + 8 + 136
       momentum:     read x v (6) m rho h sigma(6) q e vabs dispbc, count, list;
-                    write x v (6) vabs                                 136 + 4 + 4 + 4K + 56"""
+                    write x v (6) vabs                                 136 + 4 + 4 + 4K + 56
+    With skin lists the search group also reads the positions of the last
+    build (24) and at least K entries of the skin list (4K)."""
     if region == "search":
-        return 36 + 4 + 4 * kbar
+        return 36 + 4 + 4 * kbar + ((24 + 4 * kbar) if skin else 0.0)
     if region == "strain":
         return 72 + 4 + 4 * kbar
     if region == "constitutive":
@@ -340,6 +348,67 @@ def fluid_column_cost(args, local):
                     "every step; device time (CUDA events on the library stream)"}
 
 
+def ensemble_gradients(args, local, decks, prec, lanes, barrier=None):
+    """Config 5's per-body gradients: for every body of this rank's block,
+    d(final bar length)/d(G, yield stress, hardening modulus, EOS-41 s)
+    through --ens-adj-steps steps of the headline precision (FP64 reverse
+    kernels), checkpoints every --ens-adj-every steps, along each body's own
+    dt schedule (recorded from a batched run of the same bodies).  Timed once
+    as a batch (mcm_gpu_batch_adjoint_forward/backward) and once body after
+    body (mcm_gpu_adjoint_forward/backward), from fresh handles both times
+    (each includes the first allocation of its checkpoints); wall clock."""
+    from mcmtop_b200.solver import Batch, Solver
+
+    S, every = args.ens_adj_steps, args.ens_adj_every
+    rec = [Solver(d, prec, device=local) for d in decks]
+    for s in rec:
+        s.set_diagnostics(False)
+    rb = Batch(rec, lanes=lanes)
+    dts = [[s.dt] for s in rec]
+    for _ in range(S):
+        rb.run(1)
+        for k, s in enumerate(rec):
+            dts[k].append(s.dt)
+    rb.close()
+    for s in rec:
+        s.close()
+
+    def length_adjoint(x):
+        xbar = np.zeros_like(x)
+        xbar[int(x[:, 2].argmax()), 2] += 1.0
+        xbar[int(x[:, 2].argmin()), 2] -= 1.0
+        return xbar
+
+    bodies = [Solver(d, prec, device=local) for d in decks]
+    if barrier:
+        barrier()
+    t0 = time.perf_counter()
+    bb = Batch(bodies, lanes=lanes)
+    bb.adjoint_forward(dts, every)
+    xbars = [length_adjoint(s.download(["x"])["x"]) for s in bodies]
+    pb, _, _ = bb.adjoint_backward(xbars, None)
+    t_batch = time.perf_counter() - t0
+    bb.close()
+    for s in bodies:
+        s.close()
+    worst = 0.0
+    t_seq = 0.0
+    for k, d in enumerate(decks):
+        s = Solver(d, prec, device=local)
+        t0 = time.perf_counter()
+        s.adjoint_forward(dts[k], every)
+        pa, _, _ = s.adjoint_backward(length_adjoint(s.download(["x"])["x"]), None)
+        t_seq += time.perf_counter() - t0
+        s.close()
+        worst = max(worst, float(np.max(np.abs(pb[k] - pa)) / max(float(np.max(np.abs(pa))), 1e-300)))
+    return {"gradients": len(decks), "steps": S, "checkpoint_every": every, "loss": "final bar length",
+            "params": ["G", "yield", "hardening", "eos_s"], "batched_s": t_batch, "sequential_s": t_seq,
+            "max_rel_diff_batched_vs_alone": worst,
+            "note": "forward in the headline precision, FP64 reverse kernels; batched = worker threads over the "
+                    "bodies, each on its own stream; ghost-parent adjoints are summed with atomics, so batched "
+                    "and alone agree to the last bits, not bitwise"}
+
+
 def ensemble_cost(args, local, ws=1, rank=0, barrier=None):
     """The calibration ensemble: --ens-bodies independent Taylor bars (radius
     2-4 mm, L/D 6-12, 4k-64k particles log-uniform, yield 200-600 MPa, impact
@@ -394,6 +463,13 @@ def ensemble_cost(args, local, ws=1, rank=0, barrier=None):
     final_len = gather_items(lengths, len(everyone), dev)[:, 0]
     for s in batched + seq:
         s.close()
+    grads = ensemble_gradients(args, local, decks, prec, lanes, barrier) if args.ens_adj_steps > 0 else None
+    if grads is not None:
+        grads["batched_s"] = round(max_over_ranks(grads["batched_s"], dev), 3)
+        grads["sequential_s"] = round(max_over_ranks(grads["sequential_s"], dev), 3)
+        grads["speedup"] = round(grads["sequential_s"] / grads["batched_s"], 3)
+        grads["gradients"] = int(sum_over_ranks(float(grads["gradients"]), dev))
+        grads["max_rel_diff_batched_vs_alone"] = max_over_ranks(grads["max_rel_diff_batched_vs_alone"], dev)
     return {"workload": f"taylor_ensemble_{len(everyone)}x_{n_total}", "bodies": len(everyone),
             "particles": n_total, "ranks": ws, "bodies_per_rank": [len(share(len(everyone), ws, r)) for r in range(ws)],
             "particles_min": min(d.np for d in everyone), "particles_max": max(d.np for d in everyone),
@@ -406,6 +482,7 @@ def ensemble_cost(args, local, ws=1, rank=0, barrier=None):
             "sequential_done_equal": bool(list(done_seq) == [int(k) for k in done]),
             "final_length_cm": {"min": round(float(final_len.min()), 6), "max": round(float(final_len.max()), 6)},
             "init_s_per_body": round(t_init / max(len(decks), 1), 4),
+            "gradients": grads,
             "note": "batched = mcm_gpu_batch_run (graph of one iteration of every body over the tuned lanes); "
                     "sequential = mcm_gpu_run per body, one after the other; wall clock, slowest rank; "
                     "each rank advances its contiguous block of the bodies"}
@@ -425,7 +502,7 @@ def long_run(args, local):
     out = {"workload": f"taylor_bar_{deck.np}", "steps": args.long_steps}
     ends = {}
     for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
-        sol = Solver(deck, prec, device=local, reorder_interval=args.reorder)
+        sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=args.skin)
         sol.set_diagnostics(False)
         sol.timer_start()
         done = sol.run(args.long_steps)
@@ -474,7 +551,8 @@ def gpu_arm(args):
     prec = {"fp64": _abi.PREC_FP64, "exact": _abi.PREC_FP64_EXACT, "mixed": _abi.PREC_MIXED}[args.precision]
     deck = taylor_bar(dx=args.dx)
     workload = f"taylor_bar_{deck.np}"
-    sol = Solver(deck, prec, device=local, reorder_interval=args.reorder)
+    skin = args.skin if prec != _abi.PREC_FP64_EXACT else 0.0
+    sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=skin)
     sol.set_diagnostics(False)
     if args.search_kind:
         sol.set_tuning(search_kind=args.search_kind)
@@ -491,12 +569,14 @@ def gpu_arm(args):
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     gpu_index = int(vis.split(",")[local]) if vis else local
     clocks = ClockSampler(gpu_index)
+    builds0 = sol.skin_builds() if skin > 0 else 0
     barrier()
     sol.profile(True)
     clocks.start()
     sol.timer_start()
     done = sol.run(args.steps)
     ms = sol.timer_stop()
+    builds_timed = (sol.skin_builds() - builds0) if skin > 0 else None
     clk = clocks.stop()
     launches = sol.kernel_launches()
     report = sol.profile_report()
@@ -512,7 +592,7 @@ def gpu_arm(args):
     dom = max(main, key=lambda k: main[k][0])
     dom_ms, dom_n = main[dom]
     per_launch_s = dom_ms / 1e3 / max(dom_n, 1)
-    bpp = algorithmic_bytes(dom, kbar, args.precision)
+    bpp = algorithmic_bytes(dom, kbar, args.precision, skin > 0)
     achieved = bpp * deck.np / per_launch_s / 1e9
     traffic = load_traffic(workload, args.precision, dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -525,7 +605,7 @@ def gpu_arm(args):
     fp64 = None
     accuracy = None
     if args.precision == "mixed" and not args.no_compare:
-        ref = Solver(deck, _abi.PREC_FP64, device=local, reorder_interval=args.reorder)
+        ref = Solver(deck, _abi.PREC_FP64, device=local, reorder_interval=args.reorder, nbr_skin=skin)
         ref.set_diagnostics(False)
         if args.search_kind:
             ref.set_tuning(search_kind=args.search_kind)
@@ -656,7 +736,8 @@ def gpu_arm(args):
         "config": {"workload": workload, "particles": deck.np, "dx_mm": args.dx * 1e3, "precision": args.precision,
                    "material": "copper model 10 + Mie-Grueneisen EOS 41, h = 1.3 dx, CFL 0.3 (tcrit_opt 1)",
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
-                   "reorder_interval": args.reorder},
+                   "reorder_interval": args.reorder, "nbr_skin": skin,
+                "skin_builds_in_timed_steps": builds_timed},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         "fp64": fp64, "accuracy": accuracy, "long_run": longrun, "adjoint": adjoint, "ensemble": ensemble,
         "fluid_column": fluid,
