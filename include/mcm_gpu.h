@@ -74,7 +74,7 @@ typedef enum {
 /* One material, as the reference holds it after mcm_matin, the mcm_sets routines and mcm_calcg:
  * `type material` of MCM/mcm_database.f90:235-257. */
 typedef struct {
-    int model;                 /* 1, 3, 4 (cap model: FP64-exact precision, disctype 0), 9, 10 */
+    int model;                 /* 1, 3, 4 (cap model: disctype 0), 9, 10 */
     int eos;                   /* 1, 4, 13, 28, 41 (models 9, 10) */
     int visc_type;             /* 1: nodal artificial viscosity */
     double rho;                /* reference density (rho0 of every particle of this material) */

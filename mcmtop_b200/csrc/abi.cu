@@ -627,9 +627,9 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
         if (md != 1 && md != 3 && md != 4 && md != 9 && md != 10) return MCM_EINVAL;
         cap_model = cap_model || md == 4;
     }
-    // the cap model leaves sigma asymmetric, which only the FP64-exact simple-SPH
-    // momentum sum reads (both triangles); the other gathers carry 6 components
-    if (cap_model && (cfg->precision != MCM_PREC_FP64_EXACT || cfg->disctype != 0)) return MCM_EUNSUPPORTED;
+    // the cap model leaves sigma asymmetric: the simple-SPH momentum sums of
+    // every precision read both triangles; the corrected-SPH sum carries 6 components
+    if (cap_model && cfg->disctype != 0) return MCM_EUNSUPPORTED;
     if (cfg->boundary) {
         for (int d = 0; d < 3; ++d) {
             bool p0 = cfg->boundary_code[2 * d] == 2, p1 = cfg->boundary_code[2 * d + 1] == 2;

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_strain_coop(StepArgs
 // Simple SPH: four resident blocks (64 registers) hide the gather latency
 // better than three at 80 (2.37 against 2.65 ms per step on the 2M bar, and
 // 1.58 against 1.87 ms for the strain gather above).
-template <int L, int DISC>
+template <int L, int DISC, bool ASYM>
 __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepArgs a, int integrate) {
     __shared__ double sm[32];
     if (skip_step(a)) return;
@@ -211,12 +211,16 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
     const bool live = t < a.n;
     int nreal = 0, gn = 0;
     double4 xi = make_double4(0, 0, 0, 1), r1i = make_double4(0, 0, 0, 0), r2i = make_double4(0, 0, 0, 1);
+    // the cap model leaves sigma asymmetric: its lower triangle (21 31 32)
+    constexpr bool asym = ASYM;
+    double4 r3i = make_double4(0, 0, 0, 0);
     if (live) {
         nreal = stored_neighbours(a, t);
         gn = a.gnnbr[t];
         xi = a.rec0[t];
         r1i = a.rec1[t];
         r2i = a.rec2[t];
+        if (asym) r3i = a.rec3[t];
     }
     const unsigned *spos = a.nidx + (size_t)t * a.nstride;
     const int self = (a.prm.disctype == 1) ? 1 : 0;
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
     const double ihi = 1.0 / xi.w;
     double acc[3] = {0.0, 0.0, 0.0};
     if (DISC == 0) {
-        // MCM/mcm_oldacceleration.f90:66-89
+        // MCM/mcm_oldacceleration.f90:66-89: a(n) += m_j sum_m (A_j + A_i)(m,n) dW/dx_m
         for (int k = lane; k < total; k += L) {
             const Entry e = entry_at(a, t, k, nreal, self, spos);
             const double4 xj = e.kind ? a.grec0[e.idx] : a.rec0[e.idx];
@@ -234,9 +238,14 @@ __global__ void __launch_bounds__(256, DISC == 0 ? 4 : 1) k_momentum_coop(StepAr
             gradw_ih(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, inv_havg(xi.w, xj.w, ihi), d[0], d[1], d[2]);
             const double s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
             const double s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
+            double l21 = s12, l31 = s13, l32 = s23;
+            if (asym) {
+                const double4 r3 = e.kind ? a.grec3[e.idx] : a.rec3[e.idx];
+                l21 = r3.x + r3i.x; l31 = r3.y + r3i.y; l32 = r3.z + r3i.z;
+            }
             const double mj = r2.z;
-            acc[0] = fma(mj, s11 * d[0] + s12 * d[1] + s13 * d[2], acc[0]);
-            acc[1] = fma(mj, s12 * d[0] + s22 * d[1] + s23 * d[2], acc[1]);
+            acc[0] = fma(mj, s11 * d[0] + l21 * d[1] + l31 * d[2], acc[0]);
+            acc[1] = fma(mj, s12 * d[0] + s22 * d[1] + l32 * d[2], acc[1]);
             acc[2] = fma(mj, s13 * d[0] + s23 * d[1] + s33 * d[2], acc[2]);
         }
     } else {

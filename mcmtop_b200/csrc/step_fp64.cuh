@@ -1053,8 +1053,12 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
     constexpr int L = kCoopLanes;
     const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
-    if (a.prm.disctype == 0) k_momentum_coop<L, 0><<<blocks, threads, 0, s>>>(a, integrate);
-    else k_momentum_coop<L, 1><<<blocks, threads, 0, s>>>(a, integrate);
+    if (a.prm.disctype == 0) {
+        if (a.prm.asym) k_momentum_coop<L, 0, true><<<blocks, threads, 0, s>>>(a, integrate);
+        else k_momentum_coop<L, 0, false><<<blocks, threads, 0, s>>>(a, integrate);
+    } else {
+        k_momentum_coop<L, 1, false><<<blocks, threads, 0, s>>>(a, integrate);
+    }
     return blocks;
 #endif
 }

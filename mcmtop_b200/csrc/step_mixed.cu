@@ -261,6 +261,9 @@ __global__ void k_mom_prep(StepArgs a) {
         rec[1] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
                                  (float)((f[FS33][i] - q) * ir2), (float)(f[FS12][i] * ir2));
         rec[2] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
+        // the cap model's lower triangle (21 31 32), read only when a material has it
+        if (a.prm.asym)
+            rec[3] = make_float4((float)(f[FL21][i] * ir2), (float)(f[FL31][i] * ir2), (float)(f[FL32][i] * ir2), 0.0f);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -274,6 +277,8 @@ __global__ void k_mom_prep(StepArgs a) {
                                       (float)((f[FS33][j] - q) * ir2), (float)(-f[FS12][j] * ir2));
             a.gfrec2[g] = make_float4((float)(-f[FS13][j] * ir2), (float)(-f[FS23][j] * ir2), (float)a.gmass[g],
                                       (float)rho);
+            if (a.prm.asym)
+                a.grec3[g] = make_double4(-f[FL21][j] * ir2, -f[FL31][j] * ir2, -f[FL32][j] * ir2, 0.0);
         }
     }
 }
@@ -348,6 +353,7 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // Four resident blocks (64 registers) hide the record gathers' latency
 // better than three at 80 registers (measured with 16 lanes per particle:
 // 1.70 against 2.19 ms per step on the 2M bar).
+template <bool ASYM>
 __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
@@ -360,7 +366,8 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
     fill_offsets(offs, fr);
     __syncthreads();
     const int nm = a.nmat;
-    double e1[5] = {0, 0, 0, 0, 0};   // sums of material 1; others go to the partials directly
+    constexpr bool asym = ASYM;   // the cap model: sigma's lower triangle in the record's 4th slot
+    double e1[5] = {0, 0, 0, 0, 0};   // sums of material 1 (one-material bodies)
     double xlo[3] = {1.0e20, 1.0e20, 1.0e20}, xhi[3] = {-1.0e20, -1.0e20, -1.0e20};
     const bool do_int = integrate_flag && !a.time->ended;
     for (int round = 0; round < rounds; ++round) {
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
         const bool live = t < a.n;
         int nreal = 0, gn = 0, i = 0;
         float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), r1i = make_float4(0.f, 0.f, 0.f, 0.f),
-               r2i = make_float4(0.f, 0.f, 0.f, 1.f);
+               r2i = make_float4(0.f, 0.f, 0.f, 1.f), r3i = make_float4(0.f, 0.f, 0.f, 0.f);
         if (live) {
             nreal = a.nnbr[t];
             gn = a.gnnbr[t];
@@ -376,6 +383,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
             xi = r.a;
             r1i = r.b;
             r2i = ld_rec4(a.frec0 + 4 * (size_t)t + 2);
+            if (asym) r3i = ld_rec4(a.frec0 + 4 * (size_t)t + 3);
             i = a.cell_list[t];
         }
         const unsigned *spos = a.nidx + (size_t)t * a.nstride;
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
         float acc[3] = {0.0f, 0.0f, 0.0f};
         for (int k = lane; k < total; k += L) {
             float dx, dy, dz, hj;
-            float4 r1, r2;
+            float4 r1, r2, r3;
             if (k < nreal) {
                 const unsigned e = spos[k];
                 const float4 o = offs[e >> 26];
@@ -395,6 +403,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
                 const float4 xj = r.a;
                 r1 = r.b;
                 r2 = ld_rec4(a.frec0 + 4 * p + 2);
+                if (asym) r3 = ld_rec4(a.frec0 + 4 * p + 3);
                 dx = (xi.x - xj.x) - o.x;
                 dy = (xi.y - xj.y) - o.y;
                 dz = (xi.z - xj.z) - o.z;
@@ -404,6 +413,10 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
                 const double4 xj = a.grec0[q];
                 r1 = a.gfrec1[q];
                 r2 = a.gfrec2[q];
+                if (asym) {
+                    const double4 g3 = a.grec3[q];
+                    r3 = make_float4((float)g3.x, (float)g3.y, (float)g3.z, 0.0f);
+                }
                 dx = (float)(xa[0] - xj.x);
                 dy = (float)(xa[1] - xj.y);
                 dz = (float)(xa[2] - xj.z);
@@ -413,10 +426,13 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
             gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
             const float s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
             const float s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
+            float l21 = s12, l31 = s13, l32 = s23;
+            if (asym) { l21 = r3.x + r3i.x; l31 = r3.y + r3i.y; l32 = r3.z + r3i.z; }
             const float mj = r2.z;
             d0 *= mj; d1 *= mj; d2 *= mj;
-            acc[0] = fmaf(s11, d0, fmaf(s12, d1, fmaf(s13, d2, acc[0])));
-            acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(s23, d2, acc[1])));
+            // a(n) += m_j sum_m (A_j + A_i)(m,n) dW/dx_m (column n; rows for a symmetric A)
+            acc[0] = fmaf(s11, d0, fmaf(l21, d1, fmaf(l31, d2, acc[0])));
+            acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(l32, d2, acc[1])));
             acc[2] = fmaf(s13, d0, fmaf(s23, d1, fmaf(s33, d2, acc[2])));
         }
         double ac[3];
@@ -500,7 +516,8 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
     const int blocks = pair_blocks_of(a, L);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
-    k_momentum<<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
+    if (a.prm.asym) k_momentum<true><<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
+    else k_momentum<false><<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
     return blocks;
 }
 
