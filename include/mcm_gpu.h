@@ -262,7 +262,9 @@ int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const dou
 /* No counterpart in the reference (it has no differentiation).  Reverse-mode
  * gradients of a function of the final state with respect to the initial
  * state and to the material parameters, through the whole step: disctype 0,
- * every material model 10 with EOS 41, reorder_interval 0.  The forward runs
+ * every material model 10, or model 9 without viscosity (materials 1 and 2),
+ * with EOS 1, 4, 13, 28 or 41, reorder_interval 0, constant h, no repulsive
+ * contact, no skin lists.  The forward runs
  * in the handle's precision; the reverse kernels are FP64 and differentiate
  * the FP64 step along that forward trajectory (with MCM_PREC_MIXED: the
  * gradient of the step along the FP32-pair-sum trajectory).  The dt schedule is an input (the critical-timestep
@@ -277,9 +279,10 @@ int mcm_gpu_calctotale_noalloc(const double *mass, const double *vabs, const dou
  * final x and v (Fortran (3,np) layout; NULL = zero), recomputes each
  * checkpoint segment forward and runs the reverse steps backwards, and
  * returns dL/dx and dL/dv of the initial state (xbar0, vbar0, (3,np)) and, in
- * param_bar[nmat][4], dL/d(strinput[0] = G, strinput[1] = yield stress,
- * strinput[2] = hardening modulus, eosinput[1] = Mie-Grueneisen slope s) of
- * each material, in the card's units.  The device state is left as the
+ * param_bar[nmat][4], dL/d(strinput[0], strinput[1], strinput[2],
+ * eosinput[1]) of each material, in the card's units: for model 10 G, yield
+ * stress and hardening modulus; eosinput[1] is the slope s of EOS 41 and 4,
+ * the linear coefficient c1 of EOS 1 and gamma of EOS 28.  The device state is left as the
  * forward run left it. */
 int mcm_gpu_adjoint_forward(mcm_gpu_handle *h, int nsteps, const double *dts, int checkpoint_every);
 int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double *vbar, double *param_bar,

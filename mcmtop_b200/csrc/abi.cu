@@ -1436,8 +1436,19 @@ int adj_check(mcm_gpu_handle *h) {
         return set_error(h, MCM_EUNSUPPORTED, "adjoint: constant smoothing length without XSPH only");
     if (h->A.prm.contact) return set_error(h, MCM_EUNSUPPORTED, "adjoint: no repulsive contact (contacttype > 0)");
     if (h->A.prm.skin > 0.0) return set_error(h, MCM_EUNSUPPORTED, "adjoint: neighbour lists rebuilt every step (nbr_skin 0)");
-    for (const mcm_gpu_material &m : h->mats)
-        if (m.model != 10 || m.eos != 41) return set_error(h, MCM_EUNSUPPORTED, "adjoint: model 10 with EOS 41 only");
+    // models whose whole state is what the reverse constitutive step carries:
+    // model 10, and model 9 without viscosity (its deviator is zero every step;
+    // MCM/mcm_f3dm9.f90:30-32); the dual pass keeps 8 constitutive constants,
+    // which hold model 9's cm(1..2, mat) for materials 1 and 2
+    for (size_t k = 0; k < h->mats.size(); ++k) {
+        const mcm_gpu_material &m = h->mats[k];
+        const bool eos_ok = m.eos == 1 || m.eos == 4 || m.eos == 13 || m.eos == 28 || m.eos == 41;
+        const bool fluid = m.model == 9 && k < 2 && m.strinput[1 + 5 * k] == 0.0;
+        if (!eos_ok || !(m.model == 10 || fluid))
+            return set_error(h, MCM_EUNSUPPORTED,
+                             "adjoint: model 10, or model 9 with zero viscosity (materials 1-2), with EOS 1, 4, 13, 28 "
+                             "or 41");
+    }
     return MCM_OK;
 }
 

@@ -359,7 +359,10 @@ __device__ __forceinline__ void seed(PState<D> &P, DualMat &M, int s, int k) {
         case 17: P.spin[1].d[k] = 1.0; break;
         case 18: P.spin[2].d[k] = 1.0; break;
         case 19: P.tracerod.d[k] = 1.0; break;
-        case kInputs + 0: M.strinput.gmod.d[k] = 1.0; M.g.d[k] = 1.0; break;   // G
+        case kInputs + 0:                                                     // strinput(1)
+            M.strinput.gmod.d[k] = 1.0;
+            if (M.model == 10) M.g.d[k] = 1.0;   // mcm_calcg: g = strinput(1) for model 10, 0 for model 9
+            break;
         case kInputs + 1: M.strinput.yield.d[k] = 1.0; break;                 // yield stress
         case kInputs + 2: M.strinput.hard.d[k] = 1.0; break;                  // hardening modulus
         case kInputs + 3: M.eosinput.slope.d[k] = 1.0; break;                 // EOS-41 slope s

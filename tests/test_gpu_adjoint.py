@@ -16,6 +16,8 @@ branch (relative 1e-6 for the parameters of a sum over all particles; the
 measured error then falls to 1e-7 - 1e-9), and the initial-state check moves
 positions, which keeps the uniform region uniform.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -239,3 +241,116 @@ def test_adjoint_regrows_storage_within_a_segment(lib, dts):
     s2.close()
     assert np.allclose(pb2, pb1, rtol=1e-12, atol=0.0)
     assert np.allclose(x02, x01, rtol=1e-9, atol=1e-12 * np.max(np.abs(x01)))
+
+
+# ------------------------------------------------------ other models and EOS
+def _schedule(deck, nsteps):
+    s = Solver(deck, PREC)
+    out = [s.dt]
+    for _ in range(nsteps):
+        s.step_a()
+        s.dt_update()
+        out.append(s.dt)
+        s.step_b()
+        s.step_c()
+    s.close()
+    return np.array(out)
+
+
+def _linear_check(make_deck, slots, dts, rel, seed):
+    """Adjoint of L = sum W.x + U.v of the final state with respect to the
+    card values `slots` ((array, index, material)) against central
+    differences of the FP64 forward along the same dt schedule."""
+    rng = np.random.default_rng(seed)
+    s = Solver(make_deck({}), PREC)
+    s.adjoint_forward(dts, EVERY)
+    st = s.download(["x", "v"])
+    W = rng.standard_normal(st["x"].shape)
+    U = rng.standard_normal(st["v"].shape) * 1e2
+    pb, _, _ = s.adjoint_backward(W, U)
+    s.close()
+    for arr, k, m in slots:
+        v0 = getattr(make_deck({}).materials[m], arr)[k]
+        h = rel * abs(v0)
+
+        def L(val):
+            s2 = Solver(make_deck({(arr, k, m): val}), PREC)
+            s2.adjoint_forward(dts, EVERY)
+            out = s2.download(["x", "v"])
+            s2.close()
+            return float((W * out["x"]).sum() + (U * out["v"]).sum())
+
+        ref = (L(v0 + h) - L(v0 - h)) / (2 * h)
+        got = pb[m][3 if arr == "eosinput" else k]
+        assert abs(got - ref) <= 1e-3 * abs(ref), (arr, k, got, ref)
+
+
+def _with_cards(deck, changes):
+    mats = []
+    for m, card in enumerate(deck.materials):
+        c = dataclasses.replace(card, strinput=card.strinput.copy(), eosinput=card.eosinput.copy())
+        for (arr, k, mm), val in changes.items():
+            if mm == m:
+                getattr(c, arr)[k] = val
+        mats.append(c)
+    return deck.replace(materials=mats)
+
+
+def test_adjoint_model10_with_dyna_grueneisen_eos(lib):
+    """Model 10 with EOS 4 (MCM/mcm_eos4c.f90, mcm_eqos4.f90): G, yield stress
+    and the slope s1 against central differences."""
+    from test_gpu_materials import _model10_eos
+
+    card = _model10_eos(4)
+    base = taylor_bar(dx=DX, velocity=V0, material=card)
+
+    def make(changes):
+        return _with_cards(base, changes)
+
+    dts = _schedule(base, NSTEPS)
+    _linear_check(make, [("strinput", 0, 0), ("strinput", 1, 0), ("eosinput", 1, 0)], dts, REL_STEP_SUM, 31)
+
+
+def test_adjoint_fluid_column(lib):
+    """The null material (model 9, no viscosity) with the polynomial EOS 1,
+    gravity and five ghost walls: d/d(c1) and the initial positions along a
+    random direction against central differences."""
+    from mcmtop_b200.deck import fluid_column
+
+    base = fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))
+
+    def make(changes):
+        return _with_cards(base, changes)
+
+    dts = _schedule(base, NSTEPS)
+    _linear_check(make, [("eosinput", 1, 0)], dts, REL_STEP_SUM, 41)
+    rng = np.random.default_rng(43)
+    s = Solver(base, PREC)
+    s.adjoint_forward(dts, EVERY)
+    st = s.download(["x", "v"])
+    W = rng.standard_normal(st["x"].shape)
+    _, x0b, _ = s.adjoint_backward(W, None)
+    s.close()
+    dirx = rng.standard_normal(st["x"].shape) * 1e-4
+
+    def L(eps):
+        s2 = Solver(base.replace(x=base.x + eps * dirx), PREC)
+        s2.adjoint_forward(dts, EVERY)
+        out = s2.download(["x"])["x"]
+        s2.close()
+        return float((W * out).sum())
+
+    ref = (L(1e-3) - L(-1e-3)) / 2e-3
+    got = float((x0b * dirx).sum())
+    assert abs(got - ref) <= 1e-3 * abs(ref), (got, ref)
+
+
+def test_adjoint_rejects_models_with_carried_state(lib):
+    """Models whose stress state carries between steps beyond what the reverse
+    step holds (model 3's back stress, model 9 with viscosity) are rejected."""
+    from test_gpu_materials import _solid
+
+    s = Solver(taylor_bar(dx=DX, material=_solid(3)), PREC)
+    with pytest.raises(_abi.MCMError):
+        s.adjoint_forward(np.full(3, s.dt), 2)
+    s.close()
