@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--skin", type=float, default=0.0,
                     help="neighbour-list skin as a fraction of hmax for the FP64-fast and mixed runs (0: rebuild "
                          "the lists every step)")
+    ap.add_argument("--compensated", action="store_true",
+                    help="mixed precision: Kahan-compensated pair sums per lane (compensated_sums)")
     ap.add_argument("--dx", type=float, default=DX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -502,7 +504,8 @@ def long_run(args, local):
     out = {"workload": f"taylor_bar_{deck.np}", "steps": args.long_steps}
     ends = {}
     for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
-        sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=args.skin)
+        sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=args.skin,
+                     compensated=args.compensated)
         sol.set_diagnostics(False)
         sol.timer_start()
         done = sol.run(args.long_steps)
@@ -552,7 +555,8 @@ def gpu_arm(args):
     deck = taylor_bar(dx=args.dx)
     workload = f"taylor_bar_{deck.np}"
     skin = args.skin if prec != _abi.PREC_FP64_EXACT else 0.0
-    sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=skin)
+    sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=skin,
+                 compensated=args.compensated)
     sol.set_diagnostics(False)
     if args.search_kind:
         sol.set_tuning(search_kind=args.search_kind)
@@ -736,7 +740,7 @@ def gpu_arm(args):
         "config": {"workload": workload, "particles": deck.np, "dx_mm": args.dx * 1e3, "precision": args.precision,
                    "material": "copper model 10 + Mie-Grueneisen EOS 41, h = 1.3 dx, CFL 0.3 (tcrit_opt 1)",
                    "l2": "inputs larger than L2 (state ~1 GB/GPU)", "parallelism": "one independent bar per GPU",
-                   "reorder_interval": args.reorder, "nbr_skin": skin,
+                   "reorder_interval": args.reorder, "nbr_skin": skin, "compensated_sums": bool(args.compensated),
                 "skin_builds_in_timed_steps": builds_timed},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         "fp64": fp64, "accuracy": accuracy, "long_run": longrun, "adjoint": adjoint, "ensemble": ensemble,

@@ -123,6 +123,9 @@ typedef struct {
                                   rebuilt only when some particle has moved nbr_skin*hmax/2 since the
                                   last build, filtered every step to the reference's neighbour sets
                                   (not its order).  No counterpart in the reference. */
+    int compensated_sums;      /* MCM_PREC_MIXED: 1 adds each lane's FP32 pair terms with Kahan
+                                  compensation before the TwoSum lane combination; 0 adds them
+                                  plainly (the faster default).  Ignored by the FP64 precisions. */
 } mcm_gpu_config;
 
 /* Host views of the particle arrays (Fortran layout, np particles).  NULL

@@ -49,6 +49,7 @@ class Config(C.Structure):
         ("boundary_x", C.c_double * 6), ("baseaccel", C.c_int), ("base_a", C.c_double * 3),
         ("tssf", C.c_double), ("hmax", C.c_double), ("precision", C.c_int), ("nbr_stride", C.c_int),
         ("reorder_interval", C.c_int), ("block_size", C.c_int), ("nbr_skin", C.c_double),
+        ("compensated_sums", C.c_int),
     ]
 
 

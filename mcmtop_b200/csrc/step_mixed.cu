@@ -41,8 +41,8 @@ __device__ __forceinline__ bool skip_step(const StepArgs &a) { return a.status->
 // ------------------------------------------------------- compensated sums
 // Sum of one value per lane over the L lanes of a sub-warp, every addition
 // error-free transformed (TwoSum) and the errors added up; every lane gets it.
-__device__ __forceinline__ double lane_sum(float s) {
-    float c = 0.0f;
+// c: a correction the lane already carries (the compensation of a Kahan sum).
+__device__ __forceinline__ double lane_sum(float s, float c = 0.0f) {
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) {
         const float s2 = __shfl_xor_sync(0xffffffffu, s, o, L);
@@ -126,6 +126,17 @@ __device__ __forceinline__ float inv_havg_f(float hi, float hj, float ihi) {
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 
+// Kahan (compensated) addition of term to the sum (s, c): c carries the
+// low-order part that s lost, so s + c is the sum to about one FP32 rounding
+// over all the terms instead of one per addition.  Used by the compensated
+// variant of the pair sums (mcm_gpu_config.compensated_sums).
+__device__ __forceinline__ void kahan_add(float &s, float &c, float term) {
+    const float y = term + c;
+    const float t = s + y;
+    c = y - (t - s);
+    s = t;
+}
+
 // ------------------------------------------------------------ strain prep
 // MCM/mcm_strain.f90:27-31 (x - v dt/2) and V_j = m_j/rho_j, cell-relative.
 __global__ void k_strain_prep(StepArgs a) {
@@ -152,7 +163,9 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 // ----------------------------------------------------------- strain rate
-// MCM/mcm_oldstrain.f90:34-64 with FP32 pair sums.
+// MCM/mcm_oldstrain.f90:34-64 with FP32 pair sums (KAHAN: compensated per
+// lane, the compensation carried into the TwoSum lane combination).
+template <bool KAHAN>
 __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
     __shared__ float4 offs[27];
     if (skip_step(a)) return;
@@ -186,9 +199,9 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
         }
         const int total = live ? nreal + gn : 0;
         const float ihi = 1.0f / xi.w;
-        float gv[9];
+        float gv[9], gc[9];
 #pragma unroll
-        for (int u = 0; u < 9; ++u) gv[u] = 0.0f;
+        for (int u = 0; u < 9; ++u) { gv[u] = 0.0f; gc[u] = 0.0f; }
         for (int k = lane; k < total; k += L) {
             float dx, dy, dz, hj;
             float4 vj;
@@ -214,13 +227,21 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
             float d0, d1, d2;
             gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
             const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
-            gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
-            gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
-            gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
+            if (KAHAN) {
+                const float tt[3] = {t0, t1, t2}, dd[3] = {d0, d1, d2};
+#pragma unroll
+                for (int n = 0; n < 3; ++n)
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) kahan_add(gv[3 * n + m], gc[3 * n + m], tt[n] * dd[m]);
+            } else {
+                gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
+                gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
+                gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
+            }
         }
         double r[9];
 #pragma unroll
-        for (int u = 0; u < 9; ++u) r[u] = lane_sum(gv[u]);
+        for (int u = 0; u < 9; ++u) r[u] = lane_sum(gv[u], KAHAN ? gc[u] : 0.0f);
         if (live && lane == 0) {
             // MCM/mcm_oldstrain.f90:56-63
             double *const *f = a.F.f;
@@ -353,7 +374,7 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // Four resident blocks (64 registers) hide the record gathers' latency
 // better than three at 80 registers (measured with 16 lanes per particle:
 // 1.70 against 2.19 ms per step on the 2M bar).
-template <bool ASYM>
+template <bool ASYM, bool KAHAN>
 __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
@@ -391,7 +412,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
         if (live && gn > 0) { xa[0] = a.F.f[FX][i]; xa[1] = a.F.f[FY][i]; xa[2] = a.F.f[FZ][i]; }
         const int total = live ? nreal + gn : 0;
         const float ihi = 1.0f / xi.w;
-        float acc[3] = {0.0f, 0.0f, 0.0f};
+        float acc[3] = {0.0f, 0.0f, 0.0f}, comp[3] = {0.0f, 0.0f, 0.0f};
         for (int k = lane; k < total; k += L) {
             float dx, dy, dz, hj;
             float4 r1, r2, r3;
@@ -431,13 +452,19 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
             const float mj = r2.z;
             d0 *= mj; d1 *= mj; d2 *= mj;
             // a(n) += m_j sum_m (A_j + A_i)(m,n) dW/dx_m (column n; rows for a symmetric A)
-            acc[0] = fmaf(s11, d0, fmaf(l21, d1, fmaf(l31, d2, acc[0])));
-            acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(l32, d2, acc[1])));
-            acc[2] = fmaf(s13, d0, fmaf(s23, d1, fmaf(s33, d2, acc[2])));
+            if (KAHAN) {
+                kahan_add(acc[0], comp[0], fmaf(s11, d0, fmaf(l21, d1, l31 * d2)));
+                kahan_add(acc[1], comp[1], fmaf(s12, d0, fmaf(s22, d1, l32 * d2)));
+                kahan_add(acc[2], comp[2], fmaf(s13, d0, fmaf(s23, d1, s33 * d2)));
+            } else {
+                acc[0] = fmaf(s11, d0, fmaf(l21, d1, fmaf(l31, d2, acc[0])));
+                acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(l32, d2, acc[1])));
+                acc[2] = fmaf(s13, d0, fmaf(s23, d1, fmaf(s33, d2, acc[2])));
+            }
         }
         double ac[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ac[c] = lane_sum(acc[c]);
+        for (int c = 0; c < 3; ++c) ac[c] = lane_sum(acc[c], KAHAN ? comp[c] : 0.0f);
         if (live && lane == 0) {
             double *const *f = a.F.f;
             if (a.prm.contact)   // repulsive contact (MCM/mcm_oldacceleration.f90:49-51)
@@ -504,7 +531,8 @@ void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 void launch_strain(const StepArgs &a, cudaStream_t s) {
-    k_strain<<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
+    if (a.prm.kahan) k_strain<true><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
+    else k_strain<false><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
 }
 
 void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
@@ -516,8 +544,14 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
     const int blocks = pair_blocks_of(a, L);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
-    if (a.prm.asym) k_momentum<true><<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
-    else k_momentum<false><<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
+    const int th = pair_threads_of(a);
+    if (a.prm.asym) {
+        if (a.prm.kahan) k_momentum<true, true><<<blocks, th, 0, s>>>(a, integrate_flag);
+        else k_momentum<true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+    } else {
+        if (a.prm.kahan) k_momentum<false, true><<<blocks, th, 0, s>>>(a, integrate_flag);
+        else k_momentum<false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+    }
     return blocks;
 }
 

@@ -50,7 +50,7 @@ def material_table(deck: Deck) -> "C.Array":
 
 
 def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_interval: int = 0,
-                     nbr_skin: float = 0.0) -> _abi.Config:
+                     nbr_skin: float = 0.0, compensated: bool = False) -> _abi.Config:
     """Control-card processing of MCM/mcm_control_v2.f90:193-243 and the
     boundary/base-acceleration cards (mcm_inp_symmetry_v2.f90:83-137,
     mcm_baseaccel_in.f90:23-33)."""
@@ -78,12 +78,14 @@ def config_from_deck(deck: Deck, precision: int, nbr_stride: int = 0, reorder_in
     c.nbr_stride = nbr_stride
     c.reorder_interval = reorder_interval
     c.nbr_skin = nbr_skin
+    c.compensated_sums = int(bool(compensated))
     return c
 
 
 class Solver:
     def __init__(self, deck: Deck, precision: int = _abi.PREC_FP64_EXACT, nbr_stride: int = 0,
-                 device: int | None = None, reorder_interval: int = 0, nbr_skin: float = 0.0):
+                 device: int | None = None, reorder_interval: int = 0, nbr_skin: float = 0.0,
+                 compensated: bool = False):
         self.lib = _abi.load()
         if device is not None:
             check(self.lib.mcm_gpu_set_device(int(device)), "mcm_gpu_set_device")
@@ -91,7 +93,7 @@ class Solver:
         self.n = deck.np
         self.nmat = len(deck.materials)
         self._mats = material_table(deck)
-        self.cfg = config_from_deck(deck, precision, nbr_stride, reorder_interval, nbr_skin)
+        self.cfg = config_from_deck(deck, precision, nbr_stride, reorder_interval, nbr_skin, compensated)
         h = C.c_void_p()
         check(self.lib.mcm_gpu_create(C.byref(self.cfg), self._mats, self.nmat, self.n, C.byref(h)),
               "mcm_gpu_create")

@@ -144,3 +144,23 @@ def test_mixed_energy_balance_16k_thousand_steps(lib):
     assert worst <= 1e-5, worst
     errs = compare(sol, orc, STATE, 1e-4, "mixed 16k bar, 1000 steps")
     print("mixed, 1000 steps: energy drift gap", worst, "field errors", errs)
+
+
+def test_mixed_compensated_sums(lib):
+    """The Kahan-compensated variant of the pair sums (compensated_sums): the
+    same neighbour sets, fields within the mixed bound of the oracle after 20
+    steps, and no further from it than the plain sums' worst field."""
+    deck = taylor_bar(dx=0.8e-3)
+    orc = Oracle(deck)
+    plain, comp = Solver(deck, _abi.PREC_MIXED), Solver(deck, _abi.PREC_MIXED, compensated=True)
+    for _ in range(20):
+        plain.step()
+        comp.step()
+        orc.step()
+    compare_neighbours(comp, orc)
+    e_comp = compare(comp, orc, STATE, MIXED_TOL, "compensated mixed sums")
+    e_plain = compare(plain, orc, STATE, MIXED_TOL, "plain mixed sums")
+    print("worst field: compensated", max(e_comp.values()), "plain", max(e_plain.values()))
+    assert max(e_comp.values()) <= 1.5 * max(e_plain.values())
+    plain.close()
+    comp.close()
