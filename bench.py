@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--skin", type=float, default=0.0,
                     help="neighbour-list skin as a fraction of hmax for the FP64-fast and mixed runs (0: rebuild "
                          "the lists every step)")
+    ap.add_argument("--pair-kind", type=int, default=0, choices=[0, 1, 2],
+                    help="mixed strain gather: 1 records through L1, 2 rows staged in shared memory (0: default)")
     ap.add_argument("--compensated", action="store_true",
                     help="mixed precision: Kahan-compensated pair sums per lane (compensated_sums)")
     ap.add_argument("--dx", type=float, default=DX)
@@ -558,8 +560,8 @@ def gpu_arm(args):
     sol = Solver(deck, prec, device=local, reorder_interval=args.reorder, nbr_skin=skin,
                  compensated=args.compensated)
     sol.set_diagnostics(False)
-    if args.search_kind:
-        sol.set_tuning(search_kind=args.search_kind)
+    if args.search_kind or args.pair_kind:
+        sol.set_tuning(search_kind=args.search_kind, pair_kind=args.pair_kind)
     sol.run(args.warmup)
     stats = sol.stats()
     kbar = stats["mean_nbr"]

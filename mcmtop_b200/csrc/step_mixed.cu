@@ -260,6 +260,168 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
     }
 }
 
+// ------------------------------------------- strain rate, rows staged
+// The same sums as k_strain<false>, with a particle's neighbour records read
+// from shared memory.  A block takes 64 consecutive cell-order positions per
+// round; they lie in one row of cells (or two consecutive rows), and their
+// neighbours lie in the 9 rows of cells around each: for every such row the
+// contiguous range of positions from one cell left of the block's first cell
+// to one cell right of its last is a window, copied into shared memory by
+// coalesced loads (up to kStageCap records; windows that do not fit are read
+// from global memory as in k_strain).  An entry's window follows from its
+// cell code, so the lookup is one comparison.  Results are bitwise k_strain's.
+constexpr int kStageThreads = 128;
+constexpr int kStageCap = 1024;   // records of 32 bytes
+__global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) {
+    __shared__ float4 offs[27];
+    __shared__ float4 stage[2 * kStageCap];
+    __shared__ int wlo[18], wlen[18], woff[18];
+    __shared__ int row0;
+    if (skip_step(a)) return;
+    const int sub = threadIdx.x / L, lane = threadIdx.x % L;
+    constexpr int per = kStageThreads / L;
+    const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
+    const DevGrid g = *a.grid;
+    const Frame fr = make_frame(g);
+    const int gl0 = g.gridlim[0], gl1 = g.gridlim[1], gl2 = g.gridlim[2];
+    fill_offsets(offs, fr);
+    const double dt = a.time->dt;
+    for (int round = 0; round < rounds; ++round) {
+        const int tb = (round * gridDim.x + blockIdx.x) * per;
+        // the windows of the block's rows (threads 0..17: row 0 or 1 of the
+        // block, times the 9 neighbouring rows of cells)
+        if (threadIdx.x < 18) {
+            const int w = threadIdx.x;
+            int lo = 0, len = 0;
+            const int te = min(tb + per, a.n) - 1;
+            if (tb < a.n) {
+                const int k0 = a.ckey[tb], k1 = a.ckey[te];
+                if (k0 >= 0 && k1 >= 0) {
+                    const int r0 = k0 / gl0, r1 = k1 / gl0;
+                    const int rr = r0 + (w >= 9 ? 1 : 0);
+                    if (r1 - r0 <= 1 && rr <= r1) {
+                        const int xa = (rr == r0) ? k0 % gl0 + 1 : 1;
+                        const int xb = (rr == r1) ? k1 % gl0 + 1 : gl0;
+                        const int y = rr % gl1 + 1, z = rr / gl1 + 1;
+                        const int rc = w % 9;
+                        const int ty = y + rc % 3 - 1, tz = z + rc / 3 - 1;
+                        if (ty >= 1 && ty <= gl1 && tz >= 1 && tz <= gl2) {
+                            const int xl = xa > 1 ? xa - 1 : 1, xh = xb < gl0 ? xb + 1 : gl0;
+                            const int ka = (xl - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
+                            const int kb = (xh - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
+                            lo = a.cell_start[ka];
+                            len = a.cell_start[kb + 1] - lo;
+                        }
+                    }
+                }
+            }
+            wlo[w] = lo;
+            wlen[w] = len;
+        }
+        if (threadIdx.x == 0) row0 = (tb < a.n && a.ckey[tb] >= 0) ? a.ckey[tb] / gl0 : -1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int off = 0;
+            for (int w = 0; w < 18; ++w) {
+                if (off + wlen[w] > kStageCap) wlen[w] = 0;   // read from global memory
+                woff[w] = off;
+                off += wlen[w];
+            }
+        }
+        __syncthreads();
+        for (int w = 0; w < 18; ++w) {
+            const int lo = wlo[w], len = wlen[w], o = woff[w];
+            for (int u = threadIdx.x; u < len; u += kStageThreads) {
+                stage[2 * (o + u)] = a.frec0[2 * (size_t)(lo + u)];
+                stage[2 * (o + u) + 1] = a.frec0[2 * (size_t)(lo + u) + 1];
+            }
+        }
+        __syncthreads();
+        const int t = tb + sub;
+        const bool live = t < a.n;
+        int nreal = 0, gn = 0, i = 0, wbase = 0;
+        float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), vi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (live) {
+            nreal = a.nnbr[t];
+            gn = a.gnnbr[t];
+            const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)t);
+            xi = r.a;
+            vi = r.b;
+            i = a.cell_list[t];
+            const int kt = a.ckey[t];
+            wbase = (kt >= 0 && kt / gl0 != row0) ? 9 : 0;
+        }
+        const unsigned *spos = a.nidx + (size_t)t * a.nstride;
+        double xs[3] = {0.0, 0.0, 0.0};
+        if (live && gn > 0) {
+            xs[0] = a.F.f[FX][i] - 0.5 * a.F.f[FVX][i] * dt;
+            xs[1] = a.F.f[FY][i] - 0.5 * a.F.f[FVY][i] * dt;
+            xs[2] = a.F.f[FZ][i] - 0.5 * a.F.f[FVZ][i] * dt;
+        }
+        const int total = live ? nreal + gn : 0;
+        const float ihi = 1.0f / xi.w;
+        float gv[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) gv[u] = 0.0f;
+        for (int k = lane; k < total; k += L) {
+            float dx, dy, dz, hj;
+            float4 vj;
+            if (k < nreal) {
+                const unsigned e = spos[k];
+                const unsigned code = e >> 26;
+                const float4 o = offs[code];
+                const int p = (int)(e & kPosMask);
+                const int w = wbase + (int)(code / 3u);
+                const int u = p - wlo[w];
+                float4 xj;
+                if ((unsigned)u < (unsigned)wlen[w]) {
+                    xj = stage[2 * (woff[w] + u)];
+                    vj = stage[2 * (woff[w] + u) + 1];
+                } else {
+                    const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)p);
+                    xj = r.a;
+                    vj = r.b;
+                }
+                dx = (xi.x - xj.x) - o.x;
+                dy = (xi.y - xj.y) - o.y;
+                dz = (xi.z - xj.z) - o.z;
+                hj = xj.w;
+            } else {
+                const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
+                const double4 xj = a.grec0[q];
+                vj = a.gfrec1[q];
+                dx = (float)(xs[0] - xj.x);
+                dy = (float)(xs[1] - xj.y);
+                dz = (float)(xs[2] - xj.z);
+                hj = (float)xj.w;
+            }
+            float d0, d1, d2;
+            gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
+            const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
+            gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
+            gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
+            gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
+        }
+        double r[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) r[u] = lane_sum(gv[u]);
+        if (live && lane == 0) {
+            double *const *f = a.F.f;
+            f[FR11][i] = r[0];
+            f[FR22][i] = r[4];
+            f[FR33][i] = r[8];
+            f[FR12][i] = 0.5 * (r[1] + r[3]);
+            f[FR13][i] = 0.5 * (r[2] + r[6]);
+            f[FR23][i] = 0.5 * (r[5] + r[7]);
+            f[FW12][i] = 0.5 * (r[1] - r[3]);
+            f[FW13][i] = 0.5 * (r[2] - r[6]);
+            f[FW23][i] = 0.5 * (r[5] - r[7]);
+            f[FTR][i] = r[0] + r[4] + r[8];
+        }
+        __syncthreads();   // the next round overwrites the windows
+    }
+}
+
 // --------------------------------------------------------- momentum prep
 // Records: cell-relative x, h; (sigma - q)/rho^2 (formed in FP64,
 // MCM/mcm_oldacceleration.f90:79-80) and m (FP32).  Ghosts: FP64 positions,
@@ -531,6 +693,12 @@ void launch_strain_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 void launch_strain(const StepArgs &a, cudaStream_t s) {
+    if (a.pair_kind == 2 && !a.prm.kahan) {
+        int b = nblk(a.n, kStageThreads / L);
+        if (b > 148 * 6) b = 148 * 6;
+        k_strain_staged<<<b, kStageThreads, 0, s>>>(a);
+        return;
+    }
     if (a.prm.kahan) k_strain<true><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
     else k_strain<false><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
 }

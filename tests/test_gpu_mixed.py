@@ -164,3 +164,20 @@ def test_mixed_compensated_sums(lib):
     assert max(e_comp.values()) <= 1.5 * max(e_plain.values())
     plain.close()
     comp.close()
+
+
+def test_mixed_staged_strain_gather_is_bitwise_the_same(lib):
+    """The strain gather with each block's rows of neighbour records staged in
+    shared memory (pair_kind 2) reads the same records: bitwise the same state
+    as the per-neighbour gather, on the bar and on the fluid column (ghosts)."""
+    for deck in (taylor_bar(dx=0.4e-3), fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))):
+        a, b = Solver(deck, _abi.PREC_MIXED), Solver(deck, _abi.PREC_MIXED)
+        b.set_tuning(pair_kind=2)
+        assert b.tuning()["pair_kind"] == 2
+        a.run(12)
+        b.run(12)
+        ga, gb = a.download(STATE), b.download(STATE)
+        for f in STATE:
+            assert np.array_equal(ga[f], gb[f]), f
+        a.close()
+        b.close()
