@@ -69,7 +69,7 @@ def parse():
                     help="neighbour-list skin as a fraction of hmax for the FP64-fast and mixed runs (0: rebuild "
                          "the lists every step)")
     ap.add_argument("--pair-kind", type=int, default=0, choices=[0, 1, 2],
-                    help="mixed strain gather: 1 records through L1, 2 rows staged in shared memory (0: default)")
+                    help="mixed gathers: 1 records through L1, 2 rows staged in shared memory (0: default)")
     ap.add_argument("--compensated", action="store_true",
                     help="mixed precision: Kahan-compensated pair sums per lane (compensated_sums)")
     ap.add_argument("--dx", type=float, default=DX)

@@ -307,9 +307,9 @@ typedef struct {
                                 when a list outgrows it) */
     int search_kind;         /* 1: one thread per particle (the default), 2: one warp per particle,
                                 3: one warp per cell (candidates staged in shared memory) */
-    int pair_kind;           /* mixed-precision strain gather: 1 neighbour records through L1 (the
-                                default), 2 each block's rows of neighbour cells staged in shared
-                                memory */
+    int pair_kind;           /* mixed-precision strain and momentum gathers: 1 neighbour records
+                                through L1 (the default), 2 each block's rows of neighbour cells
+                                staged in shared memory (the same sums) */
     double ms_per_step;      /* mcm_gpu_autotune: device time per loop iteration of the chosen shape */
 } mcm_gpu_tuning;
 

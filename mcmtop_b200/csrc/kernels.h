@@ -85,7 +85,7 @@ struct StepArgs {
                           // 3: one warp per cell (k_search_cell)
     int pair_threads;     // threads per block of the cooperative strain and momentum gathers
     int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for
-    int pair_kind;        // mixed strain gather: 0 or 1 neighbour records through L1; 2 rows staged in shared memory
+    int pair_kind;        // mixed gathers: 0 or 1 neighbour records through L1; 2 rows staged in shared memory
     double *energy;   // 5*nmat + 3
 };
 

@@ -271,72 +271,101 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
 // from global memory as in k_strain).  An entry's window follows from its
 // cell code, so the lookup is one comparison.  Results are bitwise k_strain's.
 constexpr int kStageThreads = 128;
-constexpr int kStageCap = 1024;   // records of 32 bytes
+constexpr int kStageCap = 1024;    // strain records of 32 bytes
+constexpr int kStageCapM = 896;    // momentum records of 48 bytes
+
+// The windows of one round: for row b (0, or 1 when the block reaches into
+// the next row of cells) and each of the 9 rows of cells around it, window
+// 9b + r covers positions [lo, lo + len), staged at record offset off.
+struct StageWin {
+    int lo[18], len[18], off[18];
+    int row0;   // row of cells (key / gridlim x) of the block's first position
+};
+
+// Computes the windows of the positions [tb, tb + per) and copies the records
+// (NF float4 each, record p at src + stride * p) of those that fit in `cap`
+// records into stage.  Every thread of the block calls it; it synchronises.
+template <int NF>
+__device__ __forceinline__ void stage_rows(const StepArgs &a, int tb, int per, StageWin &W, float4 *stage, int cap,
+                                           const float4 *src, int stride) {
+    const int gl0 = a.grid->gridlim[0], gl1 = a.grid->gridlim[1], gl2 = a.grid->gridlim[2];
+    if (threadIdx.x < 18) {
+        const int w = threadIdx.x;
+        int lo = 0, len = 0;
+        const int te = min(tb + per, a.n) - 1;
+        if (tb < a.n) {
+            const int k0 = a.ckey[tb], k1 = a.ckey[te];
+            if (k0 >= 0 && k1 >= 0) {
+                const int r0 = k0 / gl0, r1 = k1 / gl0;
+                const int rr = r0 + (w >= 9 ? 1 : 0);
+                if (r1 - r0 <= 1 && rr <= r1) {
+                    const int xa = (rr == r0) ? k0 % gl0 + 1 : 1;
+                    const int xb = (rr == r1) ? k1 % gl0 + 1 : gl0;
+                    const int y = rr % gl1 + 1, z = rr / gl1 + 1;
+                    const int rc = w % 9;
+                    const int ty = y + rc % 3 - 1, tz = z + rc / 3 - 1;
+                    if (ty >= 1 && ty <= gl1 && tz >= 1 && tz <= gl2) {
+                        const int xl = xa > 1 ? xa - 1 : 1, xh = xb < gl0 ? xb + 1 : gl0;
+                        const int ka = (xl - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
+                        const int kb = (xh - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
+                        lo = a.cell_start[ka];
+                        len = a.cell_start[kb + 1] - lo;
+                    }
+                }
+            }
+        }
+        W.lo[w] = lo;
+        W.len[w] = len;
+    }
+    if (threadIdx.x == 0) W.row0 = (tb < a.n && a.ckey[tb] >= 0) ? a.ckey[tb] / gl0 : -1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int w = 0; w < 18; ++w) {
+            if (off + W.len[w] > cap) W.len[w] = 0;   // read from global memory
+            W.off[w] = off;
+            off += W.len[w];
+        }
+    }
+    __syncthreads();
+    for (int w = 0; w < 18; ++w) {
+        const int lo = W.lo[w], len = W.len[w], o = W.off[w];
+        for (int u = threadIdx.x; u < len; u += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < NF; ++c) stage[NF * (o + u) + c] = src[(size_t)stride * (lo + u) + c];
+    }
+    __syncthreads();
+}
+
+// First window of position t's row of cells (0 or 9).
+__device__ __forceinline__ int stage_base(const StepArgs &a, const StageWin &W, int t) {
+    const int kt = a.ckey[t];
+    return (kt >= 0 && kt / a.grid->gridlim[0] != W.row0) ? 9 : 0;
+}
+
+// Staged record index of neighbour entry e of a particle whose windows start
+// at wbase, or -1 when the record was not staged.
+__device__ __forceinline__ int stage_index(const StageWin &W, int wbase, unsigned e) {
+    const int w = wbase + (int)((e >> 26) / 3u);
+    const int u = (int)(e & kPosMask) - W.lo[w];
+    return ((unsigned)u < (unsigned)W.len[w]) ? W.off[w] + u : -1;
+}
+
 __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) {
     __shared__ float4 offs[27];
     __shared__ float4 stage[2 * kStageCap];
-    __shared__ int wlo[18], wlen[18], woff[18];
-    __shared__ int row0;
+    __shared__ StageWin W;
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     constexpr int per = kStageThreads / L;
     const int rounds = (a.n + per * gridDim.x - 1) / (per * gridDim.x);
     const DevGrid g = *a.grid;
     const Frame fr = make_frame(g);
-    const int gl0 = g.gridlim[0], gl1 = g.gridlim[1], gl2 = g.gridlim[2];
     fill_offsets(offs, fr);
     const double dt = a.time->dt;
     for (int round = 0; round < rounds; ++round) {
         const int tb = (round * gridDim.x + blockIdx.x) * per;
-        // the windows of the block's rows (threads 0..17: row 0 or 1 of the
-        // block, times the 9 neighbouring rows of cells)
-        if (threadIdx.x < 18) {
-            const int w = threadIdx.x;
-            int lo = 0, len = 0;
-            const int te = min(tb + per, a.n) - 1;
-            if (tb < a.n) {
-                const int k0 = a.ckey[tb], k1 = a.ckey[te];
-                if (k0 >= 0 && k1 >= 0) {
-                    const int r0 = k0 / gl0, r1 = k1 / gl0;
-                    const int rr = r0 + (w >= 9 ? 1 : 0);
-                    if (r1 - r0 <= 1 && rr <= r1) {
-                        const int xa = (rr == r0) ? k0 % gl0 + 1 : 1;
-                        const int xb = (rr == r1) ? k1 % gl0 + 1 : gl0;
-                        const int y = rr % gl1 + 1, z = rr / gl1 + 1;
-                        const int rc = w % 9;
-                        const int ty = y + rc % 3 - 1, tz = z + rc / 3 - 1;
-                        if (ty >= 1 && ty <= gl1 && tz >= 1 && tz <= gl2) {
-                            const int xl = xa > 1 ? xa - 1 : 1, xh = xb < gl0 ? xb + 1 : gl0;
-                            const int ka = (xl - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
-                            const int kb = (xh - 1) + gl0 * ((ty - 1) + gl1 * (tz - 1));
-                            lo = a.cell_start[ka];
-                            len = a.cell_start[kb + 1] - lo;
-                        }
-                    }
-                }
-            }
-            wlo[w] = lo;
-            wlen[w] = len;
-        }
-        if (threadIdx.x == 0) row0 = (tb < a.n && a.ckey[tb] >= 0) ? a.ckey[tb] / gl0 : -1;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int off = 0;
-            for (int w = 0; w < 18; ++w) {
-                if (off + wlen[w] > kStageCap) wlen[w] = 0;   // read from global memory
-                woff[w] = off;
-                off += wlen[w];
-            }
-        }
-        __syncthreads();
-        for (int w = 0; w < 18; ++w) {
-            const int lo = wlo[w], len = wlen[w], o = woff[w];
-            for (int u = threadIdx.x; u < len; u += kStageThreads) {
-                stage[2 * (o + u)] = a.frec0[2 * (size_t)(lo + u)];
-                stage[2 * (o + u) + 1] = a.frec0[2 * (size_t)(lo + u) + 1];
-            }
-        }
-        __syncthreads();
+        stage_rows<2>(a, tb, per, W, stage, kStageCap, a.frec0, 2);
         const int t = tb + sub;
         const bool live = t < a.n;
         int nreal = 0, gn = 0, i = 0, wbase = 0;
@@ -348,8 +377,7 @@ __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) 
             xi = r.a;
             vi = r.b;
             i = a.cell_list[t];
-            const int kt = a.ckey[t];
-            wbase = (kt >= 0 && kt / gl0 != row0) ? 9 : 0;
+            wbase = stage_base(a, W, t);
         }
         const unsigned *spos = a.nidx + (size_t)t * a.nstride;
         double xs[3] = {0.0, 0.0, 0.0};
@@ -368,17 +396,14 @@ __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) 
             float4 vj;
             if (k < nreal) {
                 const unsigned e = spos[k];
-                const unsigned code = e >> 26;
-                const float4 o = offs[code];
-                const int p = (int)(e & kPosMask);
-                const int w = wbase + (int)(code / 3u);
-                const int u = p - wlo[w];
+                const float4 o = offs[e >> 26];
+                const int si = stage_index(W, wbase, e);
                 float4 xj;
-                if ((unsigned)u < (unsigned)wlen[w]) {
-                    xj = stage[2 * (woff[w] + u)];
-                    vj = stage[2 * (woff[w] + u) + 1];
+                if (si >= 0) {
+                    xj = stage[2 * si];
+                    vj = stage[2 * si + 1];
                 } else {
-                    const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)p);
+                    const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)(e & kPosMask));
                     xj = r.a;
                     vj = r.b;
                 }
@@ -536,10 +561,14 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // Four resident blocks (64 registers) hide the record gathers' latency
 // better than three at 80 registers (measured with 16 lanes per particle:
 // 1.70 against 2.19 ms per step on the 2M bar).
-template <bool ASYM, bool KAHAN>
-__global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_flag) {
+// STAGED: 128-thread blocks whose rows of neighbour records are staged in
+// shared memory as in k_strain_staged (stage_rows); the same sums.
+template <bool ASYM, bool KAHAN, bool STAGED>
+__global__ void __launch_bounds__(STAGED ? kStageThreads : 256, 4) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
+    __shared__ float4 stage[STAGED ? 3 * kStageCapM : 1];
+    __shared__ StageWin W;
     if (skip_step(a)) return;
     const int sub = threadIdx.x / L, lane = threadIdx.x % L;
     const int per = blockDim.x / L;
@@ -554,12 +583,15 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
     double xlo[3] = {1.0e20, 1.0e20, 1.0e20}, xhi[3] = {-1.0e20, -1.0e20, -1.0e20};
     const bool do_int = integrate_flag && !a.time->ended;
     for (int round = 0; round < rounds; ++round) {
-        const int t = (round * gridDim.x + blockIdx.x) * per + sub;
+        const int tb = (round * gridDim.x + blockIdx.x) * per;
+        if (STAGED) stage_rows<3>(a, tb, per, W, stage, kStageCapM, a.frec0, 4);
+        const int t = tb + sub;
         const bool live = t < a.n;
-        int nreal = 0, gn = 0, i = 0;
+        int nreal = 0, gn = 0, i = 0, wbase = 0;
         float4 xi = make_float4(0.f, 0.f, 0.f, 1.f), r1i = make_float4(0.f, 0.f, 0.f, 0.f),
                r2i = make_float4(0.f, 0.f, 0.f, 1.f), r3i = make_float4(0.f, 0.f, 0.f, 0.f);
         if (live) {
+            if (STAGED) wbase = stage_base(a, W, t);
             nreal = a.nnbr[t];
             gn = a.gnnbr[t];
             const Rec8 r = ld_rec8(a.frec0 + 4 * (size_t)t);
@@ -582,10 +614,18 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
                 const unsigned e = spos[k];
                 const float4 o = offs[e >> 26];
                 const size_t p = e & kPosMask;
-                const Rec8 r = ld_rec8(a.frec0 + 4 * p);
-                const float4 xj = r.a;
-                r1 = r.b;
-                r2 = ld_rec4(a.frec0 + 4 * p + 2);
+                const int si = STAGED ? stage_index(W, wbase, e) : -1;
+                float4 xj;
+                if (si >= 0) {
+                    xj = stage[3 * si];
+                    r1 = stage[3 * si + 1];
+                    r2 = stage[3 * si + 2];
+                } else {
+                    const Rec8 r = ld_rec8(a.frec0 + 4 * p);
+                    xj = r.a;
+                    r1 = r.b;
+                    r2 = ld_rec4(a.frec0 + 4 * p + 2);
+                }
                 if (asym) r3 = ld_rec4(a.frec0 + 4 * p + 3);
                 dx = (xi.x - xj.x) - o.x;
                 dy = (xi.y - xj.y) - o.y;
@@ -663,7 +703,8 @@ __global__ void __launch_bounds__(256, 4) k_momentum(StepArgs a, int integrate_f
                 for (int d = 0; d < 3; ++d) { xlo[d] = fmin(xlo[d], xn[d]); xhi[d] = fmax(xhi[d], xn[d]); }
             }
         }
-        __syncwarp();
+        if (STAGED) __syncthreads();   // the next round overwrites the windows
+        else __syncwarp();
     }
     const int stride = 5 * nm + 6;
     double *out = a.red + (size_t)blockIdx.x * stride;
@@ -710,15 +751,24 @@ void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
 }
 
 int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
+    if (a.pair_kind == 2 && !a.prm.kahan) {
+        int blocks = nblk(a.n, kStageThreads / L);
+        if (blocks > 148 * 4) blocks = 148 * 4;
+        if (a.red_blocks > 0 && blocks > a.red_blocks) blocks = a.red_blocks;
+        if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
+        if (a.prm.asym) k_momentum<true, false, true><<<blocks, kStageThreads, 0, s>>>(a, integrate_flag);
+        else k_momentum<false, false, true><<<blocks, kStageThreads, 0, s>>>(a, integrate_flag);
+        return blocks;
+    }
     const int blocks = pair_blocks_of(a, L);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
     const int th = pair_threads_of(a);
     if (a.prm.asym) {
-        if (a.prm.kahan) k_momentum<true, true><<<blocks, th, 0, s>>>(a, integrate_flag);
-        else k_momentum<true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+        if (a.prm.kahan) k_momentum<true, true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+        else k_momentum<true, false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
     } else {
-        if (a.prm.kahan) k_momentum<false, true><<<blocks, th, 0, s>>>(a, integrate_flag);
-        else k_momentum<false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+        if (a.prm.kahan) k_momentum<false, true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
+        else k_momentum<false, false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
     }
     return blocks;
 }

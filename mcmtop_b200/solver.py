@@ -319,7 +319,7 @@ class Solver:
     def set_tuning(self, search_threads: int = 0, pair_threads: int = 0, pair_blocks_per_sm: int = 0,
                    nbr_stride: int = 0, search_kind: int = 0, pair_kind: int = 0) -> None:
         """search_kind 1: one thread per particle, 2: one warp per particle, 3: one warp per cell;
-        pair_kind (mixed strain gather) 1: records through L1, 2: rows staged in shared memory."""
+        pair_kind (mixed gathers) 1: records through L1, 2: rows staged in shared memory."""
         t = _abi.Tuning(search_threads, pair_threads, pair_blocks_per_sm, nbr_stride, search_kind, pair_kind, 0.0)
         check(self.lib.mcm_gpu_set_tuning(self.h, C.byref(t)), "mcm_gpu_set_tuning", self.h)
 

@@ -167,9 +167,10 @@ def test_mixed_compensated_sums(lib):
 
 
 def test_mixed_staged_strain_gather_is_bitwise_the_same(lib):
-    """The strain gather with each block's rows of neighbour records staged in
-    shared memory (pair_kind 2) reads the same records: bitwise the same state
-    as the per-neighbour gather, on the bar and on the fluid column (ghosts)."""
+    """The strain and momentum gathers with each block's rows of neighbour
+    records staged in shared memory (pair_kind 2) read the same records:
+    bitwise the same state as the per-neighbour gathers, on the bar and on the
+    fluid column (ghosts)."""
     for deck in (taylor_bar(dx=0.4e-3), fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))):
         a, b = Solver(deck, _abi.PREC_MIXED), Solver(deck, _abi.PREC_MIXED)
         b.set_tuning(pair_kind=2)
