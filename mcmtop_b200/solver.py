@@ -136,7 +136,12 @@ class Solver:
         self.dt = min(self.dt, 1.1 * self.dtold)
         self.ptime = self.ptime + self.dt
 
-    def step_b(self) -> np.ndarray:
+    def step_b(self, energies: bool = True):
+        """mcm_gpu_step_b; with energies False it only enqueues the step's work
+        (a driver that reads the energies at output times, energies_now())."""
+        if not energies:
+            check(self.lib.mcm_gpu_step_b(self.h, None), "mcm_gpu_step_b", self.h)
+            return None
         check(self.lib.mcm_gpu_step_b(self.h, _dptr(self.energies)), "mcm_gpu_step_b", self.h)
         return self.energies
 
@@ -153,13 +158,14 @@ class Solver:
               "mcm_gpu_step_c", self.h)
         self.timestep += 1
 
-    def step(self) -> bool:
-        """One iteration of MCM/mcm_solution.f90:37-138; False once it terminates."""
+    def step(self, energies: bool = True) -> bool:
+        """One iteration of MCM/mcm_solution.f90:37-138; False once it terminates.
+        energies False: step_b does not wait for the energy sums."""
         if self.ended:
             return False
         self.step_a()
         self.dt_update()
-        self.step_b()
+        self.step_b(energies)
         if self.ptime - self.dt >= self.deck.endtime:   # :101
             self.ended = True
             return False
