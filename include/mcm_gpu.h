@@ -251,9 +251,10 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
  * synchronisation out of the time step).  Particles whose mat lies outside
  * 1..nmat are skipped.  Its scratch is a fixed __device__ array of
  * 296 x 5 x 16 doubles (189 440 bytes per GPU, held until exit); nmat above
- * MCM_GPU_MAX_MATERIALS returns MCM_EINVAL.  Every call looks up the array's
- * address in the current device's context, which a stream capture in
- * progress may not allow: call it outside captures.  Calls share the array,
+ * MCM_GPU_MAX_MATERIALS returns MCM_EINVAL.  The first call on each device
+ * looks up the array's device address (make that first call before any
+ * stream capture) and keeps it for the process: do not call it after a
+ * cudaDeviceReset of that device.  Calls share the array,
  * so calls whose kernels overlap on the GPU race.  Runs on `stream` (NULL:
  * the default stream) and waits for it; an error already pending from the
  * caller's earlier CUDA work returns MCM_ECUDA before anything is launched. */

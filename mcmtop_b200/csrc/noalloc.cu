@@ -15,6 +15,8 @@
 // until the process exits.  All calls share it: each call overwrites every
 // slot it later reads, so nothing has to start at zero, but calls whose
 // kernels overlap on the GPU (different streams or devices sharing it) race.
+#include <mutex>
+
 #include "kernels.h"
 
 namespace {
@@ -85,13 +87,23 @@ __global__ void k_calctotale_finish(const double *partials, int nmat, double *ou
     }
 }
 
-// Device address of g_noalloc_partials in the current device's context.  It
-// is looked up on every call (cudaGetSymbolAddress allocates nothing), so a
-// context that was torn down and recreated never sees a stale address.
+// Device address of g_noalloc_partials, looked up once per device (with that
+// device current) by the first call on it and kept for the process.  The
+// address belongs to the device's primary context: a process that resets the
+// device (cudaDeviceReset) must not call the entry point afterwards.
+std::mutex g_scratch_mu;
+void *g_scratch_ptr[64] = {};
+
 int scratch_address(double **out) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return MCM_ECUDA;
-    *out = static_cast<double *>(p);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MCM_ECUDA;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return MCM_ECUDA;
+        g_scratch_ptr[dev] = p;
+    }
+    *out = static_cast<double *>(g_scratch_ptr[dev]);
     return MCM_OK;
 }
 
