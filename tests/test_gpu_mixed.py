@@ -189,18 +189,20 @@ def test_mixed_fluid_column_long_run(lib):
     for 300 mixed-precision steps, the neighbour lists rebuilt every step:
     positions and velocities within 1e-4 of their range of the FP64 oracle's,
     the same neighbour sets at the end, and the total energy of mcm_calctotale
-    drifting as the oracle's does (within 1e-4 of the initial total)."""
+    within 1e-4 of the oracle's (relative to the largest kinetic energy)."""
     deck = fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3))
     sol = Solver(deck, _abi.PREC_MIXED)
     orc = Oracle(deck)
-    e0, o0 = sol.energies_now()[-1], orc.scalar("totale")
-    gap = 0.0
+    # the column starts at rest with zero internal energy: the totals are
+    # compared against the largest kinetic energy the oracle reaches
+    gaps, scale = [], 0.0
     for _ in range(6):
         assert sol.run(50) == 50
         assert orc.run(50) == 50
-        dg = (sol.energies_now()[-1] - e0) / abs(e0)
-        do = (orc.scalar("totale") - o0) / abs(o0)
-        gap = max(gap, abs(dg - do))
+        gaps.append(abs(sol.energies_now()[-1] - orc.scalar("totale")))
+        scale = max(scale, abs(orc.scalar("kinetice")))
+    assert scale > 0.0
+    gap = max(gaps) / scale
     assert gap <= 1e-4, gap
     errs = compare(sol, orc, ["x", "v"], 1e-4, "mixed fluid column, 300 steps")
     print("fluid column, 300 mixed steps:", errs, "energy gap", gap)
