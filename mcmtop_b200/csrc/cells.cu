@@ -510,7 +510,16 @@ __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
     return s;
 }
 
+// Variants of the search, fixed at compile time so that the candidate loop of
+// the common case (one material, no repulsive contact, no minimum distance)
+// tests none of these flags per candidate.
+enum { kSrchContact = 1, kSrchTwoPass = 2, kSrchMind = 4 };
+
+template <int V>
 __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
+    constexpr bool contact = (V & kSrchContact) != 0;   // contacttype > 0: other materials -> contact list
+    constexpr bool two_pass = (V & kSrchTwoPass) != 0;  // kernel contact between materials: own material first
+    constexpr bool want_mind = (V & kSrchMind) != 0;    // FP64 minimum distance (tcrit option 2, diagnostics)
     if (a.status->code) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
@@ -519,16 +528,15 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     const int key = a.ckey[t];
     const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
-    const bool want_mind = (a.prm.tcrit_opt == 2 || a.prm.diag);
     int nn = 0, gn = 0, nc = 0, gcn = 0;
     double mind = 1.0e20;
     if (key >= 0) {
         const DevGrid g = *a.grid;
         int bx, by, bz;
         cell_coords(key, g.gridlim, bx, by, bz);
-        const int lo0 = bx > 1 ? bx - 1 : 1, hi0 = bx < g.gridlim[0] ? bx + 1 : g.gridlim[0];
         const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
         const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
+        const bool has_l = bx > 1, has_r = bx < g.gridlim[0];
         const double4 xi = a.cpos[t];
         const float4 ui = a.cposf[t];
         const float cs[3] = {(float)(1.0 / g.gridsize[0]), (float)(1.0 / g.gridsize[1]), (float)(1.0 / g.gridsize[2])};
@@ -539,16 +547,18 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         const float khi = 1.0f + 2.44140625e-4f, klo = 1.0f - 2.44140625e-4f;
         const float reach = ui.w + (float)g.hcut;
         const float reach2 = reach * reach * 1.0009765625f + 9.765625e-4f * csm * csm;
+        // this particle relative to the origins of the left, own and right cell of a row
+        const float qxl = ui.x + cs[0], qxr = ui.x - cs[0];
+        const float gxl = fmaxf(ui.x, 0.0f), gxr = fmaxf(cs[0] - ui.x, 0.0f);
         const int mati = a.cmat[t];
         unsigned *out = a.nidx + (size_t)t * cap;
         // MCM/mcm_ll_neighbours.f90:150-174, 238-267: other materials'
         // particles are appended after the own material's with kernel contact
         // (a second walk), and form the contact list otherwise (the same walk,
         // each list in walk order)
-        const bool contact = a.prm.contact != 0;
         unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
-        const int passes = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
-        for (int pass = 0; pass < passes; ++pass) {
+#pragma unroll 1
+        for (int pass = 0; pass < (two_pass ? 2 : 1); ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
                 const float qz = ui.z + (float)(bz - nz) * cs[2];
                 const float gz = fmaxf(nz < bz ? ui.z : (nz > bz ? cs[2] - ui.z : 0.0f), 0.0f);
@@ -557,44 +567,45 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     const float gy = fmaxf(my < by ? ui.y : (my > by ? cs[1] - ui.y : 0.0f), 0.0f);
                     const float gyz = gy * gy + gz * gz;
                     if (gyz > reach2) continue;
-                    const int k0 = (int)cell_key(lo0, my, nz, g.gridlim);
+                    // the row's x-adjacent cells are contiguous in position
+                    // order: one range from the first to the last cell whose
+                    // box is within reach (the own cell always is)
+                    const int kc = (int)cell_key(bx, my, nz, g.gridlim);
+                    const int s1 = a.cell_start[kc], s2 = a.cell_start[kc + 1];
+                    const int rb = (has_l && !(gyz + gxl * gxl > reach2)) ? a.cell_start[kc - 1] : s1;
+                    const int re = (has_r && !(gyz + gxr * gxr > reach2)) ? a.cell_start[kc + 2] : s2;
                     const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
-                    for (int lx = lo0; lx <= hi0; ++lx) {
-                        const float gx = fmaxf(lx < bx ? ui.x : (lx > bx ? cs[0] - ui.x : 0.0f), 0.0f);
-                        if (gyz + gx * gx > reach2) continue;
-                        const int cb = a.cell_start[k0 + (lx - lo0)], ce = a.cell_start[k0 + (lx - lo0) + 1];
-                        // this particle relative to the origin of candidate cell lx
-                        const float qx = ui.x + (float)(bx - lx) * cs[0];
-                        const unsigned code = (code_yz + (unsigned)(lx - bx + 1)) << 26;
-                        for (int p = cb; p < ce; ++p) {
-                            const float4 c = a.cposf[p];
-                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
-                            const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            const float hsf = ui.w + c.w;
-                            const float r2f = hsf * hsf;
-                            if (d2f >= fmaf(r2f, khi, kb)) continue;
-                            if (p == t) continue;
-                            double d2 = 0.0;
-                            if (d2f > fmaf(r2f, klo, -kb) || want_mind) {
-                                // near tie (or mindist wanted): the reference's FP64 test
-                                const double4 cd = a.cpos[p];
-                                d2 = exact_d2(xi, cd);
-                                const double hs = __dadd_rn(cd.w, xi.w);
-                                if (!(d2 < __dmul_rn(hs, hs))) continue;
-                            }
-                            if (contact) {
-                                if (a.cmat[p] != mati) {
-                                    if (nc < a.cstride) cout[nc] = (unsigned)p | code;
-                                    ++nc;
-                                    continue;
-                                }
-                            } else if (a.nmat > 1 && (a.cmat[p] == mati) != (pass == 0)) {
+                    for (int p = rb; p < re; ++p) {
+                        const float4 c = a.cposf[p];
+                        const bool left = p < s1, right = p >= s2;
+                        const float qx = left ? qxl : (right ? qxr : ui.x);
+                        const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                        const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float hsf = ui.w + c.w;
+                        const float r2f = hsf * hsf;
+                        if (d2f >= fmaf(r2f, khi, kb)) continue;
+                        if (p == t) continue;
+                        double d2 = 0.0;
+                        if (want_mind || d2f > fmaf(r2f, klo, -kb)) {
+                            // near tie (or mindist wanted): the reference's FP64 test
+                            const double4 cd = a.cpos[p];
+                            d2 = exact_d2(xi, cd);
+                            const double hs = __dadd_rn(cd.w, xi.w);
+                            if (!(d2 < __dmul_rn(hs, hs))) continue;
+                        }
+                        const unsigned code = (code_yz + (left ? 0u : (right ? 2u : 1u))) << 26;
+                        if (contact) {
+                            if (a.cmat[p] != mati) {
+                                if (nc < a.cstride) cout[nc] = (unsigned)p | code;
+                                ++nc;
                                 continue;
                             }
-                            if (want_mind) mind = fmin(mind, d2);
-                            if (nn < cap) out[nn] = (unsigned)p | code;
-                            ++nn;
+                        } else if (two_pass) {
+                            if ((a.cmat[p] == mati) != (pass == 0)) continue;
                         }
+                        if (want_mind) mind = fmin(mind, d2);
+                        if (nn < cap) out[nn] = (unsigned)p | code;
+                        ++nn;
                     }
                 }
             }
@@ -609,13 +620,14 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         }
         // ghosts: only neighbourhoods that reach a ghost layer
         if (a.prm.boundary) {
+            const int lo0 = has_l ? bx - 1 : bx, hi0 = has_r ? bx + 1 : bx;
             const DevPlanes &pl = a.prm.planes;
             const bool near = (lo0 == 1 && pl.code[0][0]) || (hi0 == g.gridlim[0] && pl.code[1][0]) ||
                               (lo1 == 1 && pl.code[0][1]) || (hi1 == g.gridlim[1] && pl.code[1][1]) ||
                               (lo2 == 1 && pl.code[0][2]) || (hi2 == g.gridlim[2] && pl.code[1][2]);
             if (near) {
-                const int gpasses = (a.nmat > 1 && a.prm.contacttype == 0) ? 2 : 1;
-                for (int pass = 0; pass < gpasses; ++pass) {
+#pragma unroll 1
+                for (int pass = 0; pass < (two_pass ? 2 : 1); ++pass) {
                     for (int nz = lo2; nz <= hi2; ++nz)
                         for (int my = lo1; my <= hi1; ++my)
                             for (int lx = lo0; lx <= hi0; ++lx) {
@@ -632,8 +644,8 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                                 ++gcn;
                                                 continue;
                                             }
-                                        } else if (a.nmat > 1 && (a.gmat[q] == mati) != (pass == 0)) {
-                                            continue;
+                                        } else if (two_pass) {
+                                            if ((a.gmat[q] == mati) != (pass == 0)) continue;
                                         }
                                         mind = fmin(mind, d2);
                                         if (gn < a.gstride) a.gnbr[(size_t)gn * np + t] = q;
@@ -646,7 +658,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     atomicMax(&a.status->req_gstride, gn);
                     raise_status(a.status, MCM_ENBR_OVERFLOW, i);
                 }
-                if (gcn > a.gcstride) {
+                if (contact && gcn > a.gcstride) {
                     atomicMax(&a.status->req_gcstride, gcn);
                     raise_status(a.status, MCM_ENBR_OVERFLOW, i);
                 }
@@ -657,7 +669,7 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     if (with_self) nn += 1;   // MCM/mcm_ll_neighbours.f90:288-299 (for every particle)
     a.nnbr[t] = nn;
     a.gnnbr[t] = gn;
-    if (a.prm.contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
+    if (contact) { a.ncont[t] = nc; a.gncont[t] = gcn; }
     if (want_mind) a.F.f[FMINDIST][i] = mind;
     atomicMax(&a.status->max_nbr, nn);
     atomicMax(&a.status->max_gnbr, gn);
@@ -1335,7 +1347,18 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
         const long long lanes = 32LL * a.n;
         k_search_warp<<<(unsigned)((lanes + threads - 1) / threads), threads, 0, s>>>(a);
     } else {
-        k_search<<<(a.n + threads - 1) / threads, threads, 0, s>>>(a);
+        const bool mind = a.prm.tcrit_opt == 2 || a.prm.diag;
+        const int v = (a.prm.contact ? kSrchContact : 0) | ((a.nmat > 1 && a.prm.contacttype == 0) ? kSrchTwoPass : 0) |
+                      (mind ? kSrchMind : 0);
+        const unsigned nb = (unsigned)((a.n + threads - 1) / threads);
+        switch (v) {
+            case 0: k_search<0><<<nb, threads, 0, s>>>(a); break;
+            case kSrchContact: k_search<kSrchContact><<<nb, threads, 0, s>>>(a); break;
+            case kSrchTwoPass: k_search<kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
+            case kSrchMind: k_search<kSrchMind><<<nb, threads, 0, s>>>(a); break;
+            case kSrchContact | kSrchMind: k_search<kSrchContact | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+            default: k_search<kSrchTwoPass | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+        }
     }
 }
 
