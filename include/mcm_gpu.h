@@ -311,6 +311,9 @@ typedef struct {
     int pair_kind;           /* mixed-precision strain and momentum gathers: 1 neighbour records
                                 through L1 (the default), 2 each block's rows of neighbour cells
                                 staged in shared memory (the same sums) */
+    int adj_kind;            /* reverse of the per-particle update in mcm_gpu_adjoint_backward: 1 one
+                                hand-written reverse pass when every material is model 10 with EOS 41
+                                (the default), 2 forward-mode dual numbers (any supported material) */
     double ms_per_step;      /* mcm_gpu_autotune: device time per loop iteration of the chosen shape */
 } mcm_gpu_tuning;
 

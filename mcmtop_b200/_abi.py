@@ -78,7 +78,7 @@ class Time(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("search_threads", C.c_int), ("pair_threads", C.c_int), ("pair_blocks_per_sm", C.c_int),
                 ("nbr_stride", C.c_int), ("search_kind", C.c_int), ("pair_kind", C.c_int),
-                ("ms_per_step", C.c_double)]
+                ("adj_kind", C.c_int), ("ms_per_step", C.c_double)]
 
 
 # per-particle width of every field in Fields (doubles or ints)

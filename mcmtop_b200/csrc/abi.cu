@@ -1700,6 +1700,9 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     for (int u = 0; u < 9; ++u) b.gb[u] = arr(31 + u);
     b.rec = reinterpret_cast<double4 *>(arr(40));   // 4 * kRecSlots doubles per position
     b.theta_b = h->d_theta;
+    b.rev = h->adj_kind == 1 ? 1 : 0;
+    for (const mcm_gpu_material &m : h->mats)
+        if (m.model != 10 || m.eos != 41) b.rev = 0;
     // final adjoints, Fortran (3,np) by particle -> state order
     std::vector<double> tmp(n);
     for (int d = 0; d < 3; ++d) {

@@ -28,10 +28,12 @@
 // ghost terms, which belong to a parent particle, use atomics):
 //   k_adj_move        x', v' -> x, v, a          (reflections by their branch)
 //   k_adj_momentum    a -> S (post-constitutive sigma', q', rho'), x, ghost parents
-//   k_adj_constitutive  the per-particle vector-Jacobian product of C by forward-
-//                     mode dual numbers through the same templated code the step
-//                     runs (physics.cuh), so the derivative is the one of the
-//                     branch taken (the active branch of the return map)
+//   k_adj_constitutive  the per-particle vector-Jacobian product of C: one
+//                     hand-written reverse pass when every material is model 10
+//                     with EOS 41, else forward-mode dual numbers through the same
+//                     templated code the step runs (physics.cuh); either way the
+//                     derivative is the one of the branch taken (the active
+//                     branch of the return map)
 //   k_adj_strain      G -> x, v, rho (through V = m/rho), ghost parents
 #include "nbr_iter.cuh"
 #include "physics.cuh"
@@ -423,8 +425,420 @@ __device__ __forceinline__ void constitutive_pass(int pass, const StepArgs &a, c
     }
 }
 
-__global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) {
-    __shared__ double sth[kParams][64];
+// ------------------------------------------- constitutive, reverse mode
+// The vector-Jacobian product of the per-particle update for model 10 with
+// EOS 41 in one reverse pass (no dual numbers): the forward values of
+// rhoupd, the Jaumann rotation, f3dm10, eos41c, nodalav, hieupd, eqos41 and
+// stress_up are recomputed with the step's expressions (this translation
+// unit has no fused multiply-add, like the dual passes), the branches taken
+// are kept, and the adjoints are propagated back through them.  The only
+// derivative taken in forward mode is that of the rotation matrix with
+// respect to the three spin components.
+__device__ __forceinline__ double f_tmax(double a, double b) { return a > b ? a : (b > a ? b : a); }
+
+__device__ __forceinline__ void reverse_m10_eos41(const StepArgs &a, const AdjArgs &b, int i, const DevMaterial &M,
+                                                  const double (&yb)[11], double (&ub)[kInputs],
+                                                  double (&th)[kParams]) {
+    const double *const *pre = b.pre;
+    const double *const *f = a.F.f;
+    const double dt = b.dt_prev;
+    const double third = 1.0 / 3.0;
+    const double f30 = (double)1.e-30f, f12 = (double)1.e-12f;
+    // ------------------------------------------------------------ forward
+    const double mass = pre[FMASS][i], hpart = pre[FH][i], rho0 = M.rho;
+    const double rho_in = pre[FRHO][i], e_in = pre[FE][i], efps_in = pre[FEFPS][i];
+    const double pcut_in = pre[FPCUT][i], fail_in = pre[FFAIL][i];
+    double sg[6], rod[6];
+#pragma unroll
+    for (int u = 0; u < 6; ++u) { sg[u] = pre[FS11 + u][i]; rod[u] = f[FR11 + u][i]; }
+    const double spin[3] = {f[FW12][i], f[FW13][i], f[FW23][i]};
+    const double tr_in = f[FTR][i];
+    // rhoupd (MCM/mcm_rhoupd.f90:24-56)
+    const double rfac = 1.0 - tr_in * dt;
+    const double rho_a = rho_in * rfac;
+    const bool capped = rho_a > M.rho_max;
+    const double rho1 = capped ? rho_a / rfac : rho_a;
+    const double tr = capped ? 0.0 : tr_in;
+    if (capped) {
+        rod[0] = rod[0] - third * tr_in;
+        rod[1] = rod[1] - third * tr_in;
+        rod[2] = rod[2] - third * tr_in;
+    }
+    // Jaumann rotation: sp = Q S Q^T (S symmetric, its (3,1) the upper 13)
+    double Q[9];
+    jaumann_q(spin, dt, Q);
+    const double S[9] = {sg[T11], sg[T12], sg[T13], sg[T12], sg[T22], sg[T23], sg[T13], sg[T23], sg[T33]};
+    double QS[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) QS[3 * r + c] = Q[3 * r] * S[c] + Q[3 * r + 1] * S[3 + c] + Q[3 * r + 2] * S[6 + c];
+    // the six outputs as (row, column) of Q S Q^T, storage order 11 22 33 12 13 23
+    constexpr int RR[6] = {0, 1, 2, 0, 0, 1}, RC[6] = {0, 1, 2, 1, 2, 2};
+    double sp[6];
+#pragma unroll
+    for (int u = 0; u < 6; ++u)
+        sp[u] = QS[3 * RR[u]] * Q[3 * RC[u]] + QS[3 * RR[u] + 1] * Q[3 * RC[u] + 1] + QS[3 * RR[u] + 2] * Q[3 * RC[u] + 2];
+    // f3dm10 (MCM/mcm_f3dm10.f90:28-157)
+    const double gg = M.strinput[0], qs = M.strinput[1], qh = M.strinput[2], a1 = M.strinput[4], a2 = M.strinput[5];
+    const int ispall = (int)M.strinput[6];
+    const double epf = M.strinput[7];
+    const double g2 = 2.0 * dt * gg;
+    const double davg = third * tr;
+    const double p3 = -third * (sp[0] + sp[1] + sp[2]);
+    const double mp = f_tmax(0.0, p3);
+    const double ak0 = qs + qh * efps_in + (a1 + a2 * p3) * mp;
+    double s1[6];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s1[d] = sp[d] + p3 + g2 * (rod[d] + davg);
+#pragma unroll
+    for (int d = 3; d < 6; ++d) s1[d] = sp[d] + 0.5 * g2 * rod[d];
+    double scle3 = 1.0, pcut = pcut_in;
+    if (ispall == 3) {
+        scle3 = 0.5 * (1.0 + (p3 - pcut >= 0.0 ? 1.0 : -1.0));
+        pcut = scle3 * pcut;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) s1[u] = scle3 * s1[u];
+    }
+    const double aj2 = 0.5 * (s1[0] * s1[0] + s1[1] * s1[1] + s1[2] * s1[2]) + s1[3] * s1[3] + s1[4] * s1[4] + s1[5] * s1[5];
+    const double sj2 = sqrt(3.0 * aj2);
+    const bool yielding = fail_in == 1.0;
+    double thrg = 0.0, den = 0.0, fdv = 0.0, t1 = 0.0, defps = 0.0;
+    bool fd_on = false, den_on = false, m_is_sj2 = false;
+    if (yielding) {
+        thrg = third / gg;
+        fd_on = sj2 > ak0;
+        fdv = fd_on ? sj2 - ak0 : 0.0;
+        den_on = 1.0 > -thrg * qh;
+        den = f30 + (den_on ? 1.0 - (-thrg * qh) : 0.0);
+        t1 = fdv / den;
+        m_is_sj2 = !(t1 < sj2);   // tmin(sj2, t1): sj2 unless t1 < sj2
+        defps = thrg * (m_is_sj2 ? sj2 : t1);
+    }
+    const double efps_out = yielding ? efps_in + defps : efps_in;
+    const double xk = ak0 + qh * defps;
+    const bool xk_on = !(0.0 > xk);   // tmax(xk, 0): xk unless 0 > xk
+    const double ak2 = xk_on ? xk : 0.0;
+    const double seps = f30 * gg;
+    const bool mx_is_ak = !(sj2 > ak2);   // tmax(ak2, sj2)
+    const double mx = mx_is_ak ? ak2 : sj2;
+    const double scle = (ak2 + seps) / (mx + seps);
+    double s2[6];
+#pragma unroll
+    for (int u = 0; u < 6; ++u) s2[u] = scle * s1[u];
+    const bool broke = epf != 0.0 && efps_out > epf;
+    double scle2 = 1.0;
+    if (broke) {
+#pragma unroll
+        for (int u = 0; u < 6; ++u) s2[u] = 0.0;
+    }
+    if (ispall == 2) {
+        const double aj = 0.5 * (s2[0] * s2[0] + s2[1] * s2[1] + s2[2] * s2[2]) + s2[3] * s2[3] + s2[4] * s2[4] +
+                          s2[5] * s2[5] + f12;
+        const double dj = s2[0] * s2[5] * s2[5] + s2[1] * s2[4] * s2[4] + s2[2] * s2[3] * s2[3] -
+                          s2[0] * s2[1] * s2[2] - 2.0 * s2[3] * s2[4] * s2[5];
+        double akt = -sqrt(27.0 / aj) * dj * 0.5 / aj;
+        const double am = fabs(akt) < 1.0 ? fabs(akt) : (1.0 < fabs(akt) ? 1.0 : fabs(akt));
+        akt = akt >= 0.0 ? am : -am;
+        const double ywh = acos(akt) * third;
+        const double sjp = 2.0 * sqrt(aj * third) * cos(ywh);
+        scle2 = 0.5 * (1.0 + (p3 - sjp - pcut >= 0.0 ? 1.0 : -1.0));
+        pcut = scle2 * pcut;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) s2[u] = scle2 * s2[u];
+    }
+    // eos41c (MCM/mcm_eos41c.f90:31-85): the sound speed of nodalav
+    const double cc = M.eosinput[0], sl = M.eosinput[1], gamma0 = M.eosinput[4];
+    const double e1 = e_in / mass;
+    const double ao = rho0 * (cc * cc);
+    const double mu = rho1 / rho0 - 1.0;
+    const double gam = gamma0 * rho0 / rho1;
+    const double bo = ao * (1.0 + 2.0 * (sl - 1.0));
+    const double co = ao * (2.0 * (sl - 1.0) + 3.0 * ((sl - 1.0) * (sl - 1.0)));
+    const double fg = gam * mu;
+    const double ca1 = ao * (1.0 - fg), cb1 = bo * (2.0 - 1.5 * fg), cc1 = co * (3.0 - 2.0 * fg);
+    const bool comp = mu > 0.0;
+    const double dpdrho = comp ? (ca1 + cb1 * mu + cc1 * (mu * mu)) / rho0 + gam * e1 : ao * (1.0 - fg) / rho0 + gam * e1;
+    const bool at_cut = p3 == pcut;
+    const double c2 = at_cut ? cc * cc : dpdrho + (gam * rho1) * (p3 / (rho1 * rho1));
+    const double csnd = sqrt(c2);
+    // nodalav (MCM/mcm_nodalav.f90:32-47)
+    const bool visc = M.visc_type == 1 && tr < 0.0;
+    double q = 0.0;
+    if (visc) {
+        const double ht = hpart * tr;
+        q = M.av_l * rho1 * csnd * hpart * fabs(tr) + M.av_q * rho1 * (ht * ht);
+    }
+    // hieupd (MCM/mcm_hieupd.f90:27-64)
+    const double pold = p3;
+    const double trq = third * (q + q + q);
+    const double volold = mass / rho_in, volnew = mass / rho1;
+    double einc = 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int t = sym_index(k, l);
+            const double de = (k == l) ? rod[t] * (0.5 * (sp[t] + pold + s2[t]) - q + trq) : rod[t] * (0.5 * (sp[t] + s2[t]));
+            einc = einc + de;
+        }
+    const double vavg = 0.5 * (volnew + volold);
+    const double dvh = volnew - volold;
+    const double etry = e_in + dt * (vavg * einc) - dvh * (0.5 * pold + trq);
+    // eqos41 (MCM/mcm_eqos41.f90:32-102)
+    const double etry1 = etry / mass;
+    const double dvol = mass / rho1 - mass / rho_in;
+    const double vol0 = mass / rho0;
+    const double ph = comp ? ao * mu + bo * (mu * mu) + co * (mu * mu * mu) : ao * mu;
+    const double rg = rho1 * gam;
+    const double num = ph * (1.0 - 0.5 * fg) + rg * etry1;
+    const double dnm = 1.0 + 0.5 * rho1 * gam * dvol / vol0;
+    const double pn = num / dnm;
+    const bool clamp = pn < pcut;
+    const double rfac2 = 1.0 - tr * dt;
+    // ------------------------------------------------------------ reverse
+    // outputs: rho, e, p, efps, sigma (11 22 33 12 13 23), q
+    double rho1_b = 0.0, rhoin_b = 0.0, ein_b = 0.0, tr_b = 0.0, efps_b = 0.0;
+    double gg_b = 0.0, qs_b = 0.0, qh_b = 0.0, sl_b = 0.0;
+    double sp_b[6] = {0, 0, 0, 0, 0, 0}, s2_b[6], rod_b[6] = {0, 0, 0, 0, 0, 0};
+    double p3_b = 0.0, q_b = yb[10];
+    // stress_up: sigma = s - p I
+    double p_b = yb[2] - (yb[4] + yb[5] + yb[6]);
+#pragma unroll
+    for (int u = 0; u < 6; ++u) s2_b[u] = yb[4 + u];
+    // eqos41
+    double etry_b = 0.0, rg_b = 0.0, dvol_b = 0.0, ph_b = 0.0, fg_b = 0.0, mu_b = 0.0, gam_b = 0.0, bo_b = 0.0,
+           co_b = 0.0;
+    if (clamp) {
+        // p = pcut (no derivative); rho = rho1 / (1 - tr dt); e unchanged
+        const double rho_out = rho1 / rfac2;
+        rho1_b += yb[0] / rfac2;
+        tr_b += (-yb[0] * rho_out / rfac2) * (-dt);
+        ein_b += yb[1];
+    } else {
+        rho1_b += yb[0];
+        // e = etry1 mass - dvol pn / 2
+        double pn_b = p_b - 0.5 * dvol * yb[1];
+        double etry1_b = yb[1] * mass;
+        dvol_b += -0.5 * pn * yb[1];
+        const double num_b = pn_b / dnm, dnm_b = -pn_b * pn / dnm;
+        ph_b += num_b * (1.0 - 0.5 * fg);
+        fg_b += -0.5 * ph * num_b;
+        rg_b += num_b * etry1 + dnm_b * 0.5 * dvol / vol0;
+        etry1_b += num_b * rg;
+        dvol_b += dnm_b * 0.5 * rg / vol0;
+        etry_b += etry1_b / mass;
+    }
+    // ph
+    if (comp) {
+        mu_b += ph_b * (ao + 2.0 * bo * mu + 3.0 * co * (mu * mu));
+        bo_b += ph_b * (mu * mu);
+        co_b += ph_b * (mu * mu * mu);
+    } else {
+        mu_b += ph_b * ao;
+    }
+    // rg = rho1 gam, dvol = m/rho1 - m/rho_in
+    rho1_b += rg_b * gam;
+    gam_b += rg_b * rho1;
+    rho1_b += dvol_b * (-mass / (rho1 * rho1));
+    rhoin_b += dvol_b * (mass / (rho_in * rho_in));
+    // hieupd: etry = e + dt vavg einc - dvh (pold/2 + trq)
+    ein_b += etry_b;
+    const double einc_b = etry_b * dt * vavg;
+    const double vavg_b = etry_b * dt * einc;
+    const double dvh_b = -etry_b * (0.5 * pold + trq);
+    double pold_b = -etry_b * dvh * 0.5;
+    double trq_b = -etry_b * dvh;
+    const double vn_b = dvh_b + 0.5 * vavg_b, vo_b = -dvh_b + 0.5 * vavg_b;
+    rho1_b += vn_b * (-mass / (rho1 * rho1));
+    rhoin_b += vo_b * (-mass / (rho_in * rho_in));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        rod_b[d] += einc_b * (0.5 * (sp[d] + pold + s2[d]) - q + trq);
+        sp_b[d] += einc_b * 0.5 * rod[d];
+        pold_b += einc_b * 0.5 * rod[d];
+        s2_b[d] += einc_b * 0.5 * rod[d];
+        q_b += -einc_b * rod[d];
+        trq_b += einc_b * rod[d];
+    }
+#pragma unroll
+    for (int u = 3; u < 6; ++u) {
+        // (k, l) and (l, k): twice rod (sigma + s) / 2
+        rod_b[u] += einc_b * (sp[u] + s2[u]);
+        sp_b[u] += einc_b * rod[u];
+        s2_b[u] += einc_b * rod[u];
+    }
+    q_b += trq_b;   // trq = (q + q + q) / 3
+    p3_b += pold_b;
+    // nodalav
+    double c_b = 0.0;
+    if (visc) {
+        const double atr = fabs(tr);
+        rho1_b += q_b * (M.av_l * csnd * hpart * atr + M.av_q * (hpart * tr) * (hpart * tr));
+        c_b += q_b * M.av_l * rho1 * hpart * atr;
+        tr_b += q_b * (-M.av_l * rho1 * csnd * hpart + M.av_q * rho1 * 2.0 * hpart * hpart * tr);
+    }
+    // eos41c
+    if (!at_cut) {
+        const double c2_b = csnd > 0.0 ? c_b * 0.5 / csnd : 0.0;
+        // c2 = dpdrho + (gam rho1) (p3 / rho1^2)
+        const double A = gam * rho1, B = p3 / (rho1 * rho1);
+        gam_b += c2_b * B * rho1;
+        rho1_b += c2_b * B * gam;
+        p3_b += c2_b * A / (rho1 * rho1);
+        rho1_b += c2_b * A * (-2.0 * p3 / (rho1 * rho1 * rho1));
+        const double e1_b = c2_b * gam;
+        gam_b += c2_b * e1;
+        ein_b += e1_b / mass;
+        if (comp) {
+            const double ca1_b = c2_b / rho0, cb1_b = c2_b * mu / rho0, cc1_b = c2_b * (mu * mu) / rho0;
+            mu_b += c2_b * (cb1 + 2.0 * cc1 * mu) / rho0;
+            fg_b += -ca1_b * ao - 1.5 * cb1_b * bo - 2.0 * cc1_b * co;
+            bo_b += cb1_b * (2.0 - 1.5 * fg);
+            co_b += cc1_b * (3.0 - 2.0 * fg);
+        } else {
+            fg_b += -c2_b * ao / rho0;
+        }
+    }
+    // fg = gam mu, gam = gamma0 rho0 / rho1, mu = rho1 / rho0 - 1, bo(s), co(s)
+    gam_b += fg_b * mu;
+    mu_b += fg_b * gam;
+    rho1_b += gam_b * (-gam / rho1);
+    rho1_b += mu_b / rho0;
+    sl_b += bo_b * 2.0 * ao + co_b * ao * (2.0 + 6.0 * (sl - 1.0));
+    // f3dm10, backwards
+    double s1_b[6];
+#pragma unroll
+    for (int u = 0; u < 6; ++u) s1_b[u] = (broke ? 0.0 : scle * scle2 * s2_b[u]);
+    double scle_b = 0.0;
+    if (!broke) {
+#pragma unroll
+        for (int u = 0; u < 6; ++u) scle_b += scle2 * s2_b[u] * s1[u];
+    }
+    // scle = (ak2 + seps) / (mx + seps)
+    const double nu_b = scle_b / (mx + seps), de_b = -scle_b * scle / (mx + seps);
+    double ak2_b = nu_b, sj2_b = 0.0;
+    gg_b += (nu_b + de_b) * f30;
+    if (mx_is_ak) ak2_b += de_b; else sj2_b += de_b;
+    double ak0_b = 0.0, defps_b = 0.0;
+    if (xk_on) { ak0_b += ak2_b; qh_b += ak2_b * defps; defps_b += ak2_b * qh; }
+    efps_b += yb[3];   // efps_out = efps_in (+ defps)
+    if (yielding) {
+        defps_b += yb[3];
+        const double m_b = defps_b * thrg;
+        double thrg_b = defps_b * (m_is_sj2 ? sj2 : t1);
+        double t1_b = 0.0;
+        if (m_is_sj2) sj2_b += m_b; else t1_b = m_b;
+        const double fd_b = t1_b / den, den_b = -t1_b * t1 / den;
+        if (fd_on) { sj2_b += fd_b; ak0_b -= fd_b; }
+        if (den_on) { thrg_b += den_b * qh; qh_b += den_b * thrg; }   // den = 1e-30 + 1 + thrg qh
+        gg_b += thrg_b * (-thrg / gg);
+    }
+    // sj2 = sqrt(3 aj2)
+    const double aj2_b = sj2 > 0.0 ? sj2_b * 1.5 / sj2 : 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s1_b[d] += aj2_b * s1[d];
+#pragma unroll
+    for (int u = 3; u < 6; ++u) s1_b[u] += aj2_b * 2.0 * s1[u];
+    // s1 = scle3 (sp + p3 I + g2 (rod + davg I)) on the diagonal, scle3 (sp + g2 rod / 2) off it
+    double g2_b = 0.0, davg_b = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double s0_b = scle3 * s1_b[d];
+        sp_b[d] += s0_b;
+        p3_b += s0_b;
+        g2_b += s0_b * (rod[d] + davg);
+        rod_b[d] += s0_b * g2;
+        davg_b += s0_b * g2;
+    }
+#pragma unroll
+    for (int u = 3; u < 6; ++u) {
+        const double s0_b = scle3 * s1_b[u];
+        sp_b[u] += s0_b;
+        g2_b += s0_b * 0.5 * rod[u];
+        rod_b[u] += s0_b * 0.5 * g2;
+    }
+    tr_b += davg_b * third;
+    gg_b += g2_b * 2.0 * dt;
+    // ak0 = qs + qh efps + (a1 + a2 p3) max(0, p3)
+    qs_b += ak0_b;
+    qh_b += ak0_b * efps_in;
+    efps_b += ak0_b * qh;
+    p3_b += ak0_b * (a2 * mp + (p3 > 0.0 ? a1 + a2 * p3 : 0.0));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sp_b[d] += -third * p3_b;
+    // rotation: sp_u = sum_k QS[r][k] Q[c][k]; QS = Q S
+    double QS_b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Q_b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int u = 0; u < 6; ++u)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            QS_b[3 * RR[u] + k] += sp_b[u] * Q[3 * RC[u] + k];
+            Q_b[3 * RC[u] + k] += sp_b[u] * QS[3 * RR[u] + k];
+        }
+    double S_b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                Q_b[3 * r + j] += QS_b[3 * r + k] * S[3 * j + k];
+                S_b[3 * j + k] += QS_b[3 * r + k] * Q[3 * r + j];
+            }
+    // dQ/dspin by three forward directions
+    {
+        using D3 = Dual<3>;
+        D3 w[3] = {D3(spin[0]), D3(spin[1]), D3(spin[2])};
+        w[0].d[0] = 1.0; w[1].d[1] = 1.0; w[2].d[2] = 1.0;
+        D3 Qd[9];
+        jaumann_q(w, D3(dt), Qd);
+        double wb[3] = {0, 0, 0};
+#pragma unroll
+        for (int u = 0; u < 9; ++u)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) wb[k] += Q_b[u] * Qd[u].d[k];
+        ub[16] = wb[0]; ub[17] = wb[1]; ub[18] = wb[2];
+    }
+    // rhoupd
+    if (capped) {
+        // rho1 = (rho_in rfac) / rfac; rod diagonal -= tr_in / 3; tracerod <- 0
+        const double ra_b = rho1_b / rfac;
+        double rf_b = -rho1_b * rho1 / rfac;
+        rhoin_b += ra_b * rfac;
+        rf_b += ra_b * rho_in;
+        double trin_b = rf_b * (-dt);
+        trin_b += -third * (rod_b[0] + rod_b[1] + rod_b[2]);
+        tr_b = trin_b;   // the downstream tracerod is the constant 0
+    } else {
+        rhoin_b += rho1_b * rfac;
+        tr_b += rho1_b * (-rho_in * dt);
+    }
+    // inputs: rho e p efps sigma(6) rod(6) spin(3) tr; sigma (3,1) is read as the upper 13
+    ub[0] = rhoin_b;
+    ub[1] = ein_b;
+    ub[2] = 0.0;   // the incoming pressure is overwritten by f3dm10
+    ub[3] = efps_b;
+    ub[4] = S_b[0];
+    ub[5] = S_b[4];
+    ub[6] = S_b[8];
+    ub[7] = S_b[1] + S_b[3];
+    ub[8] = S_b[2] + S_b[6];
+    ub[9] = S_b[5] + S_b[7];
+#pragma unroll
+    for (int u = 0; u < 6; ++u) ub[10 + u] = rod_b[u];
+    ub[19] = tr_b;
+    th[0] = gg_b;
+    th[1] = qs_b;
+    th[2] = qh_b;
+    th[3] = sl_b;
+}
+
+// REV: one hand-written reverse pass per particle (every material model 10
+// with EOS 41); otherwise kPasses dual-number passes.
+template <bool REV, int NT>
+__global__ void __launch_bounds__(NT) k_adj_constitutive(StepArgs a, AdjArgs b) {
+    __shared__ double sth[kParams][NT];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double th[kParams] = {0, 0, 0, 0};
     if (i < a.n) {
@@ -435,8 +849,12 @@ __global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) 
         for (int u = 0; u < kInputs; ++u) ub[u] = 0.0;
         const double yb[11] = {b.yrho[i], b.ye[i], b.yp[i], b.yefps[i], b.ysig[0][i], b.ysig[1][i],
                                b.ysig[2][i], b.ysig[3][i], b.ysig[4][i], b.ysig[5][i], b.yq[i]};
+        if constexpr (REV) {
+            reverse_m10_eos41(a, b, i, M0, yb, ub, th);
+        } else {
 #pragma unroll 1
-        for (int pass = 0; pass < kPasses; ++pass) constitutive_pass(pass, a, b, i, mat, M0, yb, ub, th);
+            for (int pass = 0; pass < kPasses; ++pass) constitutive_pass(pass, a, b, i, mat, M0, yb, ub, th);
+        }
         b.rhob[i] = ub[0] + b.rho0b[i];
         b.eb[i] = ub[1];
         b.pb[i] = ub[2];
@@ -455,7 +873,6 @@ __global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) 
         b.gb[7][i] = 0.5 * (rb[5] - wb[2]);  // G21
     }
     // parameter adjoints: block sums, one atomic per block and parameter
-    const int mat = i < a.n ? a.F.mat[i] : 0;
     for (int k = 0; k < kParams; ++k) sth[k][threadIdx.x] = th[k];
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -473,7 +890,6 @@ __global__ void __launch_bounds__(64) k_adj_constitutive(StepArgs a, AdjArgs b) 
                 for (int k = 0; k < kParams; ++k) atomicAdd(&b.theta_b[(m - 1) * kParams + k], s[k]);
         }
     }
-    (void)mat;
 }
 
 // ----------------------------------------------------------- strain rate
@@ -580,7 +996,8 @@ void launch_reverse_momentum(const StepArgs &a, const AdjArgs &b, cudaStream_t s
     k_adj_momentum<<<nblk(a.n, 128 / kLanes), 128, 0, s>>>(a, b);
 }
 void launch_reverse_constitutive(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
-    k_adj_constitutive<<<nblk(a.n, 64), 64, 0, s>>>(a, b);
+    if (b.rev) k_adj_constitutive<true, 128><<<nblk(a.n, 128), 128, 0, s>>>(a, b);
+    else k_adj_constitutive<false, 64><<<nblk(a.n, 64), 64, 0, s>>>(a, b);
 }
 void launch_reverse_strain(const StepArgs &a, const AdjArgs &b, cudaStream_t s) {
     const int gs = nblk(a.n, 256) < 148 * 8 ? nblk(a.n, 256) : 148 * 8;

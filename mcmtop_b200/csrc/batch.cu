@@ -248,11 +248,13 @@ int mcm_gpu_set_tuning(mcm_gpu_handle *h, const mcm_gpu_tuning *t) {
     if (t->pair_blocks_per_sm < 0 || t->pair_blocks_per_sm > 16 || t->nbr_stride < 0) return MCM_EINVAL;
     if (t->search_kind < 0 || t->search_kind > 3) return MCM_EINVAL;
     if (t->pair_kind < 0 || t->pair_kind > 2) return MCM_EINVAL;
+    if (t->adj_kind < 0 || t->adj_kind > 2) return MCM_EINVAL;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (t->search_threads) h->A.search_threads = t->search_threads;
     if (t->search_kind) h->A.search_kind = t->search_kind;
     if (t->pair_kind) h->A.pair_kind = t->pair_kind;
+    if (t->adj_kind) h->adj_kind = t->adj_kind;
     if (t->pair_threads) h->A.pair_threads = t->pair_threads;
     if (t->pair_blocks_per_sm) h->A.pair_bps = t->pair_blocks_per_sm;
     if (t->nbr_stride && t->nbr_stride != h->A.nstride) {
@@ -270,6 +272,7 @@ int mcm_gpu_get_tuning(mcm_gpu_handle *h, mcm_gpu_tuning *t) {
     t->nbr_stride = h->A.nstride;
     t->search_kind = search_kind_of(h);
     t->pair_kind = h->A.pair_kind == 2 ? 2 : 1;
+    t->adj_kind = h->adj_kind;
     t->ms_per_step = h->tuned_ms;
     return MCM_OK;
 }

@@ -45,6 +45,7 @@ struct mcm_gpu_handle {
     // adjoint: prescribed dt schedule, checkpoints (fields + bbox), segment snapshots
     std::vector<double> adj_dts;
     int adj_steps = 0, adj_every = 0;
+    int adj_kind = 1;   // reverse constitutive step: 1 hand-written reverse where the materials allow, 2 dual numbers
     std::vector<double *> adj_ckpt;
     double *adj_seg = nullptr;
     int adj_seg_cap = 0;

@@ -133,6 +133,7 @@ struct AdjArgs {
     double *theta_b;     // [nmat][kParams], accumulated
     double4 *rec;        // per cell-order position, kRecSlots double4: what the reverse gathers read of a neighbour
     double dt_prev, dt, dtold;   // dt of the strain/constitutive part, of the update, the one before
+    int rev;             // 1: every material is model 10 with EOS 41 (one reverse pass), 0: dual-number passes
 };
 constexpr int kRecSlots = 5;   // double4 slots per position in AdjArgs::rec
 // one reverse step = these three, in this order

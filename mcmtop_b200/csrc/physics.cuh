@@ -67,19 +67,16 @@ __device__ __forceinline__ void rhoupd(PState<T> &P, const Mat &M, T dt, int ndi
 }
 
 // --------------------------------------------------------- Jaumann rotation
-// MCM/mcm_stress_rot1.f90:35-199 (iorder = 3: the exponential map of :115-184)
+// The rotation of the exponential map, MCM/mcm_stress_rot1.f90:115-161
+// (iorder = 3), row-major: q[3 r + c] = Q(r+1, c+1).
 template <typename T>
-__device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
+__device__ __forceinline__ void jaumann_q(const T spin[3], T dt, T q[9]) {
     const T etol = T(1.0e-3f);
     const T z1 = T(1.0) / T(3.0), z2 = T(2.0) / T(15.0), z3 = T(17.0) / T(315.0), z4 = T(62.0) / T(2835.0);
-    const T s11 = P.sig[T11], s22 = P.sig[T22], s33 = P.sig[T33];
-    // the reference reads sigma(1,2), sigma(2,3) and sigma(3,1): the upper
-    // triangle except for (3,1) (MCM/mcm_stress_rot1.f90:40-48, 164-172)
-    const T s12 = P.sig[T12], s23 = P.sig[T23], s31 = P.sigl[1];
     T dt2 = T(0.5f) * dt;
-    T wzz = -dt2 * P.spin[0];
-    T wyy = dt2 * P.spin[1];
-    T wxx = -dt2 * P.spin[2];
+    T wzz = -dt2 * spin[0];
+    T wyy = dt2 * spin[1];
+    T wxx = -dt2 * spin[2];
     T wxx2 = wxx * wxx, wyy2 = wyy * wyy, wzz2 = wzz * wzz;
     T qm2 = wxx2 + wyy2 + wzz2;
     T qm = sqrt(qm2);
@@ -101,12 +98,27 @@ __device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
     T q23 = aa * wyy * wzz;
     T q21 = q12, q31 = q13, q32 = q23;
     T bwxx = bb * wxx, bwyy = bb * wyy, bwzz = bb * wzz;
-    q12 = q12 - bwzz;
-    q21 = q21 + bwzz;
-    q13 = q13 + bwyy;
-    q31 = q31 - bwyy;
-    q23 = q23 - bwxx;
-    q32 = q32 + bwxx;
+    q[1] = q12 - bwzz;
+    q[3] = q21 + bwzz;
+    q[2] = q13 + bwyy;
+    q[6] = q31 - bwyy;
+    q[5] = q23 - bwxx;
+    q[7] = q32 + bwxx;
+    q[0] = q11;
+    q[4] = q22;
+    q[8] = q33;
+}
+
+// MCM/mcm_stress_rot1.f90:35-199: sigma <- Q sigma Q^T
+template <typename T>
+__device__ __forceinline__ void stress_rot1(PState<T> &P, T dt) {
+    const T s11 = P.sig[T11], s22 = P.sig[T22], s33 = P.sig[T33];
+    // the reference reads sigma(1,2), sigma(2,3) and sigma(3,1): the upper
+    // triangle except for (3,1) (MCM/mcm_stress_rot1.f90:40-48, 164-172)
+    const T s12 = P.sig[T12], s23 = P.sig[T23], s31 = P.sigl[1];
+    T q[9];
+    jaumann_q(P.spin, dt, q);
+    const T q11 = q[0], q12 = q[1], q13 = q[2], q21 = q[3], q22 = q[4], q23 = q[5], q31 = q[6], q32 = q[7], q33 = q[8];
     T qs11 = q11 * s11 + q12 * s12 + q13 * s31;
     T qs12 = q11 * s12 + q12 * s22 + q13 * s23;
     T qs13 = q11 * s31 + q12 * s23 + q13 * s33;

@@ -323,10 +323,12 @@ class Solver:
         return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
 
     def set_tuning(self, search_threads: int = 0, pair_threads: int = 0, pair_blocks_per_sm: int = 0,
-                   nbr_stride: int = 0, search_kind: int = 0, pair_kind: int = 0) -> None:
+                   nbr_stride: int = 0, search_kind: int = 0, pair_kind: int = 0, adj_kind: int = 0) -> None:
         """search_kind 1: one thread per particle, 2: one warp per particle, 3: one warp per cell;
-        pair_kind (mixed gathers) 1: records through L1, 2: rows staged in shared memory."""
-        t = _abi.Tuning(search_threads, pair_threads, pair_blocks_per_sm, nbr_stride, search_kind, pair_kind, 0.0)
+        pair_kind (mixed gathers) 1: records through L1, 2: rows staged in shared memory;
+        adj_kind (reverse constitutive step) 1: hand-written reverse for model 10 + EOS 41, 2: dual numbers."""
+        t = _abi.Tuning(search_threads, pair_threads, pair_blocks_per_sm, nbr_stride, search_kind, pair_kind,
+                        adj_kind, 0.0)
         check(self.lib.mcm_gpu_set_tuning(self.h, C.byref(t)), "mcm_gpu_set_tuning", self.h)
 
     def autotune(self, nsteps: int = 5) -> dict:

@@ -50,6 +50,7 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", sizeof(mcm_gpu_material), sizeof(mcm_gpu_config), sizeof(mcm_gpu_fields), sizeof(mcm_gpu_time));
   printf("%zu %zu %zu %zu\n", offsetof(mcm_gpu_material, strinput), offsetof(mcm_gpu_config, boundary_x),
          offsetof(mcm_gpu_config, precision), offsetof(mcm_gpu_fields, mat));
+  printf("%zu %zu %zu\n", sizeof(mcm_gpu_tuning), offsetof(mcm_gpu_tuning, adj_kind), offsetof(mcm_gpu_tuning, ms_per_step));
   return 0;
 }
 '''
@@ -65,6 +66,8 @@ int main(void) {
     assert sizes == [C.sizeof(_abi.Material), C.sizeof(_abi.Config), C.sizeof(_abi.Fields), C.sizeof(_abi.Time)]
     assert offs == [_abi.Material.strinput.offset, _abi.Config.boundary_x.offset, _abi.Config.precision.offset,
                     _abi.Fields.mat.offset]
+    tun = [int(t) for t in lines[2].split()]
+    assert tun == [C.sizeof(_abi.Tuning), _abi.Tuning.adj_kind.offset, _abi.Tuning.ms_per_step.offset]
 
 
 def _lib_material(lib, card):

@@ -115,6 +115,29 @@ def test_adjoint_linear_functional_matches_fd(lib, dts):
     assert np.all(rel < 1e-3), (grad, ref, rel)
 
 
+def test_reverse_constitutive_matches_dual_passes(lib, dts):
+    """The hand-written reverse of the model-10 / EOS-41 update (adj_kind 1,
+    the default for this bar) and the forward-mode dual passes (adj_kind 2)
+    give the same gradients: parameters and initial-state adjoints to 1e-9
+    of their largest magnitude (the two differ only in rounding)."""
+    theta = nominal_theta()
+    rng = np.random.default_rng(5)
+    s, x, v = run(theta, V0, dts)
+    W = rng.standard_normal(x.shape)
+    U = rng.standard_normal(v.shape) * 1e2
+    assert s.tuning()["adj_kind"] == 1
+    pb1, x01, v01 = s.adjoint_backward(W, U)
+    s.set_tuning(adj_kind=2)
+    assert s.tuning()["adj_kind"] == 2
+    pb2, x02, v02 = s.adjoint_backward(W, U)
+    s.close()
+    for got, ref, name in ((pb1, pb2, "parameters"), (x01, x02, "x0"), (v01, v02, "v0")):
+        err = float(np.max(np.abs(got - ref))) / float(np.max(np.abs(ref)))
+        print(name, "reverse vs dual:", err)
+        assert err <= 1e-9, (name, err)
+    assert np.all(np.abs(pb1[0]) > 0)
+
+
 def test_adjoint_initial_state_gradient(lib, dts):
     """dL/dx of the initial state along one random direction against FD."""
     theta = nominal_theta()
