@@ -46,6 +46,10 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     p.contact = (c.contacttype > 0 && nmat > 1) ? 1 : 0;
     p.skin = c.nbr_skin > 0.0 ? c.nbr_skin : 0.0;
     p.kahan = (c.precision == MCM_PREC_MIXED && c.compensated_sums) ? 1 : 0;
+    // the sums of the FP64-fast and mixed steps do not follow the reference's
+    // neighbour order: their cells are kept in x order, which lets the search
+    // window each row of cells in x
+    p.xsort = c.precision != MCM_PREC_FP64_EXACT ? 1 : 0;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;

@@ -259,20 +259,29 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
 }
 
 // Per-cell order: descending reference index (head insertion in
-// MCM/mcm_setuplist.f90:126-130 over i = 1..np ascending).
+// MCM/mcm_setuplist.f90:126-130 over i = 1..np ascending), the order of the
+// reference's lists.  With xsort (steps whose sums do not follow that order)
+// ascending x, ties by descending reference index: a row of x-adjacent cells
+// is then one x-sorted range, which the search windows in x.
 __global__ void k_cell_sort(StepArgs a) {
     if (a.status->code) return;
     const long long ncells = a.grid->ncells;
+    const bool xs = a.prm.xsort != 0;
+    const double *X = a.F.f[FX];
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
          c += (long long)gridDim.x * blockDim.x) {
         int s = a.cell_start[c], e = a.cell_start[c + 1];
         if (e - s < 2) continue;
         for (int k = s + 1; k < e; ++k) {
-            int v = a.cell_list[k];
-            int ov = a.F.orig[v];
+            const int v = a.cell_list[k];
+            const int ov = a.F.orig[v];
+            const double xv = xs ? X[v] : 0.0;
             int m = k - 1;
-            while (m >= s && a.F.orig[a.cell_list[m]] < ov) {
-                a.cell_list[m + 1] = a.cell_list[m];
+            while (m >= s) {
+                const int u = a.cell_list[m];
+                const bool after = xs ? (X[u] > xv || (X[u] == xv && a.F.orig[u] < ov)) : a.F.orig[u] < ov;
+                if (!after) break;
+                a.cell_list[m + 1] = u;
                 --m;
             }
             a.cell_list[m + 1] = v;
@@ -513,13 +522,14 @@ __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
 // Variants of the search, fixed at compile time so that the candidate loop of
 // the common case (one material, no repulsive contact, no minimum distance)
 // tests none of these flags per candidate.
-enum { kSrchContact = 1, kSrchTwoPass = 2, kSrchMind = 4 };
+enum { kSrchContact = 1, kSrchTwoPass = 2, kSrchMind = 4, kSrchXWin = 8 };
 
 template <int V>
 __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     constexpr bool contact = (V & kSrchContact) != 0;   // contacttype > 0: other materials -> contact list
     constexpr bool two_pass = (V & kSrchTwoPass) != 0;  // kernel contact between materials: own material first
     constexpr bool want_mind = (V & kSrchMind) != 0;    // FP64 minimum distance (tcrit option 2, diagnostics)
+    constexpr bool xwin = (V & kSrchXWin) != 0;         // cells in x order: each row windowed in x
     if (a.status->code) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
@@ -575,11 +585,27 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     const int rb = (has_l && !(gyz + gxl * gxl > reach2)) ? a.cell_start[kc - 1] : s1;
                     const int re = (has_r && !(gyz + gxr * gxr > reach2)) ? a.cell_start[kc + 2] : s2;
                     const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
-                    for (int p = rb; p < re; ++p) {
+                    int pb = rb;
+                    float rxw = 0.0f;
+                    if (xwin) {
+                        // the row is x-sorted: candidates farther than rxw in x
+                        // are beyond reach (with a margin for FP32 rounding);
+                        // skip those on the left by bisection, stop at the right
+                        rxw = sqrtf(fmaxf(reach2 - gyz, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm;
+                        int hi = re;
+                        while (pb < hi) {
+                            const int mid = (pb + hi) >> 1;
+                            const float q = mid < s1 ? qxl : (mid < s2 ? ui.x : qxr);
+                            if (q - a.cposf[mid].x > rxw) pb = mid + 1;
+                            else hi = mid;
+                        }
+                    }
+                    for (int p = pb; p < re; ++p) {
                         const float4 c = a.cposf[p];
                         const bool left = p < s1, right = p >= s2;
                         const float qx = left ? qxl : (right ? qxr : ui.x);
                         const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                        if (xwin && dx < -rxw) break;
                         const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float hsf = ui.w + c.w;
                         const float r2f = hsf * hsf;
@@ -1351,13 +1377,24 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
         const int v = (a.prm.contact ? kSrchContact : 0) | ((a.nmat > 1 && a.prm.contacttype == 0) ? kSrchTwoPass : 0) |
                       (mind ? kSrchMind : 0);
         const unsigned nb = (unsigned)((a.n + threads - 1) / threads);
-        switch (v) {
-            case 0: k_search<0><<<nb, threads, 0, s>>>(a); break;
-            case kSrchContact: k_search<kSrchContact><<<nb, threads, 0, s>>>(a); break;
-            case kSrchTwoPass: k_search<kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
-            case kSrchMind: k_search<kSrchMind><<<nb, threads, 0, s>>>(a); break;
-            case kSrchContact | kSrchMind: k_search<kSrchContact | kSrchMind><<<nb, threads, 0, s>>>(a); break;
-            default: k_search<kSrchTwoPass | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+        if (a.prm.xsort) {
+            switch (v) {
+                case 0: k_search<kSrchXWin><<<nb, threads, 0, s>>>(a); break;
+                case kSrchContact: k_search<kSrchXWin | kSrchContact><<<nb, threads, 0, s>>>(a); break;
+                case kSrchTwoPass: k_search<kSrchXWin | kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
+                case kSrchMind: k_search<kSrchXWin | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+                case kSrchContact | kSrchMind: k_search<kSrchXWin | kSrchContact | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+                default: k_search<kSrchXWin | kSrchTwoPass | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+            }
+        } else {
+            switch (v) {
+                case 0: k_search<0><<<nb, threads, 0, s>>>(a); break;
+                case kSrchContact: k_search<kSrchContact><<<nb, threads, 0, s>>>(a); break;
+                case kSrchTwoPass: k_search<kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
+                case kSrchMind: k_search<kSrchMind><<<nb, threads, 0, s>>>(a); break;
+                case kSrchContact | kSrchMind: k_search<kSrchContact | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+                default: k_search<kSrchTwoPass | kSrchMind><<<nb, threads, 0, s>>>(a); break;
+            }
         }
     }
 }
