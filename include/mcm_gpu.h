@@ -303,7 +303,8 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
 typedef struct {
     int search_threads;      /* threads per block of the search: 64, 128 or 256 */
     int pair_threads;        /* threads per block of the gathers: 64, 128 or 256 */
-    int pair_blocks_per_sm;  /* blocks per SM the gathers' persistent grid is sized for: 1..16 */
+    int pair_blocks_per_sm;  /* blocks per SM the gathers' persistent grid is sized for: 1..16 (reported as
+                                0 while it is the blocks resident per SM, the default) */
     int nbr_stride;          /* neighbour-table row width in entries (rounded up to 4; still regrown
                                 when a list outgrows it) */
     int search_kind;         /* 1: one thread per particle (the default), 2: one warp per particle,

@@ -17,8 +17,30 @@
 
 #include "handle.h"
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 using namespace mcm;
 using namespace mcm_host;
+
+namespace mcm {
+int resident_per_sm(const void *kernel, int threads) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> known;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(kernel, threads);
+    auto it = known.find(key);
+    if (it != known.end()) return it->second;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    known[key] = nb;
+    return nb;
+}
+}  // namespace mcm
 
 namespace mcm_host {
 

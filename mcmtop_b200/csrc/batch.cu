@@ -268,7 +268,7 @@ int mcm_gpu_get_tuning(mcm_gpu_handle *h, mcm_gpu_tuning *t) {
     if (!h || !t) return MCM_EINVAL;
     t->search_threads = search_threads_of(h->A);
     t->pair_threads = pair_threads_of(h->A);
-    t->pair_blocks_per_sm = h->A.pair_bps > 0 ? h->A.pair_bps : 8;
+    t->pair_blocks_per_sm = h->A.pair_bps > 0 ? h->A.pair_bps : 0;
     t->nbr_stride = h->A.nstride;
     t->search_kind = search_kind_of(h);
     t->pair_kind = h->A.pair_kind == 2 ? 2 : 1;
@@ -287,7 +287,7 @@ int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best) {
     Saved saved;
     if ((st = save_body(h, saved))) { h->cfg.reorder_interval = every; return st; }
     cudaEvent_t e0 = take_event(h), e1 = take_event(h);
-    const Shape cur = {search_threads_of(h->A), pair_threads_of(h->A), h->A.pair_bps > 0 ? h->A.pair_bps : 8,
+    const Shape cur = {search_threads_of(h->A), pair_threads_of(h->A), h->A.pair_bps > 0 ? h->A.pair_bps : 0,
                        h->A.nstride, search_kind_of(h)};
     auto timed = [&](const Shape &s, double *ms) -> int {
         int r;
@@ -312,7 +312,7 @@ int mcm_gpu_autotune(mcm_gpu_handle *h, int nsteps, mcm_gpu_tuning *best) {
     double bestMs = 1e30;
     // stage 1: block sizes and grid of the search and the gathers
     const int blocks[3] = {64, 128, 256};
-    const int bpss[2] = {8, 16};
+    const int bpss[2] = {0, 8};   // 0: one wave of the resident blocks
     for (int sb : blocks)
         for (int pb : blocks)
             for (int g : bpss) {

@@ -84,7 +84,7 @@ struct StepArgs {
     int search_kind;      // 0 or 1: one thread per particle (k_search); 2: one warp per particle (k_search_warp);
                           // 3: one warp per cell (k_search_cell)
     int pair_threads;     // threads per block of the cooperative strain and momentum gathers
-    int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for
+    int pair_bps;         // blocks per SM the cooperative gathers' persistent grid is sized for (0: resident)
     int pair_kind;        // mixed gathers: 0 or 1 neighbour records through L1; 2 rows staged in shared memory
     double *energy;   // 5*nmat + 3
 };
@@ -173,15 +173,20 @@ void launch_pack(const StepArgs &a, const PackSpec &s, double *stage, cudaStream
 
 constexpr int kRedThreads = 256;
 
+// Blocks of `kernel` resident on one SM at `threads` per block (the
+// occupancy calculator's answer, kept per kernel and block size).
+int resident_per_sm(const void *kernel, int threads);
+
 // Launch shape of the cooperative gathers: per block, pair_threads / lanes
-// particles; the persistent grid covers every particle group once or
-// 148 * pair_bps blocks, whichever is fewer, and never more blocks than the
-// partials buffer holds.
+// particles; the persistent grid covers every particle group once or one
+// wave of 148 * pair_bps blocks (pair_bps 0: the blocks of `kernel` resident
+// per SM), whichever is fewer, and never more blocks than the partials
+// buffer holds.
 inline int pair_threads_of(const StepArgs &a) { return a.pair_threads > 0 ? a.pair_threads : 256; }
-inline int pair_blocks_of(const StepArgs &a, int lanes) {
+inline int pair_blocks_of(const StepArgs &a, int lanes, const void *kernel) {
     const int per = pair_threads_of(a) / lanes;
     int b = (a.n + per - 1) / per;
-    const int cap = 148 * (a.pair_bps > 0 ? a.pair_bps : 8);
+    const int cap = 148 * (a.pair_bps > 0 ? a.pair_bps : resident_per_sm(kernel, pair_threads_of(a)));
     if (b > cap) b = cap;
     if (a.red_blocks > 0 && b > a.red_blocks) b = a.red_blocks;
     return b < 1 ? 1 : b;

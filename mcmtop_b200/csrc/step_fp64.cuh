@@ -1025,9 +1025,8 @@ void launch_strain(const StepArgs &a, cudaStream_t s) {
     else k_strain<1><<<blocks, kRedThreads, 0, s>>>(a);
 #else
     constexpr int L = kCoopLanes;
-    const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
-    if (a.prm.disctype == 0) k_strain_coop<L, 0><<<blocks, threads, 0, s>>>(a);
-    else k_strain_coop<L, 1><<<blocks, threads, 0, s>>>(a);
+    void (*kern)(StepArgs) = a.prm.disctype == 0 ? k_strain_coop<L, 0> : k_strain_coop<L, 1>;
+    kern<<<pair_blocks_of(a, L, (const void *)kern), pair_threads_of(a), 0, s>>>(a);
 #endif
 }
 
@@ -1051,14 +1050,11 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate) {
     return blocks;
 #else
     constexpr int L = kCoopLanes;
-    const int blocks = pair_blocks_of(a, L), threads = pair_threads_of(a);
+    void (*kern)(StepArgs, int) = a.prm.disctype != 0 ? k_momentum_coop<L, 1, false>
+                                  : (a.prm.asym ? k_momentum_coop<L, 0, true> : k_momentum_coop<L, 0, false>);
+    const int blocks = pair_blocks_of(a, L, (const void *)kern);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
-    if (a.prm.disctype == 0) {
-        if (a.prm.asym) k_momentum_coop<L, 0, true><<<blocks, threads, 0, s>>>(a, integrate);
-        else k_momentum_coop<L, 0, false><<<blocks, threads, 0, s>>>(a, integrate);
-    } else {
-        k_momentum_coop<L, 1, false><<<blocks, threads, 0, s>>>(a, integrate);
-    }
+    kern<<<blocks, pair_threads_of(a), 0, s>>>(a, integrate);
     return blocks;
 #endif
 }

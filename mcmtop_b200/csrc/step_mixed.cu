@@ -163,6 +163,30 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 // ----------------------------------------------------------- strain rate
+// Neighbours a gather lane loads ahead before it uses the first.
+constexpr int kUnroll = 4;
+
+// One pair's terms of MCM/mcm_oldstrain.f90:42-53: V_j (v_j - v_i)_n dW/dx_m
+// added to gv[3n + m] (KAHAN: compensated, the low parts in gc).
+template <bool KAHAN>
+__device__ __forceinline__ void strain_term(float dx, float dy, float dz, float hj, float4 vj, float hi, float ihi,
+                                            float4 vi, float (&gv)[9], float (&gc)[9]) {
+    float d0, d1, d2;
+    gradw_f(dx, dy, dz, inv_havg_f(hi, hj, ihi), d0, d1, d2);
+    const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
+    if (KAHAN) {
+        const float tt[3] = {t0, t1, t2}, dd[3] = {d0, d1, d2};
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) kahan_add(gv[3 * n + m], gc[3 * n + m], tt[n] * dd[m]);
+    } else {
+        gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
+        gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
+        gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
+    }
+}
+
 // MCM/mcm_oldstrain.f90:34-64 with FP32 pair sums (KAHAN: compensated per
 // lane, the compensation carried into the TwoSum lane combination).
 template <bool KAHAN>
@@ -202,42 +226,36 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
         float gv[9], gc[9];
 #pragma unroll
         for (int u = 0; u < 9; ++u) { gv[u] = 0.0f; gc[u] = 0.0f; }
-        for (int k = lane; k < total; k += L) {
-            float dx, dy, dz, hj;
-            float4 vj;
-            if (k < nreal) {
-                const unsigned e = spos[k];
-                const float4 o = offs[e >> 26];
-                const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)(e & kPosMask));
-                const float4 xj = r.a;
-                vj = r.b;
-                dx = (xi.x - xj.x) - o.x;
-                dy = (xi.y - xj.y) - o.y;
-                dz = (xi.z - xj.z) - o.z;
-                hj = xj.w;
-            } else {
-                const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
-                const double4 xj = a.grec0[q];
-                vj = a.gfrec1[q];
-                dx = (float)(xs[0] - xj.x);
-                dy = (float)(xs[1] - xj.y);
-                dz = (float)(xs[2] - xj.z);
-                hj = (float)xj.w;
-            }
-            float d0, d1, d2;
-            gradw_f(dx, dy, dz, inv_havg_f(xi.w, hj, ihi), d0, d1, d2);
-            const float t0 = vj.w * (vj.x - vi.x), t1 = vj.w * (vj.y - vi.y), t2 = vj.w * (vj.z - vi.z);
-            if (KAHAN) {
-                const float tt[3] = {t0, t1, t2}, dd[3] = {d0, d1, d2};
+        // real neighbours kUnroll at a time per lane (their list entries and
+        // records loaded before any is used, so that several gathers are in
+        // flight), then the rest; each lane adds its terms in list order
+        int k = lane;
+        for (; k + (kUnroll - 1) * L < nreal; k += kUnroll * L) {
+            unsigned e[kUnroll];
 #pragma unroll
-                for (int n = 0; n < 3; ++n)
+            for (int u = 0; u < kUnroll; ++u) e[u] = spos[k + u * L];
+            Rec8 r[kUnroll];
 #pragma unroll
-                    for (int m = 0; m < 3; ++m) kahan_add(gv[3 * n + m], gc[3 * n + m], tt[n] * dd[m]);
-            } else {
-                gv[0] = fmaf(t0, d0, gv[0]); gv[1] = fmaf(t0, d1, gv[1]); gv[2] = fmaf(t0, d2, gv[2]);
-                gv[3] = fmaf(t1, d0, gv[3]); gv[4] = fmaf(t1, d1, gv[4]); gv[5] = fmaf(t1, d2, gv[5]);
-                gv[6] = fmaf(t2, d0, gv[6]); gv[7] = fmaf(t2, d1, gv[7]); gv[8] = fmaf(t2, d2, gv[8]);
+            for (int u = 0; u < kUnroll; ++u) r[u] = ld_rec8(a.frec0 + 2 * (size_t)(e[u] & kPosMask));
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                const float4 o = offs[e[u] >> 26];
+                strain_term<KAHAN>((xi.x - r[u].a.x) - o.x, (xi.y - r[u].a.y) - o.y, (xi.z - r[u].a.z) - o.z,
+                                   r[u].a.w, r[u].b, xi.w, ihi, vi, gv, gc);
             }
+        }
+        for (; k < nreal; k += L) {
+            const unsigned e = spos[k];
+            const float4 o = offs[e >> 26];
+            const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)(e & kPosMask));
+            strain_term<KAHAN>((xi.x - r.a.x) - o.x, (xi.y - r.a.y) - o.y, (xi.z - r.a.z) - o.z, r.a.w, r.b, xi.w,
+                               ihi, vi, gv, gc);
+        }
+        for (; k < total; k += L) {
+            const int q = a.gnbr[(size_t)(k - nreal) * a.npad + t];
+            const double4 xj = a.grec0[q];
+            strain_term<KAHAN>((float)(xs[0] - xj.x), (float)(xs[1] - xj.y), (float)(xs[2] - xj.z), (float)xj.w,
+                               a.gfrec1[q], xi.w, ihi, vi, gv, gc);
         }
         double r[9];
 #pragma unroll
@@ -563,8 +581,33 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // 1.70 against 2.19 ms per step on the 2M bar).
 // STAGED: 128-thread blocks whose rows of neighbour records are staged in
 // shared memory as in k_strain_staged (stage_rows); the same sums.
+constexpr int kUnrollM = 2;
+
+// One pair's term of MCM/mcm_oldacceleration.f90:62-90 for a symmetric sigma:
+// a(n) += m_j sum_m (A_j + A_i)(m, n) dW/dx_m, A = (sigma - q I)/rho^2 packed
+// as r1 = (11 22 33 12), r2 = (13 23 m_j -).
+template <bool KAHAN>
+__device__ __forceinline__ void momentum_term(float dx, float dy, float dz, float hj, float4 r1, float4 r2, float hi,
+                                              float ihi, float4 r1i, float4 r2i, float (&acc)[3], float (&comp)[3]) {
+    float d0, d1, d2;
+    gradw_f(dx, dy, dz, inv_havg_f(hi, hj, ihi), d0, d1, d2);
+    const float s11 = r1.x + r1i.x, s22 = r1.y + r1i.y, s33 = r1.z + r1i.z;
+    const float s12 = r1.w + r1i.w, s13 = r2.x + r2i.x, s23 = r2.y + r2i.y;
+    const float mj = r2.z;
+    d0 *= mj; d1 *= mj; d2 *= mj;
+    if (KAHAN) {
+        kahan_add(acc[0], comp[0], fmaf(s11, d0, fmaf(s12, d1, s13 * d2)));
+        kahan_add(acc[1], comp[1], fmaf(s12, d0, fmaf(s22, d1, s23 * d2)));
+        kahan_add(acc[2], comp[2], fmaf(s13, d0, fmaf(s23, d1, s33 * d2)));
+    } else {
+        acc[0] = fmaf(s11, d0, fmaf(s12, d1, fmaf(s13, d2, acc[0])));
+        acc[1] = fmaf(s12, d0, fmaf(s22, d1, fmaf(s23, d2, acc[1])));
+        acc[2] = fmaf(s13, d0, fmaf(s23, d1, fmaf(s33, d2, acc[2])));
+    }
+}
+
 template <bool ASYM, bool KAHAN, bool STAGED>
-__global__ void __launch_bounds__(STAGED ? kStageThreads : 256, 4) k_momentum(StepArgs a, int integrate_flag) {
+__global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : 3) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
     __shared__ float4 stage[STAGED ? 3 * kStageCapM : 1];
@@ -607,7 +650,30 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, 4) k_momentum(St
         const int total = live ? nreal + gn : 0;
         const float ihi = 1.0f / xi.w;
         float acc[3] = {0.0f, 0.0f, 0.0f}, comp[3] = {0.0f, 0.0f, 0.0f};
-        for (int k = lane; k < total; k += L) {
+        int k0 = lane;
+        if (!STAGED && !asym) {
+            // real neighbours kUnrollM at a time per lane, loads first (as in
+            // k_strain); the terms are added in list order
+            for (; k0 + (kUnrollM - 1) * L < nreal; k0 += kUnrollM * L) {
+                unsigned e[kUnrollM];
+#pragma unroll
+                for (int u = 0; u < kUnrollM; ++u) e[u] = spos[k0 + u * L];
+                Rec8 r[kUnrollM];
+                float4 q2[kUnrollM];
+#pragma unroll
+                for (int u = 0; u < kUnrollM; ++u) {
+                    r[u] = ld_rec8(a.frec0 + 4 * (size_t)(e[u] & kPosMask));
+                    q2[u] = ld_rec4(a.frec0 + 4 * (size_t)(e[u] & kPosMask) + 2);
+                }
+#pragma unroll
+                for (int u = 0; u < kUnrollM; ++u) {
+                    const float4 o = offs[e[u] >> 26];
+                    momentum_term<KAHAN>((xi.x - r[u].a.x) - o.x, (xi.y - r[u].a.y) - o.y, (xi.z - r[u].a.z) - o.z,
+                                         r[u].a.w, r[u].b, q2[u], xi.w, ihi, r1i, r2i, acc, comp);
+                }
+            }
+        }
+        for (int k = k0; k < total; k += L) {
             float dx, dy, dz, hj;
             float4 r1, r2, r3;
             if (k < nreal) {
@@ -740,8 +806,11 @@ void launch_strain(const StepArgs &a, cudaStream_t s) {
         k_strain_staged<<<b, kStageThreads, 0, s>>>(a);
         return;
     }
-    if (a.prm.kahan) k_strain<true><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
-    else k_strain<false><<<pair_blocks_of(a, L), pair_threads_of(a), 0, s>>>(a);
+    if (a.prm.kahan) {
+        k_strain<true><<<pair_blocks_of(a, L, (const void *)k_strain<true>), pair_threads_of(a), 0, s>>>(a);
+    } else {
+        k_strain<false><<<pair_blocks_of(a, L, (const void *)k_strain<false>), pair_threads_of(a), 0, s>>>(a);
+    }
 }
 
 void launch_mom_prep(const StepArgs &a, cudaStream_t s) {
@@ -760,16 +829,11 @@ int launch_momentum(const StepArgs &a, cudaStream_t s, int integrate_flag) {
         else k_momentum<false, false, true><<<blocks, kStageThreads, 0, s>>>(a, integrate_flag);
         return blocks;
     }
-    const int blocks = pair_blocks_of(a, L);
+    void (*kern)(StepArgs, int) = a.prm.asym ? (a.prm.kahan ? k_momentum<true, true, false> : k_momentum<true, false, false>)
+                                             : (a.prm.kahan ? k_momentum<false, true, false> : k_momentum<false, false, false>);
+    const int blocks = pair_blocks_of(a, L, (const void *)kern);
     if (a.nmat > 1) launch_energy_step_partials(a, s, blocks);
-    const int th = pair_threads_of(a);
-    if (a.prm.asym) {
-        if (a.prm.kahan) k_momentum<true, true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
-        else k_momentum<true, false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
-    } else {
-        if (a.prm.kahan) k_momentum<false, true, false><<<blocks, th, 0, s>>>(a, integrate_flag);
-        else k_momentum<false, false, false><<<blocks, th, 0, s>>>(a, integrate_flag);
-    }
+    kern<<<blocks, pair_threads_of(a), 0, s>>>(a, integrate_flag);
     return blocks;
 }
 

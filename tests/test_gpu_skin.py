@@ -14,7 +14,7 @@ from mcmtop_b200 import _abi
 from mcmtop_b200.deck import fluid_column, taylor_bar, two_material_bar
 from mcmtop_b200.solver import Solver
 from oracle.pyoracle import Oracle
-from test_gpu_parity import STATE, compare
+from test_gpu_parity import STATE, compare, compare_neighbours
 
 pytestmark = pytest.mark.gpu
 
@@ -22,13 +22,7 @@ SKIN = 0.3
 
 
 def same_sets(sol, orc, contacts=False):
-    nn, nbr, gn, gnbr = sol.neighbours()
-    assert np.array_equal(nn, orc.get_int("nnbr")), "neighbour counts differ"
-    assert np.array_equal(gn, orc.get_int("g_nnbr")), "ghost neighbour counts differ"
-    for i in range(sol.n):
-        assert np.array_equal(np.sort(nbr[i, : nn[i]]), np.sort(orc.nbrlist(i + 1))), f"particle {i + 1}"
-        if gn[i]:
-            assert np.array_equal(np.sort(gnbr[i, : gn[i]]), np.sort(orc.g_nbrlist(i + 1))), f"ghosts of {i + 1}"
+    compare_neighbours(sol, orc)   # sorted sets, ghosts by source and position
     if contacts:
         nc, cont, _, _ = sol.contacts()
         assert np.array_equal(nc, orc.get_int("ncont"))
