@@ -163,8 +163,18 @@ __global__ void k_strain_prep(StepArgs a) {
 }
 
 // ----------------------------------------------------------- strain rate
-// Neighbours a gather lane loads ahead before it uses the first.
-constexpr int kUnroll = 4;
+// Neighbours a gather lane loads ahead before it uses the first (strain,
+// momentum), and the momentum gather's resident blocks per SM.
+#ifndef MCM_STRAIN_UNROLL
+#define MCM_STRAIN_UNROLL 4
+#endif
+#ifndef MCM_MOM_UNROLL
+#define MCM_MOM_UNROLL 2
+#endif
+#ifndef MCM_MOM_MINBLOCKS
+#define MCM_MOM_MINBLOCKS 3
+#endif
+constexpr int kUnroll = MCM_STRAIN_UNROLL;
 
 // One pair's terms of MCM/mcm_oldstrain.f90:42-53: V_j (v_j - v_i)_n dW/dx_m
 // added to gv[3n + m] (KAHAN: compensated, the low parts in gc).
@@ -581,7 +591,7 @@ __device__ __forceinline__ void integrate(const StepArgs &a, int i, const double
 // 1.70 against 2.19 ms per step on the 2M bar).
 // STAGED: 128-thread blocks whose rows of neighbour records are staged in
 // shared memory as in k_strain_staged (stage_rows); the same sums.
-constexpr int kUnrollM = 2;
+constexpr int kUnrollM = MCM_MOM_UNROLL;
 
 // One pair's term of MCM/mcm_oldacceleration.f90:62-90 for a symmetric sigma:
 // a(n) += m_j sum_m (A_j + A_i)(m, n) dW/dx_m, A = (sigma - q I)/rho^2 packed
@@ -607,7 +617,7 @@ __device__ __forceinline__ void momentum_term(float dx, float dy, float dz, floa
 }
 
 template <bool ASYM, bool KAHAN, bool STAGED>
-__global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : 3) k_momentum(StepArgs a, int integrate_flag) {
+__global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM_MOM_MINBLOCKS) k_momentum(StepArgs a, int integrate_flag) {
     __shared__ double sm[32];
     __shared__ float4 offs[27];
     __shared__ float4 stage[STAGED ? 3 * kStageCapM : 1];
