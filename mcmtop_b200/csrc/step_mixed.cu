@@ -169,10 +169,10 @@ __global__ void k_strain_prep(StepArgs a) {
 #define MCM_STRAIN_UNROLL 4
 #endif
 #ifndef MCM_MOM_UNROLL
-#define MCM_MOM_UNROLL 2
+#define MCM_MOM_UNROLL 1
 #endif
 #ifndef MCM_MOM_MINBLOCKS
-#define MCM_MOM_MINBLOCKS 3
+#define MCM_MOM_MINBLOCKS 4
 #endif
 constexpr int kUnroll = MCM_STRAIN_UNROLL;
 
