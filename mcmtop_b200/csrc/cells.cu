@@ -263,28 +263,73 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
 // reference's lists.  With xsort (steps whose sums do not follow that order)
 // ascending x, ties by descending reference index: a row of x-adjacent cells
 // is then one x-sorted range, which the search windows in x.
-__global__ void k_cell_sort(StepArgs a) {
+// One warp per cell: each lane takes up to kSortPer of the cell's particles
+// and counts how many of the cell's particles come before each (a rank sort:
+// the order is total, so the ranks are a permutation); all ranks are known
+// before any entry is written back.  Cells of more than 32 * kSortPer
+// particles are sorted by insertion in one lane.
+constexpr int kSortPer = 4;
+__device__ __forceinline__ bool cell_before(bool xs, double xa, int oa, double xb, int ob) {
+    return xs ? (xa < xb || (xa == xb && oa > ob)) : oa > ob;
+}
+__global__ void __launch_bounds__(256) k_cell_sort(StepArgs a) {
     if (a.status->code) return;
     const long long ncells = a.grid->ncells;
     const bool xs = a.prm.xsort != 0;
     const double *X = a.F.f[FX];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
-         c += (long long)gridDim.x * blockDim.x) {
-        int s = a.cell_start[c], e = a.cell_start[c + 1];
-        if (e - s < 2) continue;
-        for (int k = s + 1; k < e; ++k) {
-            const int v = a.cell_list[k];
-            const int ov = a.F.orig[v];
-            const double xv = xs ? X[v] : 0.0;
-            int m = k - 1;
-            while (m >= s) {
-                const int u = a.cell_list[m];
-                const bool after = xs ? (X[u] > xv || (X[u] == xv && a.F.orig[u] < ov)) : a.F.orig[u] < ov;
-                if (!after) break;
-                a.cell_list[m + 1] = u;
-                --m;
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += nw) {
+        const int s = a.cell_start[c], e = a.cell_start[c + 1];
+        const int n = e - s;
+        if (n < 2) continue;   // warp-uniform
+        if (n <= 32 * kSortPer) {
+            int v[kSortPer], o[kSortPer], rank[kSortPer];
+            double x[kSortPer];
+#pragma unroll
+            for (int u = 0; u < kSortPer; ++u) {
+                const int j = lane + 32 * u;
+                v[u] = j < n ? a.cell_list[s + j] : 0;
+                o[u] = j < n ? a.F.orig[v[u]] : 0;
+                x[u] = (j < n && xs) ? X[v[u]] : 0.0;
+                rank[u] = 0;
             }
-            a.cell_list[m + 1] = v;
+            for (int k0 = 0; k0 < n; k0 += 32) {
+                // the chunk's keys, one per lane, broadcast by shuffles
+                const int uk = k0 >> 5;
+                double xk = 0.0;
+                int ok = 0;
+#pragma unroll
+                for (int u = 0; u < kSortPer; ++u)
+                    if (u == uk) { xk = x[u]; ok = o[u]; }
+                const int m = n - k0 < 32 ? n - k0 : 32;
+                for (int k = 0; k < m; ++k) {
+                    const double xb = __shfl_sync(0xffffffffu, xk, k);
+                    const int ob = __shfl_sync(0xffffffffu, ok, k);
+#pragma unroll
+                    for (int u = 0; u < kSortPer; ++u)
+                        if (lane + 32 * u < n && cell_before(xs, xb, ob, x[u], o[u])) ++rank[u];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < kSortPer; ++u)
+                if (lane + 32 * u < n) a.cell_list[s + rank[u]] = v[u];
+            __syncwarp();
+        } else if (lane == 0) {
+            for (int k = s + 1; k < e; ++k) {
+                const int v = a.cell_list[k];
+                const int ov = a.F.orig[v];
+                const double xv = xs ? X[v] : 0.0;
+                int m = k - 1;
+                while (m >= s) {
+                    const int u = a.cell_list[m];
+                    if (!cell_before(xs, xv, ov, xs ? X[u] : 0.0, a.F.orig[u])) break;
+                    a.cell_list[m + 1] = u;
+                    --m;
+                }
+                a.cell_list[m + 1] = v;
+            }
         }
     }
 }
@@ -303,7 +348,11 @@ void launch_cell_build(const StepArgs &a, cudaStream_t s) {
     k_cell_keys<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
     device_exclusive_scan(a.cell_count, a.cell_start, a.scan_sums, &a.grid->ncells, a.cell_cap, s);
     k_cell_scatter<<<grid_blocks(a.n, 256), 256, 0, s>>>(a);
-    k_cell_sort<<<grid_blocks(a.cell_cap, 128), 128, 0, s>>>(a);
+    {
+        long long b = (a.cell_cap + 7) / 8;   // 8 warps (cells) per block
+        if (b > 148LL * 8) b = 148LL * 8;
+        k_cell_sort<<<(unsigned)(b < 1 ? 1 : b), 256, 0, s>>>(a);
+    }
     k_cell_records<<<grid_blocks(a.n, 256) < 148 * 8 ? grid_blocks(a.n, 256) : 148 * 8, 256, 0, s>>>(a);
 }
 
