@@ -634,13 +634,12 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     const int rb = (has_l && !(gyz + gxl * gxl > reach2)) ? a.cell_start[kc - 1] : s1;
                     const int re = (has_r && !(gyz + gxr * gxr > reach2)) ? a.cell_start[kc + 2] : s2;
                     const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
-                    int pb = rb;
-                    float rxw = 0.0f;
+                    int pb = rb, pe = re;
                     if (xwin) {
                         // the row is x-sorted: candidates farther than rxw in x
                         // are beyond reach (with a margin for FP32 rounding);
-                        // skip those on the left by bisection, stop at the right
-                        rxw = sqrtf(fmaxf(reach2 - gyz, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm;
+                        // the window's ends by bisection
+                        const float rxw = sqrtf(fmaxf(reach2 - gyz, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm;
                         int hi = re;
                         while (pb < hi) {
                             const int mid = (pb + hi) >> 1;
@@ -648,13 +647,43 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                             if (q - a.cposf[mid].x > rxw) pb = mid + 1;
                             else hi = mid;
                         }
+                        int lo = pb;
+                        while (lo < pe) {
+                            const int mid = (lo + pe) >> 1;
+                            const float q = mid < s1 ? qxl : (mid < s2 ? ui.x : qxr);
+                            if (q - a.cposf[mid].x < -rxw) pe = mid;
+                            else lo = mid + 1;
+                        }
                     }
-                    for (int p = pb; p < re; ++p) {
+                    if constexpr (!contact && !two_pass && !want_mind) {
+                        // one material, no minimum distance: the accept path is
+                        // a predicated store, so the lanes stay converged
+                        for (int p = pb; p < pe; ++p) {
+                            const float4 c = a.cposf[p];
+                            const bool left = p < s1, right = p >= s2;
+                            const float qx = left ? qxl : (right ? qxr : ui.x);
+                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                            const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float hsf = ui.w + c.w;
+                            const float r2f = hsf * hsf;
+                            bool in = d2f < fmaf(r2f, khi, kb) && p != t;
+                            if (in && d2f > fmaf(r2f, klo, -kb)) {
+                                // near tie: the reference's FP64 test
+                                const double4 cd = a.cpos[p];
+                                const double hs = __dadd_rn(cd.w, xi.w);
+                                in = exact_d2(xi, cd) < __dmul_rn(hs, hs);
+                            }
+                            const unsigned code = (code_yz + (left ? 0u : (right ? 2u : 1u))) << 26;
+                            if (in && nn < cap) out[nn] = (unsigned)p | code;
+                            nn += in ? 1 : 0;
+                        }
+                        continue;
+                    }
+                    for (int p = pb; p < pe; ++p) {
                         const float4 c = a.cposf[p];
                         const bool left = p < s1, right = p >= s2;
                         const float qx = left ? qxl : (right ? qxr : ui.x);
                         const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
-                        if (xwin && dx < -rxw) break;
                         const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float hsf = ui.w + c.w;
                         const float r2f = hsf * hsf;

@@ -1035,7 +1035,16 @@ __device__ __forceinline__ int constitutive_particle(PState<T> &P, const Mat &M,
             break;
         case 4:
             if constexpr (std::is_same<T, double>::value) {
-                stress_rot1(P, dt); code = f3dm25(P, M, dt); aviscosity(P, M); lieupd(P, dt);
+                stress_rot1(P, dt);
+                {
+                    // f3dm25 is an out-of-line call: it gets a copy, so that
+                    // the caller's state is not address-taken (which would
+                    // keep it in local memory for every model)
+                    PState<double> Pc = P;
+                    code = f3dm25(Pc, M, dt);
+                    P = Pc;
+                }
+                aviscosity(P, M); lieupd(P, dt);
             }
             break;
         case 9:
