@@ -344,8 +344,11 @@ __device__ __forceinline__ void update_h(const StepArgs &a, int i, PState<double
 // MCM/mcm_rhoupd.f90, mcm_constitutive.f90:29-83 and mcm_calccritts.f90 for
 // the particle with state index i, and the forward half-step shift of
 // MCM/mcm_strain.f90:56-60 (x - v dt/2 recomputed exactly as k_strain_prep).
+// Two resident blocks per SM (128 registers, a few hundred bytes of spills)
+// measured faster than one at 154 registers: 0.27 against 0.43 ms per step
+// on the 2M bar.
 #ifndef MCM_CONST_MINBLOCKS
-#define MCM_CONST_MINBLOCKS 1
+#define MCM_CONST_MINBLOCKS 2
 #endif
 __global__ void __launch_bounds__(kRedThreads, MCM_CONST_MINBLOCKS) k_constitutive(StepArgs a) {
     __shared__ double sm[32];
