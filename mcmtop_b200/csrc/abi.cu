@@ -149,8 +149,9 @@ int alloc_particles(mcm_gpu_handle *h) {
     h->A.red_blocks = h->red_cap;
     if ((st = dalloc(h, &h->A.red, (size_t)h->red_cap * (5 * h->nmat + 6)))) return st;
     if (h->cfg.precision == MCM_PREC_MIXED) {
-        // one 64-byte slot per particle: strain records use the first 32 bytes
-        // of a 2-float4 stride, momentum records 48 bytes of a 4-float4 stride
+        // 64 bytes per particle: strain records are 32 bytes at a 2-float4
+        // stride; momentum records 32 bytes there plus 16 in the third
+        // quarter of the buffer (and the cap model's 16 in the fourth)
         if ((st = dalloc(h, &h->A.frec0, 4 * np))) return st;
     }
     return MCM_OK;

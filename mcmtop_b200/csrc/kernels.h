@@ -74,7 +74,7 @@ struct StepArgs {
     double4 *rec0, *rec1, *rec2;   // per particle
     double4 *grec0, *grec1, *grec2;  // per ghost
     double4 *rec3, *grec3;           // prm.asym: the lower triangle of (sigma - q)/rho^2 (21 31 32)
-    float4 *frec0;                   // mixed path: 64 bytes per particle (strain or momentum record)
+    float4 *frec0;                   // mixed path: 4 npad float4 (strain or momentum records)
     float4 *gfrec1, *gfrec2;         // mixed path, per ghost
     // reductions
     double *red;      // block partials

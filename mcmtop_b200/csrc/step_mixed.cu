@@ -311,11 +311,12 @@ struct StageWin {
 };
 
 // Computes the windows of the positions [tb, tb + per) and copies the records
-// (NF float4 each, record p at src + stride * p) of those that fit in `cap`
-// records into stage.  Every thread of the block calls it; it synchronises.
+// (NF float4 each: record p's first two at src + 2p, a third at src2 + p) of
+// those that fit in `cap` records into stage.  Every thread of the block calls
+// it; it synchronises.
 template <int NF>
 __device__ __forceinline__ void stage_rows(const StepArgs &a, int tb, int per, StageWin &W, float4 *stage, int cap,
-                                           const float4 *src, int stride) {
+                                           const float4 *src, const float4 *src2) {
     const int gl0 = a.grid->gridlim[0], gl1 = a.grid->gridlim[1], gl2 = a.grid->gridlim[2];
     if (threadIdx.x < 18) {
         const int w = threadIdx.x;
@@ -360,7 +361,8 @@ __device__ __forceinline__ void stage_rows(const StepArgs &a, int tb, int per, S
         const int lo = W.lo[w], len = W.len[w], o = W.off[w];
         for (int u = threadIdx.x; u < len; u += blockDim.x)
 #pragma unroll
-            for (int c = 0; c < NF; ++c) stage[NF * (o + u) + c] = src[(size_t)stride * (lo + u) + c];
+            for (int c = 0; c < NF; ++c)
+                stage[NF * (o + u) + c] = c < 2 ? src[2 * (size_t)(lo + u) + c] : src2[lo + u];
     }
     __syncthreads();
 }
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) 
     const double dt = a.time->dt;
     for (int round = 0; round < rounds; ++round) {
         const int tb = (round * gridDim.x + blockIdx.x) * per;
-        stage_rows<2>(a, tb, per, W, stage, kStageCap, a.frec0, 2);
+        stage_rows<2>(a, tb, per, W, stage, kStageCap, a.frec0, nullptr);
         const int t = tb + sub;
         const bool live = t < a.n;
         int nreal = 0, gn = 0, i = 0, wbase = 0;
@@ -475,6 +477,14 @@ __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) 
     }
 }
 
+// Momentum records in three arrays of the 64-byte-per-position buffer:
+// position p's first 32 bytes at frec0 + 2p (x y z h, A11 A22 A33 A12), the
+// next 16 at frec0 + 2 npad + p (A13 A23 m rho) and the cap model's lower
+// triangle at frec0 + 3 npad + p, so that neighbouring positions' records lie
+// next to each other in every array.
+__device__ __forceinline__ float4 *mom_tail(const StepArgs &a) { return a.frec0 + 2 * (size_t)a.npad; }
+__device__ __forceinline__ float4 *mom_lower(const StepArgs &a) { return a.frec0 + 3 * (size_t)a.npad; }
+
 // --------------------------------------------------------- momentum prep
 // Records: cell-relative x, h; (sigma - q)/rho^2 (formed in FP64,
 // MCM/mcm_oldacceleration.f90:79-80) and m (FP32).  Ghosts: FP64 positions,
@@ -491,15 +501,16 @@ __global__ void k_mom_prep(StepArgs a) {
         const double rho = f[FRHO][i];
         const double ir2 = 1.0 / (rho * rho);
         const double q = f[FQ][i];
-        float4 *rec = a.frec0 + 4 * (size_t)p;
+        float4 *rec = a.frec0 + 2 * (size_t)p;
         rec[0] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]),
                              (float)f[FH][i]);
         rec[1] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
                                  (float)((f[FS33][i] - q) * ir2), (float)(f[FS12][i] * ir2));
-        rec[2] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
+        mom_tail(a)[p] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
         // the cap model's lower triangle (21 31 32), read only when a material has it
         if (a.prm.asym)
-            rec[3] = make_float4((float)(f[FL21][i] * ir2), (float)(f[FL31][i] * ir2), (float)(f[FL32][i] * ir2), 0.0f);
+            mom_lower(a)[p] =
+                make_float4((float)(f[FL21][i] * ir2), (float)(f[FL31][i] * ir2), (float)(f[FL32][i] * ir2), 0.0f);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
@@ -637,7 +648,7 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM
     const bool do_int = integrate_flag && !a.time->ended;
     for (int round = 0; round < rounds; ++round) {
         const int tb = (round * gridDim.x + blockIdx.x) * per;
-        if (STAGED) stage_rows<3>(a, tb, per, W, stage, kStageCapM, a.frec0, 4);
+        if (STAGED) stage_rows<3>(a, tb, per, W, stage, kStageCapM, a.frec0, a.frec0 + 2 * (size_t)a.npad);
         const int t = tb + sub;
         const bool live = t < a.n;
         int nreal = 0, gn = 0, i = 0, wbase = 0;
@@ -647,11 +658,11 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM
             if (STAGED) wbase = stage_base(a, W, t);
             nreal = a.nnbr[t];
             gn = a.gnnbr[t];
-            const Rec8 r = ld_rec8(a.frec0 + 4 * (size_t)t);
+            const Rec8 r = ld_rec8(a.frec0 + 2 * (size_t)t);
             xi = r.a;
             r1i = r.b;
-            r2i = ld_rec4(a.frec0 + 4 * (size_t)t + 2);
-            if (asym) r3i = ld_rec4(a.frec0 + 4 * (size_t)t + 3);
+            r2i = ld_rec4(mom_tail(a) + t);
+            if (asym) r3i = ld_rec4(mom_lower(a) + t);
             i = a.cell_list[t];
         }
         const unsigned *spos = a.nidx + (size_t)t * a.nstride;
@@ -672,8 +683,8 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM
                 float4 q2[kUnrollM];
 #pragma unroll
                 for (int u = 0; u < kUnrollM; ++u) {
-                    r[u] = ld_rec8(a.frec0 + 4 * (size_t)(e[u] & kPosMask));
-                    q2[u] = ld_rec4(a.frec0 + 4 * (size_t)(e[u] & kPosMask) + 2);
+                    r[u] = ld_rec8(a.frec0 + 2 * (size_t)(e[u] & kPosMask));
+                    q2[u] = ld_rec4(mom_tail(a) + (e[u] & kPosMask));
                 }
 #pragma unroll
                 for (int u = 0; u < kUnrollM; ++u) {
@@ -697,12 +708,12 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM
                     r1 = stage[3 * si + 1];
                     r2 = stage[3 * si + 2];
                 } else {
-                    const Rec8 r = ld_rec8(a.frec0 + 4 * p);
+                    const Rec8 r = ld_rec8(a.frec0 + 2 * p);
                     xj = r.a;
                     r1 = r.b;
-                    r2 = ld_rec4(a.frec0 + 4 * p + 2);
+                    r2 = ld_rec4(mom_tail(a) + p);
                 }
-                if (asym) r3 = ld_rec4(a.frec0 + 4 * p + 3);
+                if (asym) r3 = ld_rec4(mom_lower(a) + p);
                 dx = (xi.x - xj.x) - o.x;
                 dy = (xi.y - xj.y) - o.y;
                 dz = (xi.z - xj.z) - o.z;
