@@ -790,16 +790,18 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     search_one<V>(a, t);
 }
 
-// The common case of the x-ordered steps (windowed rows, one material, no
-// minimum distance) with two particles per thread: positions 2u and 2u + 1,
-// when they share a cell, walk the same rows, and each candidate of the union
-// of their two windows is loaded once and tested for both.  Each particle's
+// The common case (one material, no minimum distance) with two particles per
+// thread: positions 2u and 2u + 1, when they share a cell, walk the same
+// rows, and each candidate of the union of their two ranges (XWIN: their two
+// x windows, in the x-ordered cells of the FP64-fast and mixed steps) is
+// loaded once and tested for both.  Each particle's
 // list is the one search_one builds (its candidates in position order within
 // each row; a candidate outside a particle's own window or reach fails its
 // FP32 test).  Pairs across a cell boundary, and the ghosts, counts and
 // overflow checks, go through search_one.
+template <bool XWIN>
 __global__ void __launch_bounds__(256, 3) k_search_pair(StepArgs a) {
-    constexpr int V = kSrchXWin;
+    constexpr int V = XWIN ? kSrchXWin : 0;
     if (a.status->code) return;
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int t0 = 2 * u, t1 = t0 + 1;
@@ -854,7 +856,7 @@ __global__ void __launch_bounds__(256, 3) k_search_pair(StepArgs a) {
                 const float wa = rowa ? sqrtf(fmaxf(reach2a - gyza, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm : -1.0e30f;
                 const float wb = rowb ? sqrtf(fmaxf(reach2b - gyzb, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm : -1.0e30f;
                 int hi = pe;
-                while (pb < hi) {   // first candidate inside either window on the left
+                while (XWIN && pb < hi) {   // first candidate inside either window on the left
                     const int mid = (pb + hi) >> 1;
                     const float cx = a.cposf[mid].x;
                     const bool l = mid < s1, r = mid >= s2;
@@ -863,7 +865,7 @@ __global__ void __launch_bounds__(256, 3) k_search_pair(StepArgs a) {
                     else hi = mid;
                 }
                 int lo = pb;
-                while (lo < pe) {   // first candidate beyond both windows on the right
+                while (XWIN && lo < pe) {   // first candidate beyond both windows on the right
                     const int mid = (lo + pe) >> 1;
                     const float cx = a.cposf[mid].x;
                     const bool l = mid < s1, r = mid >= s2;
@@ -1593,7 +1595,7 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
             switch (v) {
                 case 0: {
                     const long long pairs = (a.n + 1) / 2;
-                    k_search_pair<<<(unsigned)((pairs + threads - 1) / threads), threads, 0, s>>>(a);
+                    k_search_pair<true><<<(unsigned)((pairs + threads - 1) / threads), threads, 0, s>>>(a);
                     break;
                 }
                 case kSrchContact: k_search<kSrchXWin | kSrchContact><<<nb, threads, 0, s>>>(a); break;
@@ -1604,7 +1606,13 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
             }
         } else {
             switch (v) {
-                case 0: k_search<0><<<nb, threads, 0, s>>>(a); break;
+                case 0:
+#ifdef MCM_EXACT_SEARCH_PAIR
+                    k_search_pair<false><<<(unsigned)(((a.n + 1) / 2 + threads - 1) / threads), threads, 0, s>>>(a);
+#else
+                    k_search<0><<<nb, threads, 0, s>>>(a);
+#endif
+                    break;
                 case kSrchContact: k_search<kSrchContact><<<nb, threads, 0, s>>>(a); break;
                 case kSrchTwoPass: k_search<kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
                 case kSrchMind: k_search<kSrchMind><<<nb, threads, 0, s>>>(a); break;
