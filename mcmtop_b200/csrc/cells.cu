@@ -571,23 +571,23 @@ __device__ __forceinline__ double exact_d2(double4 a, double4 b) {
 // Variants of the search, fixed at compile time so that the candidate loop of
 // the common case (one material, no repulsive contact, no minimum distance)
 // tests none of these flags per candidate.
-// kSrchNoReal: the real neighbours are already in the row (nn of them); only
-// the ghosts, the overflow checks and the counts remain.
-enum { kSrchContact = 1, kSrchTwoPass = 2, kSrchMind = 4, kSrchXWin = 8, kSrchNoReal = 16 };
+enum { kSrchContact = 1, kSrchTwoPass = 2, kSrchMind = 4, kSrchXWin = 8 };
 
 template <int V>
-__device__ __forceinline__ void search_one(const StepArgs &a, int t, int nn_real = 0) {
+__global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
     constexpr bool contact = (V & kSrchContact) != 0;   // contacttype > 0: other materials -> contact list
     constexpr bool two_pass = (V & kSrchTwoPass) != 0;  // kernel contact between materials: own material first
     constexpr bool want_mind = (V & kSrchMind) != 0;    // FP64 minimum distance (tcrit option 2, diagnostics)
     constexpr bool xwin = (V & kSrchXWin) != 0;         // cells in x order: each row windowed in x
-    constexpr bool no_real = (V & kSrchNoReal) != 0;
+    if (a.status->code) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
     const int np = a.npad;
     const int cap = a.nstride;
     const int key = a.ckey[t];
     const int i = a.cell_list[t];
     const bool with_self = (a.prm.disctype == 1);
-    int nn = nn_real, gn = 0, nc = 0, gcn = 0;
+    int nn = 0, gn = 0, nc = 0, gcn = 0;
     double mind = 1.0e20;
     if (key >= 0) {
         const DevGrid g = *a.grid;
@@ -617,7 +617,7 @@ __device__ __forceinline__ void search_one(const StepArgs &a, int t, int nn_real
         // each list in walk order)
         unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
 #pragma unroll 1
-        for (int pass = 0; pass < (no_real ? 0 : (two_pass ? 2 : 1)); ++pass) {
+        for (int pass = 0; pass < (two_pass ? 2 : 1); ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
                 const float qz = ui.z + (float)(bz - nz) * cs[2];
                 const float gz = fmaxf(nz < bz ? ui.z : (nz > bz ? cs[2] - ui.z : 0.0f), 0.0f);
@@ -780,139 +780,6 @@ __device__ __forceinline__ void search_one(const StepArgs &a, int t, int nn_real
     if (want_mind) a.F.f[FMINDIST][i] = mind;
     atomicMax(&a.status->max_nbr, nn);
     atomicMax(&a.status->max_gnbr, gn);
-}
-
-template <int V>
-__global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
-    if (a.status->code) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
-    search_one<V>(a, t);
-}
-
-// The common case (one material, no minimum distance) with two particles per
-// thread: positions 2u and 2u + 1, when they share a cell, walk the same
-// rows, and each candidate of the union of their two ranges (XWIN: their two
-// x windows, in the x-ordered cells of the FP64-fast and mixed steps) is
-// loaded once and tested for both.  Each particle's
-// list is the one search_one builds (its candidates in position order within
-// each row; a candidate outside a particle's own window or reach fails its
-// FP32 test).  Pairs across a cell boundary, and the ghosts, counts and
-// overflow checks, go through search_one.
-template <bool XWIN>
-__global__ void __launch_bounds__(256, 3) k_search_pair(StepArgs a) {
-    constexpr int V = XWIN ? kSrchXWin : 0;
-    if (a.status->code) return;
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t0 = 2 * u, t1 = t0 + 1;
-    if (t0 >= a.n) return;
-    const int key = a.ckey[t0];
-    if (!(t1 < a.n && key >= 0 && a.ckey[t1] == key)) {
-        search_one<V>(a, t0);
-        if (t1 < a.n) search_one<V>(a, t1);
-        return;
-    }
-    const int cap = a.nstride;
-    int n0 = 0, n1 = 0;
-    {
-        const DevGrid g = *a.grid;
-        int bx, by, bz;
-        cell_coords(key, g.gridlim, bx, by, bz);
-        const int lo1 = by > 1 ? by - 1 : 1, hi1 = by < g.gridlim[1] ? by + 1 : g.gridlim[1];
-        const int lo2 = bz > 1 ? bz - 1 : 1, hi2 = bz < g.gridlim[2] ? bz + 1 : g.gridlim[2];
-        const bool has_l = bx > 1, has_r = bx < g.gridlim[0];
-        const double4 xa = a.cpos[t0], xb = a.cpos[t1];
-        const float4 ua = a.cposf[t0], ub = a.cposf[t1];
-        const float cs[3] = {(float)(1.0 / g.gridsize[0]), (float)(1.0 / g.gridsize[1]), (float)(1.0 / g.gridsize[2])};
-        const float csm = fmaxf(cs[0], fmaxf(cs[1], cs[2]));
-        const float kb = 2.44140625e-4f * csm * csm;
-        const float khi = 1.0f + 2.44140625e-4f, klo = 1.0f - 2.44140625e-4f;
-        const float ra = ua.w + (float)g.hcut, rb = ub.w + (float)g.hcut;
-        const float reach2a = ra * ra * 1.0009765625f + 9.765625e-4f * csm * csm;
-        const float reach2b = rb * rb * 1.0009765625f + 9.765625e-4f * csm * csm;
-        const float qxla = ua.x + cs[0], qxra = ua.x - cs[0], qxlb = ub.x + cs[0], qxrb = ub.x - cs[0];
-        const float gxla = fmaxf(ua.x, 0.0f), gxra = fmaxf(cs[0] - ua.x, 0.0f);
-        const float gxlb = fmaxf(ub.x, 0.0f), gxrb = fmaxf(cs[0] - ub.x, 0.0f);
-        unsigned *out0 = a.nidx + (size_t)t0 * cap, *out1 = a.nidx + (size_t)t1 * cap;
-        for (int nz = lo2; nz <= hi2; ++nz) {
-            const float qza = ua.z + (float)(bz - nz) * cs[2], qzb = ub.z + (float)(bz - nz) * cs[2];
-            const float gza = fmaxf(nz < bz ? ua.z : (nz > bz ? cs[2] - ua.z : 0.0f), 0.0f);
-            const float gzb = fmaxf(nz < bz ? ub.z : (nz > bz ? cs[2] - ub.z : 0.0f), 0.0f);
-            for (int my = lo1; my <= hi1; ++my) {
-                const float qya = ua.y + (float)(by - my) * cs[1], qyb = ub.y + (float)(by - my) * cs[1];
-                const float gya = fmaxf(my < by ? ua.y : (my > by ? cs[1] - ua.y : 0.0f), 0.0f);
-                const float gyb = fmaxf(my < by ? ub.y : (my > by ? cs[1] - ub.y : 0.0f), 0.0f);
-                const float gyza = gya * gya + gza * gza, gyzb = gyb * gyb + gzb * gzb;
-                const bool rowa = !(gyza > reach2a), rowb = !(gyzb > reach2b);
-                if (!rowa && !rowb) continue;
-                const int kc = (int)cell_key(bx, my, nz, g.gridlim);
-                const int s1 = a.cell_start[kc], s2 = a.cell_start[kc + 1];
-                const bool inl = has_l && ((rowa && !(gyza + gxla * gxla > reach2a)) || (rowb && !(gyzb + gxlb * gxlb > reach2b)));
-                const bool inr = has_r && ((rowa && !(gyza + gxra * gxra > reach2a)) || (rowb && !(gyzb + gxrb * gxrb > reach2b)));
-                int pb = inl ? a.cell_start[kc - 1] : s1;
-                int pe = inr ? a.cell_start[kc + 2] : s2;
-                const unsigned code_yz = (unsigned)(3 * (my - by + 1) + 9 * (nz - bz + 1));
-                // each particle's x window (empty for a particle whose row is out of reach)
-                const float wa = rowa ? sqrtf(fmaxf(reach2a - gyza, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm : -1.0e30f;
-                const float wb = rowb ? sqrtf(fmaxf(reach2b - gyzb, 0.0f)) * 1.0009765625f + 9.765625e-4f * csm : -1.0e30f;
-                int hi = pe;
-                while (XWIN && pb < hi) {   // first candidate inside either window on the left
-                    const int mid = (pb + hi) >> 1;
-                    const float cx = a.cposf[mid].x;
-                    const bool l = mid < s1, r = mid >= s2;
-                    const float qa = l ? qxla : (r ? qxra : ua.x), qb = l ? qxlb : (r ? qxrb : ub.x);
-                    if (qa - cx > wa && qb - cx > wb) pb = mid + 1;
-                    else hi = mid;
-                }
-                int lo = pb;
-                while (XWIN && lo < pe) {   // first candidate beyond both windows on the right
-                    const int mid = (lo + pe) >> 1;
-                    const float cx = a.cposf[mid].x;
-                    const bool l = mid < s1, r = mid >= s2;
-                    const float qa = l ? qxla : (r ? qxra : ua.x), qb = l ? qxlb : (r ? qxrb : ub.x);
-                    if (qa - cx < -wa && qb - cx < -wb) pe = mid;
-                    else lo = mid + 1;
-                }
-                for (int p = pb; p < pe; ++p) {
-                    const float4 c = a.cposf[p];
-                    const bool left = p < s1, right = p >= s2;
-                    const unsigned code = (code_yz + (left ? 0u : (right ? 2u : 1u))) << 26;
-                    {
-                        const float qx = left ? qxla : (right ? qxra : ua.x);
-                        const float dx = qx - c.x, dy = qya - c.y, dz = qza - c.z;
-                        const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float hsf = ua.w + c.w;
-                        const float r2f = hsf * hsf;
-                        bool in = d2f < fmaf(r2f, khi, kb) && p != t0;
-                        if (in && d2f > fmaf(r2f, klo, -kb)) {
-                            const double4 cd = a.cpos[p];
-                            const double hs = __dadd_rn(cd.w, xa.w);
-                            in = exact_d2(xa, cd) < __dmul_rn(hs, hs);
-                        }
-                        if (in && n0 < cap) out0[n0] = (unsigned)p | code;
-                        n0 += in ? 1 : 0;
-                    }
-                    {
-                        const float qx = left ? qxlb : (right ? qxrb : ub.x);
-                        const float dx = qx - c.x, dy = qyb - c.y, dz = qzb - c.z;
-                        const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float hsf = ub.w + c.w;
-                        const float r2f = hsf * hsf;
-                        bool in = d2f < fmaf(r2f, khi, kb) && p != t1;
-                        if (in && d2f > fmaf(r2f, klo, -kb)) {
-                            const double4 cd = a.cpos[p];
-                            const double hs = __dadd_rn(cd.w, xb.w);
-                            in = exact_d2(xb, cd) < __dmul_rn(hs, hs);
-                        }
-                        if (in && n1 < cap) out1[n1] = (unsigned)p | code;
-                        n1 += in ? 1 : 0;
-                    }
-                }
-            }
-        }
-    }
-    search_one<V | kSrchNoReal>(a, t0, n0);
-    search_one<V | kSrchNoReal>(a, t1, n1);
 }
 
 // The same search with one warp per position t (search_kind 2; on the
@@ -1593,11 +1460,7 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
         const unsigned nb = (unsigned)((a.n + threads - 1) / threads);
         if (a.prm.xsort) {
             switch (v) {
-                case 0: {
-                    const long long pairs = (a.n + 1) / 2;
-                    k_search_pair<true><<<(unsigned)((pairs + threads - 1) / threads), threads, 0, s>>>(a);
-                    break;
-                }
+                case 0: k_search<kSrchXWin><<<nb, threads, 0, s>>>(a); break;
                 case kSrchContact: k_search<kSrchXWin | kSrchContact><<<nb, threads, 0, s>>>(a); break;
                 case kSrchTwoPass: k_search<kSrchXWin | kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
                 case kSrchMind: k_search<kSrchXWin | kSrchMind><<<nb, threads, 0, s>>>(a); break;
@@ -1606,13 +1469,7 @@ void launch_search(const StepArgs &a, cudaStream_t s) {
             }
         } else {
             switch (v) {
-                case 0:
-#ifdef MCM_EXACT_SEARCH_PAIR
-                    k_search_pair<false><<<(unsigned)(((a.n + 1) / 2 + threads - 1) / threads), threads, 0, s>>>(a);
-#else
-                    k_search<0><<<nb, threads, 0, s>>>(a);
-#endif
-                    break;
+                case 0: k_search<0><<<nb, threads, 0, s>>>(a); break;
                 case kSrchContact: k_search<kSrchContact><<<nb, threads, 0, s>>>(a); break;
                 case kSrchTwoPass: k_search<kSrchTwoPass><<<nb, threads, 0, s>>>(a); break;
                 case kSrchMind: k_search<kSrchMind><<<nb, threads, 0, s>>>(a); break;
