@@ -72,7 +72,6 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     // neighbour order: their cells are kept in x order, which lets the search
     // window each row of cells in x
     p.xsort = c.precision != MCM_PREC_FP64_EXACT ? 1 : 0;
-    p.srec = c.precision == MCM_PREC_MIXED ? 1 : 0;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;

@@ -235,30 +235,16 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
         const int key = a.key[i];
         a.ckey[p] = key;
         float4 r = make_float4(0.f, 0.f, 0.f, (float)h);
-        double o[3] = {0.0, 0.0, 0.0};
         if (key >= 0) {
             int bx, by, bz;
             cell_coords(key, g.gridlim, bx, by, bz);
-            o[0] = cell_origin(g, 0, bx);
-            o[1] = cell_origin(g, 1, by);
-            o[2] = cell_origin(g, 2, bz);
-            r.x = (float)(x - o[0]);
-            r.y = (float)(y - o[1]);
-            r.z = (float)(z - o[2]);
+            r.x = (float)(x - cell_origin(g, 0, bx));
+            r.y = (float)(y - cell_origin(g, 1, by));
+            r.z = (float)(z - cell_origin(g, 2, bz));
             const unsigned long long hb = (unsigned long long)__double_as_longlong(h);
             hbits = hb > hbits ? hb : hbits;
         }
         a.cposf[p] = r;
-        if (a.prm.srec) {
-            // the mixed strain gather's record of position p (MCM/mcm_strain.f90:
-            // 27-31: x - v dt/2, and V = m/rho), relative to the same cell origin
-            const double dt = a.time->dt;
-            const double vx = a.F.f[FVX][i], vy = a.F.f[FVY][i], vz = a.F.f[FVZ][i];
-            const double xs = x - 0.5 * vx * dt, ys = y - 0.5 * vy * dt, zs = z - 0.5 * vz * dt;
-            a.frec0[2 * (size_t)p] = make_float4((float)(xs - o[0]), (float)(ys - o[1]), (float)(zs - o[2]), (float)h);
-            a.frec0[2 * (size_t)p + 1] =
-                make_float4((float)vx, (float)vy, (float)vz, (float)(a.F.f[FMASS][i] / a.F.f[FRHO][i]));
-        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long v = __shfl_xor_sync(0xffffffffu, hbits, o);
@@ -675,30 +661,24 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                         // converged (measured: 1.41 against 1.46 ms on the 2M
                         // bar; on the unwindowed rows of the reference order it
                         // is slower than the branching loop)
-                        // the window's part in each of the row's cells, with
-                        // that cell's offset and code fixed for its loop
-#pragma unroll
-                        for (int part = 0; part < 3; ++part) {
-                            const int q0 = part == 0 ? pb : (pb > (part == 1 ? s1 : s2) ? pb : (part == 1 ? s1 : s2));
-                            const int q1 = part == 2 ? pe : (pe < (part == 0 ? s1 : s2) ? pe : (part == 0 ? s1 : s2));
-                            const float qx = part == 0 ? qxl : (part == 1 ? ui.x : qxr);
-                            const unsigned code = (code_yz + (unsigned)part) << 26;
-                            for (int p = q0; p < q1; ++p) {
-                                const float4 c = a.cposf[p];
-                                const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
-                                const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                                const float hsf = ui.w + c.w;
-                                const float r2f = hsf * hsf;
-                                bool in = d2f < fmaf(r2f, khi, kb) && p != t;
-                                if (in && d2f > fmaf(r2f, klo, -kb)) {
-                                    // near tie: the reference's FP64 test
-                                    const double4 cd = a.cpos[p];
-                                    const double hs = __dadd_rn(cd.w, xi.w);
-                                    in = exact_d2(xi, cd) < __dmul_rn(hs, hs);
-                                }
-                                if (in && nn < cap) out[nn] = (unsigned)p | code;
-                                nn += in ? 1 : 0;
+                        for (int p = pb; p < pe; ++p) {
+                            const float4 c = a.cposf[p];
+                            const bool left = p < s1, right = p >= s2;
+                            const float qx = left ? qxl : (right ? qxr : ui.x);
+                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                            const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float hsf = ui.w + c.w;
+                            const float r2f = hsf * hsf;
+                            bool in = d2f < fmaf(r2f, khi, kb) && p != t;
+                            if (in && d2f > fmaf(r2f, klo, -kb)) {
+                                // near tie: the reference's FP64 test
+                                const double4 cd = a.cpos[p];
+                                const double hs = __dadd_rn(cd.w, xi.w);
+                                in = exact_d2(xi, cd) < __dmul_rn(hs, hs);
                             }
+                            const unsigned code = (code_yz + (left ? 0u : (right ? 2u : 1u))) << 26;
+                            if (in && nn < cap) out[nn] = (unsigned)p | code;
+                            nn += in ? 1 : 0;
                         }
                     } else {
                     for (int p = pb; p < pe; ++p) {

@@ -144,8 +144,7 @@ __global__ void k_strain_prep(StepArgs a) {
     const double dt = a.time->dt;
     const Frame fr = make_frame(*a.grid);
     const double *const *f = a.F.f;
-    // with srec the cell-record kernel has written the real particles' records
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < (a.prm.srec ? 0 : a.n); p += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
         const int i = a.cell_list[p];
         double o[3];
         frame_origin(fr, a.ckey[p], o);
