@@ -72,7 +72,6 @@ DevParams make_params(const mcm_gpu_config &c, int nmat) {
     // neighbour order: their cells are kept in x order, which lets the search
     // window each row of cells in x
     p.xsort = c.precision != MCM_PREC_FP64_EXACT ? 1 : 0;
-    p.mrec = c.precision == MCM_PREC_MIXED ? 1 : 0;
     p.veloc_opt = c.veloc_opt;
     for (int k = 0; k < 3; ++k) p.base_a[k] = c.baseaccel ? c.base_a[k] : 0.0;
     DevPlanes &pl = p.planes;
@@ -128,10 +127,8 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
     CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
     CK(cudaMemsetAsync(h->A.gnnbr, 0, sizeof(int) * np, h->stream));
-    if (h->A.prm.skin > 0.0 || h->A.prm.mrec) {
-        if ((st = dalloc(h, &h->A.pos_of, np))) return st;   // state index -> cell-order position
-    }
     if (h->A.prm.skin > 0.0) {
+        if ((st = dalloc(h, &h->A.pos_of, np))) return st;
         if ((st = dalloc(h, &h->A.supn, np))) return st;
         if ((st = dalloc(h, &h->A.xref, 3 * np))) return st;
     }

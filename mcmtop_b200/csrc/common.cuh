@@ -73,7 +73,6 @@ struct DevParams {
     int contact;      // contacttype > 0 with more than one material: contact lists and repulsion are built
     int kahan;        // mixed precision: pair sums compensated per lane (Kahan) before the lane combination
     int xsort;        // each cell's particles in ascending x (FP64-fast, mixed); else descending reference index
-    int mrec;         // mixed step: the constitutive kernel writes the momentum gather's records of real particles
     double drelax_scale, tssf, hmax;
     double skin;      // > 0: neighbour lists filtered from skin lists kept within h_i + h_j + skin * hmax
     double base_a[3];

@@ -171,29 +171,6 @@ struct PackSpec {
 void launch_unpack(const StepArgs &a, const PackSpec &s, const double *stage, cudaStream_t st);
 void launch_pack(const StepArgs &a, const PackSpec &s, double *stage, cudaStream_t st);
 
-// Mixed-step momentum records in three arrays of the 64-byte-per-position
-// buffer frec0: position p's first 32 bytes at frec0 + 2p (x y z relative to
-// the cell origin o, h; A11 A22 A33 A12 with A = (sigma - q I) / rho^2), the
-// next 16 at frec0 + 2 npad + p (A13 A23 m rho) and the cap model's lower
-// triangle at frec0 + 3 npad + p, so that neighbouring positions' records lie
-// next to each other in every array.
-__device__ __forceinline__ float4 *mom_tail(const StepArgs &a) { return a.frec0 + 2 * (size_t)a.npad; }
-__device__ __forceinline__ float4 *mom_lower(const StepArgs &a) { return a.frec0 + 3 * (size_t)a.npad; }
-__device__ __forceinline__ void write_mom_record(const StepArgs &a, int i, int p, const double o[3]) {
-    const double *const *f = a.F.f;
-    const double rho = f[FRHO][i];
-    const double ir2 = 1.0 / (rho * rho);
-    const double q = f[FQ][i];
-    float4 *rec = a.frec0 + 2 * (size_t)p;
-    rec[0] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]), (float)f[FH][i]);
-    rec[1] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2), (float)((f[FS33][i] - q) * ir2),
-                         (float)(f[FS12][i] * ir2));
-    mom_tail(a)[p] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
-    // the cap model's lower triangle (21 31 32), read only when a material has it
-    if (a.prm.asym)
-        mom_lower(a)[p] = make_float4((float)(f[FL21][i] * ir2), (float)(f[FL31][i] * ir2), (float)(f[FL32][i] * ir2), 0.0f);
-}
-
 constexpr int kRedThreads = 256;
 
 // Blocks of `kernel` resident on one SM at `threads` per block (the

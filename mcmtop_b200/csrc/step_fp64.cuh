@@ -382,18 +382,6 @@ __global__ void __launch_bounds__(kRedThreads, MCM_CONST_MINBLOCKS) k_constituti
         f[FX][i] = xs + 0.5 * vx * dt;
         f[FY][i] = ys + 0.5 * vy * dt;
         f[FZ][i] = zs + 0.5 * vz * dt;
-        if (a.prm.mrec) {
-            // the mixed momentum gather's record of this particle's position
-            const int p = a.pos_of[i];
-            const int key = a.ckey[p];
-            double o[3] = {0.0, 0.0, 0.0};
-            if (key >= 0) {
-                int b[3];
-                cell_coords(key, a.grid->gridlim, b[0], b[1], b[2]);
-                for (int d = 0; d < 3; ++d) o[d] = cell_origin(*a.grid, d, b[d]);
-            }
-            write_mom_record(a, i, p, o);
-        }
     }
     if (bad) raise_status(a.status, bad, i);
     double m = block_min(crit, sm);

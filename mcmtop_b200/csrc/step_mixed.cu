@@ -477,6 +477,14 @@ __global__ void __launch_bounds__(kStageThreads, 6) k_strain_staged(StepArgs a) 
     }
 }
 
+// Momentum records in three arrays of the 64-byte-per-position buffer:
+// position p's first 32 bytes at frec0 + 2p (x y z h, A11 A22 A33 A12), the
+// next 16 at frec0 + 2 npad + p (A13 A23 m rho) and the cap model's lower
+// triangle at frec0 + 3 npad + p, so that neighbouring positions' records lie
+// next to each other in every array.
+__device__ __forceinline__ float4 *mom_tail(const StepArgs &a) { return a.frec0 + 2 * (size_t)a.npad; }
+__device__ __forceinline__ float4 *mom_lower(const StepArgs &a) { return a.frec0 + 3 * (size_t)a.npad; }
+
 // --------------------------------------------------------- momentum prep
 // Records: cell-relative x, h; (sigma - q)/rho^2 (formed in FP64,
 // MCM/mcm_oldacceleration.f90:79-80) and m (FP32).  Ghosts: FP64 positions,
@@ -486,12 +494,23 @@ __global__ void k_mom_prep(StepArgs a) {
     if (skip_step(a)) return;
     const Frame fr = make_frame(*a.grid);
     const double *const *f = a.F.f;
-    // with mrec the constitutive kernel has written the real particles' records
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < (a.prm.mrec ? 0 : a.n); p += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
         const int i = a.cell_list[p];
         double o[3];
         frame_origin(fr, a.ckey[p], o);
-        write_mom_record(a, i, p, o);
+        const double rho = f[FRHO][i];
+        const double ir2 = 1.0 / (rho * rho);
+        const double q = f[FQ][i];
+        float4 *rec = a.frec0 + 2 * (size_t)p;
+        rec[0] = make_float4((float)(f[FX][i] - o[0]), (float)(f[FY][i] - o[1]), (float)(f[FZ][i] - o[2]),
+                             (float)f[FH][i]);
+        rec[1] = make_float4((float)((f[FS11][i] - q) * ir2), (float)((f[FS22][i] - q) * ir2),
+                                 (float)((f[FS33][i] - q) * ir2), (float)(f[FS12][i] * ir2));
+        mom_tail(a)[p] = make_float4((float)(f[FS13][i] * ir2), (float)(f[FS23][i] * ir2), (float)f[FMASS][i], (float)rho);
+        // the cap model's lower triangle (21 31 32), read only when a material has it
+        if (a.prm.asym)
+            mom_lower(a)[p] =
+                make_float4((float)(f[FL21][i] * ir2), (float)(f[FL31][i] * ir2), (float)(f[FL32][i] * ir2), 0.0f);
     }
     if (a.prm.boundary) {
         const int ngp = *a.ngp;
