@@ -191,6 +191,13 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f);
 
 /* ------------------------------------------------------------------ step */
 
+/* Returns critts as soon as the neighbour search, strain rate and
+ * constitutive update of the step are done.  The momentum sum and the energy
+ * sums of step_b do not depend on the new dt (step_c moves the particles), so
+ * step_a also enqueues them behind that work: they run on the device while
+ * the caller updates dt, and the step_b that follows enqueues nothing (the
+ * acceleration of a download between step_a and step_b is already the
+ * step's).  An upload or mcm_gpu_run between step_a and step_b discards it. */
 int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts);
 /* energies: per material ke, ie, mom(3) -> 5*nmat doubles (mcm_mat%ke, %ie, %mom),
  * then kinetice, internale, totale.  May be NULL.

@@ -771,6 +771,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->timer)
         if (e) cudaEventDestroy(e);
+    if (h->part_a_done) cudaEventDestroy(h->part_a_done);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MCM_OK;
@@ -884,21 +885,6 @@ int run_search_only(mcm_gpu_handle *h) {
 }
 
 // Enqueues part a with retries; returns the final status.
-int run_part_a(mcm_gpu_handle *h) {
-    for (int attempt = 0; attempt < 8; ++attempt) {
-        int st;
-        if ((st = reset_status(h))) return st;
-        enqueue_part_a(h);
-        if ((st = sync_status(h))) return st;
-        int code = h->h_status->code;
-        if (code == MCM_OK) return MCM_OK;
-        int grew = 0;
-        if ((st = regrow(h, &grew))) return st;
-        if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
-    }
-    return set_error(h, MCM_ENBR_OVERFLOW, "storage did not converge");
-}
-
 int finish_upload(mcm_gpu_handle *h, const double *coord_maxmin) {
     int st;
     k_iota<<<256, 256, 0, h->stream>>>(h->A.F.orig, h->np);
@@ -924,6 +910,7 @@ extern "C" {
 
 int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coord_maxmin) {
     if (!h || !f || !f->x || !f->mat) return MCM_EINVAL;
+    h->part_b_enqueued = false;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np;
@@ -1028,22 +1015,48 @@ int mcm_gpu_step_a(mcm_gpu_handle *h, double dt, double *critts) {
     int st;
     if ((st = check_handle(h))) return st;
     h->A.split_mode = 1;
+    h->part_b_enqueued = false;
     {
         Scope sc(h, R_MISC, 1);
         launch_set_time(h->A, h->stream, dt, 0.0, 0);
     }
-    if ((st = run_part_a(h))) return st;
-    h->last_max_gnbr = h->h_status->max_gnbr;
-    if (critts) *critts = h->h_time->critts;
-    return MCM_OK;
+    if (!h->part_a_done) CK(cudaEventCreateWithFlags(&h->part_a_done, cudaEventDisableTiming));
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        if ((st = reset_status(h))) return st;
+        enqueue_part_a(h);
+        CK(cudaMemcpyAsync(h->h_status, h->A.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaEventRecord(h->part_a_done, h->stream));
+        // the momentum sum of the split loop does not read dt (step_c moves):
+        // it runs while the caller computes the next dt from critts; after a
+        // failed part A its kernels see the raised status and do nothing
+        enqueue_part_b(h, 0);
+        CK(cudaEventSynchronize(h->part_a_done));
+        CK(cudaGetLastError());
+        const int code = h->h_status->code;
+        if (code == MCM_OK) {
+            h->part_b_enqueued = true;
+            h->last_max_gnbr = h->h_status->max_gnbr;
+            if (critts) *critts = h->h_time->critts;
+            return MCM_OK;
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        int grew = 0;
+        if ((st = regrow(h, &grew))) return st;
+        if (!grew) return set_error(h, code, mcm_gpu_strerror(code));
+    }
+    return set_error(h, MCM_ENBR_OVERFLOW, "storage did not converge");
 }
 
 int mcm_gpu_step_b(mcm_gpu_handle *h, double *energies) {
     int st;
     if ((st = check_handle(h))) return st;
     h->A.split_mode = 1;
-    if ((st = reset_status(h))) return st;
-    enqueue_part_b(h, 0);
+    if (!h->part_b_enqueued) {   // step_a has not enqueued it (a call out of the usual order)
+        if ((st = reset_status(h))) return st;
+        enqueue_part_b(h, 0);
+    }
+    h->part_b_enqueued = false;
     if (!energies) return MCM_OK;   // nothing to wait for: errors surface at the next waiting call
     CK(cudaMemcpyAsync(h->h_energy, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost,
                        h->stream));
@@ -1081,6 +1094,7 @@ int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done) {
     if (!t || nsteps < 0) return MCM_EINVAL;
     if (done) *done = 0;
     h->A.split_mode = 0;
+    h->part_b_enqueued = false;
     DevTime dtm;
     std::memset(&dtm, 0, sizeof(dtm));
     dtm.dt = t->dt; dtm.dtold = t->dtold; dtm.ptime = t->ptime; dtm.endtime = t->endtime;

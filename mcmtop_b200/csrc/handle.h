@@ -56,6 +56,11 @@ struct mcm_gpu_handle {
     struct StepRecord { char *buf = nullptr; size_t bytes = 0; int nstride = 0, gstride = 0, ghost_cap = 0; };
     std::vector<StepRecord> adj_rec;
     int last_max_gnbr = 0;       // longest ghost-neighbour list of the last step_a
+    // split loop: step_a enqueues the momentum sum (independent of the new dt)
+    // behind part A and waits only for part A (an event), so the GPU computes
+    // the forces while the caller updates dt; step_b then enqueues nothing
+    cudaEvent_t part_a_done = nullptr;
+    bool part_b_enqueued = false;
     double tuned_ms = 0.0;       // mcm_gpu_autotune: time per iteration of the chosen launch shape
     double *d_theta = nullptr;   // parameter adjoints (nmat x 4)
 };
