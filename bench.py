@@ -744,7 +744,8 @@ def gpu_arm(args):
                "d2h_bytes_per_step": int(d2h_bytes / k_e2e + per_step_d2h),
                "steps": k_e2e, "wall_ms": split_ms,
                "path": "mcm_gpu_upload + (step_a -> critts, host dt, step_b, step_c) x K + mcm_gpu_download; "
-                       "step_b returns the energies at the last step (the output time)"}
+                       "step_a waits for the critical timestep while the step's momentum sum runs; step_b "
+                       "returns the energies at the last step (the output time)"}
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:
