@@ -283,7 +283,22 @@ __global__ void __launch_bounds__(256) k_cell_sort(StepArgs a) {
         const int s = a.cell_start[c], e = a.cell_start[c + 1];
         const int n = e - s;
         if (n < 2) continue;   // warp-uniform
-        if (n <= 32 * kSortPer) {
+        if (n <= 32) {
+            // one particle per lane (the common case)
+            const bool on = lane < n;
+            const int v = on ? a.cell_list[s + lane] : 0;
+            const int o = on ? a.F.orig[v] : 0;
+            const double x = (on && xs) ? X[v] : 0.0;
+            int rank = 0;
+            for (int k = 0; k < n; ++k) {
+                const double xb = __shfl_sync(0xffffffffu, x, k);
+                const int ob = __shfl_sync(0xffffffffu, o, k);
+                rank += cell_before(xs, xb, ob, x, o) ? 1 : 0;
+            }
+            __syncwarp();
+            if (on) a.cell_list[s + rank] = v;
+            __syncwarp();
+        } else if (n <= 32 * kSortPer) {
             int v[kSortPer], o[kSortPer], rank[kSortPer];
             double x[kSortPer];
 #pragma unroll
@@ -482,17 +497,22 @@ __global__ void k_ghost_emit(StepArgs a, int plane) {
     const int base = *a.plane_base;
     // axes this plane mirrors (bit d: x_d -> -x_d + add_d); composed along ghost chains
     const int flips = (mult[0] < 0.0 ? 1 : 0) | (mult[1] < 0.0 ? 2 : 0) | (mult[2] < 0.0 ? 4 : 0);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < p.L; t += (long long)gridDim.x * blockDim.x) {
+    // one warp per layer cell, its lanes over the cell's ghosts (the sources
+    // are real particles or ghosts of earlier planes, so no ghost of this
+    // launch reads another)
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < p.L; t += nw) {
         int cnt = a.layer_count[t];
         if (cnt == 0) continue;
         int cs, cd;
         layer_cells(a, p, t, cs, cd);
         int g0 = base + a.layer_off[t];
-        a.gcell[cd] = make_int2(g0, cnt);
+        if (lane == 0) a.gcell[cd] = make_int2(g0, cnt);
         int rs = a.cell_start[cs];
         int nreal = a.cell_start[cs + 1] - rs;
         int2 src = a.gcell[cs];
-        for (int r = 0; r < cnt; ++r) {
+        for (int r = lane; r < cnt; r += 32) {
             int g = g0 + r;
             if (nreal > 0) {
                 // MCM/mcm_ghost_setup.f90:324-355 (create_ghost_from_real)
@@ -541,7 +561,9 @@ void launch_ghosts(const StepArgs &a, cudaStream_t s) {
         if (blocks > 592) blocks = 592;
         k_ghost_count<<<blocks, 256, 0, s>>>(a, plane);
         k_ghost_layer_scan<<<1, kScanThreads, 0, s>>>(a, plane);
-        k_ghost_emit<<<blocks, 256, 0, s>>>(a, plane);
+        long long eb = ((long long)a.layer_cap + 7) / 8;   // 8 warps (layer cells) per block
+        if (eb > 148LL * 8) eb = 148LL * 8;
+        k_ghost_emit<<<(unsigned)(eb < 1 ? 1 : eb), 256, 0, s>>>(a, plane);
     }
 }
 
