@@ -120,6 +120,7 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.cell_list, np))) return st;
     if ((st = dalloc(h, &h->A.cpos, np))) return st;
     if ((st = dalloc(h, &h->A.cposf, np))) return st;
+    if (h->A.prm.xsort && (st = dalloc(h, &h->A.cposg, np))) return st;
     if ((st = dalloc(h, &h->A.cmat, np))) return st;
     if ((st = dalloc(h, &h->A.ckey, np))) return st;
     if ((st = dalloc(h, &h->A.reorder_tmp, np))) return st;
@@ -748,7 +749,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     void *ptrs[] = {h->d_fields, h->d_stage, h->A.frec0, h->A.gfrec1, h->A.gfrec2,
                     h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
-                    h->A.cpos, h->A.cposf, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
+                    h->A.cpos, h->A.cposf, h->A.cposg, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,

@@ -245,6 +245,9 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
             hbits = hb > hbits ? hb : hbits;
         }
         a.cposf[p] = r;
+        // the windowed search's copy: x relative to the grid origin, so that the
+        // candidates of a row's two or three cells share one frame in x
+        if (a.cposg) a.cposg[p] = make_float4((float)(x - g.gridmin[0]), r.y, r.z, r.w);
     }
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long v = __shfl_xor_sync(0xffffffffu, hbits, o);
@@ -631,6 +634,11 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         // this particle relative to the origins of the left, own and right cell of a row
         const float qxl = ui.x + cs[0], qxr = ui.x - cs[0];
         const float gxl = fmaxf(ui.x, 0.0f), gxr = fmaxf(cs[0] - ui.x, 0.0f);
+        // windowed rows: x relative to the grid origin (one frame for the whole
+        // row); its rounding (up to gridlim(1) cells of magnitude) widens the
+        // decision band by gridlim(1) 2^-16 cell^2, 32 times that error's bound
+        const float ugx = xwin ? a.cposg[t].x : 0.0f;
+        const float kbx = kb + (xwin ? (float)g.gridlim[0] * 1.52587890625e-5f * csm * csm : 0.0f);
         const int mati = a.cmat[t];
         unsigned *out = a.nidx + (size_t)t * cap;
         // MCM/mcm_ll_neighbours.f90:150-174, 238-267: other materials'
@@ -665,15 +673,13 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                         int hi = re;
                         while (pb < hi) {
                             const int mid = (pb + hi) >> 1;
-                            const float q = mid < s1 ? qxl : (mid < s2 ? ui.x : qxr);
-                            if (q - a.cposf[mid].x > rxw) pb = mid + 1;
+                            if (ugx - a.cposg[mid].x > rxw) pb = mid + 1;
                             else hi = mid;
                         }
                         int lo = pb;
                         while (lo < pe) {
                             const int mid = (lo + pe) >> 1;
-                            const float q = mid < s1 ? qxl : (mid < s2 ? ui.x : qxr);
-                            if (q - a.cposf[mid].x < -rxw) pe = mid;
+                            if (ugx - a.cposg[mid].x < -rxw) pe = mid;
                             else lo = mid + 1;
                         }
                     }
@@ -684,21 +690,19 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                         // bar; on the unwindowed rows of the reference order it
                         // is slower than the branching loop)
                         for (int p = pb; p < pe; ++p) {
-                            const float4 c = a.cposf[p];
-                            const bool left = p < s1, right = p >= s2;
-                            const float qx = left ? qxl : (right ? qxr : ui.x);
-                            const float dx = qx - c.x, dy = qy - c.y, dz = qz - c.z;
+                            const float4 c = a.cposg[p];
+                            const float dx = ugx - c.x, dy = qy - c.y, dz = qz - c.z;
                             const float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                             const float hsf = ui.w + c.w;
                             const float r2f = hsf * hsf;
-                            bool in = d2f < fmaf(r2f, khi, kb) && p != t;
-                            if (in && d2f > fmaf(r2f, klo, -kb)) {
+                            bool in = d2f < fmaf(r2f, khi, kbx) && p != t;
+                            if (in && d2f > fmaf(r2f, klo, -kbx)) {
                                 // near tie: the reference's FP64 test
                                 const double4 cd = a.cpos[p];
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 in = exact_d2(xi, cd) < __dmul_rn(hs, hs);
                             }
-                            const unsigned code = (code_yz + (left ? 0u : (right ? 2u : 1u))) << 26;
+                            const unsigned code = (code_yz + (p < s1 ? 0u : (p >= s2 ? 2u : 1u))) << 26;
                             if (in && nn < cap) out[nn] = (unsigned)p | code;
                             nn += in ? 1 : 0;
                         }

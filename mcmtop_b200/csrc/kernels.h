@@ -34,6 +34,7 @@ struct StepArgs {
     int *n_inside;    // particles inside the grid (device counter)
     double4 *cpos;    // per position: x, y, z, h at neighbour time
     float4 *cposf;    // per position: x, y, z relative to the cell origin (FP32), h
+    float4 *cposg;    // x-ordered steps, per position: x relative to the grid origin, y, z relative to the cell origin (FP32), h
     int *cmat;        // per position: material
     int *ckey;        // per position: cell key or -1
     int *scan_sums;   // block sums of the scan
