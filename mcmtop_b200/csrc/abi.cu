@@ -124,6 +124,7 @@ int alloc_particles(mcm_gpu_handle *h) {
     if ((st = dalloc(h, &h->A.cmat, np))) return st;
     if ((st = dalloc(h, &h->A.ckey, np))) return st;
     if ((st = dalloc(h, &h->A.reorder_tmp, np))) return st;
+    if (h->cfg.reorder_interval > 0 && (st = dalloc(h, &h->A.reorder_grp, (size_t)kReorderGroup * np))) return st;
     if ((st = dalloc(h, &h->A.nnbr, np))) return st;
     if ((st = dalloc(h, &h->A.gnnbr, np))) return st;
     CK(cudaMemsetAsync(h->A.nnbr, 0, sizeof(int) * np, h->stream));
@@ -352,7 +353,7 @@ void enqueue_part_a(mcm_gpu_handle *h) {
     StepArgs &a = h->A;
     const int every = h->cfg.reorder_interval;
     if (every > 0 && h->have_cells && (h->steps_enqueued % every) == 0) {
-        Scope sc(h, R_MISC, 2 * (NFIELD + 4) + (a.prm.skin > 0.0 ? 1 : 0));
+        Scope sc(h, R_MISC, kReorderLaunches + (a.prm.skin > 0.0 ? 1 : 0));
         launch_reorder(a, h->stream);
         // the skin lists hold state indices, which the re-sort permutes
         if (a.prm.skin > 0.0) launch_skin_force(a, h->stream);
@@ -749,7 +750,7 @@ int mcm_gpu_destroy(mcm_gpu_handle *h) {
     void *ptrs[] = {h->d_fields, h->d_stage, h->A.frec0, h->A.gfrec1, h->A.gfrec2,
                     h->d_ints, h->d_mats, h->d_scalars, h->d_nppermat,
                     h->A.key, h->A.cell_list, h->A.nnbr, h->A.gnnbr, h->A.rec0, h->A.rec1, h->A.rec2,
-                    h->A.cpos, h->A.cposf, h->A.cposg, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.nidx,
+                    h->A.cpos, h->A.cposf, h->A.cposg, h->A.cmat, h->A.ckey, h->A.reorder_tmp, h->A.reorder_grp, h->A.nidx,
                     h->A.red, h->A.cell_count, h->A.cell_start, h->A.scan_sums, h->A.gcell,
                     h->A.layer_count, h->A.layer_off, h->A.gx, h->A.gy, h->A.gz, h->A.gvx, h->A.gvy,
                     h->A.gvz, h->A.gmass, h->A.gh, h->A.ghold, h->A.grho, h->A.gpar, h->A.gmat, h->A.gflip,

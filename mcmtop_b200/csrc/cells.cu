@@ -379,24 +379,30 @@ void launch_cell_build(const StepArgs &a, cudaStream_t s) {
 // so that the gathers of later steps walk memory nearly in order.  Results do
 // not depend on it: every order used by the step is defined by cell keys and
 // reference indices, not by storage positions.
-__global__ void k_permute_field(const double *src, double *dst, const int *perm, int n) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[perm[p]];
-}
 __global__ void k_permute_int(const int *src, int *dst, const int *perm, int n) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[perm[p]];
-}
-__global__ void k_copy_back(const double *src, double *dst, int n) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[p];
 }
 __global__ void k_copy_back_int(const int *src, int *dst, int n) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[p] = src[p];
 }
 
+// A group of nf consecutive fields (field k of the group at base + k np),
+// permuted into tmp (padding copied as it is) in one pass over the positions.
+__global__ void k_permute_group(const double *base, size_t np, int nf, double *tmp, const int *perm, int n) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < np; p += (size_t)gridDim.x * blockDim.x) {
+        const size_t j = p < (size_t)n ? (size_t)perm[p] : p;
+        for (int k = 0; k < nf; ++k) tmp[k * np + p] = base[k * np + j];
+    }
+}
+
 void launch_reorder(const StepArgs &a, cudaStream_t s) {
     const int b = grid_blocks(a.n, 256);
-    for (int f = 0; f < NFIELD; ++f) {
-        k_permute_field<<<b, 256, 0, s>>>(a.F.f[f], a.reorder_tmp, a.cell_list, a.n);
-        k_copy_back<<<b, 256, 0, s>>>(a.reorder_tmp, a.F.f[f], a.n);
+    // the fields lie at F.f[0] + f npad: each group is one contiguous range
+    const size_t np = (size_t)a.npad;
+    for (int f0 = 0; f0 < NFIELD; f0 += kReorderGroup) {
+        const int nf = NFIELD - f0 < kReorderGroup ? NFIELD - f0 : kReorderGroup;
+        k_permute_group<<<b, 256, 0, s>>>(a.F.f[f0], np, nf, a.reorder_grp, a.cell_list, a.n);
+        cudaMemcpyAsync(a.F.f[f0], a.reorder_grp, sizeof(double) * nf * np, cudaMemcpyDeviceToDevice, s);
     }
     int *ints[4] = {a.F.mat, a.F.dispbc, a.F.orig, a.F.ptype};
     for (int *p : ints) {

@@ -71,6 +71,7 @@ struct StepArgs {
     int *skin_flags;                 // [0] force a build, [1] this step builds, [2] builds so far
     unsigned long long *skin_d2;     // bits of the largest squared displacement since the build
     double *reorder_tmp;   // npad doubles of scratch for the state permutation
+    double *reorder_grp;   // kReorderGroup x npad doubles: a group of fields permuted at once (reorder_interval > 0)
     // gather records
     double4 *rec0, *rec1, *rec2;   // per particle
     double4 *grec0, *grec1, *grec2;  // per ghost
@@ -98,6 +99,8 @@ void launch_search(const StepArgs &a, cudaStream_t s);
 // skin lists: displacement check, conditional skin-list build, per-step filter
 void launch_skin_search(const StepArgs &a, cudaStream_t s);
 void launch_skin_force(const StepArgs &a, cudaStream_t s);   // the next step rebuilds the skin lists
+constexpr int kReorderGroup = 8;   // fields permuted by one kernel
+constexpr int kReorderLaunches = (NFIELD + kReorderGroup - 1) / kReorderGroup + 8;
 void launch_reorder(const StepArgs &a, cudaStream_t s);
 
 // reduce.cu
