@@ -1023,9 +1023,7 @@ __device__ __forceinline__ T critts_particle(const PState<T> &P, const Mat &M, i
 // MCM/mcm_constitutive.f90:29-83 for one particle, after mcm_rhoupd.
 // Returns 0, MCM_ECOMPLEX_C (the EOS reported a complex sound speed) or
 // MCM_ECAP_NOCONV (the cap model's iterated return did not converge).
-// CAP false: a kernel for bodies without a cap-model material, compiled
-// without the out-of-line call to f3dm25 (fewer registers, no stack frame).
-template <typename T, typename Mat, bool CAP = true>
+template <typename T, typename Mat>
 __device__ __forceinline__ int constitutive_particle(PState<T> &P, const Mat &M, T dt) {
     int code = 0;
     switch (M.model) {
@@ -1036,7 +1034,7 @@ __device__ __forceinline__ int constitutive_particle(PState<T> &P, const Mat &M,
             stress_rot1(P, dt); f3dm3(P, M, dt); sym_lower(P); aviscosity(P, M); lieupd(P, dt);
             break;
         case 4:
-            if constexpr (CAP && std::is_same<T, double>::value) {
+            if constexpr (std::is_same<T, double>::value) {
                 stress_rot1(P, dt);
                 {
                     // f3dm25 is an out-of-line call: it gets a copy, so that

@@ -350,7 +350,6 @@ __device__ __forceinline__ void update_h(const StepArgs &a, int i, PState<double
 #ifndef MCM_CONST_MINBLOCKS
 #define MCM_CONST_MINBLOCKS 2
 #endif
-template <bool CAP>
 __global__ void __launch_bounds__(kRedThreads, MCM_CONST_MINBLOCKS) k_constitutive(StepArgs a) {
     __shared__ double sm[32];
     if (skip_step(a)) return;
@@ -371,7 +370,7 @@ __global__ void __launch_bounds__(kRedThreads, MCM_CONST_MINBLOCKS) k_constituti
         P.tracerod = f[FTR][i];
         if (a.prm.h_opt) update_h(a, i, P, dt);
         rhoupd(P, M, dt, 3);
-        bad = constitutive_particle<double, DevMaterial, CAP>(P, M, dt);
+        bad = constitutive_particle(P, M, dt);
         const double vx = f[FVX][i], vy = f[FVY][i], vz = f[FVZ][i];
         const double mindist = (a.prm.tcrit_opt == 2) ? f[FMINDIST][i] : 0.0;
         crit = critts_particle(P, M, a.prm.tcrit_opt, 3, f[FVABS][i], mindist);
@@ -1039,9 +1038,7 @@ void launch_strain(const StepArgs &a, cudaStream_t s) {
 
 int launch_constitutive(const StepArgs &a, cudaStream_t s) {
     int blocks = nblk(a.n, kRedThreads);
-    // prm.asym: some material is the cap model
-    if (a.prm.asym) k_constitutive<true><<<blocks, kRedThreads, 0, s>>>(a);
-    else k_constitutive<false><<<blocks, kRedThreads, 0, s>>>(a);
+    k_constitutive<<<blocks, kRedThreads, 0, s>>>(a);
     return blocks;
 }
 
