@@ -225,6 +225,17 @@ int alloc_skin(mcm_gpu_handle *h, int sstride) {
     return MCM_OK;
 }
 
+// A copy ordered on the handle's stream and complete on return.  A plain
+// cudaMemcpy runs on the legacy default stream, which does not order against
+// the handle's non-blocking stream: kernels enqueued after it could read the
+// destination before a host-to-device copy of pageable memory has landed,
+// and a device-to-host copy could read results not yet written.
+cudaError_t scopy(mcm_gpu_handle *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e;
+}
+
 int reset_status(mcm_gpu_handle *h) {
     CK(cudaMemsetAsync(h->A.status, 0, sizeof(DevStatus), h->stream));
     return MCM_OK;
@@ -702,7 +713,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
         std::memcpy(d.eosinput, mats[m].eosinput, sizeof(d.eosinput));
     }
     TRY(dalloc(h, &h->d_mats, (size_t)nmat));
-    if (cudaMemcpy(h->d_mats, dm.data(), sizeof(DevMaterial) * nmat, cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (scopy(h, h->d_mats, dm.data(), sizeof(DevMaterial) * nmat, cudaMemcpyHostToDevice) != cudaSuccess) {
         mcm_gpu_destroy(h);
         return MCM_ECUDA;
     }
@@ -710,7 +721,7 @@ int mcm_gpu_create(const mcm_gpu_config *cfg, const mcm_gpu_material *mats, int 
     // scalars
     size_t scal = sizeof(DevTime) + sizeof(DevStatus) + sizeof(DevGrid) + 64 + sizeof(double) * (5 * nmat + 8) + 64;
     if (cudaMalloc(&h->d_scalars, 4096 + scal) != cudaSuccess) { mcm_gpu_destroy(h); return MCM_ENOMEM; }
-    cudaMemset(h->d_scalars, 0, 4096 + scal);
+    if (cudaMemsetAsync(h->d_scalars, 0, 4096 + scal, h->stream) != cudaSuccess) { mcm_gpu_destroy(h); return MCM_ECUDA; }
     char *p = (char *)h->d_scalars;
     h->A.time = (DevTime *)p; p += 256;
     h->A.status = (DevStatus *)p; p += 256;
@@ -939,10 +950,10 @@ int mcm_gpu_upload(mcm_gpu_handle *h, const mcm_gpu_fields *f, const double *coo
     if (f->alfa && (st = put_rec(h, f->alfa, spec_sym(FA11, false)))) return st;
     if (f->rod && (st = put_rec(h, f->rod, spec_sym(FR11, false)))) return st;
     if (f->q && (st = put_rec(h, f->q, spec_iso(FQ, false)))) return st;
-    CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
-    if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(scopy(h, h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (f->dispbc) CK(scopy(h, h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
     else CK(cudaMemsetAsync(h->A.F.dispbc, 0, sizeof(int) * n, h->stream));
-    if (f->ptype) CK(cudaMemcpy(h->A.F.ptype, f->ptype, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (f->ptype) CK(scopy(h, h->A.F.ptype, f->ptype, sizeof(int) * n, cudaMemcpyHostToDevice));
     return finish_upload(h, coord_maxmin);
 }
 
@@ -972,10 +983,10 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
         if ((st = put_scalar(h, f->rho, FRHO))) return st;
         if ((st = put_scalar(h, f->e, FE))) return st;
     }
-    CK(cudaMemcpy(h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
-    if (f->dispbc) CK(cudaMemcpy(h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(scopy(h, h->A.F.mat, f->mat, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (f->dispbc) CK(scopy(h, h->A.F.dispbc, f->dispbc, sizeof(int) * n, cudaMemcpyHostToDevice));
     else CK(cudaMemsetAsync(h->A.F.dispbc, 0, sizeof(int) * n, h->stream));
-    CK(cudaMemcpy(h->d_nppermat, cnt.data(), sizeof(int) * h->nmat, cudaMemcpyHostToDevice));
+    CK(scopy(h, h->d_nppermat, cnt.data(), sizeof(int) * h->nmat, cudaMemcpyHostToDevice));
     // hmax (MCM/mcm_init_h.f90:22-37; the material loop indexes particles 1..nummat)
     double hmax = 0.0;
     if (init_h_opt == 0) {
@@ -1009,7 +1020,7 @@ int mcm_gpu_initialise(mcm_gpu_handle *h, const mcm_gpu_fields *f, int massopt, 
     DevTime dtm;
     std::memset(&dtm, 0, sizeof(dtm));
     dtm.dt = dt; dtm.dtold = 0.0; dtm.ptime = 0.0; dtm.endtime = t->endtime; dtm.critts = critts;
-    CK(cudaMemcpy(h->A.time, &dtm, sizeof(dtm), cudaMemcpyHostToDevice));
+    CK(scopy(h, h->A.time, &dtm, sizeof(dtm), cudaMemcpyHostToDevice));
     return MCM_OK;
 }
 
@@ -1125,13 +1136,13 @@ int mcm_gpu_run(mcm_gpu_handle *h, int nsteps, mcm_gpu_time *t, int *done) {
             if ((st = regrow(h, &grew))) return st;
             if (!grew || ++attempts > 16) {
                 if (done) *done = total;
-                CK(cudaMemcpy(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
+                CK(scopy(h, h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
                 t->dt = h->h_time->dt; t->dtold = h->h_time->dtold; t->ptime = h->h_time->ptime;
                 return set_error(h, code, mcm_gpu_strerror(code));
             }
         }
     }
-    CK(cudaMemcpy(h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
+    CK(scopy(h, h->h_time, h->A.time, sizeof(DevTime), cudaMemcpyDeviceToHost));
     t->dt = h->h_time->dt; t->dtold = h->h_time->dtold; t->ptime = h->h_time->ptime;
     if (done) *done = total;
     h->A.split_mode = 1;
@@ -1145,7 +1156,7 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np;
     std::vector<int> orig(n);
-    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
     if (f->x && (st = get_rec(h, f->x, spec_vec3(FX)))) return st;
     if (f->v && (st = get_rec(h, f->v, spec_vec3(FVX)))) return st;
     if (f->a && (st = get_rec(h, f->a, spec_vec3(FAX)))) return st;
@@ -1171,7 +1182,7 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     CK(cudaStreamSynchronize(h->stream));
     std::vector<int> itmp(n);
     auto geti = [&](int *dst, const int *src) -> int {
-        CK(cudaMemcpy(itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(scopy(h, itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
         for (int p = 0; p < n; ++p) dst[orig[p]] = itmp[p];
         return MCM_OK;
     };
@@ -1180,9 +1191,9 @@ int mcm_gpu_download(mcm_gpu_handle *h, mcm_gpu_fields *f) {
     if (f->nnbr || f->g_nnbr) {
         // the counts are per cell-order position: position t holds state index cell_list[t]
         std::vector<int> clist(n);
-        CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(scopy(h, clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
         auto getc = [&](int *dst, const int *src) -> int {
-            CK(cudaMemcpy(itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            CK(scopy(h, itmp.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost));
             for (int t = 0; t < n; ++t) dst[orig[clist[t]]] = itmp[t];
             return MCM_OK;
         };
@@ -1199,11 +1210,11 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np, np = h->npad;
     std::vector<int> orig(n), cnt(n), gcnt(n), clist(n), ckey(n);
-    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(cnt.data(), h->A.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(gcnt.data(), h->A.gnnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ckey.data(), h->A.ckey, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, cnt.data(), h->A.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, gcnt.data(), h->A.gnnbr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, ckey.data(), h->A.ckey, sizeof(int) * n, cudaMemcpyDeviceToHost));
     int need = 0, gneed = 0;
     for (int t = 0; t < n; ++t) { need = std::max(need, cnt[t]); gneed = std::max(gneed, gcnt[t]); }
     if (nnbr) for (int t = 0; t < n; ++t) nnbr[orig[clist[t]]] = cnt[t];
@@ -1215,7 +1226,7 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
     if (nbr && stride) {
         const int ns = h->A.nstride;
         std::vector<unsigned int> tab((size_t)ns * np);
-        CK(cudaMemcpy(tab.data(), h->A.nidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
+        CK(scopy(h, tab.data(), h->A.nidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
         const int self = h->cfg.disctype == 1 ? 1 : 0;
         for (int t = 0; t < n; ++t) {
             int *row = nbr + (size_t)orig[clist[t]] * *stride;
@@ -1226,7 +1237,7 @@ int mcm_gpu_neighbours(mcm_gpu_handle *h, int *nnbr, int *nbr, int *stride, int 
     }
     if (g_nbr && g_stride) {
         std::vector<int> tab((size_t)h->A.gstride * np);
-        CK(cudaMemcpy(tab.data(), h->A.gnbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
+        CK(scopy(h, tab.data(), h->A.gnbr, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
         for (int t = 0; t < n; ++t)
             for (int k = 0; k < gcnt[t]; ++k) g_nbr[(size_t)orig[clist[t]] * *g_stride + k] = tab[(size_t)k * np + t] + 1;
     }
@@ -1240,12 +1251,12 @@ int mcm_gpu_contacts(mcm_gpu_handle *h, int *ncont, int *cont, int *stride, int 
     CK(cudaStreamSynchronize(h->stream));
     const int n = h->np, np = h->npad;
     std::vector<int> orig(n), cnt(n, 0), gcnt(n, 0), clist(n);
-    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, clist.data(), h->A.cell_list, sizeof(int) * n, cudaMemcpyDeviceToHost));
     const bool on = h->A.prm.contact != 0;
     if (on) {
-        CK(cudaMemcpy(cnt.data(), h->A.ncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(gcnt.data(), h->A.gncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(scopy(h, cnt.data(), h->A.ncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(scopy(h, gcnt.data(), h->A.gncont, sizeof(int) * n, cudaMemcpyDeviceToHost));
     }
     int need = 0, gneed = 0;
     for (int t = 0; t < n; ++t) { need = std::max(need, cnt[t]); gneed = std::max(gneed, gcnt[t]); }
@@ -1259,7 +1270,7 @@ int mcm_gpu_contacts(mcm_gpu_handle *h, int *ncont, int *cont, int *stride, int 
     if (cont && stride) {
         const int cs = h->A.cstride;
         std::vector<unsigned int> tab((size_t)cs * np);
-        CK(cudaMemcpy(tab.data(), h->A.cidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
+        CK(scopy(h, tab.data(), h->A.cidx, sizeof(unsigned int) * tab.size(), cudaMemcpyDeviceToHost));
         for (int t = 0; t < n; ++t) {
             int *row = cont + (size_t)orig[clist[t]] * *stride;
             for (int k = 0; k < cnt[t]; ++k) row[k] = orig[clist[tab[(size_t)t * cs + k] & 0x3ffffffu]] + 1;
@@ -1267,7 +1278,7 @@ int mcm_gpu_contacts(mcm_gpu_handle *h, int *ncont, int *cont, int *stride, int 
     }
     if (g_cont && g_stride) {
         std::vector<int> tab((size_t)h->A.gcstride * np);
-        CK(cudaMemcpy(tab.data(), h->A.gcont, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
+        CK(scopy(h, tab.data(), h->A.gcont, sizeof(int) * tab.size(), cudaMemcpyDeviceToHost));
         for (int t = 0; t < n; ++t)
             for (int k = 0; k < gcnt[t]; ++k)
                 g_cont[(size_t)orig[clist[t]] * *g_stride + k] = tab[(size_t)k * np + t] + 1;
@@ -1297,15 +1308,15 @@ int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, 
     if ((st = check_handle(h))) return st;
     CK(cudaStreamSynchronize(h->stream));
     int n = 0;
-    CK(cudaMemcpy(&n, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(scopy(h, &n, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
     if (ngp) *ngp = n;
     int m = std::min(n, cap);
     if (m <= 0) return MCM_OK;
     std::vector<int> orig(h->np);
-    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+    CK(scopy(h, orig.data(), h->A.F.orig, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
     if (par) {
         std::vector<int> gp(m);
-        CK(cudaMemcpy(gp.data(), h->A.gpar, sizeof(int) * m, cudaMemcpyDeviceToHost));
+        CK(scopy(h, gp.data(), h->A.gpar, sizeof(int) * m, cudaMemcpyDeviceToHost));
         for (int g = 0; g < m; ++g) par[g] = orig[gp[g]] + 1;
     }
     std::vector<double> tmp(m);
@@ -1313,11 +1324,11 @@ int mcm_gpu_ghosts(mcm_gpu_handle *h, int *ngp, int *par, double *x, double *v, 
     double *const vs[3] = {h->A.gvx, h->A.gvy, h->A.gvz};
     for (int k = 0; k < 3; ++k) {
         if (x) {
-            CK(cudaMemcpy(tmp.data(), xs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
+            CK(scopy(h, tmp.data(), xs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
             for (int g = 0; g < m; ++g) x[3 * (size_t)g + k] = tmp[g];
         }
         if (v) {
-            CK(cudaMemcpy(tmp.data(), vs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
+            CK(scopy(h, tmp.data(), vs[k], sizeof(double) * m, cudaMemcpyDeviceToHost));
             for (int g = 0; g < m; ++g) v[3 * (size_t)g + k] = tmp[g];
         }
     }
@@ -1329,7 +1340,7 @@ int mcm_gpu_grid(mcm_gpu_handle *h, int *gridlim, double *gridmin, double *grids
     if ((st = check_handle(h))) return st;
     CK(cudaStreamSynchronize(h->stream));
     DevGrid g;
-    CK(cudaMemcpy(&g, h->A.grid, sizeof(g), cudaMemcpyDeviceToHost));
+    CK(scopy(h, &g, h->A.grid, sizeof(g), cudaMemcpyDeviceToHost));
     for (int k = 0; k < 3; ++k) {
         if (gridlim) gridlim[k] = g.gridlim[k];
         if (gridmin) gridmin[k] = g.gridmin[k];
@@ -1343,7 +1354,7 @@ int mcm_gpu_energies(mcm_gpu_handle *h, double *energies) {
     if ((st = check_handle(h))) return st;
     if (!energies) return MCM_EINVAL;
     CK(cudaStreamSynchronize(h->stream));
-    CK(cudaMemcpy(energies, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost));
+    CK(scopy(h, energies, h->A.energy, sizeof(double) * (5 * h->nmat + 3), cudaMemcpyDeviceToHost));
     return MCM_OK;
 }
 
@@ -1355,7 +1366,7 @@ int mcm_gpu_skin_builds(mcm_gpu_handle *h, long long *builds) {
     if (h->A.prm.skin <= 0.0) return MCM_OK;
     CK(cudaStreamSynchronize(h->stream));
     int flags[3] = {0, 0, 0};
-    CK(cudaMemcpy(flags, h->A.skin_flags, sizeof(flags), cudaMemcpyDeviceToHost));
+    CK(scopy(h, flags, h->A.skin_flags, sizeof(flags), cudaMemcpyDeviceToHost));
     *builds = flags[2];
     return MCM_OK;
 }
@@ -1366,19 +1377,19 @@ int mcm_gpu_stats(mcm_gpu_handle *h, double *mean_nbr, int *max_nbr, int *stride
     CK(cudaStreamSynchronize(h->stream));
     if (mean_nbr) {
         std::vector<int> cnt(h->np), gcnt(h->np);
-        CK(cudaMemcpy(cnt.data(), h->A.nnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(gcnt.data(), h->A.gnnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+        CK(scopy(h, cnt.data(), h->A.nnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
+        CK(scopy(h, gcnt.data(), h->A.gnnbr, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
         double s = 0.0;
         for (int p = 0; p < h->np; ++p) s += cnt[p] + gcnt[p];
         *mean_nbr = s / h->np;
     }
     if (max_nbr) {
         DevStatus s;
-        CK(cudaMemcpy(&s, h->A.status, sizeof(s), cudaMemcpyDeviceToHost));
+        CK(scopy(h, &s, h->A.status, sizeof(s), cudaMemcpyDeviceToHost));
         *max_nbr = s.max_nbr;
     }
     if (stride) *stride = h->A.nstride;
-    if (ngp) CK(cudaMemcpy(ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ngp) CK(scopy(h, ngp, h->A.ngp, sizeof(int), cudaMemcpyDeviceToHost));
     return MCM_OK;
 }
 
@@ -1731,7 +1742,7 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     if (!h->d_theta && (st = dalloc(h, &h->d_theta, (size_t)h->nmat * adj::kParams))) return st;
     CK(cudaMemsetAsync(h->d_theta, 0, sizeof(double) * h->nmat * adj::kParams, h->stream));
     std::vector<int> orig(n);
-    CK(cudaMemcpy(orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(scopy(h, orig.data(), h->A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost));
     adj::AdjArgs b;
     std::memset(&b, 0, sizeof(b));
     double *base = h->d_adj;
@@ -1751,11 +1762,11 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     for (int d = 0; d < 3; ++d) {
         if (xbar) {
             for (int i = 0; i < n; ++i) tmp[i] = xbar[3 * (size_t)orig[i] + d];
-            CK(cudaMemcpy(b.xb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+            CK(scopy(h, b.xb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
         }
         if (vbar) {
             for (int i = 0; i < n; ++i) tmp[i] = vbar[3 * (size_t)orig[i] + d];
-            CK(cudaMemcpy(b.vb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+            CK(scopy(h, b.vb[d], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
         }
     }
     const int every = h->adj_every, nck = (int)h->adj_ckpt.size();
@@ -1807,15 +1818,15 @@ int mcm_gpu_adjoint_backward(mcm_gpu_handle *h, const double *xbar, const double
     CK(cudaStreamSynchronize(h->stream));
     for (int d = 0; d < 3; ++d) {
         if (xbar0) {
-            CK(cudaMemcpy(tmp.data(), b.xb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
+            CK(scopy(h, tmp.data(), b.xb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
             for (int i = 0; i < n; ++i) xbar0[3 * (size_t)orig[i] + d] = tmp[i];
         }
         if (vbar0) {
-            CK(cudaMemcpy(tmp.data(), b.vb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
+            CK(scopy(h, tmp.data(), b.vb[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
             for (int i = 0; i < n; ++i) vbar0[3 * (size_t)orig[i] + d] = tmp[i];
         }
     }
-    if (param_bar) CK(cudaMemcpy(param_bar, h->d_theta, sizeof(double) * h->nmat * adj::kParams, cudaMemcpyDeviceToHost));
+    if (param_bar) CK(scopy(h, param_bar, h->d_theta, sizeof(double) * h->nmat * adj::kParams, cudaMemcpyDeviceToHost));
     // leave the device state as the forward run left it
     if ((st = snap_load(h, h->adj_final))) return st;
     CK(cudaStreamSynchronize(h->stream));
