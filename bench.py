@@ -88,6 +88,18 @@ def parse():
     return ap.parse_args()
 
 
+def device_clean(label: str) -> None:
+    """Raises if a device error is pending before the leg `label` starts (an
+    asynchronous fault of an earlier leg would otherwise surface in the next
+    leg's first synchronising call)."""
+    import torch
+
+    try:
+        torch.cuda.synchronize()
+    except Exception as exc:
+        raise RuntimeError(f"device error pending before {label}: {exc}") from exc
+
+
 def dist_env():
     return ranks.dist_env()
 
@@ -749,14 +761,17 @@ def gpu_arm(args):
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:
+        device_clean("the adjoint")
         adjoint = adjoint_cost(args, local)
 
     fluid = None
     if rank == 0 and args.fluid_steps > 0:
+        device_clean("the fluid column")
         fluid = fluid_column_cost(args, local)
 
     longrun = None
     if rank == 0 and args.long_steps > 0 and args.precision == "mixed":
+        device_clean("the long run")
         longrun = long_run(args, local)
 
     cpu = None

@@ -80,7 +80,8 @@ inline int set_error(mcm_gpu_handle *h, int code, const std::string &msg) {
         cudaError_t e_ = (call);                                                                   \
         if (e_ != cudaSuccess)                                                                     \
             return set_error(h, e_ == cudaErrorMemoryAllocation ? MCM_ENOMEM : MCM_ECUDA,          \
-                             std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+                             std::string(#call) + " (" + __FILE__ + ":" + std::to_string(__LINE__) +   \
+                                 "): " + cudaGetErrorString(e_));                                  \
     } while (0)
 
 template <typename T>
