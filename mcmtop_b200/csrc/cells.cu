@@ -286,22 +286,7 @@ __global__ void __launch_bounds__(256) k_cell_sort(StepArgs a) {
         const int s = a.cell_start[c], e = a.cell_start[c + 1];
         const int n = e - s;
         if (n < 2) continue;   // warp-uniform
-        if (n <= 32) {
-            // one particle per lane (the common case)
-            const bool on = lane < n;
-            const int v = on ? a.cell_list[s + lane] : 0;
-            const int o = on ? a.F.orig[v] : 0;
-            const double x = (on && xs) ? X[v] : 0.0;
-            int rank = 0;
-            for (int k = 0; k < n; ++k) {
-                const double xb = __shfl_sync(0xffffffffu, x, k);
-                const int ob = __shfl_sync(0xffffffffu, o, k);
-                rank += cell_before(xs, xb, ob, x, o) ? 1 : 0;
-            }
-            __syncwarp();
-            if (on) a.cell_list[s + rank] = v;
-            __syncwarp();
-        } else if (n <= 32 * kSortPer) {
+        if (n <= 32 * kSortPer) {
             int v[kSortPer], o[kSortPer], rank[kSortPer];
             double x[kSortPer];
 #pragma unroll
