@@ -89,7 +89,7 @@ def parse():
 
 
 def device_clean(label: str) -> None:
-    """Raises if a device error is pending before the leg `label` starts (an
+    """Raises if a device error is pending at the point `label` (an
     asynchronous fault of an earlier leg would otherwise surface in the next
     leg's first synchronising call)."""
     import torch
@@ -97,7 +97,7 @@ def device_clean(label: str) -> None:
     try:
         torch.cuda.synchronize()
     except Exception as exc:
-        raise RuntimeError(f"device error pending before {label}: {exc}") from exc
+        raise RuntimeError(f"device error pending at {label}: {exc}") from exc
 
 
 def dist_env():
@@ -527,6 +527,7 @@ def long_run(args, local):
         sols[name] = Solver(deck, prec, device=local, reorder_interval=args.reorder,
                             nbr_skin=args.skin if prec != _abi.PREC_FP64_EXACT else 0.0, compensated=args.compensated)
         sols[name].set_diagnostics(False)
+        device_clean(f"the end of the long run's {name} handle set-up")
     ms = {name: 0.0 for name in runs}
     growth = []
     done = 0
@@ -634,6 +635,7 @@ def gpu_arm(args):
     sol.profile(False)
     if done != args.steps:
         raise RuntimeError(f"run stopped after {done} of {args.steps} steps")
+    device_clean("the end of the timed run")
     ms_max = max_over_ranks(ms, f"cuda:{local}")
     value = job_rate(deck.np * args.steps, ws, ms_max)
 
@@ -688,6 +690,7 @@ def gpu_arm(args):
                         "worst": float(f"{max(err.values()):.3e}"),
                         "length_rel_diff": float(f"{abs(la - lb) / lb:.3e}")}
         ref.close()
+        device_clean("the end of the FP64-fast comparison")
         # the plain FP64 step: the reference's expressions and summation order,
         # no fused multiply-add, one thread per particle (MCM_PREC_FP64_EXACT)
         ex = Solver(deck, _abi.PREC_FP64_EXACT, device=local, reorder_interval=args.reorder)
@@ -700,6 +703,7 @@ def gpu_arm(args):
         done_ex = ex.run(args.steps)
         ms_ex = max_over_ranks(ex.timer_stop(), f"cuda:{local}")
         ex.close()
+        device_clean("the end of the plain FP64 comparison")
         if done_ex != args.steps:
             raise RuntimeError(f"FP64-exact run stopped after {done_ex} of {args.steps} steps")
         v_ex = job_rate(deck.np * args.steps, ws, ms_ex)
@@ -761,17 +765,17 @@ def gpu_arm(args):
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:
-        device_clean("the adjoint")
+        device_clean("the start of the adjoint leg")
         adjoint = adjoint_cost(args, local)
 
     fluid = None
     if rank == 0 and args.fluid_steps > 0:
-        device_clean("the fluid column")
+        device_clean("the start of the fluid-column leg")
         fluid = fluid_column_cost(args, local)
 
     longrun = None
     if rank == 0 and args.long_steps > 0 and args.precision == "mixed":
-        device_clean("the long run")
+        device_clean("the start of the long run")
         longrun = long_run(args, local)
 
     cpu = None
