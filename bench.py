@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--oracle-check-steps", type=int, default=50,
                     help="oracle steps on the full bar for the GPU accuracy spot check")
     ap.add_argument("--reorder", type=int, default=20, help="steps between particle re-sorts")
+    ap.add_argument("--long-only", type=int, default=-1, metavar="DEVICE",
+                    help="run only the long accuracy run on this device and print its JSON (the child process "
+                         "that the long-run leg starts)")
     ap.add_argument("--search-kind", type=int, default=0, choices=[0, 1, 2, 3],
                     help="neighbour search: 1 one thread per particle, 2 one warp per particle, 3 one warp per cell (0: default)")
     return ap.parse_args()
@@ -776,7 +779,7 @@ def gpu_arm(args):
     longrun = None
     if rank == 0 and args.long_steps > 0 and args.precision == "mixed":
         device_clean("the start of the long run")
-        longrun = long_run(args, local)
+        longrun = long_run_in_child(args, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -839,8 +842,31 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def long_run_in_child(args, local):
+    """long_run in a process of its own, on the same GPU.  In one process,
+    after the earlier legs had created and destroyed some hundreds of handles,
+    the set-up of the long run's handles met an illegal memory access whose
+    cause is not found; a fresh process (a fresh CUDA context) keeps that
+    history away from the long run, and a failure of the child is recorded in
+    the line instead of ending the whole measurement."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--long-only", str(local), "--dx", repr(args.dx),
+           "--long-steps", str(args.long_steps), "--long-every", str(args.long_every), "--reorder", str(args.reorder),
+           "--skin", repr(args.skin)] + (["--compensated"] if args.compensated else [])
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = " | ".join(r.stderr.strip().splitlines()[-3:])
+        return {"error": f"long run child exited {r.returncode}: {tail}"}
+    out = json.loads(lines[-1])
+    out["process"] = "child (own CUDA context)"
+    return out
+
+
 def main():
     args = parse()
+    if args.long_only >= 0:
+        print(json.dumps(long_run(args, args.long_only)))
+        return
     if args.impl == "reference":
         reference_arm(args)
     else:

@@ -228,3 +228,40 @@ def test_mixed_fluid_column_long_run(lib):
     assert np.array_equal(nn, orc.get_int("nnbr"))
     for i in range(0, deck.np, 11):
         assert np.array_equal(np.sort(nbr[i, : nn[i]]), np.sort(orc.nbrlist(i + 1)))
+
+
+def test_mixed_search_lists_without_diagnostics(lib):
+    """With diagnostics off (one material, tcrit_opt 1) the mixed step's search
+    takes its windowed loop whose accept path is a predicated store; with
+    diagnostics on (FP64 minimum distances) it takes the branching loop.  The two must build the same lists, entry for entry, and
+    the sets must be the oracle's, on the bar, on the fluid column (ghost
+    walls, ghosts of ghosts) and on a bar with variable h, with the storage
+    re-sorted every three steps."""
+    decks = (taylor_bar(dx=0.4e-3), fluid_column(dx=0.01, block=(0.1, 0.06, 0.2), box=(0.4, 0.06, 0.3)),
+             taylor_bar(dx=0.8e-3).replace(h_opt=2))   # h varies after the first step
+    for deck in decks:
+        a = Solver(deck, _abi.PREC_MIXED, reorder_interval=3)
+        b = Solver(deck, _abi.PREC_MIXED, reorder_interval=3)
+        a.set_diagnostics(False)
+        b.set_diagnostics(True)
+        # with variable h the mixed densities move h off the oracle's by FP32
+        # amounts, so only the two GPU walks are compared there
+        orc = Oracle(deck, openmp=True) if not deck.h_opt else None
+        for _ in range(7):
+            a.step()
+            b.step()
+            if orc:
+                orc.step()
+            na, la, gna, gla = a.neighbours()
+            nb, lb, gnb, glb = b.neighbours()
+            assert np.array_equal(na, nb) and np.array_equal(gna, gnb)
+            w = int(na.max())
+            m = np.arange(w)[None, :] < na[:, None]
+            assert np.array_equal(la[:, :w][m], lb[:, :w][m])
+        if orc:
+            compare_neighbours(a, orc)
+            orc.close()
+        for f in STATE:
+            assert np.array_equal(a.download([f])[f], b.download([f])[f]), f
+        a.close()
+        b.close()
