@@ -105,7 +105,11 @@ __global__ void k_cell_keys(StepArgs a) {
         }
         int key = in ? (int)cell_key(box[0], box[1], box[2], g.gridlim) : kNoCell;
         a.key[i] = key;
-        if (key >= 0) atomicAdd(&a.cell_count[key], 1);
+        // lanes of one cell add their count once (the particles are mostly in
+        // cell order, so a warp holds few distinct cells)
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, key);
+        if (key >= 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&a.cell_count[key], __popc(grp));
     }
 }
 
@@ -207,11 +211,19 @@ __global__ void k_cell_scatter(StepArgs a) {
     const int base_out = a.cell_start[a.grid->ncells];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         int key = a.key[i];
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, key);
         if (key < 0) {
             a.cell_list[base_out + atomicAdd(a.n_inside, 1)] = i;
             continue;
         }
-        int slot = atomicSub(&a.cell_count[key], 1) - 1;
+        // one atomic per cell and warp: the group's slots are the n below the
+        // returned count, one per lane in lane order
+        const int lane = threadIdx.x & 31, lead = __ffs(grp) - 1;
+        int top = 0;
+        if (lane == lead) top = atomicSub(&a.cell_count[key], __popc(grp));
+        top = __shfl_sync(grp, top, lead);
+        int slot = top - 1 - __popc(grp & ((1u << lane) - 1u));
         a.cell_list[a.cell_start[key] + slot] = i;
     }
 }
@@ -266,11 +278,12 @@ __global__ void __launch_bounds__(256) k_cell_records(StepArgs a) {
 // reference's lists.  With xsort (steps whose sums do not follow that order)
 // ascending x, ties by descending reference index: a row of x-adjacent cells
 // is then one x-sorted range, which the search windows in x.
-// One warp per cell: each lane takes up to kSortPer of the cell's particles
-// and counts how many of the cell's particles come before each (a rank sort:
-// the order is total, so the ranks are a permutation); all ranks are known
-// before any entry is written back.  Cells of more than 32 * kSortPer
-// particles are sorted by insertion in one lane.
+// One warp per cell: each lane takes one of the cell's particles (cells of up
+// to 32, the common case) or up to kSortPer of them, and counts how many of
+// the cell's particles come before each (a rank sort: the order is total, so
+// the ranks are a permutation); all ranks are known before any entry is
+// written back.  Cells of more than 32 * kSortPer particles are sorted by
+// insertion in one lane.
 constexpr int kSortPer = 4;
 __device__ __forceinline__ bool cell_before(bool xs, double xa, int oa, double xb, int ob) {
     return xs ? (xa < xb || (xa == xb && oa > ob)) : oa > ob;
@@ -286,7 +299,22 @@ __global__ void __launch_bounds__(256) k_cell_sort(StepArgs a) {
         const int s = a.cell_start[c], e = a.cell_start[c + 1];
         const int n = e - s;
         if (n < 2) continue;   // warp-uniform
-        if (n <= 32 * kSortPer) {
+        if (n <= 32) {
+            // one particle per lane (the common case)
+            const bool on = lane < n;
+            const int v = on ? a.cell_list[s + lane] : 0;
+            const int o = on ? a.F.orig[v] : 0;
+            const double x = (on && xs) ? X[v] : 0.0;
+            int rank = 0;
+            for (int k = 0; k < n; ++k) {
+                const double xb = __shfl_sync(0xffffffffu, x, k);
+                const int ob = __shfl_sync(0xffffffffu, o, k);
+                rank += cell_before(xs, xb, ob, x, o) ? 1 : 0;
+            }
+            __syncwarp();
+            if (on) a.cell_list[s + rank] = v;
+            __syncwarp();
+        } else if (n <= 32 * kSortPer) {
             int v[kSortPer], o[kSortPer], rank[kSortPer];
             double x[kSortPer];
 #pragma unroll
