@@ -665,6 +665,12 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
         // (a second walk), and form the contact list otherwise (the same walk,
         // each list in walk order)
         unsigned *cout = contact ? a.cidx + (size_t)t * a.cstride : nullptr;
+        // Windowed common case: accepted entries collect in four registers and
+        // leave as one 16-byte store per four (t's row starts at t * cap
+        // entries, cap a multiple of 4), so a warp's lanes, whose rows lie cap
+        // entries apart, send a quarter of the scattered store requests.
+        const bool vec = (cap & 3) == 0;
+        unsigned b0 = 0u, b1 = 0u, b2 = 0u, b3 = 0u;
 #pragma unroll 1
         for (int pass = 0; pass < (two_pass ? 2 : 1); ++pass) {
             for (int nz = lo2; nz <= hi2; ++nz) {
@@ -721,9 +727,16 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                                 const double hs = __dadd_rn(cd.w, xi.w);
                                 in = exact_d2(xi, cd) < __dmul_rn(hs, hs);
                             }
-                            const unsigned code = (code_yz + (p < s1 ? 0u : (p >= s2 ? 2u : 1u))) << 26;
-                            if (in && nn < cap) out[nn] = (unsigned)p | code;
-                            nn += in ? 1 : 0;
+                            const unsigned entry = (unsigned)p | ((code_yz + (p < s1 ? 0u : (p >= s2 ? 2u : 1u))) << 26);
+                            if (vec) {
+                                if (in) { b0 = b1; b1 = b2; b2 = b3; b3 = entry; }
+                                nn += in ? 1 : 0;
+                                if (in && (nn & 3) == 0 && nn <= cap)
+                                    *reinterpret_cast<uint4 *>(out + (nn - 4)) = make_uint4(b0, b1, b2, b3);
+                            } else {
+                                if (in && nn < cap) out[nn] = entry;
+                                nn += in ? 1 : 0;
+                            }
                         }
                     } else {
                     for (int p = pb; p < pe; ++p) {
@@ -760,6 +773,15 @@ __global__ void __launch_bounds__(256, 4) k_search(StepArgs a) {
                     }
                     }
                 }
+            }
+        }
+        if constexpr (xwin && !contact && !two_pass && !want_mind) {
+            if (vec) {
+                // the last nn % 4 accepted entries are still in b(4 - nn % 4) .. b3
+                const int r = nn & 3;
+                if (r >= 3 && nn - 3 < cap) out[nn - 3] = b1;
+                if (r >= 2 && nn - 2 < cap) out[nn - 2] = b2;
+                if (r >= 1 && nn - 1 < cap) out[nn - 1] = b3;
             }
         }
         if (nn > cap) {

@@ -176,6 +176,30 @@ __global__ void k_strain_prep(StepArgs a) {
 #endif
 constexpr int kUnroll = MCM_STRAIN_UNROLL;
 
+// The list entries base[0 .. 2U) of one particle's two lanes, lane l getting
+// entries l, l + 2, ..., l + 2(U - 1) (list order within the lane): each lane
+// loads U consecutive entries in 16-byte pieces and the two lanes swap the
+// halves the other needs.  A warp's index loads touch 16 rows of the table
+// (one per particle), so fewer, wider loads mean fewer L1 wavefronts.  base
+// is 16-byte aligned (rows start at multiples of 4 entries); both lanes of
+// the pair call this together.
+template <int U>
+__device__ __forceinline__ void pair_entries(const unsigned *base, int lane, unsigned (&e)[U]) {
+    static_assert(L == 2 && U % 4 == 0, "two lanes per particle, 4 entries per 16-byte load");
+    const unsigned pm = 3u << (threadIdx.x & 30);
+#pragma unroll
+    for (int v = 0; v < U / 4; ++v) {
+        // lane 0 loads entries 8v .. 8v+3, lane 1 entries 8v+4 .. 8v+7
+        const uint4 w = __ldg(reinterpret_cast<const uint4 *>(base + 8 * v + 4 * lane));
+        const unsigned r0 = __shfl_xor_sync(pm, lane ? w.x : w.y, 1);
+        const unsigned r1 = __shfl_xor_sync(pm, lane ? w.z : w.w, 1);
+        e[4 * v + 0] = lane ? r0 : w.x;
+        e[4 * v + 1] = lane ? r1 : w.z;
+        e[4 * v + 2] = lane ? w.y : r0;
+        e[4 * v + 3] = lane ? w.w : r1;
+    }
+}
+
 // One pair's terms of MCM/mcm_oldstrain.f90:42-53: V_j (v_j - v_i)_n dW/dx_m
 // added to gv[3n + m] (KAHAN: compensated, the low parts in gc).
 template <bool KAHAN>
@@ -240,10 +264,9 @@ __global__ void __launch_bounds__(256, 3) k_strain(StepArgs a) {
         // records loaded before any is used, so that several gathers are in
         // flight), then the rest; each lane adds its terms in list order
         int k = lane;
-        for (; k + (kUnroll - 1) * L < nreal; k += kUnroll * L) {
+        for (; k - lane + kUnroll * L <= nreal; k += kUnroll * L) {
             unsigned e[kUnroll];
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) e[u] = spos[k + u * L];
+            pair_entries<kUnroll>(spos + (k - lane), lane, e);
             Rec8 r[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) r[u] = ld_rec8(a.frec0 + 2 * (size_t)(e[u] & kPosMask));
@@ -673,6 +696,25 @@ __global__ void __launch_bounds__(STAGED ? kStageThreads : 256, STAGED ? 4 : MCM
         float acc[3] = {0.0f, 0.0f, 0.0f}, comp[3] = {0.0f, 0.0f, 0.0f};
         int k0 = lane;
         if (!STAGED && !asym) {
+            // the list entries 8 at a time per particle (4 per lane, in 16-byte
+            // loads shared by the two lanes), the records one neighbour at a
+            // time; each lane's terms in list order
+            for (; k0 - lane + 4 * L <= nreal; k0 += 4 * L) {
+                unsigned e[4];
+                pair_entries<4>(spos + (k0 - lane), lane, e);
+#pragma unroll 1
+                for (int u = 0; u < 4; ++u) {
+                    const size_t p = e[0] & kPosMask;
+                    const float4 o = offs[e[0] >> 26];
+                    const Rec8 r = ld_rec8(a.frec0 + 2 * p);
+                    const float4 q2 = ld_rec4(mom_tail(a) + p);
+                    momentum_term<KAHAN>((xi.x - r.a.x) - o.x, (xi.y - r.a.y) - o.y, (xi.z - r.a.z) - o.z, r.a.w,
+                                         r.b, q2, xi.w, ihi, r1i, r2i, acc, comp);
+                    e[0] = e[1];
+                    e[1] = e[2];
+                    e[2] = e[3];
+                }
+            }
             // real neighbours kUnrollM at a time per lane, loads first (as in
             // k_strain); the terms are added in list order
             for (; k0 + (kUnrollM - 1) * L < nreal; k0 += kUnrollM * L) {
